@@ -1,0 +1,102 @@
+/*
+ * joe_b200.h -- C ABI of the B200 implicit finite-volume library (libjoe_b200.so).
+ *
+ * Drop-in for the implicit iteration of the Joe RANS solver (MUM suite):
+ * the host keeps the reference's mesh objects (Ugp / UgpWithCv) and hands
+ * their arrays, in the reference's own layouts, to these entry points.
+ * Every call returns an int status (JG_OK == 0, < 0 on error; the
+ * reference's `throw(-1)`), never throws across the ABI, and never reads
+ * host memory after it returns.  A handle is used by one thread at a time;
+ * distinct handles run concurrently on their own CUDA streams.
+ *
+ * Layouts (all host arrays, caller-owned, reference order):
+ *   cvofa[nfa][2]            boundary faces first (cvofa[f][1] == -1), zones contiguous
+ *   faocv_i[ncv+1]/faocv_v   faces of a cell, CSR
+ *   nbocv_i[ncv+1]/nbocv_v   cell neighbours, CSR, diagonal first
+ *   x_cv[ncv][3], cv_volume[ncv], x_fa[nfa][3], fa_normal[nfa][3] (area-weighted,
+ *   pointing from cvofa[f][0] to cvofa[f][1])
+ *   nbocv_lsg_coeff[nbocv_s][3], boundary_fa_lsg_coeff[nfa_b][3]
+ *   rho[ncv], rhou[ncv][3], rhoE[ncv]
+ *   A[nbocv_s][5][5] (block CSR over nbocv), rhs/dq[ncv][5]
+ */
+#ifndef JOE_B200_H
+#define JOE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JG_OK 0
+#define JG_ERR_ARG (-1)       /* bad argument / unsupported option */
+#define JG_ERR_CUDA (-2)      /* CUDA runtime error (message: jg_last_error) */
+#define JG_ERR_NOMEM (-3)     /* device allocation failed */
+#define JG_ERR_STATE (-4)     /* non-physical state (NaN, rho<=0) detected */
+#define JG_ERR_NODEVICE (-5)  /* no CUDA device */
+
+/* boundary kinds: setBC, src/joe/JoeWithModels.cpp:3857-4300 */
+enum {
+  JG_BC_SYMMETRY = 1,             /* v: -                                   */
+  JG_BC_WALL = 2,                 /* v[0] = wall T (<= 0: adiabatic)         */
+  JG_BC_CBC = 3,                  /* v[0..2] = u, v[3] = T, v[4] = p         */
+  JG_BC_CBC_SUBSONIC_INLET = 4,   /* v[0..2] = flow direction, v[3] = Ttot, v[4] = ptot */
+  JG_BC_CBC_SUBSONIC_OUTLET = 5,  /* v[0] = p                                */
+  JG_BC_NEUMANN = 6,              /* v: -                                    */
+  JG_BC_FARFIELD = 7              /* v[0..2] = u, v[3] = p, v[4] = rho, v[5] = gamma */
+};
+enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2 };
+enum { JG_MU_POWERLAW = 0, JG_MU_SUTHERLAND = 1 };
+enum { JG_SYMM_ORIGINAL_NUMERIC = 0, JG_SYMM_NEW_NUMERIC = 1, JG_SYMM_ANALYTICAL = 2 };
+enum { JG_TS_CFL = 0, JG_TS_CFL_MIN = 1, JG_TS_DT = 2 };
+enum { JG_DT_MAX_BASED = 0, JG_DT_SUM_BASED = 1 };
+/* linear solvers: BCGSTAB and LUSGS follow the reference (UgpWithCv.cpp:2660, 3172);
+ * JACOBI / SGS are block point relaxation (fixed sweep count) */
+enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3 };
+enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
+
+typedef struct jg_zone {
+  int ifa_f, ifa_l;   /* inclusive boundary-face range */
+  int kind;           /* JG_BC_* */
+  int pad;
+  double v[8];        /* parameters, see JG_BC_* */
+} jg_zone;
+
+typedef struct jg_mesh {
+  int ncv, nfa, nfa_b, nbocv_s, nzones;
+  const int *cvofa;
+  const int *faocv_i, *faocv_v;
+  const int *nbocv_i, *nbocv_v;
+  const double *x_cv, *x_fa, *fa_normal, *cv_volume;
+  const double *nbocv_lsg_coeff, *boundary_fa_lsg_coeff;
+  const jg_zone *zones;
+} jg_mesh;
+
+/* Input-file keys of the hot path (UgpWithCvCompFlow.h:57-502, JoeWithModels.cpp:881-924). */
+typedef struct jg_params {
+  double gamma;        /* GAMMA */
+  double R_gas;        /* P_REF / RHO_REF / T_REF */
+  double Pr, PrTurb;   /* PR, PRTURB */
+  int mu_mode;         /* MU_MODE: JG_MU_* (used when mu_ref > 0) */
+  int flux;            /* SPACE_INTEGRATION: JG_FLUX_* */
+  double mu_ref, mu_power_law, SL_Tref, SL_Sref, T_ref;
+  int second_order;    /* SPATIAL_SECOND_ORDER */
+  int limiter;         /* GRAD_RECONSTRUCTION LIMITER=YES */
+  double eps;          /* GRAD_RECONSTRUCTION EPS */
+  int visc_limiter;    /* VISC_LIMITER */
+  int symm_bc;         /* SYMM_BC: JG_SYMM_* */
+  int time_step_mode;  /* JG_TS_* */
+  int time_step;       /* TIME_STEP: JG_DT_* */
+  double cfl, dt;      /* CFL (or CFL_MIN) and DT */
+  int cfl_after, cfl_interval;   /* CFL_RAMP AFTER_ITER, INTERVAL_ITER */
+  double cfl_factor, cfl_max;    /* CFL_RAMP FACTOR_CFL, MAX_CFL */
+  double under_relax;  /* UNDER_RELAXATION */
+  int lin_solver;      /* LINEAR_SOLVER_NS: JG_LS_* */
+  int ls_max_iter;     /* LINEAR_SOLVER_NS_TRESHOLDS MAX_ITER (BCGSTAB) or sweeps (JACOBI/SGS) */
+  double ls_abs, ls_rel;
+  int precision;       /* JG_PREC_* */
+  int nscal;           /* transported scalars (0: laminar / inviscid) */
+} jg_params;
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JOE_B200_H */

@@ -1,0 +1,137 @@
+"""ctypes mirror of the structs in include/joe_b200.h and converters from
+the Python-side case description (``case.JoeParams`` + a control-volume
+mesh in the reference's layout)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .case import BC_KINDS, FLUX_KINDS, SOLVER_KINDS, SYMM_BC_KINDS, JoeParams
+
+
+class jg_zone(C.Structure):
+    _fields_ = [("ifa_f", C.c_int), ("ifa_l", C.c_int), ("kind", C.c_int), ("pad", C.c_int),
+                ("v", C.c_double * 8)]
+
+
+class jg_mesh(C.Structure):
+    _fields_ = [("ncv", C.c_int), ("nfa", C.c_int), ("nfa_b", C.c_int), ("nbocv_s", C.c_int),
+                ("nzones", C.c_int),
+                ("cvofa", C.POINTER(C.c_int)),
+                ("faocv_i", C.POINTER(C.c_int)), ("faocv_v", C.POINTER(C.c_int)),
+                ("nbocv_i", C.POINTER(C.c_int)), ("nbocv_v", C.POINTER(C.c_int)),
+                ("x_cv", C.POINTER(C.c_double)), ("x_fa", C.POINTER(C.c_double)),
+                ("fa_normal", C.POINTER(C.c_double)), ("cv_volume", C.POINTER(C.c_double)),
+                ("nbocv_lsg_coeff", C.POINTER(C.c_double)),
+                ("boundary_fa_lsg_coeff", C.POINTER(C.c_double)),
+                ("zones", C.POINTER(jg_zone))]
+
+
+class jg_params(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("R_gas", C.c_double), ("Pr", C.c_double), ("PrTurb", C.c_double),
+                ("mu_mode", C.c_int), ("flux", C.c_int),
+                ("mu_ref", C.c_double), ("mu_power_law", C.c_double), ("SL_Tref", C.c_double),
+                ("SL_Sref", C.c_double), ("T_ref", C.c_double),
+                ("second_order", C.c_int), ("limiter", C.c_int), ("eps", C.c_double),
+                ("visc_limiter", C.c_int), ("symm_bc", C.c_int),
+                ("time_step_mode", C.c_int), ("time_step", C.c_int),
+                ("cfl", C.c_double), ("dt", C.c_double),
+                ("cfl_after", C.c_int), ("cfl_interval", C.c_int),
+                ("cfl_factor", C.c_double), ("cfl_max", C.c_double),
+                ("under_relax", C.c_double),
+                ("lin_solver", C.c_int), ("ls_max_iter", C.c_int),
+                ("ls_abs", C.c_double), ("ls_rel", C.c_double),
+                ("precision", C.c_int), ("nscal", C.c_int)]
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def make_params(p: JoeParams, precision: int = 0) -> jg_params:
+    q = jg_params()
+    q.gamma = p.GAMMA
+    q.R_gas = p.R_gas
+    q.Pr = p.PR
+    q.PrTurb = p.PRTURB
+    q.mu_mode = 1 if p.MU_MODE == "SUTHERLAND" else 0
+    q.flux = FLUX_KINDS[p.SPACE_INTEGRATION]
+    q.mu_ref = p.MU_REF
+    q.mu_power_law = p.MU_POWER_LAW
+    q.SL_Tref = p.SL_TREF
+    q.SL_Sref = p.SL_SREF
+    q.T_ref = p.T_REF
+    q.second_order = int(p.SECOND_ORDER)
+    q.limiter = int(p.LIMITER)
+    q.eps = p.EPS
+    q.visc_limiter = int(p.VISC_LIMITER)
+    q.symm_bc = SYMM_BC_KINDS[p.SYMM_BC]
+    q.time_step_mode = 0
+    q.time_step = 0 if p.TIME_STEP == "MAX_BASED" else 1
+    q.cfl = p.CFL
+    q.dt = 0.0
+    q.cfl_after, q.cfl_interval, q.cfl_factor, q.cfl_max = p.CFL_RAMP
+    q.under_relax = p.UNDER_RELAXATION
+    q.lin_solver = SOLVER_KINDS[p.LINEAR_SOLVER_NS]
+    q.ls_max_iter = p.LS_MAX_ITER
+    q.ls_abs = p.LS_ABS_RESID
+    q.ls_rel = p.LS_REL_RESID
+    q.precision = precision
+    q.nscal = 0
+    return q
+
+
+class MeshArrays:
+    """Contiguous arrays (reference layout) + the jg_mesh struct over them.
+    ``src`` is a ``geometry.CvMesh`` or a dict of reference dumps."""
+
+    def __init__(self, src, params: JoeParams):
+        g = (lambda k: getattr(src, k)) if not isinstance(src, dict) else (lambda k: src[k])
+        self.ncv = int(g("ncv")) if not isinstance(src, dict) else int(src["meta"]["ncv"])
+        ii = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        dd = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        self.cvofa = ii(g("cvofa")).reshape(-1, 2)
+        self.nfa = self.cvofa.shape[0]
+        self.faocv_i, self.faocv_v = ii(g("faocv_i")), ii(g("faocv_v"))
+        self.nbocv_i, self.nbocv_v = ii(g("nbocv_i")), ii(g("nbocv_v"))
+        self.x_cv = dd(g("x_cv")).reshape(-1, 3)
+        self.x_fa = dd(g("x_fa")).reshape(-1, 3)
+        self.fa_normal = dd(g("fa_normal")).reshape(-1, 3)
+        self.cv_volume = dd(g("cv_volume"))
+        self.nbocv_lsg_coeff = dd(g("nbocv_lsg_coeff")).reshape(-1, 3)
+        self.boundary_fa_lsg_coeff = dd(g("boundary_fa_lsg_coeff")).reshape(-1, 3)
+        zones = src["meta"]["zones"] if isinstance(src, dict) else src.zones
+        self.nfa_b = int(src["meta"]["nfa_b"]) if isinstance(src, dict) else int(src.nfa_b)
+        self.zone_names = [z[0] for z in zones]
+        zarr = (jg_zone * max(1, len(zones)))()
+        for i, (name, f0, f1) in enumerate(zones):
+            bc = params.bcs[name]
+            zarr[i].ifa_f, zarr[i].ifa_l = f0, f1
+            zarr[i].kind = BC_KINDS[bc.kind]
+            vals = list(bc.values) + [0.0] * (8 - len(bc.values))
+            for k in range(8):
+                zarr[i].v[k] = vals[k]
+        self.zarr = zarr
+        m = jg_mesh()
+        m.ncv, m.nfa, m.nfa_b, m.nbocv_s, m.nzones = (self.ncv, self.nfa, self.nfa_b,
+                                                       self.nbocv_v.shape[0], len(zones))
+        m.cvofa = iptr(self.cvofa)
+        m.faocv_i, m.faocv_v = iptr(self.faocv_i), iptr(self.faocv_v)
+        m.nbocv_i, m.nbocv_v = iptr(self.nbocv_i), iptr(self.nbocv_v)
+        m.x_cv, m.x_fa, m.fa_normal = dptr(self.x_cv), dptr(self.x_fa), dptr(self.fa_normal)
+        m.cv_volume = dptr(self.cv_volume)
+        m.nbocv_lsg_coeff = dptr(self.nbocv_lsg_coeff)
+        m.boundary_fa_lsg_coeff = dptr(self.boundary_fa_lsg_coeff)
+        m.zones = C.cast(zarr, C.POINTER(jg_zone))
+        self.mesh = m
+
+    @property
+    def nbocv_s(self) -> int:
+        return int(self.nbocv_v.shape[0])

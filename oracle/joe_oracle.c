@@ -1,0 +1,1499 @@
+/*
+ * joe_oracle.c -- CPU restatement of the reference's implicit finite-volume
+ * iteration.  TEST INFRASTRUCTURE ONLY (the checker for libjoe_b200.so).
+ *
+ * Reference files cited below are paths inside the reference project:
+ *   src/joe/JoeWithModels.cpp, src/joe/UgpWithCvCompFlow.{h,cpp},
+ *   src/common/UgpWithCv.{h,cpp}, src/common/tc_vec3d.h
+ * Scope: the segregated Navier-Stokes path without transported scalars
+ * (inviscid or laminar), ideal gas, LSQ gradients, the smooth Barth-Jespersen
+ * limiter, HLLC / Roe / AUSM fluxes with their implicit matrices, the
+ * viscous flux, boundary conditions, local time step, BiCGSTAB / LU-SGS.
+ */
+#include "joe_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+struct jo_case {
+  jg_mesh m;
+  jg_params p;
+  int ncv, nfa, nfa_b, nbs;
+  double *rho, *rhou, *rhoE;
+  double *vel, *press, *temp, *enthalpy, *sos, *gam, *RoM;
+  double *rho_bfa, *T_bfa, *vel_bfa, *p_bfa, *h_bfa, *gam_bfa, *RoM_bfa;
+  double *mul_fa, *lamOcp_fa, *mut_fa;
+  double *grad_u, *grad_rho, *grad_p, *grad_h, *alpha_rho;
+  double *local_dt;
+  double cfl;
+  int step;
+  int dt_fixed_done;
+  double dt_fixed;
+};
+
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+static double dot3(const double *a, const double *b) {
+  /* vecDotVec3d, tc_vec3d.h:14-22 (sequential sum from 0.0) */
+  double d = 0.0;
+  for (int i = 0; i < 3; i++) d += a[i] * b[i];
+  return d;
+}
+static double norm3(double *n, const double *v) {
+  /* normVec3d(vNorm, v), tc_vec3d.h:36-46 */
+  double mag = sqrt(dot3(v, v));
+  for (int i = 0; i < 3; i++) n[i] = v[i] / mag;
+  return mag;
+}
+static double dmin(double a, double b) { return a < b ? a : b; }
+static double dmax(double a, double b) { return a > b ? a : b; }
+
+jo_case *jo_create(const jg_mesh *m, const jg_params *p) {
+  jo_case *h = (jo_case *)calloc(1, sizeof(jo_case));
+  h->m = *m;
+  h->p = *p;
+  h->ncv = m->ncv; h->nfa = m->nfa; h->nfa_b = m->nfa_b; h->nbs = m->nbocv_s;
+  int n = h->ncv, nf = h->nfa, nb = h->nfa_b;
+  h->rho = dalloc(n); h->rhou = dalloc(3 * n); h->rhoE = dalloc(n);
+  h->vel = dalloc(3 * n); h->press = dalloc(n); h->temp = dalloc(n); h->enthalpy = dalloc(n);
+  h->sos = dalloc(n); h->gam = dalloc(n); h->RoM = dalloc(n);
+  h->rho_bfa = dalloc(nb); h->T_bfa = dalloc(nb); h->vel_bfa = dalloc(3 * nb); h->p_bfa = dalloc(nb);
+  h->h_bfa = dalloc(nb); h->gam_bfa = dalloc(nb); h->RoM_bfa = dalloc(nb);
+  h->mul_fa = dalloc(nf); h->lamOcp_fa = dalloc(nf); h->mut_fa = dalloc(nf);
+  h->grad_u = dalloc(9 * n); h->grad_rho = dalloc(3 * n); h->grad_p = dalloc(3 * n);
+  h->grad_h = dalloc(3 * n); h->alpha_rho = dalloc(n); h->local_dt = dalloc(n);
+  /* initialHookScalarRansCombModel: RoM = R_gas, gamma = GAMMA (UgpWithCvCompFlow.h:1630-1640) */
+  for (int i = 0; i < n; i++) { h->gam[i] = p->gamma; h->RoM[i] = p->R_gas; }
+  h->cfl = p->cfl;
+  return h;
+}
+
+void jo_destroy(jo_case *h) {
+  if (!h) return;
+  double *arrs[] = {h->rho, h->rhou, h->rhoE, h->vel, h->press, h->temp, h->enthalpy, h->sos, h->gam, h->RoM,
+                    h->rho_bfa, h->T_bfa, h->vel_bfa, h->p_bfa, h->h_bfa, h->gam_bfa, h->RoM_bfa, h->mul_fa,
+                    h->lamOcp_fa, h->mut_fa, h->grad_u, h->grad_rho, h->grad_p, h->grad_h, h->alpha_rho,
+                    h->local_dt};
+  for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); i++) free(arrs[i]);
+  free(h);
+}
+
+void jo_set_state(jo_case *h, const double *rho, const double *rhou, const double *rhoE) {
+  memcpy(h->rho, rho, sizeof(double) * h->ncv);
+  memcpy(h->rhou, rhou, sizeof(double) * 3 * h->ncv);
+  memcpy(h->rhoE, rhoE, sizeof(double) * h->ncv);
+}
+
+void jo_get_state(jo_case *h, double *rho, double *rhou, double *rhoE) {
+  memcpy(rho, h->rho, sizeof(double) * h->ncv);
+  memcpy(rhou, h->rhou, sizeof(double) * 3 * h->ncv);
+  memcpy(rhoE, h->rhoE, sizeof(double) * h->ncv);
+}
+
+double *jo_array(jo_case *h, const char *name) {
+  struct { const char *n; double *p; } t[] = {
+      {"vel", h->vel}, {"press", h->press}, {"temp", h->temp}, {"enthalpy", h->enthalpy}, {"sos", h->sos},
+      {"rho_bfa", h->rho_bfa}, {"T_bfa", h->T_bfa}, {"vel_bfa", h->vel_bfa}, {"p_bfa", h->p_bfa},
+      {"h_bfa", h->h_bfa}, {"gam_bfa", h->gam_bfa}, {"RoM_bfa", h->RoM_bfa}, {"mul_fa", h->mul_fa},
+      {"lamOcp_fa", h->lamOcp_fa}, {"mut_fa", h->mut_fa}, {"grad_u", h->grad_u}, {"grad_rho", h->grad_rho},
+      {"grad_p", h->grad_p}, {"grad_enthalpy", h->grad_h}, {"alpha_rho", h->alpha_rho},
+      {"local_dt", h->local_dt}, {"rho", h->rho}, {"rhou", h->rhou}, {"rhoE", h->rhoE}};
+  for (size_t i = 0; i < sizeof(t) / sizeof(t[0]); i++)
+    if (strcmp(t[i].n, name) == 0) return t[i].p;
+  return NULL;
+}
+double jo_cfl(jo_case *h) { return h->cfl; }
+int jo_step_count(jo_case *h) { return h->step; }
+
+/* ------------------------------------------------------------------------ */
+/* thermodynamics                                                            */
+/* ------------------------------------------------------------------------ */
+
+static double mu_law(const jg_params *p, double T) {
+  /* calcMuLam / ComputeBCProperties_T, UgpWithCvCompFlow.h:1601-1621, 1796-1805 */
+  if (p->mu_mode == JG_MU_SUTHERLAND)
+    return p->mu_ref * pow(T / p->SL_Tref, 1.5) * (p->SL_Tref + p->SL_Sref) / (T + p->SL_Sref);
+  return p->mu_ref * pow(T / p->T_ref, p->mu_power_law);
+}
+
+/* calcStateVariables, UgpWithCvCompFlow.h:1662-1694 (no kine) */
+static void calc_state_variables(jo_case *h) {
+  for (int c = 0; c < h->ncv; c++) {
+    double r = h->rho[c];
+    double *ru = &h->rhou[3 * c];
+    for (int i = 0; i < 3; i++) h->vel[3 * c + i] = ru[i] / r;
+    double kinecv = 0.0;
+    double pr = (h->gam[c] - 1.0) * (h->rhoE[c] - 0.5 * dot3(ru, ru) / r - r * kinecv);
+    if (pr > 0.0) h->press[c] = pr;  /* negative pressure: keep the old value */
+    h->temp[c] = h->press[c] / (r * h->RoM[c]);
+    h->enthalpy[c] = h->gam[c] * h->RoM[c] / (h->gam[c] - 1.0) * h->temp[c];
+    h->sos[c] = sqrt(h->gam[c] * h->press[c] / r);
+  }
+}
+
+/* calcMaterialProperties, UgpWithCvCompFlow.h:1701-1753 (internal faces) */
+static void calc_material_properties(jo_case *h) {
+  const jg_params *p = &h->p;
+  if (!(p->mu_ref > 0.0)) return;
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = h->m.cvofa[2 * f], c1 = h->m.cvofa[2 * f + 1];
+    double dx0[3], dx1[3];
+    for (int i = 0; i < 3; i++) {
+      dx0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c0 + i];
+      dx1[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c1 + i];
+    }
+    double w0 = sqrt(dot3(dx0, dx0));
+    double w1 = sqrt(dot3(dx1, dx1));
+    double T = (w1 * h->temp[c0] + w0 * h->temp[c1]) / (w0 + w1);
+    h->mul_fa[f] = mu_law(p, T);
+    h->lamOcp_fa[f] = h->mul_fa[f] / p->Pr;
+  }
+}
+
+/* ComputeBCProperties_T, UgpWithCvCompFlow.h:1783-1812 */
+static void bc_props_T(jo_case *h, int f0, int f1) {
+  const jg_params *p = &h->p;
+  for (int f = f0; f <= f1; f++) {
+    h->gam_bfa[f] = p->gamma;
+    h->RoM_bfa[f] = p->R_gas;
+    h->h_bfa[f] = p->gamma * p->R_gas / (p->gamma - 1.0) * h->T_bfa[f];
+  }
+  if (p->mu_ref > 0.0)
+    for (int f = f0; f <= f1; f++) {
+      h->mul_fa[f] = mu_law(p, h->T_bfa[f]);
+      h->lamOcp_fa[f] = h->mul_fa[f] / p->Pr;
+    }
+}
+
+/* ComputeBCProperties_H, UgpWithCvCompFlow.h:1815-1839 */
+static void bc_props_H(jo_case *h, int f0, int f1) {
+  const jg_params *p = &h->p;
+  for (int f = f0; f <= f1; f++) {
+    h->gam_bfa[f] = p->gamma;
+    h->RoM_bfa[f] = p->R_gas;
+    h->T_bfa[f] = h->h_bfa[f] * (p->gamma - 1.0) / (p->gamma * p->R_gas);
+  }
+  if (p->mu_ref > 0.0)
+    for (int f = f0; f <= f1; f++) {
+      h->mul_fa[f] = mu_law(p, h->T_bfa[f]);
+      h->lamOcp_fa[f] = h->mul_fa[f] / p->Pr;
+    }
+}
+
+/* setBC, JoeWithModels.cpp:3857-4300 */
+static int set_bc(jo_case *h) {
+  const jg_params *p = &h->p;
+  for (int z = 0; z < h->m.nzones; z++) {
+    const jg_zone *zn = &h->m.zones[z];
+    int f0 = zn->ifa_f, f1 = zn->ifa_l;
+    const double *v = zn->v;
+    switch (zn->kind) {
+      case JG_BC_CBC: {
+        const double *u_bc = v; double T_bc = v[3], p_bc = v[4];
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          double nV[3];
+          norm3(nV, &h->m.fa_normal[3 * f]);
+          if (dot3(u_bc, nV) > 0.0) {
+            double un = dot3(&h->vel[3 * c0], nV);
+            double mach = fabs(un) / h->sos[c0];
+            h->T_bfa[f] = h->temp[c0];
+            for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = h->vel[3 * c0 + i];
+            h->p_bfa[f] = (mach >= 1.0) ? h->press[c0] : p_bc;
+          } else {
+            h->T_bfa[f] = T_bc;
+            for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = u_bc[i];
+            h->p_bfa[f] = p_bc;
+          }
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      case JG_BC_CBC_SUBSONIC_INLET: {
+        const double *ang = v; double Ttot = v[3], ptot = v[4];
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          double r = h->rho[c0];
+          double u[3] = {h->rhou[3 * c0] / r, h->rhou[3 * c0 + 1] / r, h->rhou[3 * c0 + 2] / r};
+          double vm = sqrt(dot3(u, u));
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = ang[i] * vm;
+          h->T_bfa[f] = Ttot;
+          h->p_bfa[f] = ptot;
+        }
+        bc_props_T(h, f0, f1);
+        for (int f = f0; f <= f1; f++) {
+          double w2 = dot3(&h->vel_bfa[3 * f], &h->vel_bfa[3 * f]);
+          h->h_bfa[f] -= 0.5 * w2;
+        }
+        bc_props_H(h, f0, f1);
+        for (int f = f0; f <= f1; f++)
+          h->p_bfa[f] = ptot * pow(h->T_bfa[f] / Ttot, h->gam_bfa[f] / (h->gam_bfa[f] - 1.0));
+      } break;
+      case JG_BC_CBC_SUBSONIC_OUTLET: {
+        double p_bc = v[0];
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          h->p_bfa[f] = p_bc;
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = h->rhou[3 * c0 + i] / h->rho[c0];
+          h->T_bfa[f] = h->temp[c0];
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      case JG_BC_SYMMETRY: {
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          double nV[3];
+          norm3(nV, &h->m.fa_normal[3 * f]);
+          double *u0 = &h->vel[3 * c0];
+          double un = dot3(nV, u0);
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = u0[i] - 1.0 * un * nV[i];
+          h->T_bfa[f] = h->temp[c0];
+          h->p_bfa[f] = h->press[c0];
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      case JG_BC_NEUMANN: {
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = h->rhou[3 * c0 + i] / h->rho[c0];
+          h->T_bfa[f] = h->temp[c0];
+          h->p_bfa[f] = h->press[c0];
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      case JG_BC_WALL: {
+        double T_bc = v[0];
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = 0.0;
+          h->T_bfa[f] = (T_bc > 0.0) ? T_bc : h->temp[c0];
+          h->p_bfa[f] = h->press[c0];
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      case JG_BC_FARFIELD: {
+        const double *u_bc = v; double p_bc = v[3], rho_bc = v[4], gamma_bc = v[5];
+        double gm1 = gamma_bc - 1.0;
+        double ovgm1 = 1.0 / gm1;
+        double c_bc = sqrt(gamma_bc * p_bc / rho_bc);
+        double s_bc = pow(rho_bc, gamma_bc) / p_bc;
+        for (int f = f0; f <= f1; f++) {
+          int c0 = h->m.cvofa[2 * f];
+          double nV[3];
+          norm3(nV, &h->m.fa_normal[3 * f]);
+          double qn_bc = dot3(nV, u_bc);
+          double vn_bc = qn_bc;
+          double qne = dot3(nV, &h->vel[3 * c0]);
+          double ce = sqrt(h->gam[c0] * h->press[c0] / h->rho[c0]);
+          double ac1 = (vn_bc > -c_bc) ? qne + 2.0 * ovgm1 * ce : qn_bc + 2.0 * ovgm1 * c_bc;
+          double ac2 = (vn_bc > c_bc) ? qne - 2.0 * ovgm1 * ce : qn_bc - 2.0 * ovgm1 * c_bc;
+          double qnf = 0.5 * (ac1 + ac2);
+          double cf = 0.25 * (ac1 - ac2) * gm1;
+          double velf[3], sf;
+          if (vn_bc > 0) {
+            for (int i = 0; i < 3; i++) velf[i] = h->vel[3 * c0 + i] + (qnf - qne) * nV[i];
+            sf = pow(h->rho[c0], h->gam[c0]) / h->press[c0];
+          } else {
+            for (int i = 0; i < 3; i++) velf[i] = u_bc[i] + (qnf - qn_bc) * nV[i];
+            sf = s_bc;
+          }
+          h->rho_bfa[f] = pow((sf * cf * cf / h->gam[c0]), ovgm1);
+          for (int i = 0; i < 3; i++) h->vel_bfa[3 * f + i] = velf[i];
+          h->p_bfa[f] = h->rho_bfa[f] * cf * cf / h->gam[c0];
+          h->T_bfa[f] = h->p_bfa[f] / (p->R_gas * h->rho_bfa[f]);
+        }
+        bc_props_T(h, f0, f1);
+      } break;
+      default:
+        return -1;
+    }
+  }
+  /* density from the equation of state, JoeWithModels.cpp:4291-4293 */
+  for (int f = 0; f < h->nfa_b; f++) h->rho_bfa[f] = h->p_bfa[f] / (h->RoM_bfa[f] * h->T_bfa[f]);
+  return 0;
+}
+
+int jo_calc_state(jo_case *h) {
+  calc_state_variables(h);
+  calc_material_properties(h);
+  int e = set_bc(h);
+  /* calcRansTurbViscMuet without a turbulence model: mut_fa = 0 (UgpWithCvCompFlow.h:1568-1580) */
+  for (int f = 0; f < h->nfa; f++) h->mut_fa[f] = 0.0;
+  return e;
+}
+
+/* ------------------------------------------------------------------------ */
+/* local time step, UgpWithCvCompFlow.cpp:5-110                              */
+/* ------------------------------------------------------------------------ */
+double jo_calc_dt(jo_case *h, double cfl_target) {
+  const jg_params *p = &h->p;
+  if (p->time_step_mode == JG_TS_DT) {
+    if (!h->dt_fixed_done) {
+      h->dt_fixed = p->dt;
+      for (int c = 0; c < h->ncv; c++) h->local_dt[c] = p->dt;
+      h->dt_fixed_done = 1;
+    }
+    return h->dt_fixed;
+  }
+  double dt_min = 1.0e20;
+  for (int c = 0; c < h->ncv; c++) {
+    double r = h->rho[c];
+    double cs = sqrt(h->gam[c] * h->press[c] / r);
+    const double *ru = &h->rhou[3 * c];
+    double dt_cv;
+    if (p->time_step == JG_DT_MAX_BASED) {
+      double lambdaMax = 0.0;
+      for (int k = h->m.faocv_i[c]; k < h->m.faocv_i[c + 1]; k++) {
+        int f = h->m.faocv_v[k];
+        double nV[3];
+        double area = norm3(nV, &h->m.fa_normal[3 * f]);
+        double Uk = dot3(ru, nV) / r;
+        double lambda = (fabs(Uk) + cs) * area;
+        double lamdiff = 4.0 * (h->mul_fa[f] + h->mut_fa[f]) / r * area * area / h->m.cv_volume[c];
+        lambda = dmax(lambda, lamdiff);
+        lambdaMax = dmax(lambdaMax, lambda);
+      }
+      dt_cv = cfl_target * h->m.cv_volume[c] / lambdaMax;
+    } else {
+      double lc = 0.0, ld = 0.0;
+      for (int k = h->m.faocv_i[c]; k < h->m.faocv_i[c + 1]; k++) {
+        int f = h->m.faocv_v[k];
+        double nV[3];
+        double area = norm3(nV, &h->m.fa_normal[3 * f]);
+        double Uk = dot3(ru, nV) / r;
+        int c0 = h->m.cvofa[2 * f], c1 = h->m.cvofa[2 * f + 1];
+        double vol = (c0 >= 0 && c1 >= 0) ? 0.5 * (h->m.cv_volume[c0] + h->m.cv_volume[c1]) : 0.5 * h->m.cv_volume[c];
+        lc += (fabs(Uk) + cs) * area;
+        if (p->mu_ref > 0.0) {
+          double kv = (4.0 / 3.0) * (h->mul_fa[f] + h->mut_fa[f]) / r;
+          ld += area * area * kv / vol;
+        } else
+          ld = 0.0;
+      }
+      double dt_conv = cfl_target * h->m.cv_volume[c] / lc;
+      double dt_visc = (p->mu_ref > 0.0) ? 0.25 * cfl_target * h->m.cv_volume[c] / ld : 1.0e20;
+      dt_cv = dmin(dt_conv, dt_visc);
+    }
+    dt_min = dmin(dt_min, dt_cv);
+    h->local_dt[c] = dt_cv;
+  }
+  if (p->time_step_mode == JG_TS_CFL_MIN)
+    for (int c = 0; c < h->ncv; c++) h->local_dt[c] = dt_min;
+  return dt_min;
+}
+
+/* ------------------------------------------------------------------------ */
+/* gradients + limiters, UgpWithCv.h:803-1083                                */
+/* ------------------------------------------------------------------------ */
+#define SDWLS_CLIP_SCALAR 1.0e-8 /* SDWLSClippingScalar, UgpWithCv.h:20 */
+
+static void grad_scalar(jo_case *h, double *g, const double *phi, const double *phi_bfa, int limit,
+                        const double *ref, double *alpha) {
+  const jg_mesh *m = &h->m;
+  /* calcCvScalarGrad(grad, phi) + boundary part, UgpWithCv.h:1009-1056 */
+  for (int c = 0; c < h->ncv; c++) {
+    int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
+    for (int i = 0; i < 3; i++) g[3 * c + i] = m->nbocv_lsg_coeff[3 * nf + i] * phi[c];
+    for (int k = nf + 1; k <= nl; k++) {
+      int nb = m->nbocv_v[k];
+      for (int i = 0; i < 3; i++) g[3 * c + i] += m->nbocv_lsg_coeff[3 * k + i] * phi[nb];
+    }
+  }
+  for (int f = 0; f < h->nfa_b; f++) {
+    int c = m->cvofa[2 * f];
+    for (int i = 0; i < 3; i++) g[3 * c + i] += m->boundary_fa_lsg_coeff[3 * f + i] * phi_bfa[f];
+  }
+  if (!limit) return;
+  /* limitCvScalarGradBJ (smooth form), UgpWithCv.h:881-938 */
+  for (int c = 0; c < h->ncv; c++) {
+    double pmax = phi[c], pmin = pmax;
+    for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+      int nb = m->nbocv_v[k];
+      pmax = dmax(pmax, phi[nb]);
+      pmin = dmin(pmin, phi[nb]);
+    }
+    double alfa = 1.0;
+    if ((pmax - pmin) > 1.0e-12) {
+      for (int k = m->faocv_i[c]; k < m->faocv_i[c + 1]; k++) {
+        int f = m->faocv_v[k];
+        if (f >= h->nfa_b) {
+          double r0[3];
+          for (int i = 0; i < 3; i++) r0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c + i];
+          double phifa = phi[c] + dot3(r0, &g[3 * c]);
+          double eps2 = dmax(h->p.eps * fabs(ref[c]), SDWLS_CLIP_SCALAR);
+          eps2 = pow(eps2, 2.0);
+          double dm = phifa - phi[c];
+          double dp = ((phifa - phi[c]) >= 0.0) ? pmax - phi[c] : pmin - phi[c];
+          alfa = dmin(alfa, (dp * dp + 2.0 * dm * dp + eps2) / (dp * dp + 2 * dm * dm + dm * dp + eps2));
+        }
+      }
+    } else
+      alfa = 0.0;
+    for (int i = 0; i < 3; i++) g[3 * c + i] *= alfa;
+    if (alpha) alpha[c] = alfa;
+  }
+}
+
+static void grad_vector(jo_case *h, double *g, const double *u, const double *u_bfa, int limit, const double *ref) {
+  const jg_mesh *m = &h->m;
+  /* calcCvVectorGrad(grad, u) + boundary part, UgpWithCv.h:1031-1083; g[c][i][j] = d u_i / d x_j */
+  for (int c = 0; c < h->ncv; c++) {
+    int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] = m->nbocv_lsg_coeff[3 * nf + j] * u[3 * c + i];
+    for (int k = nf + 1; k <= nl; k++) {
+      int nb = m->nbocv_v[k];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += m->nbocv_lsg_coeff[3 * k + j] * u[3 * nb + i];
+    }
+  }
+  for (int f = 0; f < h->nfa_b; f++) {
+    int c = m->cvofa[2 * f];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += m->boundary_fa_lsg_coeff[3 * f + j] * u_bfa[3 * f + i];
+  }
+  if (!limit) return;
+  /* limitCvVectorGradBJ, UgpWithCv.h:943-1000 */
+  for (int c = 0; c < h->ncv; c++) {
+    for (int i = 0; i < 3; i++) {
+      double pmax = u[3 * c + i], pmin = pmax;
+      for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+        int nb = m->nbocv_v[k];
+        pmax = dmax(pmax, u[3 * nb + i]);
+        pmin = dmin(pmin, u[3 * nb + i]);
+      }
+      double alfa = 1.0;
+      if ((pmax - pmin) > 1.0e-8) {
+        for (int k = m->faocv_i[c]; k < m->faocv_i[c + 1]; k++) {
+          int f = m->faocv_v[k];
+          if (f >= h->nfa_b) {
+            double r0[3];
+            for (int j = 0; j < 3; j++) r0[j] = m->x_fa[3 * f + j] - m->x_cv[3 * c + j];
+            double phifa = u[3 * c + i] + dot3(r0, &g[9 * c + 3 * i]);
+            double eps2 = pow(h->p.eps * ref[c], 2.0);
+            double dm = phifa - u[3 * c + i];
+            double dp = ((phifa - u[3 * c + i]) >= 0.0) ? pmax - u[3 * c + i] : pmin - u[3 * c + i];
+            alfa = dmin(alfa, (dp * dp + 2.0 * dm * dp + eps2) / (dp * dp + 2 * dm * dm + dm * dp + eps2));
+          }
+        }
+      } else
+        alfa = 0.0;
+      for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] *= alfa;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Euler fluxes and their implicit matrices                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct { double rho, u[3], p, gam, k; } fstate;
+
+/* calcEulerFlux_HLLC, UgpWithCvCompFlow.cpp:120-235 */
+static void flux_hllc(double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+  double surfv = 0.0;
+  double unL = dot3(L->u, nV) - surfv, unLr = unL - surfv;
+  double uLuL = dot3(L->u, L->u);
+  double cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->gam / (L->gam - 1.0) * L->p / L->rho + 0.5 * uLuL + L->k;
+  double eL = hL * L->rho - L->p;
+  double unR = dot3(R->u, nV) - surfv, unRr = unR - surfv;
+  double uRuR = dot3(R->u, R->u);
+  double cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->gam / (R->gam - 1.0) * R->p / R->rho + 0.5 * uRuR + R->k;
+  double eR = hR * R->rho - R->p;
+  double Rrho = sqrt(R->rho / L->rho);
+  double tmp = 1.0 / (1.0 + Rrho);
+  double velRoe[3];
+  for (int i = 0; i < 3; i++) velRoe[i] = tmp * (L->u[i] + R->u[i] * Rrho);
+  double uRoe = dot3(velRoe, nV);
+  double gamPdivRho = tmp * ((L->gam * L->p / L->rho + 0.5 * (L->gam - 1.0) * uLuL) +
+                             (R->gam * R->p / R->rho + 0.5 * (R->gam - 1.0) * uRuR) * Rrho);
+  double cRoe = sqrt(gamPdivRho - ((L->gam + R->gam) * 0.5 - 1.0) * 0.5 * dot3(velRoe, velRoe));
+  double sL = dmin(uRoe - cRoe, unLr - cL);
+  double sR = dmax(uRoe + cRoe, unRr + cR);
+  double sM = (L->p - R->p - L->rho * unL * (sL - unL) + R->rho * unR * (sR - unR)) /
+              (R->rho * (sR - unR) - L->rho * (sL - unL));
+  double pStar = R->rho * (unR - sR) * (unR - sM) + R->p;
+  if (sM >= 0.0) {
+    if (sL > 0.0) {
+      F[0] = L->rho * unLr;
+      for (int i = 0; i < 3; i++) F[1 + i] = L->rho * L->u[i] * unLr + L->p * nV[i];
+      F[4] = eL * unLr + L->p * unL;
+    } else {
+      double inv = 1.0 / (sL - sM);
+      double sLmuL = sL - unL;
+      double rhoSL = L->rho * sLmuL * inv;
+      double rhouSL[3];
+      for (int i = 0; i < 3; i++) rhouSL[i] = (L->rho * L->u[i] * sLmuL + (pStar - L->p) * nV[i]) * inv;
+      double eSL = (sLmuL * eL - L->p * unL + pStar * sM) * inv;
+      F[0] = rhoSL * sM;
+      for (int i = 0; i < 3; i++) F[1 + i] = rhouSL[i] * sM + pStar * nV[i];
+      F[4] = (eSL + pStar) * sM;
+    }
+  } else {
+    if (sR >= 0.0) {
+      double inv = 1.0 / (sR - sM);
+      double sRmuR = sR - unR;
+      double rhoSR = R->rho * sRmuR * inv;
+      double rhouSR[3];
+      for (int i = 0; i < 3; i++) rhouSR[i] = (R->rho * R->u[i] * sRmuR + (pStar - R->p) * nV[i]) * inv;
+      double eSR = (sRmuR * eR - R->p * unR + pStar * sM) * inv;
+      F[0] = rhoSR * sM;
+      for (int i = 0; i < 3; i++) F[1 + i] = rhouSR[i] * sM + pStar * nV[i];
+      F[4] = (eSR + pStar) * sM;
+    } else {
+      F[0] = R->rho * unRr;
+      for (int i = 0; i < 3; i++) F[1 + i] = R->rho * R->u[i] * unRr + R->p * nV[i];
+      F[4] = eR * unRr + R->p * unR;
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+/* calcJacobianA, UgpWithCvCompFlow.cpp:666-709 (nV carries the area) */
+static void jacobian_A(double A[5][5], const double *vel, double pp, double rrho, const double *nV, double gamma,
+                       double surfVeloc) {
+  double kapm1 = (gamma - 1.0);
+  double nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
+  double U_k = nVel[0] + nVel[1] + nVel[2];
+  double vSquHlf = 0.5 * dot3(vel, vel);
+  double c = sqrt(gamma * pp / rrho);
+  double inv_kap_m1 = 1.0 / kapm1;
+  A[0][0] = -surfVeloc; A[0][1] = nV[0]; A[0][2] = nV[1]; A[0][3] = nV[2]; A[0][4] = 0.0;
+  A[1][0] = -vel[0] * (nVel[1] + nVel[2]) + nV[0] * (kapm1 * vSquHlf - vel[0] * vel[0]);
+  A[1][1] = (2. - gamma) * nVel[0] + U_k - surfVeloc;
+  A[1][2] = vel[0] * nV[1] - kapm1 * vel[1] * nV[0];
+  A[1][3] = vel[0] * nV[2] - kapm1 * vel[2] * nV[0];
+  A[1][4] = kapm1 * nV[0];
+  A[2][0] = -vel[1] * (nVel[0] + nVel[2]) + nV[1] * (kapm1 * vSquHlf - vel[1] * vel[1]);
+  A[2][1] = -kapm1 * vel[0] * nV[1] + vel[1] * nV[0];
+  A[2][2] = (2. - gamma) * nVel[1] + U_k - surfVeloc;
+  A[2][3] = vel[1] * nV[2] - kapm1 * vel[2] * nV[1];
+  A[2][4] = kapm1 * nV[1];
+  A[3][0] = -vel[2] * (nVel[0] + nVel[1]) + nV[2] * (kapm1 * vSquHlf - vel[2] * vel[2]);
+  A[3][1] = -kapm1 * vel[0] * nV[2] + vel[2] * nV[0];
+  A[3][2] = -kapm1 * vel[1] * nV[2] + vel[2] * nV[1];
+  A[3][3] = (2. - gamma) * nVel[2] + U_k - surfVeloc;
+  A[3][4] = kapm1 * nV[2];
+  A[4][0] = U_k * ((gamma - 2.) * vSquHlf - c * c * inv_kap_m1);
+  A[4][1] = c * c * inv_kap_m1 * nV[0] - kapm1 * vel[0] * (nVel[1] + nVel[2]) - (kapm1 * vel[0] * vel[0] - vSquHlf) * nV[0];
+  A[4][2] = c * c * inv_kap_m1 * nV[1] - kapm1 * vel[1] * (nVel[0] + nVel[2]) - (kapm1 * vel[1] * vel[1] - vSquHlf) * nV[1];
+  A[4][3] = c * c * inv_kap_m1 * nV[2] - kapm1 * vel[2] * (nVel[0] + nVel[1]) - (kapm1 * vel[2] * vel[2] - vSquHlf) * nV[2];
+  A[4][4] = gamma * U_k - surfVeloc;
+}
+
+/* calcSubSonicJacobeanHLLC, UgpWithCvCompFlow.cpp:605-659 */
+static void subsonic_jac_hllc(double (*AL)[5], double (*AR)[5], double rhoL, const double *uL, double pL, double eL,
+                              double qL, double psiL, double SL, double rhoSL, const double *rhouSL, double eSL,
+                              const double *dSMdUL, const double *dSMdUR, const double *dpsdUL, const double *dpsdUR,
+                              double SM, double pS, double gamma, const double *nV) {
+  double gm1 = (gamma - 1.0);
+  double omL = 1.0 / (SL - SM);
+  if (AL) {
+    AL[0][0] = SL + rhoSL * dSMdUL[0];
+    AL[0][1] = -nV[0] + rhoSL * dSMdUL[1];
+    AL[0][2] = -nV[1] + rhoSL * dSMdUL[2];
+    AL[0][3] = -nV[2] + rhoSL * dSMdUL[3];
+    AL[0][4] = +rhoSL * dSMdUL[4];
+    AL[1][0] = qL * uL[0] - nV[0] * psiL * gm1 / 2.0 + nV[0] * dpsdUL[0] + rhouSL[0] * dSMdUL[0];
+    AL[1][1] = SL - qL + nV[0] * (gamma - 2.0) * uL[0] + nV[0] * dpsdUL[1] + rhouSL[0] * dSMdUL[1];
+    AL[1][2] = -uL[0] * nV[1] + nV[0] * gm1 * uL[1] + nV[0] * dpsdUL[2] + rhouSL[0] * dSMdUL[2];
+    AL[1][3] = -uL[0] * nV[2] + nV[0] * gm1 * uL[2] + nV[0] * dpsdUL[3] + rhouSL[0] * dSMdUL[3];
+    AL[1][4] = -gm1 * nV[0] + nV[0] * dpsdUL[4] + rhouSL[0] * dSMdUL[4];
+    AL[2][0] = qL * uL[1] - nV[1] * psiL * gm1 / 2.0 + nV[1] * dpsdUL[0] + rhouSL[1] * dSMdUL[0];
+    AL[2][1] = -uL[1] * nV[0] + nV[1] * gm1 * uL[0] + nV[1] * dpsdUL[1] + rhouSL[1] * dSMdUL[1];
+    AL[2][2] = SL - qL + nV[1] * (gamma - 2.0) * uL[1] + nV[1] * dpsdUL[2] + rhouSL[1] * dSMdUL[2];
+    AL[2][3] = -uL[1] * nV[2] + nV[1] * gm1 * uL[2] + nV[1] * dpsdUL[3] + rhouSL[1] * dSMdUL[3];
+    AL[2][4] = -gm1 * nV[1] + nV[1] * dpsdUL[4] + rhouSL[1] * dSMdUL[4];
+    AL[3][0] = qL * uL[2] - nV[2] * psiL * gm1 / 2.0 + nV[2] * dpsdUL[0] + rhouSL[2] * dSMdUL[0];
+    AL[3][1] = -uL[2] * nV[0] + nV[2] * gm1 * uL[0] + nV[2] * dpsdUL[1] + rhouSL[2] * dSMdUL[1];
+    AL[3][2] = -uL[2] * nV[1] + nV[2] * gm1 * uL[1] + nV[2] * dpsdUL[2] + rhouSL[2] * dSMdUL[2];
+    AL[3][3] = SL - qL + nV[2] * (gamma - 2.0) * uL[2] + nV[2] * dpsdUL[3] + rhouSL[2] * dSMdUL[3];
+    AL[3][4] = -gm1 * nV[2] + nV[2] * dpsdUL[4] + rhouSL[2] * dSMdUL[4];
+    AL[4][0] = qL * (eL + pL) / rhoL - qL * psiL * (gamma - 1.0) / 2.0 + SM * dpsdUL[0] + (pS + eSL) * dSMdUL[0];
+    AL[4][1] = -nV[0] * (eL + pL) / rhoL + gm1 * uL[0] * qL + SM * dpsdUL[1] + (pS + eSL) * dSMdUL[1];
+    AL[4][2] = -nV[1] * (eL + pL) / rhoL + gm1 * uL[1] * qL + SM * dpsdUL[2] + (pS + eSL) * dSMdUL[2];
+    AL[4][3] = -nV[2] * (eL + pL) / rhoL + gm1 * uL[2] * qL + SM * dpsdUL[3] + (pS + eSL) * dSMdUL[3];
+    AL[4][4] = SL - qL * gamma + SM * dpsdUL[4] + (pS + eSL) * dSMdUL[4];
+    for (int i = 0; i < 5; i++)
+      for (int j = 0; j < 5; j++) AL[i][j] *= omL;
+  }
+  if (AR) {
+    for (int i = 0; i < 5; i++) AR[0][i] = omL * rhoSL * dSMdUR[i];
+    for (int i = 0; i < 5; i++) AR[1][i] = omL * (nV[0] * dpsdUR[i] + rhouSL[0] * dSMdUR[i]);
+    for (int i = 0; i < 5; i++) AR[2][i] = omL * (nV[1] * dpsdUR[i] + rhouSL[1] * dSMdUR[i]);
+    for (int i = 0; i < 5; i++) AR[3][i] = omL * (nV[2] * dpsdUR[i] + rhouSL[2] * dSMdUR[i]);
+    for (int i = 0; i < 5; i++) AR[4][i] = omL * (dpsdUR[i] * SM + (pS + eSL) * dSMdUR[i]);
+  }
+}
+
+/* calcEulerFluxMatrices_HLLC, UgpWithCvCompFlow.cpp:242-595 (no scalars) */
+static void matrices_hllc(double (*A_L)[5], double (*A_R)[5], const fstate *L, const fstate *R, double area,
+                          const double *nV) {
+  double rhoL = L->rho, pL = L->p, gammaL = L->gam;
+  double rhoR = R->rho, pR = R->p, gammaR = R->gam;
+  const double *uL = L->u, *uR = R->u;
+  double unL = dot3(uL, nV);
+  double uLuL = dot3(uL, uL);
+  double cL = sqrt(gammaL * pL / rhoL);
+  double hL = gammaL / (gammaL - 1.0) * pL / rhoL + 0.5 * uLuL + L->k;
+  double eL = hL * rhoL - pL;
+  double unR = dot3(uR, nV);
+  double uRuR = dot3(uR, uR);
+  double cR = sqrt(gammaR * pR / rhoR);
+  double hR = gammaR / (gammaR - 1.0) * pR / rhoR + 0.5 * uRuR + R->k;
+  double eR = hR * rhoR - pR;
+  double Rrho = sqrt(rhoR / rhoL);
+  double tmp = 1.0 / (1.0 + Rrho);
+  double velRoe[3];
+  for (int i = 0; i < 3; i++) velRoe[i] = tmp * (uL[i] + uR[i] * Rrho);
+  double uRoe = dot3(velRoe, nV);
+  double gamPdivRho = tmp * ((gammaL * pL / rhoL + 0.5 * (gammaL - 1.0) * uLuL) + (gammaR * pR / rhoR + 0.5 * (gammaR - 1.0) * uRuR) * Rrho);
+  double cRoe = sqrt(gamPdivRho - ((gammaL + gammaR) * 0.5 - 1.0) * 0.5 * dot3(velRoe, velRoe));
+  double sL = dmin(uRoe - cRoe, unL - cL);
+  double sR = dmax(uRoe + cRoe, unR + cR);
+  double sM = (pL - pR - rhoL * unL * (sL - unL) + rhoR * unR * (sR - unR)) / (rhoR * (sR - unR) - rhoL * (sL - unL));
+  double pStar = rhoR * (unR - sR) * (unR - sM) + pR;
+  double gmean = 0.5 * (gammaL + gammaR);
+  if (sM >= 0.0) {
+    if (sL > 0.0) {
+      if (A_L) {
+        double nA[3];
+        for (int i = 0; i < 3; i++) nA[i] = nV[i] * area;
+        jacobian_A(A_L, uL, pL, rhoL, nA, gmean, 0.0);
+      }
+      if (A_R)
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_R[i][j] = 0.0;
+    } else {
+      double invSLmSs = 1.0 / (sL - sM);
+      double sLmuL = sL - unL;
+      double rhoSL = rhoL * sLmuL * invSLmSs;
+      double rhouSL[3];
+      for (int i = 0; i < 3; i++) rhouSL[i] = (rhoL * uL[i] * sLmuL + (pStar - pL) * nV[i]) * invSLmSs;
+      double eSL = (sLmuL * eL - pL * unL + pStar * sM) * invSLmSs;
+      double gLm1 = gammaL - 1.0, gRm1 = gammaR - 1.0;
+      double invrhotld = 1.0 / (rhoR * (sR - unR) - rhoL * (sL - unL));
+      double dSMdUL[5] = {0}, dSMdUR[5] = {0}, dpsdUL[5] = {0}, dpsdUR[5] = {0};
+      if (A_L) {
+        dSMdUL[0] = -unL * unL + uLuL * gLm1 / 2.0 + sM * sL;
+        dSMdUL[1] = nV[0] * (2.0 * unL - sL - sM) - gLm1 * uL[0];
+        dSMdUL[2] = nV[1] * (2.0 * unL - sL - sM) - gLm1 * uL[1];
+        dSMdUL[3] = nV[2] * (2.0 * unL - sL - sM) - gLm1 * uL[2];
+        dSMdUL[4] = gLm1;
+        for (int i = 0; i < 5; i++) { dSMdUL[i] *= invrhotld; dpsdUL[i] = rhoR * (sR - unR) * dSMdUL[i]; }
+      }
+      if (A_R) {
+        dSMdUR[0] = unR * unR - uRuR * gRm1 / 2.0 - sM * sR;
+        dSMdUR[1] = -nV[0] * (2.0 * unR - sR - sM) + gRm1 * uR[0];
+        dSMdUR[2] = -nV[1] * (2.0 * unR - sR - sM) + gRm1 * uR[1];
+        dSMdUR[3] = -nV[2] * (2.0 * unR - sR - sM) + gRm1 * uR[2];
+        dSMdUR[4] = -gRm1;
+        for (int i = 0; i < 5; i++) { dSMdUR[i] *= invrhotld; dpsdUR[i] = rhoL * (sL - unL) * dSMdUR[i]; }
+      }
+      subsonic_jac_hllc(A_L, A_R, rhoL, uL, pL, eL, unL, uLuL, sL, rhoSL, rhouSL, eSL, dSMdUL, dSMdUR, dpsdUL,
+                        dpsdUR, sM, pStar, gmean, nV);
+      if (A_L) {
+        for (int i = 0; i < 5; i++) A_L[0][i] = A_L[0][i] * sM + dSMdUL[i] * rhoSL;
+        for (int i = 0; i < 5; i++) A_L[1][i] = A_L[1][i] * sM + dSMdUL[i] * rhouSL[0] + dpsdUL[i] * nV[0];
+        for (int i = 0; i < 5; i++) A_L[2][i] = A_L[2][i] * sM + dSMdUL[i] * rhouSL[1] + dpsdUL[i] * nV[1];
+        for (int i = 0; i < 5; i++) A_L[3][i] = A_L[3][i] * sM + dSMdUL[i] * rhouSL[2] + dpsdUL[i] * nV[2];
+        for (int i = 0; i < 5; i++) A_L[4][i] = (A_L[4][i] + dpsdUL[i]) * sM + (eSL + pStar) * dSMdUL[i];
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_L[i][j] *= area;
+      }
+      if (A_R) {
+        for (int i = 0; i < 5; i++) A_R[0][i] = A_R[0][i] * sM + dSMdUR[i] * rhoSL;
+        for (int i = 0; i < 5; i++) A_R[1][i] = A_R[1][i] * sM + dSMdUR[i] * rhouSL[0] + dpsdUR[i] * nV[0];
+        for (int i = 0; i < 5; i++) A_R[2][i] = A_R[2][i] * sM + dSMdUR[i] * rhouSL[1] + dpsdUR[i] * nV[1];
+        for (int i = 0; i < 5; i++) A_R[3][i] = A_R[3][i] * sM + dSMdUR[i] * rhouSL[2] + dpsdUR[i] * nV[2];
+        for (int i = 0; i < 5; i++) A_R[4][i] = (A_R[4][i] + dpsdUR[i]) * sM + (eSL + pStar) * dSMdUR[i];
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_R[i][j] *= area;
+      }
+    }
+  } else {
+    if (sR >= 0.0) {
+      double invSRmSs = 1.0 / (sR - sM);
+      double sRmuR = sR - unR;
+      double rhoSR = rhoR * sRmuR * invSRmSs;
+      double rhouSR[3];
+      for (int i = 0; i < 3; i++) rhouSR[i] = (rhoR * uR[i] * sRmuR + (pStar - pR) * nV[i]) * invSRmSs;
+      double eSR = (sRmuR * eR - pR * unR + pStar * sM) * invSRmSs;
+      double gLm1 = gammaL - 1.0, gRm1 = gammaR - 1.0;
+      double invrhotld = 1.0 / (rhoR * (sR - unR) - rhoL * (sL - unL));
+      double dSMdUL[5] = {0}, dSMdUR[5] = {0}, dpsdUL[5] = {0}, dpsdUR[5] = {0};
+      if (A_L) {
+        dSMdUL[0] = -unL * unL + uLuL * gLm1 / 2.0 + sM * sL;
+        dSMdUL[1] = nV[0] * (2.0 * unL - sL - sM) - gLm1 * uL[0];
+        dSMdUL[2] = nV[1] * (2.0 * unL - sL - sM) - gLm1 * uL[1];
+        dSMdUL[3] = nV[2] * (2.0 * unL - sL - sM) - gLm1 * uL[2];
+        dSMdUL[4] = gLm1;
+        for (int i = 0; i < 5; i++) { dSMdUL[i] *= invrhotld; dpsdUL[i] = rhoR * (sR - unR) * dSMdUL[i]; }
+      }
+      if (A_R) {
+        dSMdUR[0] = unR * unR - uRuR * gRm1 / 2.0 - sM * sR;
+        dSMdUR[1] = -nV[0] * (2.0 * unR - sR - sM) + gRm1 * uR[0];
+        dSMdUR[2] = -nV[1] * (2.0 * unR - sR - sM) + gRm1 * uR[1];
+        dSMdUR[3] = -nV[2] * (2.0 * unR - sR - sM) + gRm1 * uR[2];
+        dSMdUR[4] = -gRm1;
+        for (int i = 0; i < 5; i++) { dSMdUR[i] *= invrhotld; dpsdUR[i] = rhoL * (sL - unL) * dSMdUR[i]; }
+      }
+      subsonic_jac_hllc(A_R, A_L, rhoR, uR, pR, eR, unR, uRuR, sR, rhoSR, rhouSR, eSR, dSMdUR, dSMdUL, dpsdUR,
+                        dpsdUL, sM, pStar, gmean, nV);
+      if (A_L) {
+        for (int i = 0; i < 5; i++) A_L[0][i] = A_L[0][i] * sM + dSMdUL[i] * rhoSR;
+        for (int i = 0; i < 5; i++) A_L[1][i] = A_L[1][i] * sM + dSMdUL[i] * rhouSR[0] + dpsdUL[i] * nV[0];
+        for (int i = 0; i < 5; i++) A_L[2][i] = A_L[2][i] * sM + dSMdUL[i] * rhouSR[1] + dpsdUL[i] * nV[1];
+        for (int i = 0; i < 5; i++) A_L[3][i] = A_L[3][i] * sM + dSMdUL[i] * rhouSR[2] + dpsdUL[i] * nV[2];
+        for (int i = 0; i < 5; i++) A_L[4][i] = (A_L[4][i] + dpsdUL[i]) * sM + (eSR + pStar) * dSMdUL[i];
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_L[i][j] *= area;
+      }
+      if (A_R) {
+        for (int i = 0; i < 5; i++) A_R[0][i] = A_R[0][i] * sM + dSMdUR[i] * rhoSR;
+        for (int i = 0; i < 5; i++) A_R[1][i] = A_R[1][i] * sM + dSMdUR[i] * rhouSR[0] + dpsdUR[i] * nV[0];
+        for (int i = 0; i < 5; i++) A_R[2][i] = A_R[2][i] * sM + dSMdUR[i] * rhouSR[1] + dpsdUR[i] * nV[1];
+        for (int i = 0; i < 5; i++) A_R[3][i] = A_R[3][i] * sM + dSMdUR[i] * rhouSR[2] + dpsdUR[i] * nV[2];
+        for (int i = 0; i < 5; i++) A_R[4][i] = (A_R[4][i] + dpsdUR[i]) * sM + (eSR + pStar) * dSMdUR[i];
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_R[i][j] *= area;
+      }
+    } else {
+      if (A_R) {
+        double nA[3];
+        for (int i = 0; i < 3; i++) nA[i] = nV[i] * area;
+        jacobian_A(A_R, uR, pR, rhoR, nA, gmean, 0.0);
+      }
+      if (A_L)
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) A_L[i][j] = 0.0;
+    }
+  }
+}
+
+/* calcEulerFlux_Roe, UgpWithCvCompFlow.cpp:3281-3380 (no entropy fix; when the
+ * Roe-averaged c^2 < 1e-12 the reference returns with only the central part) */
+static void flux_roe(double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+  double rho0 = L->rho, rho1 = R->rho;
+  const double *u0 = L->u, *u1 = R->u;
+  double p0 = L->p, p1 = R->p;
+  double gamma = 0.5 * (L->gam + R->gam);
+  double gm1 = gamma - 1.0;
+  double rhoun0 = rho0 * dot3(u0, nV);
+  double rhoun1 = rho1 * dot3(u1, nV);
+  double rhoE0 = p0 / gm1 + 0.5 * rho0 * dot3(u0, u0);
+  double rhoE1 = p1 / gm1 + 0.5 * rho1 * dot3(u1, u1);
+  double H0 = (rhoE0 + p0) / rho0, H1 = (rhoE1 + p1) / rho1;
+  F[0] = 0.5 * area * (rhoun0 + rhoun1);
+  F[1] = 0.5 * area * (rhoun0 * u0[0] + rhoun1 * u1[0] + (p0 + p1) * nV[0]);
+  F[2] = 0.5 * area * (rhoun0 * u0[1] + rhoun1 * u1[1] + (p0 + p1) * nV[1]);
+  F[3] = 0.5 * area * (rhoun0 * u0[2] + rhoun1 * u1[2] + (p0 + p1) * nV[2]);
+  F[4] = 0.5 * area * (rhoun0 * H0 + rhoun1 * H1);
+  double sqrt_rho0 = sqrt(rho0), sqrt_rho1 = sqrt(rho1);
+  double tmp = 1.0 / (sqrt_rho0 + sqrt_rho1);
+  double uAvg = tmp * (u0[0] * sqrt_rho0 + u1[0] * sqrt_rho1);
+  double vAvg = tmp * (u0[1] * sqrt_rho0 + u1[1] * sqrt_rho1);
+  double wAvg = tmp * (u0[2] * sqrt_rho0 + u1[2] * sqrt_rho1);
+  double hAvg = tmp * (H0 * sqrt_rho0 + H1 * sqrt_rho1);
+  double alphaAvg = 0.5 * (uAvg * uAvg + vAvg * vAvg + wAvg * wAvg);
+  double a2Avg = gm1 * (hAvg - alphaAvg);
+  if (a2Avg < 1.0E-12) return;
+  double aAvg = sqrt(a2Avg);
+  double unAvg = uAvg * nV[0] + vAvg * nV[1] + wAvg * nV[2];
+  double dr = rho1 - rho0;
+  double dru = rho1 * u1[0] - rho0 * u0[0];
+  double drv = rho1 * u1[1] - rho0 * u0[1];
+  double drw = rho1 * u1[2] - rho0 * u0[2];
+  double drE = rhoE1 - rhoE0;
+  double lam1 = fabs(unAvg), lam2 = fabs(unAvg + aAvg), lam3 = fabs(unAvg - aAvg);
+  double abv1 = 0.5 * (lam2 + lam3);
+  double abv2 = 0.5 * (lam2 - lam3);
+  double abv3 = abv1 - lam1;
+  double abv4 = gm1 * (alphaAvg * dr - uAvg * dru - vAvg * drv - wAvg * drw + drE);
+  double abv5 = unAvg * dr - nV[0] * dru - nV[1] * drv - nV[2] * drw;
+  double abv6 = abv3 * abv4 / a2Avg - abv2 * abv5 / aAvg;
+  double abv7 = abv3 * abv5 - abv2 * abv4 / aAvg;
+  F[0] -= 0.5 * area * (lam1 * dr + abv6);
+  F[1] -= 0.5 * area * (lam1 * dru + uAvg * abv6 - nV[0] * abv7);
+  F[2] -= 0.5 * area * (lam1 * drv + vAvg * abv6 - nV[1] * abv7);
+  F[3] -= 0.5 * area * (lam1 * drw + wAvg * abv6 - nV[2] * abv7);
+  F[4] -= 0.5 * area * (lam1 * drE + hAvg * abv6 - unAvg * abv7);
+}
+
+/* calcPMatrix / calcInvPMatrix, UgpWithCvCompFlow.cpp:3480-3559 */
+static void p_matrix(double P[5][5], const double *vel, double c, double rrho, const double *nV, double gamma) {
+  double kapm1 = (gamma - 1.0);
+  double rhooc = rrho / c, rhoxc = rrho * c;
+  double vSqu = dot3(vel, vel);
+  P[0][0] = nV[0]; P[0][1] = nV[1]; P[0][2] = nV[2]; P[0][3] = 0.5 * rhooc; P[0][4] = 0.5 * rhooc;
+  P[1][0] = vel[0] * nV[0]; P[1][1] = vel[0] * nV[1] - rrho * nV[2]; P[1][2] = vel[0] * nV[2] + rrho * nV[1];
+  P[1][3] = 0.5 * (vel[0] * rhooc + rrho * nV[0]); P[1][4] = 0.5 * (vel[0] * rhooc - rrho * nV[0]);
+  P[2][0] = vel[1] * nV[0] + rrho * nV[2]; P[2][1] = vel[1] * nV[1]; P[2][2] = vel[1] * nV[2] - rrho * nV[0];
+  P[2][3] = 0.5 * (vel[1] * rhooc + rrho * nV[1]); P[2][4] = 0.5 * (vel[1] * rhooc - rrho * nV[1]);
+  P[3][0] = vel[2] * nV[0] - rrho * nV[1]; P[3][1] = vel[2] * nV[1] + rrho * nV[0]; P[3][2] = vel[2] * nV[2];
+  P[3][3] = 0.5 * (vel[2] * rhooc + rrho * nV[2]); P[3][4] = 0.5 * (vel[2] * rhooc - rrho * nV[2]);
+  P[4][0] = 0.5 * vSqu * nV[0] + rrho * vel[1] * nV[2] - rrho * vel[2] * nV[1];
+  P[4][1] = 0.5 * vSqu * nV[1] - rrho * vel[0] * nV[2] + rrho * vel[2] * nV[0];
+  P[4][2] = 0.5 * vSqu * nV[2] + rrho * vel[0] * nV[1] - rrho * vel[1] * nV[0];
+  P[4][3] = 0.5 * (0.5 * vSqu * rhooc + rrho * (vel[0] * nV[0] + vel[1] * nV[1] + vel[2] * nV[2]) + rhoxc / kapm1);
+  P[4][4] = 0.5 * (0.5 * vSqu * rhooc - rrho * (vel[0] * nV[0] + vel[1] * nV[1] + vel[2] * nV[2]) + rhoxc / kapm1);
+}
+
+static void inv_p_matrix(double iP[5][5], const double *vel, double c, double rrho, const double *nV, double gamma) {
+  double kapm1 = (gamma - 1.0);
+  double rhoxc = rrho * c, c2 = c * c;
+  double vSqu = dot3(vel, vel);
+  iP[0][0] = nV[0] - nV[2] * vel[1] / rrho + nV[1] * vel[2] / rrho - nV[0] * 0.5 * kapm1 * vSqu / c2;
+  iP[0][1] = nV[0] * kapm1 * vel[0] / c2;
+  iP[0][2] = nV[2] / rrho + nV[0] * kapm1 * vel[1] / c2;
+  iP[0][3] = -nV[1] / rrho + nV[0] * kapm1 * vel[2] / c2;
+  iP[0][4] = -nV[0] * kapm1 / c2;
+  iP[1][0] = nV[1] + nV[2] * vel[0] / rrho - nV[0] * vel[2] / rrho - nV[1] * 0.5 * kapm1 * vSqu / c2;
+  iP[1][1] = -nV[2] / rrho + nV[1] * kapm1 * vel[0] / c2;
+  iP[1][2] = nV[1] * kapm1 * vel[1] / c2;
+  iP[1][3] = nV[0] / rrho + nV[1] * kapm1 * vel[2] / c2;
+  iP[1][4] = -nV[1] * kapm1 / c2;
+  iP[2][0] = nV[2] - nV[1] * vel[0] / rrho + nV[0] * vel[1] / rrho - nV[2] * 0.5 * kapm1 * vSqu / c2;
+  iP[2][1] = nV[1] / rrho + nV[2] * kapm1 * vel[0] / c2;
+  iP[2][2] = -nV[0] / rrho + nV[2] * kapm1 * vel[1] / c2;
+  iP[2][3] = nV[2] * kapm1 * vel[2] / c2;
+  iP[2][4] = -nV[2] * kapm1 / c2;
+  iP[3][0] = -(nV[0] * vel[0] + nV[1] * vel[1] + nV[2] * vel[2]) / rrho + 0.5 * kapm1 * vSqu / rhoxc;
+  iP[3][1] = nV[0] / rrho - kapm1 * vel[0] / rhoxc;
+  iP[3][2] = nV[1] / rrho - kapm1 * vel[1] / rhoxc;
+  iP[3][3] = nV[2] / rrho - kapm1 * vel[2] / rhoxc;
+  iP[3][4] = kapm1 / rhoxc;
+  iP[4][0] = (nV[0] * vel[0] + nV[1] * vel[1] + nV[2] * vel[2]) / rrho + 0.5 * kapm1 * vSqu / rhoxc;
+  iP[4][1] = -nV[0] / rrho - kapm1 * vel[0] / rhoxc;
+  iP[4][2] = -nV[1] / rrho - kapm1 * vel[1] / rhoxc;
+  iP[4][3] = -nV[2] / rrho - kapm1 * vel[2] / rhoxc;
+  iP[4][4] = kapm1 / rhoxc;
+}
+
+/* calcEulerFluxMatrices_Roe, UgpWithCvCompFlow.cpp:3382-3476 */
+static void matrices_roe(double (*A_L)[5], double (*A_R)[5], const fstate *L, const fstate *R, double area,
+                         const double *nV) {
+  double rhoL = L->rho, pL = L->p, gammaL = L->gam;
+  double rhoR = R->rho, pR = R->p, gammaR = R->gam;
+  const double *uL = L->u, *uR = R->u;
+  double uLuL = dot3(uL, uL), uRuR = dot3(uR, uR);
+  double Rrho = sqrt(rhoR / rhoL);
+  double rhoRoe = Rrho * rhoL;
+  double tmp = 1.0 / (1.0 + Rrho);
+  double velRoe[3];
+  for (int i = 0; i < 3; i++) velRoe[i] = tmp * (uL[i] + uR[i] * Rrho);
+  double uRoe = dot3(velRoe, nV);
+  double gamPdivRho = tmp * ((gammaL * pL / rhoL + 0.5 * (gammaL - 1.0) * uLuL) + (gammaR * pR / rhoR + 0.5 * (gammaR - 1.0) * uRuR) * Rrho);
+  double cRoe = sqrt(gamPdivRho - ((gammaL + gammaR) * 0.5 - 1.0) * 0.5 * dot3(velRoe, velRoe));
+  double nA[3];
+  for (int i = 0; i < 3; i++) nA[i] = nV[i] * area;
+  double Lambda[5] = {uRoe, uRoe, uRoe, uRoe + cRoe, uRoe - cRoe};
+  double P[5][5], iP[5][5];
+  double gmean = 0.5 * (gammaL + gammaR);
+  p_matrix(P, velRoe, cRoe, rhoRoe, nV, gmean);
+  inv_p_matrix(iP, velRoe, cRoe, rhoRoe, nV, gmean);
+  if (A_L) jacobian_A(A_L, uL, pL, rhoL, nA, gmean, 0.0);
+  if (A_R) jacobian_A(A_R, uR, pR, rhoR, nA, gmean, 0.0);
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) {
+      double pm = 0.0;
+      for (int k = 0; k < 5; k++) pm += P[i][k] * fabs(Lambda[k]) * iP[k][j];
+      if (A_L) A_L[i][j] = 0.5 * A_L[i][j] + 0.5 * pm * area;
+      if (A_R) A_R[i][j] = 0.5 * A_R[i][j] - 0.5 * pm * area;
+    }
+}
+
+/* calcEulerFlux_AUSM, UgpWithCvCompFlow.cpp:3566-3641 */
+static void flux_ausm(double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+  double rhoL = L->rho, pL = L->p, gammaL = L->gam;
+  double rhoR = R->rho, pR = R->p, gammaR = R->gam;
+  const double *uL = L->u, *uR = R->u;
+  double unL = dot3(uL, nV), uLuL = dot3(uL, uL);
+  double cL = sqrt(gammaL * pL / rhoL);
+  double hL = (gammaL / (gammaL - 1.0)) * (pL / rhoL) + 0.5 * uLuL + L->k;
+  double mL = unL / cL;
+  double unR = dot3(uR, nV), uRuR = dot3(uR, uR);
+  double cR = sqrt(gammaR * pR / rhoR);
+  double hR = (gammaR / (gammaR - 1.0)) * (pR / rhoR) + 0.5 * uRuR + R->k;
+  double mR = unR / cR;
+  double mLP = (fabs(mL) <= 1.0) ? 0.25 * (mL + 1.0) * (mL + 1.0) : 0.5 * (mL + fabs(mL));
+  double mRM = (fabs(mR) <= 1.0) ? -0.25 * (mR - 1.0) * (mR - 1.0) : 0.5 * (mR - fabs(mR));
+  double mF = mLP + mRM;
+  double pLP = (fabs(mL) <= 1.0) ? 0.25 * pL * (mL + 1.0) * (mL + 1.0) * (2.0 - mL) : 0.5 * pL * (mL + fabs(mL)) / mL;
+  double pRM = (fabs(mR) <= 1.0) ? 0.25 * pR * (mR - 1.0) * (mR - 1.0) * (2.0 + mR) : 0.5 * pR * (mR - fabs(mR)) / mR;
+  double pF = pLP + pRM;
+  double Phi = fabs(mF);
+  F[0] = 0.5 * (mF * ((rhoL * cL) + (rhoR * cR)) - Phi * ((rhoR * cR) - (rhoL * cL)));
+  for (int i = 0; i < 3; i++)
+    F[1 + i] = 0.5 * (mF * ((rhoL * cL * uL[i]) + (rhoR * cR * uR[i])) - Phi * ((rhoR * cR * uR[i]) - (rhoL * cL * uL[i]))) + nV[i] * pF;
+  F[4] = 0.5 * (mF * ((rhoL * cL * hL) + (rhoR * cR * hR)) - Phi * ((rhoR * cR * hR) - (rhoL * cL * hL)));
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+  if (kind == JG_FLUX_ROE) flux_roe(F, L, R, area, nV);
+  else if (kind == JG_FLUX_AUSM) flux_ausm(F, L, R, area, nV);
+  else flux_hllc(F, L, R, area, nV);
+}
+
+/* implicit matrices per flux choice: AUSM uses the HLLC matrices (JoeWithModels.cpp:3057-3061) */
+static void euler_matrices(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
+                           const double *nV) {
+  if (kind == JG_FLUX_ROE) matrices_roe(AL, AR, L, R, area, nV);
+  else matrices_hllc(AL, AR, L, R, area, nV);
+}
+
+void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
+                         double *F, double *AL, double *AR) {
+  for (int f = 0; f < n; f++) {
+    fstate sl = {L[6 * f], {L[6 * f + 1], L[6 * f + 2], L[6 * f + 3]}, L[6 * f + 4], L[6 * f + 5], 0.0};
+    fstate sr = {R[6 * f], {R[6 * f + 1], R[6 * f + 2], R[6 * f + 3]}, R[6 * f + 4], R[6 * f + 5], 0.0};
+    euler_flux(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f]);
+    if (AL || AR)
+      euler_matrices(kind, AL ? (double(*)[5]) & AL[25 * f] : NULL, AR ? (double(*)[5]) & AR[25 * f] : NULL, &sl, &sr,
+                     area[f], &nvec[3 * f]);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* calcEulerFlux, JoeWithModels.cpp:2621-3589 (nScal == 0)                   */
+/* ------------------------------------------------------------------------ */
+static int csr_slot(const jg_mesh *m, int row, int col) {
+  /* getImplDependencyIndex, UgpWithCv.h:745-755 */
+  int k = m->nbocv_i[row];
+  while (m->nbocv_v[++k] != col) {}
+  return k;
+}
+
+static fstate cell_state(jo_case *h, int c) {
+  fstate s = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->press[c], h->gam[c], 0.0};
+  return s;
+}
+static fstate bfa_state(jo_case *h, int f) {
+  fstate s = {h->rho_bfa[f], {h->vel_bfa[3 * f], h->vel_bfa[3 * f + 1], h->vel_bfa[3 * f + 2]}, h->p_bfa[f],
+              h->gam_bfa[f], 0.0};
+  return s;
+}
+
+/* reconstruct rho, p, u at x_fa from cell c (JoeWithModels.cpp:2832-2921); returns 1 on first-order fallback */
+static int reconstruct(jo_case *h, int c, int f, fstate *s) {
+  double r0[3];
+  for (int i = 0; i < 3; i++) r0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c + i];
+  double rho0 = h->rho[c] + dot3(r0, &h->grad_rho[3 * c]);
+  double p0 = h->press[c] + dot3(r0, &h->grad_p[3 * c]);
+  if ((p0 <= 0.0) || (rho0 <= 0.0)) {
+    s->rho = h->rho[c];
+    s->p = h->press[c];
+    return 1;
+  }
+  s->rho = rho0;
+  s->p = p0;
+  for (int i = 0; i < 3; i++) s->u[i] = h->vel[3 * c + i] + dot3(r0, &h->grad_u[9 * c + 3 * i]);
+  /* calcThermoProp_p: gamma = GAMMA (ideal gas) */
+  s->gam = h->p.gamma;
+  return 0;
+}
+
+static void add_block(double *A, int slot, double (*B)[5], double sgn) {
+  double *a = &A[25 * slot];
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) a[5 * i + j] += sgn * B[i][j];
+}
+
+static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, double *A, int implicit) {
+  const jg_mesh *m = &h->m;
+  const jg_params *p = &h->p;
+  int kind = p->flux;
+  if (p->second_order) {
+    grad_vector(h, h->grad_u, h->vel, h->vel_bfa, p->limiter, h->sos);
+    for (int c = 0; c < h->ncv; c++) h->alpha_rho[c] = 1.0;
+    grad_scalar(h, h->grad_rho, h->rho, h->rho_bfa, p->limiter, h->rho, h->alpha_rho);
+    grad_scalar(h, h->grad_p, h->press, h->p_bfa, p->limiter, h->press, NULL);
+  }
+  double Apl[5][5], Ami[5][5], F[5];
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double nV[3];
+    double area = norm3(nV, &m->fa_normal[3 * f]);
+    fstate L = cell_state(h, c0), R = cell_state(h, c1);
+    if (p->second_order) {
+      reconstruct(h, c0, f, &L);
+      reconstruct(h, c1, f, &R);
+    }
+    euler_flux(kind, F, &L, &R, area, nV);
+    rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+    rr[c1] += F[0]; for (int i = 0; i < 3; i++) ru[3 * c1 + i] += F[1 + i]; rE[c1] += F[4];
+    if (implicit) {
+      fstate L0 = cell_state(h, c0), R0 = cell_state(h, c1);
+      euler_matrices(kind, Apl, Ami, &L0, &R0, area, nV);
+      int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
+      add_block(A, n00, Apl, 1.0);
+      add_block(A, n01, Ami, 1.0);
+      add_block(A, n11, Ami, -1.0);
+      add_block(A, n10, Apl, -1.0);
+    }
+  }
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      int c0 = m->cvofa[2 * f];
+      double nV[3];
+      double area = norm3(nV, &m->fa_normal[3 * f]);
+      int n00 = m->nbocv_i[c0];
+      if (zn->kind == JG_BC_SYMMETRY) {
+        fstate B = bfa_state(h, f);
+        euler_flux(kind, F, &B, &B, area, nV);
+        if (p->symm_bc == JG_SYMM_ANALYTICAL) {
+          for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= h->p_bfa[f] * nV[i] * area;
+        } else {
+          rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+        }
+        if (implicit) {
+          euler_matrices(kind, Apl, Ami, &B, &B, area, nV);
+          if (p->symm_bc == JG_SYMM_ORIGINAL_NUMERIC) add_block(A, n00, Apl, 1.0);
+          else if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
+            double S[5][5];
+            for (int i = 0; i < 5; i++)
+              for (int j = 0; j < 5; j++) S[i][j] = Apl[i][j] + Ami[i][j];
+            add_block(A, n00, S, 1.0);
+          }
+          else {
+            /* analytical pressure Jacobian, JoeWithModels.cpp:3231-3251 */
+            double S[5][5];
+            const double *vb = &h->vel_bfa[3 * f];
+            double a2 = h->gam_bfa[f] - 1.0;
+            double phi = 0.5 * a2 * (vb[0] * vb[0] + vb[1] * vb[1] + vb[2] * vb[2]);
+            for (int i = 0; i < 5; i++) { S[0][i] = 0.0; S[4][i] = 0.0; }
+            for (int i = 0; i < 3; i++) {
+              S[i + 1][0] = phi * nV[i] * area;
+              for (int j = 0; j < 3; j++) S[i + 1][j + 1] = -a2 * vb[j] * nV[i] * area;
+              S[i + 1][4] = a2 * nV[i] * area;
+            }
+            add_block(A, n00, S, 1.0);
+          }
+        }
+      } else if (zn->kind == JG_BC_WALL) {
+        fstate B = bfa_state(h, f);
+        euler_flux(kind, F, &B, &B, area, nV);
+        rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+        if (implicit) {
+          euler_matrices(kind, Apl, NULL, &B, &B, area, nV);
+          add_block(A, n00, Apl, 1.0);
+        }
+      } else {
+        fstate L = cell_state(h, c0);
+        if (p->second_order) reconstruct(h, c0, f, &L);
+        fstate B = bfa_state(h, f);
+        euler_flux(kind, F, &L, &B, area, nV);
+        rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+        if (implicit) {
+          fstate L0 = cell_state(h, c0);
+          euler_matrices(kind, Apl, NULL, &L0, &B, area, nV);
+          add_block(A, n00, Apl, 1.0);
+        }
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* viscous flux: addViscFlux, UgpWithCvCompFlow.cpp:1521-1763                */
+/* ------------------------------------------------------------------------ */
+static void add_visc_flux(jo_case *h, double Fu[3], double *FE, double (*A0)[5], double (*A1)[5], double rho0,
+                          const double *u0, const double *gu0, double h0, const double *gh0, double T0, double R0,
+                          double gam0, double rho1, const double *u1, const double *gu1, double h1, const double *gh1,
+                          double T1, double R1, double gam1, double mul, double mut, double lamOcp,
+                          const double *u_fa, double area, const double *nV, double smag, const double *sV) {
+  double alpha = dot3(nV, sV);
+  double g[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) g[i][j] = 0.5 * (gu0[3 * i + j] + gu1[3 * i + j]);
+  double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
+  double tl[3], tt[3], tau[3];
+  double nonL = 0.0;
+  for (int i = 0; i < 3; i++)
+    tl[i] = mul * (alpha * (u1[i] - u0[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
+                   g[1][i] * nV[1] + g[i][2] * fC[2] + g[2][i] * nV[2]);
+  double tmp = 2.0 / 3.0 * mul * (g[0][0] + g[1][1] + g[2][2]);
+  for (int i = 0; i < 3; i++) tl[i] -= tmp * nV[i];
+  for (int i = 0; i < 3; i++)
+    tt[i] = (1.0 - nonL) * mut * (alpha * (u1[i] - u0[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
+                                  g[1][i] * nV[1] + g[i][2] * fC[2] + g[2][i] * nV[2]);
+  tmp = (1.0 - nonL) * 2.0 / 3.0 * mut * (g[0][0] + g[1][1] + g[2][2]);
+  for (int i = 0; i < 3; i++) tt[i] -= tmp * nV[i];
+  /* Reynolds-stress terms vanish (nonLinear = 0, rij = 0) */
+  for (int i = 0; i < 3; i++) tau[i] = tl[i] + tt[i];
+  for (int i = 0; i < 3; i++) Fu[i] = -area * tau[i];
+  double keff = lamOcp + mut / h->p.PrTurb;
+  double enth = keff * (alpha * (h1 - h0) / smag +
+                        0.5 * ((gh0[0] + gh1[0]) * fC[0] + (gh0[1] + gh1[1]) * fC[1] + (gh0[2] + gh1[2]) * fC[2]));
+  double psi = 0.0;
+  *FE = -area * (enth + tau[0] * u_fa[0] + tau[1] * u_fa[1] + tau[2] * u_fa[2] + psi);
+
+  for (int side = 0; side < 2; side++) {
+    double (*Ax)[5] = side == 0 ? A0 : A1;
+    if (!Ax) continue;
+    double fU[5][5] = {{0}}, UQ[5][5] = {{0}};
+    double d = (side == 0) ? -(mul + mut) * alpha / smag * area : (mul + mut) * alpha / smag * area;
+    fU[1][1] = d; fU[2][2] = d; fU[3][3] = d;
+    fU[4][1] = area * tau[0] * 0.5 + u_fa[0] * fU[1][1];
+    fU[4][2] = area * tau[1] * 0.5 + u_fa[1] * fU[2][2];
+    fU[4][3] = area * tau[2] * 0.5 + u_fa[2] * fU[3][3];
+    fU[4][4] = (side == 0) ? -area * keff * alpha / smag : area * keff * alpha / smag;
+    double r = side == 0 ? rho0 : rho1;
+    const double *u = side == 0 ? u0 : u1;
+    double hh = side == 0 ? h0 : h1, TT = side == 0 ? T0 : T1, RR = side == 0 ? R0 : R1, gg = side == 0 ? gam0 : gam1;
+    double kine = 0.0;
+    double invRho = 1.0 / r;
+    UQ[1][0] = -u[0] * invRho;
+    UQ[2][0] = -u[1] * invRho;
+    UQ[3][0] = -u[2] * invRho;
+    UQ[4][0] = gg * invRho * (-hh - kine + RR * TT + 0.5 * dot3(u, u));
+    UQ[1][1] = invRho; UQ[4][1] = -gg * u[0] * invRho;
+    UQ[2][2] = invRho; UQ[4][2] = -gg * u[1] * invRho;
+    UQ[3][3] = invRho; UQ[4][3] = -gg * u[2] * invRho;
+    UQ[4][4] = gg * invRho;
+    /* dFdU_times_dUdQ, UgpWithCvCompFlow.cpp:717-745 (rows 1..4; column 4 only in row 4) */
+    for (int i = 1; i < 4; i++) Ax[i][0] = fU[i][1] * UQ[1][0] + fU[i][2] * UQ[2][0] + fU[i][3] * UQ[3][0];
+    Ax[4][0] = fU[4][1] * UQ[1][0] + fU[4][2] * UQ[2][0] + fU[4][3] * UQ[3][0] + fU[4][4] * UQ[4][0];
+    for (int i = 1; i < 4; i++) Ax[i][1] = fU[i][1] * UQ[1][1];
+    Ax[4][1] = fU[4][1] * UQ[1][1] + fU[4][4] * UQ[4][1];
+    for (int i = 1; i < 4; i++) Ax[i][2] = fU[i][2] * UQ[2][2];
+    Ax[4][2] = fU[4][2] * UQ[2][2] + fU[4][4] * UQ[4][2];
+    for (int i = 1; i < 4; i++) Ax[i][3] = fU[i][3] * UQ[3][3];
+    Ax[4][3] = fU[4][3] * UQ[3][3] + fU[4][4] * UQ[4][3];
+    Ax[4][4] = fU[4][1] * UQ[1][4] + fU[4][2] * UQ[2][4] + fU[4][3] * UQ[3][4] + fU[4][4] * UQ[4][4];
+  }
+}
+
+/* calcViscousFluxNS, JoeWithModels.cpp:3591-3855 */
+static void calc_viscous_flux(jo_case *h, double *ru, double *rE, double *A, int implicit) {
+  const jg_mesh *m = &h->m;
+  const jg_params *p = &h->p;
+  if (p->visc_limiter) {
+    if (!p->second_order) grad_vector(h, h->grad_u, h->vel, h->vel_bfa, p->limiter, h->sos);
+    grad_scalar(h, h->grad_h, h->enthalpy, h->h_bfa, p->limiter, h->enthalpy, NULL);
+  } else {
+    grad_vector(h, h->grad_u, h->vel, h->vel_bfa, 0, h->sos);
+    grad_scalar(h, h->grad_h, h->enthalpy, h->h_bfa, 0, h->enthalpy, NULL);
+  }
+  double A0[5][5] = {{0}}, A1[5][5] = {{0}};
+  double Fu[3], FE;
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double nV[3];
+    double area = norm3(nV, &m->fa_normal[3 * f]);
+    double sV[3];
+    for (int i = 0; i < 3; i++) sV[i] = m->x_cv[3 * c1 + i] - m->x_cv[3 * c0 + i];
+    double smag = norm3(sV, sV);
+    double ufa[3] = {0.5 * (h->vel[3 * c0] + h->vel[3 * c1]), 0.5 * (h->vel[3 * c0 + 1] + h->vel[3 * c1 + 1]),
+                     0.5 * (h->vel[3 * c0 + 2] + h->vel[3 * c1 + 2])};
+    add_visc_flux(h, Fu, &FE, implicit ? A0 : NULL, implicit ? A1 : NULL, h->rho[c0], &h->vel[3 * c0],
+                  &h->grad_u[9 * c0], h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0],
+                  h->rho[c1], &h->vel[3 * c1], &h->grad_u[9 * c1], h->enthalpy[c1], &h->grad_h[3 * c1], h->temp[c1],
+                  h->RoM[c1], h->gam[c1], h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], ufa, area, nV, smag, sV);
+    if (implicit) {
+      int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
+      for (int i = 1; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+          A[25 * n00 + 5 * i + j] -= A0[i][j];
+          A[25 * n01 + 5 * i + j] -= A1[i][j];
+          A[25 * n11 + 5 * i + j] += A1[i][j];
+          A[25 * n10 + 5 * i + j] += A0[i][j];
+        }
+    }
+    for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= Fu[i];
+    rE[c0] -= FE;
+    for (int i = 0; i < 3; i++) ru[3 * c1 + i] += Fu[i];
+    rE[c1] += FE;
+  }
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    if (zn->kind == JG_BC_SYMMETRY) continue; /* nothing without a turbulence model */
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      int c0 = m->cvofa[2 * f];
+      double nV[3];
+      double area = norm3(nV, &m->fa_normal[3 * f]);
+      double sV[3];
+      for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+      double smag;
+      const double *sVec;
+      double mut;
+      if (zn->kind == JG_BC_WALL) {
+        smag = fabs(dot3(sV, nV));  /* project onto the wall normal, use nVec as sVec */
+        sVec = nV;
+        mut = 0.0;
+      } else {
+        smag = norm3(sV, sV);
+        sVec = sV;
+        mut = h->mut_fa[f];
+      }
+      add_visc_flux(h, Fu, &FE, implicit ? A0 : NULL, NULL, h->rho[c0], &h->vel[3 * c0], &h->grad_u[9 * c0],
+                    h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0], h->rho_bfa[f],
+                    &h->vel_bfa[3 * f], &h->grad_u[9 * c0], h->h_bfa[f], &h->grad_h[3 * c0], h->T_bfa[f],
+                    h->RoM_bfa[f], h->gam_bfa[f], h->mul_fa[f], mut, h->lamOcp_fa[f], &h->vel_bfa[3 * f], area, nV,
+                    smag, sVec);
+      if (implicit) {
+        int n00 = m->nbocv_i[c0];
+        for (int i = 1; i < 5; i++)
+          for (int j = 0; j < 5; j++) A[25 * n00 + 5 * i + j] -= A0[i][j];
+      }
+      for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= Fu[i];
+      rE[c0] -= FE;
+    }
+  }
+}
+
+void jo_calc_rhs(jo_case *h, double *rr, double *ru, double *rE, double *A, int implicit) {
+  /* calcRhs, JoeWithModels.cpp:2564-2619 */
+  memset(rr, 0, sizeof(double) * h->ncv);
+  memset(ru, 0, sizeof(double) * 3 * h->ncv);
+  memset(rE, 0, sizeof(double) * h->ncv);
+  calc_euler_flux(h, rr, ru, rE, A, implicit);
+  if (h->p.mu_ref > 0.0) calc_viscous_flux(h, ru, rE, A, implicit);
+}
+
+/* ------------------------------------------------------------------------ */
+/* linear solvers, UgpWithCv.cpp:2489-2876, 3172-3329                        */
+/* ------------------------------------------------------------------------ */
+static void ludeco(double (*A)[5], int order) {
+  for (int jc = 1; jc < order; jc++) A[0][jc] /= A[0][0];
+  int jrjc = 0;
+  for (;;) {
+    jrjc++;
+    int jrjcm1 = jrjc - 1, jrjcp1 = jrjc + 1;
+    for (int jr = jrjc; jr < order; jr++) {
+      double sum = A[jr][jrjc];
+      for (int jm = 0; jm <= jrjcm1; jm++) sum -= A[jr][jm] * A[jm][jrjc];
+      A[jr][jrjc] = sum;
+    }
+    if (jrjc == (order - 1)) return;
+    for (int jc = jrjcp1; jc < order; jc++) {
+      double sum = A[jrjc][jc];
+      for (int jm = 0; jm <= jrjcm1; jm++) sum -= A[jrjc][jm] * A[jm][jc];
+      A[jrjc][jc] = sum / A[jrjc][jrjc];
+    }
+  }
+}
+
+static void lusolv(double (*A)[5], double *c, int order) {
+  c[0] = c[0] / A[0][0];
+  for (int jr = 1; jr < order; jr++) {
+    double sum = c[jr];
+    for (int jm = 0; jm <= jr - 1; jm++) sum -= A[jr][jm] * c[jm];
+    c[jr] = sum / A[jr][jr];
+  }
+  for (int jrjr = 1; jrjr < order; jrjr++) {
+    int jr = (order - 1) - jrjr;
+    int jrp1 = jr + 1;
+    double sum = c[jr];
+    for (int jmjm = jrp1; jmjm < order; jmjm++) {
+      int jm = (order - 1) - jmjm + jrp1;
+      sum -= A[jr][jm] * c[jm];
+    }
+    c[jr] = sum;
+  }
+}
+
+static void matvec(jo_case *h, double *res, const double *A, const double *x) {
+  /* matTimesVecOverCVs, UgpWithCv.cpp:2580-2596 */
+  const jg_mesh *m = &h->m;
+  for (int c = 0; c < h->ncv; c++) {
+    for (int i = 0; i < 5; i++) res[5 * c + i] = 0.0;
+    for (int k = m->nbocv_i[c]; k < m->nbocv_i[c + 1]; k++) {
+      int nb = m->nbocv_v[k];
+      for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) res[5 * c + i] += A[25 * k + 5 * i + j] * x[5 * nb + j];
+    }
+  }
+}
+
+static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double *rhs, double zeroAbs, double zeroRel,
+                         int maxiter) {
+  /* solveCvVectorR5Bcgstab, UgpWithCv.cpp:2660-2876 */
+  int n = h->ncv;
+  const jg_mesh *m = &h->m;
+  double *res = dalloc(5 * n), *res0 = dalloc(5 * n), *pv = dalloc(5 * n), *v = dalloc(5 * n), *t = dalloc(5 * n),
+         *s = dalloc(5 * n), *phat = dalloc(5 * n), *shat = dalloc(5 * n), *LU = dalloc(25 * n);
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[25 * c], &A[25 * m->nbocv_i[c]], 25 * sizeof(double));
+    ludeco((double(*)[5]) & LU[25 * c], 5);
+  }
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  matvec(h, res, A, phi);
+  for (int k = 0; k < 5 * n; k++) { res[k] = rhs[k] - res[k]; res0[k] = res[k]; }
+  double res0_max = 0.0;
+  for (int c = 0; c < n; c++) {
+    double tmp[5];
+    memcpy(tmp, &res[5 * c], sizeof(tmp));
+    lusolv((double(*)[5]) & LU[25 * c], tmp, 5);
+    for (int i = 0; i < 5; i++) res0_max = dmax(res0_max, fabs(tmp[i]));
+  }
+  int iter = 0, done = 0;
+  double res_max = 0.0;
+  while (done == 0) {
+    iter++;
+    double rho_prime = -omega * rho;
+    double my_rho = 0.0;
+    for (int k = 0; k < 5 * n; k++) my_rho += res[k] * res0[k];
+    rho = my_rho;
+    if (fabs(rho_prime) < 1.0E-20) rho_prime = 1.0E-20;
+    double beta = alpha * rho / rho_prime;
+    for (int k = 0; k < 5 * n; k++) pv[k] = res[k] - beta * (pv[k] - omega * v[k]);
+    for (int c = 0; c < n; c++) {
+      memcpy(&phat[5 * c], &pv[5 * c], 5 * sizeof(double));
+      lusolv((double(*)[5]) & LU[25 * c], &phat[5 * c], 5);
+    }
+    matvec(h, v, A, phat);
+    double gamma = 0.0;
+    for (int k = 0; k < 5 * n; k++) gamma += v[k] * res0[k];
+    if (fabs(gamma) < 1.0E-20) gamma = 1.0E-20;
+    alpha = rho / gamma;
+    for (int k = 0; k < 5 * n; k++) s[k] = res[k] - alpha * v[k];
+    for (int c = 0; c < n; c++) {
+      memcpy(&shat[5 * c], &s[5 * c], 5 * sizeof(double));
+      lusolv((double(*)[5]) & LU[25 * c], &shat[5 * c], 5);
+    }
+    matvec(h, t, A, shat);
+    double b0 = 0.0, b1 = 0.0;
+    for (int k = 0; k < 5 * n; k++) { b0 += s[k] * t[k]; b1 += t[k] * t[k]; }
+    omega = b0 / (b1 + 1.0E-20);
+    for (int k = 0; k < 5 * n; k++) phi[k] += alpha * phat[k] + omega * shat[k];
+    matvec(h, res, A, phi);
+    for (int k = 0; k < 5 * n; k++) res[k] = rhs[k] - res[k];
+    res_max = 0.0;
+    for (int c = 0; c < n; c++) {
+      double tmp[5];
+      memcpy(tmp, &res[5 * c], sizeof(tmp));
+      lusolv((double(*)[5]) & LU[25 * c], tmp, 5);
+      for (int i = 0; i < 5; i++) res_max = dmax(res_max, fabs(tmp[i]));
+    }
+    if ((res_max <= zeroAbs) || (res_max / (res0_max + 1.0E-12) <= zeroRel)) done = 1;
+    else if (iter > maxiter) done = 2;
+  }
+  free(res); free(res0); free(pv); free(v); free(t); free(s); free(phat); free(shat); free(LU);
+  return iter;
+}
+
+static int solve_lusgs(jo_case *h, double *phi, const double *A, const double *rhs) {
+  /* solveCvVectorR5Lusgs, UgpWithCv.cpp:3172-3239: (D+L) x* = b with L applied to the input phi,
+   * then D x1 = D x* - U x* */
+  int n = h->ncv;
+  const jg_mesh *m = &h->m;
+  double *LU = dalloc(25 * n), *xn = dalloc(5 * n), *aux = dalloc(5 * n);
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[25 * c], &A[25 * m->nbocv_i[c]], 25 * sizeof(double));
+    ludeco((double(*)[5]) & LU[25 * c], 5);
+  }
+  for (int c = 0; c < n; c++) {
+    double low[5] = {0}, tmp[5];
+    for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+      int nb = m->nbocv_v[k];
+      if (nb < c)
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) low[i] += A[25 * k + 5 * i + j] * phi[5 * nb + j];
+    }
+    for (int i = 0; i < 5; i++) tmp[i] = rhs[5 * c + i] - low[i];
+    lusolv((double(*)[5]) & LU[25 * c], tmp, 5);
+    memcpy(&xn[5 * c], tmp, sizeof(tmp));
+  }
+  for (int c = 0; c < n; c++) {
+    double dg[5] = {0}, up[5] = {0};
+    int kd = m->nbocv_i[c];
+    for (int i = 0; i < 5; i++)
+      for (int j = 0; j < 5; j++) dg[i] += A[25 * kd + 5 * i + j] * xn[5 * c + j];
+    for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+      int nb = m->nbocv_v[k];
+      if (nb > c)
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) up[i] += A[25 * k + 5 * i + j] * xn[5 * nb + j];
+    }
+    for (int i = 0; i < 5; i++) aux[5 * c + i] = dg[i] - up[i];
+  }
+  for (int c = 0; c < n; c++) lusolv((double(*)[5]) & LU[25 * c], &aux[5 * c], 5);
+  memcpy(phi, aux, sizeof(double) * 5 * n);
+  free(LU); free(xn); free(aux);
+  return 1;
+}
+
+/* Block point relaxation as the GPU runs it (not in the reference): sweeps of
+ * block Jacobi, x <- D^-1 (b - O x) with D^-1 from ludeco + luinv. */
+static int solve_jacobi(jo_case *h, double *phi, const double *A, const double *rhs, int sweeps) {
+  int n = h->ncv;
+  const jg_mesh *m = &h->m;
+  double *LU = dalloc(25 * n), *xn = dalloc(5 * n);
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[25 * c], &A[25 * m->nbocv_i[c]], 25 * sizeof(double));
+    ludeco((double(*)[5]) & LU[25 * c], 5);
+  }
+  for (int s = 0; s < sweeps; s++) {
+    for (int c = 0; c < n; c++) {
+      double b[5];
+      for (int i = 0; i < 5; i++) b[i] = rhs[5 * c + i];
+      for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+        int nb = m->nbocv_v[k];
+        for (int i = 0; i < 5; i++)
+          for (int j = 0; j < 5; j++) b[i] -= A[25 * k + 5 * i + j] * phi[5 * nb + j];
+      }
+      lusolv((double(*)[5]) & LU[25 * c], b, 5);
+      memcpy(&xn[5 * c], b, sizeof(b));
+    }
+    memcpy(phi, xn, sizeof(double) * 5 * n);
+  }
+  free(LU); free(xn);
+  return sweeps;
+}
+
+int jo_solve(jo_case *h, double *dq, const double *A, const double *rhs, double zeroAbs, double zeroRel, int maxIter,
+             int solver) {
+  switch (solver) {
+    case JG_LS_BCGSTAB: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter);
+    case JG_LS_LUSGS: return solve_lusgs(h, dq, A, rhs);
+    case JG_LS_JACOBI: return solve_jacobi(h, dq, A, rhs, maxIter);
+    default: return -1;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* runBackwardEuler loop body, JoeWithModels.cpp:975-1159                    */
+/* ------------------------------------------------------------------------ */
+int jo_step(jo_case *h, int nsteps, double *resid) {
+  const jg_params *p = &h->p;
+  int n = h->ncv, nbs = h->nbs;
+  double *A = dalloc(25 * (size_t)nbs), *dq = dalloc(5 * n), *rhs = dalloc(5 * n);
+  double *rr = dalloc(n), *ru = dalloc(3 * n), *rE = dalloc(n);
+  int err = 0;
+  for (int it = 0; it < nsteps; it++) {
+    h->step++;
+    if ((h->step >= p->cfl_after) && (h->step % p->cfl_interval == 0) && (h->cfl < p->cfl_max)) h->cfl *= p->cfl_factor;
+    jo_calc_dt(h, h->cfl);
+    memset(A, 0, sizeof(double) * 25 * nbs);
+    memset(dq, 0, sizeof(double) * 5 * n);
+    jo_calc_rhs(h, rr, ru, rE, A, 1);
+    for (int c = 0; c < n; c++) {
+      rhs[5 * c + 0] = p->under_relax * rr[c];
+      rhs[5 * c + 1] = p->under_relax * ru[3 * c];
+      rhs[5 * c + 2] = p->under_relax * ru[3 * c + 1];
+      rhs[5 * c + 3] = p->under_relax * ru[3 * c + 2];
+      rhs[5 * c + 4] = p->under_relax * rE[c];
+      double tmp = h->m.cv_volume[c] / (h->local_dt[c]);
+      for (int i = 0; i < 5; i++) A[25 * h->m.nbocv_i[c] + 6 * i] += tmp;
+    }
+    jo_solve(h, dq, A, rhs, p->ls_abs, p->ls_rel, p->ls_max_iter, p->lin_solver);
+    for (int c = 0; c < n; c++) {
+      h->rho[c] += dq[5 * c];
+      for (int i = 0; i < 3; i++) h->rhou[3 * c + i] += dq[5 * c + 1 + i];
+      h->rhoE[c] += dq[5 * c + 4];
+    }
+    if (jo_calc_state(h) != 0) err = -1;
+    double r[5] = {0, 0, 0, 0, 0};
+    for (int c = 0; c < n; c++) {
+      r[0] += fabs(rr[c]);
+      for (int i = 0; i < 3; i++) r[1 + i] += fabs(ru[3 * c + i]);
+      r[4] += fabs(rE[c]);
+    }
+    if (resid) memcpy(resid, r, sizeof(r));
+  }
+  free(A); free(dq); free(rhs); free(rr); free(ru); free(rE);
+  return err;
+}

@@ -1,0 +1,40 @@
+/*
+ * joe_oracle.h -- CPU restatement of the reference's implicit finite-volume
+ * iteration (Joe: JoeWithModels / UgpWithCvCompFlow / UgpWithCv), used as the
+ * checker for the GPU library.  TEST INFRASTRUCTURE ONLY: nothing in the
+ * product links or calls it.  Every function cites the reference lines it
+ * restates; the restatement is pinned against dumps of the reference solver
+ * itself (oracle/_ref/ref_harness) by tests/test_oracle_vs_reference.py.
+ */
+#ifndef JOE_ORACLE_H
+#define JOE_ORACLE_H
+#include "../include/joe_b200.h"
+
+typedef struct jo_case jo_case;
+
+jo_case *jo_create(const jg_mesh *m, const jg_params *p);
+void jo_destroy(jo_case *h);
+void jo_set_state(jo_case *h, const double *rho, const double *rhou, const double *rhoE);
+void jo_get_state(jo_case *h, double *rho, double *rhou, double *rhoE);
+/* calcStateVariables + calcMaterialProperties + setBC (+ mut = 0); returns 0 or -1 */
+int jo_calc_state(jo_case *h);
+double jo_calc_dt(jo_case *h, double cfl);
+/* calcRhs; A (nbocv_s*25) may be NULL when implicit == 0 */
+void jo_calc_rhs(jo_case *h, double *rhs_rho, double *rhs_rhou, double *rhs_rhoE, double *A, int implicit);
+/* solveCoupledLinSysNS (BCGSTAB / LUSGS) plus the GPU's point relaxations; returns iterations */
+int jo_solve(jo_case *h, double *dq, const double *A, const double *rhs, double zeroAbs, double zeroRel,
+             int maxIter, int solver);
+/* nsteps iterations of the runBackwardEuler loop body; resid[5] = last L1 residual */
+int jo_step(jo_case *h, int nsteps, double *resid);
+/* named internal arrays: "vel","press","temp","enthalpy","sos","rho_bfa","T_bfa","vel_bfa","p_bfa",
+ * "h_bfa","gam_bfa","RoM_bfa","mul_fa","lamOcp_fa","mut_fa","grad_u","grad_rho","grad_p",
+ * "grad_enthalpy","alpha_rho","local_dt" */
+double *jo_array(jo_case *h, const char *name);
+double jo_cfl(jo_case *h);
+int jo_step_count(jo_case *h);
+
+/* per-face flux kernels, batched over n faces: states L/R [n][6] = (rho,u,v,w,p,gamma),
+ * area[n], nvec[n][3]; F[n][5]; AL/AR[n][25] (may be NULL) */
+void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area,
+                         const double *nvec, double *F, double *AL, double *AR);
+#endif

@@ -1,0 +1,105 @@
+"""Generates the golden fixtures in this directory by running the reference
+solver itself (oracle/_ref/ref_harness, compiled from the reference's own
+sources by oracle/Makefile) on small seeded meshes.
+
+Each fixture holds the reference's mesh arrays (its own cell/face order), the
+initial state, the case parameters, and the reference's outputs: primitive
+and boundary-face states, local time step, gradients, RHS, the implicit
+matrix A, one linear solve, and the state + L1 residuals after a few
+runBackwardEuler steps.
+
+    python tests/golden/make_golden.py     # needs the reference + g++
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from myjoe_b200 import case, meshgen  # noqa: E402
+from myjoe_b200.case import BC  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PERTURB = 0.05
+NSTEPS = 3
+
+
+def cases():
+    raw, _, prm = case.bump_case(8, 4, 2, jitter=0.15, seed=7)
+    visc = dataclasses.replace(prm, MU_MODE="SUTHERLAND", MU_REF=1.716e-5 * 2000.0, SPACE_INTEGRATION="ROE")
+    u = prm.U_INITIAL
+    bc_mix = dict(prm.bcs)
+    bc_mix["inlet"] = BC("CBC_SUBSONIC_INLET", (1.0, 0.0, 0.0, 300.0 * 1.05, 1.0e5 * 1.05 ** 3.5))
+    bc_mix["upper"] = BC("FARFIELD", u + (1.0e5, prm.RHO_REF, 1.4))
+    bc_mix["outlet"] = BC("NEUMANN")
+    bc_iso = dict(visc.bcs)
+    bc_iso["lower"] = BC("WALL", (350.0,))
+    rawp, _, prmp = case.plate_case(12, 8, 2)
+    yield "bump_hllc", raw, prm
+    yield "bump_roe", raw, dataclasses.replace(prm, SPACE_INTEGRATION="ROE")
+    yield "bump_ausm_first_order", raw, dataclasses.replace(prm, SPACE_INTEGRATION="AUSM", SECOND_ORDER=False)
+    yield "bump_hllc_symm_analytical_lusgs", raw, dataclasses.replace(prm, SYMM_BC="ANALYTICAL",
+                                                                     LINEAR_SOLVER_NS="LUSGS")
+    yield "bump_hllc_symm_new_sumdt", raw, dataclasses.replace(prm, SYMM_BC="NEW_NUMERIC", TIME_STEP="SUM_BASED",
+                                                               CFL_RAMP=(1, 1, 1.5, 5.0))
+    yield "bump_bc_mix", raw, dataclasses.replace(prm, bcs=bc_mix)
+    yield "bump_roe_laminar_isothermal", raw, dataclasses.replace(visc, bcs=bc_iso)
+    yield "bump_hllc_laminar_powerlaw_novisclim", raw, dataclasses.replace(visc, MU_MODE="POWERLAW",
+                                                                          SPACE_INTEGRATION="HLLC",
+                                                                          VISC_LIMITER=False)
+    yield "plate_roe", rawp, prmp
+
+
+def params_json(prm) -> str:
+    d = dataclasses.asdict(prm)
+    d["bcs"] = {k: [v.kind, list(v.values)] for k, v in prm.bcs.items()}
+    return json.dumps(d)
+
+
+def params_from_json(s: str):
+    d = json.loads(s)
+    bcs = {k: BC(v[0], tuple(v[1])) for k, v in d.pop("bcs").items()}
+    for k in ("CFL_RAMP", "U_INITIAL"):
+        d[k] = tuple(d[k])
+    return case.JoeParams(bcs=bcs, **d)
+
+
+def main():
+    for name, raw, prm in cases():
+        extra = "HARNESS_PERTURB = %g" % PERTURB
+        d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "dump")
+        prm_run = dataclasses.replace(prm, NSTEPS=NSTEPS)
+        r = refrun.run(lambda p: meshgen.write_msh(p, raw), prm_run.joe_in("mesh.msh", extra), "run")
+        keep = ["cvofa", "faocv_i", "faocv_v", "nbocv_i", "nbocv_v", "x_cv", "x_fa", "fa_normal", "cv_volume",
+                "nbocv_lsg_coeff", "boundary_fa_lsg_coeff", "init_rho", "init_rhou", "init_rhoE",
+                "press", "temp", "enthalpy", "sos", "vel", "rho_bfa", "T_bfa", "vel_bfa", "p_bfa", "h_bfa",
+                "mul_fa", "lamOcp_fa", "local_dt", "grad_u", "grad_rho", "grad_p", "grad_enthalpy",
+                "rhs_rho", "rhs_rhou", "rhs_rhoE", "A", "rhs_sys", "dq"]
+        out = {k: d[k] for k in keep if k in d}
+        out["final_rho"], out["final_rhou"], out["final_rhoE"] = r["final_rho"], r["final_rhou"], r["final_rhoE"]
+        out["resid"] = r["resid"]
+        out["meta"] = np.array(json.dumps(d["meta"]))
+        out["params"] = np.array(params_json(prm))
+        out["nsteps"] = np.array(NSTEPS)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print("wrote", name, d["meta"]["ncv"], "cells")
+
+
+def load(path):
+    z = np.load(path)
+    d = {k: z[k] for k in z.files}
+    d["meta"] = json.loads(str(d["meta"]))
+    d["meta"]["zones"] = [tuple(zz) for zz in d["meta"]["zones"]]
+    d["params"] = params_from_json(str(d["params"]))
+    return d
+
+
+if __name__ == "__main__":
+    main()

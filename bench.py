@@ -1,0 +1,328 @@
+"""Throughput of the implicit finite-volume iteration on B200.
+
+Workload (default): the laminar flat plate, 256 x 96 x 2 hexahedra (49,152
+cells), Re_L = 1e5, Mach 0.3, Roe flux, Sutherland viscosity, Pr 0.72,
+second-order LSQ reconstruction with the Barth-Jespersen limiter, backward
+Euler with 5x5 block Jacobians and 10 block point-relaxation sweeps per step,
+FP64.  A "step" is one backward-Euler iteration (CFL ramp, local time step,
+gradients, face loop + Jacobian assembly, 10 sweeps, update, state + BCs).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed]
+
+Multi-GPU: one process per GPU, each advancing its own replica of the case
+(the cases are independent; no collective on the data path), value = all
+cells x steps / max-over-ranks device time.  The 49k-cell working set fits
+the 126 MB L2, so L2 is flushed (a 256 MB write) between timed steps, outside
+the timed events.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SWEEPS = 10
+WORKLOAD = "laminar flat plate 256x96x2 hex (49,152 cells), Roe + Sutherland, 5x5 blocks, 10 relaxation sweeps/step"
+
+
+def plate_case():
+    from myjoe_b200 import case
+    raw, g, prm = case.plate_case(256, 96, 2)
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="JACOBI", LS_MAX_ITER=SWEEPS, CFL=1.0,
+                              CFL_RAMP=(10, 5, 1.2, 100.0))
+    return raw, g, prm
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(g, precision):
+    """Compulsory bytes per cell (each array counted once per pass): the face
+    loop (residual + Jacobian assembly) and one relaxation sweep, with this
+    mesh's internal faces per cell f, blocks per row m = 1 + f_cell, B = 5."""
+    d, i = 8, 4
+    s = 4 if precision == "mixed" else 8
+    B = 5
+    f = (g.nfa - g.nfa_b) / g.ncv            # internal faces per cell
+    m = 1.0 + 2.0 * f                        # blocks per row (diagonal + one per internal face of the cell)
+    face = d * (5 + 15 + 3 + 5) + f * (d * 6 + 4 * i) + s * (B * B + 2 * f * B * B)
+    sweep = s * m * B * B + d * 3 * B + i * (m - 1)
+    return face, sweep, f, m
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def reference_run(raw, prm, nsteps, nproc):
+    """The reference's own runBackwardEuler (oracle/_ref/ref_harness, built
+    from its sources) on the same mesh, BCGSTAB with MAX_ITER = 10; nproc
+    independent processes, one per host core.  Returns (cells*steps/s, secs)."""
+    from myjoe_b200 import meshgen
+    from oracle import refrun
+    if not refrun.available():
+        return None
+    rp = dataclasses.replace(prm, LINEAR_SOLVER_NS="BCGSTAB", LS_MAX_ITER=SWEEPS, NSTEPS=nsteps)
+    with tempfile.TemporaryDirectory(prefix="joe_ref_bench_") as d:
+        meshgen.write_msh(os.path.join(d, "mesh.msh"), raw)
+        with open(os.path.join(d, "Joe.in"), "w") as f:
+            f.write(rp.joe_in("mesh.msh"))
+        procs = []
+        for k in range(nproc):
+            wd = os.path.join(d, "r%d" % k)
+            os.mkdir(wd)
+            os.symlink(os.path.join(d, "mesh.msh"), os.path.join(wd, "mesh.msh"))
+            os.symlink(os.path.join(d, "Joe.in"), os.path.join(wd, "Joe.in"))
+            os.mkdir(os.path.join(wd, "out"))
+            procs.append(subprocess.Popen([refrun.HARNESS, "Joe.in", "0", "run", "out"], cwd=wd,
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+        secs = []
+        for p in procs:
+            out, _ = p.communicate(timeout=1800)
+            for line in out.splitlines():
+                if line.startswith("HARNESS_SECONDS"):
+                    secs.append(float(line.split()[1]))
+        if len(secs) != nproc:
+            return None
+    ncv = raw.ncv
+    return nproc * ncv * nsteps / max(secs), max(secs)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    raw, g, prm = plate_case()
+    nproc = os.cpu_count() or 1
+    nsteps = max(1, args.steps)
+    r = reference_run(raw, prm, nsteps, nproc)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref/ref_harness not built"}))
+        return
+    value, secs = r
+    line = {"metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": args.gpus,
+            "steps": nsteps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / nsteps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seed-generated mesh)", "impl": "reference",
+            "config": {"workload": WORKLOAD + " (reference: BCGSTAB MAX_ITER=10)", "cells": raw.ncv},
+            "cpu_baseline": {"value": value, "unit": "cell-iters/s", "cores": nproc, "kind": "reference",
+                             "sample": "%d backward-Euler iterations per process, %d independent processes "
+                                       "(one per host core)" % (nsteps, nproc)},
+            "e2e": {"value": value, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from myjoe_b200 import build, case, solver
+    if build.needs_build():
+        build.build()
+    raw, g, prm = plate_case()
+    precision = 1 if args.precision == "mixed" else 0
+    j = solver.JoeGpu(g, prm, precision=precision)
+    st0 = case.perturbed_state(g.x_cv, prm, 0.0)
+    j.set_state(*st0)
+    j.set_profiling(True)
+    kernels_per_step = j.step_kernel_count()
+    stream = torch.cuda.ExternalStream(j.stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(max(args.warmup, 3)):
+        j.step_async(1)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    face_ms, solve_ms = [], []
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            starts[k].record(stream)
+            j.step_async(1)
+            ends[k].record(stream)
+        prof = j.profile()
+        face_ms.append(prof["face_loop_ms"])
+        solve_ms.append(prof["linear_solve_ms"])
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)   # > L2: evict the case before the next timed step
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_s = sum(step_ms) / 1000.0
+    if world > 1:
+        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = world * g.ncv * args.steps / total_s
+    res = j.runBackwardEuler(1)
+    finite = bool(np.all(np.isfinite(res)))
+
+    # end to end through the C ABI from pinned host buffers: upload, step, download
+    n = g.ncv
+    h_rho = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    h_rhou = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    h_rhoE = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    h_res = torch.empty((1, 5), dtype=torch.float64, pin_memory=True).numpy()
+    rho, rhou, rhoE = j.get_state()
+    h_rho[:], h_rhou[:], h_rhoE[:] = rho, rhou, rhoE
+    import ctypes as C
+    from myjoe_b200.abi import dptr
+    L = solver.lib()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        solver._ck(L.jg_set_state(j.h, dptr(h_rho), dptr(h_rhou), dptr(h_rhoE)))
+        solver._ck(L.jg_step(j.h, 1, dptr(h_res)))
+        solver._ck(L.jg_get_state(j.h, dptr(h_rho), dptr(h_rhou), dptr(h_rhoE)))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * n * args.steps / e2e_s
+
+    # roofline of the dominant kernel, from the live in-graph events
+    face_b, sweep_b, f_int, m_blk = algorithmic_bytes(g, args.precision)
+    peak, peak_kind = measured_peaks()
+    face_avg = sum(face_ms) / len(face_ms)
+    solve_avg = sum(solve_ms) / len(solve_ms)
+    sweep_avg = solve_avg / SWEEPS
+    sweep_gbs = sweep_b * n / (sweep_avg * 1e-3) / 1e9
+    face_gbs = face_b * n / (face_avg * 1e-3) / 1e9
+    if solve_avg >= face_avg:
+        dom = {"kernel": "k_jacobi (block point-relaxation sweep)", "bound": "hbm", "achieved": sweep_gbs,
+               "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak, "traffic": None,
+               "bytes_per_cell": sweep_b, "launch_ms": sweep_avg}
+        other = {"kernel": "k_flux (face loop + Jacobian assembly)", "achieved": face_gbs, "frac": face_gbs / peak,
+                 "bytes_per_cell": face_b, "launch_ms": face_avg}
+    else:
+        dom = {"kernel": "k_flux (face loop + Jacobian assembly)", "bound": "hbm", "achieved": face_gbs,
+               "peak": peak, "unit": "GB/s", "frac": face_gbs / peak, "traffic": None,
+               "bytes_per_cell": face_b, "launch_ms": face_avg}
+        other = {"kernel": "k_jacobi (block point-relaxation sweep)", "achieved": sweep_gbs, "frac": sweep_gbs / peak,
+                 "bytes_per_cell": sweep_b, "launch_ms": sweep_avg}
+    dom["peak_source"] = peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind
+    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_path):
+        with open(prof_path) as f:
+            tr = json.load(f)
+        key = "k_jacobi" if dom["kernel"].startswith("k_jacobi") else "k_flux"
+        if key in tr and args.precision in tr[key]:
+            dom["traffic"] = tr[key][args.precision]["bytes_per_cell"] * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = reference_run(raw, prm, 6, 1)
+        if r is not None:
+            cpu = {"value": r[0], "unit": "cell-iters/s", "cores": 1, "kind": "reference",
+                   "sample": "6 backward-Euler iterations of the same 49,152-cell case by the reference "
+                             "(BCGSTAB MAX_ITER=10), one process"}
+
+    if rank == 0:
+        line = {"metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": world,
+                "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": 1000.0 * total_s / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64 residual / f32 Jacobian+relaxation",
+                "data": "synthetic (seed-generated mesh, uniform free-stream start)",
+                "config": {"workload": WORKLOAD, "cells": n, "internal_faces_per_cell": round(f_int, 4),
+                           "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
+                           "parallelism": "replicas" if world > 1 else "single case"},
+                "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": 5 * 8 * n,
+                        "d2h_bytes_per_step": 5 * 8 * n + 40},
+                "gpu_launches": kernels_per_step * args.steps,
+                "roofline": dom, "roofline_other": other,
+                "face_loop_ms": face_avg, "relaxation_ms": solve_avg,
+                "finite_residual": finite,
+                "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line))
+    j.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -96,6 +96,83 @@ typedef struct jg_params {
   int nscal;           /* transported scalars (0: laminar / inviscid) */
 } jg_params;
 
+
+typedef struct jg_case jg_case_t;   /* opaque per-case handle (device state + stream + graph) */
+
+/* Library / errors ---------------------------------------------------------- */
+int jg_version(void);
+const char *jg_last_error(void);   /* message of the last failing call on this thread */
+int jg_device_count(int *n);
+
+/* Case lifetime: replaces UgpWithCvCompFlow::initializeFromRestartFile's
+ * data setup (src/joe/UgpWithCvCompFlow.h:504-583) for the GPU: the mesh
+ * arrays are copied to device memory owned by the handle. */
+int jg_create(const jg_mesh *mesh, const jg_params *params, jg_case_t **out);
+int jg_destroy(jg_case_t *h);
+int jg_get_stream(jg_case_t *h, void **cuda_stream);   /* cudaStream_t of the case */
+
+/* Conserved state in/out (rho[ncv], rhou[ncv][3], rhoE[ncv]).  jg_set_state
+ * also runs the runBackwardEuler preamble (src/joe/JoeWithModels.cpp:942-957):
+ * calcStateVariables + calcMaterialProperties + setBC. */
+int jg_set_state(jg_case_t *h, const double *rho, const double *rhou, const double *rhoE);
+int jg_get_state(jg_case_t *h, double *rho, double *rhou, double *rhoE);
+
+/* calcStateVariables (UgpWithCvCompFlow.h:1662-1694) + calcMaterialProperties
+ * (1701-1753) + setBC (JoeWithModels.cpp:3857-4300) on the current state. */
+int jg_calc_state(jg_case_t *h);
+/* primitive cell state (vel[ncv][3], press, temp, enthalpy, sos); any pointer may be NULL */
+int jg_get_primitives(jg_case_t *h, double *vel, double *press, double *temp, double *enthalpy, double *sos);
+/* boundary-face state after setBC (rho_bfa, vel_bfa[nfa_b][3], p_bfa, T_bfa, h_bfa)
+ * and face viscosities mul_fa[nfa], lamOcp_fa[nfa]; any pointer may be NULL */
+int jg_get_bfa(jg_case_t *h, double *rho_bfa, double *vel_bfa, double *p_bfa, double *T_bfa, double *h_bfa,
+               double *mul_fa, double *lamOcp_fa);
+
+/* UgpWithCvCompFlow::calcDt (src/joe/UgpWithCvCompFlow.cpp:5-110): local time
+ * step per cell (local_dt[ncv], may be NULL) and its minimum. */
+int jg_calc_dt(jg_case_t *h, double cfl, double *dt_min, double *local_dt);
+
+/* JoeWithModels::calcRhs (src/joe/JoeWithModels.cpp:2564-2619): gradients,
+ * Euler + viscous fluxes, residual; with flagImplicit and A != NULL also the
+ * block Jacobian A[nbocv_s][5][5] in the reference's CSR layout. */
+int jg_calc_rhs(jg_case_t *h, double *rhs_rho, double *rhs_rhou, double *rhs_rhoE, double *A, int flagImplicit);
+/* gradients of the last jg_calc_rhs / step: calcCvVectorGrad / calcCvScalarGrad
+ * with limiting (src/common/UgpWithCv.h:803-1083); grad_u[ncv][3][3], others [ncv][3] */
+int jg_get_gradients(jg_case_t *h, double *grad_u, double *grad_rho, double *grad_p, double *grad_h);
+
+/* UgpWithCvCompFlow::solveCoupledLinSysNS (src/joe/UgpWithCvCompFlow.h:899-950):
+ * solves A dq = rhs with the solver of jg_params.lin_solver; dq is the initial
+ * guess on entry (BCGSTAB) and the solution on exit.  Also exported as
+ * solveLinSysNSCoupled. */
+int jg_solve_lin_sys(jg_case_t *h, double *dq, const double *A, const double *rhs, double zeroAbs, double zeroRel,
+                     int maxIter, int *iters);
+int solveLinSysNSCoupled(jg_case_t *h, double *dq, const double *A, const double *rhs, double zeroAbs,
+                         double zeroRel, int maxIter, int *iters);
+
+/* nsteps iterations of the JoeWithModels::runBackwardEuler loop body
+ * (src/joe/JoeWithModels.cpp:975-1159): CFL ramp, calcDt, calcRhs, linear
+ * solve, update, state + BC.  resid[nsteps][5] (may be NULL) receives the L1
+ * residual of every step.  Returns JG_ERR_STATE on a negative density or
+ * pressure or a NaN residual (doneSolver, JoeWithModels.h:42-95). */
+int jg_step(jg_case_t *h, int nsteps, double *resid);
+/* the same steps enqueued on the case stream without synchronising */
+int jg_step_async(jg_case_t *h, int nsteps);
+int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
+/* Timing hooks (no reference counterpart): with profiling on, the captured
+ * step records CUDA events around the face loop and the linear solve;
+ * jg_get_profile returns their device times (ms) for the last step. */
+int jg_set_profiling(jg_case_t *h, int on);
+int jg_get_profile(jg_case_t *h, double *ms);
+/* number of kernels one captured step launches */
+int jg_step_kernel_count(jg_case_t *h, int *n);
+
+/* Per-face Euler fluxes and implicit matrices, batched over n faces on the
+ * GPU: calcEulerFlux_{HLLC,Roe,AUSM} and calcEulerFluxMatrices_{HLLC,Roe}
+ * (src/joe/UgpWithCvCompFlow.cpp:120-709, 3281-3641).  L/R[n][6] =
+ * (rho, u, v, w, p, gamma), area[n], nvec[n][3] unit normals; F[n][5];
+ * AL/AR[n][5][5] may be NULL. */
+int jg_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
+                        double *F, double *AL, double *AR);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,872 @@
+// jg_api.cu -- host side of libjoe_b200.so: the C ABI declared in
+// include/joe_b200.h.  Builds the device layout of a case from the
+// reference's arrays, runs the operators, captures the backward-Euler step in
+// a CUDA graph, and converts between the reference's block-CSR matrix and the
+// device's sliced-ELL rows.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "jg_internal.h"
+
+using namespace jg;
+
+static thread_local std::string g_err;
+
+static int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(x)                                                                                       \
+  do {                                                                                              \
+    cudaError_t e_ = (x);                                                                           \
+    if (e_ != cudaSuccess)                                                                          \
+      return set_err(e_ == cudaErrorMemoryAllocation ? JG_ERR_NOMEM : JG_ERR_CUDA, "%s: %s (%s:%d)", \
+                     #x, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
+  } while (0)
+
+#define CKL()                                                                                      \
+  do {                                                                                             \
+    cudaError_t e_ = cudaGetLastError();                                                           \
+    if (e_ != cudaSuccess)                                                                         \
+      return set_err(JG_ERR_CUDA, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+struct jg_case {
+  // host copies needed for conversions
+  int ncv, nfa, nfa_b, nbs, nzones;
+  std::vector<int> nbocv_i, nbocv_v;
+  std::vector<int> cell_cols;     // [ncv+1] CSR over (cell, ELL column) -> neighbour
+  std::vector<int> col_nb;
+  std::vector<int> ell_off;
+  jg_params hp;
+  Params p;
+  Mesh m;
+  State st;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  size_t eltsz = 8;   // matrix element size
+  size_t ell_elems = 0;
+  int hist_cap = 0;
+  double* d_tmp = nullptr;  // BiCGSTAB work vectors (9 x 5N) + partials
+  double* d_red = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_sweeps = -1;
+  int primed = 0;           // state + BC computed since the last set_state
+  int profiling = 0;        // record events around the face loop and the relaxation in the graph
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t graph_kernels = 0;
+  double* d_io = nullptr;   // [5][N] staging for direct host<->device state copies
+};
+
+
+template <typename T>
+static int dmalloc(jg_case* h, T** p, size_t count) {
+  void* q = nullptr;
+  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  CK(cudaMalloc(&q, bytes));
+  CK(cudaMemset(q, 0, bytes));
+  h->allocs.push_back(q);
+  *p = (T*)q;
+  return JG_OK;
+}
+
+static int dmalloc_bytes(jg_case* h, void** p, size_t bytes) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, std::max<size_t>(bytes, 8)));
+  CK(cudaMemset(q, 0, std::max<size_t>(bytes, 8)));
+  h->allocs.push_back(q);
+  *p = q;
+  return JG_OK;
+}
+
+template <typename T>
+static int upload(jg_case* h, const T** dst, const T* src, size_t count) {
+  T* d = nullptr;
+  int rc = dmalloc(h, &d, count);
+  if (rc) return rc;
+  if (count) CK(cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = d;
+  return JG_OK;
+}
+
+#define RC(x)                \
+  do {                       \
+    int rc_ = (x);           \
+    if (rc_ != JG_OK) return rc_; \
+  } while (0)
+
+static Params make_params(const jg_params& q) {
+  Params p;
+  memset(&p, 0, sizeof(p));
+  p.gamma = q.gamma;
+  p.R = q.R_gas;
+  p.Pr = q.Pr;
+  p.PrTurb = q.PrTurb;
+  p.mu_mode = q.mu_mode;
+  p.flux = q.flux;
+  p.mu_ref = q.mu_ref;
+  p.mu_pow = q.mu_power_law;
+  p.SL_T = q.SL_Tref;
+  p.SL_S = q.SL_Sref;
+  p.T_ref = q.T_ref;
+  p.second_order = q.second_order;
+  p.limiter = q.limiter;
+  p.eps = q.eps;
+  p.visc_limiter = q.visc_limiter;
+  p.symm_bc = q.symm_bc;
+  p.ts_mode = q.time_step_mode;
+  p.ts_method = q.time_step;
+  p.dt_fixed = q.dt;
+  p.cfl_after = q.cfl_after;
+  p.cfl_interval = q.cfl_interval > 0 ? q.cfl_interval : 1;
+  p.cfl_factor = q.cfl_factor;
+  p.cfl_max = q.cfl_max;
+  p.under_relax = q.under_relax;
+  p.viscous = q.mu_ref > 0.0;
+  p.fp32 = q.precision == JG_PREC_MIXED;
+  return p;
+}
+
+static int check_params(const jg_params* q) {
+  if (!q) return set_err(JG_ERR_ARG, "null params");
+  if (q->flux < 0 || q->flux > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
+  if (q->symm_bc < 0 || q->symm_bc > 2) return set_err(JG_ERR_ARG, "unsupported SYMM_BC %d", q->symm_bc);
+  if (q->lin_solver < 0 || q->lin_solver > 3) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
+  if (q->precision != JG_PREC_FP64 && q->precision != JG_PREC_MIXED)
+    return set_err(JG_ERR_ARG, "unsupported precision %d", q->precision);
+  if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS))
+    return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI or SGS sweeps");
+  if (q->nscal != 0) return set_err(JG_ERR_ARG, "transported scalars are not supported by this build");
+  if (q->time_step_mode < 0 || q->time_step_mode > 2) return set_err(JG_ERR_ARG, "bad time step mode");
+  if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");
+  return JG_OK;
+}
+
+extern "C" {
+
+const char* jg_last_error(void) { return g_err.c_str(); }
+
+int jg_version(void) { return 1; }
+
+int jg_device_count(int* n) {
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) c = 0;
+  if (n) *n = c;
+  return c > 0 ? JG_OK : set_err(JG_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+}
+
+int jg_destroy(jg_case_t* h) {
+  if (!h) return JG_OK;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (int i = 0; i < 4; i++)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return JG_OK;
+}
+
+static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
+  const int N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b;
+  h->ncv = N;
+  h->nfa = nfa;
+  h->nfa_b = nfa_b;
+  h->nbs = mesh->nbocv_s;
+  h->nzones = mesh->nzones;
+  h->hp = *q;
+  h->p = make_params(*q);
+  h->eltsz = h->p.fp32 ? 4 : 8;
+  h->nbocv_i.assign(mesh->nbocv_i, mesh->nbocv_i + N + 1);
+  h->nbocv_v.assign(mesh->nbocv_v, mesh->nbocv_v + mesh->nbocv_s);
+  // boundary-face zones
+  std::vector<int> bzone(nfa_b, -1);
+  std::vector<DevZone> zones(std::max(1, mesh->nzones));
+  for (int z = 0; z < mesh->nzones; z++) {
+    const jg_zone& zn = mesh->zones[z];
+    if (zn.ifa_f < 0 || zn.ifa_l >= nfa_b || zn.ifa_f > zn.ifa_l + 1)
+      return set_err(JG_ERR_ARG, "zone %d face range [%d,%d] outside the boundary faces", z, zn.ifa_f, zn.ifa_l);
+    if (zn.kind < JG_BC_SYMMETRY || zn.kind > JG_BC_FARFIELD)
+      return set_err(JG_ERR_ARG, "zone %d: unsupported boundary kind %d", z, zn.kind);
+    zones[z].kind = zn.kind;
+    for (int k = 0; k < 8; k++) zones[z].v[k] = zn.v[k];
+    for (int f = zn.ifa_f; f <= zn.ifa_l; f++) bzone[f] = z;
+  }
+  for (int f = 0; f < nfa_b; f++)
+    if (bzone[f] < 0) return set_err(JG_ERR_ARG, "boundary face %d has no zone (reference: no bc set)", f);
+  // cell face slots
+  const int* fi = mesh->faocv_i;
+  const int* fv = mesh->faocv_v;
+  std::vector<Slot> slots(fi[N]);
+  std::vector<int> ncols(N, 0);
+  std::vector<int> bf_i(N + 1, 0), bf_v;
+  h->cell_cols.assign(N + 1, 0);
+  h->col_nb.clear();
+  for (int c = 0; c < N; c++) {
+    for (int k = fi[c]; k < fi[c + 1]; k++) {
+      int f = fv[k];
+      if (f < 0 || f >= nfa) return set_err(JG_ERR_ARG, "faocv_v[%d] = %d out of range", k, f);
+      Slot s;
+      s.f = f;
+      if (f < nfa_b) {
+        if (mesh->cvofa[2 * f] != c) return set_err(JG_ERR_ARG, "boundary face %d is not owned by cell %d", f, c);
+        s.nb = -1; s.side = 0; s.col = -1;
+        bf_v.push_back(f);
+      } else {
+        int c0 = mesh->cvofa[2 * f], c1 = mesh->cvofa[2 * f + 1];
+        if (c1 < 0 || c1 >= N || c0 < 0 || c0 >= N || (c0 != c && c1 != c))
+          return set_err(JG_ERR_ARG, "internal face %d does not connect cell %d", f, c);
+        s.side = (c0 == c) ? 0 : 1;
+        s.nb = (c0 == c) ? c1 : c0;
+        s.col = ncols[c]++;
+        h->col_nb.push_back(s.nb);
+      }
+      slots[k] = s;
+    }
+    bf_i[c + 1] = (int)bf_v.size();
+    h->cell_cols[c + 1] = (int)h->col_nb.size();
+  }
+  // sliced ELL
+  int nslices = (N + SLICE - 1) / SLICE;
+  h->ell_off.assign(nslices + 1, 0);
+  for (int s = 0; s < nslices; s++) {
+    int w = 0;
+    for (int c = s * SLICE; c < std::min(N, (s + 1) * SLICE); c++) w = std::max(w, ncols[c]);
+    h->ell_off[s + 1] = h->ell_off[s] + w;
+  }
+  int rows = h->ell_off[nslices];
+  std::vector<int> ell_nb((size_t)rows * SLICE, 0);
+  std::vector<uint8_t> ell_lower((size_t)rows * SLICE, 0);
+  for (int c = 0; c < N; c++) {
+    int s = c / SLICE, lane = c % SLICE;
+    int w = h->ell_off[s + 1] - h->ell_off[s];
+    for (int j = 0; j < w; j++) {
+      size_t e = (size_t)(h->ell_off[s] + j) * SLICE + lane;
+      if (j < ncols[c]) {
+        int nb = h->col_nb[h->cell_cols[c] + j];
+        ell_nb[e] = nb;
+        ell_lower[e] = nb < c ? 1 : 2;
+      } else {
+        ell_nb[e] = c;  // padding: zero block times the cell's own value
+      }
+    }
+  }
+  h->ell_elems = (size_t)rows * 25 * SLICE;
+  // device mesh
+  Mesh& m = h->m;
+  memset(&m, 0, sizeof(m));
+  m.ncv = N; m.nfa = nfa; m.nfa_b = nfa_b; m.nzones = mesh->nzones; m.nslices = nslices; m.ell_rows = rows;
+  RC(upload(h, &m.x_cv, mesh->x_cv, 3 * (size_t)N));
+  RC(upload(h, &m.vol, mesh->cv_volume, (size_t)N));
+  RC(upload(h, &m.x_fa, mesh->x_fa, 3 * (size_t)nfa));
+  RC(upload(h, &m.fa_n, mesh->fa_normal, 3 * (size_t)nfa));
+  RC(upload(h, &m.cvofa, mesh->cvofa, 2 * (size_t)nfa));
+  RC(upload(h, &m.slot_i, fi, (size_t)N + 1));
+  RC(upload(h, &m.slots, slots.data(), slots.size()));
+  RC(upload(h, &m.nb_i, mesh->nbocv_i, (size_t)N + 1));
+  RC(upload(h, &m.nb_v, mesh->nbocv_v, (size_t)mesh->nbocv_s));
+  RC(upload(h, &m.lsq, mesh->nbocv_lsg_coeff, 3 * (size_t)mesh->nbocv_s));
+  RC(upload(h, &m.bf_i, bf_i.data(), bf_i.size()));
+  RC(upload(h, &m.bf_v, bf_v.data(), bf_v.size()));
+  RC(upload(h, &m.blsq, mesh->boundary_fa_lsg_coeff, 3 * (size_t)nfa_b));
+  RC(upload(h, &m.bzone, bzone.data(), bzone.size()));
+  RC(upload(h, &m.zones, zones.data(), zones.size()));
+  RC(upload(h, &m.ell_off, h->ell_off.data(), h->ell_off.size()));
+  RC(upload(h, &m.ell_nb, ell_nb.data(), ell_nb.size()));
+  RC(upload(h, &m.ell_lower, ell_lower.data(), ell_lower.size()));
+  // device state
+  State& st = h->st;
+  memset(&st, 0, sizeof(st));
+  RC(dmalloc(h, &st.q, 5 * (size_t)N));
+  RC(dmalloc(h, &st.prim, 8 * (size_t)N));
+  RC(dmalloc(h, &st.bfa, 8 * (size_t)nfa_b));
+  RC(dmalloc(h, &st.mul_fa, (size_t)nfa));
+  RC(dmalloc(h, &st.lam_fa, (size_t)nfa));
+  RC(dmalloc(h, &st.gu, 9 * (size_t)N));
+  int separate = h->p.viscous && h->p.second_order && !h->p.visc_limiter && h->p.limiter;
+  if (separate) RC(dmalloc(h, &st.guv, 9 * (size_t)N));
+  else st.guv = st.gu;
+  RC(dmalloc(h, &st.grho, 3 * (size_t)N));
+  RC(dmalloc(h, &st.gp, 3 * (size_t)N));
+  RC(dmalloc(h, &st.gh, 3 * (size_t)N));
+  RC(dmalloc(h, &st.local_dt, (size_t)N));
+  RC(dmalloc(h, &st.rhs, 5 * (size_t)N));
+  RC(dmalloc(h, &st.b, 5 * (size_t)N));
+  RC(dmalloc_bytes(h, &st.D, 25 * (size_t)N * h->eltsz));
+  RC(dmalloc_bytes(h, &st.Dinv, 25 * (size_t)N * h->eltsz));
+  RC(dmalloc_bytes(h, &st.O, h->ell_elems * h->eltsz));
+  RC(dmalloc_bytes(h, &st.x0, 5 * (size_t)N * h->eltsz));
+  RC(dmalloc_bytes(h, &st.x1, 5 * (size_t)N * h->eltsz));
+  RC(dmalloc(h, &st.dq, 5 * (size_t)N));
+  RC(dmalloc(h, &st.blk, 5 * (size_t)grid_for(N, 128) + 5 * (size_t)grid_for(N, 256) + 16));
+  RC(dmalloc(h, &st.ctrl, 16));
+  RC(dmalloc(h, &st.err, 4));
+  h->hist_cap = 64;
+  st.hist_cap = h->hist_cap;
+  RC(dmalloc(h, &st.resid, 5 * (size_t)h->hist_cap));
+  double ctrl0[16] = {0};
+  ctrl0[0] = q->cfl;
+  CK(cudaMemcpy(st.ctrl, ctrl0, sizeof(ctrl0), cudaMemcpyHostToDevice));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return JG_OK;
+}
+
+int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
+  if (!mesh || !out) return set_err(JG_ERR_ARG, "null argument");
+  *out = nullptr;
+  RC(check_params(params));
+  if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
+    return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
+  jg_case* h = new jg_case();
+  int rc = build(h, mesh, params);
+  if (rc != JG_OK) {
+    std::string keep = g_err;
+    jg_destroy(h);
+    g_err = keep;
+    return rc;
+  }
+  *out = h;
+  return JG_OK;
+}
+
+int jg_get_stream(jg_case_t* h, void** stream) {
+  if (!h || !stream) return set_err(JG_ERR_ARG, "null argument");
+  *stream = (void*)h->stream;
+  return JG_OK;
+}
+
+static int check_err_flags(jg_case* h) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (e) {
+    CK(cudaMemsetAsync(h->st.err, 0, sizeof(int), h->stream));
+    if (e & 2) return set_err(JG_ERR_ARG, "unrecognised boundary condition");
+    return set_err(JG_ERR_STATE, "non-physical state (flags %d): negative density/pressure or NaN residual", e);
+  }
+  return JG_OK;
+}
+
+// calcStateVariables + calcMaterialProperties + setBC (+ mut = 0), the
+// runBackwardEuler preamble (JoeWithModels.cpp:942-957)
+static int prime(jg_case* h) {
+  launch_state(h->m, h->p, h->st, h->stream);
+  launch_face_props(h->m, h->p, h->st, h->stream);
+  launch_bc(h->m, h->p, h->st, h->stream);
+  CKL();
+  h->primed = 1;
+  return check_err_flags(h);
+}
+
+int jg_set_state(jg_case_t* h, const double* rho, const double* rhou, const double* rhoE) {
+  if (!h || !rho || !rhou || !rhoE) return set_err(JG_ERR_ARG, "null argument");
+  const size_t N = h->ncv;
+  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
+  // direct copies from the caller's arrays (pinned host memory makes them asynchronous DMA)
+  CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_pack_state((int)N, h->d_io, h->st.q, h->stream);
+  CK(cudaMemsetAsync(h->st.prim, 0, 8 * N * sizeof(double), h->stream));
+  return prime(h);
+}
+
+int jg_calc_state(jg_case_t* h) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  return prime(h);
+}
+
+int jg_get_state(jg_case_t* h, double* rho, double* rhou, double* rhoE) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  const size_t N = h->ncv;
+  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
+  launch_unpack_state((int)N, h->st.q, h->d_io, h->stream);
+  CKL();
+  if (rho) CK(cudaMemcpyAsync(rho, h->d_io, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhoE) CK(cudaMemcpyAsync(rhoE, h->d_io + 4 * N, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+int jg_get_primitives(jg_case_t* h, double* vel, double* press, double* temp, double* enthalpy, double* sos) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  const int N = h->ncv;
+  std::vector<double> pr(8 * (size_t)N);
+  CK(cudaMemcpyAsync(pr.data(), h->st.prim, pr.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < N; c++) {
+    if (vel)
+      for (int i = 0; i < 3; i++) vel[3 * c + i] = pr[8 * c + i];
+    if (press) press[c] = pr[8 * c + 3];
+    if (temp) temp[c] = pr[8 * c + 4];
+    if (enthalpy) enthalpy[c] = pr[8 * c + 5];
+    if (sos) sos[c] = pr[8 * c + 6];
+  }
+  return JG_OK;
+}
+
+int jg_get_bfa(jg_case_t* h, double* rho_bfa, double* vel_bfa, double* p_bfa, double* T_bfa, double* h_bfa,
+               double* mul_fa, double* lamOcp_fa) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  const int nb = h->nfa_b;
+  std::vector<double> b(8 * (size_t)std::max(nb, 1));
+  CK(cudaMemcpyAsync(b.data(), h->st.bfa, 8 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (mul_fa) CK(cudaMemcpyAsync(mul_fa, h->st.mul_fa, h->nfa * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (lamOcp_fa) CK(cudaMemcpyAsync(lamOcp_fa, h->st.lam_fa, h->nfa * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int f = 0; f < nb; f++) {
+    if (rho_bfa) rho_bfa[f] = b[8 * f];
+    if (vel_bfa)
+      for (int i = 0; i < 3; i++) vel_bfa[3 * f + i] = b[8 * f + 1 + i];
+    if (p_bfa) p_bfa[f] = b[8 * f + 4];
+    if (T_bfa) T_bfa[f] = b[8 * f + 5];
+    if (h_bfa) h_bfa[f] = b[8 * f + 6];
+  }
+  return JG_OK;
+}
+
+int jg_calc_dt(jg_case_t* h, double cfl, double* dt_min, double* local_dt) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (!h->primed) RC(prime(h));
+  launch_dt(h->m, h->p, h->st, 0, cfl, h->stream);
+  CKL();
+  double ctrl[3];
+  CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
+  if (local_dt) CK(cudaMemcpyAsync(local_dt, h->st.local_dt, h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (dt_min) *dt_min = ctrl[2];
+  return JG_OK;
+}
+
+// device D/O (sliced ELL) -> reference block CSR A[nbocv_s][5][5]
+static int download_csr(jg_case* h, double* A) {
+  const int N = h->ncv;
+  size_t es = h->eltsz;
+  std::vector<char> D(25 * (size_t)N * es), O(h->ell_elems * es);
+  CK(cudaMemcpyAsync(D.data(), h->st.D, D.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(O.data(), h->st.O, O.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  auto get = [&](const std::vector<char>& v, size_t i) -> double {
+    return es == 8 ? ((const double*)v.data())[i] : (double)((const float*)v.data())[i];
+  };
+  memset(A, 0, sizeof(double) * 25 * (size_t)h->nbs);
+  for (int c = 0; c < N; c++) {
+    int kd = h->nbocv_i[c];
+    for (int e = 0; e < 25; e++) A[25 * (size_t)kd + e] = get(D, (size_t)e * N + c);
+    int s = c / SLICE, lane = c % SLICE;
+    for (int j = 0; j < h->cell_cols[c + 1] - h->cell_cols[c]; j++) {
+      int nb = h->col_nb[h->cell_cols[c] + j];
+      int k = kd + 1;
+      while (k < h->nbocv_i[c + 1] && h->nbocv_v[k] != nb) k++;
+      if (k >= h->nbocv_i[c + 1]) return set_err(JG_ERR_ARG, "neighbour %d of cell %d missing from nbocv", nb, c);
+      for (int e = 0; e < 25; e++)
+        A[25 * (size_t)k + e] += get(O, ((size_t)(h->ell_off[s] + j) * 25 + e) * SLICE + lane);
+    }
+  }
+  return JG_OK;
+}
+
+// reference block CSR -> device D/O (a pair of cells sharing several faces keeps the block once)
+static int upload_csr(jg_case* h, const double* A) {
+  const int N = h->ncv;
+  size_t es = h->eltsz;
+  std::vector<char> D(25 * (size_t)N * es), O(h->ell_elems * es, 0);
+  auto put = [&](std::vector<char>& v, size_t i, double x) {
+    if (es == 8) ((double*)v.data())[i] = x;
+    else ((float*)v.data())[i] = (float)x;
+  };
+  std::vector<int> used;
+  for (int c = 0; c < N; c++) {
+    int kd = h->nbocv_i[c];
+    for (int e = 0; e < 25; e++) put(D, (size_t)e * N + c, A[25 * (size_t)kd + e]);
+    int s = c / SLICE, lane = c % SLICE;
+    used.clear();
+    for (int j = 0; j < h->cell_cols[c + 1] - h->cell_cols[c]; j++) {
+      int nb = h->col_nb[h->cell_cols[c] + j];
+      if (std::find(used.begin(), used.end(), nb) != used.end()) continue;
+      used.push_back(nb);
+      int k = kd + 1;
+      while (k < h->nbocv_i[c + 1] && h->nbocv_v[k] != nb) k++;
+      if (k >= h->nbocv_i[c + 1]) return set_err(JG_ERR_ARG, "neighbour %d of cell %d missing from nbocv", nb, c);
+      for (int e = 0; e < 25; e++) put(O, ((size_t)(h->ell_off[s] + j) * 25 + e) * SLICE + lane, A[25 * (size_t)k + e]);
+    }
+  }
+  CK(cudaMemcpyAsync(h->st.D, D.data(), D.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->st.O, O.data(), O.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+int jg_calc_rhs(jg_case_t* h, double* rhs_rho, double* rhs_rhou, double* rhs_rhoE, double* A, int flagImplicit) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (!h->primed) RC(prime(h));
+  int implicit = flagImplicit && A != nullptr;
+  launch_grad(h->m, h->p, h->st, h->stream);
+  launch_flux(h->m, h->p, h->st, implicit, 0, h->stream);
+  CKL();
+  const int N = h->ncv;
+  std::vector<double> r(5 * (size_t)N);
+  CK(cudaMemcpyAsync(r.data(), h->st.rhs, r.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < N; c++) {
+    if (rhs_rho) rhs_rho[c] = r[5 * c];
+    if (rhs_rhou)
+      for (int i = 0; i < 3; i++) rhs_rhou[3 * c + i] = r[5 * c + 1 + i];
+    if (rhs_rhoE) rhs_rhoE[c] = r[5 * c + 4];
+  }
+  if (implicit) RC(download_csr(h, A));
+  return JG_OK;
+}
+
+int jg_get_gradients(jg_case_t* h, double* grad_u, double* grad_rho, double* grad_p, double* grad_h) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  const int N = h->ncv;
+  if (grad_u) CK(cudaMemcpyAsync(grad_u, h->st.gu, 9 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (grad_rho) CK(cudaMemcpyAsync(grad_rho, h->st.grho, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (grad_p) CK(cudaMemcpyAsync(grad_p, h->st.gp, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (grad_h) CK(cudaMemcpyAsync(grad_h, h->st.gh, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+// partial-sum buffer of the BiCGSTAB reductions: launch_dot uses <= 1024
+// blocks, launch_resmax one per 256 cells; the last 16 entries hold scalars
+static size_t red_size(int N) { return (size_t)std::max(1024, grid_for(N, 256)) + 16; }
+
+// BiCGSTAB with the block-diagonal preconditioner, solveCvVectorR5Bcgstab
+// (UgpWithCv.cpp:2660-2876); operates on [5][N] vectors, phi in/out in d_tmp.
+static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, double zeroRel, int maxiter, int* iters) {
+  const int N = h->ncv;
+  const long n5 = 5L * N;
+  if (!h->d_tmp) {
+    RC(dmalloc(h, &h->d_tmp, 8 * (size_t)n5));
+    RC(dmalloc(h, &h->d_red, red_size(N)));
+  }
+  double *res = h->d_tmp, *res0 = res + n5, *p = res0 + n5, *v = p + n5, *t = v + n5, *s = t + n5, *phat = s + n5,
+         *shat = phat + n5;
+  double* part = h->d_red;
+  double* scal = h->d_red + red_size(N) - 16;
+  cudaStream_t S = h->stream;
+  auto dot = [&](const double* a, const double* b, double& out) -> int {
+    launch_dot((int)n5, a, b, part, scal, S);
+    CKL();
+    CK(cudaMemcpyAsync(&out, scal, sizeof(double), cudaMemcpyDeviceToHost, S));
+    CK(cudaStreamSynchronize(S));
+    return JG_OK;
+  };
+  auto resmax = [&](const double* r, double& out) -> int {
+    launch_resmax(h->m, h->st, r, part, scal, S);
+    CKL();
+    CK(cudaMemcpyAsync(&out, scal, sizeof(double), cudaMemcpyDeviceToHost, S));
+    CK(cudaStreamSynchronize(S));
+    return JG_OK;
+  };
+  CK(cudaMemsetAsync(p, 0, n5 * sizeof(double), S));
+  CK(cudaMemsetAsync(v, 0, n5 * sizeof(double), S));
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  launch_spmv(h->m, h->st, phi, res, S);
+  launch_lin3(n5, res, 1.0, rhs, -1.0, res, 0.0, nullptr, S);
+  CK(cudaMemcpyAsync(res0, res, n5 * sizeof(double), cudaMemcpyDeviceToDevice, S));
+  double res0_max = 0.0, res_max = 0.0;
+  RC(resmax(res, res0_max));
+  int iter = 0, done = 0;
+  while (!done) {
+    iter++;
+    double rho_prime = -omega * rho;
+    RC(dot(res, res0, rho));
+    if (fabs(rho_prime) < 1.0E-20) rho_prime = 1.0E-20;
+    double beta = alpha * rho / rho_prime;
+    // p = res - beta*(p - omega*v)
+    launch_lin3(n5, p, 1.0, res, -beta, p, beta * omega, v, S);
+    launch_precond(h->m, h->st, p, phat, S);
+    launch_spmv(h->m, h->st, phat, v, S);
+    double gamma;
+    RC(dot(v, res0, gamma));
+    if (fabs(gamma) < 1.0E-20) gamma = 1.0E-20;
+    alpha = rho / gamma;
+    launch_lin3(n5, s, 1.0, res, -alpha, v, 0.0, nullptr, S);
+    launch_precond(h->m, h->st, s, shat, S);
+    launch_spmv(h->m, h->st, shat, t, S);
+    double st_, tt_;
+    RC(dot(s, t, st_));
+    RC(dot(t, t, tt_));
+    omega = st_ / (tt_ + 1.0E-20);
+    launch_lin3(n5, phi, 1.0, phi, alpha, phat, omega, shat, S);
+    launch_spmv(h->m, h->st, phi, res, S);
+    launch_lin3(n5, res, 1.0, rhs, -1.0, res, 0.0, nullptr, S);
+    RC(resmax(res, res_max));
+    if ((res_max <= zeroAbs) || (res_max / (res0_max + 1.0E-12) <= zeroRel)) done = 1;
+    else if (iter > maxiter) done = 2;
+  }
+  if (iters) *iters = iter;
+  return JG_OK;
+}
+
+// transpose [N][5] <-> [5][N] helpers on the host
+static void to_soa(const double* aos, std::vector<double>& soa, int N) {
+  soa.resize(5 * (size_t)N);
+  for (int c = 0; c < N; c++)
+    for (int i = 0; i < 5; i++) soa[(size_t)i * N + c] = aos[5 * c + i];
+}
+
+int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rhs, double zeroAbs, double zeroRel,
+                     int maxIter, int* iters) {
+  if (!h || !dq || !A || !rhs) return set_err(JG_ERR_ARG, "null argument");
+  const int N = h->ncv;
+  RC(upload_csr(h, A));
+  launch_dinv(h->m, h->p, h->st, h->stream);
+  CK(cudaMemcpyAsync(h->st.b, rhs, 5 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CKL();
+  int it = 0;
+  switch (h->hp.lin_solver) {
+    case JG_LS_BCGSTAB: {
+      if (!h->d_tmp) {
+        RC(dmalloc(h, &h->d_tmp, 8 * 5 * (size_t)N));
+        RC(dmalloc(h, &h->d_red, red_size(N)));
+      }
+      double* phi = (double*)h->st.x0;
+      double* b = (double*)h->st.x1;
+      std::vector<double> soa;
+      to_soa(dq, soa, N);
+      CK(cudaMemcpyAsync(phi, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      to_soa(rhs, soa, N);
+      CK(cudaMemcpyAsync(b, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      RC(bcgstab(h, phi, b, zeroAbs, zeroRel, maxIter, &it));
+      launch_dq_from_x(h->m, h->p, h->st, phi, h->stream);
+    } break;
+    case JG_LS_LUSGS:
+      launch_lusgs(h->m, h->p, h->st, h->stream);
+      launch_dq_from_x(h->m, h->p, h->st, h->st.x1, h->stream);
+      it = 1;
+      break;
+    case JG_LS_JACOBI:
+    case JG_LS_SGS: {
+      int sweeps = std::max(1, maxIter);
+      launch_jacobi(h->m, h->p, h->st, sweeps, h->stream);
+      launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, h->stream);
+      it = sweeps;
+    } break;
+  }
+  CKL();
+  CK(cudaMemcpyAsync(dq, h->st.dq, 5 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (iters) *iters = it;
+  return JG_OK;
+}
+
+// one backward-Euler iteration on the device (runBackwardEuler loop body)
+static int enqueue_step(jg_case* h, int for_graph) {
+  cudaStream_t S = h->stream;
+  launch_ctrl_step(h->p, h->st, S);
+  launch_dt(h->m, h->p, h->st, 1, 0.0, S);
+  launch_grad(h->m, h->p, h->st, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
+  launch_flux(h->m, h->p, h->st, 1, 1, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
+  launch_resid(h->m, h->st, 1, S);
+  int solver = h->hp.lin_solver;
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
+  if (solver == JG_LS_LUSGS) {
+    launch_lusgs(h->m, h->p, h->st, S);
+    launch_dq_from_x(h->m, h->p, h->st, h->st.x1, S);
+  } else if (solver == JG_LS_JACOBI || solver == JG_LS_SGS) {
+    int sweeps = std::max(1, h->hp.ls_max_iter);
+    launch_jacobi(h->m, h->p, h->st, sweeps, S);
+    launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
+  } else {
+    if (for_graph) return set_err(JG_ERR_ARG, "BCGSTAB is not captured");
+    // host-driven BiCGSTAB on the assembled system, zero initial guess
+    const long n5 = 5L * h->ncv;
+    double* phi = (double*)h->st.x0;
+    double* b = (double*)h->st.x1;
+    CK(cudaMemsetAsync(phi, 0, n5 * sizeof(double), S));
+    // b is [N][5] in st.b; the solver wants [5][N]: transpose via dq_from_x's inverse on the host side is costly,
+    // so reuse the device: copy b into x1 as [5][N]
+    std::vector<double> tmp(n5), soa;
+    CK(cudaMemcpyAsync(tmp.data(), h->st.b, n5 * sizeof(double), cudaMemcpyDeviceToHost, S));
+    CK(cudaStreamSynchronize(S));
+    to_soa(tmp.data(), soa, h->ncv);
+    CK(cudaMemcpyAsync(b, soa.data(), n5 * sizeof(double), cudaMemcpyHostToDevice, S));
+    int it;
+    RC(bcgstab(h, phi, b, h->hp.ls_abs, h->hp.ls_rel, h->hp.ls_max_iter, &it));
+    launch_dq_from_x(h->m, h->p, h->st, phi, S);
+  }
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
+  launch_update_state(h->m, h->p, h->st, S);
+  launch_face_props(h->m, h->p, h->st, S);
+  launch_bc(h->m, h->p, h->st, S);
+  CKL();
+  return JG_OK;
+}
+
+static int ensure_graph(jg_case* h) {
+  int sweeps = std::max(1, h->hp.ls_max_iter);
+  if (h->graph && h->graph_sweeps == sweeps) return JG_OK;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(h, 1);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc != JG_OK) return rc;
+  if (e != cudaSuccess) return set_err(JG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+  h->graph_kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) h->graph_kernels++;
+  }
+  CK(cudaGraphInstantiate(&h->graph, g, 0));
+  cudaGraphDestroy(g);
+  h->graph_sweeps = sweeps;
+  return JG_OK;
+}
+
+int jg_step(jg_case_t* h, int nsteps, double* resid) {
+  if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
+  if (!h->primed) RC(prime(h));
+  if (nsteps > h->hist_cap) {
+    int cap = std::max(nsteps, 2 * h->hist_cap);
+    double* r = nullptr;
+    RC(dmalloc(h, &r, 5 * (size_t)cap));
+    h->st.resid = r;
+    h->hist_cap = cap;
+    h->st.hist_cap = cap;
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+  }
+  // history base: residual k of this call goes to resid[k]
+  double ctrl[16];
+  CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  ctrl[4] = ctrl[1];
+  CK(cudaMemcpyAsync(h->st.ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
+  bool use_graph = h->hp.lin_solver != JG_LS_BCGSTAB;
+  if (use_graph) RC(ensure_graph(h));
+  for (int k = 0; k < nsteps; k++) {
+    if (use_graph) CK(cudaGraphLaunch(h->graph, h->stream));
+    else RC(enqueue_step(h, 0));
+  }
+  CKL();
+  RC(check_err_flags(h));
+  if (resid && nsteps > 0)
+    CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+  return JG_OK;
+}
+
+// enqueue nsteps without synchronising (device-resident throughput runs)
+int jg_step_async(jg_case_t* h, int nsteps) {
+  if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
+  if (h->hp.lin_solver == JG_LS_BCGSTAB) return set_err(JG_ERR_ARG, "jg_step_async needs a captured solver");
+  if (!h->primed) RC(prime(h));
+  RC(ensure_graph(h));
+  for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(h->graph, h->stream));
+  return JG_OK;
+}
+
+int jg_get_cfl_step(jg_case_t* h, double* cfl, int* step) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  double ctrl[3];
+  CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (cfl) *cfl = ctrl[0];
+  if (step) *step = (int)ctrl[1];
+  return JG_OK;
+}
+
+int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
+                        double* F, double* AL, double* AR) {
+  if (n < 0 || !L || !R || !area || !nvec || !F) return set_err(JG_ERR_ARG, "bad argument");
+  if (kind < 0 || kind > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", kind);
+  if (n == 0) return JG_OK;
+  double *dL, *dR, *dA, *dN, *dF, *dAL = nullptr, *dAR = nullptr;
+  size_t b6 = 6 * (size_t)n * 8, b3 = 3 * (size_t)n * 8;
+  CK(cudaMalloc(&dL, b6));
+  CK(cudaMalloc(&dR, b6));
+  CK(cudaMalloc(&dA, (size_t)n * 8));
+  CK(cudaMalloc(&dN, b3));
+  CK(cudaMalloc(&dF, 5 * (size_t)n * 8));
+  if (AL) CK(cudaMalloc(&dAL, 25 * (size_t)n * 8));
+  if (AR) CK(cudaMalloc(&dAR, 25 * (size_t)n * 8));
+  CK(cudaMemcpy(dL, L, b6, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dR, R, b6, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dA, area, (size_t)n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dN, nvec, b3, cudaMemcpyHostToDevice));
+  launch_flux_faces(kind, n, dL, dR, dA, dN, dF, dAL, dAR, 0);
+  CKL();
+  CK(cudaMemcpy(F, dF, 5 * (size_t)n * 8, cudaMemcpyDeviceToHost));
+  if (AL) CK(cudaMemcpy(AL, dAL, 25 * (size_t)n * 8, cudaMemcpyDeviceToHost));
+  if (AR) CK(cudaMemcpy(AR, dAR, 25 * (size_t)n * 8, cudaMemcpyDeviceToHost));
+  cudaFree(dL); cudaFree(dR); cudaFree(dA); cudaFree(dN); cudaFree(dF);
+  if (dAL) cudaFree(dAL);
+  if (dAR) cudaFree(dAR);
+  return JG_OK;
+}
+
+}  // extern "C"
+
+extern "C" int jg_set_profiling(jg_case_t* h, int on) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  on = on ? 1 : 0;
+  if (on && !h->ev[0])
+    for (int i = 0; i < 4; i++) CK(cudaEventCreate(&h->ev[i]));
+  if (on != h->profiling && h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->profiling = on;
+  return JG_OK;
+}
+
+// device time (ms) of the last completed step: [0] face loop (gradients excluded),
+// [1] linear solve, waiting for that step to finish
+extern "C" int jg_get_profile(jg_case_t* h, double* ms) {
+  if (!h || !ms) return set_err(JG_ERR_ARG, "null argument");
+  if (!h->profiling) return set_err(JG_ERR_ARG, "profiling is off");
+  CK(cudaEventSynchronize(h->ev[3]));
+  float a = 0.f, b = 0.f;
+  CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+  CK(cudaEventElapsedTime(&b, h->ev[2], h->ev[3]));
+  ms[0] = a;
+  ms[1] = b;
+  return JG_OK;
+}
+
+// kernels launched by one captured step
+extern "C" int jg_step_kernel_count(jg_case_t* h, int* n) {
+  if (!h || !n) return set_err(JG_ERR_ARG, "null argument");
+  if (h->hp.lin_solver == JG_LS_BCGSTAB) return set_err(JG_ERR_ARG, "BCGSTAB steps are not captured");
+  if (!h->primed) RC(prime(h));
+  RC(ensure_graph(h));
+  *n = (int)h->graph_kernels;
+  return JG_OK;
+}
+
+extern "C" int solveLinSysNSCoupled(jg_case_t* h, double* dq, const double* A, const double* rhs, double zeroAbs,
+                                    double zeroRel, int maxIter, int* iters) {
+  return jg_solve_lin_sys(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, iters);
+}

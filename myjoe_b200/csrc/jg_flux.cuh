@@ -1,0 +1,444 @@
+// jg_flux.cuh -- pointwise FP64 face physics for the B200 face loop.
+//
+// Each function restates one reference routine (paths inside the reference
+// project); the arithmetic follows the reference term by term so that the
+// per-face results agree with it to rounding (the GPU contracts a*b+c into
+// FMA, the reference does not).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace jg {
+
+struct FState {
+  double rho, u[3], p, gam;
+};
+
+__device__ __forceinline__ double dot3(const double* a, const double* b) {
+  double d = 0.0;
+  d += a[0] * b[0];
+  d += a[1] * b[1];
+  d += a[2] * b[2];
+  return d;
+}
+
+// calcEulerFlux_HLLC, src/joe/UgpWithCvCompFlow.cpp:120-235 (k = 0, no scalars)
+__device__ inline void flux_hllc(double F[5], const FState& L, const FState& R, double area, const double nV[3]) {
+  double unL = dot3(L.u, nV);
+  double uLuL = dot3(L.u, L.u);
+  double cL = sqrt(L.gam * L.p / L.rho);
+  double hL = L.gam / (L.gam - 1.0) * L.p / L.rho + 0.5 * uLuL;
+  double eL = hL * L.rho - L.p;
+  double unR = dot3(R.u, nV);
+  double uRuR = dot3(R.u, R.u);
+  double cR = sqrt(R.gam * R.p / R.rho);
+  double hR = R.gam / (R.gam - 1.0) * R.p / R.rho + 0.5 * uRuR;
+  double eR = hR * R.rho - R.p;
+  double Rrho = sqrt(R.rho / L.rho);
+  double tmp = 1.0 / (1.0 + Rrho);
+  double vr[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
+  double uRoe = dot3(vr, nV);
+  double gpr = tmp * ((L.gam * L.p / L.rho + 0.5 * (L.gam - 1.0) * uLuL) +
+                      (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
+  double cRoe = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(vr, vr));
+  double sL = fmin(uRoe - cRoe, unL - cL);
+  double sR = fmax(uRoe + cRoe, unR + cR);
+  double sM = (L.p - R.p - L.rho * unL * (sL - unL) + R.rho * unR * (sR - unR)) /
+              (R.rho * (sR - unR) - L.rho * (sL - unL));
+  double pStar = R.rho * (unR - sR) * (unR - sM) + R.p;
+  if (sM >= 0.0) {
+    if (sL > 0.0) {
+      F[0] = L.rho * unL;
+      for (int i = 0; i < 3; i++) F[1 + i] = L.rho * L.u[i] * unL + L.p * nV[i];
+      F[4] = eL * unL + L.p * unL;
+    } else {
+      double inv = 1.0 / (sL - sM);
+      double sLmuL = sL - unL;
+      double rhoS = L.rho * sLmuL * inv;
+      double eS = (sLmuL * eL - L.p * unL + pStar * sM) * inv;
+      F[0] = rhoS * sM;
+      for (int i = 0; i < 3; i++) F[1 + i] = ((L.rho * L.u[i] * sLmuL + (pStar - L.p) * nV[i]) * inv) * sM + pStar * nV[i];
+      F[4] = (eS + pStar) * sM;
+    }
+  } else {
+    if (sR >= 0.0) {
+      double inv = 1.0 / (sR - sM);
+      double sRmuR = sR - unR;
+      double rhoS = R.rho * sRmuR * inv;
+      double eS = (sRmuR * eR - R.p * unR + pStar * sM) * inv;
+      F[0] = rhoS * sM;
+      for (int i = 0; i < 3; i++) F[1 + i] = ((R.rho * R.u[i] * sRmuR + (pStar - R.p) * nV[i]) * inv) * sM + pStar * nV[i];
+      F[4] = (eS + pStar) * sM;
+    } else {
+      F[0] = R.rho * unR;
+      for (int i = 0; i < 3; i++) F[1 + i] = R.rho * R.u[i] * unR + R.p * nV[i];
+      F[4] = eR * unR + R.p * unR;
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+// calcJacobianA, UgpWithCvCompFlow.cpp:666-709; nV carries the face area
+__device__ inline void jacobian_A(double* A, const double* vel, double pp, double rrho, const double* nV, double gamma) {
+  double km1 = gamma - 1.0;
+  double nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
+  double U_k = nVel[0] + nVel[1] + nVel[2];
+  double vsh = 0.5 * dot3(vel, vel);
+  double c2 = gamma * pp / rrho;  // c*c with c = sqrt(gamma p / rho)
+  double c = sqrt(c2);
+  c2 = c * c;
+  double ikm1 = 1.0 / km1;
+  A[0] = 0.0; A[1] = nV[0]; A[2] = nV[1]; A[3] = nV[2]; A[4] = 0.0;
+  A[5] = -vel[0] * (nVel[1] + nVel[2]) + nV[0] * (km1 * vsh - vel[0] * vel[0]);
+  A[6] = (2. - gamma) * nVel[0] + U_k;
+  A[7] = vel[0] * nV[1] - km1 * vel[1] * nV[0];
+  A[8] = vel[0] * nV[2] - km1 * vel[2] * nV[0];
+  A[9] = km1 * nV[0];
+  A[10] = -vel[1] * (nVel[0] + nVel[2]) + nV[1] * (km1 * vsh - vel[1] * vel[1]);
+  A[11] = -km1 * vel[0] * nV[1] + vel[1] * nV[0];
+  A[12] = (2. - gamma) * nVel[1] + U_k;
+  A[13] = vel[1] * nV[2] - km1 * vel[2] * nV[1];
+  A[14] = km1 * nV[1];
+  A[15] = -vel[2] * (nVel[0] + nVel[1]) + nV[2] * (km1 * vsh - vel[2] * vel[2]);
+  A[16] = -km1 * vel[0] * nV[2] + vel[2] * nV[0];
+  A[17] = -km1 * vel[1] * nV[2] + vel[2] * nV[1];
+  A[18] = (2. - gamma) * nVel[2] + U_k;
+  A[19] = km1 * nV[2];
+  A[20] = U_k * ((gamma - 2.) * vsh - c2 * ikm1);
+  A[21] = c2 * ikm1 * nV[0] - km1 * vel[0] * (nVel[1] + nVel[2]) - (km1 * vel[0] * vel[0] - vsh) * nV[0];
+  A[22] = c2 * ikm1 * nV[1] - km1 * vel[1] * (nVel[0] + nVel[2]) - (km1 * vel[1] * vel[1] - vsh) * nV[1];
+  A[23] = c2 * ikm1 * nV[2] - km1 * vel[2] * (nVel[0] + nVel[1]) - (km1 * vel[2] * vel[2] - vsh) * nV[2];
+  A[24] = gamma * U_k;
+}
+
+// calcSubSonicJacobeanHLLC, UgpWithCvCompFlow.cpp:605-659.  "S" is the side
+// whose star state is used (L when sM >= 0); "O" the other side.  AS/AO may be null.
+__device__ inline void subsonic_jac(double* AS, double* AO, double rhoS, const double* uS, double pS_, double eS_,
+                                    double qS, double psiS, double SS, double rhoSt, const double* rhouSt, double eSt,
+                                    const double* dSMdS, const double* dSMdO, const double* dpsdS, const double* dpsdO,
+                                    double SM, double pStar, double gamma, const double* nV) {
+  double gm1 = gamma - 1.0;
+  double om = 1.0 / (SS - SM);
+  if (AS) {
+    AS[0] = SS + rhoSt * dSMdS[0];
+    AS[1] = -nV[0] + rhoSt * dSMdS[1];
+    AS[2] = -nV[1] + rhoSt * dSMdS[2];
+    AS[3] = -nV[2] + rhoSt * dSMdS[3];
+    AS[4] = +rhoSt * dSMdS[4];
+    for (int r = 0; r < 3; r++) {
+      double* row = AS + 5 * (r + 1);
+      row[0] = qS * uS[r] - nV[r] * psiS * gm1 / 2.0 + nV[r] * dpsdS[0] + rhouSt[r] * dSMdS[0];
+      for (int k = 0; k < 3; k++) {
+        double base = (k == r) ? (SS - qS + nV[r] * (gamma - 2.0) * uS[r]) : (-uS[r] * nV[k] + nV[r] * gm1 * uS[k]);
+        row[1 + k] = base + nV[r] * dpsdS[1 + k] + rhouSt[r] * dSMdS[1 + k];
+      }
+      row[4] = -gm1 * nV[r] + nV[r] * dpsdS[4] + rhouSt[r] * dSMdS[4];
+    }
+    AS[20] = qS * (eS_ + pS_) / rhoS - qS * psiS * (gamma - 1.0) / 2.0 + SM * dpsdS[0] + (pStar + eSt) * dSMdS[0];
+    for (int k = 0; k < 3; k++)
+      AS[21 + k] = -nV[k] * (eS_ + pS_) / rhoS + gm1 * uS[k] * qS + SM * dpsdS[1 + k] + (pStar + eSt) * dSMdS[1 + k];
+    AS[24] = SS - qS * gamma + SM * dpsdS[4] + (pStar + eSt) * dSMdS[4];
+    for (int i = 0; i < 25; i++) AS[i] *= om;
+  }
+  if (AO) {
+    for (int i = 0; i < 5; i++) AO[i] = om * rhoSt * dSMdO[i];
+    for (int r = 0; r < 3; r++)
+      for (int i = 0; i < 5; i++) AO[5 * (r + 1) + i] = om * (nV[r] * dpsdO[i] + rhouSt[r] * dSMdO[i]);
+    for (int i = 0; i < 5; i++) AO[20 + i] = om * (dpsdO[i] * SM + (pStar + eSt) * dSMdO[i]);
+  }
+}
+
+// calcEulerFluxMatrices_HLLC, UgpWithCvCompFlow.cpp:242-595 (no scalars); AL/AR may be null
+__device__ inline void matrices_hllc(double* AL, double* AR, const FState& L, const FState& R, double area,
+                                     const double nV[3]) {
+  double unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u);
+  double cL = sqrt(L.gam * L.p / L.rho);
+  double eL = (L.gam / (L.gam - 1.0) * L.p / L.rho + 0.5 * uLuL) * L.rho - L.p;
+  double unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u);
+  double cR = sqrt(R.gam * R.p / R.rho);
+  double eR = (R.gam / (R.gam - 1.0) * R.p / R.rho + 0.5 * uRuR) * R.rho - R.p;
+  double Rrho = sqrt(R.rho / L.rho);
+  double tmp = 1.0 / (1.0 + Rrho);
+  double vr[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
+  double uRoe = dot3(vr, nV);
+  double gpr = tmp * ((L.gam * L.p / L.rho + 0.5 * (L.gam - 1.0) * uLuL) +
+                      (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
+  double cRoe = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(vr, vr));
+  double sL = fmin(uRoe - cRoe, unL - cL);
+  double sR = fmax(uRoe + cRoe, unR + cR);
+  double sM = (L.p - R.p - L.rho * unL * (sL - unL) + R.rho * unR * (sR - unR)) /
+              (R.rho * (sR - unR) - L.rho * (sL - unL));
+  double pStar = R.rho * (unR - sR) * (unR - sM) + R.p;
+  double gmean = 0.5 * (L.gam + R.gam);
+  if ((sM >= 0.0 && sL > 0.0) || (sM < 0.0 && sR < 0.0)) {
+    // supersonic: the flux depends on one side only
+    bool left = sM >= 0.0;
+    double* Aj = left ? AL : AR;
+    double* Az = left ? AR : AL;
+    const FState& S = left ? L : R;
+    if (Aj) {
+      double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+      jacobian_A(Aj, S.u, S.p, S.rho, nA, gmean);
+    }
+    if (Az)
+      for (int i = 0; i < 25; i++) Az[i] = 0.0;
+    return;
+  }
+  bool left = sM >= 0.0;  // star state of the left (sM >= 0) or right wave
+  const FState& S = left ? L : R;
+  double unS = left ? unL : unR, eS = left ? eL : eR, sS = left ? sL : sR;
+  double inv = 1.0 / (sS - sM);
+  double sSmu = sS - unS;
+  double rhoSt = S.rho * sSmu * inv;
+  double rhouSt[3];
+  for (int i = 0; i < 3; i++) rhouSt[i] = (S.rho * S.u[i] * sSmu + (pStar - S.p) * nV[i]) * inv;
+  double eSt = (sSmu * eS - S.p * unS + pStar * sM) * inv;
+  double invrhotld = 1.0 / (R.rho * (sR - unR) - L.rho * (sL - unL));
+  double dSMdUL[5] = {0, 0, 0, 0, 0}, dSMdUR[5] = {0, 0, 0, 0, 0};
+  double dpsdUL[5] = {0, 0, 0, 0, 0}, dpsdUR[5] = {0, 0, 0, 0, 0};
+  if (AL) {
+    double g1 = L.gam - 1.0;
+    dSMdUL[0] = -unL * unL + uLuL * g1 / 2.0 + sM * sL;
+    for (int i = 0; i < 3; i++) dSMdUL[1 + i] = nV[i] * (2.0 * unL - sL - sM) - g1 * L.u[i];
+    dSMdUL[4] = g1;
+    for (int i = 0; i < 5; i++) {
+      dSMdUL[i] *= invrhotld;
+      dpsdUL[i] = R.rho * (sR - unR) * dSMdUL[i];
+    }
+  }
+  if (AR) {
+    double g1 = R.gam - 1.0;
+    dSMdUR[0] = unR * unR - uRuR * g1 / 2.0 - sM * sR;
+    for (int i = 0; i < 3; i++) dSMdUR[1 + i] = -nV[i] * (2.0 * unR - sR - sM) + g1 * R.u[i];
+    dSMdUR[4] = -g1;
+    for (int i = 0; i < 5; i++) {
+      dSMdUR[i] *= invrhotld;
+      dpsdUR[i] = L.rho * (sL - unL) * dSMdUR[i];
+    }
+  }
+  if (left)
+    subsonic_jac(AL, AR, L.rho, L.u, L.p, eL, unL, uLuL, sL, rhoSt, rhouSt, eSt, dSMdUL, dSMdUR, dpsdUL, dpsdUR, sM,
+                 pStar, gmean, nV);
+  else
+    subsonic_jac(AR, AL, R.rho, R.u, R.p, eR, unR, uRuR, sR, rhoSt, rhouSt, eSt, dSMdUR, dSMdUL, dpsdUR, dpsdUL, sM,
+                 pStar, gmean, nV);
+  for (int side = 0; side < 2; side++) {
+    double* A = side == 0 ? AL : AR;
+    if (!A) continue;
+    const double* dSM = side == 0 ? dSMdUL : dSMdUR;
+    const double* dps = side == 0 ? dpsdUL : dpsdUR;
+    for (int i = 0; i < 5; i++) A[i] = A[i] * sM + dSM[i] * rhoSt;
+    for (int r = 0; r < 3; r++)
+      for (int i = 0; i < 5; i++) A[5 * (r + 1) + i] = A[5 * (r + 1) + i] * sM + dSM[i] * rhouSt[r] + dps[i] * nV[r];
+    for (int i = 0; i < 5; i++) A[20 + i] = (A[20 + i] + dps[i]) * sM + (eSt + pStar) * dSM[i];
+    for (int i = 0; i < 25; i++) A[i] *= area;
+  }
+}
+
+// calcEulerFlux_Roe, UgpWithCvCompFlow.cpp:3281-3380 (no entropy fix; a Roe-averaged
+// c^2 < 1e-12 leaves only the central part, as in the reference's early return)
+__device__ inline void flux_roe(double F[5], const FState& L, const FState& R, double area, const double nV[3]) {
+  double gamma = 0.5 * (L.gam + R.gam);
+  double gm1 = gamma - 1.0;
+  double run0 = L.rho * dot3(L.u, nV), run1 = R.rho * dot3(R.u, nV);
+  double rE0 = L.p / gm1 + 0.5 * L.rho * dot3(L.u, L.u);
+  double rE1 = R.p / gm1 + 0.5 * R.rho * dot3(R.u, R.u);
+  double H0 = (rE0 + L.p) / L.rho, H1 = (rE1 + R.p) / R.rho;
+  double ha = 0.5 * area;
+  F[0] = ha * (run0 + run1);
+  for (int i = 0; i < 3; i++) F[1 + i] = ha * (run0 * L.u[i] + run1 * R.u[i] + (L.p + R.p) * nV[i]);
+  F[4] = ha * (run0 * H0 + run1 * H1);
+  double s0 = sqrt(L.rho), s1 = sqrt(R.rho);
+  double t = 1.0 / (s0 + s1);
+  double ua = t * (L.u[0] * s0 + R.u[0] * s1), va = t * (L.u[1] * s0 + R.u[1] * s1), wa = t * (L.u[2] * s0 + R.u[2] * s1);
+  double hA = t * (H0 * s0 + H1 * s1);
+  double alA = 0.5 * (ua * ua + va * va + wa * wa);
+  double a2 = gm1 * (hA - alA);
+  if (a2 < 1.0e-12) return;
+  double aA = sqrt(a2);
+  double unA = ua * nV[0] + va * nV[1] + wa * nV[2];
+  double dr = R.rho - L.rho;
+  double dru = R.rho * R.u[0] - L.rho * L.u[0];
+  double drv = R.rho * R.u[1] - L.rho * L.u[1];
+  double drw = R.rho * R.u[2] - L.rho * L.u[2];
+  double drE = rE1 - rE0;
+  double l1 = fabs(unA), l2 = fabs(unA + aA), l3 = fabs(unA - aA);
+  double a1 = 0.5 * (l2 + l3), ab2 = 0.5 * (l2 - l3), ab3 = a1 - l1;
+  double ab4 = gm1 * (alA * dr - ua * dru - va * drv - wa * drw + drE);
+  double ab5 = unA * dr - nV[0] * dru - nV[1] * drv - nV[2] * drw;
+  double ab6 = ab3 * ab4 / a2 - ab2 * ab5 / aA;
+  double ab7 = ab3 * ab5 - ab2 * ab4 / aA;
+  F[0] -= ha * (l1 * dr + ab6);
+  F[1] -= ha * (l1 * dru + ua * ab6 - nV[0] * ab7);
+  F[2] -= ha * (l1 * drv + va * ab6 - nV[1] * ab7);
+  F[3] -= ha * (l1 * drw + wa * ab6 - nV[2] * ab7);
+  F[4] -= ha * (l1 * drE + hA * ab6 - unA * ab7);
+}
+
+// calcEulerFluxMatrices_Roe with calcPMatrix / calcInvPMatrix,
+// UgpWithCvCompFlow.cpp:3382-3559; AL/AR may be null
+__device__ inline void matrices_roe(double* AL, double* AR, const FState& L, const FState& R, double area,
+                                    const double nV[3]) {
+  double uLuL = dot3(L.u, L.u), uRuR = dot3(R.u, R.u);
+  double Rrho = sqrt(R.rho / L.rho);
+  double rr = Rrho * L.rho;
+  double tmp = 1.0 / (1.0 + Rrho);
+  double v[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
+  double uRoe = dot3(v, nV);
+  double gpr = tmp * ((L.gam * L.p / L.rho + 0.5 * (L.gam - 1.0) * uLuL) +
+                      (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
+  double c = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(v, v));
+  double gamma = 0.5 * (L.gam + R.gam);
+  double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+  if (AL) jacobian_A(AL, L.u, L.p, L.rho, nA, gamma);
+  if (AR) jacobian_A(AR, R.u, R.p, R.rho, nA, gamma);
+  double km1 = gamma - 1.0;
+  double rhooc = rr / c, rhoxc = rr * c, c2 = c * c;
+  double vS = dot3(v, v);
+  double vn = v[0] * nV[0] + v[1] * nV[1] + v[2] * nV[2];
+  double P[25], Q[25];
+  P[0] = nV[0]; P[1] = nV[1]; P[2] = nV[2]; P[3] = 0.5 * rhooc; P[4] = 0.5 * rhooc;
+  P[5] = v[0] * nV[0]; P[6] = v[0] * nV[1] - rr * nV[2]; P[7] = v[0] * nV[2] + rr * nV[1];
+  P[8] = 0.5 * (v[0] * rhooc + rr * nV[0]); P[9] = 0.5 * (v[0] * rhooc - rr * nV[0]);
+  P[10] = v[1] * nV[0] + rr * nV[2]; P[11] = v[1] * nV[1]; P[12] = v[1] * nV[2] - rr * nV[0];
+  P[13] = 0.5 * (v[1] * rhooc + rr * nV[1]); P[14] = 0.5 * (v[1] * rhooc - rr * nV[1]);
+  P[15] = v[2] * nV[0] - rr * nV[1]; P[16] = v[2] * nV[1] + rr * nV[0]; P[17] = v[2] * nV[2];
+  P[18] = 0.5 * (v[2] * rhooc + rr * nV[2]); P[19] = 0.5 * (v[2] * rhooc - rr * nV[2]);
+  P[20] = 0.5 * vS * nV[0] + rr * v[1] * nV[2] - rr * v[2] * nV[1];
+  P[21] = 0.5 * vS * nV[1] - rr * v[0] * nV[2] + rr * v[2] * nV[0];
+  P[22] = 0.5 * vS * nV[2] + rr * v[0] * nV[1] - rr * v[1] * nV[0];
+  P[23] = 0.5 * (0.5 * vS * rhooc + rr * vn + rhoxc / km1);
+  P[24] = 0.5 * (0.5 * vS * rhooc - rr * vn + rhoxc / km1);
+  Q[0] = nV[0] - nV[2] * v[1] / rr + nV[1] * v[2] / rr - nV[0] * 0.5 * km1 * vS / c2;
+  Q[1] = nV[0] * km1 * v[0] / c2;
+  Q[2] = nV[2] / rr + nV[0] * km1 * v[1] / c2;
+  Q[3] = -nV[1] / rr + nV[0] * km1 * v[2] / c2;
+  Q[4] = -nV[0] * km1 / c2;
+  Q[5] = nV[1] + nV[2] * v[0] / rr - nV[0] * v[2] / rr - nV[1] * 0.5 * km1 * vS / c2;
+  Q[6] = -nV[2] / rr + nV[1] * km1 * v[0] / c2;
+  Q[7] = nV[1] * km1 * v[1] / c2;
+  Q[8] = nV[0] / rr + nV[1] * km1 * v[2] / c2;
+  Q[9] = -nV[1] * km1 / c2;
+  Q[10] = nV[2] - nV[1] * v[0] / rr + nV[0] * v[1] / rr - nV[2] * 0.5 * km1 * vS / c2;
+  Q[11] = nV[1] / rr + nV[2] * km1 * v[0] / c2;
+  Q[12] = -nV[0] / rr + nV[2] * km1 * v[1] / c2;
+  Q[13] = nV[2] * km1 * v[2] / c2;
+  Q[14] = -nV[2] * km1 / c2;
+  Q[15] = -vn / rr + 0.5 * km1 * vS / rhoxc;
+  Q[16] = nV[0] / rr - km1 * v[0] / rhoxc;
+  Q[17] = nV[1] / rr - km1 * v[1] / rhoxc;
+  Q[18] = nV[2] / rr - km1 * v[2] / rhoxc;
+  Q[19] = km1 / rhoxc;
+  Q[20] = vn / rr + 0.5 * km1 * vS / rhoxc;
+  Q[21] = -nV[0] / rr - km1 * v[0] / rhoxc;
+  Q[22] = -nV[1] / rr - km1 * v[1] / rhoxc;
+  Q[23] = -nV[2] / rr - km1 * v[2] / rhoxc;
+  Q[24] = km1 / rhoxc;
+  double lam[5] = {fabs(uRoe), fabs(uRoe), fabs(uRoe), fabs(uRoe + c), fabs(uRoe - c)};
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) {
+      double pm = 0.0;
+      for (int k = 0; k < 5; k++) pm += P[5 * i + k] * lam[k] * Q[5 * k + j];
+      if (AL) AL[5 * i + j] = 0.5 * AL[5 * i + j] + 0.5 * pm * area;
+      if (AR) AR[5 * i + j] = 0.5 * AR[5 * i + j] - 0.5 * pm * area;
+    }
+}
+
+// calcEulerFlux_AUSM, UgpWithCvCompFlow.cpp:3566-3641
+__device__ inline void flux_ausm(double F[5], const FState& L, const FState& R, double area, const double nV[3]) {
+  double unL = dot3(L.u, nV), cL = sqrt(L.gam * L.p / L.rho);
+  double hL = (L.gam / (L.gam - 1.0)) * (L.p / L.rho) + 0.5 * dot3(L.u, L.u);
+  double mL = unL / cL;
+  double unR = dot3(R.u, nV), cR = sqrt(R.gam * R.p / R.rho);
+  double hR = (R.gam / (R.gam - 1.0)) * (R.p / R.rho) + 0.5 * dot3(R.u, R.u);
+  double mR = unR / cR;
+  double mLP = (fabs(mL) <= 1.0) ? 0.25 * (mL + 1.0) * (mL + 1.0) : 0.5 * (mL + fabs(mL));
+  double mRM = (fabs(mR) <= 1.0) ? -0.25 * (mR - 1.0) * (mR - 1.0) : 0.5 * (mR - fabs(mR));
+  double mF = mLP + mRM;
+  double pLP = (fabs(mL) <= 1.0) ? 0.25 * L.p * (mL + 1.0) * (mL + 1.0) * (2.0 - mL) : 0.5 * L.p * (mL + fabs(mL)) / mL;
+  double pRM = (fabs(mR) <= 1.0) ? 0.25 * R.p * (mR - 1.0) * (mR - 1.0) * (2.0 + mR) : 0.5 * R.p * (mR - fabs(mR)) / mR;
+  double pF = pLP + pRM;
+  double Phi = fabs(mF);
+  double mL_ = L.rho * cL, mR_ = R.rho * cR;
+  F[0] = 0.5 * (mF * (mL_ + mR_) - Phi * (mR_ - mL_));
+  for (int i = 0; i < 3; i++)
+    F[1 + i] = 0.5 * (mF * ((L.rho * cL * L.u[i]) + (R.rho * cR * R.u[i])) - Phi * ((R.rho * cR * R.u[i]) - (L.rho * cL * L.u[i]))) + nV[i] * pF;
+  F[4] = 0.5 * (mF * ((L.rho * cL * hL) + (R.rho * cR * hR)) - Phi * ((R.rho * cR * hR) - (L.rho * cL * hL)));
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+__device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& L, const FState& R, double area,
+                                           const double nV[3]) {
+  if (kind == 1) flux_roe(F, L, R, area, nV);
+  else if (kind == 2) flux_ausm(F, L, R, area, nV);
+  else flux_hllc(F, L, R, area, nV);
+}
+
+// implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061)
+__device__ __forceinline__ void euler_matrices(int kind, double* AL, double* AR, const FState& L, const FState& R,
+                                               double area, const double nV[3]) {
+  if (kind == 1) matrices_roe(AL, AR, L, R, area, nV);
+  else matrices_hllc(AL, AR, L, R, area, nV);
+}
+
+// One side of the viscous flux state (addViscFlux arguments).
+struct VSide {
+  double rho, u[3], h, T, R, gam;
+  const double* gu;  // grad_u [3][3] (row i = d u_i / d x_j)
+  const double* gh;  // grad_h [3]
+};
+
+// addViscFlux, UgpWithCvCompFlow.cpp:1521-1763 (laminar + mut, no k, no Reynolds
+// stresses), split into the flux and the implicit matrices.  The flux returns
+// the "left hand side" momentum/energy fluxes and the face stress tau.
+struct VFace {
+  double alpha, smag, area, mul, mut, keff;
+  double tau[3];
+};
+
+__device__ inline void visc_flux(double Fu[3], double& FE, VFace& vf, const VSide& s0, const VSide& s1, double mul,
+                                 double mut, double lamOcp, double PrTurb, const double* u_fa, double area,
+                                 const double nV[3], double smag, const double sV[3]) {
+  double alpha = dot3(nV, sV);
+  double g[9];
+  for (int i = 0; i < 9; i++) g[i] = 0.5 * (s0.gu[i] + s1.gu[i]);
+  double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
+  double div = g[0] + g[4] + g[8];
+  double tau[3];
+  for (int i = 0; i < 3; i++) {
+    double b = alpha * (s1.u[i] - s0.u[i]) / smag + g[3 * i + 0] * fC[0] + g[0 + i] * nV[0] + g[3 * i + 1] * fC[1] +
+               g[3 + i] * nV[1] + g[3 * i + 2] * fC[2] + g[6 + i] * nV[2];
+    double tl = mul * b - (2.0 / 3.0 * mul * div) * nV[i];
+    double tt = mut * b - (2.0 / 3.0 * mut * div) * nV[i];
+    tau[i] = tl + tt;
+  }
+  for (int i = 0; i < 3; i++) Fu[i] = -area * tau[i];
+  double keff = lamOcp + mut / PrTurb;
+  double enth = keff * (alpha * (s1.h - s0.h) / smag +
+                        0.5 * ((s0.gh[0] + s1.gh[0]) * fC[0] + (s0.gh[1] + s1.gh[1]) * fC[1] + (s0.gh[2] + s1.gh[2]) * fC[2]));
+  FE = -area * (enth + tau[0] * u_fa[0] + tau[1] * u_fa[1] + tau[2] * u_fa[2]);
+  vf.alpha = alpha; vf.smag = smag; vf.area = area; vf.mul = mul; vf.mut = mut; vf.keff = keff;
+  for (int i = 0; i < 3; i++) vf.tau[i] = tau[i];
+}
+
+// dF/dU x dU/dQ of the viscous flux (UgpWithCvCompFlow.cpp:717-745, 1692-1760) for
+// side 0 (A0) or side 1 (A1), scaled by sgn and added into the 5x5 row-major
+// accumulator acc (rows 1..4; the other entries are zero).
+__device__ inline void visc_jac_add(double* acc, double sgn, int side, const VFace& vf, const VSide& s,
+                                    const double* u_fa) {
+  double d = (side == 0) ? -(vf.mul + vf.mut) * vf.alpha / vf.smag * vf.area : (vf.mul + vf.mut) * vf.alpha / vf.smag * vf.area;
+  double f44 = (side == 0) ? -vf.area * vf.keff * vf.alpha / vf.smag : vf.area * vf.keff * vf.alpha / vf.smag;
+  double f4[3] = {vf.area * vf.tau[0] * 0.5 + u_fa[0] * d, vf.area * vf.tau[1] * 0.5 + u_fa[1] * d,
+                  vf.area * vf.tau[2] * 0.5 + u_fa[2] * d};
+  double ir = 1.0 / s.rho;
+  double uq0[3] = {-s.u[0] * ir, -s.u[1] * ir, -s.u[2] * ir};
+  double uq40 = s.gam * ir * (-s.h + s.R * s.T + 0.5 * dot3(s.u, s.u));
+  for (int r = 0; r < 3; r++) {
+    acc[5 * (r + 1) + 0] += sgn * (d * uq0[r]);
+    acc[5 * (r + 1) + 1 + r] += sgn * (d * ir);
+  }
+  acc[20] += sgn * (f4[0] * uq0[0] + f4[1] * uq0[1] + f4[2] * uq0[2] + f44 * uq40);
+  for (int k = 0; k < 3; k++) acc[21 + k] += sgn * (f4[k] * ir + f44 * (-s.gam * s.u[k] * ir));
+  acc[24] += sgn * (f44 * (s.gam * ir));
+}
+
+}  // namespace jg

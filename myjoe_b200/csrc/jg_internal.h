@@ -1,0 +1,129 @@
+// jg_internal.h -- device-side data layout of one case and the kernel launchers.
+//
+// Cells keep the reference's numbering.  Per-cell vectors are stored
+// cell-major ([N][k], a warp reads them contiguously); the implicit matrix is
+// stored per row in a sliced-ELL layout: 32-cell slices (one warp), each
+// slice padded to its widest row, components innermost across the 32 cells,
+// so that writing a row block (flux kernel) and reading it (relaxation) are
+// 256-byte coalesced transactions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/joe_b200.h"
+
+namespace jg {
+
+constexpr int SLICE = 32;
+
+struct DevZone {
+  int kind;
+  int pad;
+  double v[8];
+};
+
+// face slot of a cell: face index, neighbour (-1 on boundary faces), side (0:
+// the cell is cvofa[f][0], 1: it is cvofa[f][1]), ELL column (-1 on boundary faces)
+struct Slot {
+  int f, nb, side, col;
+};
+
+struct Mesh {
+  int ncv, nfa, nfa_b, nzones;
+  int nslices;
+  const double* x_cv;      // [N][3]
+  const double* vol;       // [N]
+  const double* x_fa;      // [nfa][3]
+  const double* fa_n;      // [nfa][3] area-weighted normal
+  const int* cvofa;        // [nfa][2]
+  const int* slot_i;       // [N+1] cell -> face slots (reference faocv order)
+  const Slot* slots;       // [faocv_s]
+  const int* nb_i;         // [N+1] nbocv CSR (diagonal first)
+  const int* nb_v;         // [nbocv_s]
+  const double* lsq;       // [nbocv_s][3]
+  const int* bf_i;         // [N+1] cell -> its boundary faces (increasing face index)
+  const int* bf_v;
+  const double* blsq;      // [nfa_b][3]
+  const int* bzone;        // [nfa_b] zone of each boundary face
+  const DevZone* zones;
+  const int* ell_off;      // [nslices+1] first ELL column row of each slice
+  const int* ell_nb;       // [ell_rows*32] neighbour per ELL entry (padding: the cell itself)
+  const uint8_t* ell_lower;// [ell_rows*32] 1 when the neighbour precedes the cell (LU-SGS)
+  int ell_rows;
+};
+
+// Per-case device state.  Primitive record: u,v,w,p,T,h,c,pad.  Boundary
+// record: rho,u,v,w,p,T,h,pad.  Gradients: [N][9] u, [N][3] rho, p, h.
+struct State {
+  double* q;        // [N][5] conserved (rho, rhou, rhoE)
+  double* prim;     // [N][8]
+  double* bfa;      // [nfa_b][8]
+  double* mul_fa;   // [nfa]
+  double* lam_fa;   // [nfa] lambda/cp
+  double* gu;       // [N][9] Euler (second order) gradient of velocity
+  double* guv;      // [N][9] viscous gradient of velocity (may alias gu)
+  double* grho;     // [N][3]
+  double* gp;       // [N][3]
+  double* gh;       // [N][3]
+  double* local_dt; // [N]
+  double* rhs;      // [N][5] RHS of calcRhs (rho, rhou, rhoE)
+  double* b;        // [N][5] under-relaxed rhs of the linear system
+  void* D;          // [25][N] diagonal block (double or float), component-major
+  void* Dinv;       // [25][N] its inverse
+  void* O;          // ELL off-diagonal blocks
+  void* x0;         // [5][N] relaxation vectors (double or float)
+  void* x1;
+  double* dq;       // [N][5]
+  double* blk;      // per-block partial sums (residual, dt min)
+  double* ctrl;     // device control: [0]=cfl [1]=step [2]=dt_min [3..]=flags
+  double* resid;    // [hist_cap][5] residual history (ring buffer)
+  int hist_cap;
+  int* err;         // error flags
+};
+
+struct Params {
+  double gamma, R, Pr, PrTurb;
+  int mu_mode, flux;
+  double mu_ref, mu_pow, SL_T, SL_S, T_ref;
+  int second_order, limiter;
+  double eps;
+  int visc_limiter, symm_bc;
+  int ts_mode, ts_method;
+  double dt_fixed;
+  int cfl_after, cfl_interval;
+  double cfl_factor, cfl_max;
+  double under_relax;
+  int viscous;      // mu_ref > 0
+  int fp32;         // matrix + relaxation in FP32
+};
+
+// launchers (jg_kernels.cu); all enqueue on stream s
+void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_ctrl_step(const Params& p, State& st, cudaStream_t s);
+void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl_cfl, double cfl, cudaStream_t s);
+void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
+void launch_resid(const Mesh& m, State& st, int hist_index_from_ctrl, cudaStream_t s);
+void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
+void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s);
+void launch_lusgs(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_dinv(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+// BiCGSTAB building blocks (FP64)
+void launch_spmv(const Mesh& m, const State& st, const double* x, double* y, cudaStream_t s);
+void launch_precond(const Mesh& m, const State& st, const double* x, double* y, cudaStream_t s);
+void launch_dot(int n, const double* a, const double* b, double* partial, double* out, cudaStream_t s);
+void launch_resmax(const Mesh& m, const State& st, const double* r, double* partial, double* out, cudaStream_t s);
+void launch_lin3(long n, double* out, double a, const double* x, double b, const double* y, double c, const double* z,
+                 cudaStream_t s);
+void launch_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
+                       double* F, double* AL, double* AR, cudaStream_t s);
+
+void launch_pack_state(int n, const double* io, double* q, cudaStream_t s);
+void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s);
+
+int grid_for(long n, int block);
+
+}  // namespace jg

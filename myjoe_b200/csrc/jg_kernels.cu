@@ -1,0 +1,1000 @@
+// jg_kernels.cu -- sm_100a kernels of the implicit finite-volume iteration.
+//
+// One thread per cell for every cell pass.  The face loop is cell-centric:
+// each cell walks its faces, evaluates every face flux in the face's own
+// orientation (cvofa[f][0] -> cvofa[f][1]) so that the two cells of a face
+// obtain bit-identical fluxes, and owns its residual, its diagonal block and
+// its row of off-diagonal blocks.  No atomics, no colouring, deterministic.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "jg_flux.cuh"
+#include "jg_internal.h"
+
+namespace jg {
+
+int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
+
+// ---------------------------------------------------------------------------
+// thermodynamics helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mu_law(const Params& p, double T) {
+  // calcMuLam / calcMaterialProperties, src/joe/UgpWithCvCompFlow.h:1601-1621, 1701-1753
+  if (p.mu_mode == JG_MU_SUTHERLAND) return p.mu_ref * pow(T / p.SL_T, 1.5) * (p.SL_T + p.SL_S) / (T + p.SL_S);
+  return p.mu_ref * pow(T / p.T_ref, p.mu_pow);
+}
+
+// calcStateVariables, UgpWithCvCompFlow.h:1662-1694: a non-positive pressure keeps the old one
+__device__ __forceinline__ void state_from_q(const Params& p, const double* q, double* prim, int* err) {
+  double r = q[0];
+  double ru[3] = {q[1], q[2], q[3]};
+  double u[3] = {ru[0] / r, ru[1] / r, ru[2] / r};
+  double pr = (p.gamma - 1.0) * (q[4] - 0.5 * dot3(ru, ru) / r);
+  double pp = prim[3];
+  if (pr > 0.0) pp = pr;
+  if (!(r > 0.0) || !(pp > 0.0)) atomicOr(err, 1);
+  double T = pp / (r * p.R);
+  prim[0] = u[0];
+  prim[1] = u[1];
+  prim[2] = u[2];
+  prim[3] = pp;
+  prim[4] = T;
+  prim[5] = p.gamma * p.R / (p.gamma - 1.0) * T;
+  prim[6] = sqrt(p.gamma * pp / r);
+}
+
+__global__ void k_state(Mesh m, Params p, State st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  double q[5], prim[8];
+  for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i];
+  for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
+  state_from_q(p, q, prim, st.err);
+  for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
+}
+
+// Q += dq (runBackwardEuler, JoeWithModels.cpp:1028-1035), then the new state.
+__global__ void k_update_state(Mesh m, Params p, State st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  double q[5], prim[8];
+  for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i] + st.dq[5 * c + i];
+  for (int i = 0; i < 5; i++) st.q[5 * c + i] = q[i];
+  for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
+  state_from_q(p, q, prim, st.err);
+  for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
+}
+
+// calcMaterialProperties on internal faces: distance-weighted face temperature
+__global__ void k_face_props(Mesh m, Params p, State st) {
+  int f = m.nfa_b + blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nfa) return;
+  int c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
+  double d0[3], d1[3];
+  for (int i = 0; i < 3; i++) {
+    d0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c0 + i];
+    d1[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c1 + i];
+  }
+  double w0 = sqrt(dot3(d0, d0)), w1 = sqrt(dot3(d1, d1));
+  double T = (w1 * st.prim[8 * c0 + 4] + w0 * st.prim[8 * c1 + 4]) / (w0 + w1);
+  double mu = mu_law(p, T);
+  st.mul_fa[f] = mu;
+  st.lam_fa[f] = mu / p.Pr;
+}
+
+__device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
+  double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
+  area = sqrt(dot3(n, n));
+  for (int i = 0; i < 3; i++) nV[i] = n[i] / area;
+}
+
+// setBC + ComputeBCProperties_T/H + the EOS density, JoeWithModels.cpp:3857-4300,
+// UgpWithCvCompFlow.h:1783-1839.  One thread per boundary face.
+__global__ void k_bc(Mesh m, Params p, State st) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nfa_b) return;
+  const DevZone z = m.zones[m.bzone[f]];
+  int c0 = m.cvofa[2 * f];
+  const double* pc = &st.prim[8 * c0];
+  const double* qc = &st.q[5 * c0];
+  double nV[3], area;
+  unit_normal(m, f, nV, area);
+  double T = 0.0, v[3] = {0.0, 0.0, 0.0}, pb = 0.0, h;
+  double rho_ff = 0.0;
+  double cp = p.gamma * p.R / (p.gamma - 1.0);
+  switch (z.kind) {
+    case JG_BC_CBC: {
+      if (dot3(z.v, nV) > 0.0) {
+        double un = dot3(pc, nV);
+        double mach = fabs(un) / pc[6];
+        T = pc[4];
+        for (int i = 0; i < 3; i++) v[i] = pc[i];
+        pb = (mach >= 1.0) ? pc[3] : z.v[4];
+      } else {
+        T = z.v[3];
+        for (int i = 0; i < 3; i++) v[i] = z.v[i];
+        pb = z.v[4];
+      }
+    } break;
+    case JG_BC_CBC_SUBSONIC_INLET: {
+      double r = qc[0];
+      double u[3] = {qc[1] / r, qc[2] / r, qc[3] / r};
+      double vm = sqrt(dot3(u, u));
+      for (int i = 0; i < 3; i++) v[i] = z.v[i] * vm;
+      double Ttot = z.v[3], ptot = z.v[4];
+      double htot = cp * Ttot;               // ComputeBCProperties_T with T = Ttot
+      double hs = htot - 0.5 * dot3(v, v);   // static enthalpy
+      T = hs * (p.gamma - 1.0) / (p.gamma * p.R);  // ComputeBCProperties_H
+      pb = ptot * pow(T / Ttot, p.gamma / (p.gamma - 1.0));
+      h = hs;
+    } break;
+    case JG_BC_CBC_SUBSONIC_OUTLET: {
+      pb = z.v[0];
+      for (int i = 0; i < 3; i++) v[i] = qc[1 + i] / qc[0];
+      T = pc[4];
+    } break;
+    case JG_BC_SYMMETRY: {
+      double un = dot3(nV, pc);
+      for (int i = 0; i < 3; i++) v[i] = pc[i] - 1.0 * un * nV[i];
+      T = pc[4];
+      pb = pc[3];
+    } break;
+    case JG_BC_NEUMANN: {
+      for (int i = 0; i < 3; i++) v[i] = qc[1 + i] / qc[0];
+      T = pc[4];
+      pb = pc[3];
+    } break;
+    case JG_BC_WALL: {
+      T = (z.v[0] > 0.0) ? z.v[0] : pc[4];
+      pb = pc[3];
+    } break;
+    case JG_BC_FARFIELD: {
+      double gb = z.v[5], pbc = z.v[3], rbc = z.v[4];
+      double gm1 = gb - 1.0, ovgm1 = 1.0 / gm1;
+      double c_bc = sqrt(gb * pbc / rbc);
+      double s_bc = pow(rbc, gb) / pbc;
+      double qn_bc = dot3(nV, z.v);
+      double vn_bc = qn_bc;
+      double qne = dot3(nV, pc);
+      double r0 = qc[0];
+      double ce = sqrt(p.gamma * pc[3] / r0);
+      double ac1 = (vn_bc > -c_bc) ? qne + 2.0 * ovgm1 * ce : qn_bc + 2.0 * ovgm1 * c_bc;
+      double ac2 = (vn_bc > c_bc) ? qne - 2.0 * ovgm1 * ce : qn_bc - 2.0 * ovgm1 * c_bc;
+      double qnf = 0.5 * (ac1 + ac2);
+      double cf = 0.25 * (ac1 - ac2) * gm1;
+      double sf;
+      if (vn_bc > 0) {
+        for (int i = 0; i < 3; i++) v[i] = pc[i] + (qnf - qne) * nV[i];
+        sf = pow(r0, p.gamma) / pc[3];
+      } else {
+        for (int i = 0; i < 3; i++) v[i] = z.v[i] + (qnf - qn_bc) * nV[i];
+        sf = s_bc;
+      }
+      rho_ff = pow((sf * cf * cf / p.gamma), ovgm1);
+      pb = rho_ff * cf * cf / p.gamma;
+      T = pb / (p.R * rho_ff);
+    } break;
+    default:
+      atomicOr(st.err, 2);
+      break;
+  }
+  if (z.kind != JG_BC_CBC_SUBSONIC_INLET) h = cp * T;
+  double* b = &st.bfa[8 * f];
+  b[0] = pb / (p.R * T);  // EOS, JoeWithModels.cpp:4291-4293
+  b[1] = v[0];
+  b[2] = v[1];
+  b[3] = v[2];
+  b[4] = pb;
+  b[5] = T;
+  b[6] = h;
+  if (p.viscous) {
+    double mu = mu_law(p, T);
+    st.mul_fa[f] = mu;
+    st.lam_fa[f] = mu / p.Pr;
+  }
+}
+
+// CFL ramp of runBackwardEuler (JoeWithModels.cpp:977-978), on the device so a
+// captured step graph can be replayed: ctrl[0] = cfl, ctrl[1] = step
+__global__ void k_ctrl_step(Params p, State st) {
+  double step = st.ctrl[1] + 1.0;
+  st.ctrl[1] = step;
+  long s = (long)step;
+  if ((s >= p.cfl_after) && (s % p.cfl_interval == 0) && (st.ctrl[0] < p.cfl_max)) st.ctrl[0] *= p.cfl_factor;
+}
+
+// calcDt, UgpWithCvCompFlow.cpp:5-110 (per-block minimum in st.blk)
+__global__ void k_dt(Mesh m, Params p, State st, int use_ctrl, double cfl_arg) {
+  __shared__ double smin[256];
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtc = 1.0e20;
+  double cfl = use_ctrl ? st.ctrl[0] : cfl_arg;
+  if (c < m.ncv) {
+    if (p.ts_mode == JG_TS_DT) {
+      dtc = p.dt_fixed;
+    } else {
+      const double* q = &st.q[5 * c];
+      double r = q[0];
+      double pr = st.prim[8 * c + 3];
+      double cs = sqrt(p.gamma * pr / r);
+      double ru[3] = {q[1], q[2], q[3]};
+      double vol = m.vol[c];
+      if (p.ts_method == JG_DT_MAX_BASED) {
+        double lmax = 0.0;
+        for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+          int f = m.slots[k].f;
+          double nV[3], area;
+          unit_normal(m, f, nV, area);
+          double Uk = dot3(ru, nV) / r;
+          double lam = (fabs(Uk) + cs) * area;
+          double ld = p.viscous ? 4.0 * (st.mul_fa[f] + 0.0) / r * area * area / vol : 0.0;
+          lam = fmax(lam, ld);
+          lmax = fmax(lmax, lam);
+        }
+        dtc = cfl * vol / lmax;
+      } else {
+        double lc = 0.0, ld = 0.0;
+        for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+          Slot s = m.slots[k];
+          double nV[3], area;
+          unit_normal(m, s.f, nV, area);
+          double Uk = dot3(ru, nV) / r;
+          double v2 = (s.nb >= 0) ? 0.5 * (m.vol[c] + m.vol[s.nb]) : 0.5 * vol;
+          if (s.nb >= 0 && s.side == 1) v2 = 0.5 * (m.vol[s.nb] + m.vol[c]);
+          lc += (fabs(Uk) + cs) * area;
+          if (p.viscous) ld += area * area * ((4.0 / 3.0) * (st.mul_fa[s.f] + 0.0) / r) / v2;
+        }
+        double dconv = cfl * vol / lc;
+        double dvisc = p.viscous ? 0.25 * cfl * vol / ld : 1.0e20;
+        dtc = fmin(dconv, dvisc);
+      }
+    }
+    st.local_dt[c] = dtc;
+  }
+  smin[threadIdx.x] = dtc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st.blk[blockIdx.x] = smin[0];
+}
+
+__global__ void k_dt_final(Mesh m, Params p, State st, int nblk) {
+  __shared__ double smin[256];
+  double v = 1.0e20;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) v = fmin(v, st.blk[i]);
+  smin[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st.ctrl[2] = smin[0];
+}
+
+__global__ void k_dt_min_all(Mesh m, State st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < m.ncv) st.local_dt[c] = st.ctrl[2];
+}
+
+// ---------------------------------------------------------------------------
+// LSQ gradients + smooth Barth-Jespersen limiter, UgpWithCv.h:803-1083.
+// Fields: velocity (ref = speed of sound), density, pressure, enthalpy.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double bj_factor(double phi_c, double phifa, double pmax, double pmin, double eps2) {
+  double dm = phifa - phi_c;
+  double dp = ((phifa - phi_c) >= 0.0) ? pmax - phi_c : pmin - phi_c;
+  return (dp * dp + 2.0 * dm * dp + eps2) / (dp * dp + 2 * dm * dm + dm * dp + eps2);
+}
+
+__global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, int visc_lim_u, int visc_lim_h,
+                       int separate_guv) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  const double* pc = &st.prim[8 * c];
+  double rc = st.q[5 * c];
+  // raw LSQ sums: diagonal, neighbours (nbocv order), then boundary faces
+  double gu[9], gr[3], gpr[3], gh[3];
+  int k0 = m.nb_i[c], k1 = m.nb_i[c + 1];
+  {
+    double w[3] = {m.lsq[3 * k0], m.lsq[3 * k0 + 1], m.lsq[3 * k0 + 2]};
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) gu[3 * i + j] = w[j] * pc[i];
+    for (int j = 0; j < 3; j++) {
+      gr[j] = w[j] * rc;
+      gpr[j] = w[j] * pc[3];
+      gh[j] = w[j] * pc[5];
+    }
+  }
+  double umax[3], umin[3], rmax = rc, rmin = rc, pmax = pc[3], pmin = pc[3], hmax = pc[5], hmin = pc[5];
+  for (int i = 0; i < 3; i++) umax[i] = umin[i] = pc[i];
+  for (int k = k0 + 1; k < k1; k++) {
+    int nb = m.nb_v[k];
+    double w[3] = {m.lsq[3 * k], m.lsq[3 * k + 1], m.lsq[3 * k + 2]};
+    const double* pn = &st.prim[8 * nb];
+    double rn = st.q[5 * nb];
+    for (int i = 0; i < 3; i++) {
+      for (int j = 0; j < 3; j++) gu[3 * i + j] += w[j] * pn[i];
+      umax[i] = fmax(umax[i], pn[i]);
+      umin[i] = fmin(umin[i], pn[i]);
+    }
+    for (int j = 0; j < 3; j++) {
+      gr[j] += w[j] * rn;
+      gpr[j] += w[j] * pn[3];
+      gh[j] += w[j] * pn[5];
+    }
+    rmax = fmax(rmax, rn); rmin = fmin(rmin, rn);
+    pmax = fmax(pmax, pn[3]); pmin = fmin(pmin, pn[3]);
+    hmax = fmax(hmax, pn[5]); hmin = fmin(hmin, pn[5]);
+  }
+  for (int k = m.bf_i[c]; k < m.bf_i[c + 1]; k++) {
+    int f = m.bf_v[k];
+    double w[3] = {m.blsq[3 * f], m.blsq[3 * f + 1], m.blsq[3 * f + 2]};
+    const double* b = &st.bfa[8 * f];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) gu[3 * i + j] += w[j] * b[1 + i];
+    for (int j = 0; j < 3; j++) {
+      gr[j] += w[j] * b[0];
+      gpr[j] += w[j] * b[4];
+      gh[j] += w[j] * b[6];
+    }
+  }
+  // limiter factors over the internal faces of the cell
+  double au[3] = {1.0, 1.0, 1.0}, ar = 1.0, ap = 1.0, ah = 1.0;
+  const double eps = p.eps;
+  double e2u = pow(eps * pc[6], 2.0);
+  double e2r = pow(fmax(eps * fabs(rc), 1.0e-8), 2.0);
+  double e2p = pow(fmax(eps * fabs(pc[3]), 1.0e-8), 2.0);
+  double e2h = pow(fmax(eps * fabs(pc[5]), 1.0e-8), 2.0);
+  bool lu[3], lr = (rmax - rmin) > 1.0e-12, lp = (pmax - pmin) > 1.0e-12, lh = (hmax - hmin) > 1.0e-12;
+  for (int i = 0; i < 3; i++) lu[i] = (umax[i] - umin[i]) > 1.0e-8;
+  if (p.limiter) {
+    for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+      Slot s = m.slots[k];
+      if (s.nb < 0) continue;
+      double r0[3];
+      for (int j = 0; j < 3; j++) r0[j] = m.x_fa[3 * s.f + j] - m.x_cv[3 * c + j];
+      for (int i = 0; i < 3; i++)
+        if (lu[i]) au[i] = fmin(au[i], bj_factor(pc[i], pc[i] + dot3(r0, &gu[3 * i]), umax[i], umin[i], e2u));
+      if (lr) ar = fmin(ar, bj_factor(rc, rc + dot3(r0, gr), rmax, rmin, e2r));
+      if (lp) ap = fmin(ap, bj_factor(pc[3], pc[3] + dot3(r0, gpr), pmax, pmin, e2p));
+      if (lh && do_visc) ah = fmin(ah, bj_factor(pc[5], pc[5] + dot3(r0, gh), hmax, hmin, e2h));
+    }
+    for (int i = 0; i < 3; i++)
+      if (!lu[i]) au[i] = 0.0;
+    if (!lr) ar = 0.0;
+    if (!lp) ap = 0.0;
+    if (!lh) ah = 0.0;
+  }
+  if (do_euler) {
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) st.gu[9 * c + 3 * i + j] = p.limiter ? gu[3 * i + j] * au[i] : gu[3 * i + j];
+    for (int j = 0; j < 3; j++) {
+      st.grho[3 * c + j] = p.limiter ? gr[j] * ar : gr[j];
+      st.gp[3 * c + j] = p.limiter ? gpr[j] * ap : gpr[j];
+    }
+  }
+  if (do_visc) {
+    if (separate_guv || !do_euler) {
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) st.guv[9 * c + 3 * i + j] = visc_lim_u ? gu[3 * i + j] * au[i] : gu[3 * i + j];
+    }
+    for (int j = 0; j < 3; j++) st.gh[3 * c + j] = visc_lim_h ? gh[j] * ah : gh[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face loop (calcEulerFlux + calcViscousFluxNS, JoeWithModels.cpp:2621-3855)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, int c) {
+  FState s;
+  s.rho = st.q[5 * c];
+  for (int i = 0; i < 3; i++) s.u[i] = st.prim[8 * c + i];
+  s.p = st.prim[8 * c + 3];
+  s.gam = p.gamma;
+  return s;
+}
+
+// second-order reconstruction at x_fa with the first-order fallback, JoeWithModels.cpp:2832-2921
+__device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const State& st, int c, int f) {
+  FState s = cell_fstate(p, st, c);
+  if (!p.second_order) return s;
+  double r0[3];
+  for (int i = 0; i < 3; i++) r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+  double rr = s.rho + dot3(r0, &st.grho[3 * c]);
+  double pp = s.p + dot3(r0, &st.gp[3 * c]);
+  if ((pp <= 0.0) || (rr <= 0.0)) return s;
+  s.rho = rr;
+  s.p = pp;
+  for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
+  return s;
+}
+
+__device__ __forceinline__ VSide cell_vside(const Params& p, const State& st, int c) {
+  VSide v;
+  v.rho = st.q[5 * c];
+  for (int i = 0; i < 3; i++) v.u[i] = st.prim[8 * c + i];
+  v.h = st.prim[8 * c + 5];
+  v.T = st.prim[8 * c + 4];
+  v.R = p.R;
+  v.gam = p.gamma;
+  v.gu = &st.guv[9 * c];
+  v.gh = &st.gh[3 * c];
+  return v;
+}
+
+template <typename BT>
+__device__ __forceinline__ size_t ell_index(const Mesh& m, int c, int col, int e) {
+  int slice = c / SLICE, lane = c % SLICE;
+  return ((size_t)(m.ell_off[slice] + col) * 25 + e) * SLICE + lane;
+}
+
+// 5x5 LU without pivoting + inverse, ludeco / luinv (UgpWithCv.cpp:2489-2577)
+__device__ inline void block_inverse(double* A, double* Ai) {
+  for (int jc = 1; jc < 5; jc++) A[jc] /= A[0];
+  for (int jrjc = 1;; jrjc++) {
+    for (int jr = jrjc; jr < 5; jr++) {
+      double sum = A[5 * jr + jrjc];
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jr + jm] * A[5 * jm + jrjc];
+      A[5 * jr + jrjc] = sum;
+    }
+    if (jrjc == 4) break;
+    for (int jc = jrjc + 1; jc < 5; jc++) {
+      double sum = A[5 * jrjc + jc];
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jrjc + jm] * A[5 * jm + jc];
+      A[5 * jrjc + jc] = sum / A[5 * jrjc + jrjc];
+    }
+  }
+  for (int col = 0; col < 5; col++) {
+    double cv[5];
+    for (int i = 0; i < 5; i++) cv[i] = (i == col) ? 1.0 : 0.0;
+    cv[0] = cv[0] / A[0];
+    for (int jr = 1; jr < 5; jr++) {
+      double sum = cv[jr];
+      for (int jm = 0; jm < jr; jm++) sum -= A[5 * jr + jm] * cv[jm];
+      cv[jr] = sum / A[5 * jr + jr];
+    }
+    for (int jr = 3; jr >= 0; jr--) {
+      double sum = cv[jr];
+      for (int jm = jr + 1; jm < 5; jm++) sum -= A[5 * jr + jm] * cv[jm];
+      cv[jr] = sum;
+    }
+    for (int i = 0; i < 5; i++) Ai[5 * i + col] = cv[i];
+  }
+}
+
+template <typename BT>
+__global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
+  extern __shared__ double sD[];  // [25][blockDim.x] diagonal-block accumulators
+  __shared__ double sres[5][128];
+  const int t = threadIdx.x, bd = blockDim.x;
+  int c = blockIdx.x * bd + t;
+  bool active = c < m.ncv;
+  double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    for (int e = 0; e < 25; e++) sD[e * bd + t] = 0.0;
+    BT* O = (BT*)st.O;
+    const int kind = p.flux;
+    for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+      const Slot s = m.slots[k];
+      const int f = s.f;
+      double nV[3], area;
+      unit_normal(m, f, nV, area);
+      if (s.nb >= 0) {
+        // ---------------- internal face ----------------
+        const int c0 = s.side == 0 ? c : s.nb;
+        const int c1 = s.side == 0 ? s.nb : c;
+        const double sg = s.side == 0 ? -1.0 : 1.0;  // residual sign of this cell
+        {
+          FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
+          double F[5];
+          euler_flux(kind, F, L, R, area, nV);
+          for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
+        }
+        double Ob[25];
+        if (implicit) {
+          FState L0 = cell_fstate(p, st, c0), R0 = cell_fstate(p, st, c1);
+          double Apl[25], Ami[25];
+          euler_matrices(kind, Apl, Ami, L0, R0, area, nV);
+          // row of c0: D += Apl, O(c0,c1) = Ami ; row of c1: D -= Ami, O(c1,c0) = -Apl
+          if (s.side == 0) {
+            for (int e = 0; e < 25; e++) { sD[e * bd + t] += Apl[e]; Ob[e] = Ami[e]; }
+          } else {
+            for (int e = 0; e < 25; e++) { sD[e * bd + t] -= Ami[e]; Ob[e] = -Apl[e]; }
+          }
+        }
+        if (p.viscous) {
+          VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
+          double sV[3];
+          for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
+          double smag = sqrt(dot3(sV, sV));
+          for (int i = 0; i < 3; i++) sV[i] /= smag;
+          double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
+          double Fu[3], FE;
+          VFace vf;
+          visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, ufa, area, nV, smag, sV);
+          for (int i = 0; i < 3; i++) rhs[1 + i] += sg * Fu[i];
+          rhs[4] += sg * FE;
+          if (implicit) {
+            // row of c0: D -= A0, O -= A1 ; row of c1: D += A1, O += A0  (calcViscousFluxNS 3678-3696)
+            double Dv[25];
+            for (int e = 0; e < 25; e++) Dv[e] = 0.0;
+            if (s.side == 0) {
+              visc_jac_add(Dv, -1.0, 0, vf, v0, ufa);
+              visc_jac_add(Ob, -1.0, 1, vf, v1, ufa);
+            } else {
+              visc_jac_add(Dv, 1.0, 1, vf, v1, ufa);
+              visc_jac_add(Ob, 1.0, 0, vf, v0, ufa);
+            }
+            for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
+          }
+        }
+        if (implicit)
+          for (int e = 0; e < 25; e++) O[ell_index<BT>(m, c, s.col, e)] = (BT)Ob[e];
+      } else {
+        // ---------------- boundary face (the cell is cvofa[f][0]) ----------------
+        const DevZone z = m.zones[m.bzone[f]];
+        const double* bb = &st.bfa[8 * f];
+        FState B;
+        B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
+        double F[5];
+        if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
+          euler_flux(kind, F, B, B, area, nV);
+          if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
+            for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
+          } else {
+            for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+          }
+          if (implicit) {
+            if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
+              // analytical pressure Jacobian, JoeWithModels.cpp:3231-3251
+              double a2 = p.gamma - 1.0;
+              double phi = 0.5 * a2 * (B.u[0] * B.u[0] + B.u[1] * B.u[1] + B.u[2] * B.u[2]);
+              for (int i = 0; i < 3; i++) {
+                sD[(5 * (i + 1) + 0) * bd + t] += phi * nV[i] * area;
+                for (int j = 0; j < 3; j++) sD[(5 * (i + 1) + 1 + j) * bd + t] += -a2 * B.u[j] * nV[i] * area;
+                sD[(5 * (i + 1) + 4) * bd + t] += a2 * nV[i] * area;
+              }
+            } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
+              double Apl[25], Ami[25];
+              euler_matrices(kind, Apl, Ami, B, B, area, nV);
+              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
+            } else {
+              double Apl[25];
+              euler_matrices(kind, Apl, nullptr, B, B, area, nV);
+              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
+            }
+          }
+        } else {
+          FState L = recon(m, p, st, c, f);
+          euler_flux(kind, F, L, B, area, nV);
+          for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+          if (implicit) {
+            FState L0 = cell_fstate(p, st, c);
+            double Apl[25];
+            euler_matrices(kind, Apl, nullptr, L0, B, area, nV);
+            for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
+          }
+        }
+        if (p.viscous && z.kind != JG_BC_SYMMETRY) {
+          VSide v0 = cell_vside(p, st, c);
+          VSide v1;
+          v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
+          v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
+          v1.gu = v0.gu; v1.gh = v0.gh;
+          double sV[3], smag;
+          for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+          if (z.kind == JG_BC_WALL) {
+            smag = fabs(dot3(sV, nV));  // projected on the wall normal; nVec is used as sVec
+            for (int i = 0; i < 3; i++) sV[i] = nV[i];
+          } else {
+            smag = sqrt(dot3(sV, sV));
+            for (int i = 0; i < 3; i++) sV[i] /= smag;
+          }
+          double Fu[3], FE;
+          VFace vf;
+          visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
+          for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
+          rhs[4] -= FE;
+          if (implicit) {
+            double Dv[25];
+            for (int e = 0; e < 25; e++) Dv[e] = 0.0;
+            visc_jac_add(Dv, -1.0, 0, vf, v0, v1.u);
+            for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
+          }
+        }
+      }
+    }
+    // ---------------- epilogue ----------------
+    for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
+    if (implicit) {
+      double Dm[25];
+      for (int e = 0; e < 25; e++) Dm[e] = sD[e * bd + t];
+      if (for_step) {
+        double tmp = m.vol[c] / st.local_dt[c];
+        for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;
+        for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
+      }
+      BT* Dg = (BT*)st.D;
+      for (int e = 0; e < 25; e++) Dg[(size_t)e * m.ncv + c] = (BT)Dm[e];
+      if (for_step) {
+        double Di[25];
+        block_inverse(Dm, Di);
+        BT* Dig = (BT*)st.Dinv;
+        for (int e = 0; e < 25; e++) Dig[(size_t)e * m.ncv + c] = (BT)Di[e];
+      }
+    }
+  }
+  // residual partial sums (|RHS|, runBackwardEuler JoeWithModels.cpp:1125-1136), fixed order
+  if (for_step) {
+    for (int i = 0; i < 5; i++) sres[i][t] = active ? fabs(rhs[i]) : 0.0;
+    __syncthreads();
+    for (int w = bd / 2; w > 0; w >>= 1) {
+      if (t < w)
+        for (int i = 0; i < 5; i++) sres[i][t] += sres[i][t + w];
+      __syncthreads();
+    }
+    if (t == 0)
+      for (int i = 0; i < 5; i++) st.blk[5 * blockIdx.x + i] = sres[i][0];
+  }
+}
+
+// residual history entry: sum of the per-block partials in block order
+__global__ void k_resid_final(State st, int nblk, int hist_from_ctrl) {
+  __shared__ double s[5][256];
+  int t = threadIdx.x;
+  double v[5] = {0, 0, 0, 0, 0};
+  for (int b = t; b < nblk; b += blockDim.x)
+    for (int i = 0; i < 5; i++) v[i] += st.blk[5 * b + i];
+  for (int i = 0; i < 5; i++) s[i][t] = v[i];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (t < w)
+      for (int i = 0; i < 5; i++) s[i][t] += s[i][t + w];
+    __syncthreads();
+  }
+  if (t == 0) {
+    long idx = hist_from_ctrl ? (long)st.ctrl[1] - (long)st.ctrl[4] - 1 : 0;
+    idx = ((idx % st.hist_cap) + st.hist_cap) % st.hist_cap;  // ring buffer
+    for (int i = 0; i < 5; i++) st.resid[5 * idx + i] = s[i][0];
+    if (!(s[4][0] == s[4][0])) atomicOr(st.err, 4);  // NaN energy residual (doneSolver)
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block point relaxation: x_out = Dinv (b - O x_in); x in [5][N]
+// ---------------------------------------------------------------------------
+template <typename BT>
+__global__ void __launch_bounds__(128) k_jacobi(Mesh m, State st, const BT* __restrict__ xin, BT* __restrict__ xout,
+                                                int first) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  const int N = m.ncv;
+  BT acc[5];
+  for (int i = 0; i < 5; i++) acc[i] = (BT)st.b[5 * c + i];
+  if (!first) {
+    const BT* O = (const BT*)st.O;
+    int slice = c / SLICE, lane = c % SLICE;
+    int j0 = m.ell_off[slice], j1 = m.ell_off[slice + 1];
+    for (int j = j0; j < j1; j++) {
+      int nb = m.ell_nb[(size_t)j * SLICE + lane];
+      BT xn[5];
+      for (int k = 0; k < 5; k++) xn[k] = xin[(size_t)k * N + nb];
+      const BT* Ob = O + (size_t)j * 25 * SLICE + lane;
+      for (int i = 0; i < 5; i++) {
+        BT s = 0;
+        for (int k = 0; k < 5; k++) s += Ob[(5 * i + k) * SLICE] * xn[k];
+        acc[i] -= s;
+      }
+    }
+  }
+  const BT* Di = (const BT*)st.Dinv;
+  for (int i = 0; i < 5; i++) {
+    BT s = 0;
+    for (int k = 0; k < 5; k++) s += Di[(size_t)(5 * i + k) * N + c] * acc[k];
+    xout[(size_t)i * N + c] = s;
+  }
+}
+
+template <typename BT>
+__global__ void k_dq_from_x(Mesh m, State st, const BT* x) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  for (int i = 0; i < 5; i++) st.dq[5 * c + i] = (double)x[(size_t)i * m.ncv + c];
+}
+
+// Dinv from D (for linear systems handed in from the host)
+template <typename BT>
+__global__ void k_dinv(Mesh m, State st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  double A[25], Ai[25];
+  const BT* D = (const BT*)st.D;
+  for (int e = 0; e < 25; e++) A[e] = (double)D[(size_t)e * m.ncv + c];
+  block_inverse(A, Ai);
+  BT* Dg = (BT*)st.Dinv;
+  for (int e = 0; e < 25; e++) Dg[(size_t)e * m.ncv + c] = (BT)Ai[e];
+}
+
+// solveCvVectorR5Lusgs, UgpWithCv.cpp:3172-3239 (phi = 0 on entry):
+//   x* = D^-1 b ;  x1 = D^-1 (D x* - U x*)
+__global__ void k_lusgs2(Mesh m, State st, const double* xs, double* x1) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  const int N = m.ncv;
+  const double* D = (const double*)st.D;
+  const double* Di = (const double*)st.Dinv;
+  const double* O = (const double*)st.O;
+  double aux[5];
+  for (int i = 0; i < 5; i++) {
+    double s = 0.0;
+    for (int k = 0; k < 5; k++) s += D[(size_t)(5 * i + k) * N + c] * xs[(size_t)k * N + c];
+    aux[i] = s;
+  }
+  int slice = c / SLICE, lane = c % SLICE;
+  for (int j = m.ell_off[slice]; j < m.ell_off[slice + 1]; j++) {
+    size_t e = (size_t)j * SLICE + lane;
+    if (m.ell_lower[e] != 2) continue;  // 2 = upper neighbour
+    int nb = m.ell_nb[e];
+    const double* Ob = O + (size_t)j * 25 * SLICE + lane;
+    for (int i = 0; i < 5; i++) {
+      double s = 0.0;
+      for (int k = 0; k < 5; k++) s += Ob[(5 * i + k) * SLICE] * xs[(size_t)k * N + nb];
+      aux[i] -= s;
+    }
+  }
+  for (int i = 0; i < 5; i++) {
+    double s = 0.0;
+    for (int k = 0; k < 5; k++) s += Di[(size_t)(5 * i + k) * N + c] * aux[k];
+    x1[(size_t)i * N + c] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB building blocks (solveCvVectorR5Bcgstab, UgpWithCv.cpp:2660-2876), FP64, [5][N]
+// ---------------------------------------------------------------------------
+__global__ void k_spmv(Mesh m, State st, const double* x, double* y) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  const int N = m.ncv;
+  const double* D = (const double*)st.D;
+  const double* O = (const double*)st.O;
+  double acc[5];
+  for (int i = 0; i < 5; i++) {
+    double s = 0.0;
+    for (int k = 0; k < 5; k++) s += D[(size_t)(5 * i + k) * N + c] * x[(size_t)k * N + c];
+    acc[i] = s;
+  }
+  int slice = c / SLICE, lane = c % SLICE;
+  for (int j = m.ell_off[slice]; j < m.ell_off[slice + 1]; j++) {
+    int nb = m.ell_nb[(size_t)j * SLICE + lane];
+    const double* Ob = O + (size_t)j * 25 * SLICE + lane;
+    for (int i = 0; i < 5; i++) {
+      double s = 0.0;
+      for (int k = 0; k < 5; k++) s += Ob[(5 * i + k) * SLICE] * x[(size_t)k * N + nb];
+      acc[i] += s;
+    }
+  }
+  for (int i = 0; i < 5; i++) y[(size_t)i * N + c] = acc[i];
+}
+
+__global__ void k_precond(Mesh m, State st, const double* x, double* y) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  const int N = m.ncv;
+  const double* Di = (const double*)st.Dinv;
+  double xv[5];
+  for (int k = 0; k < 5; k++) xv[k] = x[(size_t)k * N + c];
+  for (int i = 0; i < 5; i++) {
+    double s = 0.0;
+    for (int k = 0; k < 5; k++) s += Di[(size_t)(5 * i + k) * N + c] * xv[k];
+    y[(size_t)i * N + c] = s;
+  }
+}
+
+__global__ void k_dot_partial(int n, const double* a, const double* b, double* partial) {
+  __shared__ double s[256];
+  double v = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v += a[i] * b[i];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+__global__ void k_sum_final(int nblk, const double* partial, double* out, int is_max) {
+  __shared__ double s[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) v = is_max ? fmax(v, partial[i]) : v + partial[i];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] = is_max ? fmax(s[threadIdx.x], s[threadIdx.x + w]) : s[threadIdx.x] + s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+// max over cells of |D^-1 r| (the reference's preconditioned residual norm)
+__global__ void k_resmax_partial(Mesh m, State st, const double* r, double* partial) {
+  __shared__ double s[256];
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (c < m.ncv) {
+    const int N = m.ncv;
+    const double* Di = (const double*)st.Dinv;
+    double rv[5];
+    for (int k = 0; k < 5; k++) rv[k] = r[(size_t)k * N + c];
+    for (int i = 0; i < 5; i++) {
+      double t = 0.0;
+      for (int k = 0; k < 5; k++) t += Di[(size_t)(5 * i + k) * N + c] * rv[k];
+      v = fmax(v, fabs(t));
+    }
+  }
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+// out = a*x + b*y + c*z (z may be null); out may alias x, y or z
+__global__ void k_lin3(long n, double* out, double a, const double* x, double b, const double* y, double c,
+                       const double* z) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = a * x[i] + b * y[i];
+  if (z) v += c * z[i];
+  out[i] = v;
+}
+
+// batched face fluxes (per-face parity entry point)
+__global__ void k_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
+                             double* F, double* AL, double* AR) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  FState sl, sr;
+  sl.rho = L[6 * f]; sl.u[0] = L[6 * f + 1]; sl.u[1] = L[6 * f + 2]; sl.u[2] = L[6 * f + 3]; sl.p = L[6 * f + 4]; sl.gam = L[6 * f + 5];
+  sr.rho = R[6 * f]; sr.u[0] = R[6 * f + 1]; sr.u[1] = R[6 * f + 2]; sr.u[2] = R[6 * f + 3]; sr.p = R[6 * f + 4]; sr.gam = R[6 * f + 5];
+  double nV[3] = {nvec[3 * f], nvec[3 * f + 1], nvec[3 * f + 2]};
+  double Fl[5];
+  euler_flux(kind, Fl, sl, sr, area[f], nV);
+  for (int i = 0; i < 5; i++) F[5 * f + i] = Fl[i];
+  if (AL || AR) {
+    double a[25], b[25];
+    euler_matrices(kind, AL ? a : nullptr, AR ? b : nullptr, sl, sr, area[f], nV);
+    if (AL)
+      for (int e = 0; e < 25; e++) AL[25 * f + e] = a[e];
+    if (AR)
+      for (int e = 0; e < 25; e++) AR[25 * f + e] = b[e];
+  }
+}
+
+// state staging: io = [rho(N) | rhou(N*3) | rhoE(N)] in the reference's layouts
+__global__ void k_pack_state(int n, const double* io, double* q) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  q[5 * c] = io[c];
+  for (int i = 0; i < 3; i++) q[5 * c + 1 + i] = io[n + 3 * c + i];
+  q[5 * c + 4] = io[4 * n + c];
+}
+
+__global__ void k_unpack_state(int n, const double* q, double* io) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  io[c] = q[5 * c];
+  for (int i = 0; i < 3; i++) io[n + 3 * c + i] = q[5 * c + 1 + i];
+  io[4 * n + c] = q[5 * c + 4];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_pack_state(int n, const double* io, double* q, cudaStream_t s) {
+  k_pack_state<<<grid_for(n, 256), 256, 0, s>>>(n, io, q);
+}
+void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s) {
+  k_unpack_state<<<grid_for(n, 256), 256, 0, s>>>(n, q, io);
+}
+constexpr int TB = 128;
+
+void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  k_state<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
+}
+void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  k_update_state<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
+}
+void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  if (!p.viscous || m.nfa == m.nfa_b) return;
+  k_face_props<<<grid_for(m.nfa - m.nfa_b, TB), TB, 0, s>>>(m, p, st);
+}
+void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  if (m.nfa_b == 0) return;
+  k_bc<<<grid_for(m.nfa_b, TB), TB, 0, s>>>(m, p, st);
+}
+void launch_ctrl_step(const Params& p, State& st, cudaStream_t s) { k_ctrl_step<<<1, 1, 0, s>>>(p, st); }
+void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl, double cfl, cudaStream_t s) {
+  int nb = grid_for(m.ncv, 256);
+  k_dt<<<nb, 256, 0, s>>>(m, p, st, use_ctrl, cfl);
+  k_dt_final<<<1, 256, 0, s>>>(m, p, st, nb);
+  if (p.ts_mode == JG_TS_CFL_MIN) k_dt_min_all<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st);
+}
+void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  int do_euler = p.second_order;
+  int do_visc = p.viscous;
+  if (!do_euler && !do_visc) return;
+  // viscous velocity gradient: limited like the Euler one when VISC_LIMITER=YES
+  int visc_lim = p.visc_limiter && p.limiter;
+  int separate = do_visc && do_euler && !p.visc_limiter && p.limiter;
+  k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate);
+}
+void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
+  size_t shm = 25 * TB * sizeof(double);
+  if (p.fp32)
+    k_flux<float><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, implicit, for_step);
+  else
+    k_flux<double><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, implicit, for_step);
+}
+void launch_resid(const Mesh& m, State& st, int hist_from_ctrl, cudaStream_t s) {
+  k_resid_final<<<1, 256, 0, s>>>(st, grid_for(m.ncv, TB), hist_from_ctrl);
+}
+void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {
+  for (int it = 0; it < sweeps; it++) {
+    void* xin = (it % 2 == 0) ? st.x1 : st.x0;
+    void* xout = (it % 2 == 0) ? st.x0 : st.x1;
+    if (p.fp32)
+      k_jacobi<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const float*)xin, (float*)xout, it == 0);
+    else
+      k_jacobi<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
+  }
+}
+void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s) {
+  if (p.fp32)
+    k_dq_from_x<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const float*)x);
+  else
+    k_dq_from_x<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)x);
+}
+void launch_dinv(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  if (p.fp32)
+    k_dinv<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st);
+  else
+    k_dinv<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st);
+}
+void launch_lusgs(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  // x* = Dinv b into x0 (one Jacobi sweep from zero), then the upper correction into x1
+  k_jacobi<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)st.x1, (double*)st.x0, 1);
+  k_lusgs2<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)st.x0, (double*)st.x1);
+}
+void launch_spmv(const Mesh& m, const State& st, const double* x, double* y, cudaStream_t s) {
+  k_spmv<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, x, y);
+}
+void launch_precond(const Mesh& m, const State& st, const double* x, double* y, cudaStream_t s) {
+  k_precond<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, x, y);
+}
+void launch_dot(int n, const double* a, const double* b, double* partial, double* out, cudaStream_t s) {
+  int nb = grid_for(n, 256);
+  if (nb > 1024) nb = 1024;
+  k_dot_partial<<<nb, 256, 0, s>>>(n, a, b, partial);
+  k_sum_final<<<1, 256, 0, s>>>(nb, partial, out, 0);
+}
+void launch_resmax(const Mesh& m, const State& st, const double* r, double* partial, double* out, cudaStream_t s) {
+  int nb = grid_for(m.ncv, 256);
+  k_resmax_partial<<<nb, 256, 0, s>>>(m, st, r, partial);
+  k_sum_final<<<1, 256, 0, s>>>(nb, partial, out, 1);
+}
+void launch_lin3(long n, double* out, double a, const double* x, double b, const double* y, double c, const double* z,
+                 cudaStream_t s) {
+  k_lin3<<<grid_for(n, 256), 256, 0, s>>>(n, out, a, x, b, y, c, z);
+}
+void launch_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
+                       double* F, double* AL, double* AR, cudaStream_t s) {
+  k_flux_faces<<<grid_for(n, 64), 64, 0, s>>>(kind, n, L, R, area, nvec, F, AL, AR);
+}
+
+}  // namespace jg

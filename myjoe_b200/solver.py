@@ -1,0 +1,205 @@
+"""Python host mirror of the reference's operator surface over libjoe_b200.so.
+
+``JoeGpu`` keeps the names of the reference's ``UgpWithCvCompFlow`` /
+``JoeWithModels`` operators (calcStateVariables, calcDt, calcRhs,
+solveCoupledLinSysNS, runBackwardEuler) and forwards each to the C ABI in
+include/joe_b200.h.  The library must be the CUDA build: loading fails loudly
+when it is missing; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import MeshArrays, dptr, jg_mesh, jg_params, make_params
+from .case import JoeParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libjoe_b200.so")
+_lib = None
+
+JG_ERR = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory", -4: "non-physical state",
+          -5: "no CUDA device"}
+
+
+class JoeGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (JG_ERR.get(code, "error"), code, msg))
+        self.code = code
+
+
+def lib():
+    """Load libjoe_b200.so (built by myjoe_b200.build); raise if it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError("libjoe_b200.so is not built (python -m myjoe_b200.build): %s" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        D = C.POINTER(C.c_double)
+        I = C.c_int
+        L.jg_last_error.restype = C.c_char_p
+        L.jg_version.restype = I
+        L.jg_device_count.argtypes = [C.POINTER(I)]
+        L.jg_create.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
+        L.jg_destroy.argtypes = [P]
+        L.jg_get_stream.argtypes = [P, C.POINTER(P)]
+        L.jg_set_state.argtypes = [P, D, D, D]
+        L.jg_get_state.argtypes = [P, D, D, D]
+        L.jg_calc_state.argtypes = [P]
+        L.jg_get_primitives.argtypes = [P, D, D, D, D, D]
+        L.jg_get_bfa.argtypes = [P, D, D, D, D, D, D, D]
+        L.jg_calc_dt.argtypes = [P, C.c_double, D, D]
+        L.jg_calc_rhs.argtypes = [P, D, D, D, D, I]
+        L.jg_get_gradients.argtypes = [P, D, D, D, D]
+        L.jg_solve_lin_sys.argtypes = [P, D, D, D, C.c_double, C.c_double, I, C.POINTER(I)]
+        L.jg_step.argtypes = [P, I, D]
+        L.jg_step_async.argtypes = [P, I]
+        L.jg_get_cfl_step.argtypes = [P, D, C.POINTER(I)]
+        L.jg_euler_flux_faces.argtypes = [I, I, D, D, D, D, D, D, D]
+        L.jg_set_profiling.argtypes = [P, I]
+        L.jg_get_profile.argtypes = [P, D]
+        L.jg_step_kernel_count.argtypes = [P, C.POINTER(I)]
+        _lib = L
+    return _lib
+
+
+def _ck(rc):
+    if rc != 0:
+        raise JoeGpuError(rc, lib().jg_last_error().decode())
+
+
+def _p(a):
+    return None if a is None else dptr(a)
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().jg_device_count(C.byref(n))
+    return n.value
+
+
+class JoeGpu:
+    """One case on the GPU.  ``mesh_src`` is a ``geometry.CvMesh`` or a dict of
+    reference-layout arrays; ``params`` a ``case.JoeParams``."""
+
+    def __init__(self, mesh_src, params: JoeParams, precision: int = 0):
+        self.params = params
+        self.ma = MeshArrays(mesh_src, params)
+        self.jp = make_params(params, precision)
+        self.ncv = self.ma.ncv
+        h = C.c_void_p()
+        _ck(lib().jg_create(C.byref(self.ma.mesh), C.byref(self.jp), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().jg_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _ck(lib().jg_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    # -- state ---------------------------------------------------------------
+    def set_state(self, rho, rhou, rhoE):
+        rho, rhou, rhoE = (np.ascontiguousarray(a, np.float64) for a in (rho, rhou, rhoE))
+        _ck(lib().jg_set_state(self.h, dptr(rho), dptr(rhou), dptr(rhoE)))
+
+    def get_state(self):
+        n = self.ncv
+        rho, rhou, rhoE = np.empty(n), np.empty((n, 3)), np.empty(n)
+        _ck(lib().jg_get_state(self.h, dptr(rho), dptr(rhou), dptr(rhoE)))
+        return rho, rhou, rhoE
+
+    def calcStateVariables(self):
+        """calcStateVariables + calcMaterialProperties + setBC."""
+        _ck(lib().jg_calc_state(self.h))
+
+    def primitives(self):
+        n = self.ncv
+        vel, p, T, h, c = np.empty((n, 3)), np.empty(n), np.empty(n), np.empty(n), np.empty(n)
+        _ck(lib().jg_get_primitives(self.h, dptr(vel), dptr(p), dptr(T), dptr(h), dptr(c)))
+        return {"vel": vel, "press": p, "temp": T, "enthalpy": h, "sos": c}
+
+    def boundary(self):
+        nb, nf = self.ma.nfa_b, self.ma.nfa
+        out = {"rho_bfa": np.empty(nb), "vel_bfa": np.empty((nb, 3)), "p_bfa": np.empty(nb), "T_bfa": np.empty(nb),
+               "h_bfa": np.empty(nb), "mul_fa": np.empty(nf), "lamOcp_fa": np.empty(nf)}
+        _ck(lib().jg_get_bfa(self.h, *(dptr(out[k]) for k in ("rho_bfa", "vel_bfa", "p_bfa", "T_bfa", "h_bfa",
+                                                              "mul_fa", "lamOcp_fa"))))
+        return out
+
+    # -- operators -----------------------------------------------------------
+    def calcDt(self, cfl=None):
+        dtmin = C.c_double(0.0)
+        local = np.empty(self.ncv)
+        _ck(lib().jg_calc_dt(self.h, self.params.CFL if cfl is None else cfl, C.byref(dtmin), dptr(local)))
+        return dtmin.value, local
+
+    def calcRhs(self, flagImplicit=True):
+        n = self.ncv
+        rr, ru, rE = np.empty(n), np.empty((n, 3)), np.empty(n)
+        A = np.empty((self.ma.nbocv_s, 5, 5)) if flagImplicit else None
+        _ck(lib().jg_calc_rhs(self.h, dptr(rr), dptr(ru), dptr(rE), _p(A), int(flagImplicit)))
+        return rr, ru, rE, A
+
+    def gradients(self):
+        n = self.ncv
+        gu, gr, gp, gh = np.empty((n, 3, 3)), np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        _ck(lib().jg_get_gradients(self.h, dptr(gu), dptr(gr), dptr(gp), dptr(gh)))
+        return {"grad_u": gu, "grad_rho": gr, "grad_p": gp, "grad_enthalpy": gh}
+
+    def solveCoupledLinSysNS(self, A, rhs, zeroAbs, zeroRel, maxIter, dq0=None):
+        dq = np.zeros((self.ncv, 5)) if dq0 is None else np.array(dq0, np.float64, order="C")
+        A = np.ascontiguousarray(A, np.float64)
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        it = C.c_int(0)
+        _ck(lib().jg_solve_lin_sys(self.h, dptr(dq), dptr(A), dptr(rhs), zeroAbs, zeroRel, int(maxIter),
+                                   C.byref(it)))
+        return dq, it.value
+
+    def runBackwardEuler(self, nsteps):
+        """``nsteps`` iterations of the backward-Euler loop; returns the L1
+        residual history [nsteps][5]."""
+        r = np.zeros((max(nsteps, 1), 5))
+        _ck(lib().jg_step(self.h, int(nsteps), dptr(r)))
+        return r[:nsteps]
+
+    def step_async(self, nsteps):
+        _ck(lib().jg_step_async(self.h, int(nsteps)))
+
+    def set_profiling(self, on=True):
+        _ck(lib().jg_set_profiling(self.h, int(on)))
+
+    def profile(self):
+        ms = np.zeros(2)
+        _ck(lib().jg_get_profile(self.h, dptr(ms)))
+        return {"face_loop_ms": float(ms[0]), "linear_solve_ms": float(ms[1])}
+
+    def step_kernel_count(self):
+        n = C.c_int(0)
+        _ck(lib().jg_step_kernel_count(self.h, C.byref(n)))
+        return n.value
+
+    def cfl_step(self):
+        cfl = C.c_double(0.0)
+        step = C.c_int(0)
+        _ck(lib().jg_get_cfl_step(self.h, C.byref(cfl), C.byref(step)))
+        return cfl.value, step.value
+
+
+def euler_flux_faces(kind, L, R, area, nvec, matrices=True):
+    n = L.shape[0]
+    L, R, area, nvec = (np.ascontiguousarray(a, np.float64) for a in (L, R, area, nvec))
+    F = np.zeros((n, 5))
+    AL = np.zeros((n, 5, 5)) if matrices else None
+    AR = np.zeros((n, 5, 5)) if matrices else None
+    _ck(lib().jg_euler_flux_faces(kind, n, dptr(L), dptr(R), dptr(area), dptr(nvec), dptr(F), _p(AL), _p(AR)))
+    return F, AL, AR

@@ -26,6 +26,7 @@ struct jo_case {
   double *mul_fa, *lamOcp_fa, *mut_fa;
   double *grad_u, *grad_rho, *grad_p, *grad_h, *alpha_rho;
   double *local_dt;
+  double *fscale;   /* [N][5] sum over the cell's faces of |F| (rounding scale of the residual) */
   double cfl;
   int step;
   int dt_fixed_done;
@@ -62,6 +63,7 @@ jo_case *jo_create(const jg_mesh *m, const jg_params *p) {
   h->mul_fa = dalloc(nf); h->lamOcp_fa = dalloc(nf); h->mut_fa = dalloc(nf);
   h->grad_u = dalloc(9 * n); h->grad_rho = dalloc(3 * n); h->grad_p = dalloc(3 * n);
   h->grad_h = dalloc(3 * n); h->alpha_rho = dalloc(n); h->local_dt = dalloc(n);
+  h->fscale = dalloc(5 * n);
   /* initialHookScalarRansCombModel: RoM = R_gas, gamma = GAMMA (UgpWithCvCompFlow.h:1630-1640) */
   for (int i = 0; i < n; i++) { h->gam[i] = p->gamma; h->RoM[i] = p->R_gas; }
   h->cfl = p->cfl;
@@ -73,7 +75,7 @@ void jo_destroy(jo_case *h) {
   double *arrs[] = {h->rho, h->rhou, h->rhoE, h->vel, h->press, h->temp, h->enthalpy, h->sos, h->gam, h->RoM,
                     h->rho_bfa, h->T_bfa, h->vel_bfa, h->p_bfa, h->h_bfa, h->gam_bfa, h->RoM_bfa, h->mul_fa,
                     h->lamOcp_fa, h->mut_fa, h->grad_u, h->grad_rho, h->grad_p, h->grad_h, h->alpha_rho,
-                    h->local_dt};
+                    h->local_dt, h->fscale};
   for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); i++) free(arrs[i]);
   free(h);
 }
@@ -97,7 +99,7 @@ double *jo_array(jo_case *h, const char *name) {
       {"h_bfa", h->h_bfa}, {"gam_bfa", h->gam_bfa}, {"RoM_bfa", h->RoM_bfa}, {"mul_fa", h->mul_fa},
       {"lamOcp_fa", h->lamOcp_fa}, {"mut_fa", h->mut_fa}, {"grad_u", h->grad_u}, {"grad_rho", h->grad_rho},
       {"grad_p", h->grad_p}, {"grad_enthalpy", h->grad_h}, {"alpha_rho", h->alpha_rho},
-      {"local_dt", h->local_dt}, {"rho", h->rho}, {"rhou", h->rhou}, {"rhoE", h->rhoE}};
+      {"local_dt", h->local_dt}, {"flux_scale", h->fscale}, {"rho", h->rho}, {"rhou", h->rhou}, {"rhoE", h->rhoE}};
   for (size_t i = 0; i < sizeof(t) / sizeof(t[0]); i++)
     if (strcmp(t[i].n, name) == 0) return t[i].p;
   return NULL;
@@ -1023,6 +1025,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
     euler_flux(kind, F, &L, &R, area, nV);
     rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
     rr[c1] += F[0]; for (int i = 0; i < 3; i++) ru[3 * c1 + i] += F[1 + i]; rE[c1] += F[4];
+    for (int i = 0; i < 5; i++) { h->fscale[5 * c0 + i] += fabs(F[i]); h->fscale[5 * c1 + i] += fabs(F[i]); }
     if (implicit) {
       fstate L0 = cell_state(h, c0), R0 = cell_state(h, c1);
       euler_matrices(kind, Apl, Ami, &L0, &R0, area, nV);
@@ -1043,6 +1046,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
       if (zn->kind == JG_BC_SYMMETRY) {
         fstate B = bfa_state(h, f);
         euler_flux(kind, F, &B, &B, area, nV);
+        for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (p->symm_bc == JG_SYMM_ANALYTICAL) {
           for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= h->p_bfa[f] * nV[i] * area;
         } else {
@@ -1076,6 +1080,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
         fstate B = bfa_state(h, f);
         euler_flux(kind, F, &B, &B, area, nV);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+        for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {
           euler_matrices(kind, Apl, NULL, &B, &B, area, nV);
           add_block(A, n00, Apl, 1.0);
@@ -1086,6 +1091,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
         fstate B = bfa_state(h, f);
         euler_flux(kind, F, &L, &B, area, nV);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
+        for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {
           fstate L0 = cell_state(h, c0);
           euler_matrices(kind, Apl, NULL, &L0, &B, area, nV);
@@ -1206,6 +1212,8 @@ static void calc_viscous_flux(jo_case *h, double *ru, double *rE, double *A, int
     rE[c0] -= FE;
     for (int i = 0; i < 3; i++) ru[3 * c1 + i] += Fu[i];
     rE[c1] += FE;
+    for (int i = 0; i < 3; i++) { h->fscale[5 * c0 + 1 + i] += fabs(Fu[i]); h->fscale[5 * c1 + 1 + i] += fabs(Fu[i]); }
+    h->fscale[5 * c0 + 4] += fabs(FE); h->fscale[5 * c1 + 4] += fabs(FE);
   }
   for (int z = 0; z < m->nzones; z++) {
     const jg_zone *zn = &m->zones[z];
@@ -1240,6 +1248,8 @@ static void calc_viscous_flux(jo_case *h, double *ru, double *rE, double *A, int
       }
       for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= Fu[i];
       rE[c0] -= FE;
+      for (int i = 0; i < 3; i++) h->fscale[5 * c0 + 1 + i] += fabs(Fu[i]);
+      h->fscale[5 * c0 + 4] += fabs(FE);
     }
   }
 }
@@ -1249,6 +1259,7 @@ void jo_calc_rhs(jo_case *h, double *rr, double *ru, double *rE, double *A, int 
   memset(rr, 0, sizeof(double) * h->ncv);
   memset(ru, 0, sizeof(double) * 3 * h->ncv);
   memset(rE, 0, sizeof(double) * h->ncv);
+  memset(h->fscale, 0, sizeof(double) * 5 * h->ncv);
   calc_euler_flux(h, rr, ru, rE, A, implicit);
   if (h->p.mu_ref > 0.0) calc_viscous_flux(h, ru, rE, A, implicit);
 }

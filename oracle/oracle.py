@@ -51,7 +51,7 @@ def lib():
     return _lib
 
 
-_SIZES = {"vel": 3, "grad_u": 9, "grad_rho": 3, "grad_p": 3, "grad_enthalpy": 3, "vel_bfa": 3, "rhou": 3}
+_SIZES = {"flux_scale": 5, "vel": 3, "grad_u": 9, "grad_rho": 3, "grad_p": 3, "grad_enthalpy": 3, "vel_bfa": 3, "rhou": 3}
 _BFA = {"rho_bfa", "T_bfa", "vel_bfa", "p_bfa", "h_bfa", "gam_bfa", "RoM_bfa"}
 _FA = {"mul_fa", "lamOcp_fa", "mut_fa"}
 

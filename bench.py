@@ -75,7 +75,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -149,7 +149,8 @@ def run_reference_arm(args):
         return
     raw, g, prm = plate_case()
     nproc = os.cpu_count() or 1
-    nsteps = max(1, args.steps)
+    # bounded sample: the reference takes ~0.3-0.5 s per iteration of this case on one core
+    nsteps = max(1, min(args.steps, 20))
     r = reference_run(raw, prm, nsteps, nproc)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref/ref_harness not built"}))
@@ -170,8 +171,8 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -136,7 +136,9 @@ int jg_calc_dt(jg_case_t *h, double cfl, double *dt_min, double *local_dt);
  * block Jacobian A[nbocv_s][5][5] in the reference's CSR layout. */
 int jg_calc_rhs(jg_case_t *h, double *rhs_rho, double *rhs_rhou, double *rhs_rhoE, double *A, int flagImplicit);
 /* gradients of the last jg_calc_rhs / step: calcCvVectorGrad / calcCvScalarGrad
- * with limiting (src/common/UgpWithCv.h:803-1083); grad_u[ncv][3][3], others [ncv][3] */
+ * with limiting (src/common/UgpWithCv.h:803-1083); grad_u[ncv][3][3], others [ncv][3].
+ * grad_u is what the reference holds after calcRhs: the viscous gradient when
+ * MU_REF > 0 (unlimited under VISC_LIMITER=NO), else the Euler one. */
 int jg_get_gradients(jg_case_t *h, double *grad_u, double *grad_rho, double *grad_p, double *grad_h);
 
 /* UgpWithCvCompFlow::solveCoupledLinSysNS (src/joe/UgpWithCvCompFlow.h:899-950):

@@ -311,7 +311,8 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(dmalloc_bytes(h, &st.x0, 5 * (size_t)N * h->eltsz));
   RC(dmalloc_bytes(h, &st.x1, 5 * (size_t)N * h->eltsz));
   RC(dmalloc(h, &st.dq, 5 * (size_t)N));
-  RC(dmalloc(h, &st.blk, 5 * (size_t)grid_for(N, 128) + 5 * (size_t)grid_for(N, 256) + 16));
+  // per-block partials: k_flux2 writes 5 per 16-cell block, k_dt 1 per 256-cell block
+  RC(dmalloc(h, &st.blk, 5 * (size_t)grid_for(N, 16) + 5 * (size_t)grid_for(N, 256) + 16));
   RC(dmalloc(h, &st.ctrl, 16));
   RC(dmalloc(h, &st.err, 4));
   h->hist_cap = 64;
@@ -537,7 +538,9 @@ int jg_calc_rhs(jg_case_t* h, double* rhs_rho, double* rhs_rhou, double* rhs_rho
 int jg_get_gradients(jg_case_t* h, double* grad_u, double* grad_rho, double* grad_p, double* grad_h) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
   const int N = h->ncv;
-  if (grad_u) CK(cudaMemcpyAsync(grad_u, h->st.gu, 9 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  // the reference's grad_u after calcRhs: the viscous pass overwrites it (unlimited when VISC_LIMITER=NO)
+  const double* gu = h->p.viscous ? h->st.guv : h->st.gu;
+  if (grad_u) CK(cudaMemcpyAsync(grad_u, gu, 9 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (grad_rho) CK(cudaMemcpyAsync(grad_rho, h->st.grho, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (grad_p) CK(cudaMemcpyAsync(grad_p, h->st.gp, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (grad_h) CK(cudaMemcpyAsync(grad_h, h->st.gh, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

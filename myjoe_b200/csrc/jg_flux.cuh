@@ -275,7 +275,32 @@ __device__ inline void flux_roe(double F[5], const FState& L, const FState& R, d
 }
 
 // calcEulerFluxMatrices_Roe with calcPMatrix / calcInvPMatrix,
-// UgpWithCvCompFlow.cpp:3382-3559; AL/AR may be null
+// UgpWithCvCompFlow.cpp:3382-3559; AL/AR may be null.  The dissipation matrix
+// P |Lambda| P^-1 is formed row by row (P row i generated on the fly) to keep
+// the live register set small; each entry is the same k-ordered sum.
+__device__ __forceinline__ void roe_p_row(double Pr[5], int i, const double* v, double rr, double rhooc, double rhoxc,
+                                          double km1, double vS, double vn, const double* nV) {
+  switch (i) {
+    case 0: Pr[0] = nV[0]; Pr[1] = nV[1]; Pr[2] = nV[2]; Pr[3] = 0.5 * rhooc; Pr[4] = 0.5 * rhooc; break;
+    case 1:
+      Pr[0] = v[0] * nV[0]; Pr[1] = v[0] * nV[1] - rr * nV[2]; Pr[2] = v[0] * nV[2] + rr * nV[1];
+      Pr[3] = 0.5 * (v[0] * rhooc + rr * nV[0]); Pr[4] = 0.5 * (v[0] * rhooc - rr * nV[0]); break;
+    case 2:
+      Pr[0] = v[1] * nV[0] + rr * nV[2]; Pr[1] = v[1] * nV[1]; Pr[2] = v[1] * nV[2] - rr * nV[0];
+      Pr[3] = 0.5 * (v[1] * rhooc + rr * nV[1]); Pr[4] = 0.5 * (v[1] * rhooc - rr * nV[1]); break;
+    case 3:
+      Pr[0] = v[2] * nV[0] - rr * nV[1]; Pr[1] = v[2] * nV[1] + rr * nV[0]; Pr[2] = v[2] * nV[2];
+      Pr[3] = 0.5 * (v[2] * rhooc + rr * nV[2]); Pr[4] = 0.5 * (v[2] * rhooc - rr * nV[2]); break;
+    default:
+      Pr[0] = 0.5 * vS * nV[0] + rr * v[1] * nV[2] - rr * v[2] * nV[1];
+      Pr[1] = 0.5 * vS * nV[1] - rr * v[0] * nV[2] + rr * v[2] * nV[0];
+      Pr[2] = 0.5 * vS * nV[2] + rr * v[0] * nV[1] - rr * v[1] * nV[0];
+      Pr[3] = 0.5 * (0.5 * vS * rhooc + rr * vn + rhoxc / km1);
+      Pr[4] = 0.5 * (0.5 * vS * rhooc - rr * vn + rhoxc / km1);
+      break;
+  }
+}
+
 __device__ inline void matrices_roe(double* AL, double* AR, const FState& L, const FState& R, double area,
                                     const double nV[3]) {
   double uLuL = dot3(L.u, L.u), uRuR = dot3(R.u, R.u);
@@ -288,59 +313,57 @@ __device__ inline void matrices_roe(double* AL, double* AR, const FState& L, con
                       (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
   double c = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(v, v));
   double gamma = 0.5 * (L.gam + R.gam);
-  double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
-  if (AL) jacobian_A(AL, L.u, L.p, L.rho, nA, gamma);
-  if (AR) jacobian_A(AR, R.u, R.p, R.rho, nA, gamma);
   double km1 = gamma - 1.0;
   double rhooc = rr / c, rhoxc = rr * c, c2 = c * c;
   double vS = dot3(v, v);
   double vn = v[0] * nV[0] + v[1] * nV[1] + v[2] * nV[2];
-  double P[25], Q[25];
-  P[0] = nV[0]; P[1] = nV[1]; P[2] = nV[2]; P[3] = 0.5 * rhooc; P[4] = 0.5 * rhooc;
-  P[5] = v[0] * nV[0]; P[6] = v[0] * nV[1] - rr * nV[2]; P[7] = v[0] * nV[2] + rr * nV[1];
-  P[8] = 0.5 * (v[0] * rhooc + rr * nV[0]); P[9] = 0.5 * (v[0] * rhooc - rr * nV[0]);
-  P[10] = v[1] * nV[0] + rr * nV[2]; P[11] = v[1] * nV[1]; P[12] = v[1] * nV[2] - rr * nV[0];
-  P[13] = 0.5 * (v[1] * rhooc + rr * nV[1]); P[14] = 0.5 * (v[1] * rhooc - rr * nV[1]);
-  P[15] = v[2] * nV[0] - rr * nV[1]; P[16] = v[2] * nV[1] + rr * nV[0]; P[17] = v[2] * nV[2];
-  P[18] = 0.5 * (v[2] * rhooc + rr * nV[2]); P[19] = 0.5 * (v[2] * rhooc - rr * nV[2]);
-  P[20] = 0.5 * vS * nV[0] + rr * v[1] * nV[2] - rr * v[2] * nV[1];
-  P[21] = 0.5 * vS * nV[1] - rr * v[0] * nV[2] + rr * v[2] * nV[0];
-  P[22] = 0.5 * vS * nV[2] + rr * v[0] * nV[1] - rr * v[1] * nV[0];
-  P[23] = 0.5 * (0.5 * vS * rhooc + rr * vn + rhoxc / km1);
-  P[24] = 0.5 * (0.5 * vS * rhooc - rr * vn + rhoxc / km1);
-  Q[0] = nV[0] - nV[2] * v[1] / rr + nV[1] * v[2] / rr - nV[0] * 0.5 * km1 * vS / c2;
-  Q[1] = nV[0] * km1 * v[0] / c2;
-  Q[2] = nV[2] / rr + nV[0] * km1 * v[1] / c2;
-  Q[3] = -nV[1] / rr + nV[0] * km1 * v[2] / c2;
-  Q[4] = -nV[0] * km1 / c2;
-  Q[5] = nV[1] + nV[2] * v[0] / rr - nV[0] * v[2] / rr - nV[1] * 0.5 * km1 * vS / c2;
-  Q[6] = -nV[2] / rr + nV[1] * km1 * v[0] / c2;
-  Q[7] = nV[1] * km1 * v[1] / c2;
-  Q[8] = nV[0] / rr + nV[1] * km1 * v[2] / c2;
-  Q[9] = -nV[1] * km1 / c2;
-  Q[10] = nV[2] - nV[1] * v[0] / rr + nV[0] * v[1] / rr - nV[2] * 0.5 * km1 * vS / c2;
-  Q[11] = nV[1] / rr + nV[2] * km1 * v[0] / c2;
-  Q[12] = -nV[0] / rr + nV[2] * km1 * v[1] / c2;
-  Q[13] = nV[2] * km1 * v[2] / c2;
-  Q[14] = -nV[2] * km1 / c2;
-  Q[15] = -vn / rr + 0.5 * km1 * vS / rhoxc;
-  Q[16] = nV[0] / rr - km1 * v[0] / rhoxc;
-  Q[17] = nV[1] / rr - km1 * v[1] / rhoxc;
-  Q[18] = nV[2] / rr - km1 * v[2] / rhoxc;
-  Q[19] = km1 / rhoxc;
-  Q[20] = vn / rr + 0.5 * km1 * vS / rhoxc;
-  Q[21] = -nV[0] / rr - km1 * v[0] / rhoxc;
-  Q[22] = -nV[1] / rr - km1 * v[1] / rhoxc;
-  Q[23] = -nV[2] / rr - km1 * v[2] / rhoxc;
-  Q[24] = km1 / rhoxc;
+  // P^-1 (calcInvPMatrix): the reference divides by rho, c^2 and rho*c entry by
+  // entry; one reciprocal of each replaces ~30 FP64 divides (<= 1 ulp per term)
+  const double ir = 1.0 / rr, ic2 = 1.0 / c2, irc = 1.0 / rhoxc;
+  const double kc = km1 * ic2, kr = km1 * irc;
+  double Q[25];
+  Q[0] = nV[0] - nV[2] * v[1] * ir + nV[1] * v[2] * ir - nV[0] * 0.5 * vS * kc;
+  Q[1] = nV[0] * v[0] * kc;
+  Q[2] = nV[2] * ir + nV[0] * v[1] * kc;
+  Q[3] = -nV[1] * ir + nV[0] * v[2] * kc;
+  Q[4] = -nV[0] * kc;
+  Q[5] = nV[1] + nV[2] * v[0] * ir - nV[0] * v[2] * ir - nV[1] * 0.5 * vS * kc;
+  Q[6] = -nV[2] * ir + nV[1] * v[0] * kc;
+  Q[7] = nV[1] * v[1] * kc;
+  Q[8] = nV[0] * ir + nV[1] * v[2] * kc;
+  Q[9] = -nV[1] * kc;
+  Q[10] = nV[2] - nV[1] * v[0] * ir + nV[0] * v[1] * ir - nV[2] * 0.5 * vS * kc;
+  Q[11] = nV[1] * ir + nV[2] * v[0] * kc;
+  Q[12] = -nV[0] * ir + nV[2] * v[1] * kc;
+  Q[13] = nV[2] * v[2] * kc;
+  Q[14] = -nV[2] * kc;
+  Q[15] = -vn * ir + 0.5 * vS * kr;
+  Q[16] = nV[0] * ir - v[0] * kr;
+  Q[17] = nV[1] * ir - v[1] * kr;
+  Q[18] = nV[2] * ir - v[2] * kr;
+  Q[19] = kr;
+  Q[20] = vn * ir + 0.5 * vS * kr;
+  Q[21] = -nV[0] * ir - v[0] * kr;
+  Q[22] = -nV[1] * ir - v[1] * kr;
+  Q[23] = -nV[2] * ir - v[2] * kr;
+  Q[24] = kr;
   double lam[5] = {fabs(uRoe), fabs(uRoe), fabs(uRoe), fabs(uRoe + c), fabs(uRoe - c)};
-  for (int i = 0; i < 5; i++)
+  double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+  if (AL) jacobian_A(AL, L.u, L.p, L.rho, nA, gamma);
+  if (AR) jacobian_A(AR, R.u, R.p, R.rho, nA, gamma);
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    double Pr[5];
+    roe_p_row(Pr, i, v, rr, rhooc, rhoxc, km1, vS, vn, nV);
+#pragma unroll
     for (int j = 0; j < 5; j++) {
       double pm = 0.0;
-      for (int k = 0; k < 5; k++) pm += P[5 * i + k] * lam[k] * Q[5 * k + j];
+#pragma unroll
+      for (int k = 0; k < 5; k++) pm += Pr[k] * lam[k] * Q[5 * k + j];
       if (AL) AL[5 * i + j] = 0.5 * AL[5 * i + j] + 0.5 * pm * area;
       if (AR) AR[5 * i + j] = 0.5 * AR[5 * i + j] - 0.5 * pm * area;
     }
+  }
 }
 
 // calcEulerFlux_AUSM, UgpWithCvCompFlow.cpp:3566-3641
@@ -364,6 +387,21 @@ __device__ inline void flux_ausm(double F[5], const FState& L, const FState& R, 
     F[1 + i] = 0.5 * (mF * ((L.rho * cL * L.u[i]) + (R.rho * cR * R.u[i])) - Phi * ((R.rho * cR * R.u[i]) - (L.rho * cL * L.u[i]))) + nV[i] * pF;
   F[4] = 0.5 * (mF * ((L.rho * cL * hL) + (R.rho * cR * hR)) - Phi * ((R.rho * cR * hR) - (L.rho * cL * hL)));
   for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+template <int KIND>
+__device__ __forceinline__ void euler_flux_t(double F[5], const FState& L, const FState& R, double area,
+                                             const double nV[3]) {
+  if (KIND == 1) flux_roe(F, L, R, area, nV);
+  else if (KIND == 2) flux_ausm(F, L, R, area, nV);
+  else flux_hllc(F, L, R, area, nV);
+}
+
+template <int KIND>
+__device__ __forceinline__ void euler_matrices_t(double* AL, double* AR, const FState& L, const FState& R, double area,
+                                                 const double nV[3]) {
+  if (KIND == 1) matrices_roe(AL, AR, L, R, area, nV);
+  else matrices_hllc(AL, AR, L, R, area, nV);
 }
 
 __device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& L, const FState& R, double area,

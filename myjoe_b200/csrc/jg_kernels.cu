@@ -464,7 +464,7 @@ __device__ inline void block_inverse(double* A, double* Ai) {
   }
 }
 
-template <typename BT>
+template <typename BT, int KIND, int VISC>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   extern __shared__ double sD[];  // [25][blockDim.x] diagonal-block accumulators
   __shared__ double sres[5][128];
@@ -475,7 +475,6 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
   if (active) {
     for (int e = 0; e < 25; e++) sD[e * bd + t] = 0.0;
     BT* O = (BT*)st.O;
-    const int kind = p.flux;
     for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
       const Slot s = m.slots[k];
       const int f = s.f;
@@ -489,14 +488,14 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         {
           FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
           double F[5];
-          euler_flux(kind, F, L, R, area, nV);
+          euler_flux_t<KIND>(F, L, R, area, nV);
           for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
         }
         double Ob[25];
         if (implicit) {
           FState L0 = cell_fstate(p, st, c0), R0 = cell_fstate(p, st, c1);
           double Apl[25], Ami[25];
-          euler_matrices(kind, Apl, Ami, L0, R0, area, nV);
+          euler_matrices_t<KIND>(Apl, Ami, L0, R0, area, nV);
           // row of c0: D += Apl, O(c0,c1) = Ami ; row of c1: D -= Ami, O(c1,c0) = -Apl
           if (s.side == 0) {
             for (int e = 0; e < 25; e++) { sD[e * bd + t] += Apl[e]; Ob[e] = Ami[e]; }
@@ -504,7 +503,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
             for (int e = 0; e < 25; e++) { sD[e * bd + t] -= Ami[e]; Ob[e] = -Apl[e]; }
           }
         }
-        if (p.viscous) {
+        if (VISC) {
           VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
           double sV[3];
           for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
@@ -540,7 +539,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
         double F[5];
         if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-          euler_flux(kind, F, B, B, area, nV);
+          euler_flux_t<KIND>(F, B, B, area, nV);
           if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
             for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
           } else {
@@ -558,26 +557,26 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
               }
             } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
               double Apl[25], Ami[25];
-              euler_matrices(kind, Apl, Ami, B, B, area, nV);
+              euler_matrices_t<KIND>(Apl, Ami, B, B, area, nV);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
             } else {
               double Apl[25];
-              euler_matrices(kind, Apl, nullptr, B, B, area, nV);
+              euler_matrices_t<KIND>(Apl, nullptr, B, B, area, nV);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
             }
           }
         } else {
           FState L = recon(m, p, st, c, f);
-          euler_flux(kind, F, L, B, area, nV);
+          euler_flux_t<KIND>(F, L, B, area, nV);
           for (int i = 0; i < 5; i++) rhs[i] -= F[i];
           if (implicit) {
             FState L0 = cell_fstate(p, st, c);
             double Apl[25];
-            euler_matrices(kind, Apl, nullptr, L0, B, area, nV);
+            euler_matrices_t<KIND>(Apl, nullptr, L0, B, area, nV);
             for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
           }
         }
-        if (p.viscous && z.kind != JG_BC_SYMMETRY) {
+        if (VISC && z.kind != JG_BC_SYMMETRY) {
           VSide v0 = cell_vside(p, st, c);
           VSide v1;
           v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
@@ -637,6 +636,150 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
     }
     if (t == 0)
       for (int i = 0; i < 5; i++) st.blk[5 * blockIdx.x + i] = sres[i][0];
+  }
+}
+
+// 8 lanes per cell: lane l of a cell evaluates the cell's faces l, l+8, ...;
+// the contributions are summed over the lanes with an XOR butterfly (every
+// lane ends with the same order-fixed sum: deterministic).
+constexpr int FL = 8;  // lanes per cell
+
+__device__ __forceinline__ double lane_sum(double v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  return v;
+}
+
+// Residual-only face loop (calcRhs with flagImplicit = 0), 8 lanes per cell.
+// Without the Jacobian blocks the live set is small (~120 registers), so the
+// lanes-per-cell split pays: many warps per SM.
+template <int KIND, int VISC>
+__global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int for_step) {
+  __shared__ double sres[5][128 / FL];
+  const int t = threadIdx.x, lane = t % FL, cl = t / FL;
+  const int c = blockIdx.x * (128 / FL) + cl;
+  const bool active = c < m.ncv;
+  double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const int k0 = active ? m.slot_i[c] : 0, k1 = active ? m.slot_i[c + 1] : 0;
+  for (int k = k0 + lane; k < k1; k += FL) {
+    const Slot s = m.slots[k];
+    const int f = s.f;
+    double nV[3], area;
+    unit_normal(m, f, nV, area);
+    if (s.nb >= 0) {
+      const int c0 = s.side == 0 ? c : s.nb;
+      const int c1 = s.side == 0 ? s.nb : c;
+      const double sg = s.side == 0 ? -1.0 : 1.0;
+      {
+        FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
+        double F[5];
+        euler_flux_t<KIND>(F, L, R, area, nV);
+        for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
+      }
+      if (VISC) {
+        VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
+        double sV[3];
+        for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
+        double smag = sqrt(dot3(sV, sV));
+        for (int i = 0; i < 3; i++) sV[i] /= smag;
+        double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
+        double Fu[3], FE;
+        VFace vf;
+        visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, ufa, area, nV, smag, sV);
+        for (int i = 0; i < 3; i++) rhs[1 + i] += sg * Fu[i];
+        rhs[4] += sg * FE;
+      }
+    } else {
+      const DevZone z = m.zones[m.bzone[f]];
+      const double* bb = &st.bfa[8 * f];
+      FState B;
+      B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
+      double F[5];
+      if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
+        euler_flux_t<KIND>(F, B, B, area, nV);
+        if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
+          for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
+        } else {
+          for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+        }
+      } else {
+        FState L = recon(m, p, st, c, f);
+        euler_flux_t<KIND>(F, L, B, area, nV);
+        for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+      }
+      if (VISC && z.kind != JG_BC_SYMMETRY) {
+        VSide v0 = cell_vside(p, st, c);
+        VSide v1;
+        v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
+        v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
+        v1.gu = v0.gu; v1.gh = v0.gh;
+        double sV[3], smag;
+        for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+        if (z.kind == JG_BC_WALL) {
+          smag = fabs(dot3(sV, nV));
+          for (int i = 0; i < 3; i++) sV[i] = nV[i];
+        } else {
+          smag = sqrt(dot3(sV, sV));
+          for (int i = 0; i < 3; i++) sV[i] /= smag;
+        }
+        double Fu[3], FE;
+        VFace vf;
+        visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
+        for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
+        rhs[4] -= FE;
+      }
+    }
+  }
+  for (int i = 0; i < 5; i++) rhs[i] = lane_sum(rhs[i]);
+  if (active && lane == 0) {
+    for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
+    if (for_step)
+      for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
+  }
+  if (for_step) {
+    if (lane == 0)
+      for (int i = 0; i < 5; i++) sres[i][cl] = active ? fabs(rhs[i]) : 0.0;
+    __syncthreads();
+    if (t < 5) {
+      double v = 0.0;
+      for (int q = 0; q < 128 / FL; q++) v += sres[t][q];
+      st.blk[5 * blockIdx.x + t] = v;
+    }
+  }
+}
+
+// Block point relaxation, one warp per block row: a 160-thread block handles
+// one 32-cell slice; warp i computes row i of (b - O x) for the 32 cells
+// (coalesced ELL reads), the 5 rows meet in shared memory for the Dinv product.
+template <typename BT>
+__global__ void __launch_bounds__(160) k_jacobi2(Mesh m, State st, const BT* __restrict__ xin,
+                                                 BT* __restrict__ xout, int first) {
+  __shared__ BT sacc[5][SLICE];
+  const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
+  const int slice = blockIdx.x;
+  const int c = slice * SLICE + lane;
+  const bool active = c < m.ncv;
+  const int N = m.ncv;
+  BT acc = active ? (BT)st.b[5 * c + row] : (BT)0;
+  if (!first && active) {
+    const BT* O = (const BT*)st.O;
+    int j0 = m.ell_off[slice], j1 = m.ell_off[slice + 1];
+    for (int j = j0; j < j1; j++) {
+      int nb = m.ell_nb[(size_t)j * SLICE + lane];
+      const BT* Ob = O + ((size_t)j * 25 + 5 * row) * SLICE + lane;
+      BT s = 0;
+      for (int k = 0; k < 5; k++) s += Ob[k * SLICE] * xin[(size_t)k * N + nb];
+      acc -= s;
+    }
+  }
+  sacc[row][lane] = acc;
+  __syncthreads();
+  if (active) {
+    const BT* Di = (const BT*)st.Dinv;
+    BT s = 0;
+    for (int k = 0; k < 5; k++) s += Di[(size_t)(5 * row + k) * N + c] * sacc[k][lane];
+    xout[(size_t)row * N + c] = s;
   }
 }
 
@@ -934,24 +1077,57 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   int separate = do_visc && do_euler && !p.visc_limiter && p.limiter;
   k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate);
 }
-void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
-  size_t shm = 25 * TB * sizeof(double);
-  if (p.fp32)
-    k_flux<float><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, implicit, for_step);
-  else
-    k_flux<double><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, implicit, for_step);
+constexpr int FLUX_CELLS = 128 / FL;  // cells per k_flux2 block
+// residual only: 8 lanes per cell (light kernel, many warps)
+template <typename BT, int KIND>
+static void launch_flux_k(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
+  int g = grid_for(m.ncv, FLUX_CELLS);
+  if (p.viscous) k_rhs2<KIND, 1><<<g, 128, 0, s>>>(m, p, st, for_step);
+  else k_rhs2<KIND, 0><<<g, 128, 0, s>>>(m, p, st, for_step);
 }
+template <typename BT>
+static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
+  if (p.flux == JG_FLUX_ROE) launch_flux_k<BT, 1>(m, p, st, implicit, for_step, s);
+  else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
+  else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
+}
+template <typename BT, int KIND>
+static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
+  size_t shm = 25 * TB * sizeof(double);
+  if (p.viscous) k_flux<BT, KIND, 1><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
+  else k_flux<BT, KIND, 0><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
+}
+template <typename BT>
+static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
+  if (p.flux == JG_FLUX_ROE) launch_flux_cell_k<BT, 1>(m, p, st, for_step, s);
+  else if (p.flux == JG_FLUX_AUSM) launch_flux_cell_k<BT, 2>(m, p, st, for_step, s);
+  else launch_flux_cell_k<BT, 0>(m, p, st, for_step, s);
+}
+// residual + Jacobian: one thread per cell, so that the 32 lanes of a warp
+// walk the same face position of 32 neighbouring cells (coherent branches);
+// residual only: the light 8-lanes-per-cell kernel
+void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
+  if (!implicit) {
+    if (p.fp32) launch_flux_t<float>(m, p, st, 0, for_step, s);
+    else launch_flux_t<double>(m, p, st, 0, for_step, s);
+    return;
+  }
+  if (p.fp32) launch_flux_cell<float>(m, p, st, for_step, s);
+  else launch_flux_cell<double>(m, p, st, for_step, s);
+}
+// number of per-block residual partials written by launch_flux
+int flux_partials(const Mesh& m, int implicit) { return implicit ? grid_for(m.ncv, TB) : grid_for(m.ncv, FLUX_CELLS); }
 void launch_resid(const Mesh& m, State& st, int hist_from_ctrl, cudaStream_t s) {
-  k_resid_final<<<1, 256, 0, s>>>(st, grid_for(m.ncv, TB), hist_from_ctrl);
+  k_resid_final<<<1, 256, 0, s>>>(st, flux_partials(m, 1), hist_from_ctrl);
 }
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {
   for (int it = 0; it < sweeps; it++) {
     void* xin = (it % 2 == 0) ? st.x1 : st.x0;
     void* xout = (it % 2 == 0) ? st.x0 : st.x1;
     if (p.fp32)
-      k_jacobi<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const float*)xin, (float*)xout, it == 0);
+      k_jacobi2<float><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (const float*)xin, (float*)xout, it == 0);
     else
-      k_jacobi<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
+      k_jacobi2<double><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
   }
 }
 void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s) {

@@ -1,0 +1,49 @@
+"""Converged-field golden: the reference solver itself (oracle/_ref/ref_harness)
+run to steady state on the 64x32x4 inviscid channel-with-bump case (8,192
+cells; HLLC, second order LSQ + Barth-Jespersen EPS 0.01, backward Euler,
+BiCGSTAB, CFL ramp 1 -> 100), stopped at a 1e-10 drop of the L1 energy
+residual or 2,000 iterations.  Stores the reference's cell centroids, the
+converged conserved state and the residual history.
+
+    python tests/golden/make_converged.py      # a few minutes on one core
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from myjoe_b200 import case, meshgen  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DROP = 1.0e-10
+
+
+def bump_config():
+    raw, g, prm = case.bump_case(64, 32, 4)
+    prm = dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 100.0), EPS=0.01)
+    return raw, g, prm
+
+
+def main():
+    raw, g, prm = bump_config()
+    write = lambda p: meshgen.write_msh(p, raw)
+    first = refrun.run(write, dataclasses.replace(prm, NSTEPS=1).joe_in("mesh.msh"), "run")
+    r0 = float(first["resid"][0][4])
+    run = dataclasses.replace(prm, NSTEPS=2000)
+    r = refrun.run(write, run.joe_in("mesh.msh", "RESID_ENERG_TH = %.17g" % (DROP * r0)), "run", timeout=3600)
+    np.savez_compressed(os.path.join(HERE, "converged_bump_64x32x4.npz"), x_cv=r["x_cv"].reshape(-1, 3),
+                        rho=r["final_rho"], rhou=r["final_rhou"].reshape(-1, 3), rhoE=r["final_rhoE"],
+                        resid=r["resid"], steps=np.array(r["steps"]), seconds=np.array(r["seconds"]))
+    print("steps", r["steps"], "seconds", r["seconds"], "final/initial energy residual",
+          r["resid"][-1][4] / r0)
+
+
+if __name__ == "__main__":
+    main()

@@ -12,7 +12,8 @@ from oracle.oracle import Oracle
 from myjoe_b200.case import SOLVER_KINDS
 from tests.golden.make_golden import load
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
+                if not os.path.basename(p).startswith("converged_"))
 
 
 @pytest.fixture(params=GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])

@@ -65,6 +65,7 @@ struct jg_case {
   cudaGraphExec_t graph = nullptr;
   int graph_sweeps = -1;
   int primed = 0;           // state + BC computed since the last set_state
+  int ncolors = 1;
   int profiling = 0;        // record events around the face loop and the relaxation in the graph
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t graph_kernels = 0;
@@ -265,6 +266,23 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     }
   }
   h->ell_elems = (size_t)rows * 25 * SLICE;
+  // greedy colouring of the cell graph (neighbours through internal faces), in cell order
+  std::vector<uint8_t> color(N, 0);
+  int ncolors = 1;
+  {
+    std::vector<int> mark(256, -1);
+    for (int c = 0; c < N; c++) {
+      for (int j = h->cell_cols[c]; j < h->cell_cols[c + 1]; j++) {
+        int nb = h->col_nb[j];
+        if (nb < c) mark[color[nb]] = c;
+      }
+      int k = 0;
+      while (k < 255 && mark[k] == c) k++;
+      color[c] = (uint8_t)k;
+      ncolors = std::max(ncolors, k + 1);
+    }
+  }
+  h->ncolors = ncolors;
   // device mesh
   Mesh& m = h->m;
   memset(&m, 0, sizeof(m));
@@ -287,6 +305,8 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(upload(h, &m.ell_off, h->ell_off.data(), h->ell_off.size()));
   RC(upload(h, &m.ell_nb, ell_nb.data(), ell_nb.size()));
   RC(upload(h, &m.ell_lower, ell_lower.data(), ell_lower.size()));
+  RC(upload(h, &m.color, color.data(), color.size()));
+  m.ncolors = ncolors;
   // device state
   State& st = h->st;
   memset(&st, 0, sizeof(st));
@@ -658,11 +678,16 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
       launch_dq_from_x(h->m, h->p, h->st, h->st.x1, h->stream);
       it = 1;
       break;
-    case JG_LS_JACOBI:
-    case JG_LS_SGS: {
+    case JG_LS_JACOBI: {
       int sweeps = std::max(1, maxIter);
       launch_jacobi(h->m, h->p, h->st, sweeps, h->stream);
       launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, h->stream);
+      it = sweeps;
+    } break;
+    case JG_LS_SGS: {
+      int sweeps = std::max(1, maxIter);
+      launch_sgs(h->m, h->p, h->st, sweeps, h->stream);
+      launch_dq_from_x(h->m, h->p, h->st, h->st.x0, h->stream);
       it = sweeps;
     } break;
   }
@@ -688,10 +713,13 @@ static int enqueue_step(jg_case* h, int for_graph) {
   if (solver == JG_LS_LUSGS) {
     launch_lusgs(h->m, h->p, h->st, S);
     launch_dq_from_x(h->m, h->p, h->st, h->st.x1, S);
-  } else if (solver == JG_LS_JACOBI || solver == JG_LS_SGS) {
+  } else if (solver == JG_LS_JACOBI) {
     int sweeps = std::max(1, h->hp.ls_max_iter);
     launch_jacobi(h->m, h->p, h->st, sweeps, S);
     launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
+  } else if (solver == JG_LS_SGS) {
+    launch_sgs(h->m, h->p, h->st, std::max(1, h->hp.ls_max_iter), S);
+    launch_dq_from_x(h->m, h->p, h->st, h->st.x0, S);
   } else {
     if (for_graph) return set_err(JG_ERR_ARG, "BCGSTAB is not captured");
     // host-driven BiCGSTAB on the assembled system, zero initial guess

@@ -50,6 +50,8 @@ struct Mesh {
   const int* ell_nb;       // [ell_rows*32] neighbour per ELL entry (padding: the cell itself)
   const uint8_t* ell_lower;// [ell_rows*32] 1 when the neighbour precedes the cell (LU-SGS)
   int ell_rows;
+  const uint8_t* color;    // [N] colour of the cell (no two neighbours share one)
+  int ncolors;
 };
 
 // Per-case device state.  Primitive record: u,v,w,p,T,h,c,pad.  Boundary
@@ -108,6 +110,8 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
 void launch_resid(const Mesh& m, State& st, int hist_index_from_ctrl, cudaStream_t s);
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
+// multicolour Gauss-Seidel: result in st.x0
+void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
 void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s);
 void launch_lusgs(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_dinv(const Mesh& m, const Params& p, State& st, cudaStream_t s);

@@ -840,6 +840,40 @@ __global__ void __launch_bounds__(128) k_jacobi(Mesh m, State st, const BT* __re
   }
 }
 
+// Multicolour block Gauss-Seidel pass over one colour, in place: the cells of
+// a colour have no neighbours of the same colour, so each reads the latest
+// values of the others.  Same row-parallel layout as k_jacobi2.
+template <typename BT>
+__global__ void __launch_bounds__(160) k_gs2(Mesh m, State st, BT* __restrict__ x, int color) {
+  __shared__ BT sacc[5][SLICE];
+  const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
+  const int slice = blockIdx.x;
+  const int c = slice * SLICE + lane;
+  const bool active = c < m.ncv && m.color[c] == color;
+  const int N = m.ncv;
+  BT acc = 0;
+  if (active) {
+    acc = (BT)st.b[5 * c + row];
+    const BT* O = (const BT*)st.O;
+    int j0 = m.ell_off[slice], j1 = m.ell_off[slice + 1];
+    for (int j = j0; j < j1; j++) {
+      int nb = m.ell_nb[(size_t)j * SLICE + lane];
+      const BT* Ob = O + ((size_t)j * 25 + 5 * row) * SLICE + lane;
+      BT s = 0;
+      for (int k = 0; k < 5; k++) s += Ob[k * SLICE] * x[(size_t)k * N + nb];
+      acc -= s;
+    }
+  }
+  sacc[row][lane] = acc;
+  __syncthreads();
+  if (active) {
+    const BT* Di = (const BT*)st.Dinv;
+    BT s = 0;
+    for (int k = 0; k < 5; k++) s += Di[(size_t)(5 * row + k) * N + c] * sacc[k][lane];
+    x[(size_t)row * N + c] = s;
+  }
+}
+
 template <typename BT>
 __global__ void k_dq_from_x(Mesh m, State st, const BT* x) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1129,6 +1163,16 @@ void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaSt
     else
       k_jacobi2<double><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
   }
+}
+void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {
+  size_t bytes = 5 * (size_t)m.ncv * (p.fp32 ? sizeof(float) : sizeof(double));
+  cudaMemsetAsync(st.x0, 0, bytes, s);
+  for (int it = 0; it < sweeps; it++)
+    for (int q = 0; q < m.ncolors; q++) {
+      int col = (it % 2 == 0) ? q : m.ncolors - 1 - q;  // forward, then backward colour order
+      if (p.fp32) k_gs2<float><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (float*)st.x0, col);
+      else k_gs2<double><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (double*)st.x0, col);
+    }
 }
 void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s) {
   if (p.fp32)

@@ -1455,12 +1455,58 @@ static int solve_jacobi(jo_case *h, double *phi, const double *A, const double *
   return sweeps;
 }
 
+/* Multicolour block Gauss-Seidel as the GPU runs it (not in the reference):
+ * greedy colouring of the cell graph in cell order; each pass updates the
+ * colours in turn (forward, then backward on the next pass) from x = 0. */
+static int solve_sgs(jo_case *h, double *phi, const double *A, const double *rhs, int sweeps) {
+  int n = h->ncv;
+  const jg_mesh *m = &h->m;
+  double *LU = dalloc(25 * n);
+  int *color = (int *)calloc(n, sizeof(int));
+  int ncol = 1;
+  int mark[256];
+  for (int k = 0; k < 256; k++) mark[k] = -1;
+  for (int c = 0; c < n; c++) {
+    for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++)
+      if (m->nbocv_v[k] < c) mark[color[m->nbocv_v[k]]] = c;
+    int q = 0;
+    while (q < 255 && mark[q] == c) q++;
+    color[c] = q;
+    if (q + 1 > ncol) ncol = q + 1;
+  }
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[25 * c], &A[25 * m->nbocv_i[c]], 25 * sizeof(double));
+    ludeco((double(*)[5]) & LU[25 * c], 5);
+  }
+  memset(phi, 0, sizeof(double) * 5 * n);
+  for (int s = 0; s < sweeps; s++)
+    for (int q = 0; q < ncol; q++) {
+      int col = (s % 2 == 0) ? q : ncol - 1 - q;
+      for (int c = 0; c < n; c++) {
+        if (color[c] != col) continue;
+        double b[5];
+        for (int i = 0; i < 5; i++) b[i] = rhs[5 * c + i];
+        for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+          int nb = m->nbocv_v[k];
+          for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++) b[i] -= A[25 * k + 5 * i + j] * phi[5 * nb + j];
+        }
+        lusolv((double(*)[5]) & LU[25 * c], b, 5);
+        memcpy(&phi[5 * c], b, sizeof(b));
+      }
+    }
+  free(LU);
+  free(color);
+  return sweeps;
+}
+
 int jo_solve(jo_case *h, double *dq, const double *A, const double *rhs, double zeroAbs, double zeroRel, int maxIter,
              int solver) {
   switch (solver) {
     case JG_LS_BCGSTAB: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter);
     case JG_LS_LUSGS: return solve_lusgs(h, dq, A, rhs);
     case JG_LS_JACOBI: return solve_jacobi(h, dq, A, rhs, maxIter);
+    case JG_LS_SGS: return solve_sgs(h, dq, A, rhs, maxIter);
     default: return -1;
   }
 }

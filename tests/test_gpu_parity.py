@@ -145,7 +145,8 @@ def test_linear_solve_reference_solvers(golden):
         assert nrel(dq_g, g["dq"].reshape(-1, 5)) <= 1e-10
 
 
-def test_point_relaxation_matches_oracle(golden):
+@pytest.mark.parametrize("relax", ["JACOBI", "SGS"])
+def test_point_relaxation_matches_oracle(golden, relax):
     g = golden
     A = g["A"].copy()
     vol_dt = g["cv_volume"] / g["local_dt"]
@@ -153,8 +154,8 @@ def test_point_relaxation_matches_oracle(golden):
         A[g["nbocv_i"][:-1], i, i] += vol_dt
     rhs = g["rhs_sys"].reshape(-1, 5)
     o = Oracle(dict(g), g["params"])
-    dq_o, _ = o.solve(A, rhs, 0, 0, 7, SOLVER_KINDS["JACOBI"])
-    j = gpu_case(g, "JACOBI")
+    dq_o, _ = o.solve(A, rhs, 0, 0, 7, SOLVER_KINDS[relax])
+    j = gpu_case(g, relax)
     dq_g, _ = j.solveCoupledLinSysNS(A, rhs, 0, 0, 7)
     assert nrel(dq_g, dq_o) <= TOL
 

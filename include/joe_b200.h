@@ -167,6 +167,26 @@ int jg_get_profile(jg_case_t *h, double *ms);
 /* number of kernels one captured step launches */
 int jg_step_kernel_count(jg_case_t *h, int *n);
 
+/* Block point relaxation that allocates nothing.  No counterpart in the
+ * reference.  For hosts that cannot call cudaMalloc when they need the solve:
+ * their device memory is owned by another allocator (a pool that claimed the
+ * GPU up front, an application that budgets every byte), or an allocation's
+ * device synchronisation or out-of-memory failure mid-run is not acceptable.
+ * All pointers are DEVICE memory owned by the caller, in the reference's
+ * layouts: nbocv_i[ncv+1], nbocv_v[nnz] (CSR, diagonal first), A[nnz][5][5],
+ * rhs[ncv][5]; dq[ncv][5] receives the result of `sweeps` block Jacobi sweeps
+ * from zero (the iteration of jg_solve_lin_sys with JG_LS_JACOBI).  Work
+ * memory is a fixed array of JG_NOALLOC_MAX_CELLS x 5 doubles (2.5 MiB) inside
+ * the library, held by every GPU that loads it until the process exits;
+ * ncv > JG_NOALLOC_MAX_CELLS is rejected with JG_ERR_ARG.  The first call on
+ * each device looks up that array's device address (cudaGetSymbolAddress, no
+ * allocation); make that first call before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU race.  Enqueued on
+ * `stream` (a cudaStream_t, NULL = default stream); no synchronisation. */
+#define JG_NOALLOC_MAX_CELLS 65536
+int jg_relax_csr_noalloc(int ncv, const int *nbocv_i, const int *nbocv_v, const double *A, const double *rhs,
+                         double *dq, int sweeps, void *stream);
+
 /* Per-face Euler fluxes and implicit matrices, batched over n faces on the
  * GPU: calcEulerFlux_{HLLC,Roe,AUSM} and calcEulerFluxMatrices_{HLLC,Roe}
  * (src/joe/UgpWithCvCompFlow.cpp:120-709, 3281-3641).  L/R[n][6] =

@@ -156,6 +156,11 @@ static int check_params(const jg_params* q) {
   return JG_OK;
 }
 
+namespace jg {
+// lets the other translation units of the library set the jg_last_error message
+int record_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+}  // namespace jg
+
 extern "C" {
 
 const char* jg_last_error(void) { return g_err.c_str(); }

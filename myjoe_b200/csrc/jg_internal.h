@@ -129,5 +129,6 @@ void launch_pack_state(int n, const double* io, double* q, cudaStream_t s);
 void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s);
 
 int grid_for(long n, int block);
+int record_error(int code, const char* msg);  // sets the jg_last_error message
 
 }  // namespace jg

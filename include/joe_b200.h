@@ -159,6 +159,28 @@ int jg_step(jg_case_t *h, int nsteps, double *resid);
 /* the same steps enqueued on the case stream without synchronising */
 int jg_step_async(jg_case_t *h, int nsteps);
 int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
+/* Batching form (no reference counterpart; the reference runs one case per
+ * process): ncases independent cases, each with its own mesh and boundary
+ * values, concatenated into one block-diagonal system so that every stage of
+ * the iteration is one launch over all cases.  Each case keeps its own
+ * residual reduction and never reads another case's data, so its results are
+ * bit-identical alone and in any batch.  Linear solver JACOBI, SGS or LUSGS;
+ * time step CFL or DT.  The batch handle accepts every single-case call
+ * (jg_step reports the residual summed over the cases). */
+int jg_batch_create(int ncases, const jg_mesh *meshes, const jg_params *params, jg_case_t **out);
+int jg_batch_info(jg_case_t *h, int *ncases, int *cell_offsets /* [ncases+1], may be NULL */);
+/* sets one case's state; the state/BC preamble runs at the next step (set every case first) */
+int jg_batch_set_state(jg_case_t *h, int case_id, const double *rho, const double *rhou, const double *rhoE);
+int jg_batch_get_state(jg_case_t *h, int case_id, double *rho, double *rhou, double *rhoE);
+/* resid[nsteps][ncases][5]: the L1 residual of every case at every step.  A
+ * case that goes non-physical does not stop the batch: see jg_batch_status. */
+int jg_batch_step(jg_case_t *h, int nsteps, double *resid);
+/* status[ncases]: error flags of each case since the last call (1: density or
+ * pressure <= 0, 4: NaN residual); cleared by the call */
+int jg_batch_status(jg_case_t *h, int *status);
+/* freeze (0) or resume (1) a case: a frozen case keeps its state (retired) */
+int jg_batch_set_active(jg_case_t *h, int case_id, int active);
+
 /* Timing hooks (no reference counterpart): with profiling on, the captured
  * step records CUDA events around the face loop and the linear solve;
  * jg_get_profile returns their device times (ms) for the last step. */

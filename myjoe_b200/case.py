@@ -148,20 +148,35 @@ def perturbed_state(x_cv: np.ndarray, params: JoeParams, amp: float):
 # ----------------------------------------------------------------------------
 
 def bump_case(nx=64, ny=32, nz=4, mach=0.5, p=1.0e5, T=300.0, flux="HLLC", jitter=0.0,
-              seed=0, bump_h=0.1, aoa_deg=0.0, shuffle=False):
+              seed=0, bump_h=0.1, aoa_deg=0.0, shuffle=False, inlet="CBC"):
     """Inviscid channel-with-bump (channel length 3 chords, height 1; the
-    bump is 0.1 sin^2 on the middle chord): CBC inlet, CBC_SUBSONIC_OUTLET
-    outlet, WALL lower, SYMMETRY upper and z planes."""
+    bump is bump_h sin^2 on the middle chord): WALL lower, SYMMETRY upper and
+    z planes, CBC_SUBSONIC_OUTLET at p.  ``inlet="CBC"`` prescribes the inflow
+    state (u, T, p), i.e. the mass flow; ``inlet="TOTAL"`` prescribes total
+    pressure and temperature for the inflow Mach number and direction
+    (CBC_SUBSONIC_INLET), so the mass flow follows from the pressure ratio and
+    a choked throat with a shock is a valid steady state; ``inlet="FARFIELD"``
+    makes inlet, outlet and top far-field boundaries (flow over a bump at an
+    angle of attack)."""
     gam, R = 1.4, 287.0
     rho = p / (R * T)
     c = math.sqrt(gam * R * T)
     a = math.radians(aoa_deg)
     u = (mach * c * math.cos(a), mach * c * math.sin(a), 0.0)
     raw = meshgen.channel_bump(nx, ny, nz, bump_h=bump_h, jitter=jitter, seed=seed)
+    bcs = {"outlet": BC("CBC_SUBSONIC_OUTLET", (p,)), "lower": BC("WALL"), "upper": BC("SYMMETRY"),
+           "sides": BC("SYMMETRY")}
+    if inlet == "TOTAL":
+        f = 1.0 + 0.5 * (gam - 1.0) * mach * mach
+        bcs["inlet"] = BC("CBC_SUBSONIC_INLET", (math.cos(a), math.sin(a), 0.0, T * f, p * f ** (gam / (gam - 1.0))))
+    elif inlet == "FARFIELD":
+        # external flow over the bump: Riemann-invariant far field on inlet, outlet and top
+        ff = BC("FARFIELD", u + (p, rho, gam))
+        bcs.update(inlet=ff, outlet=ff, upper=ff)
+    else:
+        bcs["inlet"] = BC("CBC", u + (T, p))
     prm = JoeParams(T_REF=T, P_REF=p, RHO_REF=rho, GAMMA=gam, SPACE_INTEGRATION=flux,
-                    U_INITIAL=u, P_INITIAL=p, RHO_INITIAL=rho,
-                    bcs={"inlet": BC("CBC", u + (T, p)), "outlet": BC("CBC_SUBSONIC_OUTLET", (p,)),
-                         "lower": BC("WALL"), "upper": BC("SYMMETRY"), "sides": BC("SYMMETRY")})
+                    U_INITIAL=u, P_INITIAL=p, RHO_INITIAL=rho, bcs=bcs)
     return raw, geometry.build_cv_mesh(raw, seed=seed, shuffle=shuffle), prm
 
 

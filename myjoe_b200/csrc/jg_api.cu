@@ -66,6 +66,10 @@ struct jg_case {
   int graph_sweeps = -1;
   int primed = 0;           // state + BC computed since the last set_state
   int ncolors = 1;
+  int ncases = 1;           // independent cases concatenated in this handle (jg_batch_create)
+  std::vector<int> case_off;        // [ncases+1] first cell of each case
+  std::vector<int> case_nfa_b_off;  // [ncases+1] first boundary face of each case
+  int* d_case_off = nullptr;
   int profiling = 0;        // record events around the face loop and the relaxation in the graph
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t graph_kernels = 0;
@@ -342,7 +346,26 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(dmalloc(h, &st.err, 4));
   h->hist_cap = 64;
   st.hist_cap = h->hist_cap;
-  RC(dmalloc(h, &st.resid, 5 * (size_t)h->hist_cap));
+  if (h->case_off.empty()) {
+    h->case_off = {0, N};
+    h->case_nfa_b_off = {0, nfa_b};
+  }
+  h->ncases = (int)h->case_off.size() - 1;
+  RC(dmalloc(h, &st.resid, 5 * (size_t)h->hist_cap * h->ncases));
+  {
+    const int* d = nullptr;
+    RC(upload(h, &d, h->case_off.data(), h->case_off.size()));
+    h->d_case_off = (int*)d;
+    std::vector<int> case_of(N);
+    for (int k = 0; k < h->ncases; k++)
+      for (int c = h->case_off[k]; c < h->case_off[k + 1]; c++) case_of[c] = k;
+    RC(upload(h, &h->m.case_of, case_of.data(), case_of.size()));
+    RC(dmalloc(h, &st.case_err, (size_t)h->ncases));
+    std::vector<uint8_t> on(h->ncases, 1);
+    const uint8_t* da = nullptr;
+    RC(upload(h, &da, on.data(), on.size()));
+    st.case_active = (uint8_t*)da;
+  }
   double ctrl0[16] = {0};
   ctrl0[0] = q->cfl;
   CK(cudaMemcpy(st.ctrl, ctrl0, sizeof(ctrl0), cudaMemcpyHostToDevice));
@@ -370,6 +393,151 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
   return JG_OK;
 }
 
+static int prime(jg_case* h);
+
+// ---------------------------------------------------------------------------
+// batches: many independent cases concatenated into one block-diagonal system
+// ---------------------------------------------------------------------------
+struct MeshCat {
+  std::vector<int> cvofa, faocv_i, faocv_v, nbocv_i, nbocv_v;
+  std::vector<double> x_cv, x_fa, fa_normal, vol, lsq, blsq;
+  std::vector<jg_zone> zones;
+  jg_mesh m;
+};
+
+// Boundary faces of every case first (case by case), then the internal faces
+// (case by case); cells case by case.  Per case, the relative order of cells,
+// faces and CSR entries is the case's own, so every per-cell computation sees
+// exactly what it sees when the case runs alone.
+static int concat_meshes(int ncases, const jg_mesh* ms, MeshCat& o, std::vector<int>& case_off,
+                         std::vector<int>& bfa_off) {
+  long N = 0, NF = 0, NB = 0, NBS = 0, NZ = 0;
+  for (int k = 0; k < ncases; k++) {
+    const jg_mesh& m = ms[k];
+    if (m.ncv <= 0 || m.nfa < m.nfa_b || m.nfa_b < 0 || m.nbocv_s < m.ncv)
+      return set_err(JG_ERR_ARG, "case %d: inconsistent mesh sizes", k);
+    N += m.ncv; NF += m.nfa; NB += m.nfa_b; NBS += m.nbocv_s; NZ += m.nzones;
+  }
+  if (N > 2000000000L || NF > 2000000000L || NBS > 2000000000L) return set_err(JG_ERR_ARG, "batch too large");
+  case_off.assign(ncases + 1, 0);
+  bfa_off.assign(ncases + 1, 0);
+  for (int k = 0; k < ncases; k++) {
+    case_off[k + 1] = case_off[k] + ms[k].ncv;
+    bfa_off[k + 1] = bfa_off[k] + ms[k].nfa_b;
+  }
+  std::vector<long> int_off(ncases + 1, 0);
+  for (int k = 0; k < ncases; k++) int_off[k + 1] = int_off[k] + (ms[k].nfa - ms[k].nfa_b);
+  o.cvofa.assign(2 * NF, -1);
+  o.x_fa.assign(3 * NF, 0.0);
+  o.fa_normal.assign(3 * NF, 0.0);
+  o.blsq.assign(3 * NB, 0.0);
+  o.faocv_i.assign(N + 1, 0);
+  o.nbocv_i.assign(N + 1, 0);
+  o.faocv_v.clear();
+  o.nbocv_v.clear();
+  o.x_cv.clear(); o.vol.clear(); o.lsq.clear(); o.zones.clear();
+  for (int k = 0; k < ncases; k++) {
+    const jg_mesh& m = ms[k];
+    const int co = case_off[k];
+    auto gf = [&](int f) -> long { return f < m.nfa_b ? bfa_off[k] + f : NB + int_off[k] + (f - m.nfa_b); };
+    for (int f = 0; f < m.nfa; f++) {
+      long g = gf(f);
+      o.cvofa[2 * g] = m.cvofa[2 * f] + co;
+      o.cvofa[2 * g + 1] = m.cvofa[2 * f + 1] >= 0 ? m.cvofa[2 * f + 1] + co : -1;
+      for (int i = 0; i < 3; i++) {
+        o.x_fa[3 * g + i] = m.x_fa[3 * f + i];
+        o.fa_normal[3 * g + i] = m.fa_normal[3 * f + i];
+      }
+    }
+    for (int f = 0; f < m.nfa_b; f++)
+      for (int i = 0; i < 3; i++) o.blsq[3 * (bfa_off[k] + f) + i] = m.boundary_fa_lsg_coeff[3 * f + i];
+    for (int c = 0; c < m.ncv; c++) {
+      for (int q = m.faocv_i[c]; q < m.faocv_i[c + 1]; q++) o.faocv_v.push_back((int)gf(m.faocv_v[q]));
+      o.faocv_i[co + c + 1] = (int)o.faocv_v.size();
+      for (int q = m.nbocv_i[c]; q < m.nbocv_i[c + 1]; q++) {
+        o.nbocv_v.push_back(m.nbocv_v[q] + co);
+        for (int i = 0; i < 3; i++) o.lsq.push_back(m.nbocv_lsg_coeff[3 * q + i]);
+      }
+      o.nbocv_i[co + c + 1] = (int)o.nbocv_v.size();
+      for (int i = 0; i < 3; i++) o.x_cv.push_back(m.x_cv[3 * c + i]);
+      o.vol.push_back(m.cv_volume[c]);
+    }
+    for (int z = 0; z < m.nzones; z++) {
+      jg_zone zz = m.zones[z];
+      zz.ifa_f += bfa_off[k];
+      zz.ifa_l += bfa_off[k];
+      o.zones.push_back(zz);
+    }
+  }
+  jg_mesh& m = o.m;
+  m.ncv = (int)N; m.nfa = (int)NF; m.nfa_b = (int)NB; m.nbocv_s = (int)NBS; m.nzones = (int)o.zones.size();
+  m.cvofa = o.cvofa.data(); m.faocv_i = o.faocv_i.data(); m.faocv_v = o.faocv_v.data();
+  m.nbocv_i = o.nbocv_i.data(); m.nbocv_v = o.nbocv_v.data();
+  m.x_cv = o.x_cv.data(); m.x_fa = o.x_fa.data(); m.fa_normal = o.fa_normal.data(); m.cv_volume = o.vol.data();
+  m.nbocv_lsg_coeff = o.lsq.data(); m.boundary_fa_lsg_coeff = o.blsq.data(); m.zones = o.zones.data();
+  return JG_OK;
+}
+
+int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, jg_case_t** out) {
+  if (ncases <= 0 || !meshes || !out) return set_err(JG_ERR_ARG, "bad argument");
+  *out = nullptr;
+  RC(check_params(params));
+  if (params->lin_solver == JG_LS_BCGSTAB)
+    return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
+  if (params->time_step_mode == JG_TS_CFL_MIN)
+    return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
+  MeshCat cat;
+  jg_case* h = new jg_case();
+  int rc = concat_meshes(ncases, meshes, cat, h->case_off, h->case_nfa_b_off);
+  if (rc == JG_OK) rc = build(h, &cat.m, params);
+  if (rc != JG_OK) {
+    std::string keep = g_err;
+    jg_destroy(h);
+    g_err = keep;
+    return rc;
+  }
+  *out = h;
+  return JG_OK;
+}
+
+int jg_batch_info(jg_case_t* h, int* ncases, int* cell_offsets) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (ncases) *ncases = h->ncases;
+  if (cell_offsets)
+    for (int k = 0; k <= h->ncases; k++) cell_offsets[k] = h->case_off[k];
+  return JG_OK;
+}
+
+int jg_batch_set_state(jg_case_t* h, int k, const double* rho, const double* rhou, const double* rhoE) {
+  if (!h || !rho || !rhou || !rhoE || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
+  const size_t N = h->ncv, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
+  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
+  CK(cudaMemcpyAsync(h->d_io, rho, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + n, rhou, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + 4 * n, rhoE, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_pack_state((int)n, h->d_io, h->st.q + 5 * c0, h->stream);
+  CK(cudaMemsetAsync(h->st.prim + 8 * c0, 0, 8 * n * sizeof(double), h->stream));
+  CKL();
+  // the state/BC preamble runs at the next operator call, once every case has its state
+  h->primed = 0;
+  return JG_OK;
+}
+
+int jg_batch_get_state(jg_case_t* h, int k, double* rho, double* rhou, double* rhoE) {
+  if (!h || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
+  const size_t N = h->ncv, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
+  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
+  launch_unpack_state((int)n, h->st.q + 5 * c0, h->d_io, h->stream);
+  CKL();
+  if (rho) CK(cudaMemcpyAsync(rho, h->d_io, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhoE) CK(cudaMemcpyAsync(rhoE, h->d_io + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
 int jg_get_stream(jg_case_t* h, void** stream) {
   if (!h || !stream) return set_err(JG_ERR_ARG, "null argument");
   *stream = (void*)h->stream;
@@ -377,9 +545,14 @@ int jg_get_stream(jg_case_t* h, void** stream) {
 }
 
 static int check_err_flags(jg_case* h) {
-  int e = 0;
+  int e = 0, ec = 0;
   CK(cudaMemcpyAsync(&e, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (h->ncases == 1) CK(cudaMemcpyAsync(&ec, h->st.case_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (ec) {
+    CK(cudaMemsetAsync(h->st.case_err, 0, sizeof(int), h->stream));
+    e |= ec;
+  }
   if (e) {
     CK(cudaMemsetAsync(h->st.err, 0, sizeof(int), h->stream));
     if (e & 2) return set_err(JG_ERR_ARG, "unrecognised boundary condition");
@@ -712,7 +885,7 @@ static int enqueue_step(jg_case* h, int for_graph) {
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
   launch_flux(h->m, h->p, h->st, 1, 1, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
-  launch_resid(h->m, h->st, 1, S);
+  launch_resid_cases(h->st, h->d_case_off, h->ncases, 1, S);
   int solver = h->hp.lin_solver;
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
   if (solver == JG_LS_LUSGS) {
@@ -786,7 +959,7 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   if (nsteps > h->hist_cap) {
     int cap = std::max(nsteps, 2 * h->hist_cap);
     double* r = nullptr;
-    RC(dmalloc(h, &r, 5 * (size_t)cap));
+    RC(dmalloc(h, &r, 5 * (size_t)cap * h->ncases));
     h->st.resid = r;
     h->hist_cap = cap;
     h->st.hist_cap = cap;
@@ -809,8 +982,51 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   }
   CKL();
   RC(check_err_flags(h));
-  if (resid && nsteps > 0)
-    CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+  if (resid && nsteps > 0) {
+    if (h->ncases == 1) {
+      CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+      // the sum over the cases of the batch, per step
+      std::vector<double> all(5 * (size_t)nsteps * h->ncases);
+      CK(cudaMemcpy(all.data(), h->st.resid, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int k = 0; k < nsteps; k++)
+        for (int i = 0; i < 5; i++) {
+          double v = 0.0;
+          for (int c = 0; c < h->ncases; c++) v += all[((size_t)k * h->ncases + c) * 5 + i];
+          resid[5 * k + i] = v;
+        }
+    }
+  }
+  return JG_OK;
+}
+
+// per-case status of a batch: status[k] = error flags of case k since the last
+// call (1: non-positive density or pressure, 4: NaN residual), then cleared
+int jg_batch_status(jg_case_t* h, int* status) {
+  if (!h || !status) return set_err(JG_ERR_ARG, "bad argument");
+  CK(cudaMemcpyAsync(status, h->st.case_err, h->ncases * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->st.case_err, 0, h->ncases * sizeof(int), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+// freeze (active = 0) or resume a case of the batch; a frozen case's state is not updated
+int jg_batch_set_active(jg_case_t* h, int k, int active) {
+  if (!h || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
+  uint8_t v = active ? 1 : 0;
+  CK(cudaMemcpyAsync(h->st.case_active + k, &v, 1, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+// nsteps backward-Euler iterations of every case of the batch; resid[nsteps][ncases][5]
+int jg_batch_step(jg_case_t* h, int nsteps, double* resid) {
+  if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
+  RC(jg_step(h, nsteps, nullptr));
+  if (resid && nsteps > 0) {
+    // jg_step sized the ring buffer to hold nsteps entries starting at index 0
+    CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * h->ncases * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   return JG_OK;
 }
 

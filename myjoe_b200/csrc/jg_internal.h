@@ -52,6 +52,7 @@ struct Mesh {
   int ell_rows;
   const uint8_t* color;    // [N] colour of the cell (no two neighbours share one)
   int ncolors;
+  const int* case_of;      // [N] case of each cell (batches)
 };
 
 // Per-case device state.  Primitive record: u,v,w,p,T,h,c,pad.  Boundary
@@ -78,9 +79,11 @@ struct State {
   double* dq;       // [N][5]
   double* blk;      // per-block partial sums (residual, dt min)
   double* ctrl;     // device control: [0]=cfl [1]=step [2]=dt_min [3..]=flags
-  double* resid;    // [hist_cap][5] residual history (ring buffer)
+  double* resid;    // [hist_cap][ncases][5] residual history (ring buffer)
   int hist_cap;
   int* err;         // error flags
+  int* case_err;    // [ncases] per-case error flags (1: rho/p <= 0, 4: NaN residual)
+  uint8_t* case_active;  // [ncases] 0: case frozen (retired), its state is not updated
 };
 
 struct Params {
@@ -109,6 +112,8 @@ void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl_cfl, doub
 void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
 void launch_resid(const Mesh& m, State& st, int hist_index_from_ctrl, cudaStream_t s);
+// per-case residual history, resid[(idx*ncases + case)*5 + i]
+void launch_resid_cases(State& st, const int* case_off, int ncases, int hist_from_ctrl, cudaStream_t s);
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
 // multicolour Gauss-Seidel: result in st.x0
 void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);

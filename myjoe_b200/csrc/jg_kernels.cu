@@ -54,14 +54,18 @@ __global__ void k_state(Mesh m, Params p, State st) {
 }
 
 // Q += dq (runBackwardEuler, JoeWithModels.cpp:1028-1035), then the new state.
+// Cells of a frozen (retired) case keep their state; state errors are
+// recorded per case.
 __global__ void k_update_state(Mesh m, Params p, State st) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ncv) return;
+  int k = m.case_of[c];
+  if (!st.case_active[k]) return;
   double q[5], prim[8];
   for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i] + st.dq[5 * c + i];
   for (int i = 0; i < 5; i++) st.q[5 * c + i] = q[i];
   for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
-  state_from_q(p, q, prim, st.err);
+  state_from_q(p, q, prim, st.case_err + k);
   for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
 }
 
@@ -803,6 +807,34 @@ __global__ void k_resid_final(State st, int nblk, int hist_from_ctrl) {
     for (int i = 0; i < 5; i++) st.resid[5 * idx + i] = s[i][0];
     if (!(s[4][0] == s[4][0])) atomicOr(st.err, 4);  // NaN energy residual (doneSolver)
   }
+}
+
+// Per-case L1 residual: block k sums |RHS| over the cells of case k in a fixed
+// order that depends only on that case, so a case's residual history is the
+// same alone and inside a batch.  out[(idx*ncases + k)*5 + i].
+__global__ void k_resid_cases(State st, const int* case_off, int ncases, int hist_from_ctrl) {
+  __shared__ double s[5][256];
+  int k = blockIdx.x, t = threadIdx.x;
+  double v[5] = {0, 0, 0, 0, 0};
+  for (int c = case_off[k] + t; c < case_off[k + 1]; c += blockDim.x)
+    for (int i = 0; i < 5; i++) v[i] += fabs(st.rhs[5 * c + i]);
+  for (int i = 0; i < 5; i++) s[i][t] = v[i];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (t < w)
+      for (int i = 0; i < 5; i++) s[i][t] += s[i][t + w];
+    __syncthreads();
+  }
+  if (t == 0) {
+    long idx = hist_from_ctrl ? (long)st.ctrl[1] - (long)st.ctrl[4] - 1 : 0;
+    idx = ((idx % st.hist_cap) + st.hist_cap) % st.hist_cap;  // ring buffer
+    for (int i = 0; i < 5; i++) st.resid[(idx * ncases + k) * 5 + i] = s[i][0];
+    if (!(s[4][0] == s[4][0]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN residual (doneSolver)
+  }
+}
+
+void launch_resid_cases(State& st, const int* case_off, int ncases, int hist_from_ctrl, cudaStream_t s) {
+  k_resid_cases<<<ncases, 256, 0, s>>>(st, case_off, ncases, hist_from_ctrl);
 }
 
 // ---------------------------------------------------------------------------

@@ -59,6 +59,13 @@ def lib():
         L.jg_step_async.argtypes = [P, I]
         L.jg_get_cfl_step.argtypes = [P, D, C.POINTER(I)]
         L.jg_euler_flux_faces.argtypes = [I, I, D, D, D, D, D, D, D]
+        L.jg_batch_create.argtypes = [I, C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
+        L.jg_batch_info.argtypes = [P, C.POINTER(I), C.POINTER(I)]
+        L.jg_batch_set_state.argtypes = [P, I, D, D, D]
+        L.jg_batch_get_state.argtypes = [P, I, D, D, D]
+        L.jg_batch_step.argtypes = [P, I, D]
+        L.jg_batch_status.argtypes = [P, C.POINTER(I)]
+        L.jg_batch_set_active.argtypes = [P, I, I]
         L.jg_set_profiling.argtypes = [P, I]
         L.jg_get_profile.argtypes = [P, D]
         L.jg_step_kernel_count.argtypes = [P, C.POINTER(I)]
@@ -203,3 +210,46 @@ def euler_flux_faces(kind, L, R, area, nvec, matrices=True):
     AR = np.zeros((n, 5, 5)) if matrices else None
     _ck(lib().jg_euler_flux_faces(kind, n, dptr(L), dptr(R), dptr(area), dptr(nvec), dptr(F), _p(AL), _p(AR)))
     return F, AL, AR
+
+
+class JoeGpuBatch(JoeGpu):
+    """Many independent cases advanced together (jg_batch_create): one launch
+    per stage over all cases.  ``cases`` is a list of (mesh, JoeParams); the
+    solver settings (flux, precision, linear solver, CFL ramp) come from the
+    first case, the boundary values from each case's own parameters."""
+
+    def __init__(self, cases, precision: int = 0):
+        self.params = cases[0][1]
+        self.mas = [MeshArrays(m, p) for m, p in cases]
+        self.jp = make_params(self.params, precision)
+        arr = (jg_mesh * len(cases))(*[ma.mesh for ma in self.mas])
+        h = C.c_void_p()
+        _ck(lib().jg_batch_create(len(cases), arr, C.byref(self.jp), C.byref(h)))
+        self.h = h
+        self.ncases = len(cases)
+        self.sizes = [ma.ncv for ma in self.mas]
+        self.ncv = sum(self.sizes)
+
+    def set_case_state(self, k, rho, rhou, rhoE):
+        rho, rhou, rhoE = (np.ascontiguousarray(a, np.float64) for a in (rho, rhou, rhoE))
+        _ck(lib().jg_batch_set_state(self.h, int(k), dptr(rho), dptr(rhou), dptr(rhoE)))
+
+    def get_case_state(self, k):
+        n = self.sizes[k]
+        rho, rhou, rhoE = np.empty(n), np.empty((n, 3)), np.empty(n)
+        _ck(lib().jg_batch_get_state(self.h, int(k), dptr(rho), dptr(rhou), dptr(rhoE)))
+        return rho, rhou, rhoE
+
+    def status(self):
+        st = (C.c_int * self.ncases)()
+        _ck(lib().jg_batch_status(self.h, st))
+        return np.array(list(st))
+
+    def set_active(self, k, active):
+        _ck(lib().jg_batch_set_active(self.h, int(k), int(bool(active))))
+
+    def runBackwardEulerCases(self, nsteps):
+        """residuals [nsteps][ncases][5]"""
+        r = np.zeros((max(nsteps, 1), self.ncases, 5))
+        _ck(lib().jg_batch_step(self.h, int(nsteps), dptr(r)))
+        return r[:nsteps]

@@ -181,6 +181,66 @@ int jg_batch_status(jg_case_t *h, int *status);
 /* freeze (0) or resume (1) a case: a frozen case keeps its state (retired) */
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
+/* Device bytes jg_create + jg_set_state allocate for a case (exact, before
+ * creating it) and the bytes a live handle holds. */
+int jg_case_footprint(const jg_mesh *mesh, const jg_params *params, double *bytes);
+int jg_case_device_bytes(jg_case_t *h, double *bytes);
+
+/* Serving form (no reference counterpart; the reference solves one case per
+ * run): a request loop on one GPU.  Submitted cases wait in a FIFO queue and
+ * are admitted while the device-memory budget and the resident-case limit
+ * allow; each resident case has its own handle, stream and captured step, so
+ * the cases' steps overlap on the device and every case's result is the one
+ * it gets alone.  jg_serve_poll is the progress engine: it launches
+ * steps_per_poll steps per resident case, reads each case's residuals without
+ * blocking the others, retires a case when its L1 energy residual has fallen
+ * to resid_drop x its first-step value (or after max_steps), and admits queued
+ * cases into the freed memory.  A case that reaches a non-physical state is
+ * restarted from its initial state with CFL_RAMP MAX_CFL (and the starting
+ * CFL, if above it) multiplied by restart_cfl_factor, up to max_restarts
+ * times.  Single-threaded: call every jg_serve_* of one server from one
+ * thread. */
+typedef struct jg_server jg_server_t;
+typedef struct {
+  int device;                /* CUDA device */
+  int max_resident;          /* cases on the device at once (>= 1) */
+  double hbm_budget;         /* device bytes the resident cases may hold; <= 0: 90% of the free memory */
+  int steps_per_poll;        /* steps launched per case between residual checks (1..64) */
+  double resid_drop;         /* convergence: energy residual / first-step energy residual */
+  int max_steps;             /* retire unconverged after this many steps */
+  int max_restarts;          /* restarts after a non-physical state */
+  double restart_cfl_factor; /* CFL scaling per restart (0 < f <= 1) */
+} jg_serve_config;
+enum { JG_SERVE_CONVERGED = 0, JG_SERVE_MAX_STEPS = 1, JG_SERVE_FAILED = 2 };
+typedef struct {
+  long long id;
+  int status;       /* JG_SERVE_* */
+  int steps;        /* steps of the final attempt (the state returned is after these) */
+  int steps_total;  /* steps over all attempts */
+  int restarts;
+  int ncv;
+  int conv_step;    /* first step whose residual met resid_drop (-1 if none) */
+  double drop;      /* energy residual / first-step energy residual at the last step */
+  double t_arrival; /* server clock (seconds since jg_serve_create) */
+  double t_admit;   /* first admission */
+  double t_done;
+  double bytes;     /* device footprint while resident */
+} jg_serve_result;
+int jg_serve_create(const jg_serve_config *cfg, jg_server_t **out);
+/* seconds since jg_serve_create on the server's monotonic clock */
+int jg_serve_now(jg_server_t *s, double *t);
+/* queue a case; the server copies mesh, params and the initial state.
+ * t_arrival < 0: now.  The mesh's host arrays may be freed on return. */
+int jg_serve_submit(jg_server_t *s, const jg_mesh *mesh, const jg_params *params, const double *rho,
+                    const double *rhou, const double *rhoE, double t_arrival, long long *id);
+/* run the progress engine for up to max_wait_s seconds or until a case
+ * retires; finished cases are written to out[0..*n) (at most cap) */
+int jg_serve_poll(jg_server_t *s, double max_wait_s, jg_serve_result *out, int cap, int *n);
+/* copy a retired case's final state and release it (each id once) */
+int jg_serve_fetch(jg_server_t *s, long long id, double *rho, double *rhou, double *rhoE);
+int jg_serve_stats(jg_server_t *s, int *resident, int *queued, int *finished_unfetched, double *bytes_resident);
+int jg_serve_destroy(jg_server_t *s);
+
 /* Timing hooks (no reference counterpart): with profiling on, the captured
  * step records CUDA events around the face loop and the linear solve;
  * jg_get_profile returns their device times (ms) for the last step. */

@@ -45,6 +45,19 @@ class jg_params(C.Structure):
                 ("precision", C.c_int), ("nscal", C.c_int)]
 
 
+class jg_serve_config(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_resident", C.c_int), ("hbm_budget", C.c_double),
+                ("steps_per_poll", C.c_int), ("resid_drop", C.c_double), ("max_steps", C.c_int),
+                ("max_restarts", C.c_int), ("restart_cfl_factor", C.c_double)]
+
+
+class jg_serve_result(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("status", C.c_int), ("steps", C.c_int), ("steps_total", C.c_int),
+                ("restarts", C.c_int), ("ncv", C.c_int), ("conv_step", C.c_int), ("drop", C.c_double),
+                ("t_arrival", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("bytes", C.c_double)]
+
+
 def dptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))

@@ -58,7 +58,9 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--solver", default="SGS", choices=["SGS", "JACOBI"])
     ap.add_argument("--sweeps", type=int, default=10)
-    ap.add_argument("--cfl-max", type=float, default=20.0)
+    ap.add_argument("--cfl-ramp", default="10,5,1.2,20",
+                    help="CFL_RAMP AFTER_ITER,INTERVAL_ITER,FACTOR_CFL,MAX_CFL")
+    ap.add_argument("--under-relax", type=float, default=0.3)
     ap.add_argument("--drop", type=float, default=1e-8)
     ap.add_argument("--max-steps", type=int, default=3000)
     ap.add_argument("--chunk", type=int, default=50)
@@ -74,9 +76,11 @@ def main(argv=None):
     if build.needs_build():
         build.build()
     cases = []
+    ra, ri, rf, rm = args.cfl_ramp.split(",")
+    ramp = (int(ra), int(ri), float(rf), float(rm))
     for g, prm in built:
         prm = dataclasses.replace(prm, LINEAR_SOLVER_NS=args.solver, LS_MAX_ITER=args.sweeps, CFL=1.0,
-                                  CFL_RAMP=(10, 5, 1.2, args.cfl_max))
+                                  CFL_RAMP=ramp, UNDER_RELAXATION=args.under_relax)
         cases.append((g, prm))
     b = solver.JoeGpuBatch(cases, precision=1 if args.precision == "mixed" else 0)
     for k, (g, prm) in enumerate(cases):
@@ -119,6 +123,7 @@ def main(argv=None):
     out = {
         "form": "batch", "cases": args.cases, "cells": int(ncv), "precision": args.precision,
         "solver": "%s x%d" % (args.solver, args.sweeps), "drop": args.drop,
+        "cfl_ramp": list(ramp), "under_relax": args.under_relax,
         "steps": steps, "ms_per_step": step_ms, "cell_iters_per_s": ncv * steps / (dev_ms / 1000.0),
         "converged": int(done.sum()), "failed": int(failed.sum()),
         "failed_cases": [dict(specs[k], cells=int(b.sizes[k])) for k in np.nonzero(failed)[0]][:20],

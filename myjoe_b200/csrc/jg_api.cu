@@ -70,40 +70,36 @@ struct jg_case {
   std::vector<int> case_off;        // [ncases+1] first cell of each case
   std::vector<int> case_nfa_b_off;  // [ncases+1] first boundary face of each case
   int* d_case_off = nullptr;
+  int nrblk = 0;                    // residual chunks (RCHUNK cells, case-local)
+  int* d_rblk_off = nullptr;        // [ncases+1]
+  int* d_rblk_case = nullptr;       // [nrblk]
   int profiling = 0;        // record events around the face loop and the relaxation in the graph
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t graph_kernels = 0;
   double* d_io = nullptr;   // [5][N] staging for direct host<->device state copies
+  int async_alloc = 0;      // stream-ordered allocation (serving): no device-wide sync on free
+  size_t bytes = 0;         // device bytes held by this handle
 };
 
 
-template <typename T>
-static int dmalloc(jg_case* h, T** p, size_t count) {
-  void* q = nullptr;
-  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  CK(cudaMalloc(&q, bytes));
-  CK(cudaMemset(q, 0, bytes));
-  h->allocs.push_back(q);
-  *p = (T*)q;
-  return JG_OK;
-}
+// every device allocation of a handle goes through here; sizes are rounded to
+// 256 bytes so that the footprint estimate (jg_case_footprint) can mirror them
+static inline size_t alloc_round(size_t bytes) { return (std::max<size_t>(bytes, 8) + 255) & ~(size_t)255; }
 
 static int dmalloc_bytes(jg_case* h, void** p, size_t bytes) {
   void* q = nullptr;
-  CK(cudaMalloc(&q, std::max<size_t>(bytes, 8)));
-  CK(cudaMemset(q, 0, std::max<size_t>(bytes, 8)));
-  h->allocs.push_back(q);
+  bytes = alloc_round(bytes);
+  if (h->async_alloc) {
+    CK(cudaMallocAsync(&q, bytes, h->stream));
+    h->allocs.push_back(q);
+    CK(cudaMemsetAsync(q, 0, bytes, h->stream));
+  } else {
+    CK(cudaMalloc(&q, bytes));
+    h->allocs.push_back(q);
+    CK(cudaMemsetAsync(q, 0, bytes, h->stream));  // ordered before the handle's own kernels
+  }
+  h->bytes += bytes;
   *p = q;
-  return JG_OK;
-}
-
-template <typename T>
-static int upload(jg_case* h, const T** dst, const T* src, size_t count) {
-  T* d = nullptr;
-  int rc = dmalloc(h, &d, count);
-  if (rc) return rc;
-  if (count) CK(cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice));
-  *dst = d;
   return JG_OK;
 }
 
@@ -112,6 +108,27 @@ static int upload(jg_case* h, const T** dst, const T* src, size_t count) {
     int rc_ = (x);           \
     if (rc_ != JG_OK) return rc_; \
   } while (0)
+
+template <typename T>
+static int dmalloc(jg_case* h, T** p, size_t count) {
+  void* q = nullptr;
+  RC(dmalloc_bytes(h, &q, std::max<size_t>(count, 1) * sizeof(T)));
+  *p = (T*)q;
+  return JG_OK;
+}
+
+template <typename T>
+static int upload(jg_case* h, const T** dst, const T* src, size_t count) {
+  T* d = nullptr;
+  int rc = dmalloc(h, &d, count);
+  if (rc) return rc;
+  // pageable source: the call returns once the data is staged, so the caller's
+  // (temporary) host array may go away at once
+  if (count) CK(cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  *dst = d;
+  return JG_OK;
+}
+
 
 static Params make_params(const jg_params& q) {
   Params p;
@@ -184,7 +201,12 @@ int jg_destroy(jg_case_t* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   for (int i = 0; i < 4; i++)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
-  for (void* p : h->allocs) cudaFree(p);
+  if (h->async_alloc) {
+    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
+  } else {
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+  }
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return JG_OK;
@@ -192,6 +214,7 @@ int jg_destroy(jg_case_t* h) {
 
 static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   const int N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b;
+  if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   h->ncv = N;
   h->nfa = nfa;
   h->nfa_b = nfa_b;
@@ -361,6 +384,18 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
       for (int c = h->case_off[k]; c < h->case_off[k + 1]; c++) case_of[c] = k;
     RC(upload(h, &h->m.case_of, case_of.data(), case_of.size()));
     RC(dmalloc(h, &st.case_err, (size_t)h->ncases));
+    std::vector<int> rblk_off(h->ncases + 1, 0), rblk_case;
+    for (int k = 0; k < h->ncases; k++) {
+      int nb = (h->case_off[k + 1] - h->case_off[k] + RCHUNK - 1) / RCHUNK;
+      rblk_off[k + 1] = rblk_off[k] + nb;
+      rblk_case.insert(rblk_case.end(), nb, k);
+    }
+    h->nrblk = rblk_off[h->ncases];
+    RC(upload(h, &d, rblk_off.data(), rblk_off.size()));
+    h->d_rblk_off = (int*)d;
+    RC(upload(h, &d, rblk_case.data(), rblk_case.size()));
+    h->d_rblk_case = (int*)d;
+    RC(dmalloc(h, &st.rpart, 5 * (size_t)h->nrblk));
     std::vector<uint8_t> on(h->ncases, 1);
     const uint8_t* da = nullptr;
     RC(upload(h, &da, on.data(), on.size()));
@@ -368,8 +403,8 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   }
   double ctrl0[16] = {0};
   ctrl0[0] = q->cfl;
-  CK(cudaMemcpy(st.ctrl, ctrl0, sizeof(ctrl0), cudaMemcpyHostToDevice));
-  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaMemcpyAsync(st.ctrl, ctrl0, sizeof(ctrl0), cudaMemcpyHostToDevice, h->stream));
+  if (!h->async_alloc) CK(cudaStreamSynchronize(h->stream));
   return JG_OK;
 }
 
@@ -390,6 +425,63 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
     return rc;
   }
   *out = h;
+  return JG_OK;
+}
+
+// Device bytes a handle made by jg_create holds once its state is set: the
+// allocations of build() plus the state staging buffer, each rounded like
+// dmalloc_bytes rounds it.  CUDA-graph and event storage is not included.
+static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
+  const size_t N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b, nbs = mesh->nbocv_s;
+  const size_t e = q->precision == JG_PREC_MIXED ? 4 : 8;
+  const int* fi = mesh->faocv_i;
+  const int* fv = mesh->faocv_v;
+  size_t nbslot = 0, rows = 0;
+  const size_t nslices = (N + SLICE - 1) / SLICE;
+  for (size_t sl = 0; sl < nslices; sl++) {
+    size_t w = 0;
+    for (size_t c = sl * SLICE; c < std::min(N, (sl + 1) * SLICE); c++) {
+      size_t nc = 0;
+      for (int k = fi[c]; k < fi[c + 1]; k++) (fv[k] < (int)nfa_b) ? nbslot++ : nc++;
+      w = std::max(w, nc);
+    }
+    rows += w;
+  }
+  const size_t d = 8, i = 4;
+  const size_t nz = std::max(1, mesh->nzones);
+  const size_t a[] = {
+      // mesh
+      3 * N * d, N * d, 3 * nfa * d, 3 * nfa * d, 2 * nfa * i, (N + 1) * i, (size_t)fi[N] * sizeof(Slot),
+      (N + 1) * i, nbs * i, 3 * nbs * d, (N + 1) * i, std::max<size_t>(nbslot, 1) * i, 3 * nfa_b * d,
+      nfa_b * i, nz * sizeof(DevZone), (nslices + 1) * i, rows * SLICE * i, rows * SLICE, N,
+      // state
+      5 * N * d, 8 * N * d, 8 * nfa_b * d, nfa * d, nfa * d, 9 * N * d,
+      (q->mu_ref > 0.0 && q->second_order && !q->visc_limiter && q->limiter) ? 9 * N * d : 0,
+      3 * N * d, 3 * N * d, 3 * N * d, N * d, 5 * N * d, 5 * N * d,
+      25 * N * e, 25 * N * e, rows * 25 * SLICE * e, 5 * N * e, 5 * N * e, 5 * N * d,
+      (5 * (size_t)grid_for((int)N, 16) + 5 * (size_t)grid_for((int)N, 256) + 16) * d, 16 * d, 4 * i,
+      5 * 64 * d, 2 * i, N * i, 1 * i, 1,
+      2 * i, ((N + RCHUNK - 1) / RCHUNK) * i, 5 * ((N + RCHUNK - 1) / RCHUNK) * d,
+      // state staging (jg_set_state / jg_get_state)
+      5 * N * d};
+  size_t b = 0;
+  for (size_t x : a)
+    if (x) b += alloc_round(x);
+  return b;
+}
+
+extern "C" int jg_case_footprint(const jg_mesh* mesh, const jg_params* params, double* bytes) {
+  if (!mesh || !params || !bytes) return set_err(JG_ERR_ARG, "null argument");
+  RC(check_params(params));
+  if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
+    return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
+  *bytes = (double)footprint(mesh, params);
+  return JG_OK;
+}
+
+extern "C" int jg_case_device_bytes(jg_case_t* h, double* bytes) {
+  if (!h || !bytes) return set_err(JG_ERR_ARG, "null argument");
+  *bytes = (double)h->bytes;
   return JG_OK;
 }
 
@@ -885,7 +977,7 @@ static int enqueue_step(jg_case* h, int for_graph) {
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
   launch_flux(h->m, h->p, h->st, 1, 1, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
-  launch_resid_cases(h->st, h->d_case_off, h->ncases, 1, S);
+  launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, S);
   int solver = h->hp.lin_solver;
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
   if (solver == JG_LS_LUSGS) {
@@ -1080,6 +1172,72 @@ int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// per-case operations of the serving engine (jg_serve.cu): nothing here waits
+// on the device, so one host thread can keep many cases in flight
+// ---------------------------------------------------------------------------
+namespace jg {
+
+int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** out) {
+  if (!mesh || !out) return set_err(JG_ERR_ARG, "null argument");
+  *out = nullptr;
+  RC(check_params(params));
+  if (params->lin_solver == JG_LS_BCGSTAB)
+    return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
+  if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
+    return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
+  jg_case* h = new jg_case();
+  h->async_alloc = 1;
+  int rc = build(h, mesh, params);
+  if (rc == JG_OK) rc = dmalloc(h, &h->d_io, 5 * (size_t)mesh->ncv);
+  if (rc != JG_OK) {
+    std::string keep = g_err;
+    jg_destroy(h);
+    g_err = keep;
+    return rc;
+  }
+  *out = h;
+  return JG_OK;
+}
+
+// initial state: staged copies, then the state/face/boundary pass of jg_set_state
+int serve_case_start(jg_case* h, const double* rho, const double* rhou, const double* rhoE) {
+  const size_t N = h->ncv;
+  CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_pack_state((int)N, h->d_io, h->st.q, h->stream);
+  launch_state(h->m, h->p, h->st, h->stream);
+  launch_face_props(h->m, h->p, h->st, h->stream);
+  launch_bc(h->m, h->p, h->st, h->stream);
+  CKL();
+  h->primed = 1;
+  return JG_OK;
+}
+
+int serve_case_ring(jg_case* h) { return h->hist_cap; }
+
+// nsteps captured steps, then the residual ring and the error flags into
+// (pinned) host memory, then ev.  Residual of step s (1-based, counted from
+// the handle's creation) lands at ring[(s - 1) % ring size].
+int serve_case_launch(jg_case* h, int nsteps, double* h_ring, int* h_err, cudaEvent_t ev) {
+  if (nsteps < 1 || nsteps > h->hist_cap) return set_err(JG_ERR_ARG, "steps per launch must be 1..%d", h->hist_cap);
+  RC(ensure_graph(h));
+  for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(h->graph, h->stream));
+  CK(cudaMemcpyAsync(h_ring, h->st.resid, 5 * (size_t)h->hist_cap * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaMemcpyAsync(h_err, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h_err + 1, h->st.case_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaEventRecord(ev, h->stream));
+  return JG_OK;
+}
+
+size_t serve_case_bytes(jg_case* h) { return h->bytes; }
+int serve_case_ncv(jg_case* h) { return h->ncv; }
+int serve_set_err(int code, const char* msg) { return set_err(code, "%s", msg); }
+
+}  // namespace jg
 
 extern "C" int jg_set_profiling(jg_case_t* h, int on) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");

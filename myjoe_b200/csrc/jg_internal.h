@@ -80,6 +80,7 @@ struct State {
   double* blk;      // per-block partial sums (residual, dt min)
   double* ctrl;     // device control: [0]=cfl [1]=step [2]=dt_min [3..]=flags
   double* resid;    // [hist_cap][ncases][5] residual history (ring buffer)
+  double* rpart;    // [nrblk][5] per-chunk L1 residual partials (chunks never straddle cases)
   int hist_cap;
   int* err;         // error flags
   int* case_err;    // [ncases] per-case error flags (1: rho/p <= 0, 4: NaN residual)
@@ -113,7 +114,12 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
 void launch_resid(const Mesh& m, State& st, int hist_index_from_ctrl, cudaStream_t s);
 // per-case residual history, resid[(idx*ncases + case)*5 + i]
-void launch_resid_cases(State& st, const int* case_off, int ncases, int hist_from_ctrl, cudaStream_t s);
+// per-case L1 residual: RCHUNK-cell chunks counted from each case's first cell
+// (rblk_off[k]..rblk_off[k+1] are case k's chunks, rblk_case maps a chunk to
+// its case), then one warp per case sums its chunks in order
+constexpr int RCHUNK = 256;
+void launch_resid_cases(State& st, const int* case_off, const int* rblk_off, const int* rblk_case, int nrblk,
+                        int ncases, int hist_from_ctrl, cudaStream_t s);
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
 // multicolour Gauss-Seidel: result in st.x0
 void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s);
@@ -136,4 +142,16 @@ void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s);
 int grid_for(long n, int block);
 int record_error(int code, const char* msg);  // sets the jg_last_error message
 
+}  // namespace jg
+
+// per-case operations used by the serving engine (defined in jg_api.cu)
+struct jg_case;
+namespace jg {
+int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** out);
+int serve_case_start(jg_case* h, const double* rho, const double* rhou, const double* rhoE);
+int serve_case_launch(jg_case* h, int nsteps, double* h_ring, int* h_err, cudaEvent_t ev);
+int serve_case_ring(jg_case* h);
+size_t serve_case_bytes(jg_case* h);
+int serve_case_ncv(jg_case* h);
+int serve_set_err(int code, const char* msg);
 }  // namespace jg

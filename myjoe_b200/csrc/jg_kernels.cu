@@ -812,29 +812,45 @@ __global__ void k_resid_final(State st, int nblk, int hist_from_ctrl) {
 // Per-case L1 residual: block k sums |RHS| over the cells of case k in a fixed
 // order that depends only on that case, so a case's residual history is the
 // same alone and inside a batch.  out[(idx*ncases + k)*5 + i].
-__global__ void k_resid_cases(State st, const int* case_off, int ncases, int hist_from_ctrl) {
-  __shared__ double s[5][256];
-  int k = blockIdx.x, t = threadIdx.x;
-  double v[5] = {0, 0, 0, 0, 0};
-  for (int c = case_off[k] + t; c < case_off[k + 1]; c += blockDim.x)
-    for (int i = 0; i < 5; i++) v[i] += fabs(st.rhs[5 * c + i]);
-  for (int i = 0; i < 5; i++) s[i][t] = v[i];
+__global__ void __launch_bounds__(320) k_resid_chunks(State st, const int* __restrict__ case_off,
+                                                       const int* __restrict__ rblk_off,
+                                                       const int* __restrict__ rblk_case) {
+  __shared__ double s[320];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int k = rblk_case[b];
+  const long c0 = case_off[k] + (long)(b - rblk_off[k]) * RCHUNK;
+  const long c1 = min((long)case_off[k + 1], c0 + RCHUNK);
+  const double* r = st.rhs + 5 * c0;
+  const long n = 5 * (c1 - c0);
+  double v = 0.0;  // stride 320 = 64 x 5: thread t always sums component t % 5
+  for (long e = t; e < n; e += 320) v += fabs(r[e]);
+  s[t] = v;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (t < w)
-      for (int i = 0; i < 5; i++) s[i][t] += s[i][t + w];
+  for (int w = 32; w > 0; w >>= 1) {  // fixed-order tree over the 64 threads of each component
+    if (t / 5 < w) s[t] += s[t + 5 * w];
     __syncthreads();
   }
-  if (t == 0) {
+  if (t < 5) st.rpart[5 * b + t] = s[t];
+}
+__global__ void k_resid_cases(State st, const int* __restrict__ rblk_off, int ncases, int hist_from_ctrl) {
+  const int k = blockIdx.x, lane = threadIdx.x;
+  double v[5] = {0, 0, 0, 0, 0};
+  for (int b = rblk_off[k] + lane; b < rblk_off[k + 1]; b += 32)
+    for (int i = 0; i < 5; i++) v[i] += st.rpart[5 * b + i];
+  for (int o = 16; o > 0; o >>= 1)
+    for (int i = 0; i < 5; i++) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+  if (lane == 0) {
     long idx = hist_from_ctrl ? (long)st.ctrl[1] - (long)st.ctrl[4] - 1 : 0;
     idx = ((idx % st.hist_cap) + st.hist_cap) % st.hist_cap;  // ring buffer
-    for (int i = 0; i < 5; i++) st.resid[(idx * ncases + k) * 5 + i] = s[i][0];
-    if (!(s[4][0] == s[4][0]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN residual (doneSolver)
+    for (int i = 0; i < 5; i++) st.resid[(idx * ncases + k) * 5 + i] = v[i];
+    if (!(v[4] == v[4]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN residual (doneSolver)
   }
 }
 
-void launch_resid_cases(State& st, const int* case_off, int ncases, int hist_from_ctrl, cudaStream_t s) {
-  k_resid_cases<<<ncases, 256, 0, s>>>(st, case_off, ncases, hist_from_ctrl);
+void launch_resid_cases(State& st, const int* case_off, const int* rblk_off, const int* rblk_case, int nrblk,
+                        int ncases, int hist_from_ctrl, cudaStream_t s) {
+  k_resid_chunks<<<nrblk, 320, 0, s>>>(st, case_off, rblk_off, rblk_case);
+  k_resid_cases<<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
 }
 
 // ---------------------------------------------------------------------------

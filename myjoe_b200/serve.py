@@ -1,0 +1,173 @@
+"""Serving form: a Poisson stream of seed-generated cases through the request loop.
+
+    python -m myjoe_b200.serve --rate 20 --horizon 600 --min-cells 5000 --max-cells 500000
+                               [--arms serve,plain] [--max-resident 48]
+
+Requests arrive as a Poisson process (``--rate`` per second for
+``--horizon`` seconds).  Each request is an external flow over a channel bump
+with cells log-uniform on [min, max] (hex, two cell layers in z), inflow Mach
+uniform on 0.3-0.8, angle of attack uniform on +-4 degrees and bump height
+uniform on 0.05-0.12 (the batching form's parameters), inviscid HLLC, far-field
+inlet/outlet/top.  Meshes are built by a spawn pool of client processes in
+arrival order and submitted when they have arrived; a case retires at a 1e-8
+drop of its energy residual.
+
+Two arms see the same arrival stream:
+
+* ``serve``: the serving form -- mixed precision (FP32 Jacobian and
+  relaxation inside FP64 defect correction), up to ``--max-resident`` cases on
+  the device at once, admitted by device-memory footprint (jg_serve_*);
+* ``plain``: the plain FP64 GPU path, one case at a time in arrival order
+  (the same server with one resident case and FP64 throughout).
+
+Both use the same relaxation (SGS sweeps), CFL ramp, step limit and restart
+policy.  One JSON line per arm: converged solves/hour over the horizon,
+p50/p99 time-to-converge (arrival to retirement) and service time (admission
+to retirement), cell-iterations/s, failures and restarts.
+"""
+from __future__ import annotations
+
+import argparse
+import collections
+import dataclasses
+import json
+import math
+import multiprocessing as mp
+import time
+
+import numpy as np
+
+
+def request_stream(rate, horizon, lo, hi, seed):
+    """Arrival times and case specs of the Poisson stream (seeded)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= horizon:
+            break
+        cells = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        ny = max(4, int(round(math.sqrt(cells / 4.0))))
+        out.append(dict(t=t, nx=2 * ny, ny=ny, nz=2, mach=float(rng.uniform(0.3, 0.8)),
+                        aoa=float(rng.uniform(-4.0, 4.0)), bump=float(rng.uniform(0.05, 0.12)),
+                        seed=len(out)))
+    return out
+
+
+def build_request(spec):
+    from myjoe_b200 import case
+    _, g, prm = case.bump_case(spec["nx"], spec["ny"], spec["nz"], mach=spec["mach"], aoa_deg=spec["aoa"],
+                               bump_h=spec["bump"], seed=spec["seed"], inlet="FARFIELD")
+    state = case.perturbed_state(g.x_cv, prm, 0.0)
+    return g, prm, state
+
+
+def solver_params(prm, args):
+    ra, ri, rf, rm = args.cfl_ramp.split(",")
+    return dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=args.sweeps, CFL=1.0,
+                               CFL_RAMP=(int(ra), int(ri), float(rf), float(rm)))
+
+
+def pct(a, q):
+    return float(np.percentile(a, q)) if len(a) else None
+
+
+def run_arm(arm, stream, args):
+    from myjoe_b200 import solver
+    precision = 1 if arm == "serve" else 0
+    resident = args.max_resident if arm == "serve" else 1
+    srv = solver.JoeServer(max_resident=resident, hbm_budget=args.hbm_budget * 1e9, steps_per_poll=args.chunk,
+                           resid_drop=args.drop, max_steps=args.max_steps, max_restarts=args.max_restarts,
+                           restart_cfl_factor=args.restart_factor)
+    pool = mp.get_context("spawn").Pool(args.workers)
+    pending = collections.deque()   # mesh builds in flight, in arrival order (bounded lookahead)
+    queued = 0                      # next request handed to the pool
+
+    def top_up():
+        nonlocal queued
+        while queued < len(stream) and len(pending) < args.lookahead:
+            pending.append(pool.apply_async(build_request, (stream[queued],)))
+            queued += 1
+
+    top_up()
+    t0 = srv.now()
+    nxt = 0                 # next request to submit
+    results = []
+    horizon = args.horizon
+    while True:
+        now = srv.now() - t0
+        if now >= horizon:
+            break
+        st = srv.stats()
+        # keep a short server-side queue; the rest wait on the client side
+        while nxt < len(stream) and stream[nxt]["t"] <= now and st["queued"] < args.queue:
+            if not pending[0].ready():
+                break       # the client is still building this mesh: keep the device busy meanwhile
+            g, prm, state = pending.popleft().get()
+            top_up()
+            srv.submit(g, solver_params(prm, args), state, precision=precision, t_arrival=t0 + stream[nxt]["t"])
+            nxt += 1
+            st["queued"] += 1
+        for r in srv.poll(max_wait=0.02):
+            srv.fetch(r["id"])
+            if r["t_done"] - t0 <= horizon:
+                results.append(r)
+    arrived = sum(1 for s in stream if s["t"] < horizon)
+    srv.close()
+    pool.terminate()
+    conv = [r for r in results if r["status"] == 0]
+    ttc = [r["t_done"] - r["t_arrival"] for r in conv]
+    svc = [r["t_done"] - r["t_admit"] for r in conv]
+    cell_iters = sum(r["ncv"] * r["steps_total"] for r in results)
+    return {
+        "form": "serve", "arm": arm, "precision": "mixed" if precision else "fp64", "max_resident": resident,
+        "rate_per_s": args.rate, "horizon_s": horizon, "arrived": arrived, "submitted": nxt,
+        "retired": len(results), "converged": len(conv),
+        "failed": sum(1 for r in results if r["status"] == 2),
+        "max_steps_hit": sum(1 for r in results if r["status"] == 1),
+        "restarts": sum(r["restarts"] for r in results),
+        "converged_solves_per_hour": len(conv) / horizon * 3600.0,
+        "time_to_converge_p50_s": pct(ttc, 50), "time_to_converge_p99_s": pct(ttc, 99),
+        "service_time_p50_s": pct(svc, 50), "service_time_p99_s": pct(svc, 99),
+        "steps_to_converge_p50": pct([r["conv_step"] for r in conv], 50),
+        "cell_iters_per_s": cell_iters / horizon,
+        "drop": args.drop, "solver": "SGS x%d" % args.sweeps, "cfl_ramp": args.cfl_ramp,
+        "cells": [args.min_cells, args.max_cells],
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--horizon", type=float, default=600.0)
+    ap.add_argument("--min-cells", type=int, default=5000)
+    ap.add_argument("--max-cells", type=int, default=500000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--arms", default="serve,plain")
+    ap.add_argument("--max-resident", type=int, default=48)
+    ap.add_argument("--hbm-budget", type=float, default=0.0, help="GB; 0: 90%% of free device memory")
+    ap.add_argument("--queue", type=int, default=8, help="server-side queue length")
+    ap.add_argument("--chunk", type=int, default=25)
+    ap.add_argument("--sweeps", type=int, default=10)
+    ap.add_argument("--cfl-ramp", default="10,5,1.2,20")
+    ap.add_argument("--drop", type=float, default=1e-8)
+    ap.add_argument("--max-steps", type=int, default=6000)
+    ap.add_argument("--max-restarts", type=int, default=2)
+    ap.add_argument("--restart-factor", type=float, default=0.25)
+    ap.add_argument("--workers", type=int, default=min(32, mp.cpu_count()))
+    ap.add_argument("--lookahead", type=int, default=48, help="mesh builds in flight")
+    args = ap.parse_args(argv)
+
+    from myjoe_b200 import build
+    if build.needs_build():
+        build.build()
+    stream = request_stream(args.rate, args.horizon, args.min_cells, args.max_cells, args.seed)
+    for arm in args.arms.split(","):
+        t = time.perf_counter()
+        out = run_arm(arm, stream, args)
+        out["wall_s"] = time.perf_counter() - t
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

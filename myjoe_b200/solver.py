@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-from .abi import MeshArrays, dptr, jg_mesh, jg_params, make_params
+from .abi import MeshArrays, dptr, jg_mesh, jg_params, jg_serve_config, jg_serve_result, make_params
 from .case import JoeParams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -69,6 +69,16 @@ def lib():
         L.jg_set_profiling.argtypes = [P, I]
         L.jg_get_profile.argtypes = [P, D]
         L.jg_step_kernel_count.argtypes = [P, C.POINTER(I)]
+        L.jg_case_footprint.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), D]
+        L.jg_case_device_bytes.argtypes = [P, D]
+        L.jg_serve_create.argtypes = [C.POINTER(jg_serve_config), C.POINTER(P)]
+        L.jg_serve_now.argtypes = [P, D]
+        L.jg_serve_submit.argtypes = [P, C.POINTER(jg_mesh), C.POINTER(jg_params), D, D, D, C.c_double,
+                                      C.POINTER(C.c_longlong)]
+        L.jg_serve_poll.argtypes = [P, C.c_double, C.POINTER(jg_serve_result), I, C.POINTER(I)]
+        L.jg_serve_fetch.argtypes = [P, C.c_longlong, D, D, D]
+        L.jg_serve_stats.argtypes = [P, C.POINTER(I), C.POINTER(I), C.POINTER(I), D]
+        L.jg_serve_destroy.argtypes = [P]
         _lib = L
     return _lib
 
@@ -195,6 +205,11 @@ class JoeGpu:
         _ck(lib().jg_step_kernel_count(self.h, C.byref(n)))
         return n.value
 
+    def device_bytes(self) -> float:
+        b = C.c_double()
+        _ck(lib().jg_case_device_bytes(self.h, C.byref(b)))
+        return b.value
+
     def cfl_step(self):
         cfl = C.c_double(0.0)
         step = C.c_int(0)
@@ -253,3 +268,73 @@ class JoeGpuBatch(JoeGpu):
         r = np.zeros((max(nsteps, 1), self.ncases, 5))
         _ck(lib().jg_batch_step(self.h, int(nsteps), dptr(r)))
         return r[:nsteps]
+
+
+SERVE_STATUS = {0: "converged", 1: "max_steps", 2: "failed"}
+
+
+class JoeServer:
+    """Serving form over the C ABI (jg_serve_*): cases are submitted with their
+    mesh, parameters and initial state, admitted by device-memory footprint,
+    stepped concurrently (one stream and captured step per case) and retired
+    at the residual drop.  ``poll`` runs the progress engine and returns the
+    retired cases as dicts; ``fetch`` returns a retired case's final state."""
+
+    def __init__(self, max_resident=32, hbm_budget=0.0, steps_per_poll=20, resid_drop=1e-8, max_steps=20000,
+                 max_restarts=2, restart_cfl_factor=0.25, device=0):
+        cfg = jg_serve_config(device=device, max_resident=max_resident, hbm_budget=float(hbm_budget),
+                              steps_per_poll=steps_per_poll, resid_drop=resid_drop, max_steps=max_steps,
+                              max_restarts=max_restarts, restart_cfl_factor=restart_cfl_factor)
+        h = C.c_void_p()
+        _ck(lib().jg_serve_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.sizes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().jg_serve_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def now(self) -> float:
+        t = C.c_double()
+        _ck(lib().jg_serve_now(self.h, C.byref(t)))
+        return t.value
+
+    def submit(self, mesh_src, params: JoeParams, state, precision: int = 0, t_arrival: float = -1.0) -> int:
+        ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
+        jp = make_params(params, precision)
+        rho, rhou, rhoE = (np.ascontiguousarray(a, np.float64) for a in state)
+        i = C.c_longlong()
+        _ck(lib().jg_serve_submit(self.h, C.byref(ma.mesh), C.byref(jp), dptr(rho), dptr(rhou), dptr(rhoE),
+                                  float(t_arrival), C.byref(i)))
+        self.sizes[i.value] = ma.ncv
+        return i.value
+
+    def poll(self, max_wait=0.05, cap=64):
+        out = (jg_serve_result * cap)()
+        n = C.c_int()
+        _ck(lib().jg_serve_poll(self.h, float(max_wait), out, cap, C.byref(n)))
+        return [{f: getattr(out[k], f) for f, _ in jg_serve_result._fields_} for k in range(n.value)]
+
+    def fetch(self, rid):
+        n = self.sizes.pop(rid)
+        rho, rhou, rhoE = np.empty(n), np.empty((n, 3)), np.empty(n)
+        _ck(lib().jg_serve_fetch(self.h, C.c_longlong(rid), dptr(rho), dptr(rhou), dptr(rhoE)))
+        return rho, rhou, rhoE
+
+    def stats(self):
+        r, q, f = C.c_int(), C.c_int(), C.c_int()
+        b = C.c_double()
+        _ck(lib().jg_serve_stats(self.h, C.byref(r), C.byref(q), C.byref(f), C.byref(b)))
+        return {"resident": r.value, "queued": q.value, "unfetched": f.value, "bytes_resident": b.value}
+
+
+def case_footprint(mesh_src, params: JoeParams, precision: int = 0) -> float:
+    """Device bytes jg_create + jg_set_state allocate for this case."""
+    ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
+    jp = make_params(params, precision)
+    b = C.c_double()
+    _ck(lib().jg_case_footprint(C.byref(ma.mesh), C.byref(jp), C.byref(b)))
+    return b.value

@@ -56,8 +56,10 @@ enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
 typedef struct jg_zone {
   int ifa_f, ifa_l;   /* inclusive boundary-face range */
   int kind;           /* JG_BC_* */
-  int pad;
-  double v[8];        /* parameters, see JG_BC_* */
+  int scal_bc;        /* bit s set: transported scalar s is Dirichlet here with value v[6+s]
+                         (Joe.in key "<zone>.<scalar> = value", Scalars.cpp:289-360);
+                         bit clear: zero-flux (phi_bfa = phi of the cell) */
+  double v[8];        /* parameters, see JG_BC_* (v[6], v[7]: scalar Dirichlet values) */
 } jg_zone;
 
 typedef struct jg_mesh {
@@ -93,8 +95,13 @@ typedef struct jg_params {
   int ls_max_iter;     /* LINEAR_SOLVER_NS_TRESHOLDS MAX_ITER (BCGSTAB) or sweeps (JACOBI/SGS) */
   double ls_abs, ls_rel;
   int precision;       /* JG_PREC_* */
-  int nscal;           /* transported scalars (0: laminar / inviscid) */
+  int nscal;           /* transported scalars: 0 (laminar / inviscid), 1 with JG_TURB_SA */
+  int turb_model;      /* JG_TURB_*: with a model the case runs runBackwardEulerCoupled's
+                          (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
 } jg_params;
+/* turbulence models: JG_TURB_SA = Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h)
+ * with the reference's default constants, scalar nuSA (bounds 1e-10 .. 1) */
+enum { JG_TURB_NONE = 0, JG_TURB_SA = 1 };
 
 
 typedef struct jg_case jg_case_t;   /* opaque per-case handle (device state + stream + graph) */
@@ -198,8 +205,10 @@ int jg_case_device_bytes(jg_case_t *h, double *bytes);
  * cases into the freed memory.  A case that reaches a non-physical state is
  * restarted from its initial state with CFL_RAMP MAX_CFL (and the starting
  * CFL, if above it) multiplied by restart_cfl_factor, up to max_restarts
- * times.  Single-threaded: call every jg_serve_* of one server from one
- * thread. */
+ * times; with stall_steps > 0 a case whose residual has stopped falling is
+ * retired early as stalled.  Admission is in arrival order, or smallest
+ * footprint first among the queued cases (JG_ADMIT_SMALLEST).
+ * Single-threaded: call every jg_serve_* of one server from one thread. */
 typedef struct jg_server jg_server_t;
 typedef struct {
   int device;                /* CUDA device */
@@ -210,8 +219,11 @@ typedef struct {
   int max_steps;             /* retire unconverged after this many steps */
   int max_restarts;          /* restarts after a non-physical state */
   double restart_cfl_factor; /* CFL scaling per restart (0 < f <= 1) */
+  int stall_steps;           /* > 0: retire as stalled when the best residual drop has not halved over this many steps */
+  int admission;             /* JG_ADMIT_FIFO: arrival order; JG_ADMIT_SMALLEST: smallest footprint first */
 } jg_serve_config;
-enum { JG_SERVE_CONVERGED = 0, JG_SERVE_MAX_STEPS = 1, JG_SERVE_FAILED = 2 };
+enum { JG_ADMIT_FIFO = 0, JG_ADMIT_SMALLEST = 1 };
+enum { JG_SERVE_CONVERGED = 0, JG_SERVE_MAX_STEPS = 1, JG_SERVE_FAILED = 2, JG_SERVE_STALLED = 3 };
 typedef struct {
   long long id;
   int status;       /* JG_SERVE_* */

@@ -11,7 +11,7 @@ from .case import BC_KINDS, FLUX_KINDS, SOLVER_KINDS, SYMM_BC_KINDS, JoeParams
 
 
 class jg_zone(C.Structure):
-    _fields_ = [("ifa_f", C.c_int), ("ifa_l", C.c_int), ("kind", C.c_int), ("pad", C.c_int),
+    _fields_ = [("ifa_f", C.c_int), ("ifa_l", C.c_int), ("kind", C.c_int), ("scal_bc", C.c_int),
                 ("v", C.c_double * 8)]
 
 
@@ -42,13 +42,14 @@ class jg_params(C.Structure):
                 ("under_relax", C.c_double),
                 ("lin_solver", C.c_int), ("ls_max_iter", C.c_int),
                 ("ls_abs", C.c_double), ("ls_rel", C.c_double),
-                ("precision", C.c_int), ("nscal", C.c_int)]
+                ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int)]
 
 
 class jg_serve_config(C.Structure):
     _fields_ = [("device", C.c_int), ("max_resident", C.c_int), ("hbm_budget", C.c_double),
                 ("steps_per_poll", C.c_int), ("resid_drop", C.c_double), ("max_steps", C.c_int),
-                ("max_restarts", C.c_int), ("restart_cfl_factor", C.c_double)]
+                ("max_restarts", C.c_int), ("restart_cfl_factor", C.c_double), ("stall_steps", C.c_int),
+                ("admission", C.c_int)]
 
 
 class jg_serve_result(C.Structure):
@@ -97,7 +98,8 @@ def make_params(p: JoeParams, precision: int = 0) -> jg_params:
     q.ls_abs = p.LS_ABS_RESID
     q.ls_rel = p.LS_REL_RESID
     q.precision = precision
-    q.nscal = 0
+    q.nscal = p.nscal
+    q.turb_model = 1 if p.TURB_MODEL == "SA" else 0
     return q
 
 
@@ -129,6 +131,9 @@ class MeshArrays:
             zarr[i].ifa_f, zarr[i].ifa_l = f0, f1
             zarr[i].kind = BC_KINDS[bc.kind]
             vals = list(bc.values) + [0.0] * (8 - len(bc.values))
+            if name in params.scalar_bcs:
+                zarr[i].scal_bc = 1
+                vals[6] = params.scalar_bcs[name]
             for k in range(8):
                 zarr[i].v[k] = vals[k]
         self.zarr = zarr

@@ -71,6 +71,14 @@ class JoeParams:
     P_INITIAL: float = 1.0e5
     RHO_INITIAL: float = 1.0e5 / (287.0 * 300.0)
     bcs: Dict[str, BC] = dataclasses.field(default_factory=dict)
+    TURB_MODEL: str = "NONE"          # "SA": Spalart-Allmaras, coupled 6x6 system
+    NUSA_INITIAL: float = 0.0         # INITIAL_CONDITION_TURB (nuSA)
+    # Dirichlet values of the transported scalar per zone ("<zone>.nuSA = v"); absent: zero flux
+    scalar_bcs: Dict[str, float] = dataclasses.field(default_factory=dict)
+
+    @property
+    def nscal(self) -> int:
+        return 1 if self.TURB_MODEL == "SA" else 0
 
     @property
     def R_gas(self) -> float:
@@ -101,7 +109,7 @@ class JoeParams:
                 self.LS_MAX_ITER, self.LS_ABS_RESID, self.LS_REL_RESID),
             "U_INITIAL = %.17g %.17g %.17g" % tuple(self.U_INITIAL),
             "P_INITIAL = %.17g" % self.P_INITIAL, "RHO_INITIAL = %.17g" % self.RHO_INITIAL,
-            "INITIAL_CONDITION_TURB = 0.0 0.0",
+            "INITIAL_CONDITION_TURB = %.17g 0.0" % self.NUSA_INITIAL,
             "CHECK_INTERVAL = 1",
             "INITIAL_FLOWFIELD_OUTPUT = NO",
         ]
@@ -109,6 +117,8 @@ class JoeParams:
             L.append("SPATIAL_SECOND_ORDER")
         for name, bc in self.bcs.items():
             L.append("%s = %s" % (name, bc.joe_in()))
+        for name, v in self.scalar_bcs.items():
+            L.append("%s.nuSA = %.17g" % (name, v))
         if extra:
             L.append(extra)
         return "\n".join(L) + "\n"
@@ -141,6 +151,14 @@ def perturbed_state(x_cv: np.ndarray, params: JoeParams, amp: float):
     v = np.stack([u[:, 0] + umag * f1, u[:, 1] + umag * f2, u[:, 2] + umag * f3], 1)
     pp = p0 * f4
     return r, r[:, None] * v, pp / (g - 1.0) + 0.5 * r * (v * v).sum(1)
+
+
+def perturbed_scalar(x_cv: np.ndarray, value: float, amp: float) -> np.ndarray:
+    """Uniform transported scalar times the perturbation factor compiled into
+    the reference harness (oracle/ref_harness.cpp ``scal_perturb``)."""
+    x, y, z = x_cv[:, 0], x_cv[:, 1], x_cv[:, 2]
+    f = 1.0 + amp * np.sin(1.3 * x + 0.4) * np.cos(0.7 * y + 0.1) * (1.0 + 0.2 * np.cos(2.3 * z))
+    return value * f
 
 
 # ----------------------------------------------------------------------------
@@ -201,3 +219,35 @@ def plate_case(nx=256, ny=96, nz=2, mach=0.3, re_l=1.0e5, p=1.0e5, T=300.0, flux
                          "lower_sym": BC("SYMMETRY"), "plate": BC("WALL"),
                          "upper": BC("CBC", u + (T, p)), "sides": BC("SYMMETRY")})
     return raw, geometry.build_cv_mesh(raw), prm
+
+
+def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
+                 stretch=1.0, inlet="FARFIELD", nu_factor=3.0):
+    """Turbulent (SA) flow over the channel bump: viscous WALL lower (nuSA = 0),
+    HLLC, Sutherland viscosity with MU_REF set so that the Reynolds number on
+    the bump chord (length 1) is ``re``; inflow nuSA = ``nu_factor`` x the
+    kinematic viscosity (the usual SA free-stream value), far-field inlet,
+    outlet and top (or CBC inlet with ``inlet="CBC"``), SYMMETRY z planes.
+    ``stretch`` > 1 clusters the rows towards the lower wall."""
+    gam, R = 1.4, 287.0
+    rho = p / (R * T)
+    c = math.sqrt(gam * R * T)
+    U = mach * c
+    tref, sref = 273.15, 110.4
+    mu = rho * U * 1.0 / re
+    mu_ref = mu / ((T / tref) ** 1.5 * (tref + sref) / (T + sref))
+    nu_inf = nu_factor * mu / rho
+    u = (U, 0.0, 0.0)
+    raw = meshgen.channel_bump(nx, ny, nz, bump_h=bump_h, jitter=jitter, seed=seed, stretch=stretch)
+    bcs = {"lower": BC("WALL"), "sides": BC("SYMMETRY")}
+    if inlet == "CBC":
+        bcs.update(inlet=BC("CBC", u + (T, p)), outlet=BC("CBC_SUBSONIC_OUTLET", (p,)), upper=BC("SYMMETRY"))
+        sbc = {"inlet": nu_inf, "lower": 0.0}
+    else:
+        ff = BC("FARFIELD", u + (p, rho, gam))
+        bcs.update(inlet=ff, outlet=ff, upper=ff)
+        sbc = {"inlet": nu_inf, "outlet": nu_inf, "upper": nu_inf, "lower": 0.0}
+    prm = JoeParams(T_REF=T, P_REF=p, RHO_REF=rho, GAMMA=gam, SPACE_INTEGRATION="HLLC", MU_MODE="SUTHERLAND",
+                    MU_REF=mu_ref, SYMM_BC="ANALYTICAL", U_INITIAL=u, P_INITIAL=p, RHO_INITIAL=rho, bcs=bcs,
+                    TURB_MODEL="SA", NUSA_INITIAL=nu_inf, scalar_bcs=sbc)
+    return raw, geometry.build_cv_mesh(raw, seed=seed), prm

@@ -106,6 +106,9 @@ struct Request {
   double r0 = 0.0;    // first-step energy residual of the current attempt
   int conv_step = -1;
   double drop = NAN;
+  double best = INFINITY;         // smallest drop of the current attempt
+  double window_best = INFINITY;  // ... at the last stall check
+  int next_check = 0;             // step of the next stall check
   int flags = 0;
   size_t bytes = 0;
 };
@@ -122,7 +125,7 @@ struct Finished {
   std::vector<double> rho, rhou, rhoE;
 };
 
-enum Outcome { RUNNING, CONVERGED, MAX_STEPS, FAILED };
+enum Outcome { RUNNING, CONVERGED, MAX_STEPS, FAILED, STALLED };
 
 }  // namespace
 
@@ -176,6 +179,8 @@ static int start_case(jg_server* s, Request* r) {
   r->r0 = 0.0;
   r->conv_step = -1;
   r->drop = NAN;
+  r->best = r->window_best = INFINITY;
+  r->next_check = s->cfg.stall_steps;
   r->flags = 0;
   SRC(jg::serve_case_start(r->h, r->rho.data(), r->rhou.data(), r->rhoE.data()));
   return JG_OK;
@@ -203,6 +208,7 @@ static Outcome check_batch(jg_server* s, Request* r) {
     if (step == 1) r->r0 = e;
     const double drop = r->r0 > 0.0 ? e / r->r0 : 0.0;
     r->drop = drop;
+    r->best = std::min(r->best, drop);
     if (r->conv_step < 0 && drop <= s->cfg.resid_drop) r->conv_step = step;
   }
   r->steps += r->launched;
@@ -212,6 +218,11 @@ static Outcome check_batch(jg_server* s, Request* r) {
   if (flags) return FAILED;
   if (r->conv_step > 0) return CONVERGED;
   if (r->steps >= s->cfg.max_steps) return MAX_STEPS;
+  if (s->cfg.stall_steps > 0 && r->steps >= r->next_check) {
+    if (!(r->best <= 0.5 * r->window_best)) return STALLED;
+    r->window_best = r->best;
+    r->next_check += s->cfg.stall_steps;
+  }
   return RUNNING;
 }
 
@@ -248,7 +259,8 @@ int jg_serve_create(const jg_serve_config* cfg, jg_server_t** out) {
   *out = nullptr;
   if (cfg->max_resident < 1 || cfg->steps_per_poll < 1 || cfg->steps_per_poll > 64 || cfg->max_steps < 1 ||
       !(cfg->resid_drop > 0.0) || cfg->max_restarts < 0 ||
-      !(cfg->restart_cfl_factor > 0.0 && cfg->restart_cfl_factor <= 1.0))
+      !(cfg->restart_cfl_factor > 0.0 && cfg->restart_cfl_factor <= 1.0) || cfg->stall_steps < 0 ||
+      (cfg->admission != JG_ADMIT_FIFO && cfg->admission != JG_ADMIT_SMALLEST))
     return fail(JG_ERR_ARG, "bad serve config (max_resident >= 1, steps_per_poll 1..64, resid_drop > 0, "
                             "0 < restart_cfl_factor <= 1)");
   int ndev = 0;
@@ -335,8 +347,11 @@ int jg_serve_poll(jg_server_t* s, double max_wait_s, jg_serve_result* out, int c
           continue;
         }
         if (oc != RUNNING) {
-          SRC(finish(s, r, oc == CONVERGED ? JG_SERVE_CONVERGED : oc == MAX_STEPS ? JG_SERVE_MAX_STEPS
-                                                                                  : JG_SERVE_FAILED));
+          const int status = oc == CONVERGED ? JG_SERVE_CONVERGED
+                             : oc == MAX_STEPS ? JG_SERVE_MAX_STEPS
+                             : oc == STALLED ? JG_SERVE_STALLED
+                                             : JG_SERVE_FAILED;
+          SRC(finish(s, r, status));
           s->resident.erase(s->resident.begin() + i);
           continue;
         }
@@ -346,15 +361,19 @@ int jg_serve_poll(jg_server_t* s, double max_wait_s, jg_serve_result* out, int c
     }
     // admissions, in arrival order, into the memory and slots that are free
     while (!s->queue.empty() && (int)s->resident.size() < s->cfg.max_resident) {
-      Request* r = s->queue.front().get();
+      size_t pick = 0;
+      if (s->cfg.admission == JG_ADMIT_SMALLEST)
+        for (size_t k = 1; k < s->queue.size(); k++)
+          if (s->queue[k]->footprint < s->queue[pick]->footprint) pick = k;
+      Request* r = s->queue[pick].get();
       if (!s->resident.empty() && s->bytes_resident + r->footprint > s->budget) break;
-      std::unique_ptr<Request> own = std::move(s->queue.front());
-      s->queue.pop_front();
+      std::unique_ptr<Request> own = std::move(s->queue[pick]);
+      s->queue.erase(s->queue.begin() + pick);
       int rc = start_case(s, r);
       if (rc == JG_ERR_NOMEM && !s->resident.empty()) {
         // the pool is fuller than the estimate says: wait for a retirement
         release_case(s, r);
-        s->queue.push_front(std::move(own));
+        s->queue.insert(s->queue.begin() + pick, std::move(own));
         break;
       }
       if (rc != JG_OK) {

@@ -124,18 +124,23 @@ def structured_hex(X: np.ndarray, Y: np.ndarray, z: np.ndarray,
 
 
 def channel_bump(nx=64, ny=32, nz=4, length=3.0, height=1.0, bump_h=0.1,
-                 bump_x0=1.0, bump_x1=2.0, depth=None, jitter=0.0, seed=0) -> RawMesh:
+                 bump_x0=1.0, bump_x1=2.0, depth=None, jitter=0.0, seed=0, stretch=1.0) -> RawMesh:
     """Channel of length ``length`` and height ``height`` with the lower-wall
     bump y_b(x) = bump_h * sin^2(pi (x - x0) / (x1 - x0)) on [x0, x1].
 
     Zones: ``inlet`` (x=0), ``outlet`` (x=L), ``lower`` (bump wall),
     ``upper`` (top), ``sides`` (the two z planes).  ``jitter`` (fraction of
     the local spacing, seeded) moves interior nodes in x/y to make the mesh
-    non-orthogonal.
+    non-orthogonal.  ``stretch`` > 1 grows the row heights geometrically away
+    from the lower wall by that ratio.
     """
     rng = np.random.default_rng(seed)
     xs = np.linspace(0.0, length, nx + 1)
-    eta = np.linspace(0.0, 1.0, ny + 1)
+    if stretch != 1.0:
+        h = stretch ** np.arange(ny)
+        eta = np.concatenate([[0.0], np.cumsum(h)]) / h.sum()
+    else:
+        eta = np.linspace(0.0, 1.0, ny + 1)
     yb = np.where((xs >= bump_x0) & (xs <= bump_x1),
                   bump_h * np.sin(math.pi * (xs - bump_x0) / (bump_x1 - bump_x0)) ** 2, 0.0)
     X = np.repeat(xs[:, None], ny + 1, 1)

@@ -17,11 +17,12 @@ Two arms see the same arrival stream:
 * ``serve``: the serving form -- mixed precision (FP32 Jacobian and
   relaxation inside FP64 defect correction), up to ``--max-resident`` cases on
   the device at once, admitted by device-memory footprint (jg_serve_*);
+* ``serve-smallest``: the same, admitting the smallest queued footprint first;
 * ``plain``: the plain FP64 GPU path, one case at a time in arrival order
   (the same server with one resident case and FP64 throughout).
 
-Both use the same relaxation (SGS sweeps), CFL ramp, step limit and restart
-policy.  One JSON line per arm: converged solves/hour over the horizon,
+All arms use the same relaxation (SGS sweeps), CFL ramp, step limit, stall
+rule and restart policy.  One JSON line per arm: converged solves/hour over the horizon,
 p50/p99 time-to-converge (arrival to retirement) and service time (admission
 to retirement), cell-iterations/s, failures and restarts.
 """
@@ -74,11 +75,14 @@ def pct(a, q):
 
 def run_arm(arm, stream, args):
     from myjoe_b200 import solver
-    precision = 1 if arm == "serve" else 0
-    resident = args.max_resident if arm == "serve" else 1
+    serving = arm.startswith("serve")
+    precision = 1 if serving else 0
+    resident = args.max_resident if serving else 1
+    admission = "smallest" if arm == "serve-smallest" else "fifo"
     srv = solver.JoeServer(max_resident=resident, hbm_budget=args.hbm_budget * 1e9, steps_per_poll=args.chunk,
                            resid_drop=args.drop, max_steps=args.max_steps, max_restarts=args.max_restarts,
-                           restart_cfl_factor=args.restart_factor)
+                           restart_cfl_factor=args.restart_factor, stall_steps=args.stall_steps,
+                           admission=admission)
     pool = mp.get_context("spawn").Pool(args.workers)
     pending = collections.deque()   # mesh builds in flight, in arrival order (bounded lookahead)
     queued = 0                      # next request handed to the pool
@@ -121,10 +125,14 @@ def run_arm(arm, stream, args):
     cell_iters = sum(r["ncv"] * r["steps_total"] for r in results)
     return {
         "form": "serve", "arm": arm, "precision": "mixed" if precision else "fp64", "max_resident": resident,
+        "arrived_cells_p50": pct([s["nx"] * s["ny"] * s["nz"] for s in stream if s["t"] < horizon], 50),
         "rate_per_s": args.rate, "horizon_s": horizon, "arrived": arrived, "submitted": nxt,
         "retired": len(results), "converged": len(conv),
         "failed": sum(1 for r in results if r["status"] == 2),
         "max_steps_hit": sum(1 for r in results if r["status"] == 1),
+        "stalled": sum(1 for r in results if r["status"] == 3),
+        "admission": admission, "stall_steps": args.stall_steps,
+        "converged_cells_p50": pct([r["ncv"] for r in conv], 50),
         "restarts": sum(r["restarts"] for r in results),
         "converged_solves_per_hour": len(conv) / horizon * 3600.0,
         "time_to_converge_p50_s": pct(ttc, 50), "time_to_converge_p99_s": pct(ttc, 99),
@@ -143,7 +151,7 @@ def main(argv=None):
     ap.add_argument("--min-cells", type=int, default=5000)
     ap.add_argument("--max-cells", type=int, default=500000)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--arms", default="serve,plain")
+    ap.add_argument("--arms", default="serve,plain", help="any of serve, serve-smallest, plain")
     ap.add_argument("--max-resident", type=int, default=48)
     ap.add_argument("--hbm-budget", type=float, default=0.0, help="GB; 0: 90%% of free device memory")
     ap.add_argument("--queue", type=int, default=8, help="server-side queue length")
@@ -154,6 +162,8 @@ def main(argv=None):
     ap.add_argument("--max-steps", type=int, default=6000)
     ap.add_argument("--max-restarts", type=int, default=2)
     ap.add_argument("--restart-factor", type=float, default=0.25)
+    ap.add_argument("--stall-steps", type=int, default=1000,
+                    help="retire a case whose best residual drop has not halved in this many steps (0: off)")
     ap.add_argument("--workers", type=int, default=min(32, mp.cpu_count()))
     ap.add_argument("--lookahead", type=int, default=48, help="mesh builds in flight")
     args = ap.parse_args(argv)

@@ -270,7 +270,7 @@ class JoeGpuBatch(JoeGpu):
         return r[:nsteps]
 
 
-SERVE_STATUS = {0: "converged", 1: "max_steps", 2: "failed"}
+SERVE_STATUS = {0: "converged", 1: "max_steps", 2: "failed", 3: "stalled"}
 
 
 class JoeServer:
@@ -281,10 +281,11 @@ class JoeServer:
     retired cases as dicts; ``fetch`` returns a retired case's final state."""
 
     def __init__(self, max_resident=32, hbm_budget=0.0, steps_per_poll=20, resid_drop=1e-8, max_steps=20000,
-                 max_restarts=2, restart_cfl_factor=0.25, device=0):
+                 max_restarts=2, restart_cfl_factor=0.25, stall_steps=0, admission="fifo", device=0):
         cfg = jg_serve_config(device=device, max_resident=max_resident, hbm_budget=float(hbm_budget),
                               steps_per_poll=steps_per_poll, resid_drop=resid_drop, max_steps=max_steps,
-                              max_restarts=max_restarts, restart_cfl_factor=restart_cfl_factor)
+                              max_restarts=max_restarts, restart_cfl_factor=restart_cfl_factor,
+                              stall_steps=stall_steps, admission={"fifo": 0, "smallest": 1}[admission])
         h = C.c_void_p()
         _ck(lib().jg_serve_create(C.byref(cfg), C.byref(h)))
         self.h = h

@@ -1554,3 +1554,852 @@ int jo_step(jo_case *h, int nsteps, double *resid) {
   free(A); free(dq); free(rhs); free(rr); free(ru); free(rE);
   return err;
 }
+
+/* ======================================================================== */
+/* Coupled path with the Spalart-Allmaras model (nScal = 1):                 */
+/* runBackwardEulerCoupled / calcRhsCoupled / calcFluxCoupled,               */
+/* JoeWithModels.cpp:4326-5826; TurbModel_SA.h; UgpWithCvCompFlow.cpp        */
+/* 1808-2292, 3040-3276; Scalars.cpp:289-360; UgpWithCvCompFlow.h:1305-1552. */
+/* Row/column 5 of every block is the scalar rho*nuSA.                       */
+/* ======================================================================== */
+#define SA_CV1_3 357.911
+#define SA_CW1 3.239067817
+#define SA_CW2 0.3
+#define SA_CW3_6 64.0
+#define SA_SIGMA 0.6666666
+#define SA_CB1 0.1355
+#define SA_CB2 0.622
+#define SA_K2 0.1681
+#define SA_LOWER 1.0e-10
+#define SA_UPPER 1.0
+#define NB 6 /* block size of the coupled SA system */
+
+typedef struct {
+  double *phi, *phi_bfa, *grad_phi, *diff, *wallDist, *strMag, *vortMag;
+} jo_sa;
+
+static jo_sa *sa_of(jo_case *h);
+
+/* the SA arrays live beside the case; allocated on first use */
+static jo_sa g_sa_none;
+typedef struct sa_node { jo_case *h; jo_sa sa; struct sa_node *next; } sa_node;
+static sa_node *g_sa_list = NULL;
+
+static jo_sa *sa_of(jo_case *h) {
+  for (sa_node *n = g_sa_list; n; n = n->next)
+    if (n->h == h) return &n->sa;
+  sa_node *n = (sa_node *)calloc(1, sizeof(sa_node));
+  n->h = h;
+  int c = h->ncv, nb = h->nfa_b, nf = h->nfa;
+  n->sa.phi = dalloc(c); n->sa.phi_bfa = dalloc(nb); n->sa.grad_phi = dalloc(3 * c); n->sa.diff = dalloc(nf);
+  n->sa.wallDist = dalloc(c); n->sa.strMag = dalloc(c); n->sa.vortMag = dalloc(c);
+  n->next = g_sa_list;
+  g_sa_list = n;
+  return &n->sa;
+}
+
+void jo_sa_release(jo_case *h) {
+  sa_node **pp = &g_sa_list;
+  while (*pp) {
+    if ((*pp)->h == h) {
+      sa_node *n = *pp;
+      *pp = n->next;
+      free(n->sa.phi); free(n->sa.phi_bfa); free(n->sa.grad_phi); free(n->sa.diff);
+      free(n->sa.wallDist); free(n->sa.strMag); free(n->sa.vortMag);
+      free(n);
+      return;
+    }
+    pp = &(*pp)->next;
+  }
+}
+
+void jo_set_scalar(jo_case *h, const double *phi) { memcpy(sa_of(h)->phi, phi, sizeof(double) * h->ncv); }
+void jo_get_scalar(jo_case *h, double *phi) { memcpy(phi, sa_of(h)->phi, sizeof(double) * h->ncv); }
+
+double *jo_sa_array(jo_case *h, const char *name) {
+  jo_sa *s = sa_of(h);
+  if (!strcmp(name, "phi")) return s->phi;
+  if (!strcmp(name, "phi_bfa")) return s->phi_bfa;
+  if (!strcmp(name, "grad_phi")) return s->grad_phi;
+  if (!strcmp(name, "diff")) return s->diff;
+  if (!strcmp(name, "wallDist")) return s->wallDist;
+  if (!strcmp(name, "strMag")) return s->strMag;
+  if (!strcmp(name, "vortMag")) return s->vortMag;
+  return NULL;
+}
+
+/* calcWallDistance, UgpWithCvCompFlow.h:1395-1535: nearest WALL face
+ * centroid, then the normal projection when the cell sits over that face */
+void jo_wall_distance(jo_case *h) {
+  const jg_mesh *m = &h->m;
+  jo_sa *s = sa_of(h);
+  int nw = 0;
+  for (int z = 0; z < m->nzones; z++)
+    if (m->zones[z].kind == JG_BC_WALL) nw += m->zones[z].ifa_l - m->zones[z].ifa_f + 1;
+  int *wf = (int *)malloc(sizeof(int) * (nw ? nw : 1));
+  nw = 0;
+  for (int z = 0; z < m->nzones; z++)
+    if (m->zones[z].kind == JG_BC_WALL)
+      for (int f = m->zones[z].ifa_f; f <= m->zones[z].ifa_l; f++) wf[nw++] = f;
+  for (int c = 0; c < h->ncv; c++) {
+    double minDist = 1.0e20;
+    int save = 0;
+    const double *x = &m->x_cv[3 * c];
+    for (int k = 0; k < nw; k++) {
+      const double *xf = &m->x_fa[3 * wf[k]];
+      double dist = sqrt(pow(x[0] - xf[0], 2.0) + pow(x[1] - xf[1], 2.0) + pow(x[2] - xf[2], 2.0));
+      if (dist < minDist) { save = k; minDist = dist; }
+    }
+    int f = wf[save];
+    double n[3], sh[3];
+    double nmag = norm3(n, &m->fa_normal[3 * f]);
+    for (int i = 0; i < 3; i++) sh[i] = m->x_fa[3 * f + i] - x[i];
+    double sMag2 = dot3(sh, sh);
+    double dNorm2 = dot3(sh, n) * dot3(sh, n);
+    double dTang2 = sMag2 - dNorm2;
+    double specRadius2 = 0.5 * nmag;
+    s->wallDist[c] = (dTang2 > specRadius2) ? minDist : fabs(dot3(sh, n));
+  }
+  free(wf);
+}
+
+/* setScalarBC, Scalars.cpp:289-360 (Dirichlet or zero flux per zone) */
+static void set_scalar_bc(jo_case *h) {
+  const jg_mesh *m = &h->m;
+  jo_sa *s = sa_of(h);
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      int c0 = m->cvofa[2 * f];
+      if (zn->scal_bc & 1)
+        s->phi_bfa[f] = (dot3(&h->vel_bfa[3 * f], &m->fa_normal[3 * f]) > 1.0e-8) ? s->phi[c0] : zn->v[6];
+      else
+        s->phi_bfa[f] = s->phi[c0];
+    }
+  }
+}
+
+/* InterpolateAtCellCenterFromFaceValues, UgpWithCvCompFlow.h:1538-1552 */
+static double face_avg(jo_case *h, const double *phi, int c) {
+  double v = 0.0;
+  int f0 = h->m.faocv_i[c], f1 = h->m.faocv_i[c + 1] - 1;
+  for (int k = f0; k <= f1; k++) v += phi[h->m.faocv_v[k]];
+  return v / (double)(f1 - f0 + 1);
+}
+
+static int zone_of_face(jo_case *h, int f) {
+  for (int z = 0; z < h->m.nzones; z++)
+    if (f >= h->m.zones[z].ifa_f && f <= h->m.zones[z].ifa_l) return z;
+  return -1;
+}
+
+/* RansTurbSA::calcRansTurbViscMuet, TurbModel_SA.h:74-128 (with calcGradVel,
+ * calcStrainRate, calcVorticity, UgpWithCvCompFlow.h:1305-1393) */
+static void sa_turb_visc(jo_case *h) {
+  const jg_mesh *m = &h->m;
+  jo_sa *s = sa_of(h);
+  grad_vector(h, h->grad_u, h->vel, h->vel_bfa, h->p.limiter, h->sos);
+  for (int c = 0; c < h->ncv; c++) {
+    const double *g = &h->grad_u[9 * c];
+    double sm = 0.0, vm = 0.0;
+    double div = g[0] + g[4] + g[8];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        if (i == j) sm += pow(0.5 * (g[3 * i + j] + g[3 * j + i]) - 1. / 3. * div, 2.0);
+        else sm += pow(0.5 * (g[3 * i + j] + g[3 * j + i]), 2.0);
+      }
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) vm += pow(0.5 * (g[3 * i + j] - g[3 * j + i]), 2.0);
+    s->strMag[c] = sqrt(2.0 * sm);
+    s->vortMag[c] = sqrt(2.0 * vm);
+  }
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double dx0[3], dx1[3];
+    for (int i = 0; i < 3; i++) {
+      dx0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+      dx1[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c1 + i];
+    }
+    double w0 = sqrt(dot3(dx0, dx0)), w1 = sqrt(dot3(dx1, dx1));
+    double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
+    double nu_fa = (w1 * s->phi[c0] + w0 * s->phi[c1]) / (w0 + w1);
+    double muSA = rho_fa * nu_fa;
+    double chi_3 = pow(muSA / h->mul_fa[f], 3.0);
+    double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+    h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+  }
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      if (zn->kind == JG_BC_WALL) { h->mut_fa[f] = 0.0; continue; }
+      int c0 = m->cvofa[2 * f];
+      double muSA = h->rho[c0] * s->phi[c0];
+      double mul0 = face_avg(h, h->mul_fa, c0);
+      double chi_3 = pow(muSA / mul0, 3.0);
+      double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+      h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+    }
+  }
+}
+
+/* state + material + BC (NS and scalar) + turbulent viscosity: the preamble of
+ * runBackwardEulerCoupled, JoeWithModels.cpp:4379-4401 */
+int jo_calc_state_coupled(jo_case *h) {
+  calc_state_variables(h);
+  calc_material_properties(h);
+  int e = set_bc(h);
+  set_scalar_bc(h);
+  sa_turb_visc(h);
+  return e;
+}
+
+/* calcEulerFluxCoupled_HLLC, UgpWithCvCompFlow.cpp:1808-1926 (nScal = 1, k = 0, ConvTerm = 1) */
+typedef struct { double rho, u[3], p, T, h, R, gam, sc; } cstate;
+
+static void flux_hllc_coupled(double F[NB], const cstate *L, const cstate *R, double area, const double *nV,
+                              int only_pressure) {
+  if (only_pressure) {
+    F[0] = 0.0;
+    for (int i = 1; i < 4; i++) F[i] = L->p * nV[i - 1];
+    for (int i = 4; i < NB; i++) F[i] = 0.0;
+  } else {
+    double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+    double rhoeL = (L->h + 0.5 * uLuL + 0.0) * L->rho - L->p;
+    double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+    double rhoeR = (R->h + 0.5 * uRuR + 0.0) * R->rho - R->p;
+    double Rrho = sqrt(R->rho / L->rho);
+    double tmp = 1.0 / (1.0 + Rrho);
+    double velRoe[3];
+    for (int i = 0; i < 3; i++) velRoe[i] = tmp * (L->u[i] + R->u[i] * Rrho);
+    double uRoe = dot3(velRoe, nV);
+    double gamPdivRho = tmp * ((L->gam * L->p / L->rho + 0.5 * (L->gam - 1.0) * uLuL) +
+                               (R->gam * R->p / R->rho + 0.5 * (R->gam - 1.0) * uRuR) * Rrho);
+    double cRoe = sqrt(gamPdivRho - ((L->gam + R->gam) * 0.5 - 1.0) * 0.5 * dot3(velRoe, velRoe));
+    double sL = dmin(uRoe - cRoe, unL - cL);
+    double sR = dmax(uRoe + cRoe, unR + cR);
+    double sM = (L->p - R->p - L->rho * unL * (sL - unL) + R->rho * unR * (sR - unR)) /
+                (R->rho * (sR - unR) - L->rho * (sL - unL));
+    double pStar = R->rho * (unR - sR) * (unR - sM) + R->p;
+    if (sM >= 0.0) {
+      if (sL > 0.0) {
+        F[0] = L->rho * unL;
+        for (int i = 0; i < 3; i++) F[1 + i] = L->rho * L->u[i] * unL + L->p * nV[i];
+        F[4] = (rhoeL + L->p) * unL;
+        F[5] = 1.0 * F[0] * L->sc;
+      } else {
+        double inv = 1.0 / (sL - sM), sLmuL = sL - unL;
+        double rhoS = L->rho * sLmuL * inv, rhouS[3];
+        for (int i = 0; i < 3; i++) rhouS[i] = (L->rho * L->u[i] * sLmuL + (pStar - L->p) * nV[i]) * inv;
+        double rhoeS = (sLmuL * rhoeL - L->p * unL + pStar * sM) * inv;
+        F[0] = rhoS * sM;
+        for (int i = 0; i < 3; i++) F[1 + i] = rhouS[i] * sM + pStar * nV[i];
+        F[4] = (rhoeS + pStar) * sM;
+        F[5] = 1.0 * F[0] * L->sc;
+      }
+    } else {
+      if (sR >= 0.0) {
+        double inv = 1.0 / (sR - sM), sRmuR = sR - unR;
+        double rhoS = R->rho * sRmuR * inv, rhouS[3];
+        for (int i = 0; i < 3; i++) rhouS[i] = (R->rho * R->u[i] * sRmuR + (pStar - R->p) * nV[i]) * inv;
+        double rhoeS = (sRmuR * rhoeR - R->p * unR + pStar * sM) * inv;
+        F[0] = rhoS * sM;
+        for (int i = 0; i < 3; i++) F[1 + i] = rhouS[i] * sM + pStar * nV[i];
+        F[4] = (rhoeS + pStar) * sM;
+        F[5] = 1.0 * F[0] * R->sc;
+      } else {
+        F[0] = R->rho * unR;
+        for (int i = 0; i < 3; i++) F[1 + i] = R->rho * R->u[i] * unR + R->p * nV[i];
+        F[4] = (rhoeR + R->p) * unR;
+        F[5] = 1.0 * F[0] * R->sc;
+      }
+    }
+  }
+  for (int i = 0; i < NB; i++) F[i] *= area;
+}
+
+/* calcJacobianCoupled_HLLC, UgpWithCvCompFlow.cpp:2180-2244 (dp/dscal = 0) */
+static void jac_coupled(double A[NB][NB], const double *vel, double pp, double rrho, double hh, double sc,
+                        const double *nV, double gamma) {
+  double kapm1 = gamma - 1.0;
+  double nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
+  double U_k = nVel[0] + nVel[1] + nVel[2];
+  double vSquHlf = 0.5 * dot3(vel, vel);
+  A[0][0] = 0.0; A[0][1] = nV[0]; A[0][2] = nV[1]; A[0][3] = nV[2]; A[0][4] = 0.0; A[0][5] = 0.0;
+  for (int r = 0; r < 3; r++) {
+    A[1 + r][0] = -vel[r] * U_k + nV[r] * (kapm1 * vSquHlf + gamma * pp / rrho - kapm1 * hh);
+    for (int c = 0; c < 3; c++)
+      A[1 + r][1 + c] = (r == c) ? (2.0 - gamma) * nVel[r] + U_k : vel[r] * nV[c] - kapm1 * vel[c] * nV[r];
+    A[1 + r][4] = kapm1 * nV[r];
+    A[1 + r][5] = 0.0 * nV[r];
+  }
+  A[4][0] = U_k * ((gamma - 2.0) * vSquHlf - gamma * (hh - pp / rrho));
+  for (int c = 0; c < 3; c++) A[4][1 + c] = (hh + vSquHlf) * nV[c] - kapm1 * vel[c] * U_k;
+  A[4][4] = gamma * U_k;
+  A[4][5] = 0.0 * U_k;
+  A[5][0] = 0.0;
+  for (int c = 0; c < 3; c++) A[5][1 + c] = sc * nV[c];
+  A[5][4] = 0.0;
+  A[5][5] = rrho * U_k;
+}
+
+/* calcdSMdU_HLLC, UgpWithCvCompFlow.cpp:2247-2266 */
+static void dsmdu(double d[NB], const double *vel, double pp, double rrho, double hh, const double *nV, double gamma,
+                  double SM, double S, double invertrho, double Factor) {
+  double kapm1 = gamma - 1.0;
+  double U_k = vel[0] * nV[0] + vel[1] * nV[1] + vel[2] * nV[2];
+  double vSquHlf = 0.5 * dot3(vel, vel);
+  d[0] = Factor * invertrho * (-U_k * U_k + kapm1 * vSquHlf + gamma * pp / rrho - kapm1 * hh + SM * S);
+  for (int i = 0; i < 3; i++) d[1 + i] = Factor * invertrho * ((2 * U_k - S - SM) * nV[i] - kapm1 * vel[i]);
+  d[4] = Factor * invertrho * kapm1;
+  d[5] = Factor * invertrho * 0.0;
+}
+
+/* calcSubSonicJacobianCoupled_HLLC, UgpWithCvCompFlow.cpp:2270-2289 */
+static void subsonic_coupled(double A[NB][NB], const double *d, double rhoS, const double *rhouS, double rhoeS,
+                             double sc, double pS, double Omega, double sM, double rhoSmq, const double *nV,
+                             double area) {
+  double OmSM = Omega * sM, OmSMp1 = OmSM + 1.0;
+  for (int i = 0; i < NB; i++) {
+    A[0][i] = -OmSM * A[0][i] + area * OmSMp1 * d[i] * rhoS;
+    A[1][i] = -OmSM * A[1][i] + area * OmSMp1 * d[i] * (rhouS[0] + rhoSmq * nV[0]);
+    A[2][i] = -OmSM * A[2][i] + area * OmSMp1 * d[i] * (rhouS[1] + rhoSmq * nV[1]);
+    A[3][i] = -OmSM * A[3][i] + area * OmSMp1 * d[i] * (rhouS[2] + rhoSmq * nV[2]);
+    A[4][i] = -OmSM * A[4][i] + area * OmSMp1 * d[i] * (rhoeS + pS + rhoSmq * sM);
+    A[5][i] = -OmSM * A[5][i] + area * OmSMp1 * d[i] * rhoS * sc;
+  }
+}
+
+/* calcEulerFluxMatricesCoupled_HLLC, UgpWithCvCompFlow.cpp:1934-2176 (ALL_TERMS / ONLY_PRESSURE) */
+static void matrices_hllc_coupled(double (*AL)[NB], double (*AR)[NB], const cstate *L, const cstate *R, double area,
+                                  const double *nV, int only_pressure) {
+  if (!only_pressure) {
+    double dL[NB], dR[NB];
+    double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+    double hL = L->h + 0.0;
+    double rhoeL = (hL + 0.5 * uLuL) * L->rho - L->p;
+    double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+    double hR = R->h + 0.0;
+    double rhoeR = (hR + 0.5 * uRuR) * R->rho - R->p;
+    double Rrho = sqrt(R->rho / L->rho);
+    double tmp = 1.0 / (1.0 + Rrho);
+    double velRoe[3];
+    for (int i = 0; i < 3; i++) velRoe[i] = tmp * (L->u[i] + R->u[i] * Rrho);
+    double uRoe = dot3(velRoe, nV);
+    double gamPdivRho = tmp * ((L->gam * L->p / L->rho + 0.5 * (L->gam - 1.0) * uLuL) +
+                               (R->gam * R->p / R->rho + 0.5 * (R->gam - 1.0) * uRuR) * Rrho);
+    double cRoe = sqrt(gamPdivRho - ((L->gam + R->gam) * 0.5 - 1.0) * 0.5 * dot3(velRoe, velRoe));
+    double sL = dmin(uRoe - cRoe, unL - cL);
+    double sR = dmax(uRoe + cRoe, unR + cR);
+    double invrhotld = 1.0 / (R->rho * (sR - unR) - L->rho * (sL - unL));
+    double sM = (L->p - R->p - L->rho * unL * (sL - unL) + R->rho * unR * (sR - unR)) /
+                (R->rho * (sR - unR) - L->rho * (sL - unL));
+    double pStar = R->rho * (unR - sR) * (unR - sM) + R->p;
+    double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+    if (sM >= 0.0) {
+      if (sL > 0.0) {
+        if (AL) jac_coupled(AL, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
+        if (AR) memset(AR, 0, sizeof(double) * NB * NB);
+      } else {
+        double Om = 1.0 / (sL - sM), sLmuL = sL - unL;
+        double rhoS = L->rho * sLmuL * Om, rhouS[3];
+        for (int i = 0; i < 3; i++) rhouS[i] = (L->rho * L->u[i] * sLmuL + (pStar - L->p) * nV[i]) * Om;
+        double rhoeS = (sLmuL * rhoeL - L->p * unL + pStar * sM) * Om;
+        if (AL) {
+          dsmdu(dL, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
+          jac_coupled(AL, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
+          double rhoSmqR = R->rho * (sR - unR);
+          subsonic_coupled(AL, dL, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, rhoSmqR, nV, area);
+          for (int i = 0; i < 5; i++) AL[i][i] += area * Om * sM * sL;
+          AL[5][0] += area * Om * sM * sL * L->sc;
+          AL[5][5] += area * Om * sM * sL * L->rho;
+        }
+        if (AR) {
+          dsmdu(dR, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
+          memset(AR, 0, sizeof(double) * NB * NB);
+          double rhoSmqL = L->rho * (sL - unL);
+          subsonic_coupled(AR, dR, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, rhoSmqL, nV, area);
+        }
+      }
+    } else {
+      if (sR >= 0.0) {
+        double Om = 1.0 / (sR - sM), sRmuR = sR - unR;
+        double rhoS = R->rho * sRmuR * Om, rhouS[3];
+        for (int i = 0; i < 3; i++) rhouS[i] = (R->rho * R->u[i] * sRmuR + (pStar - R->p) * nV[i]) * Om;
+        double rhoeS = (sRmuR * rhoeR - R->p * unR + pStar * sM) * Om;
+        if (AR) {
+          dsmdu(dR, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
+          jac_coupled(AR, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
+          double rhoSmqL = L->rho * (sL - unL);
+          subsonic_coupled(AR, dR, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, rhoSmqL, nV, area);
+          for (int i = 0; i < 5; i++) AR[i][i] += area * Om * sM * sR;
+          AR[5][0] += area * Om * sM * sR * R->sc;
+          AR[5][5] += area * Om * sM * sR * R->rho;
+        }
+        if (AL) {
+          dsmdu(dL, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
+          memset(AL, 0, sizeof(double) * NB * NB);
+          double rhoSmqR = R->rho * (sR - unR);
+          subsonic_coupled(AL, dL, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, rhoSmqR, nV, area);
+        }
+      } else {
+        if (AR) jac_coupled(AR, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
+        if (AL) memset(AL, 0, sizeof(double) * NB * NB);
+      }
+    }
+  } else {
+    if (AL) {
+      double uLuL = dot3(L->u, L->u), hL = L->h + 0.0, g = L->gam;
+      for (int j = 0; j < NB; j++) AL[0][j] = 0.0;
+      double dpdrho = 0.5 * (g - 1.0) * uLuL - (g - 1.0) * hL + g * L->p / L->rho;
+      for (int r = 0; r < 3; r++) {
+        AL[1 + r][0] = dpdrho * nV[r] * area;
+        for (int c = 0; c < 3; c++) AL[1 + r][1 + c] = -(g - 1.0) * L->u[c] * nV[r] * area;
+        AL[1 + r][4] = (g - 1.0) * nV[r] * area;
+        AL[1 + r][5] = 0.0 * nV[r] * area;
+      }
+      for (int i = 4; i < NB; i++)
+        for (int j = 0; j < NB; j++) AL[i][j] = 0.0;
+    }
+    if (AR) memset(AR, 0, sizeof(double) * NB * NB);
+  }
+  /* dU/dQ for the scalar column (Q holds rho*phi, U holds phi) */
+  if (AL)
+    for (int j = 0; j < NB; j++) {
+      AL[j][0] -= L->sc / L->rho * AL[j][5];
+      AL[j][5] /= L->rho;
+    }
+  if (AR)
+    for (int j = 0; j < NB; j++) {
+      AR[j][0] -= R->sc / R->rho * AR[j][5];
+      AR[j][5] /= R->rho;
+    }
+}
+
+/* calcViscousFluxCoupled, UgpWithCvCompFlow.cpp:3040-3276 (nScal = 1, kine = 0, turbulence on) */
+static void visc_coupled(double Fv[NB], double (*A0)[NB], double (*A1)[NB], double rho0, const double *u0,
+                         const double *gu0, double h0, const double *gh0, double T0, double R0, double gam0,
+                         double sc0, const double *gs0, double rho1, const double *u1, const double *gu1, double h1,
+                         const double *gh1, double T1, double R1, double gam1, double sc1, const double *gs1,
+                         double mul, double mut, double lamOcp, double PrTurb, const double *u_fa, double diff,
+                         double diffTerm, double area, const double *nV, double smag, const double *sV,
+                         double alpha) {
+  double g[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) g[i][j] = 0.5 * (gu0[3 * i + j] + gu1[3 * i + j]);
+  double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
+  double muT = mul + mut;
+  double tn[3];
+  Fv[0] = 0.0;
+  for (int i = 0; i < 3; i++)
+    tn[i] = muT * (alpha * (u1[i] - u0[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
+                   g[1][i] * nV[1] + g[i][2] * fC[2] + g[2][i] * nV[2]);
+  double tmp = 2.0 / 3.0 * muT * (g[0][0] + g[1][1] + g[2][2]);
+  tmp += 1.0 / 3.0 * (rho0 + rho1) * 0.0;
+  for (int i = 0; i < 3; i++) tn[i] -= tmp * nV[i];
+  for (int i = 0; i < 3; i++) Fv[1 + i] = -area * tn[i];
+  double keff = lamOcp + mut / PrTurb;
+  double enth = keff * (alpha * (h1 - h0) / smag + 0.5 * ((gh0[0] + gh1[0]) * fC[0] + (gh0[1] + gh1[1]) * fC[1] +
+                                                          (gh0[2] + gh1[2]) * fC[2]));
+  double psi = muT * (alpha * (0.0 - 0.0) / smag);
+  Fv[4] = -area * (enth + tn[0] * u_fa[0] + tn[1] * u_fa[1] + tn[2] * u_fa[2] + psi);
+  Fv[5] = -area * diffTerm * diff * (alpha * (sc1 - sc0) / smag + 0.5 * ((gs0[0] + gs1[0]) * fC[0] +
+                                                                          (gs0[1] + gs1[1]) * fC[1] +
+                                                                          (gs0[2] + gs1[2]) * fC[2]));
+  double aas = area * alpha / smag;
+  for (int side = 0; side < 2; side++) {
+    double (*A)[NB] = side ? A1 : A0;
+    if (!A) continue;
+    double sg = side ? -1.0 : 1.0;
+    double rho = side ? rho1 : rho0, hh = side ? h1 : h0, TT = side ? T1 : T0, RR = side ? R1 : R0;
+    double gm = side ? gam1 : gam0, sc = side ? sc1 : sc0;
+    const double *u = side ? u1 : u0;
+    double d11 = sg * muT * aas, d22 = d11, d33 = d11;
+    double d41 = -area * tn[0] * 0.5 + u_fa[0] * d11;
+    double d42 = -area * tn[1] * 0.5 + u_fa[1] * d22;
+    double d43 = -area * tn[2] * 0.5 + u_fa[2] * d33;
+    double d44 = sg * keff * aas;
+    double dss = sg * diffTerm * diff * aas;
+    double iR = 1.0 / rho;
+    double q10 = -iR * u[0], q11 = iR, q20 = -iR * u[1], q22 = iR, q30 = -iR * u[2], q33 = iR;
+    double q40 = iR * gm * (-hh - 0.0 + RR * TT + 0.5 * dot3(u, u));
+    double q41 = -iR * u[0] * gm, q42 = -iR * u[1] * gm, q43 = -iR * u[2] * gm, q44 = iR * gm;
+    double q4s = iR * iR * 0.0, qs0 = -iR * sc, qss = iR;
+    A[1][0] = d11 * q10; A[1][1] = d11 * q11;
+    A[2][0] = d22 * q20; A[2][2] = d22 * q22;
+    A[3][0] = d33 * q30; A[3][3] = d33 * q33;
+    A[4][0] = d41 * q10 + d42 * q20 + d43 * q30 + d44 * q40;
+    A[4][1] = d41 * q11 + d44 * q41;
+    A[4][2] = d42 * q22 + d44 * q42;
+    A[4][3] = d43 * q33 + d44 * q43;
+    A[4][4] = d44 * q44;
+    A[4][5] = d44 * q4s;
+    A[5][0] = dss * qs0;
+    A[5][5] = dss * qss;
+  }
+}
+
+static void add_blk6(double *A, int slot, double (*B)[NB], double sgn) {
+  double *a = &A[NB * NB * slot];
+  for (int i = 0; i < NB; i++)
+    for (int j = 0; j < NB; j++) a[NB * i + j] += sgn * B[i][j];
+}
+
+static cstate cell_cstate(jo_case *h, int c) {
+  cstate s = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->press[c], h->temp[c],
+              h->enthalpy[c], h->RoM[c], h->gam[c], sa_of(h)->phi[c]};
+  return s;
+}
+static cstate bfa_cstate(jo_case *h, int f) {
+  cstate s = {h->rho_bfa[f], {h->vel_bfa[3 * f], h->vel_bfa[3 * f + 1], h->vel_bfa[3 * f + 2]}, h->p_bfa[f],
+              h->T_bfa[f], h->h_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], sa_of(h)->phi_bfa[f]};
+  return s;
+}
+
+/* face reconstruction with the scalar (JoeWithModels.cpp:4837-4921), then
+ * calcThermoProp_p for T and h (ideal gas) */
+static void reconstruct_c(jo_case *h, int c, int f, cstate *s) {
+  double r0[3];
+  for (int i = 0; i < 3; i++) r0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c + i];
+  double rho0 = h->rho[c] + dot3(r0, &h->grad_rho[3 * c]);
+  double p0 = h->press[c] + dot3(r0, &h->grad_p[3 * c]);
+  if ((p0 <= 0.0) || (rho0 <= 0.0)) {
+    s->p = h->press[c];
+    s->rho = h->rho[c];
+  } else {
+    s->rho = rho0;
+    s->p = p0;
+    for (int i = 0; i < 3; i++) s->u[i] = h->vel[3 * c + i] + dot3(r0, &h->grad_u[9 * c + 3 * i]);
+    s->sc += dot3(r0, &sa_of(h)->grad_phi[3 * c]);
+  }
+  s->R = h->p.R_gas;
+  s->gam = h->p.gamma;
+  s->T = s->p / (s->rho * s->R);
+  s->h = s->gam * s->R / (s->gam - 1.0) * s->T;
+}
+
+/* calcRhsCoupled (JoeWithModels.cpp:4597-4611) for SA: rhs[ncv][6], A[nbocv_s][6][6] (accumulated) */
+void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
+  const jg_mesh *m = &h->m;
+  const jg_params *p = &h->p;
+  jo_sa *s = sa_of(h);
+  int visc = p->mu_ref > 0.0;
+  int only_p = p->symm_bc == JG_SYMM_ANALYTICAL;
+  memset(rhs, 0, sizeof(double) * NB * h->ncv);
+  /* gradients, JoeWithModels.cpp:4683-4754 */
+  if (p->second_order || visc) grad_vector(h, h->grad_u, h->vel, h->vel_bfa, p->limiter, h->sos);
+  if (p->second_order) {
+    grad_scalar(h, h->grad_rho, h->rho, h->rho_bfa, p->limiter, h->rho, NULL);
+    grad_scalar(h, h->grad_p, h->press, h->p_bfa, p->limiter, h->press, NULL);
+  }
+  if (visc) grad_scalar(h, h->grad_h, h->enthalpy, h->h_bfa, p->limiter, h->enthalpy, NULL);
+  if (p->second_order || visc) grad_scalar(h, s->grad_phi, s->phi, s->phi_bfa, p->limiter, s->phi, NULL);
+  if (visc) {
+    /* RansTurbSA::diffusivityHookScalarRansTurb, TurbModel_SA.h:130-173 */
+    double invSigma = 1.0 / SA_SIGMA;
+    for (int f = h->nfa_b; f < h->nfa; f++) {
+      int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+      double dx0[3], dx1[3];
+      for (int i = 0; i < 3; i++) {
+        dx0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+        dx1[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c1 + i];
+      }
+      double w0 = sqrt(dot3(dx0, dx0)), w1 = sqrt(dot3(dx1, dx1));
+      double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
+      double nu_fa = (w1 * s->phi[c0] + w0 * s->phi[c1]) / (w0 + w1);
+      s->diff[f] = invSigma * (h->mul_fa[f] + rho_fa * nu_fa);
+    }
+    for (int z = 0; z < m->nzones; z++) {
+      const jg_zone *zn = &m->zones[z];
+      for (int f = zn->ifa_f; f <= zn->ifa_l; f++)
+        s->diff[f] = (zn->kind == JG_BC_WALL) ? invSigma * h->mul_fa[f]
+                                              : invSigma * (h->mul_fa[f] + h->rho_bfa[f] * s->phi_bfa[f]);
+    }
+  }
+  double F[NB], Fv[NB], Apl[NB][NB], Ami[NB][NB], A0[NB][NB], A1[NB][NB];
+  memset(A0, 0, sizeof(A0));
+  memset(A1, 0, sizeof(A1));
+  /* internal faces, JoeWithModels.cpp:4797-5132 */
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double nV[3];
+    double area = norm3(nV, &m->fa_normal[3 * f]);
+    cstate L = cell_cstate(h, c0), R = cell_cstate(h, c1);
+    if (p->second_order) {
+      reconstruct_c(h, c0, f, &L);
+      reconstruct_c(h, c1, f, &R);
+    }
+    flux_hllc_coupled(F, &L, &R, area, nV, 0);
+    for (int i = 0; i < NB; i++) { rhs[NB * c0 + i] -= F[i]; rhs[NB * c1 + i] += F[i]; }
+    int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
+    if (implicit) {
+      cstate L0 = cell_cstate(h, c0), R0 = cell_cstate(h, c1);
+      matrices_hllc_coupled(Apl, Ami, &L0, &R0, area, nV, 0);
+      add_blk6(A, n00, Apl, 1.0);
+      add_blk6(A, n01, Ami, 1.0);
+      add_blk6(A, n11, Ami, -1.0);
+      add_blk6(A, n10, Apl, -1.0);
+    }
+    if (visc) {
+      double sV[3];
+      for (int i = 0; i < 3; i++) sV[i] = m->x_cv[3 * c1 + i] - m->x_cv[3 * c0 + i];
+      double smag = norm3(sV, sV);
+      double alpha = dot3(nV, sV);
+      double uf[3];
+      for (int i = 0; i < 3; i++) uf[i] = 0.5 * (h->vel[3 * c0 + i] + h->vel[3 * c1 + i]);
+      visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, h->rho[c0], &h->vel[3 * c0],
+                   &h->grad_u[9 * c0], h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0],
+                   s->phi[c0], &s->grad_phi[3 * c0], h->rho[c1], &h->vel[3 * c1], &h->grad_u[9 * c1],
+                   h->enthalpy[c1], &h->grad_h[3 * c1], h->temp[c1], h->RoM[c1], h->gam[c1], s->phi[c1],
+                   &s->grad_phi[3 * c1], h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, uf, s->diff[f],
+                   1.0, area, nV, smag, sV, alpha);
+      for (int i = 0; i < NB; i++) { rhs[NB * c0 + i] -= Fv[i]; rhs[NB * c1 + i] += Fv[i]; }
+      if (implicit) {
+        add_blk6(A, n00, A0, 1.0);
+        add_blk6(A, n01, A1, 1.0);
+        add_blk6(A, n11, A1, -1.0);
+        add_blk6(A, n10, A0, -1.0);
+      }
+    }
+  }
+  /* boundary faces, JoeWithModels.cpp:5139-5799 */
+  double zero3[3] = {0.0, 0.0, 0.0};
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    double diffTerm = (zn->scal_bc & 1) ? 1.0 : 0.0;
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      int c0 = m->cvofa[2 * f];
+      int n00 = m->nbocv_i[c0];
+      double nV[3];
+      double area = norm3(nV, &m->fa_normal[3 * f]);
+      cstate B = bfa_cstate(h, f);
+      if (zn->kind == JG_BC_SYMMETRY || zn->kind == JG_BC_WALL) {
+        flux_hllc_coupled(F, &B, &B, area, nV, only_p);
+        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+        if (implicit) {
+          if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
+            matrices_hllc_coupled(Apl, Ami, &B, &B, area, nV, 0);
+            for (int i = 0; i < NB; i++)
+              for (int j = 0; j < NB; j++) A[NB * NB * n00 + NB * i + j] += Apl[i][j] + Ami[i][j];
+          } else {
+            matrices_hllc_coupled(Apl, NULL, &B, &B, area, nV, only_p);
+            add_blk6(A, n00, Apl, 1.0);
+          }
+        }
+        if (visc && zn->kind == JG_BC_SYMMETRY) {
+          const double *g = &h->grad_u[9 * c0];
+          double tmp = 2.0 / 3.0 * ((h->mul_fa[f] + h->mut_fa[f]) * (g[0] + g[4] + g[8]) + h->rho_bfa[f] * 0.0);
+          for (int i = 0; i < 3; i++) rhs[NB * c0 + 1 + i] -= area * tmp * nV[i];
+        }
+        if (visc && zn->kind == JG_BC_WALL) {
+          double sV[3];
+          for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+          double smag = fabs(dot3(sV, nV));
+          visc_coupled(Fv, implicit ? A0 : NULL, NULL, h->rho[c0], &h->vel[3 * c0], &h->grad_u[9 * c0],
+                       h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0], s->phi[c0],
+                       &s->grad_phi[3 * c0], h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0], h->h_bfa[f],
+                       &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], s->phi_bfa[f],
+                       &s->grad_phi[3 * c0], h->mul_fa[f], 0.0, h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f],
+                       s->diff[f], diffTerm, area, nV, smag, nV, 1.0);
+          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
+          if (implicit) add_blk6(A, n00, A0, 1.0);
+        }
+      } else if (zn->kind == JG_BC_NEUMANN) {
+        flux_hllc_coupled(F, &B, &B, area, nV, 0);
+        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+        if (implicit) {
+          matrices_hllc_coupled(Apl, Ami, &B, &B, area, nV, 0);
+          for (int i = 0; i < NB; i++)
+            for (int j = 0; j < NB; j++)
+              A[NB * NB * n00 + NB * i + j] += (p->symm_bc == JG_SYMM_NEW_NUMERIC) ? Apl[i][j] + Ami[i][j] : Apl[i][j];
+        }
+        if (visc) {
+          double sV[3];
+          for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+          double smag = fabs(dot3(sV, nV));
+          visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, h->rho_bfa[f], &h->vel_bfa[3 * f],
+                       &h->grad_u[9 * c0], h->h_bfa[f], &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f],
+                       h->gam_bfa[f], s->phi_bfa[f], zero3, h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0],
+                       h->h_bfa[f], &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], s->phi_bfa[f],
+                       zero3, h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f], s->diff[f],
+                       1.0, area, nV, smag, nV, 1.0);
+          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
+          if (implicit) add_blk6(A, n00, A0, 1.0);
+        }
+      } else {
+        /* CBC, CBC_SUBSONIC_INLET/OUTLET, FARFIELD: JoeWithModels.cpp:5624-5788 */
+        cstate L = cell_cstate(h, c0);
+        if (p->second_order) reconstruct_c(h, c0, f, &L);
+        flux_hllc_coupled(F, &L, &B, area, nV, 0);
+        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+        if (implicit) {
+          cstate L0 = cell_cstate(h, c0);
+          matrices_hllc_coupled(Apl, NULL, &L0, &B, area, nV, 0);
+          add_blk6(A, n00, Apl, 1.0);
+        }
+        if (visc) {
+          double sV[3];
+          for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+          double smag = norm3(sV, sV);
+          double alpha = dot3(nV, sV);
+          /* the outer state's scalar is the reconstructed face value (as the reference passes it) */
+          visc_coupled(Fv, implicit ? A0 : NULL, NULL, h->rho[c0], &h->vel[3 * c0], &h->grad_u[9 * c0],
+                       h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0], s->phi[c0],
+                       &s->grad_phi[3 * c0], h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0], h->h_bfa[f],
+                       &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], L.sc, &s->grad_phi[3 * c0],
+                       h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f], s->diff[f],
+                       diffTerm, area, nV, smag, sV, alpha);
+          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
+          if (implicit) add_blk6(A, n00, A0, 1.0);
+        }
+      }
+    }
+  }
+  /* RansTurbSA::sourceHookRansTurbCoupled, TurbModel_SA.h:359-434 */
+  for (int c = 0; c < h->ncv; c++) {
+    double mue = face_avg(h, h->mul_fa, c);
+    double Om = dmax(s->vortMag[c], 1.e-8);
+    double Strainrate = dmax(s->strMag[c], 1.e-8);
+    double d = s->wallDist[c];
+    double nu = s->phi[c];
+    double chi = nu * h->rho[c] / mue;
+    double chi_3 = pow(chi, 3.0);
+    double inv_K2d2 = 1.0 / (SA_K2 * d * d);
+    double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+    double fv2 = 1.0 - chi / (1.0 + chi * fv1);
+    double S = dmax(Om + dmin(0.0, Strainrate - Om) * 0.0, 0.0);
+    double Shat = S + nu * fv2 * inv_K2d2;
+    double inv_Shat = 1.0 / dmax(Shat, 1.0e-8);
+    double r = dmin(nu * inv_Shat * inv_K2d2, 10.0);
+    double g = r + SA_CW2 * (pow(r, 6.0) - r);
+    double g_6 = pow(g, 6.0);
+    double fw = g * pow((1.0 + SA_CW3_6) / (g_6 + SA_CW3_6), 1.0 / 6.0);
+    double H1 = SA_CB1 * Shat * nu;
+    double H2 = -SA_CW1 * fw * nu * nu / pow(d, 2.0);
+    double H3 = SA_CB2 / SA_SIGMA * dot3(&s->grad_phi[3 * c], &s->grad_phi[3 * c]);
+    rhs[NB * c + 5] += h->rho[c] * m->cv_volume[c] * (H1 + H2 + H3);
+    if (implicit) {
+      double d_H1 = 0.0;
+      double d_H2 = -2.0 * SA_CW1 * fw * nu / pow(d, 2.0);
+      A[NB * NB * m->nbocv_i[c] + NB * 5 + 5] -= (d_H1 + d_H2) * m->cv_volume[c];
+    }
+  }
+}
+
+/* n x n LU without pivoting (ludeco / lusolv, UgpWithCv.cpp:2489-2577, any order) */
+static void ludeco_n(double *A, int n) {
+  for (int jc = 1; jc < n; jc++) A[jc] /= A[0];
+  int jrjc = 0;
+  for (;;) {
+    jrjc++;
+    int jrjcm1 = jrjc - 1, jrjcp1 = jrjc + 1;
+    for (int jr = jrjc; jr < n; jr++) {
+      double sum = A[n * jr + jrjc];
+      for (int jm = 0; jm <= jrjcm1; jm++) sum -= A[n * jr + jm] * A[n * jm + jrjc];
+      A[n * jr + jrjc] = sum;
+    }
+    if (jrjc == (n - 1)) return;
+    for (int jc = jrjcp1; jc < n; jc++) {
+      double sum = A[n * jrjc + jc];
+      for (int jm = 0; jm <= jrjcm1; jm++) sum -= A[n * jrjc + jm] * A[n * jm + jc];
+      A[n * jrjc + jc] = sum / A[n * jrjc + jrjc];
+    }
+  }
+}
+static void lusolv_n(const double *A, double *c, int n) {
+  c[0] = c[0] / A[0];
+  for (int jr = 1; jr < n; jr++) {
+    double sum = c[jr];
+    for (int jm = 0; jm <= jr - 1; jm++) sum -= A[n * jr + jm] * c[jm];
+    c[jr] = sum / A[n * jr + jr];
+  }
+  for (int jrjr = 1; jrjr < n; jrjr++) {
+    int jr = (n - 1) - jrjr, jrp1 = jr + 1;
+    double sum = c[jr];
+    for (int jmjm = jrp1; jmjm < n; jmjm++) {
+      int jm = (n - 1) - jmjm + jrp1;
+      sum -= A[n * jr + jm] * c[jm];
+    }
+    c[jr] = sum;
+  }
+}
+
+/* block Jacobi (sgs = 0) or multicolour block Gauss-Seidel (sgs = 1) sweeps
+ * of the B x B system from x = 0, as the GPU runs them */
+int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps, int sgs) {
+  int n = h->ncv;
+  const jg_mesh *m = &h->m;
+  double *LU = dalloc((size_t)B * B * n), *xn = dalloc((size_t)B * n);
+  int *color = (int *)calloc(n, sizeof(int));
+  int ncol = 1, mark[256];
+  for (int k = 0; k < 256; k++) mark[k] = -1;
+  for (int c = 0; c < n; c++) {
+    for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++)
+      if (m->nbocv_v[k] < c) mark[color[m->nbocv_v[k]]] = c;
+    int q = 0;
+    while (q < 255 && mark[q] == c) q++;
+    color[c] = q;
+    if (q + 1 > ncol) ncol = q + 1;
+  }
+  if (!sgs) ncol = 1;
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[(size_t)B * B * c], &A[(size_t)B * B * m->nbocv_i[c]], sizeof(double) * B * B);
+    ludeco_n(&LU[(size_t)B * B * c], B);
+  }
+  memset(x, 0, sizeof(double) * B * n);
+  double b[8];
+  for (int s = 0; s < sweeps; s++)
+    for (int q = 0; q < ncol; q++) {
+      int col = (s % 2 == 0) ? q : ncol - 1 - q;
+      for (int c = 0; c < n; c++) {
+        if (sgs && color[c] != col) continue;
+        for (int i = 0; i < B; i++) b[i] = rhs[B * c + i];
+        for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+          int nb = m->nbocv_v[k];
+          for (int i = 0; i < B; i++)
+            for (int j = 0; j < B; j++) b[i] -= A[(size_t)B * B * k + B * i + j] * x[B * nb + j];
+        }
+        lusolv_n(&LU[(size_t)B * B * c], b, B);
+        memcpy(sgs ? &x[B * c] : &xn[B * c], b, sizeof(double) * B);
+      }
+      if (!sgs) memcpy(x, xn, sizeof(double) * B * n);
+    }
+  free(LU); free(xn); free(color);
+  return sweeps;
+}
+
+/* runBackwardEulerCoupled loop body (JoeWithModels.cpp:4416-4529) with the
+ * GPU's block relaxation for the linear solve; resid[6] = last L1 residual */
+int jo_step_coupled(jo_case *h, int nsteps, double *resid) {
+  const jg_params *p = &h->p;
+  int n = h->ncv, nbs = h->nbs;
+  jo_sa *s = sa_of(h);
+  double *A = dalloc((size_t)NB * NB * nbs), *dq = dalloc((size_t)NB * n), *rhs = dalloc((size_t)NB * n);
+  int err = 0;
+  for (int it = 0; it < nsteps; it++) {
+    h->step++;
+    if ((h->step >= p->cfl_after) && (h->step % p->cfl_interval == 0) && (h->cfl < p->cfl_max)) h->cfl *= p->cfl_factor;
+    jo_calc_dt(h, h->cfl);
+    memset(A, 0, sizeof(double) * NB * NB * nbs);
+    jo_calc_rhs_coupled(h, rhs, A, 1);
+    double r[NB] = {0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < n; c++)
+      for (int i = 0; i < NB; i++) r[i] += fabs(rhs[NB * c + i]);
+    for (int c = 0; c < n; c++) {
+      for (int i = 0; i < NB; i++) rhs[NB * c + i] *= p->under_relax;
+      double tmp = h->m.cv_volume[c] / (h->local_dt[c]);
+      for (int i = 0; i < NB; i++) A[(size_t)NB * NB * h->m.nbocv_i[c] + (NB + 1) * i] += tmp;
+    }
+    jo_solve_blocks(h, NB, dq, A, rhs, p->ls_max_iter, p->lin_solver == JG_LS_SGS);
+    for (int c = 0; c < n; c++) {
+      h->rho[c] += dq[NB * c];
+      for (int i = 0; i < 3; i++) h->rhou[3 * c + i] += dq[NB * c + 1 + i];
+      h->rhoE[c] += dq[NB * c + 4];
+    }
+    for (int c = 0; c < n; c++)
+      s->phi[c] = dmin(dmax((s->phi[c] * (h->rho[c] - dq[NB * c]) + dq[NB * c + 5]) / h->rho[c], SA_LOWER), SA_UPPER);
+    if (jo_calc_state_coupled(h) != 0) err = -1;
+    if (resid) memcpy(resid, r, sizeof(r));
+  }
+  free(A); free(dq); free(rhs);
+  return err;
+}

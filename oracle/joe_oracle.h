@@ -37,4 +37,20 @@ int jo_step_count(jo_case *h);
  * area[n], nvec[n][3]; F[n][5]; AL/AR[n][25] (may be NULL) */
 void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area,
                          const double *nvec, double *F, double *AL, double *AR);
+
+/* Coupled path with the Spalart-Allmaras model (nscal = 1, block size 6):
+ * scalar nuSA in/out, wall distance (calcWallDistance), the coupled preamble
+ * (state + material + BC + scalar BC + calcRansTurbViscMuet), calcRhsCoupled
+ * (rhs[ncv][6], A[nbocv_s][6][6] accumulated), block relaxation of a B x B
+ * system (sgs 0: Jacobi, 1: multicolour Gauss-Seidel) and the coupled step.
+ * Named SA arrays: "phi","phi_bfa","grad_phi","diff","wallDist","strMag","vortMag". */
+void jo_set_scalar(jo_case *h, const double *phi);
+void jo_get_scalar(jo_case *h, double *phi);
+void jo_wall_distance(jo_case *h);
+int jo_calc_state_coupled(jo_case *h);
+void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit);
+int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps, int sgs);
+int jo_step_coupled(jo_case *h, int nsteps, double *resid);
+double *jo_sa_array(jo_case *h, const char *name);
+void jo_sa_release(jo_case *h);
 #endif

@@ -47,6 +47,18 @@ def lib():
         L.jo_cfl.argtypes = [P]
         L.jo_cfl.restype = C.c_double
         L.jo_euler_flux_faces.argtypes = [C.c_int, C.c_int, D, D, D, D, D, D, D]
+        L.jo_set_scalar.argtypes = [P, D]
+        L.jo_get_scalar.argtypes = [P, D]
+        L.jo_wall_distance.argtypes = [P]
+        L.jo_calc_state_coupled.argtypes = [P]
+        L.jo_calc_state_coupled.restype = C.c_int
+        L.jo_calc_rhs_coupled.argtypes = [P, D, D, C.c_int]
+        L.jo_solve_blocks.argtypes = [P, C.c_int, D, D, D, C.c_int, C.c_int]
+        L.jo_step_coupled.argtypes = [P, C.c_int, D]
+        L.jo_step_coupled.restype = C.c_int
+        L.jo_sa_array.argtypes = [P, C.c_char_p]
+        L.jo_sa_array.restype = D
+        L.jo_sa_release.argtypes = [P]
         _lib = L
     return _lib
 
@@ -66,6 +78,7 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "h", None):
+            lib().jo_sa_release(self.h)
             lib().jo_destroy(self.h)
             self.h = None
 
@@ -116,6 +129,56 @@ class Oracle:
         r = np.zeros(5)
         err = lib().jo_step(self.h, nsteps, dptr(r))
         if err:
+            raise ValueError("oracle step failed")
+        return r
+
+
+class OracleSA(Oracle):
+    """The coupled Spalart-Allmaras path (6x6 blocks): state + nuSA."""
+
+    B = 6
+
+    def __init__(self, mesh_src, params, precision=0):
+        super().__init__(mesh_src, params, precision)
+        lib().jo_wall_distance(self.h)
+
+    def set_scalar(self, phi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        lib().jo_set_scalar(self.h, dptr(phi))
+
+    def get_scalar(self):
+        phi = np.empty(self.ncv)
+        lib().jo_get_scalar(self.h, dptr(phi))
+        return phi
+
+    def calc_state(self):
+        if lib().jo_calc_state_coupled(self.h) != 0:
+            raise ValueError("unsupported boundary condition")
+
+    def sa_array(self, name):
+        n = {"phi_bfa": self.ma.nfa_b, "diff": self.ma.nfa}.get(name, self.ncv)
+        k = 3 if name == "grad_phi" else 1
+        ptr = lib().jo_sa_array(self.h, name.encode())
+        a = np.ctypeslib.as_array(ptr, shape=(n * k,)).copy()
+        return a.reshape(n, k) if k > 1 else a
+
+    def calc_rhs(self, implicit=True):
+        n, B = self.ncv, self.B
+        rhs = np.zeros((n, B))
+        A = np.zeros((self.ma.nbocv_s, B, B))
+        lib().jo_calc_rhs_coupled(self.h, dptr(rhs), dptr(A), int(implicit))
+        return rhs, A
+
+    def solve_blocks(self, A, rhs, sweeps, sgs=True):
+        x = np.zeros((self.ncv, self.B))
+        A = np.ascontiguousarray(A, np.float64)
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        lib().jo_solve_blocks(self.h, self.B, dptr(x), dptr(A), dptr(rhs), int(sweeps), int(sgs))
+        return x
+
+    def step(self, nsteps=1):
+        r = np.zeros(self.B)
+        if lib().jo_step_coupled(self.h, nsteps, dptr(r)):
             raise ValueError("oracle step failed")
         return r
 

@@ -6,19 +6,25 @@
 // GPU path can be checked against them, and it times the reference's own
 // runBackwardEuler as the CPU baseline.
 //
-// usage: ref_harness <Joe.in> <run 0|1|2> <dump|run> <outdir>
-//   dump : init -> state/material/BC -> calcDt -> calcRhs(implicit) -> one
-//          linear solve (solveCoupledLinSysNS); every array written to outdir
-//   run  : init -> runBackwardEuler (NSTEPS from the input); prints the
-//          wall-clock of the iteration loop and writes the final state
+// usage: ref_harness <Joe.in> <run 0|1> <dump|coupled|run> <outdir>
+//   run 0 : JoeWithModels (laminar / inviscid); run 1 : JoeWithModels + RansTurbSA
+//   dump    : init -> state/material/BC -> calcDt -> calcRhs(implicit) -> one
+//             linear solve (solveCoupledLinSysNS); every array written to outdir
+//   coupled : init -> state/material/BC/turbulent viscosity -> calcDt ->
+//             calcRhsCoupled(implicit): the (5+nScal) residual and block
+//             Jacobian of runBackwardEulerCoupled, plus the turbulence arrays
+//   run     : init -> runBackwardEuler (NSTEPS from the input); prints the
+//             wall-clock of the iteration loop and writes the final state
 //
 // Extra input keys read only by this harness:
 //   HARNESS_PERTURB = a   smooth perturbation of the uniform initial state
-//                         (same formula as myjoe_b200.case.perturbed_state)
+//                         (same formula as myjoe_b200.case.perturbed_state);
+//                         transported scalars get the factor of scal_perturb
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
+#include <vector>
 
 #include "JoeWithModels.h"
 #include "turbModels/TurbModel_SA.h"
@@ -45,6 +51,17 @@ static void perturb(double x, double y, double z, double a, double f[5]) {
   f[4] = 1.0 + 0.5 * a * cos(1.5 * x + 0.6) * sin(1.2 * y + 0.8);
 }
 
+// Perturbation factor of transported scalars (same formula in myjoe_b200.case).
+static double scal_perturb(double x, double y, double z, double a) {
+  return 1.0 + a * sin(1.3 * x + 0.4) * cos(0.7 * y + 0.1) * (1.0 + 0.2 * cos(2.3 * z));
+}
+
+// the reference's case-local SA class (src/joe/joe.cpp:286-298 pattern)
+class JoeSA : public JoeWithModels, public RansTurbSA {
+public:
+  JoeSA(char *name) : JoeWithModels(name), UgpWithCvCompFlow(name) {}
+};
+
 template <class Base>
 class Harness : public Base {
 public:
@@ -70,6 +87,11 @@ public:
         this->rho[icv] = r;
         for (int i = 0; i < 3; i++) this->rhou[icv][i] = r * v[i];
         this->rhoE[icv] = pp / (this->gamma[icv] - 1.0) + 0.5 * r * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      }
+      for (size_t s = 0; s < this->scalarTranspEqVector.size(); s++) {
+        double *phi = this->scalarTranspEqVector[s].phi;
+        for (int icv = 0; icv < this->ncv; icv++)
+          phi[icv] *= scal_perturb(this->x_cv[icv][0], this->x_cv[icv][1], this->x_cv[icv][2], a);
       }
     }
   }
@@ -186,6 +208,96 @@ public:
     DUMPD("dq", dq, 5 * ncv);
   }
 
+  // calcRhsCoupled as runBackwardEulerCoupled calls it (JoeWithModels.cpp:4326-4611)
+  void dumpCoupled() {
+    int ncv = this->ncv, nfa = this->nfa, nfa_b = this->nfa_b, nbocv_s = this->nbocv_s;
+    int nScal = this->scalarTranspEqVector.size();
+    int B = 5 + nScal;
+    writeMeta();
+    DUMPI("cvofa", this->cvofa, 2 * nfa);
+    DUMPI("faocv_i", this->faocv_i, ncv + 1);
+    DUMPI("faocv_v", this->faocv_v, this->faocv_i[ncv]);
+    DUMPI("nbocv_i", this->nbocv_i, ncv + 1);
+    DUMPI("nbocv_v", this->nbocv_v, nbocv_s);
+    DUMPD("x_cv", this->x_cv, 3 * ncv);
+    DUMPD("x_fa", this->x_fa, 3 * nfa);
+    DUMPD("fa_normal", this->fa_normal, 3 * nfa);
+    DUMPD("cv_volume", this->cv_volume, ncv);
+    DUMPD("nbocv_lsg_coeff", this->nbocv_lsg_coeff, 3 * nbocv_s);
+    DUMPD("boundary_fa_lsg_coeff", this->boundary_fa_lsg_coeff, 3 * nfa_b);
+    dumpState("init");
+    for (int s = 0; s < nScal; s++) {
+      char nm[64];
+      sprintf(nm, "init_scal%d.f64", s);
+      dumpRaw(nm, this->scalarTranspEqVector[s].phi, sizeof(double) * ncv);
+    }
+
+    for (int iScal = 0; iScal < nScal; iScal++) this->scalarTranspEqVector[iScal].coupling = "COUPLED";
+    this->calcStateVariables();
+    this->calcMaterialProperties();
+    this->setBC();
+    this->calcRansTurbViscMuet();
+    DUMPD("mul_fa", this->mul_fa, nfa);
+    DUMPD("lamOcp_fa", this->lamOcp_fa, nfa);
+    DUMPD("mut_fa", this->mut_fa, nfa);
+    DUMPD("rho_bfa", this->rho_bfa, nfa_b);
+    DUMPD("vel_bfa", this->vel_bfa, 3 * nfa_b);
+    DUMPD("p_bfa", this->p_bfa, nfa_b);
+    DUMPD("T_bfa", this->T_bfa, nfa_b);
+    DUMPD("h_bfa", this->h_bfa, nfa_b);
+    for (int s = 0; s < nScal; s++) {
+      char nm[64];
+      sprintf(nm, "scal%d_bfa.f64", s);
+      dumpRaw(nm, this->scalarTranspEqVector[s].phi_bfa, sizeof(double) * nfa_b);
+    }
+    double *wd = NULL, *sm = NULL, *vm = NULL;
+    if (this->getScalarData("wallDist")) wd = *(this->getScalarData("wallDist")->ptr);
+    if (this->getScalarData("strMag")) sm = *(this->getScalarData("strMag")->ptr);
+    if (this->getScalarData("vortMag")) vm = *(this->getScalarData("vortMag")->ptr);
+    if (wd) DUMPD("wallDist", wd, ncv);
+    if (sm) DUMPD("strMag", sm, ncv);
+    if (vm) DUMPD("vortMag", vm, ncv);
+
+    double dt_min = this->calcDt(this->cfl);
+    DUMPD("local_dt", this->local_dt, ncv);
+    DUMPD("dt_min", &dt_min, 1);
+
+    // A[nbocv_s][B][B] and rhs[ncv][B] as the pointer tables calcRhsCoupled takes
+    std::vector<double> Abuf((size_t)nbocv_s * B * B, 0.0), rbuf((size_t)ncv * B, 0.0);
+    std::vector<double *> Arows((size_t)nbocv_s * B), rrows(ncv);
+    std::vector<double **> Ablk(nbocv_s);
+    for (int noc = 0; noc < nbocv_s; noc++) {
+      for (int i = 0; i < B; i++) Arows[(size_t)noc * B + i] = &Abuf[((size_t)noc * B + i) * B];
+      Ablk[noc] = &Arows[(size_t)noc * B];
+    }
+    for (int icv = 0; icv < ncv; icv++) rrows[icv] = &rbuf[(size_t)icv * B];
+    double ***A = Ablk.data();
+    double **rhs = rrows.data();
+    for (int noc = 0; noc < nbocv_s; noc++)
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) A[noc][i][j] = 0.0;
+    this->calcRhsCoupled(rhs, A, nScal, true);
+    std::vector<double> flat((size_t)nbocv_s * B * B), r((size_t)ncv * B);
+    for (int noc = 0; noc < nbocv_s; noc++)
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) flat[((size_t)noc * B + i) * B + j] = A[noc][i][j];
+    for (int icv = 0; icv < ncv; icv++)
+      for (int i = 0; i < B; i++) r[(size_t)icv * B + i] = rhs[icv][i];
+    DUMPD("A_coupled", flat.data(), flat.size());
+    DUMPD("rhs_coupled", r.data(), r.size());
+    DUMPD("grad_u", this->grad_u, 9 * ncv);
+    if (this->grad_rho) DUMPD("grad_rho", this->grad_rho, 3 * ncv);
+    if (this->grad_p) DUMPD("grad_p", this->grad_p, 3 * ncv);
+    if (this->grad_enthalpy) DUMPD("grad_enthalpy", this->grad_enthalpy, 3 * ncv);
+    for (int s = 0; s < nScal; s++) {
+      char nm[64];
+      sprintf(nm, "scal%d_grad.f64", s);
+      dumpRaw(nm, this->scalarTranspEqVector[s].grad_phi, sizeof(double) * 3 * ncv);
+      sprintf(nm, "scal%d_diff.f64", s);
+      dumpRaw(nm, this->scalarTranspEqVector[s].diff, sizeof(double) * nfa);
+    }
+  }
+
   void runTimed() {
     writeMeta();
     DUMPD("x_cv", this->x_cv, 3 * this->ncv);
@@ -213,7 +325,11 @@ int main(int argc, char *argv[]) {
     if (run == 0) {
       Harness<JoeWithModels> *j = new Harness<JoeWithModels>(argv[1]);
       j->setup();
-      if (mode == "dump") j->dumpAll(); else j->runTimed();
+      if (mode == "dump") j->dumpAll(); else if (mode == "coupled") j->dumpCoupled(); else j->runTimed();
+    } else if (run == 1) {
+      Harness<JoeSA> *j = new Harness<JoeSA>(argv[1]);
+      j->setup();
+      if (mode == "dump") j->dumpAll(); else if (mode == "coupled") j->dumpCoupled(); else j->runTimed();
     } else {
       fprintf(stderr, "run %d not built into this harness yet\n", run);
       return 2;

@@ -8,7 +8,7 @@ and boundary-face states, local time step, gradients, RHS, the implicit
 matrix A, one linear solve, and the state + L1 residuals after a few
 runBackwardEuler steps.
 
-    python tests/golden/make_golden.py     # needs the reference + g++
+    python tests/golden/make_golden.py [segregated] [sa]    # needs the reference + g++
 """
 from __future__ import annotations
 
@@ -57,6 +57,18 @@ def cases():
     yield "plate_roe", rawp, prmp
 
 
+def sa_cases():
+    """Coupled Spalart-Allmaras cases (runBackwardEulerCoupled's calcRhsCoupled)."""
+    raw, _, prm = case.sa_bump_case(16, 8, 2, stretch=1.2, jitter=0.1, seed=3)
+    rawc, _, prmc = case.sa_bump_case(16, 8, 2, stretch=1.15, jitter=0.1, seed=5, inlet="CBC", mach=0.5)
+    bc_n = dict(prmc.bcs)
+    bc_n["outlet"] = BC("NEUMANN")
+    yield "sa_bump_farfield", raw, prm
+    yield "sa_bump_cbc_symm_original", rawc, dataclasses.replace(prmc, SYMM_BC="ORIGINAL_NUMERIC")
+    yield "sa_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
+        prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
+
+
 def params_json(prm) -> str:
     d = dataclasses.asdict(prm)
     d["bcs"] = {k: [v.kind, list(v.values)] for k, v in prm.bcs.items()}
@@ -71,8 +83,8 @@ def params_from_json(s: str):
     return case.JoeParams(bcs=bcs, **d)
 
 
-def main():
-    for name, raw, prm in cases():
+def main(which=("segregated", "sa")):
+    for name, raw, prm in (cases() if "segregated" in which else ()):
         extra = "HARNESS_PERTURB = %g" % PERTURB
         d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "dump")
         prm_run = dataclasses.replace(prm, NSTEPS=NSTEPS)
@@ -90,6 +102,18 @@ def main():
         out["nsteps"] = np.array(NSTEPS)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print("wrote", name, d["meta"]["ncv"], "cells")
+    for name, raw, prm in (sa_cases() if "sa" in which else ()):
+        extra = "HARNESS_PERTURB = %g" % PERTURB
+        d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "coupled", run_kind=1)
+        keep = ["cvofa", "faocv_i", "faocv_v", "nbocv_i", "nbocv_v", "x_cv", "x_fa", "fa_normal", "cv_volume",
+                "nbocv_lsg_coeff", "boundary_fa_lsg_coeff", "init_rho", "init_rhou", "init_rhoE", "init_scal0",
+                "mul_fa", "lamOcp_fa", "mut_fa", "scal0_bfa", "wallDist", "strMag", "vortMag", "local_dt",
+                "grad_u", "scal0_grad", "scal0_diff", "rhs_coupled", "A_coupled"]
+        out = {k: d[k] for k in keep if k in d}
+        out["meta"] = np.array(json.dumps(d["meta"]))
+        out["params"] = np.array(params_json(prm))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print("wrote", name, d["meta"]["ncv"], "cells")
 
 
 def load(path):
@@ -102,4 +126,4 @@ def load(path):
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("segregated", "sa"))

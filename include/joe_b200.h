@@ -142,6 +142,24 @@ int jg_calc_dt(jg_case_t *h, double cfl, double *dt_min, double *local_dt);
  * Euler + viscous fluxes, residual; with flagImplicit and A != NULL also the
  * block Jacobian A[nbocv_s][5][5] in the reference's CSR layout. */
 int jg_calc_rhs(jg_case_t *h, double *rhs_rho, double *rhs_rhou, double *rhs_rhoE, double *A, int flagImplicit);
+
+/* Coupled path (jg_params.turb_model = JG_TURB_SA, nscal = 1, HLLC, JACOBI or
+ * SGS relaxation).  The handle computes the wall distance at creation
+ * (calcWallDistance, UgpWithCvCompFlow.h:1395-1535).  Transported scalars
+ * phi[ncv][nscal] (nuSA; ScalarTranspEq phi) in/out: set them after
+ * jg_set_state, before the first step.  jg_calc_rhs_coupled is
+ * JoeWithModels::calcRhsCoupled (JoeWithModels.cpp:4597-4611) with
+ * RansTurbSA's hooks: rhs[ncv][5+nscal], A[nbocv_s][5+nscal][5+nscal] (NULL:
+ * residual only).  jg_step on such a handle runs runBackwardEulerCoupled's
+ * iteration (4416-4529) and reports resid[nsteps][5+nscal].  jg_get_turb
+ * returns the model arrays of the current state (any pointer may be NULL):
+ * wallDist[ncv], mut_fa[nfa], strMag[ncv], vortMag[ncv], phi_bfa[nfa_b],
+ * grad_phi[ncv][3], diff[nfa] (scalar diffusivity). */
+int jg_set_scalars(jg_case_t *h, const double *phi);
+int jg_get_scalars(jg_case_t *h, double *phi);
+int jg_calc_rhs_coupled(jg_case_t *h, double *rhs, double *A, int flagImplicit);
+int jg_get_turb(jg_case_t *h, double *wallDist, double *mut_fa, double *strMag, double *vortMag, double *phi_bfa,
+                double *grad_phi, double *diff);
 /* gradients of the last jg_calc_rhs / step: calcCvVectorGrad / calcCvScalarGrad
  * with limiting (src/common/UgpWithCv.h:803-1083); grad_u[ncv][3][3], others [ncv][3].
  * grad_u is what the reference holds after calcRhs: the viscous gradient when

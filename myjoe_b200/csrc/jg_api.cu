@@ -79,6 +79,8 @@ struct jg_case {
   double* d_io = nullptr;   // [5][N] staging for direct host<->device state copies
   int async_alloc = 0;      // stream-ordered allocation (serving): no device-wide sync on free
   size_t bytes = 0;         // device bytes held by this handle
+  int bs = 5;               // block size: 5, or 6 on the coupled SA path
+  Turb turb{};              // SA arrays (coupled path)
 };
 
 
@@ -171,7 +173,17 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "unsupported precision %d", q->precision);
   if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS))
     return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI or SGS sweeps");
-  if (q->nscal != 0) return set_err(JG_ERR_ARG, "transported scalars are not supported by this build");
+  if (q->turb_model == JG_TURB_SA) {
+    if (q->nscal != 1) return set_err(JG_ERR_ARG, "the SA model transports one scalar (nscal = 1)");
+    if (!(q->mu_ref > 0.0)) return set_err(JG_ERR_ARG, "the SA model needs a viscous case (mu_ref > 0)");
+    if (q->flux != JG_FLUX_HLLC) return set_err(JG_ERR_ARG, "the coupled path uses the HLLC flux");
+    if (q->lin_solver != JG_LS_JACOBI && q->lin_solver != JG_LS_SGS)
+      return set_err(JG_ERR_ARG, "the coupled path relaxes with JACOBI or SGS sweeps");
+  } else if (q->turb_model != JG_TURB_NONE) {
+    return set_err(JG_ERR_ARG, "unsupported turbulence model %d", q->turb_model);
+  } else if (q->nscal != 0) {
+    return set_err(JG_ERR_ARG, "transported scalars need a turbulence model");
+  }
   if (q->time_step_mode < 0 || q->time_step_mode > 2) return set_err(JG_ERR_ARG, "bad time step mode");
   if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");
   return JG_OK;
@@ -223,6 +235,8 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   h->hp = *q;
   h->p = make_params(*q);
   h->eltsz = h->p.fp32 ? 4 : 8;
+  h->bs = (q->turb_model == JG_TURB_SA) ? 6 : 5;
+  const int bs = h->bs;
   h->nbocv_i.assign(mesh->nbocv_i, mesh->nbocv_i + N + 1);
   h->nbocv_v.assign(mesh->nbocv_v, mesh->nbocv_v + mesh->nbocv_s);
   // boundary-face zones
@@ -235,6 +249,7 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     if (zn.kind < JG_BC_SYMMETRY || zn.kind > JG_BC_FARFIELD)
       return set_err(JG_ERR_ARG, "zone %d: unsupported boundary kind %d", z, zn.kind);
     zones[z].kind = zn.kind;
+    zones[z].scal_bc = zn.scal_bc;
     for (int k = 0; k < 8; k++) zones[z].v[k] = zn.v[k];
     for (int f = zn.ifa_f; f <= zn.ifa_l; f++) bzone[f] = z;
   }
@@ -297,7 +312,7 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
       }
     }
   }
-  h->ell_elems = (size_t)rows * 25 * SLICE;
+  h->ell_elems = (size_t)rows * bs * bs * SLICE;
   // greedy colouring of the cell graph (neighbours through internal faces), in cell order
   std::vector<uint8_t> color(N, 0);
   int ncolors = 1;
@@ -348,21 +363,22 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(dmalloc(h, &st.mul_fa, (size_t)nfa));
   RC(dmalloc(h, &st.lam_fa, (size_t)nfa));
   RC(dmalloc(h, &st.gu, 9 * (size_t)N));
-  int separate = h->p.viscous && h->p.second_order && !h->p.visc_limiter && h->p.limiter;
+  int separate = h->p.viscous && h->p.second_order && !h->p.visc_limiter && h->p.limiter && bs == 5;
   if (separate) RC(dmalloc(h, &st.guv, 9 * (size_t)N));
   else st.guv = st.gu;
   RC(dmalloc(h, &st.grho, 3 * (size_t)N));
   RC(dmalloc(h, &st.gp, 3 * (size_t)N));
   RC(dmalloc(h, &st.gh, 3 * (size_t)N));
   RC(dmalloc(h, &st.local_dt, (size_t)N));
-  RC(dmalloc(h, &st.rhs, 5 * (size_t)N));
-  RC(dmalloc(h, &st.b, 5 * (size_t)N));
-  RC(dmalloc_bytes(h, &st.D, 25 * (size_t)N * h->eltsz));
-  RC(dmalloc_bytes(h, &st.Dinv, 25 * (size_t)N * h->eltsz));
+  RC(dmalloc(h, &st.rhs, bs * (size_t)N));
+  RC(dmalloc(h, &st.b, bs * (size_t)N));
+  RC(dmalloc_bytes(h, &st.D, bs * bs * (size_t)N * h->eltsz));
+  RC(dmalloc_bytes(h, &st.Dinv, bs * bs * (size_t)N * h->eltsz));
   RC(dmalloc_bytes(h, &st.O, h->ell_elems * h->eltsz));
-  RC(dmalloc_bytes(h, &st.x0, 5 * (size_t)N * h->eltsz));
-  RC(dmalloc_bytes(h, &st.x1, 5 * (size_t)N * h->eltsz));
-  RC(dmalloc(h, &st.dq, 5 * (size_t)N));
+  RC(dmalloc_bytes(h, &st.x0, bs * (size_t)N * h->eltsz));
+  RC(dmalloc_bytes(h, &st.x1, bs * (size_t)N * h->eltsz));
+  RC(dmalloc(h, &st.dq, bs * (size_t)N));
+  st.bs = bs;
   // per-block partials: k_flux2 writes 5 per 16-cell block, k_dt 1 per 256-cell block
   RC(dmalloc(h, &st.blk, 5 * (size_t)grid_for(N, 16) + 5 * (size_t)grid_for(N, 256) + 16));
   RC(dmalloc(h, &st.ctrl, 16));
@@ -374,7 +390,7 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     h->case_nfa_b_off = {0, nfa_b};
   }
   h->ncases = (int)h->case_off.size() - 1;
-  RC(dmalloc(h, &st.resid, 5 * (size_t)h->hist_cap * h->ncases));
+  RC(dmalloc(h, &st.resid, bs * (size_t)h->hist_cap * h->ncases));
   {
     const int* d = nullptr;
     RC(upload(h, &d, h->case_off.data(), h->case_off.size()));
@@ -395,11 +411,34 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     h->d_rblk_off = (int*)d;
     RC(upload(h, &d, rblk_case.data(), rblk_case.size()));
     h->d_rblk_case = (int*)d;
-    RC(dmalloc(h, &st.rpart, 5 * (size_t)h->nrblk));
+    RC(dmalloc(h, &st.rpart, bs * (size_t)h->nrblk));
     std::vector<uint8_t> on(h->ncases, 1);
     const uint8_t* da = nullptr;
     RC(upload(h, &da, on.data(), on.size()));
     st.case_active = (uint8_t*)da;
+  }
+  if (bs == 6) {
+    // SA arrays, the WALL faces in zone order and the wall distance (initialHookScalarRansTurbModel)
+    Turb& t = h->turb;
+    RC(dmalloc(h, &t.phi, (size_t)N));
+    RC(dmalloc(h, &t.phi_bfa, (size_t)nfa_b));
+    RC(dmalloc(h, &t.grad_phi, 3 * (size_t)N));
+    RC(dmalloc(h, &t.diff, (size_t)nfa));
+    RC(dmalloc(h, &t.wd, (size_t)N));
+    RC(dmalloc(h, &t.strMag, (size_t)N));
+    RC(dmalloc(h, &t.vortMag, (size_t)N));
+    RC(dmalloc(h, &st.mut_fa, (size_t)nfa));
+    std::vector<int> wall;
+    for (int z = 0; z < mesh->nzones; z++)
+      if (mesh->zones[z].kind == JG_BC_WALL)
+        for (int f = mesh->zones[z].ifa_f; f <= mesh->zones[z].ifa_l; f++) wall.push_back(f);
+    if (wall.empty()) return set_err(JG_ERR_ARG, "the SA model needs a WALL zone (wall distance)");
+    const int* dw = nullptr;
+    RC(upload(h, &dw, wall.data(), wall.size()));
+    t.wall_f = dw;
+    t.nwall = (int)wall.size();
+    launch_wall_distance(h->m, t, h->stream);
+    CKL();
   }
   double ctrl0[16] = {0};
   ctrl0[0] = q->cfl;
@@ -434,6 +473,7 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
 static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
   const size_t N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b, nbs = mesh->nbocv_s;
   const size_t e = q->precision == JG_PREC_MIXED ? 4 : 8;
+  const size_t bs = q->turb_model == JG_TURB_SA ? 6 : 5, b2 = bs * bs;
   const int* fi = mesh->faocv_i;
   const int* fv = mesh->faocv_v;
   size_t nbslot = 0, rows = 0;
@@ -456,17 +496,25 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
       nfa_b * i, nz * sizeof(DevZone), (nslices + 1) * i, rows * SLICE * i, rows * SLICE, N,
       // state
       5 * N * d, 8 * N * d, 8 * nfa_b * d, nfa * d, nfa * d, 9 * N * d,
-      (q->mu_ref > 0.0 && q->second_order && !q->visc_limiter && q->limiter) ? 9 * N * d : 0,
-      3 * N * d, 3 * N * d, 3 * N * d, N * d, 5 * N * d, 5 * N * d,
-      25 * N * e, 25 * N * e, rows * 25 * SLICE * e, 5 * N * e, 5 * N * e, 5 * N * d,
+      (q->mu_ref > 0.0 && q->second_order && !q->visc_limiter && q->limiter && bs == 5) ? 9 * N * d : 0,
+      3 * N * d, 3 * N * d, 3 * N * d, N * d, bs * N * d, bs * N * d,
+      b2 * N * e, b2 * N * e, rows * b2 * SLICE * e, bs * N * e, bs * N * e, bs * N * d,
       (5 * (size_t)grid_for((int)N, 16) + 5 * (size_t)grid_for((int)N, 256) + 16) * d, 16 * d, 4 * i,
-      5 * 64 * d, 2 * i, N * i, 1 * i, 1,
-      2 * i, ((N + RCHUNK - 1) / RCHUNK) * i, 5 * ((N + RCHUNK - 1) / RCHUNK) * d,
+      bs * 64 * d, 2 * i, N * i, 1 * i, 1,
+      2 * i, ((N + RCHUNK - 1) / RCHUNK) * i, bs * ((N + RCHUNK - 1) / RCHUNK) * d,
       // state staging (jg_set_state / jg_get_state)
       5 * N * d};
   size_t b = 0;
   for (size_t x : a)
     if (x) b += alloc_round(x);
+  if (bs == 6) {
+    // SA arrays: phi, phi_bfa, grad_phi, diff, wall distance, strain, vorticity, mut_fa, wall faces
+    size_t nwall = 0;
+    for (int z = 0; z < mesh->nzones; z++)
+      if (mesh->zones[z].kind == JG_BC_WALL) nwall += mesh->zones[z].ifa_l - mesh->zones[z].ifa_f + 1;
+    const size_t t[] = {N * d, nfa_b * d, 3 * N * d, nfa * d, N * d, N * d, N * d, nfa * d, nwall * i};
+    for (size_t x : t) b += alloc_round(x);
+  }
   return b;
 }
 
@@ -574,6 +622,7 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (ncases <= 0 || !meshes || !out) return set_err(JG_ERR_ARG, "bad argument");
   *out = nullptr;
   RC(check_params(params));
+  if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "batches hold laminar / inviscid cases");
   if (params->lin_solver == JG_LS_BCGSTAB)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
   if (params->time_step_mode == JG_TS_CFL_MIN)
@@ -659,6 +708,10 @@ static int prime(jg_case* h) {
   launch_state(h->m, h->p, h->st, h->stream);
   launch_face_props(h->m, h->p, h->st, h->stream);
   launch_bc(h->m, h->p, h->st, h->stream);
+  if (h->bs == 6) {
+    launch_scalar_bc(h->m, h->st, h->turb, h->stream);
+    launch_turb_props(h->m, h->p, h->st, h->turb, h->stream);
+  }
   CKL();
   h->primed = 1;
   return check_err_flags(h);
@@ -747,27 +800,27 @@ int jg_calc_dt(jg_case_t* h, double cfl, double* dt_min, double* local_dt) {
 
 // device D/O (sliced ELL) -> reference block CSR A[nbocv_s][5][5]
 static int download_csr(jg_case* h, double* A) {
-  const int N = h->ncv;
+  const int N = h->ncv, bs = h->bs, b2 = bs * bs;
   size_t es = h->eltsz;
-  std::vector<char> D(25 * (size_t)N * es), O(h->ell_elems * es);
+  std::vector<char> D(b2 * (size_t)N * es), O(h->ell_elems * es);
   CK(cudaMemcpyAsync(D.data(), h->st.D, D.size(), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(O.data(), h->st.O, O.size(), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   auto get = [&](const std::vector<char>& v, size_t i) -> double {
     return es == 8 ? ((const double*)v.data())[i] : (double)((const float*)v.data())[i];
   };
-  memset(A, 0, sizeof(double) * 25 * (size_t)h->nbs);
+  memset(A, 0, sizeof(double) * b2 * (size_t)h->nbs);
   for (int c = 0; c < N; c++) {
     int kd = h->nbocv_i[c];
-    for (int e = 0; e < 25; e++) A[25 * (size_t)kd + e] = get(D, (size_t)e * N + c);
+    for (int e = 0; e < b2; e++) A[b2 * (size_t)kd + e] = get(D, (size_t)e * N + c);
     int s = c / SLICE, lane = c % SLICE;
     for (int j = 0; j < h->cell_cols[c + 1] - h->cell_cols[c]; j++) {
       int nb = h->col_nb[h->cell_cols[c] + j];
       int k = kd + 1;
       while (k < h->nbocv_i[c + 1] && h->nbocv_v[k] != nb) k++;
       if (k >= h->nbocv_i[c + 1]) return set_err(JG_ERR_ARG, "neighbour %d of cell %d missing from nbocv", nb, c);
-      for (int e = 0; e < 25; e++)
-        A[25 * (size_t)k + e] += get(O, ((size_t)(h->ell_off[s] + j) * 25 + e) * SLICE + lane);
+      for (int e = 0; e < b2; e++)
+        A[b2 * (size_t)k + e] += get(O, ((size_t)(h->ell_off[s] + j) * b2 + e) * SLICE + lane);
     }
   }
   return JG_OK;
@@ -806,6 +859,7 @@ static int upload_csr(jg_case* h, const double* A) {
 
 int jg_calc_rhs(jg_case_t* h, double* rhs_rho, double* rhs_rhou, double* rhs_rhoE, double* A, int flagImplicit) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (h->bs != 5) return set_err(JG_ERR_ARG, "a turbulence-model case assembles with jg_calc_rhs_coupled");
   if (!h->primed) RC(prime(h));
   int implicit = flagImplicit && A != nullptr;
   launch_grad(h->m, h->p, h->st, h->stream);
@@ -921,6 +975,7 @@ static void to_soa(const double* aos, std::vector<double>& soa, int N) {
 int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rhs, double zeroAbs, double zeroRel,
                      int maxIter, int* iters) {
   if (!h || !dq || !A || !rhs) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs != 5) return set_err(JG_ERR_ARG, "jg_solve_lin_sys takes the 5x5 system");
   const int N = h->ncv;
   RC(upload_csr(h, A));
   launch_dinv(h->m, h->p, h->st, h->stream);
@@ -969,7 +1024,32 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
 }
 
 // one backward-Euler iteration on the device (runBackwardEuler loop body)
+// one runBackwardEulerCoupled iteration (JoeWithModels.cpp:4416-4529) with the SA model
+static int enqueue_step_coupled(jg_case* h) {
+  cudaStream_t S = h->stream;
+  launch_ctrl_step(h->p, h->st, S);
+  launch_dt(h->m, h->p, h->st, 1, 0.0, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
+  launch_flux6(h->m, h->p, h->st, h->turb, 1, 1, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
+  launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
+  int sgs = h->hp.lin_solver == JG_LS_SGS;
+  int sweeps = std::max(1, h->hp.ls_max_iter);
+  launch_relax6(h->m, h->p, h->st, sgs, sweeps, S);
+  if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
+  launch_update6(h->m, h->p, h->st, h->turb, (sgs || sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
+  launch_state(h->m, h->p, h->st, S);
+  launch_face_props(h->m, h->p, h->st, S);
+  launch_bc(h->m, h->p, h->st, S);
+  launch_scalar_bc(h->m, h->st, h->turb, S);
+  launch_turb_props(h->m, h->p, h->st, h->turb, S);
+  CKL();
+  return JG_OK;
+}
+
 static int enqueue_step(jg_case* h, int for_graph) {
+  if (h->bs == 6) return enqueue_step_coupled(h);
   cudaStream_t S = h->stream;
   launch_ctrl_step(h->p, h->st, S);
   launch_dt(h->m, h->p, h->st, 1, 0.0, S);
@@ -1051,7 +1131,7 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   if (nsteps > h->hist_cap) {
     int cap = std::max(nsteps, 2 * h->hist_cap);
     double* r = nullptr;
-    RC(dmalloc(h, &r, 5 * (size_t)cap * h->ncases));
+    RC(dmalloc(h, &r, h->bs * (size_t)cap * h->ncases));
     h->st.resid = r;
     h->hist_cap = cap;
     h->st.hist_cap = cap;
@@ -1076,7 +1156,7 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   RC(check_err_flags(h));
   if (resid && nsteps > 0) {
     if (h->ncases == 1) {
-      CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(resid, h->st.resid, h->bs * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
     } else {
       // the sum over the cases of the batch, per step
       std::vector<double> all(5 * (size_t)nsteps * h->ncases);
@@ -1174,6 +1254,55 @@ int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// coupled path (turbulence model): scalars, calcRhsCoupled, model arrays
+// ---------------------------------------------------------------------------
+extern "C" int jg_set_scalars(jg_case_t* h, const double* phi) {
+  if (!h || !phi) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the case transports no scalar");
+  CK(cudaMemcpyAsync(h->turb.phi, phi, (size_t)h->ncv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->primed = 0;  // the scalar boundary values and the turbulent viscosity follow at the next call
+  return JG_OK;
+}
+
+extern "C" int jg_get_scalars(jg_case_t* h, double* phi) {
+  if (!h || !phi) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the case transports no scalar");
+  CK(cudaMemcpyAsync(phi, h->turb.phi, (size_t)h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+extern "C" int jg_calc_rhs_coupled(jg_case_t* h, double* rhs, double* A, int flagImplicit) {
+  if (!h || !rhs) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "a case without a turbulence model assembles with jg_calc_rhs");
+  if (!h->primed) RC(prime(h));
+  int implicit = flagImplicit && A != nullptr;
+  launch_flux6(h->m, h->p, h->st, h->turb, implicit, 0, h->stream);
+  CKL();
+  CK(cudaMemcpyAsync(rhs, h->st.rhs, (size_t)h->bs * h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (implicit) RC(download_csr(h, A));
+  return check_err_flags(h);
+}
+
+extern "C" int jg_get_turb(jg_case_t* h, double* wallDist, double* mut_fa, double* strMag, double* vortMag,
+                           double* phi_bfa, double* grad_phi, double* diff) {
+  if (!h) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the case has no turbulence model");
+  if (!h->primed) RC(prime(h));
+  const size_t N = h->ncv;
+  struct { double* dst; const double* src; size_t n; } t[] = {
+      {wallDist, h->turb.wd, N}, {mut_fa, h->st.mut_fa, (size_t)h->nfa}, {strMag, h->turb.strMag, N},
+      {vortMag, h->turb.vortMag, N}, {phi_bfa, h->turb.phi_bfa, (size_t)h->nfa_b},
+      {grad_phi, h->turb.grad_phi, 3 * N}, {diff, h->turb.diff, (size_t)h->nfa}};
+  for (auto& e : t)
+    if (e.dst) CK(cudaMemcpyAsync(e.dst, e.src, e.n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // per-case operations of the serving engine (jg_serve.cu): nothing here waits
 // on the device, so one host thread can keep many cases in flight
 // ---------------------------------------------------------------------------
@@ -1185,6 +1314,7 @@ int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** ou
   RC(check_params(params));
   if (params->lin_solver == JG_LS_BCGSTAB)
     return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
+  if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "served cases are laminar / inviscid");
   if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
     return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
   jg_case* h = new jg_case();

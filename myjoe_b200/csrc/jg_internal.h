@@ -18,7 +18,7 @@ constexpr int SLICE = 32;
 
 struct DevZone {
   int kind;
-  int pad;
+  int scal_bc;      // bit 0: the transported scalar is Dirichlet (value v[6]) on this zone
   double v[8];
 };
 
@@ -85,6 +85,21 @@ struct State {
   int* err;         // error flags
   int* case_err;    // [ncases] per-case error flags (1: rho/p <= 0, 4: NaN residual)
   uint8_t* case_active;  // [ncases] 0: case frozen (retired), its state is not updated
+  double* mut_fa;   // [nfa] turbulent viscosity (coupled SA path), nullptr without a model
+  int bs;           // block size of the system: 5, or 6 with SA (rhs, b, dq, x, D, O, resid use it)
+};
+
+// Spalart-Allmaras scalar and model arrays (coupled path only)
+struct Turb {
+  double* phi;       // [N] nuSA
+  double* phi_bfa;   // [nfa_b]
+  double* grad_phi;  // [N][3] (limited like the flow gradients)
+  double* diff;      // [nfa] scalar diffusivity (mu + rho nuSA) / sigma
+  double* wd;        // [N] wall distance
+  double* strMag;    // [N]
+  double* vortMag;   // [N]
+  const int* wall_f; // [nwall] WALL faces in zone order
+  int nwall;
 };
 
 struct Params {
@@ -101,6 +116,7 @@ struct Params {
   double under_relax;
   int viscous;      // mu_ref > 0
   int fp32;         // matrix + relaxation in FP32
+  int turb;         // JG_TURB_*
 };
 
 // launchers (jg_kernels.cu); all enqueue on stream s
@@ -142,6 +158,22 @@ void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s);
 int grid_for(long n, int block);
 int record_error(int code, const char* msg);  // sets the jg_last_error message
 
+}  // namespace jg
+
+namespace jg {
+// coupled Spalart-Allmaras path (jg_coupled.cu), block size 6
+void launch_wall_distance(const Mesh& m, Turb& t, cudaStream_t s);
+void launch_scalar_bc(const Mesh& m, State& st, Turb& t, cudaStream_t s);
+// gradients of the flow (limited, as calcFluxCoupled takes them) and of nuSA,
+// strain/vorticity magnitudes, turbulent viscosity and scalar diffusivity
+void launch_turb_props(const Mesh& m, const Params& p, State& st, Turb& t, cudaStream_t s);
+// calcRhsCoupled + the implicit-step epilogue: rhs[N][6], D/O (6x6), b, Dinv
+void launch_flux6(const Mesh& m, const Params& p, State& st, Turb& t, int implicit, int for_step, cudaStream_t s);
+void launch_relax6(const Mesh& m, const Params& p, State& st, int sgs, int sweeps, cudaStream_t s);
+// Q += dq (x: the relaxation result, [6][N]), nuSA = clip((nuSA (rho_new - dq0) + dq5) / rho_new)
+void launch_update6(const Mesh& m, const Params& p, State& st, Turb& t, const void* x, cudaStream_t s);
+// the flow gradients as calcFluxCoupled takes them (jg_kernels.cu)
+void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 }  // namespace jg
 
 // per-case operations used by the serving engine (defined in jg_api.cu)

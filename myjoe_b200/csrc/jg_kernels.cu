@@ -231,7 +231,8 @@ __global__ void k_dt(Mesh m, Params p, State st, int use_ctrl, double cfl_arg) {
           unit_normal(m, f, nV, area);
           double Uk = dot3(ru, nV) / r;
           double lam = (fabs(Uk) + cs) * area;
-          double ld = p.viscous ? 4.0 * (st.mul_fa[f] + 0.0) / r * area * area / vol : 0.0;
+          double mut = st.mut_fa ? st.mut_fa[f] : 0.0;
+          double ld = p.viscous ? 4.0 * (st.mul_fa[f] + mut) / r * area * area / vol : 0.0;
           lam = fmax(lam, ld);
           lmax = fmax(lmax, lam);
         }
@@ -246,7 +247,8 @@ __global__ void k_dt(Mesh m, Params p, State st, int use_ctrl, double cfl_arg) {
           double v2 = (s.nb >= 0) ? 0.5 * (m.vol[c] + m.vol[s.nb]) : 0.5 * vol;
           if (s.nb >= 0 && s.side == 1) v2 = 0.5 * (m.vol[s.nb] + m.vol[c]);
           lc += (fabs(Uk) + cs) * area;
-          if (p.viscous) ld += area * area * ((4.0 / 3.0) * (st.mul_fa[s.f] + 0.0) / r) / v2;
+          double mut = st.mut_fa ? st.mut_fa[s.f] : 0.0;
+          if (p.viscous) ld += area * area * ((4.0 / 3.0) * (st.mul_fa[s.f] + mut) / r) / v2;
         }
         double dconv = cfl * vol / lc;
         double dvisc = p.viscous ? 0.25 * cfl * vol / ld : 1.0e20;
@@ -812,45 +814,53 @@ __global__ void k_resid_final(State st, int nblk, int hist_from_ctrl) {
 // Per-case L1 residual: block k sums |RHS| over the cells of case k in a fixed
 // order that depends only on that case, so a case's residual history is the
 // same alone and inside a batch.  out[(idx*ncases + k)*5 + i].
-__global__ void __launch_bounds__(320) k_resid_chunks(State st, const int* __restrict__ case_off,
-                                                       const int* __restrict__ rblk_off,
-                                                       const int* __restrict__ rblk_case) {
-  __shared__ double s[320];
+template <int B>
+__global__ void __launch_bounds__(64 * B) k_resid_chunks(State st, const int* __restrict__ case_off,
+                                                         const int* __restrict__ rblk_off,
+                                                         const int* __restrict__ rblk_case) {
+  constexpr int T = 64 * B;
+  __shared__ double s[T];
   const int b = blockIdx.x, t = threadIdx.x;
   const int k = rblk_case[b];
   const long c0 = case_off[k] + (long)(b - rblk_off[k]) * RCHUNK;
   const long c1 = min((long)case_off[k + 1], c0 + RCHUNK);
-  const double* r = st.rhs + 5 * c0;
-  const long n = 5 * (c1 - c0);
-  double v = 0.0;  // stride 320 = 64 x 5: thread t always sums component t % 5
-  for (long e = t; e < n; e += 320) v += fabs(r[e]);
+  const double* r = st.rhs + B * c0;
+  const long n = B * (c1 - c0);
+  double v = 0.0;  // stride 64 x B: thread t always sums component t % B
+  for (long e = t; e < n; e += T) v += fabs(r[e]);
   s[t] = v;
   __syncthreads();
   for (int w = 32; w > 0; w >>= 1) {  // fixed-order tree over the 64 threads of each component
-    if (t / 5 < w) s[t] += s[t + 5 * w];
+    if (t / B < w) s[t] += s[t + B * w];
     __syncthreads();
   }
-  if (t < 5) st.rpart[5 * b + t] = s[t];
+  if (t < B) st.rpart[B * b + t] = s[t];
 }
+template <int B>
 __global__ void k_resid_cases(State st, const int* __restrict__ rblk_off, int ncases, int hist_from_ctrl) {
   const int k = blockIdx.x, lane = threadIdx.x;
-  double v[5] = {0, 0, 0, 0, 0};
+  double v[B];
+  for (int i = 0; i < B; i++) v[i] = 0.0;
   for (int b = rblk_off[k] + lane; b < rblk_off[k + 1]; b += 32)
-    for (int i = 0; i < 5; i++) v[i] += st.rpart[5 * b + i];
+    for (int i = 0; i < B; i++) v[i] += st.rpart[B * b + i];
   for (int o = 16; o > 0; o >>= 1)
-    for (int i = 0; i < 5; i++) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+    for (int i = 0; i < B; i++) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
   if (lane == 0) {
     long idx = hist_from_ctrl ? (long)st.ctrl[1] - (long)st.ctrl[4] - 1 : 0;
     idx = ((idx % st.hist_cap) + st.hist_cap) % st.hist_cap;  // ring buffer
-    for (int i = 0; i < 5; i++) st.resid[(idx * ncases + k) * 5 + i] = v[i];
-    if (!(v[4] == v[4]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN residual (doneSolver)
+    for (int i = 0; i < B; i++) st.resid[(idx * ncases + k) * B + i] = v[i];
+    if (!(v[4] == v[4]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN energy residual (doneSolver)
   }
 }
-
 void launch_resid_cases(State& st, const int* case_off, const int* rblk_off, const int* rblk_case, int nrblk,
                         int ncases, int hist_from_ctrl, cudaStream_t s) {
-  k_resid_chunks<<<nrblk, 320, 0, s>>>(st, case_off, rblk_off, rblk_case);
-  k_resid_cases<<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
+  if (st.bs == 6) {
+    k_resid_chunks<6><<<nrblk, 64 * 6, 0, s>>>(st, case_off, rblk_off, rblk_case);
+    k_resid_cases<6><<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
+  } else {
+    k_resid_chunks<5><<<nrblk, 64 * 5, 0, s>>>(st, case_off, rblk_off, rblk_case);
+    k_resid_cases<5><<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1158,6 +1168,11 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   int visc_lim = p.visc_limiter && p.limiter;
   int separate = do_visc && do_euler && !p.visc_limiter && p.limiter;
   k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate);
+}
+// calcFluxCoupled (JoeWithModels.cpp:4683-4702): grad_u (second order or viscous), grad_rho,
+// grad_p (second order) and grad_enthalpy (viscous), all with the flow limiter; one grad_u
+void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, p.second_order, 1, p.limiter, p.limiter, 0);
 }
 constexpr int FLUX_CELLS = 128 / FL;  // cells per k_flux2 block
 // residual only: 8 lanes per cell (light kernel, many warps)

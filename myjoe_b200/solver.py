@@ -69,6 +69,10 @@ def lib():
         L.jg_set_profiling.argtypes = [P, I]
         L.jg_get_profile.argtypes = [P, D]
         L.jg_step_kernel_count.argtypes = [P, C.POINTER(I)]
+        L.jg_set_scalars.argtypes = [P, D]
+        L.jg_get_scalars.argtypes = [P, D]
+        L.jg_calc_rhs_coupled.argtypes = [P, D, D, I]
+        L.jg_get_turb.argtypes = [P, D, D, D, D, D, D, D]
         L.jg_case_footprint.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), D]
         L.jg_case_device_bytes.argtypes = [P, D]
         L.jg_serve_create.argtypes = [C.POINTER(jg_serve_config), C.POINTER(P)]
@@ -182,10 +186,41 @@ class JoeGpu:
                                    C.byref(it)))
         return dq, it.value
 
+    # -- coupled path (turbulence model) -------------------------------------
+    @property
+    def nvar(self) -> int:
+        return 5 + self.params.nscal
+
+    def set_scalars(self, phi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        _ck(lib().jg_set_scalars(self.h, dptr(phi)))
+
+    def get_scalars(self):
+        phi = np.empty(self.ncv)
+        _ck(lib().jg_get_scalars(self.h, dptr(phi)))
+        return phi
+
+    def calcRhsCoupled(self, flagImplicit=True):
+        """rhs[ncv][6], A[nbocv_s][6][6] (None without flagImplicit)."""
+        B = self.nvar
+        rhs = np.zeros((self.ncv, B))
+        A = np.zeros((self.ma.nbocv_s, B, B)) if flagImplicit else None
+        _ck(lib().jg_calc_rhs_coupled(self.h, dptr(rhs), _p(A), int(flagImplicit)))
+        return rhs, A
+
+    def turb(self):
+        """wallDist, mut_fa, strMag, vortMag, phi_bfa, grad_phi, diff of the current state."""
+        n, nf, nb = self.ncv, self.ma.nfa, self.ma.nfa_b
+        out = {"wallDist": np.empty(n), "mut_fa": np.empty(nf), "strMag": np.empty(n), "vortMag": np.empty(n),
+               "phi_bfa": np.empty(nb), "grad_phi": np.empty((n, 3)), "diff": np.empty(nf)}
+        _ck(lib().jg_get_turb(self.h, *(dptr(out[k]) for k in ("wallDist", "mut_fa", "strMag", "vortMag",
+                                                                  "phi_bfa", "grad_phi", "diff"))))
+        return out
+
     def runBackwardEuler(self, nsteps):
         """``nsteps`` iterations of the backward-Euler loop; returns the L1
-        residual history [nsteps][5]."""
-        r = np.zeros((max(nsteps, 1), 5))
+        residual history [nsteps][5] ([nsteps][6] on the coupled SA path)."""
+        r = np.zeros((max(nsteps, 1), self.nvar))
         _ck(lib().jg_step(self.h, int(nsteps), dptr(r)))
         return r[:nsteps]
 

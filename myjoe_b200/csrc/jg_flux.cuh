@@ -9,16 +9,30 @@
 
 namespace jg {
 
-struct FState {
-  double rho, u[3], p, gam;
+// face state; the implicit matrices are templated on the arithmetic type (FP64
+// for the plain form, FP32 for the preconditioner of the mixed form)
+template <typename T>
+struct FStateT {
+  T rho, u[3], p, gam;
 };
+using FState = FStateT<double>;
 
-__device__ __forceinline__ double dot3(const double* a, const double* b) {
-  double d = 0.0;
+template <typename T>
+__device__ __forceinline__ T dot3(const T* a, const T* b) {
+  T d = T(0.0);
   d += a[0] * b[0];
   d += a[1] * b[1];
   d += a[2] * b[2];
   return d;
+}
+template <typename T>
+__device__ __forceinline__ FStateT<T> fstate_as(const FState& s) {
+  FStateT<T> o;
+  o.rho = (T)s.rho;
+  for (int i = 0; i < 3; i++) o.u[i] = (T)s.u[i];
+  o.p = (T)s.p;
+  o.gam = (T)s.gam;
+  return o;
 }
 
 // calcEulerFlux_HLLC, src/joe/UgpWithCvCompFlow.cpp:120-235 (k = 0, no scalars)
@@ -78,32 +92,33 @@ __device__ inline void flux_hllc(double F[5], const FState& L, const FState& R, 
 }
 
 // calcJacobianA, UgpWithCvCompFlow.cpp:666-709; nV carries the face area
-__device__ inline void jacobian_A(double* A, const double* vel, double pp, double rrho, const double* nV, double gamma) {
-  double km1 = gamma - 1.0;
-  double nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
-  double U_k = nVel[0] + nVel[1] + nVel[2];
-  double vsh = 0.5 * dot3(vel, vel);
-  double c2 = gamma * pp / rrho;  // c*c with c = sqrt(gamma p / rho)
-  double c = sqrt(c2);
+template <typename T>
+__device__ inline void jacobian_A(T* A, const T* vel, T pp, T rrho, const T* nV, T gamma) {
+  T km1 = gamma - T(1.0);
+  T nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
+  T U_k = nVel[0] + nVel[1] + nVel[2];
+  T vsh = T(0.5) * dot3(vel, vel);
+  T c2 = gamma * pp / rrho;  // c*c with c = sqrt(gamma p / rho)
+  T c = sqrt(c2);
   c2 = c * c;
-  double ikm1 = 1.0 / km1;
-  A[0] = 0.0; A[1] = nV[0]; A[2] = nV[1]; A[3] = nV[2]; A[4] = 0.0;
+  T ikm1 = T(1.0) / km1;
+  A[0] = T(0.0); A[1] = nV[0]; A[2] = nV[1]; A[3] = nV[2]; A[4] = T(0.0);
   A[5] = -vel[0] * (nVel[1] + nVel[2]) + nV[0] * (km1 * vsh - vel[0] * vel[0]);
-  A[6] = (2. - gamma) * nVel[0] + U_k;
+  A[6] = (T(2.) - gamma) * nVel[0] + U_k;
   A[7] = vel[0] * nV[1] - km1 * vel[1] * nV[0];
   A[8] = vel[0] * nV[2] - km1 * vel[2] * nV[0];
   A[9] = km1 * nV[0];
   A[10] = -vel[1] * (nVel[0] + nVel[2]) + nV[1] * (km1 * vsh - vel[1] * vel[1]);
   A[11] = -km1 * vel[0] * nV[1] + vel[1] * nV[0];
-  A[12] = (2. - gamma) * nVel[1] + U_k;
+  A[12] = (T(2.) - gamma) * nVel[1] + U_k;
   A[13] = vel[1] * nV[2] - km1 * vel[2] * nV[1];
   A[14] = km1 * nV[1];
   A[15] = -vel[2] * (nVel[0] + nVel[1]) + nV[2] * (km1 * vsh - vel[2] * vel[2]);
   A[16] = -km1 * vel[0] * nV[2] + vel[2] * nV[0];
   A[17] = -km1 * vel[1] * nV[2] + vel[2] * nV[1];
-  A[18] = (2. - gamma) * nVel[2] + U_k;
+  A[18] = (T(2.) - gamma) * nVel[2] + U_k;
   A[19] = km1 * nV[2];
-  A[20] = U_k * ((gamma - 2.) * vsh - c2 * ikm1);
+  A[20] = U_k * ((gamma - T(2.)) * vsh - c2 * ikm1);
   A[21] = c2 * ikm1 * nV[0] - km1 * vel[0] * (nVel[1] + nVel[2]) - (km1 * vel[0] * vel[0] - vsh) * nV[0];
   A[22] = c2 * ikm1 * nV[1] - km1 * vel[1] * (nVel[0] + nVel[2]) - (km1 * vel[1] * vel[1] - vsh) * nV[1];
   A[23] = c2 * ikm1 * nV[2] - km1 * vel[2] * (nVel[0] + nVel[1]) - (km1 * vel[2] * vel[2] - vsh) * nV[2];
@@ -112,12 +127,13 @@ __device__ inline void jacobian_A(double* A, const double* vel, double pp, doubl
 
 // calcSubSonicJacobeanHLLC, UgpWithCvCompFlow.cpp:605-659.  "S" is the side
 // whose star state is used (L when sM >= 0); "O" the other side.  AS/AO may be null.
-__device__ inline void subsonic_jac(double* AS, double* AO, double rhoS, const double* uS, double pS_, double eS_,
-                                    double qS, double psiS, double SS, double rhoSt, const double* rhouSt, double eSt,
-                                    const double* dSMdS, const double* dSMdO, const double* dpsdS, const double* dpsdO,
-                                    double SM, double pStar, double gamma, const double* nV) {
-  double gm1 = gamma - 1.0;
-  double om = 1.0 / (SS - SM);
+template <typename T>
+__device__ inline void subsonic_jac(T* AS, T* AO, T rhoS, const T* uS, T pS_, T eS_,
+                                    T qS, T psiS, T SS, T rhoSt, const T* rhouSt, T eSt,
+                                    const T* dSMdS, const T* dSMdO, const T* dpsdS, const T* dpsdO,
+                                    T SM, T pStar, T gamma, const T* nV) {
+  T gm1 = gamma - T(1.0);
+  T om = T(1.0) / (SS - SM);
   if (AS) {
     AS[0] = SS + rhoSt * dSMdS[0];
     AS[1] = -nV[0] + rhoSt * dSMdS[1];
@@ -125,15 +141,15 @@ __device__ inline void subsonic_jac(double* AS, double* AO, double rhoS, const d
     AS[3] = -nV[2] + rhoSt * dSMdS[3];
     AS[4] = +rhoSt * dSMdS[4];
     for (int r = 0; r < 3; r++) {
-      double* row = AS + 5 * (r + 1);
-      row[0] = qS * uS[r] - nV[r] * psiS * gm1 / 2.0 + nV[r] * dpsdS[0] + rhouSt[r] * dSMdS[0];
+      T* row = AS + 5 * (r + 1);
+      row[0] = qS * uS[r] - nV[r] * psiS * gm1 / T(2.0) + nV[r] * dpsdS[0] + rhouSt[r] * dSMdS[0];
       for (int k = 0; k < 3; k++) {
-        double base = (k == r) ? (SS - qS + nV[r] * (gamma - 2.0) * uS[r]) : (-uS[r] * nV[k] + nV[r] * gm1 * uS[k]);
+        T base = (k == r) ? (SS - qS + nV[r] * (gamma - T(2.0)) * uS[r]) : (-uS[r] * nV[k] + nV[r] * gm1 * uS[k]);
         row[1 + k] = base + nV[r] * dpsdS[1 + k] + rhouSt[r] * dSMdS[1 + k];
       }
       row[4] = -gm1 * nV[r] + nV[r] * dpsdS[4] + rhouSt[r] * dSMdS[4];
     }
-    AS[20] = qS * (eS_ + pS_) / rhoS - qS * psiS * (gamma - 1.0) / 2.0 + SM * dpsdS[0] + (pStar + eSt) * dSMdS[0];
+    AS[20] = qS * (eS_ + pS_) / rhoS - qS * psiS * (gamma - T(1.0)) / T(2.0) + SM * dpsdS[0] + (pStar + eSt) * dSMdS[0];
     for (int k = 0; k < 3; k++)
       AS[21 + k] = -nV[k] * (eS_ + pS_) / rhoS + gm1 * uS[k] * qS + SM * dpsdS[1 + k] + (pStar + eSt) * dSMdS[1 + k];
     AS[24] = SS - qS * gamma + SM * dpsdS[4] + (pStar + eSt) * dSMdS[4];
@@ -148,57 +164,58 @@ __device__ inline void subsonic_jac(double* AS, double* AO, double rhoS, const d
 }
 
 // calcEulerFluxMatrices_HLLC, UgpWithCvCompFlow.cpp:242-595 (no scalars); AL/AR may be null
-__device__ inline void matrices_hllc(double* AL, double* AR, const FState& L, const FState& R, double area,
-                                     const double nV[3]) {
-  double unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u);
-  double cL = sqrt(L.gam * L.p / L.rho);
-  double eL = (L.gam / (L.gam - 1.0) * L.p / L.rho + 0.5 * uLuL) * L.rho - L.p;
-  double unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u);
-  double cR = sqrt(R.gam * R.p / R.rho);
-  double eR = (R.gam / (R.gam - 1.0) * R.p / R.rho + 0.5 * uRuR) * R.rho - R.p;
-  double Rrho = sqrt(R.rho / L.rho);
-  double tmp = 1.0 / (1.0 + Rrho);
-  double vr[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
-  double uRoe = dot3(vr, nV);
-  double gpr = tmp * ((L.gam * L.p / L.rho + 0.5 * (L.gam - 1.0) * uLuL) +
-                      (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
-  double cRoe = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(vr, vr));
-  double sL = fmin(uRoe - cRoe, unL - cL);
-  double sR = fmax(uRoe + cRoe, unR + cR);
-  double sM = (L.p - R.p - L.rho * unL * (sL - unL) + R.rho * unR * (sR - unR)) /
+template <typename T>
+__device__ inline void matrices_hllc(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area,
+                                     const T nV[3]) {
+  T unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u);
+  T cL = sqrt(L.gam * L.p / L.rho);
+  T eL = (L.gam / (L.gam - T(1.0)) * L.p / L.rho + T(0.5) * uLuL) * L.rho - L.p;
+  T unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u);
+  T cR = sqrt(R.gam * R.p / R.rho);
+  T eR = (R.gam / (R.gam - T(1.0)) * R.p / R.rho + T(0.5) * uRuR) * R.rho - R.p;
+  T Rrho = sqrt(R.rho / L.rho);
+  T tmp = T(1.0) / (T(1.0) + Rrho);
+  T vr[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
+  T uRoe = dot3(vr, nV);
+  T gpr = tmp * ((L.gam * L.p / L.rho + T(0.5) * (L.gam - T(1.0)) * uLuL) +
+                      (R.gam * R.p / R.rho + T(0.5) * (R.gam - T(1.0)) * uRuR) * Rrho);
+  T cRoe = sqrt(gpr - ((L.gam + R.gam) * T(0.5) - T(1.0)) * T(0.5) * dot3(vr, vr));
+  T sL = fmin(uRoe - cRoe, unL - cL);
+  T sR = fmax(uRoe + cRoe, unR + cR);
+  T sM = (L.p - R.p - L.rho * unL * (sL - unL) + R.rho * unR * (sR - unR)) /
               (R.rho * (sR - unR) - L.rho * (sL - unL));
-  double pStar = R.rho * (unR - sR) * (unR - sM) + R.p;
-  double gmean = 0.5 * (L.gam + R.gam);
-  if ((sM >= 0.0 && sL > 0.0) || (sM < 0.0 && sR < 0.0)) {
+  T pStar = R.rho * (unR - sR) * (unR - sM) + R.p;
+  T gmean = T(0.5) * (L.gam + R.gam);
+  if ((sM >= T(0.0) && sL > T(0.0)) || (sM < T(0.0) && sR < T(0.0))) {
     // supersonic: the flux depends on one side only
-    bool left = sM >= 0.0;
-    double* Aj = left ? AL : AR;
-    double* Az = left ? AR : AL;
-    const FState& S = left ? L : R;
+    bool left = sM >= T(0.0);
+    T* Aj = left ? AL : AR;
+    T* Az = left ? AR : AL;
+    const FStateT<T>& S = left ? L : R;
     if (Aj) {
-      double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+      T nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
       jacobian_A(Aj, S.u, S.p, S.rho, nA, gmean);
     }
     if (Az)
-      for (int i = 0; i < 25; i++) Az[i] = 0.0;
+      for (int i = 0; i < 25; i++) Az[i] = T(0.0);
     return;
   }
-  bool left = sM >= 0.0;  // star state of the left (sM >= 0) or right wave
-  const FState& S = left ? L : R;
-  double unS = left ? unL : unR, eS = left ? eL : eR, sS = left ? sL : sR;
-  double inv = 1.0 / (sS - sM);
-  double sSmu = sS - unS;
-  double rhoSt = S.rho * sSmu * inv;
-  double rhouSt[3];
+  bool left = sM >= T(0.0);  // star state of the left (sM >= 0) or right wave
+  const FStateT<T>& S = left ? L : R;
+  T unS = left ? unL : unR, eS = left ? eL : eR, sS = left ? sL : sR;
+  T inv = T(1.0) / (sS - sM);
+  T sSmu = sS - unS;
+  T rhoSt = S.rho * sSmu * inv;
+  T rhouSt[3];
   for (int i = 0; i < 3; i++) rhouSt[i] = (S.rho * S.u[i] * sSmu + (pStar - S.p) * nV[i]) * inv;
-  double eSt = (sSmu * eS - S.p * unS + pStar * sM) * inv;
-  double invrhotld = 1.0 / (R.rho * (sR - unR) - L.rho * (sL - unL));
-  double dSMdUL[5] = {0, 0, 0, 0, 0}, dSMdUR[5] = {0, 0, 0, 0, 0};
-  double dpsdUL[5] = {0, 0, 0, 0, 0}, dpsdUR[5] = {0, 0, 0, 0, 0};
+  T eSt = (sSmu * eS - S.p * unS + pStar * sM) * inv;
+  T invrhotld = T(1.0) / (R.rho * (sR - unR) - L.rho * (sL - unL));
+  T dSMdUL[5] = {0, 0, 0, 0, 0}, dSMdUR[5] = {0, 0, 0, 0, 0};
+  T dpsdUL[5] = {0, 0, 0, 0, 0}, dpsdUR[5] = {0, 0, 0, 0, 0};
   if (AL) {
-    double g1 = L.gam - 1.0;
-    dSMdUL[0] = -unL * unL + uLuL * g1 / 2.0 + sM * sL;
-    for (int i = 0; i < 3; i++) dSMdUL[1 + i] = nV[i] * (2.0 * unL - sL - sM) - g1 * L.u[i];
+    T g1 = L.gam - T(1.0);
+    dSMdUL[0] = -unL * unL + uLuL * g1 / T(2.0) + sM * sL;
+    for (int i = 0; i < 3; i++) dSMdUL[1 + i] = nV[i] * (T(2.0) * unL - sL - sM) - g1 * L.u[i];
     dSMdUL[4] = g1;
     for (int i = 0; i < 5; i++) {
       dSMdUL[i] *= invrhotld;
@@ -206,9 +223,9 @@ __device__ inline void matrices_hllc(double* AL, double* AR, const FState& L, co
     }
   }
   if (AR) {
-    double g1 = R.gam - 1.0;
-    dSMdUR[0] = unR * unR - uRuR * g1 / 2.0 - sM * sR;
-    for (int i = 0; i < 3; i++) dSMdUR[1 + i] = -nV[i] * (2.0 * unR - sR - sM) + g1 * R.u[i];
+    T g1 = R.gam - T(1.0);
+    dSMdUR[0] = unR * unR - uRuR * g1 / T(2.0) - sM * sR;
+    for (int i = 0; i < 3; i++) dSMdUR[1 + i] = -nV[i] * (T(2.0) * unR - sR - sM) + g1 * R.u[i];
     dSMdUR[4] = -g1;
     for (int i = 0; i < 5; i++) {
       dSMdUR[i] *= invrhotld;
@@ -222,10 +239,10 @@ __device__ inline void matrices_hllc(double* AL, double* AR, const FState& L, co
     subsonic_jac(AR, AL, R.rho, R.u, R.p, eR, unR, uRuR, sR, rhoSt, rhouSt, eSt, dSMdUR, dSMdUL, dpsdUR, dpsdUL, sM,
                  pStar, gmean, nV);
   for (int side = 0; side < 2; side++) {
-    double* A = side == 0 ? AL : AR;
+    T* A = side == 0 ? AL : AR;
     if (!A) continue;
-    const double* dSM = side == 0 ? dSMdUL : dSMdUR;
-    const double* dps = side == 0 ? dpsdUL : dpsdUR;
+    const T* dSM = side == 0 ? dSMdUL : dSMdUR;
+    const T* dps = side == 0 ? dpsdUL : dpsdUR;
     for (int i = 0; i < 5; i++) A[i] = A[i] * sM + dSM[i] * rhoSt;
     for (int r = 0; r < 3; r++)
       for (int i = 0; i < 5; i++) A[5 * (r + 1) + i] = A[5 * (r + 1) + i] * sM + dSM[i] * rhouSt[r] + dps[i] * nV[r];
@@ -278,90 +295,92 @@ __device__ inline void flux_roe(double F[5], const FState& L, const FState& R, d
 // UgpWithCvCompFlow.cpp:3382-3559; AL/AR may be null.  The dissipation matrix
 // P |Lambda| P^-1 is formed row by row (P row i generated on the fly) to keep
 // the live register set small; each entry is the same k-ordered sum.
-__device__ __forceinline__ void roe_p_row(double Pr[5], int i, const double* v, double rr, double rhooc, double rhoxc,
-                                          double km1, double vS, double vn, const double* nV) {
+template <typename T>
+__device__ __forceinline__ void roe_p_row(T Pr[5], int i, const T* v, T rr, T rhooc, T rhoxc,
+                                          T km1, T vS, T vn, const T* nV) {
   switch (i) {
-    case 0: Pr[0] = nV[0]; Pr[1] = nV[1]; Pr[2] = nV[2]; Pr[3] = 0.5 * rhooc; Pr[4] = 0.5 * rhooc; break;
+    case 0: Pr[0] = nV[0]; Pr[1] = nV[1]; Pr[2] = nV[2]; Pr[3] = T(0.5) * rhooc; Pr[4] = T(0.5) * rhooc; break;
     case 1:
       Pr[0] = v[0] * nV[0]; Pr[1] = v[0] * nV[1] - rr * nV[2]; Pr[2] = v[0] * nV[2] + rr * nV[1];
-      Pr[3] = 0.5 * (v[0] * rhooc + rr * nV[0]); Pr[4] = 0.5 * (v[0] * rhooc - rr * nV[0]); break;
+      Pr[3] = T(0.5) * (v[0] * rhooc + rr * nV[0]); Pr[4] = T(0.5) * (v[0] * rhooc - rr * nV[0]); break;
     case 2:
       Pr[0] = v[1] * nV[0] + rr * nV[2]; Pr[1] = v[1] * nV[1]; Pr[2] = v[1] * nV[2] - rr * nV[0];
-      Pr[3] = 0.5 * (v[1] * rhooc + rr * nV[1]); Pr[4] = 0.5 * (v[1] * rhooc - rr * nV[1]); break;
+      Pr[3] = T(0.5) * (v[1] * rhooc + rr * nV[1]); Pr[4] = T(0.5) * (v[1] * rhooc - rr * nV[1]); break;
     case 3:
       Pr[0] = v[2] * nV[0] - rr * nV[1]; Pr[1] = v[2] * nV[1] + rr * nV[0]; Pr[2] = v[2] * nV[2];
-      Pr[3] = 0.5 * (v[2] * rhooc + rr * nV[2]); Pr[4] = 0.5 * (v[2] * rhooc - rr * nV[2]); break;
+      Pr[3] = T(0.5) * (v[2] * rhooc + rr * nV[2]); Pr[4] = T(0.5) * (v[2] * rhooc - rr * nV[2]); break;
     default:
-      Pr[0] = 0.5 * vS * nV[0] + rr * v[1] * nV[2] - rr * v[2] * nV[1];
-      Pr[1] = 0.5 * vS * nV[1] - rr * v[0] * nV[2] + rr * v[2] * nV[0];
-      Pr[2] = 0.5 * vS * nV[2] + rr * v[0] * nV[1] - rr * v[1] * nV[0];
-      Pr[3] = 0.5 * (0.5 * vS * rhooc + rr * vn + rhoxc / km1);
-      Pr[4] = 0.5 * (0.5 * vS * rhooc - rr * vn + rhoxc / km1);
+      Pr[0] = T(0.5) * vS * nV[0] + rr * v[1] * nV[2] - rr * v[2] * nV[1];
+      Pr[1] = T(0.5) * vS * nV[1] - rr * v[0] * nV[2] + rr * v[2] * nV[0];
+      Pr[2] = T(0.5) * vS * nV[2] + rr * v[0] * nV[1] - rr * v[1] * nV[0];
+      Pr[3] = T(0.5) * (T(0.5) * vS * rhooc + rr * vn + rhoxc / km1);
+      Pr[4] = T(0.5) * (T(0.5) * vS * rhooc - rr * vn + rhoxc / km1);
       break;
   }
 }
 
-__device__ inline void matrices_roe(double* AL, double* AR, const FState& L, const FState& R, double area,
-                                    const double nV[3]) {
-  double uLuL = dot3(L.u, L.u), uRuR = dot3(R.u, R.u);
-  double Rrho = sqrt(R.rho / L.rho);
-  double rr = Rrho * L.rho;
-  double tmp = 1.0 / (1.0 + Rrho);
-  double v[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
-  double uRoe = dot3(v, nV);
-  double gpr = tmp * ((L.gam * L.p / L.rho + 0.5 * (L.gam - 1.0) * uLuL) +
-                      (R.gam * R.p / R.rho + 0.5 * (R.gam - 1.0) * uRuR) * Rrho);
-  double c = sqrt(gpr - ((L.gam + R.gam) * 0.5 - 1.0) * 0.5 * dot3(v, v));
-  double gamma = 0.5 * (L.gam + R.gam);
-  double km1 = gamma - 1.0;
-  double rhooc = rr / c, rhoxc = rr * c, c2 = c * c;
-  double vS = dot3(v, v);
-  double vn = v[0] * nV[0] + v[1] * nV[1] + v[2] * nV[2];
+template <typename T>
+__device__ inline void matrices_roe(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area,
+                                    const T nV[3]) {
+  T uLuL = dot3(L.u, L.u), uRuR = dot3(R.u, R.u);
+  T Rrho = sqrt(R.rho / L.rho);
+  T rr = Rrho * L.rho;
+  T tmp = T(1.0) / (T(1.0) + Rrho);
+  T v[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
+  T uRoe = dot3(v, nV);
+  T gpr = tmp * ((L.gam * L.p / L.rho + T(0.5) * (L.gam - T(1.0)) * uLuL) +
+                      (R.gam * R.p / R.rho + T(0.5) * (R.gam - T(1.0)) * uRuR) * Rrho);
+  T c = sqrt(gpr - ((L.gam + R.gam) * T(0.5) - T(1.0)) * T(0.5) * dot3(v, v));
+  T gamma = T(0.5) * (L.gam + R.gam);
+  T km1 = gamma - T(1.0);
+  T rhooc = rr / c, rhoxc = rr * c, c2 = c * c;
+  T vS = dot3(v, v);
+  T vn = v[0] * nV[0] + v[1] * nV[1] + v[2] * nV[2];
   // P^-1 (calcInvPMatrix): the reference divides by rho, c^2 and rho*c entry by
   // entry; one reciprocal of each replaces ~30 FP64 divides (<= 1 ulp per term)
-  const double ir = 1.0 / rr, ic2 = 1.0 / c2, irc = 1.0 / rhoxc;
-  const double kc = km1 * ic2, kr = km1 * irc;
-  double Q[25];
-  Q[0] = nV[0] - nV[2] * v[1] * ir + nV[1] * v[2] * ir - nV[0] * 0.5 * vS * kc;
+  const T ir = T(1.0) / rr, ic2 = T(1.0) / c2, irc = T(1.0) / rhoxc;
+  const T kc = km1 * ic2, kr = km1 * irc;
+  T Q[25];
+  Q[0] = nV[0] - nV[2] * v[1] * ir + nV[1] * v[2] * ir - nV[0] * T(0.5) * vS * kc;
   Q[1] = nV[0] * v[0] * kc;
   Q[2] = nV[2] * ir + nV[0] * v[1] * kc;
   Q[3] = -nV[1] * ir + nV[0] * v[2] * kc;
   Q[4] = -nV[0] * kc;
-  Q[5] = nV[1] + nV[2] * v[0] * ir - nV[0] * v[2] * ir - nV[1] * 0.5 * vS * kc;
+  Q[5] = nV[1] + nV[2] * v[0] * ir - nV[0] * v[2] * ir - nV[1] * T(0.5) * vS * kc;
   Q[6] = -nV[2] * ir + nV[1] * v[0] * kc;
   Q[7] = nV[1] * v[1] * kc;
   Q[8] = nV[0] * ir + nV[1] * v[2] * kc;
   Q[9] = -nV[1] * kc;
-  Q[10] = nV[2] - nV[1] * v[0] * ir + nV[0] * v[1] * ir - nV[2] * 0.5 * vS * kc;
+  Q[10] = nV[2] - nV[1] * v[0] * ir + nV[0] * v[1] * ir - nV[2] * T(0.5) * vS * kc;
   Q[11] = nV[1] * ir + nV[2] * v[0] * kc;
   Q[12] = -nV[0] * ir + nV[2] * v[1] * kc;
   Q[13] = nV[2] * v[2] * kc;
   Q[14] = -nV[2] * kc;
-  Q[15] = -vn * ir + 0.5 * vS * kr;
+  Q[15] = -vn * ir + T(0.5) * vS * kr;
   Q[16] = nV[0] * ir - v[0] * kr;
   Q[17] = nV[1] * ir - v[1] * kr;
   Q[18] = nV[2] * ir - v[2] * kr;
   Q[19] = kr;
-  Q[20] = vn * ir + 0.5 * vS * kr;
+  Q[20] = vn * ir + T(0.5) * vS * kr;
   Q[21] = -nV[0] * ir - v[0] * kr;
   Q[22] = -nV[1] * ir - v[1] * kr;
   Q[23] = -nV[2] * ir - v[2] * kr;
   Q[24] = kr;
-  double lam[5] = {fabs(uRoe), fabs(uRoe), fabs(uRoe), fabs(uRoe + c), fabs(uRoe - c)};
-  double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
+  T lam[5] = {fabs(uRoe), fabs(uRoe), fabs(uRoe), fabs(uRoe + c), fabs(uRoe - c)};
+  T nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
   if (AL) jacobian_A(AL, L.u, L.p, L.rho, nA, gamma);
   if (AR) jacobian_A(AR, R.u, R.p, R.rho, nA, gamma);
 #pragma unroll
   for (int i = 0; i < 5; i++) {
-    double Pr[5];
+    T Pr[5];
     roe_p_row(Pr, i, v, rr, rhooc, rhoxc, km1, vS, vn, nV);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
-      double pm = 0.0;
+      T pm = T(0.0);
 #pragma unroll
       for (int k = 0; k < 5; k++) pm += Pr[k] * lam[k] * Q[5 * k + j];
-      if (AL) AL[5 * i + j] = 0.5 * AL[5 * i + j] + 0.5 * pm * area;
-      if (AR) AR[5 * i + j] = 0.5 * AR[5 * i + j] - 0.5 * pm * area;
+      if (AL) AL[5 * i + j] = T(0.5) * AL[5 * i + j] + T(0.5) * pm * area;
+      if (AR) AR[5 * i + j] = T(0.5) * AR[5 * i + j] - T(0.5) * pm * area;
     }
   }
 }
@@ -397,11 +416,11 @@ __device__ __forceinline__ void euler_flux_t(double F[5], const FState& L, const
   else flux_hllc(F, L, R, area, nV);
 }
 
-template <int KIND>
-__device__ __forceinline__ void euler_matrices_t(double* AL, double* AR, const FState& L, const FState& R, double area,
-                                                 const double nV[3]) {
-  if (KIND == 1) matrices_roe(AL, AR, L, R, area, nV);
-  else matrices_hllc(AL, AR, L, R, area, nV);
+template <int KIND, typename T>
+__device__ __forceinline__ void euler_matrices_t(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area,
+                                                 const T nV[3]) {
+  if (KIND == 1) matrices_roe<T>(AL, AR, L, R, area, nV);
+  else matrices_hllc<T>(AL, AR, L, R, area, nV);
 }
 
 __device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& L, const FState& R, double area,
@@ -414,8 +433,8 @@ __device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& 
 // implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061)
 __device__ __forceinline__ void euler_matrices(int kind, double* AL, double* AR, const FState& L, const FState& R,
                                                double area, const double nV[3]) {
-  if (kind == 1) matrices_roe(AL, AR, L, R, area, nV);
-  else matrices_hllc(AL, AR, L, R, area, nV);
+  if (kind == 1) matrices_roe<double>(AL, AR, L, R, area, nV);
+  else matrices_hllc<double>(AL, AR, L, R, area, nV);
 }
 
 // One side of the viscous flux state (addViscFlux arguments).
@@ -461,22 +480,29 @@ __device__ inline void visc_flux(double Fu[3], double& FE, VFace& vf, const VSid
 // dF/dU x dU/dQ of the viscous flux (UgpWithCvCompFlow.cpp:717-745, 1692-1760) for
 // side 0 (A0) or side 1 (A1), scaled by sgn and added into the 5x5 row-major
 // accumulator acc (rows 1..4; the other entries are zero).
-__device__ inline void visc_jac_add(double* acc, double sgn, int side, const VFace& vf, const VSide& s,
+template <typename T>
+__device__ inline void visc_jac_add(T* acc, T sgn, int side, const VFace& vf, const VSide& s,
                                     const double* u_fa) {
-  double d = (side == 0) ? -(vf.mul + vf.mut) * vf.alpha / vf.smag * vf.area : (vf.mul + vf.mut) * vf.alpha / vf.smag * vf.area;
-  double f44 = (side == 0) ? -vf.area * vf.keff * vf.alpha / vf.smag : vf.area * vf.keff * vf.alpha / vf.smag;
-  double f4[3] = {vf.area * vf.tau[0] * 0.5 + u_fa[0] * d, vf.area * vf.tau[1] * 0.5 + u_fa[1] * d,
-                  vf.area * vf.tau[2] * 0.5 + u_fa[2] * d};
-  double ir = 1.0 / s.rho;
-  double uq0[3] = {-s.u[0] * ir, -s.u[1] * ir, -s.u[2] * ir};
-  double uq40 = s.gam * ir * (-s.h + s.R * s.T + 0.5 * dot3(s.u, s.u));
+  // inputs rounded to T once, the arithmetic in T (FP64: the reference's expressions term by term)
+  const T mm = (T)(vf.mul + vf.mut), alpha = (T)vf.alpha, smag = (T)vf.smag, area = (T)vf.area, keff = (T)vf.keff;
+  const T tau[3] = {(T)vf.tau[0], (T)vf.tau[1], (T)vf.tau[2]};
+  const T uf[3] = {(T)u_fa[0], (T)u_fa[1], (T)u_fa[2]};
+  const T rho = (T)s.rho, hh = (T)s.h, RR = (T)s.R, TT = (T)s.T, gam = (T)s.gam;
+  const T u[3] = {(T)s.u[0], (T)s.u[1], (T)s.u[2]};
+  T d = (side == 0) ? -mm * alpha / smag * area : mm * alpha / smag * area;
+  T f44 = (side == 0) ? -area * keff * alpha / smag : area * keff * alpha / smag;
+  T f4[3] = {area * tau[0] * T(0.5) + uf[0] * d, area * tau[1] * T(0.5) + uf[1] * d,
+             area * tau[2] * T(0.5) + uf[2] * d};
+  T ir = T(1.0) / rho;
+  T uq0[3] = {-u[0] * ir, -u[1] * ir, -u[2] * ir};
+  T uq40 = gam * ir * (-hh + RR * TT + T(0.5) * dot3(u, u));
   for (int r = 0; r < 3; r++) {
     acc[5 * (r + 1) + 0] += sgn * (d * uq0[r]);
     acc[5 * (r + 1) + 1 + r] += sgn * (d * ir);
   }
   acc[20] += sgn * (f4[0] * uq0[0] + f4[1] * uq0[1] + f4[2] * uq0[2] + f44 * uq40);
-  for (int k = 0; k < 3; k++) acc[21 + k] += sgn * (f4[k] * ir + f44 * (-s.gam * s.u[k] * ir));
-  acc[24] += sgn * (f44 * (s.gam * ir));
+  for (int k = 0; k < 3; k++) acc[21 + k] += sgn * (f4[k] * ir + f44 * (-gam * u[k] * ir));
+  acc[24] += sgn * (f44 * (gam * ir));
 }
 
 }  // namespace jg

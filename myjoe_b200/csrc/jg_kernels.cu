@@ -472,14 +472,18 @@ __device__ inline void block_inverse(double* A, double* Ai) {
 
 template <typename BT, int KIND, int VISC>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
-  extern __shared__ double sD[];  // [25][blockDim.x] diagonal-block accumulators
+  // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
+  // FP32 for the mixed form's preconditioner (the residual is FP64 in both)
+  using JT = BT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  JT* sD = reinterpret_cast<JT*>(smem_raw);  // [25][blockDim.x] diagonal-block accumulators
   __shared__ double sres[5][128];
   const int t = threadIdx.x, bd = blockDim.x;
   int c = blockIdx.x * bd + t;
   bool active = c < m.ncv;
   double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (active) {
-    for (int e = 0; e < 25; e++) sD[e * bd + t] = 0.0;
+    for (int e = 0; e < 25; e++) sD[e * bd + t] = JT(0);
     BT* O = (BT*)st.O;
     for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
       const Slot s = m.slots[k];
@@ -497,11 +501,12 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           euler_flux_t<KIND>(F, L, R, area, nV);
           for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
         }
-        double Ob[25];
+        JT Ob[25];
+        const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
         if (implicit) {
-          FState L0 = cell_fstate(p, st, c0), R0 = cell_fstate(p, st, c1);
-          double Apl[25], Ami[25];
-          euler_matrices_t<KIND>(Apl, Ami, L0, R0, area, nV);
+          FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c0)), R0 = fstate_as<JT>(cell_fstate(p, st, c1));
+          JT Apl[25], Ami[25];
+          euler_matrices_t<KIND, JT>(Apl, Ami, L0, R0, (JT)area, nVt);
           // row of c0: D += Apl, O(c0,c1) = Ami ; row of c1: D -= Ami, O(c1,c0) = -Apl
           if (s.side == 0) {
             for (int e = 0; e < 25; e++) { sD[e * bd + t] += Apl[e]; Ob[e] = Ami[e]; }
@@ -523,14 +528,14 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           rhs[4] += sg * FE;
           if (implicit) {
             // row of c0: D -= A0, O -= A1 ; row of c1: D += A1, O += A0  (calcViscousFluxNS 3678-3696)
-            double Dv[25];
-            for (int e = 0; e < 25; e++) Dv[e] = 0.0;
+            JT Dv[25];
+            for (int e = 0; e < 25; e++) Dv[e] = JT(0);
             if (s.side == 0) {
-              visc_jac_add(Dv, -1.0, 0, vf, v0, ufa);
-              visc_jac_add(Ob, -1.0, 1, vf, v1, ufa);
+              visc_jac_add<JT>(Dv, JT(-1.0), 0, vf, v0, ufa);
+              visc_jac_add<JT>(Ob, JT(-1.0), 1, vf, v1, ufa);
             } else {
-              visc_jac_add(Dv, 1.0, 1, vf, v1, ufa);
-              visc_jac_add(Ob, 1.0, 0, vf, v0, ufa);
+              visc_jac_add<JT>(Dv, JT(1.0), 1, vf, v1, ufa);
+              visc_jac_add<JT>(Ob, JT(1.0), 0, vf, v0, ufa);
             }
             for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
           }
@@ -543,6 +548,8 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         const double* bb = &st.bfa[8 * f];
         FState B;
         B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
+        const FStateT<JT> Bt = fstate_as<JT>(B);
+        const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
         double F[5];
         if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
           euler_flux_t<KIND>(F, B, B, area, nV);
@@ -557,17 +564,17 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
               double a2 = p.gamma - 1.0;
               double phi = 0.5 * a2 * (B.u[0] * B.u[0] + B.u[1] * B.u[1] + B.u[2] * B.u[2]);
               for (int i = 0; i < 3; i++) {
-                sD[(5 * (i + 1) + 0) * bd + t] += phi * nV[i] * area;
-                for (int j = 0; j < 3; j++) sD[(5 * (i + 1) + 1 + j) * bd + t] += -a2 * B.u[j] * nV[i] * area;
-                sD[(5 * (i + 1) + 4) * bd + t] += a2 * nV[i] * area;
+                sD[(5 * (i + 1) + 0) * bd + t] += (JT)(phi * nV[i] * area);
+                for (int j = 0; j < 3; j++) sD[(5 * (i + 1) + 1 + j) * bd + t] += (JT)(-a2 * B.u[j] * nV[i] * area);
+                sD[(5 * (i + 1) + 4) * bd + t] += (JT)(a2 * nV[i] * area);
               }
             } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
-              double Apl[25], Ami[25];
-              euler_matrices_t<KIND>(Apl, Ami, B, B, area, nV);
+              JT Apl[25], Ami[25];
+              euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
             } else {
-              double Apl[25];
-              euler_matrices_t<KIND>(Apl, nullptr, B, B, area, nV);
+              JT Apl[25];
+              euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
             }
           }
@@ -576,9 +583,9 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           euler_flux_t<KIND>(F, L, B, area, nV);
           for (int i = 0; i < 5; i++) rhs[i] -= F[i];
           if (implicit) {
-            FState L0 = cell_fstate(p, st, c);
-            double Apl[25];
-            euler_matrices_t<KIND>(Apl, nullptr, L0, B, area, nV);
+            FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
+            JT Apl[25];
+            euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt);
             for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
           }
         }
@@ -603,9 +610,9 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
           rhs[4] -= FE;
           if (implicit) {
-            double Dv[25];
-            for (int e = 0; e < 25; e++) Dv[e] = 0.0;
-            visc_jac_add(Dv, -1.0, 0, vf, v0, v1.u);
+            JT Dv[25];
+            for (int e = 0; e < 25; e++) Dv[e] = JT(0);
+            visc_jac_add<JT>(Dv, JT(-1.0), 0, vf, v0, v1.u);
             for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
           }
         }
@@ -615,7 +622,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
     for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
     if (implicit) {
       double Dm[25];
-      for (int e = 0; e < 25; e++) Dm[e] = sD[e * bd + t];
+      for (int e = 0; e < 25; e++) Dm[e] = (double)sD[e * bd + t];
       if (for_step) {
         double tmp = m.vol[c] / st.local_dt[c];
         for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;
@@ -1190,7 +1197,7 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
 }
 template <typename BT, int KIND>
 static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  size_t shm = 25 * TB * sizeof(double);
+  size_t shm = 25 * TB * sizeof(BT);
   if (p.viscous) k_flux<BT, KIND, 1><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
   else k_flux<BT, KIND, 0><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
 }

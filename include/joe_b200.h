@@ -58,7 +58,8 @@ typedef struct jg_zone {
   int kind;           /* JG_BC_* */
   int scal_bc;        /* bit s set: transported scalar s is Dirichlet here with value v[6+s]
                          (Joe.in key "<zone>.<scalar> = value", Scalars.cpp:289-360);
-                         bit clear: zero-flux (phi_bfa = phi of the cell) */
+                         bit 4+s: the model's HOOK boundary ("<zone>.<scalar> = HOOK");
+                         neither: zero flux (phi_bfa = phi of the cell) */
   double v[8];        /* parameters, see JG_BC_* (v[6], v[7]: scalar Dirichlet values) */
 } jg_zone;
 
@@ -95,13 +96,17 @@ typedef struct jg_params {
   int ls_max_iter;     /* LINEAR_SOLVER_NS_TRESHOLDS MAX_ITER (BCGSTAB) or sweeps (JACOBI/SGS) */
   double ls_abs, ls_rel;
   int precision;       /* JG_PREC_* */
-  int nscal;           /* transported scalars: 0 (laminar / inviscid), 1 with JG_TURB_SA */
+  int nscal;           /* transported scalars: 0 (laminar / inviscid), 1 (SA), 2 (SST) */
   int turb_model;      /* JG_TURB_*: with a model the case runs runBackwardEulerCoupled's
                           (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
 } jg_params;
-/* turbulence models: JG_TURB_SA = Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h)
- * with the reference's default constants, scalar nuSA (bounds 1e-10 .. 1) */
-enum { JG_TURB_NONE = 0, JG_TURB_SA = 1 };
+/* turbulence models, with the reference's default constants:
+ *   JG_TURB_SA  Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h): nscal 1, nuSA (1e-10 .. 1)
+ *   JG_TURB_SST Menter k-omega SST (TurbModel_KOMSST.h): nscal 2, kine (1e-10 .. 1e10) and
+ *               omega (1e-4 .. 1e15); Pk limiter on, shear-stress limiter = vorticity;
+ *               zone.scal_bc bit 4+s marks the model's HOOK boundary for scalar s (SST:
+ *               omega on a WALL = 60 mu / (rho beta_1 d^2)) */
+enum { JG_TURB_NONE = 0, JG_TURB_SA = 1, JG_TURB_SST = 2 };
 
 
 typedef struct jg_case jg_case_t;   /* opaque per-case handle (device state + stream + graph) */

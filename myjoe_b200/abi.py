@@ -99,7 +99,7 @@ def make_params(p: JoeParams, precision: int = 0) -> jg_params:
     q.ls_rel = p.LS_REL_RESID
     q.precision = precision
     q.nscal = p.nscal
-    q.turb_model = 1 if p.TURB_MODEL == "SA" else 0
+    q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
     return q
 
 
@@ -131,9 +131,14 @@ class MeshArrays:
             zarr[i].ifa_f, zarr[i].ifa_l = f0, f1
             zarr[i].kind = BC_KINDS[bc.kind]
             vals = list(bc.values) + [0.0] * (8 - len(bc.values))
-            if name in params.scalar_bcs:
-                zarr[i].scal_bc = 1
-                vals[6] = params.scalar_bcs[name]
+            bits = 0
+            for sc, (kind, v) in enumerate(params.zone_scalar_bcs(name)):
+                if kind == "dirichlet":
+                    bits |= 1 << sc
+                    vals[6 + sc] = v
+                elif kind == "hook":
+                    bits |= 1 << (4 + sc)
+            zarr[i].scal_bc = bits
             for k in range(8):
                 zarr[i].v[k] = vals[k]
         self.zarr = zarr

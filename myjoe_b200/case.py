@@ -71,14 +71,36 @@ class JoeParams:
     P_INITIAL: float = 1.0e5
     RHO_INITIAL: float = 1.0e5 / (287.0 * 300.0)
     bcs: Dict[str, BC] = dataclasses.field(default_factory=dict)
-    TURB_MODEL: str = "NONE"          # "SA": Spalart-Allmaras, coupled 6x6 system
-    NUSA_INITIAL: float = 0.0         # INITIAL_CONDITION_TURB (nuSA)
-    # Dirichlet values of the transported scalar per zone ("<zone>.nuSA = v"); absent: zero flux
-    scalar_bcs: Dict[str, float] = dataclasses.field(default_factory=dict)
+    TURB_MODEL: str = "NONE"          # "SA" (coupled 6x6) or "SST" (Menter k-omega SST, coupled 7x7)
+    NUSA_INITIAL: float = 0.0         # INITIAL_CONDITION_TURB for SA (nuSA)
+    KINE_INITIAL: float = 0.0         # INITIAL_CONDITION_TURB for SST (kine, omega)
+    OMEGA_INITIAL: float = 0.0
+    # scalar boundary values per zone ("<zone>.<scalar> = v" / "= HOOK"); absent: zero flux.
+    # SA: {zone: nuSA}; SST: {zone: (kine or None, omega or "HOOK" or None)}
+    scalar_bcs: Dict[str, object] = dataclasses.field(default_factory=dict)
 
     @property
     def nscal(self) -> int:
-        return 1 if self.TURB_MODEL == "SA" else 0
+        return {"SA": 1, "SST": 2}.get(self.TURB_MODEL, 0)
+
+    @property
+    def scalar_names(self):
+        return {"SA": ["nuSA"], "SST": ["kine", "omega"]}.get(self.TURB_MODEL, [])
+
+    def zone_scalar_bcs(self, zone):
+        """[(kind, value)] per scalar for a zone: kind "dirichlet", "hook" or None."""
+        v = self.scalar_bcs.get(zone)
+        vals = [v] if (self.TURB_MODEL == "SA" and v is not None) else (list(v) if v is not None else [])
+        out = []
+        for s in range(self.nscal):
+            x = vals[s] if s < len(vals) else None
+            if x is None:
+                out.append((None, 0.0))
+            elif isinstance(x, str):
+                out.append(("hook", 0.0))
+            else:
+                out.append(("dirichlet", float(x)))
+        return out
 
     @property
     def R_gas(self) -> float:
@@ -109,7 +131,8 @@ class JoeParams:
                 self.LS_MAX_ITER, self.LS_ABS_RESID, self.LS_REL_RESID),
             "U_INITIAL = %.17g %.17g %.17g" % tuple(self.U_INITIAL),
             "P_INITIAL = %.17g" % self.P_INITIAL, "RHO_INITIAL = %.17g" % self.RHO_INITIAL,
-            "INITIAL_CONDITION_TURB = %.17g 0.0" % self.NUSA_INITIAL,
+            ("INITIAL_CONDITION_TURB = %.17g %.17g" % (self.KINE_INITIAL, self.OMEGA_INITIAL)
+             if self.TURB_MODEL == "SST" else "INITIAL_CONDITION_TURB = %.17g 0.0" % self.NUSA_INITIAL),
             "CHECK_INTERVAL = 1",
             "INITIAL_FLOWFIELD_OUTPUT = NO",
         ]
@@ -117,8 +140,12 @@ class JoeParams:
             L.append("SPATIAL_SECOND_ORDER")
         for name, bc in self.bcs.items():
             L.append("%s = %s" % (name, bc.joe_in()))
-        for name, v in self.scalar_bcs.items():
-            L.append("%s.nuSA = %.17g" % (name, v))
+        for name in self.scalar_bcs:
+            for (kind, v), sname in zip(self.zone_scalar_bcs(name), self.scalar_names):
+                if kind == "dirichlet":
+                    L.append("%s.%s = %.17g" % (name, sname, v))
+                elif kind == "hook":
+                    L.append("%s.%s = HOOK" % (name, sname))
         if extra:
             L.append(extra)
         return "\n".join(L) + "\n"
@@ -251,3 +278,24 @@ def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_
                     MU_REF=mu_ref, SYMM_BC="ANALYTICAL", U_INITIAL=u, P_INITIAL=p, RHO_INITIAL=rho, bcs=bcs,
                     TURB_MODEL="SA", NUSA_INITIAL=nu_inf, scalar_bcs=sbc)
     return raw, geometry.build_cv_mesh(raw, seed=seed), prm
+
+
+def sst_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
+                  stretch=1.0, inlet="FARFIELD", tu=0.005, visc_ratio=0.1):
+    """Turbulent (Menter SST) flow over the channel bump, set up like
+    ``sa_bump_case``: free-stream k = 1.5 (tu U)^2 and omega from the
+    free-stream eddy-viscosity ratio mu_t/mu = ``visc_ratio``; at the wall
+    k = 0 and omega from the model's wall hook (60 nu / (beta_1 d^2))."""
+    raw, g, prm = sa_bump_case(nx, ny, nz, mach=mach, re=re, p=p, T=T, bump_h=bump_h, jitter=jitter, seed=seed,
+                               stretch=stretch, inlet=inlet)
+    U = prm.U_INITIAL[0]
+    rho = prm.RHO_INITIAL
+    tref, sref = 273.15, 110.4
+    mu = prm.MU_REF * (T / tref) ** 1.5 * (tref + sref) / (T + sref)
+    k = 1.5 * (tu * U) ** 2
+    om = rho * k / (visc_ratio * mu)
+    sbc = {z: (k, om) for z, v in prm.scalar_bcs.items() if z != "lower"}
+    sbc["lower"] = (0.0, "HOOK")
+    prm = dataclasses.replace(prm, TURB_MODEL="SST", NUSA_INITIAL=0.0, KINE_INITIAL=k, OMEGA_INITIAL=om,
+                              scalar_bcs=sbc)
+    return raw, g, prm

@@ -31,6 +31,7 @@ struct jo_case {
   int step;
   int dt_fixed_done;
   double dt_fixed;
+  double *kine;     /* turbulent kinetic energy per cell (SST), NULL otherwise */
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -125,6 +126,7 @@ static void calc_state_variables(jo_case *h) {
     double *ru = &h->rhou[3 * c];
     for (int i = 0; i < 3; i++) h->vel[3 * c + i] = ru[i] / r;
     double kinecv = 0.0;
+    if (h->kine) kinecv = h->kine[c];
     double pr = (h->gam[c] - 1.0) * (h->rhoE[c] - 0.5 * dot3(ru, ru) / r - r * kinecv);
     if (pr > 0.0) h->press[c] = pr;  /* negative pressure: keep the old value */
     h->temp[c] = h->press[c] / (r * h->RoM[c]);
@@ -1555,13 +1557,19 @@ int jo_step(jo_case *h, int nsteps, double *resid) {
   return err;
 }
 
+
 /* ======================================================================== */
-/* Coupled path with the Spalart-Allmaras model (nScal = 1):                 */
-/* runBackwardEulerCoupled / calcRhsCoupled / calcFluxCoupled,               */
-/* JoeWithModels.cpp:4326-5826; TurbModel_SA.h; UgpWithCvCompFlow.cpp        */
-/* 1808-2292, 3040-3276; Scalars.cpp:289-360; UgpWithCvCompFlow.h:1305-1552. */
-/* Row/column 5 of every block is the scalar rho*nuSA.                       */
+/* Coupled path with a turbulence model: runBackwardEulerCoupled /           */
+/* calcRhsCoupled / calcFluxCoupled, JoeWithModels.cpp:4326-5826;           */
+/* UgpWithCvCompFlow.cpp:1808-2292, 3040-3276; Scalars.cpp:289-360;          */
+/* UgpWithCvCompFlow.h:1305-1552.  SA (TurbModel_SA.h): one scalar, nuSA,    */
+/* block size 6.  SST (TurbModel_KOMSST.h): kine and omega, block size 7;    */
+/* kine also enters the pressure, the HLLC energy and the viscous terms.    */
+/* Row/column 5+s of every block is rho*phi_s.                               */
 /* ======================================================================== */
+#define MAXS 2
+#define MAXB 7
+/* RansTurbSA defaults (TurbModel_SA.h:21-36) */
 #define SA_CV1_3 357.911
 #define SA_CW1 3.239067817
 #define SA_CW2 0.3
@@ -1570,42 +1578,65 @@ int jo_step(jo_case *h, int nsteps, double *resid) {
 #define SA_CB1 0.1355
 #define SA_CB2 0.622
 #define SA_K2 0.1681
-#define SA_LOWER 1.0e-10
-#define SA_UPPER 1.0
-#define NB 6 /* block size of the coupled SA system */
+/* RansTurbKOmSST defaults (TurbModel_KOMSST.h:19-54) */
+#define SST_SK1 0.85
+#define SST_SK2 1.0
+#define SST_SO1 0.5
+#define SST_SO2 0.856
+#define SST_B1 0.075
+#define SST_B2 0.0828
+#define SST_BS 0.09
+#define SST_A1 0.31
 
 typedef struct {
-  double *phi, *phi_bfa, *grad_phi, *diff, *wallDist, *strMag, *vortMag;
-} jo_sa;
+  int model, ns;
+  double *phi[MAXS], *phi_bfa[MAXS], *grad_phi[MAXS], *diff[MAXS];
+  double *wallDist, *strMag, *vortMag, *diverg, *crossDiff, *F1, *F2;
+  double lower[MAXS], upper[MAXS];
+} jo_turb;
 
-static jo_sa *sa_of(jo_case *h);
+typedef struct turb_node { jo_case *h; jo_turb t; struct turb_node *next; } turb_node;
+static turb_node *g_turb = NULL;
 
-/* the SA arrays live beside the case; allocated on first use */
-static jo_sa g_sa_none;
-typedef struct sa_node { jo_case *h; jo_sa sa; struct sa_node *next; } sa_node;
-static sa_node *g_sa_list = NULL;
-
-static jo_sa *sa_of(jo_case *h) {
-  for (sa_node *n = g_sa_list; n; n = n->next)
-    if (n->h == h) return &n->sa;
-  sa_node *n = (sa_node *)calloc(1, sizeof(sa_node));
+static jo_turb *turb_of(jo_case *h) {
+  for (turb_node *n = g_turb; n; n = n->next)
+    if (n->h == h) return &n->t;
+  turb_node *n = (turb_node *)calloc(1, sizeof(turb_node));
   n->h = h;
+  jo_turb *t = &n->t;
   int c = h->ncv, nb = h->nfa_b, nf = h->nfa;
-  n->sa.phi = dalloc(c); n->sa.phi_bfa = dalloc(nb); n->sa.grad_phi = dalloc(3 * c); n->sa.diff = dalloc(nf);
-  n->sa.wallDist = dalloc(c); n->sa.strMag = dalloc(c); n->sa.vortMag = dalloc(c);
-  n->next = g_sa_list;
-  g_sa_list = n;
-  return &n->sa;
+  t->model = h->p.turb_model;
+  t->ns = h->p.nscal;
+  for (int s = 0; s < t->ns; s++) {
+    t->phi[s] = dalloc(c); t->phi_bfa[s] = dalloc(nb); t->grad_phi[s] = dalloc(3 * c); t->diff[s] = dalloc(nf);
+  }
+  t->wallDist = dalloc(c); t->strMag = dalloc(c); t->vortMag = dalloc(c); t->diverg = dalloc(c);
+  t->crossDiff = dalloc(c); t->F1 = dalloc(c); t->F2 = dalloc(c);
+  if (t->model == JG_TURB_SA) {
+    t->lower[0] = 1.0e-10; t->upper[0] = 1.0;
+  } else {
+    t->lower[0] = 1.0e-10; t->upper[0] = 1.0e10;  /* kine */
+    t->lower[1] = 1.0e-4; t->upper[1] = 1.0e15;   /* omega */
+    h->kine = t->phi[0];
+  }
+  n->next = g_turb;
+  g_turb = n;
+  return t;
 }
 
 void jo_sa_release(jo_case *h) {
-  sa_node **pp = &g_sa_list;
+  turb_node **pp = &g_turb;
   while (*pp) {
     if ((*pp)->h == h) {
-      sa_node *n = *pp;
+      turb_node *n = *pp;
       *pp = n->next;
-      free(n->sa.phi); free(n->sa.phi_bfa); free(n->sa.grad_phi); free(n->sa.diff);
-      free(n->sa.wallDist); free(n->sa.strMag); free(n->sa.vortMag);
+      jo_turb *t = &n->t;
+      for (int s = 0; s < t->ns; s++) {
+        free(t->phi[s]); free(t->phi_bfa[s]); free(t->grad_phi[s]); free(t->diff[s]);
+      }
+      free(t->wallDist); free(t->strMag); free(t->vortMag); free(t->diverg); free(t->crossDiff);
+      free(t->F1); free(t->F2);
+      h->kine = NULL;
       free(n);
       return;
     }
@@ -1613,18 +1644,27 @@ void jo_sa_release(jo_case *h) {
   }
 }
 
-void jo_set_scalar(jo_case *h, const double *phi) { memcpy(sa_of(h)->phi, phi, sizeof(double) * h->ncv); }
-void jo_get_scalar(jo_case *h, double *phi) { memcpy(phi, sa_of(h)->phi, sizeof(double) * h->ncv); }
+/* transported scalars in/out: phi[ncv][ns] */
+void jo_set_scalars(jo_case *h, const double *phi) {
+  jo_turb *t = turb_of(h);
+  for (int c = 0; c < h->ncv; c++)
+    for (int s = 0; s < t->ns; s++) t->phi[s][c] = phi[t->ns * c + s];
+}
+void jo_get_scalars(jo_case *h, double *phi) {
+  jo_turb *t = turb_of(h);
+  for (int c = 0; c < h->ncv; c++)
+    for (int s = 0; s < t->ns; s++) phi[t->ns * c + s] = t->phi[s][c];
+}
 
 double *jo_sa_array(jo_case *h, const char *name) {
-  jo_sa *s = sa_of(h);
-  if (!strcmp(name, "phi")) return s->phi;
-  if (!strcmp(name, "phi_bfa")) return s->phi_bfa;
-  if (!strcmp(name, "grad_phi")) return s->grad_phi;
-  if (!strcmp(name, "diff")) return s->diff;
-  if (!strcmp(name, "wallDist")) return s->wallDist;
-  if (!strcmp(name, "strMag")) return s->strMag;
-  if (!strcmp(name, "vortMag")) return s->vortMag;
+  jo_turb *t = turb_of(h);
+  struct { const char *n; double *p; } tab[] = {
+      {"phi", t->phi[0]}, {"phi_bfa", t->phi_bfa[0]}, {"grad_phi", t->grad_phi[0]}, {"diff", t->diff[0]},
+      {"phi1", t->phi[1]}, {"phi1_bfa", t->phi_bfa[1]}, {"grad_phi1", t->grad_phi[1]}, {"diff1", t->diff[1]},
+      {"wallDist", t->wallDist}, {"strMag", t->strMag}, {"vortMag", t->vortMag}, {"diverg", t->diverg},
+      {"crossDiff", t->crossDiff}, {"blendFuncF1", t->F1}, {"blendFuncF2", t->F2}};
+  for (size_t i = 0; i < sizeof(tab) / sizeof(tab[0]); i++)
+    if (strcmp(tab[i].n, name) == 0) return tab[i].p;
   return NULL;
 }
 
@@ -1632,7 +1672,7 @@ double *jo_sa_array(jo_case *h, const char *name) {
  * centroid, then the normal projection when the cell sits over that face */
 void jo_wall_distance(jo_case *h) {
   const jg_mesh *m = &h->m;
-  jo_sa *s = sa_of(h);
+  jo_turb *t = turb_of(h);
   int nw = 0;
   for (int z = 0; z < m->nzones; z++)
     if (m->zones[z].kind == JG_BC_WALL) nw += m->zones[z].ifa_l - m->zones[z].ifa_f + 1;
@@ -1658,24 +1698,32 @@ void jo_wall_distance(jo_case *h) {
     double dNorm2 = dot3(sh, n) * dot3(sh, n);
     double dTang2 = sMag2 - dNorm2;
     double specRadius2 = 0.5 * nmag;
-    s->wallDist[c] = (dTang2 > specRadius2) ? minDist : fabs(dot3(sh, n));
+    t->wallDist[c] = (dTang2 > specRadius2) ? minDist : fabs(dot3(sh, n));
   }
   free(wf);
 }
 
-/* setScalarBC, Scalars.cpp:289-360 (Dirichlet or zero flux per zone) */
+/* setScalarBC (Scalars.cpp:289-360) with the SST omega wall hook
+ * (boundaryHookScalarRansTurb, TurbModel_KOMSST.h:342-358) */
 static void set_scalar_bc(jo_case *h) {
   const jg_mesh *m = &h->m;
-  jo_sa *s = sa_of(h);
+  jo_turb *t = turb_of(h);
   for (int z = 0; z < m->nzones; z++) {
     const jg_zone *zn = &m->zones[z];
-    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
-      int c0 = m->cvofa[2 * f];
-      if (zn->scal_bc & 1)
-        s->phi_bfa[f] = (dot3(&h->vel_bfa[3 * f], &m->fa_normal[3 * f]) > 1.0e-8) ? s->phi[c0] : zn->v[6];
-      else
-        s->phi_bfa[f] = s->phi[c0];
-    }
+    for (int s = 0; s < t->ns; s++)
+      for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+        int c0 = m->cvofa[2 * f];
+        if (zn->scal_bc & (1 << (4 + s))) {
+          if (t->model == JG_TURB_SST && s == 1 && zn->kind == JG_BC_WALL) {
+            double muLamCV = mu_law(&h->p, h->temp[c0]);
+            t->phi_bfa[s][f] = 60.0 * muLamCV / (h->rho[c0] * SST_B1 * t->wallDist[c0] * t->wallDist[c0]);
+          }
+        } else if (zn->scal_bc & (1 << s)) {
+          t->phi_bfa[s][f] = (dot3(&h->vel_bfa[3 * f], &m->fa_normal[3 * f]) > 1.0e-8) ? t->phi[s][c0] : zn->v[6 + s];
+        } else {
+          t->phi_bfa[s][f] = t->phi[s][c0];
+        }
+      }
   }
 }
 
@@ -1687,17 +1735,21 @@ static double face_avg(jo_case *h, const double *phi, int c) {
   return v / (double)(f1 - f0 + 1);
 }
 
-static int zone_of_face(jo_case *h, int f) {
-  for (int z = 0; z < h->m.nzones; z++)
-    if (f >= h->m.zones[z].ifa_f && f <= h->m.zones[z].ifa_l) return z;
-  return -1;
+static void face_weights(jo_case *h, int f, int c0, int c1, double *w0, double *w1) {
+  double dx0[3], dx1[3];
+  for (int i = 0; i < 3; i++) {
+    dx0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c0 + i];
+    dx1[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c1 + i];
+  }
+  *w0 = sqrt(dot3(dx0, dx0));
+  *w1 = sqrt(dot3(dx1, dx1));
 }
 
-/* RansTurbSA::calcRansTurbViscMuet, TurbModel_SA.h:74-128 (with calcGradVel,
- * calcStrainRate, calcVorticity, UgpWithCvCompFlow.h:1305-1393) */
-static void sa_turb_visc(jo_case *h) {
+/* calcRansTurbViscMuet of the model (TurbModel_SA.h:74-128; TurbModel_KOMSST.h:109-167 with
+ * calcMenterBlendingFunctions 360-386), calcGradVel / calcStrainRate(AndDivergence) / calcVorticity */
+static void turb_visc(jo_case *h) {
   const jg_mesh *m = &h->m;
-  jo_sa *s = sa_of(h);
+  jo_turb *t = turb_of(h);
   grad_vector(h, h->grad_u, h->vel, h->vel_bfa, h->p.limiter, h->sos);
   for (int c = 0; c < h->ncv; c++) {
     const double *g = &h->grad_u[9 * c];
@@ -1710,63 +1762,105 @@ static void sa_turb_visc(jo_case *h) {
       }
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) vm += pow(0.5 * (g[3 * i + j] - g[3 * j + i]), 2.0);
-    s->strMag[c] = sqrt(2.0 * sm);
-    s->vortMag[c] = sqrt(2.0 * vm);
+    t->strMag[c] = sqrt(2.0 * sm);
+    t->vortMag[c] = sqrt(2.0 * vm);
+    t->diverg[c] = div;
   }
+  if (t->model == JG_TURB_SA) {
+    const double *nu = t->phi[0];
+    for (int f = h->nfa_b; f < h->nfa; f++) {
+      int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+      double w0, w1;
+      face_weights(h, f, c0, c1, &w0, &w1);
+      double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
+      double nu_fa = (w1 * nu[c0] + w0 * nu[c1]) / (w0 + w1);
+      double muSA = rho_fa * nu_fa;
+      double chi_3 = pow(muSA / h->mul_fa[f], 3.0);
+      double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+      h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+    }
+    for (int z = 0; z < m->nzones; z++) {
+      const jg_zone *zn = &m->zones[z];
+      for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+        if (zn->kind == JG_BC_WALL) { h->mut_fa[f] = 0.0; continue; }
+        int c0 = m->cvofa[2 * f];
+        double muSA = h->rho[c0] * nu[c0];
+        double mul0 = face_avg(h, h->mul_fa, c0);
+        double chi_3 = pow(muSA / mul0, 3.0);
+        double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+        h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+      }
+    }
+    return;
+  }
+  /* SST: Menter blending functions, then mut with the shear-stress limiter (vorticity) */
+  const double *k = t->phi[0], *om = t->phi[1];
+  grad_scalar(h, t->grad_phi[0], k, t->phi_bfa[0], h->p.limiter, k, NULL);
+  grad_scalar(h, t->grad_phi[1], om, t->phi_bfa[1], h->p.limiter, om, NULL);
+  for (int c = 0; c < h->ncv; c++) {
+    double d = t->wallDist[c];
+    double mue = face_avg(h, h->mul_fa, c);
+    t->crossDiff[c] = dmax(2.0 * h->rho[c] * SST_SO2 / om[c] * dot3(&t->grad_phi[0][3 * c], &t->grad_phi[1][3 * c]),
+                           1.0e-20);
+    double gamma1 = 500.0 * mue / (pow(d, 2.0) * h->rho[c] * om[c]);
+    double gamma2 = 4.0 * SST_SO2 * h->rho[c] * k[c] / (d * d * t->crossDiff[c]);
+    double gamma3 = sqrt(k[c]) / (SST_BS * om[c] * d);
+    double gamma = dmin(dmax(gamma1, gamma3), gamma2);
+    t->F1[c] = tanh(pow(gamma, 4.0));
+    gamma = dmax(2.0 * gamma3, gamma1);
+    t->F2[c] = tanh(pow(gamma, 2.0));
+  }
+  const double *lim = t->vortMag;
   for (int f = h->nfa_b; f < h->nfa; f++) {
     int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
-    double dx0[3], dx1[3];
-    for (int i = 0; i < 3; i++) {
-      dx0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
-      dx1[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c1 + i];
-    }
-    double w0 = sqrt(dot3(dx0, dx0)), w1 = sqrt(dot3(dx1, dx1));
+    double w0, w1;
+    face_weights(h, f, c0, c1, &w0, &w1);
     double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
-    double nu_fa = (w1 * s->phi[c0] + w0 * s->phi[c1]) / (w0 + w1);
-    double muSA = rho_fa * nu_fa;
-    double chi_3 = pow(muSA / h->mul_fa[f], 3.0);
-    double fv1 = chi_3 / (chi_3 + SA_CV1_3);
-    h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+    double kine_fa = (w1 * k[c0] + w0 * k[c1]) / (w0 + w1);
+    double om_fa = (w1 * om[c0] + w0 * om[c1]) / (w0 + w1);
+    double lim_fa = (w1 * lim[c0] + w0 * lim[c1]) / (w0 + w1);
+    double F2_fa = (w1 * t->F2[c0] + w0 * t->F2[c1]) / (w0 + w1);
+    double zeta = dmin(1.0 / om_fa, SST_A1 / (lim_fa * F2_fa));
+    h->mut_fa[f] = dmin(dmax(rho_fa * kine_fa * zeta, 0.0), 1.0);
   }
   for (int z = 0; z < m->nzones; z++) {
     const jg_zone *zn = &m->zones[z];
     for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
       if (zn->kind == JG_BC_WALL) { h->mut_fa[f] = 0.0; continue; }
       int c0 = m->cvofa[2 * f];
-      double muSA = h->rho[c0] * s->phi[c0];
-      double mul0 = face_avg(h, h->mul_fa, c0);
-      double chi_3 = pow(muSA / mul0, 3.0);
-      double fv1 = chi_3 / (chi_3 + SA_CV1_3);
-      h->mut_fa[f] = dmax(muSA * fv1, 0.0);
+      double zeta = dmin(1.0 / om[c0], SST_A1 / (lim[c0] * t->F2[c0]));
+      h->mut_fa[f] = dmin(dmax(h->rho[c0] * k[c0] * zeta, 0.0), 1.0);
     }
   }
 }
 
-/* state + material + BC (NS and scalar) + turbulent viscosity: the preamble of
+/* state + material + BC (NS and scalars) + turbulent viscosity: the preamble of
  * runBackwardEulerCoupled, JoeWithModels.cpp:4379-4401 */
 int jo_calc_state_coupled(jo_case *h) {
+  turb_of(h);
   calc_state_variables(h);
   calc_material_properties(h);
   int e = set_bc(h);
   set_scalar_bc(h);
-  sa_turb_visc(h);
+  turb_visc(h);
   return e;
 }
 
-/* calcEulerFluxCoupled_HLLC, UgpWithCvCompFlow.cpp:1808-1926 (nScal = 1, k = 0, ConvTerm = 1) */
-typedef struct { double rho, u[3], p, T, h, R, gam, sc; } cstate;
+/* ---- coupled HLLC (UgpWithCvCompFlow.cpp:1808-2289), nScal scalars, ConvTerm = 1, dp/dscal = 0 ---- */
+typedef struct { double rho, u[3], p, T, h, R, gam, sc[MAXS], k; } cstate;
 
-static void flux_hllc_coupled(double F[NB], const cstate *L, const cstate *R, double area, const double *nV,
+static void flux_hllc_coupled(double *F, int ns, const cstate *L, const cstate *R, double area, const double *nV,
                               int only_pressure) {
+  int B = 5 + ns;
   if (only_pressure) {
     F[0] = 0.0;
     for (int i = 1; i < 4; i++) F[i] = L->p * nV[i - 1];
-    for (int i = 4; i < NB; i++) F[i] = 0.0;
+    for (int i = 4; i < B; i++) F[i] = 0.0;
   } else {
     double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
-    double rhoeL = (L->h + 0.5 * uLuL + 0.0) * L->rho - L->p;
+    double rhoeL = (L->h + 0.5 * uLuL + L->k) * L->rho - L->p;
     double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
-    double rhoeR = (R->h + 0.5 * uRuR + 0.0) * R->rho - R->p;
+    double rhoeR = (R->h + 0.5 * uRuR + R->k) * R->rho - R->p;
     double Rrho = sqrt(R->rho / L->rho);
     double tmp = 1.0 / (1.0 + Rrho);
     double velRoe[3];
@@ -1780,12 +1874,13 @@ static void flux_hllc_coupled(double F[NB], const cstate *L, const cstate *R, do
     double sM = (L->p - R->p - L->rho * unL * (sL - unL) + R->rho * unR * (sR - unR)) /
                 (R->rho * (sR - unR) - L->rho * (sL - unL));
     double pStar = R->rho * (unR - sR) * (unR - sM) + R->p;
+    const cstate *S;
     if (sM >= 0.0) {
+      S = L;
       if (sL > 0.0) {
         F[0] = L->rho * unL;
         for (int i = 0; i < 3; i++) F[1 + i] = L->rho * L->u[i] * unL + L->p * nV[i];
         F[4] = (rhoeL + L->p) * unL;
-        F[5] = 1.0 * F[0] * L->sc;
       } else {
         double inv = 1.0 / (sL - sM), sLmuL = sL - unL;
         double rhoS = L->rho * sLmuL * inv, rhouS[3];
@@ -1794,9 +1889,9 @@ static void flux_hllc_coupled(double F[NB], const cstate *L, const cstate *R, do
         F[0] = rhoS * sM;
         for (int i = 0; i < 3; i++) F[1 + i] = rhouS[i] * sM + pStar * nV[i];
         F[4] = (rhoeS + pStar) * sM;
-        F[5] = 1.0 * F[0] * L->sc;
       }
     } else {
+      S = R;
       if (sR >= 0.0) {
         double inv = 1.0 / (sR - sM), sRmuR = sR - unR;
         double rhoS = R->rho * sRmuR * inv, rhouS[3];
@@ -1805,80 +1900,90 @@ static void flux_hllc_coupled(double F[NB], const cstate *L, const cstate *R, do
         F[0] = rhoS * sM;
         for (int i = 0; i < 3; i++) F[1 + i] = rhouS[i] * sM + pStar * nV[i];
         F[4] = (rhoeS + pStar) * sM;
-        F[5] = 1.0 * F[0] * R->sc;
       } else {
         F[0] = R->rho * unR;
         for (int i = 0; i < 3; i++) F[1 + i] = R->rho * R->u[i] * unR + R->p * nV[i];
         F[4] = (rhoeR + R->p) * unR;
-        F[5] = 1.0 * F[0] * R->sc;
       }
     }
+    for (int s = 0; s < ns; s++) F[5 + s] = 1.0 * F[0] * S->sc[s];
   }
-  for (int i = 0; i < NB; i++) F[i] *= area;
+  for (int i = 0; i < B; i++) F[i] *= area;
 }
 
-/* calcJacobianCoupled_HLLC, UgpWithCvCompFlow.cpp:2180-2244 (dp/dscal = 0) */
-static void jac_coupled(double A[NB][NB], const double *vel, double pp, double rrho, double hh, double sc,
+/* calcJacobianCoupled_HLLC (:2180-2244), row-major A[B][B] */
+static void jac_coupled(double *A, int ns, const double *vel, double pp, double rrho, double hh, const double *sc,
                         const double *nV, double gamma) {
+  int B = 5 + ns;
   double kapm1 = gamma - 1.0;
   double nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
   double U_k = nVel[0] + nVel[1] + nVel[2];
   double vSquHlf = 0.5 * dot3(vel, vel);
-  A[0][0] = 0.0; A[0][1] = nV[0]; A[0][2] = nV[1]; A[0][3] = nV[2]; A[0][4] = 0.0; A[0][5] = 0.0;
+  A[0] = 0.0; A[1] = nV[0]; A[2] = nV[1]; A[3] = nV[2]; A[4] = 0.0;
+  for (int s = 0; s < ns; s++) A[5 + s] = 0.0;
   for (int r = 0; r < 3; r++) {
-    A[1 + r][0] = -vel[r] * U_k + nV[r] * (kapm1 * vSquHlf + gamma * pp / rrho - kapm1 * hh);
+    double *a = A + B * (1 + r);
+    a[0] = -vel[r] * U_k + nV[r] * (kapm1 * vSquHlf + gamma * pp / rrho - kapm1 * hh);
     for (int c = 0; c < 3; c++)
-      A[1 + r][1 + c] = (r == c) ? (2.0 - gamma) * nVel[r] + U_k : vel[r] * nV[c] - kapm1 * vel[c] * nV[r];
-    A[1 + r][4] = kapm1 * nV[r];
-    A[1 + r][5] = 0.0 * nV[r];
+      a[1 + c] = (r == c) ? (2.0 - gamma) * nVel[r] + U_k : vel[r] * nV[c] - kapm1 * vel[c] * nV[r];
+    a[4] = kapm1 * nV[r];
+    for (int s = 0; s < ns; s++) a[5 + s] = 0.0 * nV[r];
   }
-  A[4][0] = U_k * ((gamma - 2.0) * vSquHlf - gamma * (hh - pp / rrho));
-  for (int c = 0; c < 3; c++) A[4][1 + c] = (hh + vSquHlf) * nV[c] - kapm1 * vel[c] * U_k;
-  A[4][4] = gamma * U_k;
-  A[4][5] = 0.0 * U_k;
-  A[5][0] = 0.0;
-  for (int c = 0; c < 3; c++) A[5][1 + c] = sc * nV[c];
-  A[5][4] = 0.0;
-  A[5][5] = rrho * U_k;
+  double *a4 = A + 4 * B;
+  a4[0] = U_k * ((gamma - 2.0) * vSquHlf - gamma * (hh - pp / rrho));
+  for (int c = 0; c < 3; c++) a4[1 + c] = (hh + vSquHlf) * nV[c] - kapm1 * vel[c] * U_k;
+  a4[4] = gamma * U_k;
+  for (int s = 0; s < ns; s++) a4[5 + s] = 0.0 * U_k;
+  for (int s = 0; s < ns; s++) {
+    double *a = A + B * (5 + s);
+    a[0] = 0.0;
+    for (int c = 0; c < 3; c++) a[1 + c] = sc[s] * nV[c];
+    a[4] = 0.0;
+    for (int q = 0; q < ns; q++) a[5 + q] = 0.0;
+    a[5 + s] = rrho * U_k;
+  }
 }
 
-/* calcdSMdU_HLLC, UgpWithCvCompFlow.cpp:2247-2266 */
-static void dsmdu(double d[NB], const double *vel, double pp, double rrho, double hh, const double *nV, double gamma,
-                  double SM, double S, double invertrho, double Factor) {
+/* calcdSMdU_HLLC (:2247-2266) */
+static void dsmdu(double *d, int ns, const double *vel, double pp, double rrho, double hh, const double *nV,
+                  double gamma, double SM, double S, double invertrho, double Factor) {
   double kapm1 = gamma - 1.0;
   double U_k = vel[0] * nV[0] + vel[1] * nV[1] + vel[2] * nV[2];
   double vSquHlf = 0.5 * dot3(vel, vel);
   d[0] = Factor * invertrho * (-U_k * U_k + kapm1 * vSquHlf + gamma * pp / rrho - kapm1 * hh + SM * S);
   for (int i = 0; i < 3; i++) d[1 + i] = Factor * invertrho * ((2 * U_k - S - SM) * nV[i] - kapm1 * vel[i]);
   d[4] = Factor * invertrho * kapm1;
-  d[5] = Factor * invertrho * 0.0;
+  for (int s = 0; s < ns; s++) d[5 + s] = Factor * invertrho * 0.0;
 }
 
-/* calcSubSonicJacobianCoupled_HLLC, UgpWithCvCompFlow.cpp:2270-2289 */
-static void subsonic_coupled(double A[NB][NB], const double *d, double rhoS, const double *rhouS, double rhoeS,
-                             double sc, double pS, double Omega, double sM, double rhoSmq, const double *nV,
+/* calcSubSonicJacobianCoupled_HLLC (:2270-2289) */
+static void subsonic_coupled(double *A, int ns, const double *d, double rhoS, const double *rhouS, double rhoeS,
+                             const double *sc, double pS, double Omega, double sM, double rhoSmq, const double *nV,
                              double area) {
+  int B = 5 + ns;
   double OmSM = Omega * sM, OmSMp1 = OmSM + 1.0;
-  for (int i = 0; i < NB; i++) {
-    A[0][i] = -OmSM * A[0][i] + area * OmSMp1 * d[i] * rhoS;
-    A[1][i] = -OmSM * A[1][i] + area * OmSMp1 * d[i] * (rhouS[0] + rhoSmq * nV[0]);
-    A[2][i] = -OmSM * A[2][i] + area * OmSMp1 * d[i] * (rhouS[1] + rhoSmq * nV[1]);
-    A[3][i] = -OmSM * A[3][i] + area * OmSMp1 * d[i] * (rhouS[2] + rhoSmq * nV[2]);
-    A[4][i] = -OmSM * A[4][i] + area * OmSMp1 * d[i] * (rhoeS + pS + rhoSmq * sM);
-    A[5][i] = -OmSM * A[5][i] + area * OmSMp1 * d[i] * rhoS * sc;
+  for (int i = 0; i < B; i++) {
+    A[i] = -OmSM * A[i] + area * OmSMp1 * d[i] * rhoS;
+    A[B + i] = -OmSM * A[B + i] + area * OmSMp1 * d[i] * (rhouS[0] + rhoSmq * nV[0]);
+    A[2 * B + i] = -OmSM * A[2 * B + i] + area * OmSMp1 * d[i] * (rhouS[1] + rhoSmq * nV[1]);
+    A[3 * B + i] = -OmSM * A[3 * B + i] + area * OmSMp1 * d[i] * (rhouS[2] + rhoSmq * nV[2]);
+    A[4 * B + i] = -OmSM * A[4 * B + i] + area * OmSMp1 * d[i] * (rhoeS + pS + rhoSmq * sM);
+    for (int s = 0; s < ns; s++)
+      A[(5 + s) * B + i] = -OmSM * A[(5 + s) * B + i] + area * OmSMp1 * d[i] * rhoS * sc[s];
   }
 }
 
-/* calcEulerFluxMatricesCoupled_HLLC, UgpWithCvCompFlow.cpp:1934-2176 (ALL_TERMS / ONLY_PRESSURE) */
-static void matrices_hllc_coupled(double (*AL)[NB], double (*AR)[NB], const cstate *L, const cstate *R, double area,
+/* calcEulerFluxMatricesCoupled_HLLC (:1934-2176): ALL_TERMS / ONLY_PRESSURE, then dU/dQ of the scalar columns */
+static void matrices_hllc_coupled(double *AL, double *AR, int ns, const cstate *L, const cstate *R, double area,
                                   const double *nV, int only_pressure) {
+  int B = 5 + ns, BB = B * B;
   if (!only_pressure) {
-    double dL[NB], dR[NB];
+    double dL[MAXB], dR[MAXB];
     double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
-    double hL = L->h + 0.0;
+    double hL = L->h + L->k;
     double rhoeL = (hL + 0.5 * uLuL) * L->rho - L->p;
     double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
-    double hR = R->h + 0.0;
+    double hR = R->h + R->k;
     double rhoeR = (hR + 0.5 * uRuR) * R->rho - R->p;
     double Rrho = sqrt(R->rho / L->rho);
     double tmp = 1.0 / (1.0 + Rrho);
@@ -1897,27 +2002,27 @@ static void matrices_hllc_coupled(double (*AL)[NB], double (*AR)[NB], const csta
     double nA[3] = {nV[0] * area, nV[1] * area, nV[2] * area};
     if (sM >= 0.0) {
       if (sL > 0.0) {
-        if (AL) jac_coupled(AL, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
-        if (AR) memset(AR, 0, sizeof(double) * NB * NB);
+        if (AL) jac_coupled(AL, ns, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
+        if (AR) memset(AR, 0, sizeof(double) * BB);
       } else {
         double Om = 1.0 / (sL - sM), sLmuL = sL - unL;
         double rhoS = L->rho * sLmuL * Om, rhouS[3];
         for (int i = 0; i < 3; i++) rhouS[i] = (L->rho * L->u[i] * sLmuL + (pStar - L->p) * nV[i]) * Om;
         double rhoeS = (sLmuL * rhoeL - L->p * unL + pStar * sM) * Om;
         if (AL) {
-          dsmdu(dL, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
-          jac_coupled(AL, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
-          double rhoSmqR = R->rho * (sR - unR);
-          subsonic_coupled(AL, dL, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, rhoSmqR, nV, area);
-          for (int i = 0; i < 5; i++) AL[i][i] += area * Om * sM * sL;
-          AL[5][0] += area * Om * sM * sL * L->sc;
-          AL[5][5] += area * Om * sM * sL * L->rho;
+          dsmdu(dL, ns, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
+          jac_coupled(AL, ns, L->u, L->p, L->rho, hL, L->sc, nA, L->gam);
+          subsonic_coupled(AL, ns, dL, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, R->rho * (sR - unR), nV, area);
+          for (int i = 0; i < 5; i++) AL[(B + 1) * i] += area * Om * sM * sL;
+          for (int s = 0; s < ns; s++) {
+            AL[(5 + s) * B] += area * Om * sM * sL * L->sc[s];
+            AL[(5 + s) * B + 5 + s] += area * Om * sM * sL * L->rho;
+          }
         }
         if (AR) {
-          dsmdu(dR, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
-          memset(AR, 0, sizeof(double) * NB * NB);
-          double rhoSmqL = L->rho * (sL - unL);
-          subsonic_coupled(AR, dR, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, rhoSmqL, nV, area);
+          dsmdu(dR, ns, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
+          memset(AR, 0, sizeof(double) * BB);
+          subsonic_coupled(AR, ns, dR, rhoS, rhouS, rhoeS, L->sc, pStar, Om, sM, L->rho * (sL - unL), nV, area);
         }
       }
     } else {
@@ -1927,137 +2032,160 @@ static void matrices_hllc_coupled(double (*AL)[NB], double (*AR)[NB], const csta
         for (int i = 0; i < 3; i++) rhouS[i] = (R->rho * R->u[i] * sRmuR + (pStar - R->p) * nV[i]) * Om;
         double rhoeS = (sRmuR * rhoeR - R->p * unR + pStar * sM) * Om;
         if (AR) {
-          dsmdu(dR, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
-          jac_coupled(AR, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
-          double rhoSmqL = L->rho * (sL - unL);
-          subsonic_coupled(AR, dR, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, rhoSmqL, nV, area);
-          for (int i = 0; i < 5; i++) AR[i][i] += area * Om * sM * sR;
-          AR[5][0] += area * Om * sM * sR * R->sc;
-          AR[5][5] += area * Om * sM * sR * R->rho;
+          dsmdu(dR, ns, R->u, R->p, R->rho, hR, nV, R->gam, sM, sR, invrhotld, -1.0);
+          jac_coupled(AR, ns, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
+          subsonic_coupled(AR, ns, dR, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, L->rho * (sL - unL), nV, area);
+          for (int i = 0; i < 5; i++) AR[(B + 1) * i] += area * Om * sM * sR;
+          for (int s = 0; s < ns; s++) {
+            AR[(5 + s) * B] += area * Om * sM * sR * R->sc[s];
+            AR[(5 + s) * B + 5 + s] += area * Om * sM * sR * R->rho;
+          }
         }
         if (AL) {
-          dsmdu(dL, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
-          memset(AL, 0, sizeof(double) * NB * NB);
-          double rhoSmqR = R->rho * (sR - unR);
-          subsonic_coupled(AL, dL, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, rhoSmqR, nV, area);
+          dsmdu(dL, ns, L->u, L->p, L->rho, hL, nV, L->gam, sM, sL, invrhotld, 1.0);
+          memset(AL, 0, sizeof(double) * BB);
+          subsonic_coupled(AL, ns, dL, rhoS, rhouS, rhoeS, R->sc, pStar, Om, sM, R->rho * (sR - unR), nV, area);
         }
       } else {
-        if (AR) jac_coupled(AR, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
-        if (AL) memset(AL, 0, sizeof(double) * NB * NB);
+        if (AR) jac_coupled(AR, ns, R->u, R->p, R->rho, hR, R->sc, nA, R->gam);
+        if (AL) memset(AL, 0, sizeof(double) * BB);
       }
     }
   } else {
     if (AL) {
-      double uLuL = dot3(L->u, L->u), hL = L->h + 0.0, g = L->gam;
-      for (int j = 0; j < NB; j++) AL[0][j] = 0.0;
+      double uLuL = dot3(L->u, L->u), hL = L->h + L->k, g = L->gam;
+      for (int j = 0; j < B; j++) AL[j] = 0.0;
       double dpdrho = 0.5 * (g - 1.0) * uLuL - (g - 1.0) * hL + g * L->p / L->rho;
       for (int r = 0; r < 3; r++) {
-        AL[1 + r][0] = dpdrho * nV[r] * area;
-        for (int c = 0; c < 3; c++) AL[1 + r][1 + c] = -(g - 1.0) * L->u[c] * nV[r] * area;
-        AL[1 + r][4] = (g - 1.0) * nV[r] * area;
-        AL[1 + r][5] = 0.0 * nV[r] * area;
+        double *a = AL + B * (1 + r);
+        a[0] = dpdrho * nV[r] * area;
+        for (int c = 0; c < 3; c++) a[1 + c] = -(g - 1.0) * L->u[c] * nV[r] * area;
+        a[4] = (g - 1.0) * nV[r] * area;
+        for (int s = 0; s < ns; s++) a[5 + s] = 0.0 * nV[r] * area;
       }
-      for (int i = 4; i < NB; i++)
-        for (int j = 0; j < NB; j++) AL[i][j] = 0.0;
+      for (int e = 4 * B; e < BB; e++) AL[e] = 0.0;
     }
-    if (AR) memset(AR, 0, sizeof(double) * NB * NB);
+    if (AR) memset(AR, 0, sizeof(double) * BB);
   }
-  /* dU/dQ for the scalar column (Q holds rho*phi, U holds phi) */
-  if (AL)
-    for (int j = 0; j < NB; j++) {
-      AL[j][0] -= L->sc / L->rho * AL[j][5];
-      AL[j][5] /= L->rho;
-    }
-  if (AR)
-    for (int j = 0; j < NB; j++) {
-      AR[j][0] -= R->sc / R->rho * AR[j][5];
-      AR[j][5] /= R->rho;
-    }
+  for (int side = 0; side < 2; side++) {
+    double *A = side ? AR : AL;
+    const cstate *S = side ? R : L;
+    if (!A) continue;
+    for (int j = 0; j < B; j++)
+      for (int s = 0; s < ns; s++) {
+        A[B * j] -= S->sc[s] / S->rho * A[B * j + 5 + s];
+        A[B * j + 5 + s] /= S->rho;
+      }
+  }
 }
 
-/* calcViscousFluxCoupled, UgpWithCvCompFlow.cpp:3040-3276 (nScal = 1, kine = 0, turbulence on) */
-static void visc_coupled(double Fv[NB], double (*A0)[NB], double (*A1)[NB], double rho0, const double *u0,
-                         const double *gu0, double h0, const double *gh0, double T0, double R0, double gam0,
-                         double sc0, const double *gs0, double rho1, const double *u1, const double *gu1, double h1,
-                         const double *gh1, double T1, double R1, double gam1, double sc1, const double *gs1,
-                         double mul, double mut, double lamOcp, double PrTurb, const double *u_fa, double diff,
-                         double diffTerm, double area, const double *nV, double smag, const double *sV,
-                         double alpha) {
+/* calcViscousFluxCoupled (UgpWithCvCompFlow.cpp:3040-3276), turbulence model on */
+typedef struct {
+  double rho, u[3], h, T, R, gam, sc[MAXS], k;
+  const double *gu, *gh, *gs[MAXS];
+} vstate;
+
+static void visc_coupled(double *Fv, double *A0, double *A1, int ns, const vstate *a, const vstate *b, double mul,
+                         double mut, double lamOcp, double PrTurb, double kine_fa, const double *u_fa,
+                         const double *diff, const double *diffTerm, double area, const double *nV, double smag,
+                         const double *sV, double alpha) {
+  int B = 5 + ns;
   double g[3][3];
   for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) g[i][j] = 0.5 * (gu0[3 * i + j] + gu1[3 * i + j]);
+    for (int j = 0; j < 3; j++) g[i][j] = 0.5 * (a->gu[3 * i + j] + b->gu[3 * i + j]);
   double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
   double muT = mul + mut;
   double tn[3];
   Fv[0] = 0.0;
   for (int i = 0; i < 3; i++)
-    tn[i] = muT * (alpha * (u1[i] - u0[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
+    tn[i] = muT * (alpha * (b->u[i] - a->u[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
                    g[1][i] * nV[1] + g[i][2] * fC[2] + g[2][i] * nV[2]);
   double tmp = 2.0 / 3.0 * muT * (g[0][0] + g[1][1] + g[2][2]);
-  tmp += 1.0 / 3.0 * (rho0 + rho1) * 0.0;
+  tmp += 1.0 / 3.0 * (a->rho + b->rho) * kine_fa;
   for (int i = 0; i < 3; i++) tn[i] -= tmp * nV[i];
   for (int i = 0; i < 3; i++) Fv[1 + i] = -area * tn[i];
   double keff = lamOcp + mut / PrTurb;
-  double enth = keff * (alpha * (h1 - h0) / smag + 0.5 * ((gh0[0] + gh1[0]) * fC[0] + (gh0[1] + gh1[1]) * fC[1] +
-                                                          (gh0[2] + gh1[2]) * fC[2]));
-  double psi = muT * (alpha * (0.0 - 0.0) / smag);
+  double enth = keff * (alpha * (b->h - a->h) / smag + 0.5 * ((a->gh[0] + b->gh[0]) * fC[0] +
+                                                             (a->gh[1] + b->gh[1]) * fC[1] +
+                                                             (a->gh[2] + b->gh[2]) * fC[2]));
+  double psi = muT * (alpha * (b->k - a->k) / smag);
   Fv[4] = -area * (enth + tn[0] * u_fa[0] + tn[1] * u_fa[1] + tn[2] * u_fa[2] + psi);
-  Fv[5] = -area * diffTerm * diff * (alpha * (sc1 - sc0) / smag + 0.5 * ((gs0[0] + gs1[0]) * fC[0] +
-                                                                          (gs0[1] + gs1[1]) * fC[1] +
-                                                                          (gs0[2] + gs1[2]) * fC[2]));
+  static const double zero3[3] = {0.0, 0.0, 0.0};
+  for (int s = 0; s < ns; s++) {
+    const double *g0 = a->gs[s] ? a->gs[s] : zero3, *g1 = b->gs[s] ? b->gs[s] : zero3;
+    Fv[5 + s] = -area * diffTerm[s] * diff[s] * (alpha * (b->sc[s] - a->sc[s]) / smag +
+                                                 0.5 * ((g0[0] + g1[0]) * fC[0] + (g0[1] + g1[1]) * fC[1] +
+                                                        (g0[2] + g1[2]) * fC[2]));
+  }
   double aas = area * alpha / smag;
   for (int side = 0; side < 2; side++) {
-    double (*A)[NB] = side ? A1 : A0;
+    double *A = side ? A1 : A0;
     if (!A) continue;
+    const vstate *v = side ? b : a;
     double sg = side ? -1.0 : 1.0;
-    double rho = side ? rho1 : rho0, hh = side ? h1 : h0, TT = side ? T1 : T0, RR = side ? R1 : R0;
-    double gm = side ? gam1 : gam0, sc = side ? sc1 : sc0;
-    const double *u = side ? u1 : u0;
-    double d11 = sg * muT * aas, d22 = d11, d33 = d11;
+    double d11 = sg * muT * aas;
     double d41 = -area * tn[0] * 0.5 + u_fa[0] * d11;
-    double d42 = -area * tn[1] * 0.5 + u_fa[1] * d22;
-    double d43 = -area * tn[2] * 0.5 + u_fa[2] * d33;
+    double d42 = -area * tn[1] * 0.5 + u_fa[1] * d11;
+    double d43 = -area * tn[2] * 0.5 + u_fa[2] * d11;
     double d44 = sg * keff * aas;
-    double dss = sg * diffTerm * diff * aas;
-    double iR = 1.0 / rho;
-    double q10 = -iR * u[0], q11 = iR, q20 = -iR * u[1], q22 = iR, q30 = -iR * u[2], q33 = iR;
-    double q40 = iR * gm * (-hh - 0.0 + RR * TT + 0.5 * dot3(u, u));
-    double q41 = -iR * u[0] * gm, q42 = -iR * u[1] * gm, q43 = -iR * u[2] * gm, q44 = iR * gm;
-    double q4s = iR * iR * 0.0, qs0 = -iR * sc, qss = iR;
-    A[1][0] = d11 * q10; A[1][1] = d11 * q11;
-    A[2][0] = d22 * q20; A[2][2] = d22 * q22;
-    A[3][0] = d33 * q30; A[3][3] = d33 * q33;
-    A[4][0] = d41 * q10 + d42 * q20 + d43 * q30 + d44 * q40;
-    A[4][1] = d41 * q11 + d44 * q41;
-    A[4][2] = d42 * q22 + d44 * q42;
-    A[4][3] = d43 * q33 + d44 * q43;
-    A[4][4] = d44 * q44;
-    A[4][5] = d44 * q4s;
-    A[5][0] = dss * qs0;
-    A[5][5] = dss * qss;
+    double iR = 1.0 / v->rho;
+    double q10 = -iR * v->u[0], q20 = -iR * v->u[1], q30 = -iR * v->u[2];
+    double q40 = iR * v->gam * (-v->h - v->k + v->R * v->T + 0.5 * dot3(v->u, v->u));
+    double q41 = -iR * v->u[0] * v->gam, q42 = -iR * v->u[1] * v->gam, q43 = -iR * v->u[2] * v->gam;
+    double q44 = iR * v->gam;
+    A[B + 0] = d11 * q10; A[B + 1] = d11 * iR;
+    A[2 * B + 0] = d11 * q20; A[2 * B + 2] = d11 * iR;
+    A[3 * B + 0] = d11 * q30; A[3 * B + 3] = d11 * iR;
+    A[4 * B + 0] = d41 * q10 + d42 * q20 + d43 * q30 + d44 * q40;
+    A[4 * B + 1] = d41 * iR + d44 * q41;
+    A[4 * B + 2] = d42 * iR + d44 * q42;
+    A[4 * B + 3] = d43 * iR + d44 * q43;
+    A[4 * B + 4] = d44 * q44;
+    for (int s = 0; s < ns; s++) {
+      double dss = sg * diffTerm[s] * diff[s] * aas;
+      A[4 * B + 5 + s] = d44 * (iR * iR * 0.0);
+      A[(5 + s) * B + 0] = dss * (-iR * v->sc[s]);
+      A[(5 + s) * B + 5 + s] = dss * iR;
+    }
   }
 }
 
-static void add_blk6(double *A, int slot, double (*B)[NB], double sgn) {
-  double *a = &A[NB * NB * slot];
-  for (int i = 0; i < NB; i++)
-    for (int j = 0; j < NB; j++) a[NB * i + j] += sgn * B[i][j];
+static void add_blk(double *A, int B, int slot, const double *M, double sgn) {
+  double *a = &A[(size_t)B * B * slot];
+  for (int e = 0; e < B * B; e++) a[e] += sgn * M[e];
 }
 
-static cstate cell_cstate(jo_case *h, int c) {
+static cstate cell_cstate(jo_case *h, const jo_turb *t, int c) {
   cstate s = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->press[c], h->temp[c],
-              h->enthalpy[c], h->RoM[c], h->gam[c], sa_of(h)->phi[c]};
+              h->enthalpy[c], h->RoM[c], h->gam[c], {0.0, 0.0}, 0.0};
+  for (int q = 0; q < t->ns; q++) s.sc[q] = t->phi[q][c];
   return s;
 }
-static cstate bfa_cstate(jo_case *h, int f) {
+static cstate bfa_cstate(jo_case *h, const jo_turb *t, int f) {
   cstate s = {h->rho_bfa[f], {h->vel_bfa[3 * f], h->vel_bfa[3 * f + 1], h->vel_bfa[3 * f + 2]}, h->p_bfa[f],
-              h->T_bfa[f], h->h_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], sa_of(h)->phi_bfa[f]};
+              h->T_bfa[f], h->h_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], {0.0, 0.0}, 0.0};
+  for (int q = 0; q < t->ns; q++) s.sc[q] = t->phi_bfa[q][f];
   return s;
+}
+static vstate cell_vstate(jo_case *h, const jo_turb *t, int c) {
+  vstate v = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->enthalpy[c], h->temp[c],
+              h->RoM[c], h->gam[c], {0.0, 0.0}, 0.0, &h->grad_u[9 * c], &h->grad_h[3 * c], {NULL, NULL}};
+  for (int q = 0; q < t->ns; q++) {
+    v.sc[q] = t->phi[q][c];
+    v.gs[q] = &t->grad_phi[q][3 * c];
+  }
+  if (t->model == JG_TURB_SST) v.k = t->phi[0][c];
+  return v;
+}
+static vstate bfa_vstate(jo_case *h, const jo_turb *t, int f, int c) {
+  vstate v = {h->rho_bfa[f], {h->vel_bfa[3 * f], h->vel_bfa[3 * f + 1], h->vel_bfa[3 * f + 2]}, h->h_bfa[f],
+              h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], {0.0, 0.0}, 0.0, &h->grad_u[9 * c], &h->grad_h[3 * c],
+              {NULL, NULL}};
+  return v;
 }
 
-/* face reconstruction with the scalar (JoeWithModels.cpp:4837-4921), then
- * calcThermoProp_p for T and h (ideal gas) */
-static void reconstruct_c(jo_case *h, int c, int f, cstate *s) {
+/* face reconstruction with the scalars (JoeWithModels.cpp:4837-4921), then calcThermoProp_p */
+static void reconstruct_c(jo_case *h, const jo_turb *t, int c, int f, cstate *s) {
   double r0[3];
   for (int i = 0; i < 3; i++) r0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c + i];
   double rho0 = h->rho[c] + dot3(r0, &h->grad_rho[3 * c]);
@@ -2069,7 +2197,7 @@ static void reconstruct_c(jo_case *h, int c, int f, cstate *s) {
     s->rho = rho0;
     s->p = p0;
     for (int i = 0; i < 3; i++) s->u[i] = h->vel[3 * c + i] + dot3(r0, &h->grad_u[9 * c + 3 * i]);
-    s->sc += dot3(r0, &sa_of(h)->grad_phi[3 * c]);
+    for (int q = 0; q < t->ns; q++) s->sc[q] += dot3(r0, &t->grad_phi[q][3 * c]);
   }
   s->R = h->p.R_gas;
   s->gam = h->p.gamma;
@@ -2077,14 +2205,52 @@ static void reconstruct_c(jo_case *h, int c, int f, cstate *s) {
   s->h = s->gam * s->R / (s->gam - 1.0) * s->T;
 }
 
-/* calcRhsCoupled (JoeWithModels.cpp:4597-4611) for SA: rhs[ncv][6], A[nbocv_s][6][6] (accumulated) */
+/* scalar diffusivities (diffusivityHookScalarRansTurb: TurbModel_SA.h:130-173, TurbModel_KOMSST.h:169-256) */
+static void turb_diffusivity(jo_case *h, jo_turb *t) {
+  const jg_mesh *m = &h->m;
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double w0, w1;
+    face_weights(h, f, c0, c1, &w0, &w1);
+    if (t->model == JG_TURB_SA) {
+      double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
+      double nu_fa = (w1 * t->phi[0][c0] + w0 * t->phi[0][c1]) / (w0 + w1);
+      t->diff[0][f] = (1.0 / SA_SIGMA) * (h->mul_fa[f] + rho_fa * nu_fa);
+    } else {
+      double f1_fa = (w1 * t->F1[c0] + w0 * t->F1[c1]) / (w0 + w1);
+      t->diff[0][f] = h->mul_fa[f] + (SST_SK1 * f1_fa + (1. - f1_fa) * SST_SK2) * h->mut_fa[f];
+      t->diff[1][f] = h->mul_fa[f] + (SST_SO1 * f1_fa + (1. - f1_fa) * SST_SO2) * h->mut_fa[f];
+    }
+  }
+  for (int z = 0; z < m->nzones; z++) {
+    const jg_zone *zn = &m->zones[z];
+    for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
+      int c0 = m->cvofa[2 * f];
+      if (t->model == JG_TURB_SA) {
+        t->diff[0][f] = (zn->kind == JG_BC_WALL) ? (1.0 / SA_SIGMA) * h->mul_fa[f]
+                                                 : (1.0 / SA_SIGMA) * (h->mul_fa[f] + h->rho_bfa[f] * t->phi_bfa[0][f]);
+      } else if (zn->kind == JG_BC_WALL) {
+        t->diff[0][f] = h->mul_fa[f];
+        t->diff[1][f] = h->mul_fa[f];
+      } else {
+        double F1 = t->F1[c0];
+        t->diff[0][f] = h->mul_fa[f] + (SST_SK1 * F1 + (1. - F1) * SST_SK2) * h->mut_fa[f];
+        t->diff[1][f] = h->mul_fa[f] + (SST_SO1 * F1 + (1. - F1) * SST_SO2) * h->mut_fa[f];
+      }
+    }
+  }
+}
+
+/* calcRhsCoupled (JoeWithModels.cpp:4597-4611): rhs[ncv][B], A[nbocv_s][B][B] (accumulated), B = 5 + nscal */
 void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
   const jg_mesh *m = &h->m;
   const jg_params *p = &h->p;
-  jo_sa *s = sa_of(h);
+  jo_turb *t = turb_of(h);
+  const int ns = t->ns, B = 5 + ns, BB = B * B;
+  const int sst = t->model == JG_TURB_SST;
   int visc = p->mu_ref > 0.0;
   int only_p = p->symm_bc == JG_SYMM_ANALYTICAL;
-  memset(rhs, 0, sizeof(double) * NB * h->ncv);
+  memset(rhs, 0, sizeof(double) * B * h->ncv);
   /* gradients, JoeWithModels.cpp:4683-4754 */
   if (p->second_order || visc) grad_vector(h, h->grad_u, h->vel, h->vel_bfa, p->limiter, h->sos);
   if (p->second_order) {
@@ -2092,52 +2258,42 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
     grad_scalar(h, h->grad_p, h->press, h->p_bfa, p->limiter, h->press, NULL);
   }
   if (visc) grad_scalar(h, h->grad_h, h->enthalpy, h->h_bfa, p->limiter, h->enthalpy, NULL);
-  if (p->second_order || visc) grad_scalar(h, s->grad_phi, s->phi, s->phi_bfa, p->limiter, s->phi, NULL);
-  if (visc) {
-    /* RansTurbSA::diffusivityHookScalarRansTurb, TurbModel_SA.h:130-173 */
-    double invSigma = 1.0 / SA_SIGMA;
-    for (int f = h->nfa_b; f < h->nfa; f++) {
-      int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
-      double dx0[3], dx1[3];
-      for (int i = 0; i < 3; i++) {
-        dx0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
-        dx1[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c1 + i];
-      }
-      double w0 = sqrt(dot3(dx0, dx0)), w1 = sqrt(dot3(dx1, dx1));
-      double rho_fa = (w1 * h->rho[c0] + w0 * h->rho[c1]) / (w0 + w1);
-      double nu_fa = (w1 * s->phi[c0] + w0 * s->phi[c1]) / (w0 + w1);
-      s->diff[f] = invSigma * (h->mul_fa[f] + rho_fa * nu_fa);
-    }
-    for (int z = 0; z < m->nzones; z++) {
-      const jg_zone *zn = &m->zones[z];
-      for (int f = zn->ifa_f; f <= zn->ifa_l; f++)
-        s->diff[f] = (zn->kind == JG_BC_WALL) ? invSigma * h->mul_fa[f]
-                                              : invSigma * (h->mul_fa[f] + h->rho_bfa[f] * s->phi_bfa[f]);
-    }
-  }
-  double F[NB], Fv[NB], Apl[NB][NB], Ami[NB][NB], A0[NB][NB], A1[NB][NB];
+  if (p->second_order || visc)
+    for (int q = 0; q < ns; q++) grad_scalar(h, t->grad_phi[q], t->phi[q], t->phi_bfa[q], p->limiter, t->phi[q], NULL);
+  if (visc) turb_diffusivity(h, t);
+  double F[MAXB], Fv[MAXB], Apl[MAXB * MAXB], Ami[MAXB * MAXB], A0[MAXB * MAXB], A1[MAXB * MAXB];
   memset(A0, 0, sizeof(A0));
   memset(A1, 0, sizeof(A1));
+  double ones[MAXS] = {1.0, 1.0}, dterm[MAXS], dfa[MAXS];
   /* internal faces, JoeWithModels.cpp:4797-5132 */
   for (int f = h->nfa_b; f < h->nfa; f++) {
     int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
     double nV[3];
     double area = norm3(nV, &m->fa_normal[3 * f]);
-    cstate L = cell_cstate(h, c0), R = cell_cstate(h, c1);
+    cstate L = cell_cstate(h, t, c0), R = cell_cstate(h, t, c1);
     if (p->second_order) {
-      reconstruct_c(h, c0, f, &L);
-      reconstruct_c(h, c1, f, &R);
+      reconstruct_c(h, t, c0, f, &L);
+      reconstruct_c(h, t, c1, f, &R);
     }
-    flux_hllc_coupled(F, &L, &R, area, nV, 0);
-    for (int i = 0; i < NB; i++) { rhs[NB * c0 + i] -= F[i]; rhs[NB * c1 + i] += F[i]; }
+    double kine_fa = 0.0;
+    if (sst) {
+      L.k = L.sc[0];  /* face value (reconstructed in second order) */
+      R.k = R.sc[0];
+      double w0, w1;
+      face_weights(h, f, c0, c1, &w0, &w1);
+      kine_fa = (w1 * t->phi[0][c0] + w0 * t->phi[0][c1]) / (w0 + w1);
+    }
+    flux_hllc_coupled(F, ns, &L, &R, area, nV, 0);
+    for (int i = 0; i < B; i++) { rhs[B * c0 + i] -= F[i]; rhs[B * c1 + i] += F[i]; }
     int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
     if (implicit) {
-      cstate L0 = cell_cstate(h, c0), R0 = cell_cstate(h, c1);
-      matrices_hllc_coupled(Apl, Ami, &L0, &R0, area, nV, 0);
-      add_blk6(A, n00, Apl, 1.0);
-      add_blk6(A, n01, Ami, 1.0);
-      add_blk6(A, n11, Ami, -1.0);
-      add_blk6(A, n10, Apl, -1.0);
+      cstate L0 = cell_cstate(h, t, c0), R0 = cell_cstate(h, t, c1);
+      if (sst) { L0.k = t->phi[0][c0]; R0.k = t->phi[0][c1]; }
+      matrices_hllc_coupled(Apl, Ami, ns, &L0, &R0, area, nV, 0);
+      add_blk(A, B, n00, Apl, 1.0);
+      add_blk(A, B, n01, Ami, 1.0);
+      add_blk(A, B, n11, Ami, -1.0);
+      add_blk(A, B, n10, Apl, -1.0);
     }
     if (visc) {
       double sV[3];
@@ -2146,141 +2302,175 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
       double alpha = dot3(nV, sV);
       double uf[3];
       for (int i = 0; i < 3; i++) uf[i] = 0.5 * (h->vel[3 * c0 + i] + h->vel[3 * c1 + i]);
-      visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, h->rho[c0], &h->vel[3 * c0],
-                   &h->grad_u[9 * c0], h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0],
-                   s->phi[c0], &s->grad_phi[3 * c0], h->rho[c1], &h->vel[3 * c1], &h->grad_u[9 * c1],
-                   h->enthalpy[c1], &h->grad_h[3 * c1], h->temp[c1], h->RoM[c1], h->gam[c1], s->phi[c1],
-                   &s->grad_phi[3 * c1], h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, uf, s->diff[f],
-                   1.0, area, nV, smag, sV, alpha);
-      for (int i = 0; i < NB; i++) { rhs[NB * c0 + i] -= Fv[i]; rhs[NB * c1 + i] += Fv[i]; }
+      vstate v0 = cell_vstate(h, t, c0), v1 = cell_vstate(h, t, c1);
+      for (int q = 0; q < ns; q++) dfa[q] = t->diff[q][f];
+      visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, ns, &v0, &v1, h->mul_fa[f], h->mut_fa[f],
+                   h->lamOcp_fa[f], p->PrTurb, kine_fa, uf, dfa, ones, area, nV, smag, sV, alpha);
+      for (int i = 0; i < B; i++) { rhs[B * c0 + i] -= Fv[i]; rhs[B * c1 + i] += Fv[i]; }
       if (implicit) {
-        add_blk6(A, n00, A0, 1.0);
-        add_blk6(A, n01, A1, 1.0);
-        add_blk6(A, n11, A1, -1.0);
-        add_blk6(A, n10, A0, -1.0);
+        add_blk(A, B, n00, A0, 1.0);
+        add_blk(A, B, n01, A1, 1.0);
+        add_blk(A, B, n11, A1, -1.0);
+        add_blk(A, B, n10, A0, -1.0);
       }
     }
   }
   /* boundary faces, JoeWithModels.cpp:5139-5799 */
-  double zero3[3] = {0.0, 0.0, 0.0};
   for (int z = 0; z < m->nzones; z++) {
     const jg_zone *zn = &m->zones[z];
-    double diffTerm = (zn->scal_bc & 1) ? 1.0 : 0.0;
+    for (int q = 0; q < ns; q++) dterm[q] = (zn->scal_bc & ((1 << q) | (1 << (4 + q)))) ? 1.0 : 0.0;
     for (int f = zn->ifa_f; f <= zn->ifa_l; f++) {
       int c0 = m->cvofa[2 * f];
       int n00 = m->nbocv_i[c0];
       double nV[3];
       double area = norm3(nV, &m->fa_normal[3 * f]);
-      cstate B = bfa_cstate(h, f);
-      if (zn->kind == JG_BC_SYMMETRY || zn->kind == JG_BC_WALL) {
-        flux_hllc_coupled(F, &B, &B, area, nV, only_p);
-        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+      cstate Bs = bfa_cstate(h, t, f);
+      for (int q = 0; q < ns; q++) dfa[q] = t->diff[q][f];
+      if (zn->kind == JG_BC_SYMMETRY || zn->kind == JG_BC_NEUMANN) {
+        if (sst) Bs.k = t->phi_bfa[0][f];
+        int op = (zn->kind == JG_BC_SYMMETRY) ? only_p : 0;
+        flux_hllc_coupled(F, ns, &Bs, &Bs, area, nV, op);
+        for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
-          if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
-            matrices_hllc_coupled(Apl, Ami, &B, &B, area, nV, 0);
-            for (int i = 0; i < NB; i++)
-              for (int j = 0; j < NB; j++) A[NB * NB * n00 + NB * i + j] += Apl[i][j] + Ami[i][j];
+          if (zn->kind == JG_BC_NEUMANN || p->symm_bc == JG_SYMM_NEW_NUMERIC) {
+            matrices_hllc_coupled(Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
+            for (int e = 0; e < BB; e++)
+              A[(size_t)BB * n00 + e] += (p->symm_bc == JG_SYMM_NEW_NUMERIC) ? Apl[e] + Ami[e] : Apl[e];
           } else {
-            matrices_hllc_coupled(Apl, NULL, &B, &B, area, nV, only_p);
-            add_blk6(A, n00, Apl, 1.0);
+            matrices_hllc_coupled(Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
+            add_blk(A, B, n00, Apl, 1.0);
           }
         }
         if (visc && zn->kind == JG_BC_SYMMETRY) {
           const double *g = &h->grad_u[9 * c0];
-          double tmp = 2.0 / 3.0 * ((h->mul_fa[f] + h->mut_fa[f]) * (g[0] + g[4] + g[8]) + h->rho_bfa[f] * 0.0);
-          for (int i = 0; i < 3; i++) rhs[NB * c0 + 1 + i] -= area * tmp * nV[i];
+          double tmp = 2.0 / 3.0 * ((h->mul_fa[f] + h->mut_fa[f]) * (g[0] + g[4] + g[8]) + h->rho_bfa[f] * Bs.k);
+          for (int i = 0; i < 3; i++) rhs[B * c0 + 1 + i] -= area * tmp * nV[i];
         }
-        if (visc && zn->kind == JG_BC_WALL) {
+        if (visc && zn->kind == JG_BC_NEUMANN) {
           double sV[3];
           for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
           double smag = fabs(dot3(sV, nV));
-          visc_coupled(Fv, implicit ? A0 : NULL, NULL, h->rho[c0], &h->vel[3 * c0], &h->grad_u[9 * c0],
-                       h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0], s->phi[c0],
-                       &s->grad_phi[3 * c0], h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0], h->h_bfa[f],
-                       &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], s->phi_bfa[f],
-                       &s->grad_phi[3 * c0], h->mul_fa[f], 0.0, h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f],
-                       s->diff[f], diffTerm, area, nV, smag, nV, 1.0);
-          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
-          if (implicit) add_blk6(A, n00, A0, 1.0);
+          vstate vb = bfa_vstate(h, t, f, c0);
+          for (int q = 0; q < ns; q++) vb.sc[q] = t->phi_bfa[q][f];
+          vb.k = Bs.k;
+          visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, ns, &vb, &vb, h->mul_fa[f], h->mut_fa[f],
+                       h->lamOcp_fa[f], p->PrTurb, Bs.k, &h->vel_bfa[3 * f], dfa, ones, area, nV, smag, nV, 1.0);
+          for (int i = 0; i < B; i++) rhs[B * c0 + i] -= Fv[i];
+          if (implicit) add_blk(A, B, n00, A0, 1.0);
         }
-      } else if (zn->kind == JG_BC_NEUMANN) {
-        flux_hllc_coupled(F, &B, &B, area, nV, 0);
-        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+      } else if (zn->kind == JG_BC_WALL) {
+        /* the wall branch keeps the face kinetic energy at 0 (JoeWithModels.cpp:5448-5452) */
+        flux_hllc_coupled(F, ns, &Bs, &Bs, area, nV, only_p);
+        for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
-          matrices_hllc_coupled(Apl, Ami, &B, &B, area, nV, 0);
-          for (int i = 0; i < NB; i++)
-            for (int j = 0; j < NB; j++)
-              A[NB * NB * n00 + NB * i + j] += (p->symm_bc == JG_SYMM_NEW_NUMERIC) ? Apl[i][j] + Ami[i][j] : Apl[i][j];
+          if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
+            matrices_hllc_coupled(Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
+            for (int e = 0; e < BB; e++) A[(size_t)BB * n00 + e] += Apl[e] + Ami[e];
+          } else {
+            matrices_hllc_coupled(Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
+            add_blk(A, B, n00, Apl, 1.0);
+          }
         }
         if (visc) {
           double sV[3];
           for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
           double smag = fabs(dot3(sV, nV));
-          visc_coupled(Fv, implicit ? A0 : NULL, implicit ? A1 : NULL, h->rho_bfa[f], &h->vel_bfa[3 * f],
-                       &h->grad_u[9 * c0], h->h_bfa[f], &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f],
-                       h->gam_bfa[f], s->phi_bfa[f], zero3, h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0],
-                       h->h_bfa[f], &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], s->phi_bfa[f],
-                       zero3, h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f], s->diff[f],
-                       1.0, area, nV, smag, nV, 1.0);
-          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
-          if (implicit) add_blk6(A, n00, A0, 1.0);
+          vstate v0 = cell_vstate(h, t, c0);
+          vstate vb = bfa_vstate(h, t, f, c0);
+          for (int q = 0; q < ns; q++) {
+            vb.sc[q] = t->phi_bfa[q][f];
+            vb.gs[q] = &t->grad_phi[q][3 * c0];
+          }
+          vb.k = 0.0;
+          visc_coupled(Fv, implicit ? A0 : NULL, NULL, ns, &v0, &vb, h->mul_fa[f], 0.0, h->lamOcp_fa[f], p->PrTurb,
+                       0.0, &h->vel_bfa[3 * f], dfa, dterm, area, nV, smag, nV, 1.0);
+          for (int i = 0; i < B; i++) rhs[B * c0 + i] -= Fv[i];
+          if (implicit) add_blk(A, B, n00, A0, 1.0);
         }
       } else {
         /* CBC, CBC_SUBSONIC_INLET/OUTLET, FARFIELD: JoeWithModels.cpp:5624-5788 */
-        cstate L = cell_cstate(h, c0);
-        if (p->second_order) reconstruct_c(h, c0, f, &L);
-        flux_hllc_coupled(F, &L, &B, area, nV, 0);
-        for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= F[i];
+        cstate L = cell_cstate(h, t, c0);
+        if (p->second_order) reconstruct_c(h, t, c0, f, &L);
+        if (sst) { L.k = L.sc[0]; Bs.k = t->phi_bfa[0][f]; }
+        flux_hllc_coupled(F, ns, &L, &Bs, area, nV, 0);
+        for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
-          cstate L0 = cell_cstate(h, c0);
-          matrices_hllc_coupled(Apl, NULL, &L0, &B, area, nV, 0);
-          add_blk6(A, n00, Apl, 1.0);
+          cstate L0 = cell_cstate(h, t, c0);
+          if (sst) L0.k = t->phi[0][c0];
+          matrices_hllc_coupled(Apl, NULL, ns, &L0, &Bs, area, nV, 0);
+          add_blk(A, B, n00, Apl, 1.0);
         }
         if (visc) {
           double sV[3];
           for (int i = 0; i < 3; i++) sV[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
           double smag = norm3(sV, sV);
           double alpha = dot3(nV, sV);
-          /* the outer state's scalar is the reconstructed face value (as the reference passes it) */
-          visc_coupled(Fv, implicit ? A0 : NULL, NULL, h->rho[c0], &h->vel[3 * c0], &h->grad_u[9 * c0],
-                       h->enthalpy[c0], &h->grad_h[3 * c0], h->temp[c0], h->RoM[c0], h->gam[c0], s->phi[c0],
-                       &s->grad_phi[3 * c0], h->rho_bfa[f], &h->vel_bfa[3 * f], &h->grad_u[9 * c0], h->h_bfa[f],
-                       &h->grad_h[3 * c0], h->T_bfa[f], h->RoM_bfa[f], h->gam_bfa[f], L.sc, &s->grad_phi[3 * c0],
-                       h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f], p->PrTurb, &h->vel_bfa[3 * f], s->diff[f],
-                       diffTerm, area, nV, smag, sV, alpha);
-          for (int i = 0; i < NB; i++) rhs[NB * c0 + i] -= Fv[i];
-          if (implicit) add_blk6(A, n00, A0, 1.0);
+          vstate v0 = cell_vstate(h, t, c0);
+          vstate vb = bfa_vstate(h, t, f, c0);
+          /* the outer state carries the reconstructed face scalars, as the reference passes them */
+          for (int q = 0; q < ns; q++) {
+            vb.sc[q] = L.sc[q];
+            vb.gs[q] = &t->grad_phi[q][3 * c0];
+          }
+          vb.k = Bs.k;
+          visc_coupled(Fv, implicit ? A0 : NULL, NULL, ns, &v0, &vb, h->mul_fa[f], h->mut_fa[f], h->lamOcp_fa[f],
+                       p->PrTurb, Bs.k, &h->vel_bfa[3 * f], dfa, dterm, area, nV, smag, sV, alpha);
+          for (int i = 0; i < B; i++) rhs[B * c0 + i] -= Fv[i];
+          if (implicit) add_blk(A, B, n00, A0, 1.0);
         }
       }
     }
   }
-  /* RansTurbSA::sourceHookRansTurbCoupled, TurbModel_SA.h:359-434 */
+  /* source terms: sourceHookRansTurbCoupled (TurbModel_SA.h:359-434; TurbModel_KOMSST.h:306-340) */
   for (int c = 0; c < h->ncv; c++) {
-    double mue = face_avg(h, h->mul_fa, c);
-    double Om = dmax(s->vortMag[c], 1.e-8);
-    double Strainrate = dmax(s->strMag[c], 1.e-8);
-    double d = s->wallDist[c];
-    double nu = s->phi[c];
-    double chi = nu * h->rho[c] / mue;
-    double chi_3 = pow(chi, 3.0);
-    double inv_K2d2 = 1.0 / (SA_K2 * d * d);
-    double fv1 = chi_3 / (chi_3 + SA_CV1_3);
-    double fv2 = 1.0 - chi / (1.0 + chi * fv1);
-    double S = dmax(Om + dmin(0.0, Strainrate - Om) * 0.0, 0.0);
-    double Shat = S + nu * fv2 * inv_K2d2;
-    double inv_Shat = 1.0 / dmax(Shat, 1.0e-8);
-    double r = dmin(nu * inv_Shat * inv_K2d2, 10.0);
-    double g = r + SA_CW2 * (pow(r, 6.0) - r);
-    double g_6 = pow(g, 6.0);
-    double fw = g * pow((1.0 + SA_CW3_6) / (g_6 + SA_CW3_6), 1.0 / 6.0);
-    double H1 = SA_CB1 * Shat * nu;
-    double H2 = -SA_CW1 * fw * nu * nu / pow(d, 2.0);
-    double H3 = SA_CB2 / SA_SIGMA * dot3(&s->grad_phi[3 * c], &s->grad_phi[3 * c]);
-    rhs[NB * c + 5] += h->rho[c] * m->cv_volume[c] * (H1 + H2 + H3);
-    if (implicit) {
-      double d_H1 = 0.0;
-      double d_H2 = -2.0 * SA_CW1 * fw * nu / pow(d, 2.0);
-      A[NB * NB * m->nbocv_i[c] + NB * 5 + 5] -= (d_H1 + d_H2) * m->cv_volume[c];
+    size_t d0 = (size_t)BB * m->nbocv_i[c];
+    double vol = m->cv_volume[c], rho = h->rho[c];
+    if (t->model == JG_TURB_SA) {
+      double mue = face_avg(h, h->mul_fa, c);
+      double Om = dmax(t->vortMag[c], 1.e-8);
+      double Strainrate = dmax(t->strMag[c], 1.e-8);
+      double d = t->wallDist[c];
+      double nu = t->phi[0][c];
+      double chi = nu * rho / mue;
+      double chi_3 = pow(chi, 3.0);
+      double inv_K2d2 = 1.0 / (SA_K2 * d * d);
+      double fv1 = chi_3 / (chi_3 + SA_CV1_3);
+      double fv2 = 1.0 - chi / (1.0 + chi * fv1);
+      double S = dmax(Om + dmin(0.0, Strainrate - Om) * 0.0, 0.0);
+      double Shat = S + nu * fv2 * inv_K2d2;
+      double inv_Shat = 1.0 / dmax(Shat, 1.0e-8);
+      double r = dmin(nu * inv_Shat * inv_K2d2, 10.0);
+      double g = r + SA_CW2 * (pow(r, 6.0) - r);
+      double g_6 = pow(g, 6.0);
+      double fw = g * pow((1.0 + SA_CW3_6) / (g_6 + SA_CW3_6), 1.0 / 6.0);
+      double H1 = SA_CB1 * Shat * nu;
+      double H2 = -SA_CW1 * fw * nu * nu / pow(d, 2.0);
+      double H3 = SA_CB2 / SA_SIGMA * dot3(&t->grad_phi[0][3 * c], &t->grad_phi[0][3 * c]);
+      rhs[B * c + 5] += rho * vol * (H1 + H2 + H3);
+      if (implicit) {
+        double d_H1 = 0.0;
+        double d_H2 = -2.0 * SA_CW1 * fw * nu / pow(d, 2.0);
+        A[d0 + B * 5 + 5] -= (d_H1 + d_H2) * vol;
+      }
+    } else {
+      double k = t->phi[0][c], om = t->phi[1][c];
+      double F1 = t->F1[c];
+      double alfa_1 = SST_B1 / SST_BS - SST_SO1 * pow(0.41, 2.0) / sqrt(SST_BS);
+      double alfa_2 = SST_B2 / SST_BS - SST_SO2 * pow(0.41, 2.0) / sqrt(SST_BS);
+      double alfa = F1 * alfa_1 + (1.0 - F1) * alfa_2;
+      double beta = F1 * SST_B1 + (1.0 - F1) * SST_B2;
+      double zeta = dmin(1.0 / om, SST_A1 / (t->vortMag[c] * t->F2[c]));
+      double mut = dmin(dmax(rho * k * zeta, 1.0e-8), 1.0e5);
+      double Pk = dmax(mut * t->strMag[c] * t->strMag[c] - 2. / 3. * rho * k * t->diverg[c], 0.0);
+      Pk = dmin(Pk, 20.0 * SST_BS * rho * k * om);
+      rhs[B * c + 5] += (Pk - SST_BS * rho * om * k) * vol;
+      zeta = dmax(om, t->vortMag[c] * t->F2[c] / SST_A1);
+      Pk = dmax(t->strMag[c] * t->strMag[c] - 2. / 3. * zeta * t->diverg[c], 0.0);
+      rhs[B * c + 6] += (alfa * rho * Pk + (1.0 - F1) * t->crossDiff[c] - beta * rho * om * om) * vol;
+      if (implicit) {
+        A[d0 + B * 5 + 5] -= -SST_BS * om * vol;
+        A[d0 + B * 6 + 6] -= -2.0 * beta * om * vol;
+      }
     }
   }
 }
@@ -2346,7 +2536,7 @@ int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double 
     ludeco_n(&LU[(size_t)B * B * c], B);
   }
   memset(x, 0, sizeof(double) * B * n);
-  double b[8];
+  double b[MAXB];
   for (int s = 0; s < sweeps; s++)
     for (int q = 0; q < ncol; q++) {
       int col = (s % 2 == 0) ? q : ncol - 1 - q;
@@ -2368,37 +2558,40 @@ int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double 
 }
 
 /* runBackwardEulerCoupled loop body (JoeWithModels.cpp:4416-4529) with the
- * GPU's block relaxation for the linear solve; resid[6] = last L1 residual */
+ * GPU's block relaxation for the linear solve; resid[B] = last L1 residual */
 int jo_step_coupled(jo_case *h, int nsteps, double *resid) {
   const jg_params *p = &h->p;
+  jo_turb *t = turb_of(h);
+  const int ns = t->ns, B = 5 + ns;
   int n = h->ncv, nbs = h->nbs;
-  jo_sa *s = sa_of(h);
-  double *A = dalloc((size_t)NB * NB * nbs), *dq = dalloc((size_t)NB * n), *rhs = dalloc((size_t)NB * n);
+  double *A = dalloc((size_t)B * B * nbs), *dq = dalloc((size_t)B * n), *rhs = dalloc((size_t)B * n);
   int err = 0;
   for (int it = 0; it < nsteps; it++) {
     h->step++;
     if ((h->step >= p->cfl_after) && (h->step % p->cfl_interval == 0) && (h->cfl < p->cfl_max)) h->cfl *= p->cfl_factor;
     jo_calc_dt(h, h->cfl);
-    memset(A, 0, sizeof(double) * NB * NB * nbs);
+    memset(A, 0, sizeof(double) * B * B * nbs);
     jo_calc_rhs_coupled(h, rhs, A, 1);
-    double r[NB] = {0, 0, 0, 0, 0, 0};
+    double r[MAXB] = {0, 0, 0, 0, 0, 0, 0};
     for (int c = 0; c < n; c++)
-      for (int i = 0; i < NB; i++) r[i] += fabs(rhs[NB * c + i]);
+      for (int i = 0; i < B; i++) r[i] += fabs(rhs[B * c + i]);
     for (int c = 0; c < n; c++) {
-      for (int i = 0; i < NB; i++) rhs[NB * c + i] *= p->under_relax;
+      for (int i = 0; i < B; i++) rhs[B * c + i] *= p->under_relax;
       double tmp = h->m.cv_volume[c] / (h->local_dt[c]);
-      for (int i = 0; i < NB; i++) A[(size_t)NB * NB * h->m.nbocv_i[c] + (NB + 1) * i] += tmp;
+      for (int i = 0; i < B; i++) A[(size_t)B * B * h->m.nbocv_i[c] + (B + 1) * i] += tmp;
     }
-    jo_solve_blocks(h, NB, dq, A, rhs, p->ls_max_iter, p->lin_solver == JG_LS_SGS);
+    jo_solve_blocks(h, B, dq, A, rhs, p->ls_max_iter, p->lin_solver == JG_LS_SGS);
     for (int c = 0; c < n; c++) {
-      h->rho[c] += dq[NB * c];
-      for (int i = 0; i < 3; i++) h->rhou[3 * c + i] += dq[NB * c + 1 + i];
-      h->rhoE[c] += dq[NB * c + 4];
+      h->rho[c] += dq[B * c];
+      for (int i = 0; i < 3; i++) h->rhou[3 * c + i] += dq[B * c + 1 + i];
+      h->rhoE[c] += dq[B * c + 4];
     }
-    for (int c = 0; c < n; c++)
-      s->phi[c] = dmin(dmax((s->phi[c] * (h->rho[c] - dq[NB * c]) + dq[NB * c + 5]) / h->rho[c], SA_LOWER), SA_UPPER);
+    for (int q = 0; q < ns; q++)
+      for (int c = 0; c < n; c++)
+        t->phi[q][c] = dmin(dmax((t->phi[q][c] * (h->rho[c] - dq[B * c]) + dq[B * c + 5 + q]) / h->rho[c], t->lower[q]),
+                            t->upper[q]);
     if (jo_calc_state_coupled(h) != 0) err = -1;
-    if (resid) memcpy(resid, r, sizeof(r));
+    if (resid) memcpy(resid, r, sizeof(double) * B);
   }
   free(A); free(dq); free(rhs);
   return err;

@@ -38,14 +38,16 @@ int jo_step_count(jo_case *h);
 void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area,
                          const double *nvec, double *F, double *AL, double *AR);
 
-/* Coupled path with the Spalart-Allmaras model (nscal = 1, block size 6):
- * scalar nuSA in/out, wall distance (calcWallDistance), the coupled preamble
- * (state + material + BC + scalar BC + calcRansTurbViscMuet), calcRhsCoupled
- * (rhs[ncv][6], A[nbocv_s][6][6] accumulated), block relaxation of a B x B
- * system (sgs 0: Jacobi, 1: multicolour Gauss-Seidel) and the coupled step.
- * Named SA arrays: "phi","phi_bfa","grad_phi","diff","wallDist","strMag","vortMag". */
-void jo_set_scalar(jo_case *h, const double *phi);
-void jo_get_scalar(jo_case *h, double *phi);
+/* Coupled path with a turbulence model (jg_params.turb_model SA: nscal 1, block
+ * 6; SST: nscal 2 (kine, omega), block 7): scalars phi[ncv][nscal] in/out,
+ * wall distance (calcWallDistance), the coupled preamble (state + material +
+ * BC + scalar BC + calcRansTurbViscMuet), calcRhsCoupled (rhs[ncv][B],
+ * A[nbocv_s][B][B] accumulated), block relaxation of a B x B system (sgs 0:
+ * Jacobi, 1: multicolour Gauss-Seidel) and the coupled step.  Named arrays:
+ * "phi","phi_bfa","grad_phi","diff" (scalar 0), "phi1",... (scalar 1),
+ * "wallDist","strMag","vortMag","diverg","crossDiff","blendFuncF1","blendFuncF2". */
+void jo_set_scalars(jo_case *h, const double *phi);
+void jo_get_scalars(jo_case *h, double *phi);
 void jo_wall_distance(jo_case *h);
 int jo_calc_state_coupled(jo_case *h);
 void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit);

@@ -47,8 +47,8 @@ def lib():
         L.jo_cfl.argtypes = [P]
         L.jo_cfl.restype = C.c_double
         L.jo_euler_flux_faces.argtypes = [C.c_int, C.c_int, D, D, D, D, D, D, D]
-        L.jo_set_scalar.argtypes = [P, D]
-        L.jo_get_scalar.argtypes = [P, D]
+        L.jo_set_scalars.argtypes = [P, D]
+        L.jo_get_scalars.argtypes = [P, D]
         L.jo_wall_distance.argtypes = [P]
         L.jo_calc_state_coupled.argtypes = [P]
         L.jo_calc_state_coupled.restype = C.c_int
@@ -134,30 +134,32 @@ class Oracle:
 
 
 class OracleSA(Oracle):
-    """The coupled Spalart-Allmaras path (6x6 blocks): state + nuSA."""
-
-    B = 6
+    """The coupled path with a turbulence model: SA (6x6 blocks, nuSA) or SST
+    (7x7, kine and omega).  ``set_scalar`` takes phi[ncv] (SA) or phi[ncv][2]."""
 
     def __init__(self, mesh_src, params, precision=0):
         super().__init__(mesh_src, params, precision)
+        self.ns = params.nscal
+        self.B = 5 + self.ns
         lib().jo_wall_distance(self.h)
 
     def set_scalar(self, phi):
-        phi = np.ascontiguousarray(phi, np.float64)
-        lib().jo_set_scalar(self.h, dptr(phi))
+        phi = np.ascontiguousarray(np.asarray(phi, np.float64).reshape(self.ncv, self.ns))
+        lib().jo_set_scalars(self.h, dptr(phi))
 
     def get_scalar(self):
-        phi = np.empty(self.ncv)
-        lib().jo_get_scalar(self.h, dptr(phi))
-        return phi
+        phi = np.empty((self.ncv, self.ns))
+        lib().jo_get_scalars(self.h, dptr(phi))
+        return phi[:, 0] if self.ns == 1 else phi
 
     def calc_state(self):
         if lib().jo_calc_state_coupled(self.h) != 0:
             raise ValueError("unsupported boundary condition")
 
     def sa_array(self, name):
-        n = {"phi_bfa": self.ma.nfa_b, "diff": self.ma.nfa}.get(name, self.ncv)
-        k = 3 if name == "grad_phi" else 1
+        n = {"phi_bfa": self.ma.nfa_b, "diff": self.ma.nfa, "phi1_bfa": self.ma.nfa_b, "diff1": self.ma.nfa}.get(
+            name, self.ncv)
+        k = 3 if name in ("grad_phi", "grad_phi1") else 1
         ptr = lib().jo_sa_array(self.h, name.encode())
         a = np.ctypeslib.as_array(ptr, shape=(n * k,)).copy()
         return a.reshape(n, k) if k > 1 else a

@@ -6,8 +6,8 @@
 // GPU path can be checked against them, and it times the reference's own
 // runBackwardEuler as the CPU baseline.
 //
-// usage: ref_harness <Joe.in> <run 0|1> <dump|coupled|run> <outdir>
-//   run 0 : JoeWithModels (laminar / inviscid); run 1 : JoeWithModels + RansTurbSA
+// usage: ref_harness <Joe.in> <run 0|1|2> <dump|coupled|run> <outdir>
+//   run 0 : JoeWithModels (laminar / inviscid); run 1 : + RansTurbSA; run 2 : + RansTurbKOmSST
 //   dump    : init -> state/material/BC -> calcDt -> calcRhs(implicit) -> one
 //             linear solve (solveCoupledLinSysNS); every array written to outdir
 //   coupled : init -> state/material/BC/turbulent viscosity -> calcDt ->
@@ -56,10 +56,14 @@ static double scal_perturb(double x, double y, double z, double a) {
   return 1.0 + a * sin(1.3 * x + 0.4) * cos(0.7 * y + 0.1) * (1.0 + 0.2 * cos(2.3 * z));
 }
 
-// the reference's case-local SA class (src/joe/joe.cpp:286-298 pattern)
+// the reference's case-local SA / SST classes (src/joe/joe.cpp:286-313 pattern)
 class JoeSA : public JoeWithModels, public RansTurbSA {
 public:
   JoeSA(char *name) : JoeWithModels(name), UgpWithCvCompFlow(name) {}
+};
+class JoeSST : public JoeWithModels, public RansTurbKOmSST {
+public:
+  JoeSST(char *name) : JoeWithModels(name), UgpWithCvCompFlow(name) {}
 };
 
 template <class Base>
@@ -250,13 +254,13 @@ public:
       sprintf(nm, "scal%d_bfa.f64", s);
       dumpRaw(nm, this->scalarTranspEqVector[s].phi_bfa, sizeof(double) * nfa_b);
     }
-    double *wd = NULL, *sm = NULL, *vm = NULL;
-    if (this->getScalarData("wallDist")) wd = *(this->getScalarData("wallDist")->ptr);
-    if (this->getScalarData("strMag")) sm = *(this->getScalarData("strMag")->ptr);
-    if (this->getScalarData("vortMag")) vm = *(this->getScalarData("vortMag")->ptr);
-    if (wd) DUMPD("wallDist", wd, ncv);
-    if (sm) DUMPD("strMag", sm, ncv);
-    if (vm) DUMPD("vortMag", vm, ncv);
+    const char *cvnames[] = {"wallDist", "strMag", "vortMag", "diverg", "crossDiff", "blendFuncF1", "blendFuncF2"};
+    for (const char *nm : cvnames)
+      if (this->getScalarData(nm)) {
+        char fn[64];
+        sprintf(fn, "%s.f64", nm);
+        dumpRaw(fn, *(this->getScalarData(nm)->ptr), sizeof(double) * ncv);
+      }
 
     double dt_min = this->calcDt(this->cfl);
     DUMPD("local_dt", this->local_dt, ncv);
@@ -328,6 +332,10 @@ int main(int argc, char *argv[]) {
       if (mode == "dump") j->dumpAll(); else if (mode == "coupled") j->dumpCoupled(); else j->runTimed();
     } else if (run == 1) {
       Harness<JoeSA> *j = new Harness<JoeSA>(argv[1]);
+      j->setup();
+      if (mode == "dump") j->dumpAll(); else if (mode == "coupled") j->dumpCoupled(); else j->runTimed();
+    } else if (run == 2) {
+      Harness<JoeSST> *j = new Harness<JoeSST>(argv[1]);
       j->setup();
       if (mode == "dump") j->dumpAll(); else if (mode == "coupled") j->dumpCoupled(); else j->runTimed();
     } else {

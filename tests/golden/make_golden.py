@@ -8,7 +8,7 @@ and boundary-face states, local time step, gradients, RHS, the implicit
 matrix A, one linear solve, and the state + L1 residuals after a few
 runBackwardEuler steps.
 
-    python tests/golden/make_golden.py [segregated] [sa]    # needs the reference + g++
+    python tests/golden/make_golden.py [segregated] [sa] [sst]    # needs the reference + g++
 """
 from __future__ import annotations
 
@@ -69,6 +69,18 @@ def sa_cases():
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
 
 
+def sst_cases():
+    """Coupled Menter SST cases (runBackwardEulerCoupled's calcRhsCoupled, 7x7 blocks)."""
+    raw, _, prm = case.sst_bump_case(16, 8, 2, stretch=1.2, jitter=0.1, seed=3)
+    rawc, _, prmc = case.sst_bump_case(16, 8, 2, stretch=1.15, jitter=0.1, seed=5, inlet="CBC", mach=0.5)
+    bc_n = dict(prmc.bcs)
+    bc_n["outlet"] = BC("NEUMANN")
+    yield "sst_bump_farfield", raw, prm
+    yield "sst_bump_cbc_symm_original", rawc, dataclasses.replace(prmc, SYMM_BC="ORIGINAL_NUMERIC")
+    yield "sst_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
+        prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
+
+
 def params_json(prm) -> str:
     d = dataclasses.asdict(prm)
     d["bcs"] = {k: [v.kind, list(v.values)] for k, v in prm.bcs.items()}
@@ -102,13 +114,17 @@ def main(which=("segregated", "sa")):
         out["nsteps"] = np.array(NSTEPS)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print("wrote", name, d["meta"]["ncv"], "cells")
-    for name, raw, prm in (sa_cases() if "sa" in which else ()):
+    turb = [(n, r, p, 1) for n, r, p in (sa_cases() if "sa" in which else ())]
+    turb += [(n, r, p, 2) for n, r, p in (sst_cases() if "sst" in which else ())]
+    for name, raw, prm, run_kind in turb:
         extra = "HARNESS_PERTURB = %g" % PERTURB
-        d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "coupled", run_kind=1)
+        d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "coupled",
+                       run_kind=run_kind)
         keep = ["cvofa", "faocv_i", "faocv_v", "nbocv_i", "nbocv_v", "x_cv", "x_fa", "fa_normal", "cv_volume",
                 "nbocv_lsg_coeff", "boundary_fa_lsg_coeff", "init_rho", "init_rhou", "init_rhoE", "init_scal0",
-                "mul_fa", "lamOcp_fa", "mut_fa", "scal0_bfa", "wallDist", "strMag", "vortMag", "local_dt",
-                "grad_u", "scal0_grad", "scal0_diff", "rhs_coupled", "A_coupled"]
+                "init_scal1", "mul_fa", "lamOcp_fa", "mut_fa", "scal0_bfa", "scal1_bfa", "wallDist", "strMag",
+                "vortMag", "diverg", "crossDiff", "blendFuncF1", "blendFuncF2", "local_dt", "grad_u",
+                "scal0_grad", "scal0_diff", "scal1_grad", "scal1_diff", "rhs_coupled", "A_coupled"]
         out = {k: d[k] for k in keep if k in d}
         out["meta"] = np.array(json.dumps(d["meta"]))
         out["params"] = np.array(params_json(prm))
@@ -126,4 +142,4 @@ def load(path):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("segregated", "sa"))
+    main(tuple(sys.argv[1:]) or ("segregated", "sa", "sst"))

@@ -148,8 +148,8 @@ int jg_calc_dt(jg_case_t *h, double cfl, double *dt_min, double *local_dt);
  * block Jacobian A[nbocv_s][5][5] in the reference's CSR layout. */
 int jg_calc_rhs(jg_case_t *h, double *rhs_rho, double *rhs_rhou, double *rhs_rhoE, double *A, int flagImplicit);
 
-/* Coupled path (jg_params.turb_model = JG_TURB_SA, nscal = 1, HLLC, JACOBI or
- * SGS relaxation).  The handle computes the wall distance at creation
+/* Coupled path (jg_params.turb_model = JG_TURB_SA with nscal = 1, or
+ * JG_TURB_SST with nscal = 2 (kine, omega); HLLC, JACOBI or SGS relaxation).  The handle computes the wall distance at creation
  * (calcWallDistance, UgpWithCvCompFlow.h:1395-1535).  Transported scalars
  * phi[ncv][nscal] (nuSA; ScalarTranspEq phi) in/out: set them after
  * jg_set_state, before the first step.  jg_calc_rhs_coupled is
@@ -165,6 +165,11 @@ int jg_get_scalars(jg_case_t *h, double *phi);
 int jg_calc_rhs_coupled(jg_case_t *h, double *rhs, double *A, int flagImplicit);
 int jg_get_turb(jg_case_t *h, double *wallDist, double *mut_fa, double *strMag, double *vortMag, double *phi_bfa,
                 double *grad_phi, double *diff);
+/* one model array by the reference's name: "wallDist", "strMag", "vortMag",
+ * "diverg", "crossDiff", "blendFuncF1", "blendFuncF2" ([ncv], the last four
+ * SST only), "mut_fa" [nfa], and per scalar s, component-major: "phi_bfa"
+ * [nscal][nfa_b], "grad_phi" [nscal][ncv][3], "diff" [nscal][nfa] */
+int jg_get_turb_array(jg_case_t *h, const char *name, double *out);
 /* gradients of the last jg_calc_rhs / step: calcCvVectorGrad / calcCvScalarGrad
  * with limiting (src/common/UgpWithCv.h:803-1083); grad_u[ncv][3][3], others [ncv][3].
  * grad_u is what the reference holds after calcRhs: the viscous gradient when

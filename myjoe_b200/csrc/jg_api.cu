@@ -173,9 +173,10 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "unsupported precision %d", q->precision);
   if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS))
     return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI or SGS sweeps");
-  if (q->turb_model == JG_TURB_SA) {
-    if (q->nscal != 1) return set_err(JG_ERR_ARG, "the SA model transports one scalar (nscal = 1)");
-    if (!(q->mu_ref > 0.0)) return set_err(JG_ERR_ARG, "the SA model needs a viscous case (mu_ref > 0)");
+  if (q->turb_model == JG_TURB_SA || q->turb_model == JG_TURB_SST) {
+    if (q->nscal != (q->turb_model == JG_TURB_SA ? 1 : 2))
+      return set_err(JG_ERR_ARG, "SA transports one scalar (nscal = 1), SST two (nscal = 2)");
+    if (!(q->mu_ref > 0.0)) return set_err(JG_ERR_ARG, "a turbulence model needs a viscous case (mu_ref > 0)");
     if (q->flux != JG_FLUX_HLLC) return set_err(JG_ERR_ARG, "the coupled path uses the HLLC flux");
     if (q->lin_solver != JG_LS_JACOBI && q->lin_solver != JG_LS_SGS)
       return set_err(JG_ERR_ARG, "the coupled path relaxes with JACOBI or SGS sweeps");
@@ -235,7 +236,7 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   h->hp = *q;
   h->p = make_params(*q);
   h->eltsz = h->p.fp32 ? 4 : 8;
-  h->bs = (q->turb_model == JG_TURB_SA) ? 6 : 5;
+  h->bs = (q->turb_model == JG_TURB_NONE) ? 5 : 5 + q->nscal;
   const int bs = h->bs;
   h->nbocv_i.assign(mesh->nbocv_i, mesh->nbocv_i + N + 1);
   h->nbocv_v.assign(mesh->nbocv_v, mesh->nbocv_v + mesh->nbocv_s);
@@ -417,22 +418,32 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     RC(upload(h, &da, on.data(), on.size()));
     st.case_active = (uint8_t*)da;
   }
-  if (bs == 6) {
-    // SA arrays, the WALL faces in zone order and the wall distance (initialHookScalarRansTurbModel)
+  if (bs > 5) {
+    // model arrays, the WALL faces in zone order and the wall distance (initialHookScalarRansTurbModel)
     Turb& t = h->turb;
-    RC(dmalloc(h, &t.phi, (size_t)N));
-    RC(dmalloc(h, &t.phi_bfa, (size_t)nfa_b));
-    RC(dmalloc(h, &t.grad_phi, 3 * (size_t)N));
-    RC(dmalloc(h, &t.diff, (size_t)nfa));
+    t.model = q->turb_model;
+    t.ns = q->nscal;
+    const size_t ns = t.ns;
+    RC(dmalloc(h, &t.phi, ns * N));
+    RC(dmalloc(h, &t.phi_bfa, ns * nfa_b));
+    RC(dmalloc(h, &t.grad_phi, 3 * ns * N));
+    RC(dmalloc(h, &t.diff, ns * nfa));
     RC(dmalloc(h, &t.wd, (size_t)N));
     RC(dmalloc(h, &t.strMag, (size_t)N));
     RC(dmalloc(h, &t.vortMag, (size_t)N));
+    if (t.model == JG_TURB_SST) {
+      RC(dmalloc(h, &t.diverg, (size_t)N));
+      RC(dmalloc(h, &t.crossDiff, (size_t)N));
+      RC(dmalloc(h, &t.F1, (size_t)N));
+      RC(dmalloc(h, &t.F2, (size_t)N));
+      st.kine = t.phi;  // scalar 0: the pressure recovery subtracts rho k
+    }
     RC(dmalloc(h, &st.mut_fa, (size_t)nfa));
     std::vector<int> wall;
     for (int z = 0; z < mesh->nzones; z++)
       if (mesh->zones[z].kind == JG_BC_WALL)
         for (int f = mesh->zones[z].ifa_f; f <= mesh->zones[z].ifa_l; f++) wall.push_back(f);
-    if (wall.empty()) return set_err(JG_ERR_ARG, "the SA model needs a WALL zone (wall distance)");
+    if (wall.empty()) return set_err(JG_ERR_ARG, "a turbulence model needs a WALL zone (wall distance)");
     const int* dw = nullptr;
     RC(upload(h, &dw, wall.data(), wall.size()));
     t.wall_f = dw;
@@ -473,7 +484,7 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
 static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
   const size_t N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b, nbs = mesh->nbocv_s;
   const size_t e = q->precision == JG_PREC_MIXED ? 4 : 8;
-  const size_t bs = q->turb_model == JG_TURB_SA ? 6 : 5, b2 = bs * bs;
+  const size_t bs = q->turb_model == JG_TURB_NONE ? 5 : 5 + q->nscal, b2 = bs * bs;
   const int* fi = mesh->faocv_i;
   const int* fv = mesh->faocv_v;
   size_t nbslot = 0, rows = 0;
@@ -507,13 +518,17 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
   size_t b = 0;
   for (size_t x : a)
     if (x) b += alloc_round(x);
-  if (bs == 6) {
-    // SA arrays: phi, phi_bfa, grad_phi, diff, wall distance, strain, vorticity, mut_fa, wall faces
+  if (bs > 5) {
+    // model arrays: phi, phi_bfa, grad_phi, diff (per scalar), wall distance, strain, vorticity
+    // (+ divergence, cross-diffusion, F1, F2 for SST), mut_fa, the wall faces
+    const size_t ns = bs - 5;
     size_t nwall = 0;
     for (int z = 0; z < mesh->nzones; z++)
       if (mesh->zones[z].kind == JG_BC_WALL) nwall += mesh->zones[z].ifa_l - mesh->zones[z].ifa_f + 1;
-    const size_t t[] = {N * d, nfa_b * d, 3 * N * d, nfa * d, N * d, N * d, N * d, nfa * d, nwall * i};
+    const size_t t[] = {ns * N * d, ns * nfa_b * d, 3 * ns * N * d, ns * nfa * d, N * d, N * d, N * d,
+                        nfa * d, nwall * i};
     for (size_t x : t) b += alloc_round(x);
+    if (q->turb_model == JG_TURB_SST) b += 4 * alloc_round(N * d);
   }
   return b;
 }
@@ -708,8 +723,8 @@ static int prime(jg_case* h) {
   launch_state(h->m, h->p, h->st, h->stream);
   launch_face_props(h->m, h->p, h->st, h->stream);
   launch_bc(h->m, h->p, h->st, h->stream);
-  if (h->bs == 6) {
-    launch_scalar_bc(h->m, h->st, h->turb, h->stream);
+  if (h->bs > 5) {
+    launch_scalar_bc(h->m, h->p, h->st, h->turb, h->stream);
     launch_turb_props(h->m, h->p, h->st, h->turb, h->stream);
   }
   CKL();
@@ -1036,20 +1051,20 @@ static int enqueue_step_coupled(jg_case* h) {
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
   int sgs = h->hp.lin_solver == JG_LS_SGS;
   int sweeps = std::max(1, h->hp.ls_max_iter);
-  launch_relax6(h->m, h->p, h->st, sgs, sweeps, S);
+  launch_relax6(h->m, h->p, h->st, sgs, sweeps, h->bs, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
   launch_update6(h->m, h->p, h->st, h->turb, (sgs || sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
   launch_state(h->m, h->p, h->st, S);
   launch_face_props(h->m, h->p, h->st, S);
   launch_bc(h->m, h->p, h->st, S);
-  launch_scalar_bc(h->m, h->st, h->turb, S);
+  launch_scalar_bc(h->m, h->p, h->st, h->turb, S);
   launch_turb_props(h->m, h->p, h->st, h->turb, S);
   CKL();
   return JG_OK;
 }
 
 static int enqueue_step(jg_case* h, int for_graph) {
-  if (h->bs == 6) return enqueue_step_coupled(h);
+  if (h->bs > 5) return enqueue_step_coupled(h);
   cudaStream_t S = h->stream;
   launch_ctrl_step(h->p, h->st, S);
   launch_dt(h->m, h->p, h->st, 1, 0.0, S);
@@ -1259,18 +1274,47 @@ int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const
 extern "C" int jg_set_scalars(jg_case_t* h, const double* phi) {
   if (!h || !phi) return set_err(JG_ERR_ARG, "null argument");
   if (h->bs == 5) return set_err(JG_ERR_ARG, "the case transports no scalar");
-  CK(cudaMemcpyAsync(h->turb.phi, phi, (size_t)h->ncv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const size_t N = h->ncv, ns = h->turb.ns;
+  std::vector<double> cm(ns * N);  // [ncv][ns] -> [ns][ncv]
+  for (size_t c = 0; c < N; c++)
+    for (size_t q = 0; q < ns; q++) cm[q * N + c] = phi[ns * c + q];
+  CK(cudaMemcpyAsync(h->turb.phi, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  h->primed = 0;  // the scalar boundary values and the turbulent viscosity follow at the next call
+  h->primed = 0;  // the state, scalar boundary values and turbulent viscosity follow at the next call
   return JG_OK;
 }
 
 extern "C" int jg_get_scalars(jg_case_t* h, double* phi) {
   if (!h || !phi) return set_err(JG_ERR_ARG, "null argument");
   if (h->bs == 5) return set_err(JG_ERR_ARG, "the case transports no scalar");
-  CK(cudaMemcpyAsync(phi, h->turb.phi, (size_t)h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  const size_t N = h->ncv, ns = h->turb.ns;
+  std::vector<double> cm(ns * N);
+  CK(cudaMemcpyAsync(cm.data(), h->turb.phi, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  for (size_t c = 0; c < N; c++)
+    for (size_t q = 0; q < ns; q++) phi[ns * c + q] = cm[q * N + c];
   return JG_OK;
+}
+
+extern "C" int jg_get_turb_array(jg_case_t* h, const char* name, double* out) {
+  if (!h || !name || !out) return set_err(JG_ERR_ARG, "null argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the case has no turbulence model");
+  if (!h->primed) RC(prime(h));
+  const size_t N = h->ncv, ns = h->turb.ns;
+  const Turb& t = h->turb;
+  struct { const char* n; const double* p; size_t len; } tab[] = {
+      {"wallDist", t.wd, N}, {"strMag", t.strMag, N}, {"vortMag", t.vortMag, N}, {"diverg", t.diverg, N},
+      {"crossDiff", t.crossDiff, N}, {"blendFuncF1", t.F1, N}, {"blendFuncF2", t.F2, N},
+      {"mut_fa", h->st.mut_fa, (size_t)h->nfa}, {"phi_bfa", t.phi_bfa, ns * h->nfa_b},
+      {"grad_phi", t.grad_phi, 3 * ns * N}, {"diff", t.diff, ns * h->nfa}};
+  for (auto& e : tab)
+    if (strcmp(e.n, name) == 0) {
+      if (!e.p) return set_err(JG_ERR_ARG, "%s is not an array of this model", name);
+      CK(cudaMemcpyAsync(out, e.p, e.len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      return JG_OK;
+    }
+  return set_err(JG_ERR_ARG, "unknown turbulence array %s", name);
 }
 
 extern "C" int jg_calc_rhs_coupled(jg_case_t* h, double* rhs, double* A, int flagImplicit) {

@@ -85,19 +85,29 @@ struct State {
   int* err;         // error flags
   int* case_err;    // [ncases] per-case error flags (1: rho/p <= 0, 4: NaN residual)
   uint8_t* case_active;  // [ncases] 0: case frozen (retired), its state is not updated
-  double* mut_fa;   // [nfa] turbulent viscosity (coupled SA path), nullptr without a model
+  double* mut_fa;   // [nfa] turbulent viscosity (coupled path), nullptr without a model
+  const double* kine;  // [N] turbulent kinetic energy in the pressure recovery (SST), nullptr otherwise
   int bs;           // block size of the system: 5, or 6 with SA (rhs, b, dq, x, D, O, resid use it)
 };
 
-// Spalart-Allmaras scalar and model arrays (coupled path only)
+// Transported scalars and turbulence-model arrays (coupled path only).
+// Scalars are stored component-major: phi[s*N + c], phi_bfa[s*nfa_b + f],
+// grad_phi[(s*N + c)*3 + j], diff[s*nfa + f].  SA: s = 0 nuSA; SST: s = 0
+// kine, s = 1 omega.
 struct Turb {
-  double* phi;       // [N] nuSA
-  double* phi_bfa;   // [nfa_b]
-  double* grad_phi;  // [N][3] (limited like the flow gradients)
-  double* diff;      // [nfa] scalar diffusivity (mu + rho nuSA) / sigma
+  int model;         // JG_TURB_SA / JG_TURB_SST
+  int ns;            // scalars
+  double* phi;
+  double* phi_bfa;
+  double* grad_phi;  // limited like the flow gradients
+  double* diff;      // scalar diffusivities at faces
   double* wd;        // [N] wall distance
   double* strMag;    // [N]
   double* vortMag;   // [N]
+  double* diverg;    // [N] (SST)
+  double* crossDiff; // [N] (SST)
+  double* F1;        // [N] Menter blending functions (SST)
+  double* F2;
   const int* wall_f; // [nwall] WALL faces in zone order
   int nwall;
 };
@@ -161,15 +171,15 @@ int record_error(int code, const char* msg);  // sets the jg_last_error message
 }  // namespace jg
 
 namespace jg {
-// coupled Spalart-Allmaras path (jg_coupled.cu), block size 6
+// coupled turbulence-model path (jg_coupled.cu), block size 5 + ns
 void launch_wall_distance(const Mesh& m, Turb& t, cudaStream_t s);
-void launch_scalar_bc(const Mesh& m, State& st, Turb& t, cudaStream_t s);
+void launch_scalar_bc(const Mesh& m, const Params& p, State& st, Turb& t, cudaStream_t s);
 // gradients of the flow (limited, as calcFluxCoupled takes them) and of nuSA,
 // strain/vorticity magnitudes, turbulent viscosity and scalar diffusivity
 void launch_turb_props(const Mesh& m, const Params& p, State& st, Turb& t, cudaStream_t s);
 // calcRhsCoupled + the implicit-step epilogue: rhs[N][6], D/O (6x6), b, Dinv
 void launch_flux6(const Mesh& m, const Params& p, State& st, Turb& t, int implicit, int for_step, cudaStream_t s);
-void launch_relax6(const Mesh& m, const Params& p, State& st, int sgs, int sweeps, cudaStream_t s);
+void launch_relax6(const Mesh& m, const Params& p, State& st, int sgs, int sweeps, int bs, cudaStream_t s);
 // Q += dq (x: the relaxation result, [6][N]), nuSA = clip((nuSA (rho_new - dq0) + dq5) / rho_new)
 void launch_update6(const Mesh& m, const Params& p, State& st, Turb& t, const void* x, cudaStream_t s);
 // the flow gradients as calcFluxCoupled takes them (jg_kernels.cu)

@@ -25,11 +25,12 @@ __device__ __forceinline__ double mu_law(const Params& p, double T) {
 }
 
 // calcStateVariables, UgpWithCvCompFlow.h:1662-1694: a non-positive pressure keeps the old one
-__device__ __forceinline__ void state_from_q(const Params& p, const double* q, double* prim, int* err) {
+__device__ __forceinline__ void state_from_q(const Params& p, const double* q, double* prim, int* err,
+                                             double kinecv = 0.0) {
   double r = q[0];
   double ru[3] = {q[1], q[2], q[3]};
   double u[3] = {ru[0] / r, ru[1] / r, ru[2] / r};
-  double pr = (p.gamma - 1.0) * (q[4] - 0.5 * dot3(ru, ru) / r);
+  double pr = (p.gamma - 1.0) * (q[4] - 0.5 * dot3(ru, ru) / r - r * kinecv);
   double pp = prim[3];
   if (pr > 0.0) pp = pr;
   if (!(r > 0.0) || !(pp > 0.0)) atomicOr(err, 1);
@@ -49,7 +50,7 @@ __global__ void k_state(Mesh m, Params p, State st) {
   double q[5], prim[8];
   for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i];
   for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
-  state_from_q(p, q, prim, st.err);
+  state_from_q(p, q, prim, st.err, st.kine ? st.kine[c] : 0.0);
   for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
 }
 
@@ -861,7 +862,10 @@ __global__ void k_resid_cases(State st, const int* __restrict__ rblk_off, int nc
 }
 void launch_resid_cases(State& st, const int* case_off, const int* rblk_off, const int* rblk_case, int nrblk,
                         int ncases, int hist_from_ctrl, cudaStream_t s) {
-  if (st.bs == 6) {
+  if (st.bs == 7) {
+    k_resid_chunks<7><<<nrblk, 64 * 7, 0, s>>>(st, case_off, rblk_off, rblk_case);
+    k_resid_cases<7><<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
+  } else if (st.bs == 6) {
     k_resid_chunks<6><<<nrblk, 64 * 6, 0, s>>>(st, case_off, rblk_off, rblk_case);
     k_resid_cases<6><<<ncases, 32, 0, s>>>(st, rblk_off, ncases, hist_from_ctrl);
   } else {

@@ -73,6 +73,7 @@ def lib():
         L.jg_get_scalars.argtypes = [P, D]
         L.jg_calc_rhs_coupled.argtypes = [P, D, D, I]
         L.jg_get_turb.argtypes = [P, D, D, D, D, D, D, D]
+        L.jg_get_turb_array.argtypes = [P, C.c_char_p, D]
         L.jg_case_footprint.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), D]
         L.jg_case_device_bytes.argtypes = [P, D]
         L.jg_serve_create.argtypes = [C.POINTER(jg_serve_config), C.POINTER(P)]
@@ -192,13 +193,24 @@ class JoeGpu:
         return 5 + self.params.nscal
 
     def set_scalars(self, phi):
-        phi = np.ascontiguousarray(phi, np.float64)
+        """phi[ncv] (SA: nuSA) or phi[ncv][2] (SST: kine, omega)."""
+        phi = np.ascontiguousarray(np.asarray(phi, np.float64).reshape(self.ncv, self.params.nscal))
         _ck(lib().jg_set_scalars(self.h, dptr(phi)))
 
     def get_scalars(self):
-        phi = np.empty(self.ncv)
+        ns = self.params.nscal
+        phi = np.empty((self.ncv, ns))
         _ck(lib().jg_get_scalars(self.h, dptr(phi)))
-        return phi
+        return phi[:, 0] if ns == 1 else phi
+
+    def turb_array(self, name):
+        """one model array by its reference name (jg_get_turb_array); per-scalar arrays come
+        back as [nscal][...]."""
+        n, nf, nb, ns = self.ncv, self.ma.nfa, self.ma.nfa_b, self.params.nscal
+        shape = {"mut_fa": (nf,), "phi_bfa": (ns, nb), "grad_phi": (ns, n, 3), "diff": (ns, nf)}.get(name, (n,))
+        out = np.empty(shape)
+        _ck(lib().jg_get_turb_array(self.h, name.encode(), dptr(out)))
+        return out
 
     def calcRhsCoupled(self, flagImplicit=True):
         """rhs[ncv][6], A[nbocv_s][6][6] (None without flagImplicit)."""

@@ -99,7 +99,17 @@ typedef struct jg_params {
   int nscal;           /* transported scalars: 0 (laminar / inviscid), 1 (SA), 2 (SST) */
   int turb_model;      /* JG_TURB_*: with a model the case runs runBackwardEulerCoupled's
                           (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
+  int renumber;        /* JG_RENUMBER_*: the handle's own cell/face order (jg_create only) */
 } jg_params;
+/* Cell and face order inside a handle.  JG_RENUMBER_NONE keeps the caller's
+ * order (a mesh the reference loaded is already in reverse Cuthill-McKee
+ * order, Ugp::init, src/common/Ugp.cpp:3389-3399).  JG_RENUMBER_RCM renumbers
+ * cells by reverse Cuthill-McKee and sorts faces by their cells inside the
+ * handle; every entry point still takes and returns arrays in the caller's
+ * order (cells, faces and nbocv entries), so only the speed changes.  Block
+ * Jacobi steps and calcRhs give bit-identical results either way; the L1
+ * residual sum and the Gauss-Seidel colouring follow the internal order. */
+enum { JG_RENUMBER_NONE = 0, JG_RENUMBER_RCM = 1 };
 /* turbulence models, with the reference's default constants:
  *   JG_TURB_SA  Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h): nscal 1, nuSA (1e-10 .. 1)
  *   JG_TURB_SST Menter k-omega SST (TurbModel_KOMSST.h): nscal 2, kine (1e-10 .. 1e10) and
@@ -220,6 +230,12 @@ int jg_batch_set_active(jg_case_t *h, int case_id, int active);
  * creating it) and the bytes a live handle holds. */
 int jg_case_footprint(const jg_mesh *mesh, const jg_params *params, double *bytes);
 int jg_case_device_bytes(jg_case_t *h, double *bytes);
+
+/* The cell order jg_create uses with params.renumber = method:
+ * cell_old[ncv] = the caller's id of each cell in the handle's order.  Host
+ * only (no device needed).  For JG_RENUMBER_RCM: reverse Cuthill-McKee over
+ * the nbocv graph, each connected component from a pseudo-peripheral cell. */
+int jg_renumber_cells(const jg_mesh *mesh, int method, int *cell_old);
 
 /* Serving form (no reference counterpart; the reference solves one case per
  * run): a request loop on one GPU.  Submitted cases wait in a FIFO queue and

@@ -42,7 +42,7 @@ class jg_params(C.Structure):
                 ("under_relax", C.c_double),
                 ("lin_solver", C.c_int), ("ls_max_iter", C.c_int),
                 ("ls_abs", C.c_double), ("ls_rel", C.c_double),
-                ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int)]
+                ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int)]
 
 
 class jg_serve_config(C.Structure):
@@ -69,7 +69,7 @@ def iptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int))
 
 
-def make_params(p: JoeParams, precision: int = 0) -> jg_params:
+def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_params:
     q = jg_params()
     q.gamma = p.GAMMA
     q.R_gas = p.R_gas
@@ -100,6 +100,7 @@ def make_params(p: JoeParams, precision: int = 0) -> jg_params:
     q.precision = precision
     q.nscal = p.nscal
     q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
+    q.renumber = 1 if renumber else 0
     return q
 
 

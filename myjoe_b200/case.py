@@ -249,13 +249,15 @@ def plate_case(nx=256, ny=96, nz=2, mach=0.3, re_l=1.0e5, p=1.0e5, T=300.0, flux
 
 
 def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
-                 stretch=1.0, inlet="FARFIELD", nu_factor=3.0):
+                 stretch=1.0, inlet="FARFIELD", nu_factor=3.0, n_prism=0, shuffle=False, alternate=False):
     """Turbulent (SA) flow over the channel bump: viscous WALL lower (nuSA = 0),
     HLLC, Sutherland viscosity with MU_REF set so that the Reynolds number on
     the bump chord (length 1) is ``re``; inflow nuSA = ``nu_factor`` x the
     kinematic viscosity (the usual SA free-stream value), far-field inlet,
     outlet and top (or CBC inlet with ``inlet="CBC"``), SYMMETRY z planes.
-    ``stretch`` > 1 clusters the rows towards the lower wall."""
+    ``stretch`` > 1 clusters the rows towards the lower wall.  ``n_prism`` > 0
+    meshes that many wall rows with triangular prisms (``channel_bump_mixed``);
+    ``shuffle`` permutes cells and faces from ``seed``."""
     gam, R = 1.4, 287.0
     rho = p / (R * T)
     c = math.sqrt(gam * R * T)
@@ -265,7 +267,11 @@ def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_
     mu_ref = mu / ((T / tref) ** 1.5 * (tref + sref) / (T + sref))
     nu_inf = nu_factor * mu / rho
     u = (U, 0.0, 0.0)
-    raw = meshgen.channel_bump(nx, ny, nz, bump_h=bump_h, jitter=jitter, seed=seed, stretch=stretch)
+    if n_prism > 0:
+        raw = meshgen.channel_bump_mixed(nx, ny, nz, n_prism=n_prism, bump_h=bump_h, jitter=jitter, seed=seed,
+                                         stretch=stretch, alternate=alternate)
+    else:
+        raw = meshgen.channel_bump(nx, ny, nz, bump_h=bump_h, jitter=jitter, seed=seed, stretch=stretch)
     bcs = {"lower": BC("WALL"), "sides": BC("SYMMETRY")}
     if inlet == "CBC":
         bcs.update(inlet=BC("CBC", u + (T, p)), outlet=BC("CBC_SUBSONIC_OUTLET", (p,)), upper=BC("SYMMETRY"))
@@ -277,17 +283,18 @@ def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_
     prm = JoeParams(T_REF=T, P_REF=p, RHO_REF=rho, GAMMA=gam, SPACE_INTEGRATION="HLLC", MU_MODE="SUTHERLAND",
                     MU_REF=mu_ref, SYMM_BC="ANALYTICAL", U_INITIAL=u, P_INITIAL=p, RHO_INITIAL=rho, bcs=bcs,
                     TURB_MODEL="SA", NUSA_INITIAL=nu_inf, scalar_bcs=sbc)
-    return raw, geometry.build_cv_mesh(raw, seed=seed), prm
+    return raw, geometry.build_cv_mesh(raw, seed=seed, shuffle=shuffle), prm
 
 
 def sst_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
-                  stretch=1.0, inlet="FARFIELD", tu=0.005, visc_ratio=0.1):
+                  stretch=1.0, inlet="FARFIELD", tu=0.005, visc_ratio=0.1, n_prism=0, shuffle=False,
+                  alternate=False):
     """Turbulent (Menter SST) flow over the channel bump, set up like
     ``sa_bump_case``: free-stream k = 1.5 (tu U)^2 and omega from the
     free-stream eddy-viscosity ratio mu_t/mu = ``visc_ratio``; at the wall
     k = 0 and omega from the model's wall hook (60 nu / (beta_1 d^2))."""
     raw, g, prm = sa_bump_case(nx, ny, nz, mach=mach, re=re, p=p, T=T, bump_h=bump_h, jitter=jitter, seed=seed,
-                               stretch=stretch, inlet=inlet)
+                               stretch=stretch, inlet=inlet, n_prism=n_prism, shuffle=shuffle, alternate=alternate)
     U = prm.U_INITIAL[0]
     rho = prm.RHO_INITIAL
     tref, sref = 273.15, 110.4

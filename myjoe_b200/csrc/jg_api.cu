@@ -81,7 +81,32 @@ struct jg_case {
   size_t bytes = 0;         // device bytes held by this handle
   int bs = 5;               // block size: 5, or 6 on the coupled SA path
   Turb turb{};              // SA arrays (coupled path)
+  Renumbering rn;           // caller's id of each internal cell / face / nbocv entry (empty: same order)
+  int* d_cell_old = nullptr;  // rn.cell_old on the device (state staging)
 };
+
+// Rows between the handle's order and the caller's: an array of nblk blocks
+// of n rows of w doubles; perm[r] is the caller's row of internal row r
+// (empty: the same order).
+static void rows_to_caller(const std::vector<int>& perm, const double* in, double* out, size_t n, size_t w,
+                           size_t nblk = 1) {
+  if (perm.empty()) {
+    memcpy(out, in, n * w * nblk * sizeof(double));
+    return;
+  }
+  for (size_t b = 0; b < nblk; b++)
+    for (size_t r = 0; r < n; r++) memcpy(out + (b * n + perm[r]) * w, in + (b * n + r) * w, w * sizeof(double));
+}
+
+static void rows_from_caller(const std::vector<int>& perm, const double* in, double* out, size_t n, size_t w,
+                             size_t nblk = 1) {
+  if (perm.empty()) {
+    memcpy(out, in, n * w * nblk * sizeof(double));
+    return;
+  }
+  for (size_t b = 0; b < nblk; b++)
+    for (size_t r = 0; r < n; r++) memcpy(out + (b * n + r) * w, in + (b * n + perm[r]) * w, w * sizeof(double));
+}
 
 
 // every device allocation of a handle goes through here; sizes are rounded to
@@ -131,6 +156,32 @@ static int upload(jg_case* h, const T** dst, const T* src, size_t count) {
   return JG_OK;
 }
 
+// a device array of the handle -> the caller's host array, rows in the caller's order
+static int download_rows(jg_case* h, const double* dev, double* host, const std::vector<int>& perm, size_t n,
+                         size_t w, size_t nblk = 1) {
+  const size_t len = n * w * nblk;
+  if (perm.empty()) {
+    if (len) CK(cudaMemcpyAsync(host, dev, len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return JG_OK;
+  }
+  std::vector<double> tmp(len);
+  if (len) CK(cudaMemcpyAsync(tmp.data(), dev, len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  rows_to_caller(perm, tmp.data(), host, n, w, nblk);
+  return JG_OK;
+}
+
+// the caller's host rows -> a device array of the handle (synchronous: the caller's array may go away)
+static int upload_rows(jg_case* h, double* dev, const double* host, const std::vector<int>& perm, size_t n,
+                       size_t w, size_t nblk = 1) {
+  const size_t len = n * w * nblk;
+  std::vector<double> tmp(len);
+  rows_from_caller(perm, host, tmp.data(), n, w, nblk);
+  if (len) CK(cudaMemcpyAsync(dev, tmp.data(), len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
 
 static Params make_params(const jg_params& q) {
   Params p;
@@ -186,6 +237,8 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "transported scalars need a turbulence model");
   }
   if (q->time_step_mode < 0 || q->time_step_mode > 2) return set_err(JG_ERR_ARG, "bad time step mode");
+  if (q->renumber != JG_RENUMBER_NONE && q->renumber != JG_RENUMBER_RCM)
+    return set_err(JG_ERR_ARG, "unsupported renumbering %d", q->renumber);
   if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");
   return JG_OK;
 }
@@ -439,10 +492,16 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
       st.kine = t.phi;  // scalar 0: the pressure recovery subtracts rho k
     }
     RC(dmalloc(h, &st.mut_fa, (size_t)nfa));
+    // WALL faces zone by zone in the caller's face order (the nearest-face search keeps the first of equals)
     std::vector<int> wall;
     for (int z = 0; z < mesh->nzones; z++)
-      if (mesh->zones[z].kind == JG_BC_WALL)
+      if (mesh->zones[z].kind == JG_BC_WALL) {
+        size_t w0 = wall.size();
         for (int f = mesh->zones[z].ifa_f; f <= mesh->zones[z].ifa_l; f++) wall.push_back(f);
+        if (!h->rn.face_old.empty())
+          std::sort(wall.begin() + w0, wall.end(),
+                    [&](int a, int b) { return h->rn.face_old[a] < h->rn.face_old[b]; });
+      }
     if (wall.empty()) return set_err(JG_ERR_ARG, "a turbulence model needs a WALL zone (wall distance)");
     const int* dw = nullptr;
     RC(upload(h, &dw, wall.data(), wall.size()));
@@ -467,7 +526,23 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
   jg_case* h = new jg_case();
-  int rc = build(h, mesh, params);
+  int rc = JG_OK;
+  if (params->renumber == JG_RENUMBER_RCM) {
+    MeshOwned mo;
+    rc = renumber_mesh(*mesh, params->renumber, mo, h->rn);
+    if (rc == JG_OK) rc = build(h, &mo.m, params);
+    if (rc == JG_OK) {
+      const int* d = nullptr;
+      rc = upload(h, &d, h->rn.cell_old.data(), h->rn.cell_old.size());
+      h->d_cell_old = (int*)d;
+    }
+    if (rc == JG_OK) {
+      cudaError_t e = cudaStreamSynchronize(h->stream);  // the renumbered host arrays go out of scope
+      if (e != cudaSuccess) rc = set_err(JG_ERR_CUDA, "%s", cudaGetErrorString(e));
+    }
+  } else {
+    rc = build(h, mesh, params);
+  }
   if (rc != JG_OK) {
     std::string keep = g_err;
     jg_destroy(h);
@@ -538,6 +613,14 @@ extern "C" int jg_case_footprint(const jg_mesh* mesh, const jg_params* params, d
   RC(check_params(params));
   if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
     return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
+  if (params->renumber == JG_RENUMBER_RCM) {
+    // the sliced-ELL padding follows the renumbered order; plus the device copy of the cell order
+    MeshOwned mo;
+    Renumbering rn;
+    RC(renumber_mesh(*mesh, params->renumber, mo, rn));
+    *bytes = (double)(footprint(&mo.m, params) + alloc_round((size_t)mesh->ncv * sizeof(int)));
+    return JG_OK;
+  }
   *bytes = (double)footprint(mesh, params);
   return JG_OK;
 }
@@ -553,18 +636,11 @@ static int prime(jg_case* h);
 // ---------------------------------------------------------------------------
 // batches: many independent cases concatenated into one block-diagonal system
 // ---------------------------------------------------------------------------
-struct MeshCat {
-  std::vector<int> cvofa, faocv_i, faocv_v, nbocv_i, nbocv_v;
-  std::vector<double> x_cv, x_fa, fa_normal, vol, lsq, blsq;
-  std::vector<jg_zone> zones;
-  jg_mesh m;
-};
-
 // Boundary faces of every case first (case by case), then the internal faces
 // (case by case); cells case by case.  Per case, the relative order of cells,
 // faces and CSR entries is the case's own, so every per-cell computation sees
 // exactly what it sees when the case runs alone.
-static int concat_meshes(int ncases, const jg_mesh* ms, MeshCat& o, std::vector<int>& case_off,
+static int concat_meshes(int ncases, const jg_mesh* ms, MeshOwned& o, std::vector<int>& case_off,
                          std::vector<int>& bfa_off) {
   long N = 0, NF = 0, NB = 0, NBS = 0, NZ = 0;
   for (int k = 0; k < ncases; k++) {
@@ -638,13 +714,14 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   *out = nullptr;
   RC(check_params(params));
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "batches hold laminar / inviscid cases");
+  if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
   if (params->lin_solver == JG_LS_BCGSTAB)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
   if (params->time_step_mode == JG_TS_CFL_MIN)
     return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
-  MeshCat cat;
+  MeshOwned cat;
   jg_case* h = new jg_case();
   int rc = concat_meshes(ncases, meshes, cat, h->case_off, h->case_nfa_b_off);
   if (rc == JG_OK) rc = build(h, &cat.m, params);
@@ -673,7 +750,7 @@ int jg_batch_set_state(jg_case_t* h, int k, const double* rho, const double* rho
   CK(cudaMemcpyAsync(h->d_io, rho, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + n, rhou, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * n, rhoE, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  launch_pack_state((int)n, h->d_io, h->st.q + 5 * c0, h->stream);
+  launch_pack_state((int)n, h->d_io, h->st.q + 5 * c0, nullptr, h->stream);
   CK(cudaMemsetAsync(h->st.prim + 8 * c0, 0, 8 * n * sizeof(double), h->stream));
   CKL();
   // the state/BC preamble runs at the next operator call, once every case has its state
@@ -685,7 +762,7 @@ int jg_batch_get_state(jg_case_t* h, int k, double* rho, double* rhou, double* r
   if (!h || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
   const size_t N = h->ncv, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
   if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
-  launch_unpack_state((int)n, h->st.q + 5 * c0, h->d_io, h->stream);
+  launch_unpack_state((int)n, h->st.q + 5 * c0, h->d_io, nullptr, h->stream);
   CKL();
   if (rho) CK(cudaMemcpyAsync(rho, h->d_io, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -740,7 +817,7 @@ int jg_set_state(jg_case_t* h, const double* rho, const double* rhou, const doub
   CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  launch_pack_state((int)N, h->d_io, h->st.q, h->stream);
+  launch_pack_state((int)N, h->d_io, h->st.q, h->d_cell_old, h->stream);
   CK(cudaMemsetAsync(h->st.prim, 0, 8 * N * sizeof(double), h->stream));
   return prime(h);
 }
@@ -754,7 +831,7 @@ int jg_get_state(jg_case_t* h, double* rho, double* rhou, double* rhoE) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
   const size_t N = h->ncv;
   if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
-  launch_unpack_state((int)N, h->st.q, h->d_io, h->stream);
+  launch_unpack_state((int)N, h->st.q, h->d_io, h->d_cell_old, h->stream);
   CKL();
   if (rho) CK(cudaMemcpyAsync(rho, h->d_io, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -769,13 +846,15 @@ int jg_get_primitives(jg_case_t* h, double* vel, double* press, double* temp, do
   std::vector<double> pr(8 * (size_t)N);
   CK(cudaMemcpyAsync(pr.data(), h->st.prim, pr.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int c = 0; c < N; c++) {
+  const std::vector<int>& perm = h->rn.cell_old;
+  for (int r = 0; r < N; r++) {
+    const int c = perm.empty() ? r : perm[r];
     if (vel)
-      for (int i = 0; i < 3; i++) vel[3 * c + i] = pr[8 * c + i];
-    if (press) press[c] = pr[8 * c + 3];
-    if (temp) temp[c] = pr[8 * c + 4];
-    if (enthalpy) enthalpy[c] = pr[8 * c + 5];
-    if (sos) sos[c] = pr[8 * c + 6];
+      for (int i = 0; i < 3; i++) vel[3 * c + i] = pr[8 * r + i];
+    if (press) press[c] = pr[8 * r + 3];
+    if (temp) temp[c] = pr[8 * r + 4];
+    if (enthalpy) enthalpy[c] = pr[8 * r + 5];
+    if (sos) sos[c] = pr[8 * r + 6];
   }
   return JG_OK;
 }
@@ -786,17 +865,19 @@ int jg_get_bfa(jg_case_t* h, double* rho_bfa, double* vel_bfa, double* p_bfa, do
   const int nb = h->nfa_b;
   std::vector<double> b(8 * (size_t)std::max(nb, 1));
   CK(cudaMemcpyAsync(b.data(), h->st.bfa, 8 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (mul_fa) CK(cudaMemcpyAsync(mul_fa, h->st.mul_fa, h->nfa * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (lamOcp_fa) CK(cudaMemcpyAsync(lamOcp_fa, h->st.lam_fa, h->nfa * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int f = 0; f < nb; f++) {
-    if (rho_bfa) rho_bfa[f] = b[8 * f];
+  const std::vector<int>& perm = h->rn.face_old;
+  for (int r = 0; r < nb; r++) {
+    const int f = perm.empty() ? r : perm[r];
+    if (rho_bfa) rho_bfa[f] = b[8 * r];
     if (vel_bfa)
-      for (int i = 0; i < 3; i++) vel_bfa[3 * f + i] = b[8 * f + 1 + i];
-    if (p_bfa) p_bfa[f] = b[8 * f + 4];
-    if (T_bfa) T_bfa[f] = b[8 * f + 5];
-    if (h_bfa) h_bfa[f] = b[8 * f + 6];
+      for (int i = 0; i < 3; i++) vel_bfa[3 * f + i] = b[8 * r + 1 + i];
+    if (p_bfa) p_bfa[f] = b[8 * r + 4];
+    if (T_bfa) T_bfa[f] = b[8 * r + 5];
+    if (h_bfa) h_bfa[f] = b[8 * r + 6];
   }
+  if (mul_fa) RC(download_rows(h, h->st.mul_fa, mul_fa, perm, h->nfa, 1));
+  if (lamOcp_fa) RC(download_rows(h, h->st.lam_fa, lamOcp_fa, perm, h->nfa, 1));
   return JG_OK;
 }
 
@@ -807,8 +888,8 @@ int jg_calc_dt(jg_case_t* h, double cfl, double* dt_min, double* local_dt) {
   CKL();
   double ctrl[3];
   CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
-  if (local_dt) CK(cudaMemcpyAsync(local_dt, h->st.local_dt, h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (local_dt) RC(download_rows(h, h->st.local_dt, local_dt, h->rn.cell_old, h->ncv, 1));
   if (dt_min) *dt_min = ctrl[2];
   return JG_OK;
 }
@@ -825,9 +906,11 @@ static int download_csr(jg_case* h, double* A) {
     return es == 8 ? ((const double*)v.data())[i] : (double)((const float*)v.data())[i];
   };
   memset(A, 0, sizeof(double) * b2 * (size_t)h->nbs);
+  const std::vector<int>& so = h->rn.nbs_old;  // the caller's nbocv entry of each internal one
+  auto slot = [&](int k) -> size_t { return so.empty() ? (size_t)k : (size_t)so[k]; };
   for (int c = 0; c < N; c++) {
     int kd = h->nbocv_i[c];
-    for (int e = 0; e < b2; e++) A[b2 * (size_t)kd + e] = get(D, (size_t)e * N + c);
+    for (int e = 0; e < b2; e++) A[b2 * slot(kd) + e] = get(D, (size_t)e * N + c);
     int s = c / SLICE, lane = c % SLICE;
     for (int j = 0; j < h->cell_cols[c + 1] - h->cell_cols[c]; j++) {
       int nb = h->col_nb[h->cell_cols[c] + j];
@@ -835,7 +918,7 @@ static int download_csr(jg_case* h, double* A) {
       while (k < h->nbocv_i[c + 1] && h->nbocv_v[k] != nb) k++;
       if (k >= h->nbocv_i[c + 1]) return set_err(JG_ERR_ARG, "neighbour %d of cell %d missing from nbocv", nb, c);
       for (int e = 0; e < b2; e++)
-        A[b2 * (size_t)k + e] += get(O, ((size_t)(h->ell_off[s] + j) * b2 + e) * SLICE + lane);
+        A[b2 * slot(k) + e] += get(O, ((size_t)(h->ell_off[s] + j) * b2 + e) * SLICE + lane);
     }
   }
   return JG_OK;
@@ -851,9 +934,11 @@ static int upload_csr(jg_case* h, const double* A) {
     else ((float*)v.data())[i] = (float)x;
   };
   std::vector<int> used;
+  const std::vector<int>& so = h->rn.nbs_old;
+  auto slot = [&](int k) -> size_t { return so.empty() ? (size_t)k : (size_t)so[k]; };
   for (int c = 0; c < N; c++) {
     int kd = h->nbocv_i[c];
-    for (int e = 0; e < 25; e++) put(D, (size_t)e * N + c, A[25 * (size_t)kd + e]);
+    for (int e = 0; e < 25; e++) put(D, (size_t)e * N + c, A[25 * slot(kd) + e]);
     int s = c / SLICE, lane = c % SLICE;
     used.clear();
     for (int j = 0; j < h->cell_cols[c + 1] - h->cell_cols[c]; j++) {
@@ -863,7 +948,7 @@ static int upload_csr(jg_case* h, const double* A) {
       int k = kd + 1;
       while (k < h->nbocv_i[c + 1] && h->nbocv_v[k] != nb) k++;
       if (k >= h->nbocv_i[c + 1]) return set_err(JG_ERR_ARG, "neighbour %d of cell %d missing from nbocv", nb, c);
-      for (int e = 0; e < 25; e++) put(O, ((size_t)(h->ell_off[s] + j) * 25 + e) * SLICE + lane, A[25 * (size_t)k + e]);
+      for (int e = 0; e < 25; e++) put(O, ((size_t)(h->ell_off[s] + j) * 25 + e) * SLICE + lane, A[25 * slot(k) + e]);
     }
   }
   CK(cudaMemcpyAsync(h->st.D, D.data(), D.size(), cudaMemcpyHostToDevice, h->stream));
@@ -884,11 +969,13 @@ int jg_calc_rhs(jg_case_t* h, double* rhs_rho, double* rhs_rhou, double* rhs_rho
   std::vector<double> r(5 * (size_t)N);
   CK(cudaMemcpyAsync(r.data(), h->st.rhs, r.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int c = 0; c < N; c++) {
-    if (rhs_rho) rhs_rho[c] = r[5 * c];
+  const std::vector<int>& perm = h->rn.cell_old;
+  for (int q = 0; q < N; q++) {
+    const int c = perm.empty() ? q : perm[q];
+    if (rhs_rho) rhs_rho[c] = r[5 * q];
     if (rhs_rhou)
-      for (int i = 0; i < 3; i++) rhs_rhou[3 * c + i] = r[5 * c + 1 + i];
-    if (rhs_rhoE) rhs_rhoE[c] = r[5 * c + 4];
+      for (int i = 0; i < 3; i++) rhs_rhou[3 * c + i] = r[5 * q + 1 + i];
+    if (rhs_rhoE) rhs_rhoE[c] = r[5 * q + 4];
   }
   if (implicit) RC(download_csr(h, A));
   return JG_OK;
@@ -899,11 +986,11 @@ int jg_get_gradients(jg_case_t* h, double* grad_u, double* grad_rho, double* gra
   const int N = h->ncv;
   // the reference's grad_u after calcRhs: the viscous pass overwrites it (unlimited when VISC_LIMITER=NO)
   const double* gu = h->p.viscous ? h->st.guv : h->st.gu;
-  if (grad_u) CK(cudaMemcpyAsync(grad_u, gu, 9 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (grad_rho) CK(cudaMemcpyAsync(grad_rho, h->st.grho, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (grad_p) CK(cudaMemcpyAsync(grad_p, h->st.gp, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (grad_h) CK(cudaMemcpyAsync(grad_h, h->st.gh, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  const std::vector<int>& perm = h->rn.cell_old;
+  if (grad_u) RC(download_rows(h, gu, grad_u, perm, N, 9));
+  if (grad_rho) RC(download_rows(h, h->st.grho, grad_rho, perm, N, 3));
+  if (grad_p) RC(download_rows(h, h->st.gp, grad_p, perm, N, 3));
+  if (grad_h) RC(download_rows(h, h->st.gh, grad_h, perm, N, 3));
   return JG_OK;
 }
 
@@ -980,11 +1067,13 @@ static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, d
   return JG_OK;
 }
 
-// transpose [N][5] <-> [5][N] helpers on the host
-static void to_soa(const double* aos, std::vector<double>& soa, int N) {
+// the caller's [N][5] rows -> [5][N] planes in the handle's order
+static void to_soa(const double* aos, std::vector<double>& soa, int N, const std::vector<int>& perm) {
   soa.resize(5 * (size_t)N);
-  for (int c = 0; c < N; c++)
-    for (int i = 0; i < 5; i++) soa[(size_t)i * N + c] = aos[5 * c + i];
+  for (int c = 0; c < N; c++) {
+    const int o = perm.empty() ? c : perm[c];
+    for (int i = 0; i < 5; i++) soa[(size_t)i * N + c] = aos[5 * o + i];
+  }
 }
 
 int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rhs, double zeroAbs, double zeroRel,
@@ -994,7 +1083,7 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
   const int N = h->ncv;
   RC(upload_csr(h, A));
   launch_dinv(h->m, h->p, h->st, h->stream);
-  CK(cudaMemcpyAsync(h->st.b, rhs, 5 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  RC(upload_rows(h, h->st.b, rhs, h->rn.cell_old, N, 5));
   CKL();
   int it = 0;
   switch (h->hp.lin_solver) {
@@ -1006,9 +1095,9 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
       double* phi = (double*)h->st.x0;
       double* b = (double*)h->st.x1;
       std::vector<double> soa;
-      to_soa(dq, soa, N);
+      to_soa(dq, soa, N, h->rn.cell_old);
       CK(cudaMemcpyAsync(phi, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-      to_soa(rhs, soa, N);
+      to_soa(rhs, soa, N, h->rn.cell_old);
       CK(cudaMemcpyAsync(b, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
       RC(bcgstab(h, phi, b, zeroAbs, zeroRel, maxIter, &it));
       launch_dq_from_x(h->m, h->p, h->st, phi, h->stream);
@@ -1032,8 +1121,7 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
     } break;
   }
   CKL();
-  CK(cudaMemcpyAsync(dq, h->st.dq, 5 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  RC(download_rows(h, h->st.dq, dq, h->rn.cell_old, N, 5));
   if (iters) *iters = it;
   return JG_OK;
 }
@@ -1097,7 +1185,7 @@ static int enqueue_step(jg_case* h, int for_graph) {
     std::vector<double> tmp(n5), soa;
     CK(cudaMemcpyAsync(tmp.data(), h->st.b, n5 * sizeof(double), cudaMemcpyDeviceToHost, S));
     CK(cudaStreamSynchronize(S));
-    to_soa(tmp.data(), soa, h->ncv);
+    to_soa(tmp.data(), soa, h->ncv, {});  // already in the handle's order
     CK(cudaMemcpyAsync(b, soa.data(), n5 * sizeof(double), cudaMemcpyHostToDevice, S));
     int it;
     RC(bcgstab(h, phi, b, h->hp.ls_abs, h->hp.ls_rel, h->hp.ls_max_iter, &it));
@@ -1276,8 +1364,11 @@ extern "C" int jg_set_scalars(jg_case_t* h, const double* phi) {
   if (h->bs == 5) return set_err(JG_ERR_ARG, "the case transports no scalar");
   const size_t N = h->ncv, ns = h->turb.ns;
   std::vector<double> cm(ns * N);  // [ncv][ns] -> [ns][ncv]
-  for (size_t c = 0; c < N; c++)
-    for (size_t q = 0; q < ns; q++) cm[q * N + c] = phi[ns * c + q];
+  const std::vector<int>& perm = h->rn.cell_old;
+  for (size_t c = 0; c < N; c++) {
+    const size_t o = perm.empty() ? c : (size_t)perm[c];
+    for (size_t q = 0; q < ns; q++) cm[q * N + c] = phi[ns * o + q];
+  }
   CK(cudaMemcpyAsync(h->turb.phi, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->primed = 0;  // the state, scalar boundary values and turbulent viscosity follow at the next call
@@ -1291,8 +1382,11 @@ extern "C" int jg_get_scalars(jg_case_t* h, double* phi) {
   std::vector<double> cm(ns * N);
   CK(cudaMemcpyAsync(cm.data(), h->turb.phi, cm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (size_t c = 0; c < N; c++)
-    for (size_t q = 0; q < ns; q++) phi[ns * c + q] = cm[q * N + c];
+  const std::vector<int>& perm = h->rn.cell_old;
+  for (size_t c = 0; c < N; c++) {
+    const size_t o = perm.empty() ? c : (size_t)perm[c];
+    for (size_t q = 0; q < ns; q++) phi[ns * o + q] = cm[q * N + c];
+  }
   return JG_OK;
 }
 
@@ -1302,17 +1396,19 @@ extern "C" int jg_get_turb_array(jg_case_t* h, const char* name, double* out) {
   if (!h->primed) RC(prime(h));
   const size_t N = h->ncv, ns = h->turb.ns;
   const Turb& t = h->turb;
-  struct { const char* n; const double* p; size_t len; } tab[] = {
-      {"wallDist", t.wd, N}, {"strMag", t.strMag, N}, {"vortMag", t.vortMag, N}, {"diverg", t.diverg, N},
-      {"crossDiff", t.crossDiff, N}, {"blendFuncF1", t.F1, N}, {"blendFuncF2", t.F2, N},
-      {"mut_fa", h->st.mut_fa, (size_t)h->nfa}, {"phi_bfa", t.phi_bfa, ns * h->nfa_b},
-      {"grad_phi", t.grad_phi, 3 * ns * N}, {"diff", t.diff, ns * h->nfa}};
+  const std::vector<int>&cp = h->rn.cell_old, &fp = h->rn.face_old;
+  const size_t nfa = h->nfa, nfa_b = h->nfa_b;
+  // name, array, order, rows, doubles per row, blocks (one per scalar)
+  struct { const char* n; const double* p; const std::vector<int>* perm; size_t rows, w, nblk; } tab[] = {
+      {"wallDist", t.wd, &cp, N, 1, 1}, {"strMag", t.strMag, &cp, N, 1, 1}, {"vortMag", t.vortMag, &cp, N, 1, 1},
+      {"diverg", t.diverg, &cp, N, 1, 1}, {"crossDiff", t.crossDiff, &cp, N, 1, 1},
+      {"blendFuncF1", t.F1, &cp, N, 1, 1}, {"blendFuncF2", t.F2, &cp, N, 1, 1},
+      {"mut_fa", h->st.mut_fa, &fp, nfa, 1, 1}, {"phi_bfa", t.phi_bfa, &fp, nfa_b, 1, ns},
+      {"grad_phi", t.grad_phi, &cp, N, 3, ns}, {"diff", t.diff, &fp, nfa, 1, ns}};
   for (auto& e : tab)
     if (strcmp(e.n, name) == 0) {
       if (!e.p) return set_err(JG_ERR_ARG, "%s is not an array of this model", name);
-      CK(cudaMemcpyAsync(out, e.p, e.len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-      CK(cudaStreamSynchronize(h->stream));
-      return JG_OK;
+      return download_rows(h, e.p, out, *e.perm, e.rows, e.w, e.nblk);
     }
   return set_err(JG_ERR_ARG, "unknown turbulence array %s", name);
 }
@@ -1324,8 +1420,7 @@ extern "C" int jg_calc_rhs_coupled(jg_case_t* h, double* rhs, double* A, int fla
   int implicit = flagImplicit && A != nullptr;
   launch_flux6(h->m, h->p, h->st, h->turb, implicit, 0, h->stream);
   CKL();
-  CK(cudaMemcpyAsync(rhs, h->st.rhs, (size_t)h->bs * h->ncv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  RC(download_rows(h, h->st.rhs, rhs, h->rn.cell_old, h->ncv, h->bs));
   if (implicit) RC(download_csr(h, A));
   return check_err_flags(h);
 }
@@ -1336,13 +1431,14 @@ extern "C" int jg_get_turb(jg_case_t* h, double* wallDist, double* mut_fa, doubl
   if (h->bs == 5) return set_err(JG_ERR_ARG, "the case has no turbulence model");
   if (!h->primed) RC(prime(h));
   const size_t N = h->ncv;
-  struct { double* dst; const double* src; size_t n; } t[] = {
-      {wallDist, h->turb.wd, N}, {mut_fa, h->st.mut_fa, (size_t)h->nfa}, {strMag, h->turb.strMag, N},
-      {vortMag, h->turb.vortMag, N}, {phi_bfa, h->turb.phi_bfa, (size_t)h->nfa_b},
-      {grad_phi, h->turb.grad_phi, 3 * N}, {diff, h->turb.diff, (size_t)h->nfa}};
+  const std::vector<int>&cp = h->rn.cell_old, &fp = h->rn.face_old;
+  struct { double* dst; const double* src; const std::vector<int>* perm; size_t n, w; } t[] = {
+      {wallDist, h->turb.wd, &cp, N, 1}, {mut_fa, h->st.mut_fa, &fp, (size_t)h->nfa, 1},
+      {strMag, h->turb.strMag, &cp, N, 1}, {vortMag, h->turb.vortMag, &cp, N, 1},
+      {phi_bfa, h->turb.phi_bfa, &fp, (size_t)h->nfa_b, 1}, {grad_phi, h->turb.grad_phi, &cp, N, 3},
+      {diff, h->turb.diff, &fp, (size_t)h->nfa, 1}};
   for (auto& e : t)
-    if (e.dst) CK(cudaMemcpyAsync(e.dst, e.src, e.n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+    if (e.dst) RC(download_rows(h, e.src, e.dst, *e.perm, e.n, e.w));
   return JG_OK;
 }
 
@@ -1359,6 +1455,7 @@ int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** ou
   if (params->lin_solver == JG_LS_BCGSTAB)
     return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "served cases are laminar / inviscid");
+  if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "served cases keep their own order");
   if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
     return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
   jg_case* h = new jg_case();
@@ -1381,7 +1478,7 @@ int serve_case_start(jg_case* h, const double* rho, const double* rhou, const do
   CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  launch_pack_state((int)N, h->d_io, h->st.q, h->stream);
+  launch_pack_state((int)N, h->d_io, h->st.q, nullptr, h->stream);
   launch_state(h->m, h->p, h->st, h->stream);
   launch_face_props(h->m, h->p, h->st, h->stream);
   launch_bc(h->m, h->p, h->st, h->stream);

@@ -1,6 +1,7 @@
 // jg_internal.h -- device-side data layout of one case and the kernel launchers.
 //
-// Cells keep the reference's numbering.  Per-cell vectors are stored
+// Cells keep the caller's numbering unless the handle renumbers them
+// (jg_renumber.cu).  Per-cell vectors are stored
 // cell-major ([N][k], a warp reads them contiguously); the implicit matrix is
 // stored per row in a sliced-ELL layout: 32-cell slices (one warp), each
 // slice padded to its widest row, components innermost across the 32 cells,
@@ -9,6 +10,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <vector>
 
 #include "../../include/joe_b200.h"
 
@@ -162,8 +165,9 @@ void launch_lin3(long n, double* out, double a, const double* x, double b, const
 void launch_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
                        double* F, double* AL, double* AR, cudaStream_t s);
 
-void launch_pack_state(int n, const double* io, double* q, cudaStream_t s);
-void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s);
+// io ([5][n] planes rho, rhou, rhoE) <-> q ([n][5]); perm (or nullptr): the io row of each cell
+void launch_pack_state(int n, const double* io, double* q, const int* perm, cudaStream_t s);
+void launch_unpack_state(int n, const double* q, double* io, const int* perm, cudaStream_t s);
 
 int grid_for(long n, int block);
 int record_error(int code, const char* msg);  // sets the jg_last_error message
@@ -184,6 +188,24 @@ void launch_relax6(const Mesh& m, const Params& p, State& st, int sgs, int sweep
 void launch_update6(const Mesh& m, const Params& p, State& st, Turb& t, const void* x, cudaStream_t s);
 // the flow gradients as calcFluxCoupled takes them (jg_kernels.cu)
 void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+}  // namespace jg
+
+namespace jg {
+// A mesh in jg_mesh's layout whose arrays the struct owns (concatenated
+// batches, renumbered cases); bind() points m at the vectors.
+struct MeshOwned {
+  std::vector<int> cvofa, faocv_i, faocv_v, nbocv_i, nbocv_v;
+  std::vector<double> x_cv, x_fa, fa_normal, vol, lsq, blsq;
+  std::vector<jg_zone> zones;
+  jg_mesh m{};
+  void bind();
+};
+// the caller's id of each cell, face and nbocv entry in a handle's own order (jg_renumber.cu)
+struct Renumbering {
+  std::vector<int> cell_old, face_old, nbs_old;
+};
+int rcm_order(const jg_mesh& m, std::vector<int>& cell_old);
+int renumber_mesh(const jg_mesh& in, int method, MeshOwned& out, Renumbering& r);
 }  // namespace jg
 
 // per-case operations used by the serving engine (defined in jg_api.cu)

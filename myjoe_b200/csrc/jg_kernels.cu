@@ -1123,30 +1123,32 @@ __global__ void k_flux_faces(int kind, int n, const double* L, const double* R, 
 }
 
 // state staging: io = [rho(N) | rhou(N*3) | rhoE(N)] in the reference's layouts
-__global__ void k_pack_state(int n, const double* io, double* q) {
+__global__ void k_pack_state(int n, const double* io, double* q, const int* perm) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  q[5 * c] = io[c];
-  for (int i = 0; i < 3; i++) q[5 * c + 1 + i] = io[n + 3 * c + i];
-  q[5 * c + 4] = io[4 * n + c];
+  int r = perm ? perm[c] : c;
+  q[5 * c] = io[r];
+  for (int i = 0; i < 3; i++) q[5 * c + 1 + i] = io[n + 3 * r + i];
+  q[5 * c + 4] = io[4 * n + r];
 }
 
-__global__ void k_unpack_state(int n, const double* q, double* io) {
+__global__ void k_unpack_state(int n, const double* q, double* io, const int* perm) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  io[c] = q[5 * c];
-  for (int i = 0; i < 3; i++) io[n + 3 * c + i] = q[5 * c + 1 + i];
-  io[4 * n + c] = q[5 * c + 4];
+  int r = perm ? perm[c] : c;
+  io[r] = q[5 * c];
+  for (int i = 0; i < 3; i++) io[n + 3 * r + i] = q[5 * c + 1 + i];
+  io[4 * n + r] = q[5 * c + 4];
 }
 
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-void launch_pack_state(int n, const double* io, double* q, cudaStream_t s) {
-  k_pack_state<<<grid_for(n, 256), 256, 0, s>>>(n, io, q);
+void launch_pack_state(int n, const double* io, double* q, const int* perm, cudaStream_t s) {
+  k_pack_state<<<grid_for(n, 256), 256, 0, s>>>(n, io, q, perm);
 }
-void launch_unpack_state(int n, const double* q, double* io, cudaStream_t s) {
-  k_unpack_state<<<grid_for(n, 256), 256, 0, s>>>(n, q, io);
+void launch_unpack_state(int n, const double* q, double* io, const int* perm, cudaStream_t s) {
+  k_unpack_state<<<grid_for(n, 256), 256, 0, s>>>(n, q, io, perm);
 }
 constexpr int TB = 128;
 

@@ -31,7 +31,8 @@ class RawMesh:
     cvofa: np.ndarray         # [nfa, 2] cell ids, cvofa[:,1] == -1 on boundaries
     ncv: int
     zones: list               # [(name, face ids ndarray)] boundary zones, in order
-    cell_type: int = 4        # Fluent cell type of the (single) cell zone: 4 = hex
+    cell_type: int = 4        # Fluent cell type of the (single) cell zone: 4 = hex, 0 = mixed
+    cell_types: np.ndarray | None = None   # [ncv] per-cell Fluent types of a mixed zone (6 = prism)
 
     @property
     def nfa(self) -> int:
@@ -213,7 +214,14 @@ def write_msh(path: str, mesh: RawMesh) -> None:
     lines.extend("%.17e %.17e %.17e" % tuple(p) for p in mesh.x_no)
     lines.append("))")
     lines.append("(12 (0 1 %x 0))" % mesh.ncv)
-    lines.append("(12 (2 1 %x 1 %x))" % (mesh.ncv, mesh.cell_type))
+    if mesh.cell_types is not None:
+        # mixed zone: element type 0 followed by one type per cell
+        lines.append("(12 (2 1 %x 1 0)(" % mesh.ncv)
+        ct = np.asarray(mesh.cell_types)
+        lines.extend(" ".join("%x" % int(v) for v in ct[i:i + 16]) for i in range(0, ct.size, 16))
+        lines.append("))")
+    else:
+        lines.append("(12 (2 1 %x 1 %x))" % (mesh.ncv, mesh.cell_type))
     lines.append("(13 (0 1 %x 0))" % nfa)
     start = 1
     zone_ids = []
@@ -240,3 +248,152 @@ def write_msh(path: str, mesh: RawMesh) -> None:
     with open(path, "w") as f:
         f.write("\n".join(lines))
         f.write("\n")
+
+
+def channel_bump_mixed(nx=64, ny=32, nz=2, n_prism=8, length=3.0, height=1.0, bump_h=0.1, bump_x0=1.0,
+                       bump_x1=2.0, depth=None, jitter=0.0, seed=0, stretch=1.0, alternate=False) -> RawMesh:
+    """The channel-bump domain of ``channel_bump`` with a hybrid mesh: the
+    wall surface (x-z) is triangulated, each (i, k) quad split along its
+    (i, k)-(i+1, k+1) diagonal (with ``alternate``, quads with i + k odd along
+    the other one), and extruded wall-normal into ``n_prism`` rows of
+    triangular prisms; hexahedra fill the rows above.  The hexahedra
+    on the last prism row see two triangles where a hexahedron has its lower
+    quad (a 7-faced polyhedron, which the face-based reader takes as it
+    takes any cell).  Zones as ``channel_bump``; faces are triangles (the
+    prism caps) or quadrilaterals."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, length, nx + 1)
+    if stretch != 1.0:
+        h = stretch ** np.arange(ny)
+        eta = np.concatenate([[0.0], np.cumsum(h)]) / h.sum()
+    else:
+        eta = np.linspace(0.0, 1.0, ny + 1)
+    yb = np.where((xs >= bump_x0) & (xs <= bump_x1),
+                  bump_h * np.sin(math.pi * (xs - bump_x0) / (bump_x1 - bump_x0)) ** 2, 0.0)
+    X = np.repeat(xs[:, None], ny + 1, 1)
+    Y = yb[:, None] + (height - yb[:, None]) * eta[None, :]
+    if jitter > 0.0:
+        X[1:-1, 1:-1] += jitter * (length / nx) * rng.uniform(-1, 1, size=(nx - 1, ny - 1))
+        Y[1:-1, 1:-1] += jitter * (height / ny) * rng.uniform(-1, 1, size=(nx - 1, ny - 1))
+    if depth is None:
+        depth = nz * length / nx
+    zs = np.linspace(0.0, depth, nz + 1)
+    npr = int(min(max(n_prism, 0), ny))
+
+    # nodes (i, j, k)
+    def nid(i, j, k):
+        return (np.asarray(i) * (ny + 1) + j) * (nz + 1) + k
+
+    I3, J3, K3 = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    x_no = np.stack([X[I3, J3], Y[I3, J3], zs[K3]], -1).reshape(-1, 3)
+
+    # cells: prisms A (i,k)(i+1,k)(i+1,k+1) and B (i,k)(i+1,k+1)(i,k+1) of each (i, k) quad in rows j < npr,
+    # then hexahedra, row by row
+    P = 2 * nx * nz * npr
+
+    def prism(i, j, k, t):
+        return ((np.asarray(j) * nx + i) * nz + k) * 2 + t
+
+    def hexa(i, j, k):
+        return P + ((np.asarray(j) - npr) * nx + i) * nz + k
+
+    def flip(i, k):
+        return ((np.asarray(i) + k) % 2 == 1) if alternate else np.zeros(np.broadcast(i, k).shape, bool)
+
+    def cell(i, j, k, t):
+        """cell of row j at quad (i, k); in a prism row the triangle t (0: A, 1: B)"""
+        return np.where(np.asarray(j) < npr, prism(i, j, k, t), hexa(i, j, k))
+
+    # the triangle holding each edge of quad (i, k): the k edge is A's, the k+1 edge B's; the i+1 edge
+    # is A's and the i edge B's, the other way round on a flipped quad (A' = (i,k) (i+1,k) (i,k+1),
+    # B' = (i+1,k) (i+1,k+1) (i,k+1))
+    def t_i1(i, k):
+        return np.where(flip(i, k), 1, 0)
+
+    def t_i0(i, k):
+        return np.where(flip(i, k), 0, 1)
+
+    ncv = P + nx * nz * (ny - npr)
+    faces, cv, zone = [], [], []
+
+    def add(nodes, c0, c1, name):
+        nodes = np.asarray(nodes).reshape(-1, nodes.shape[-1])
+        if nodes.shape[1] == 3:
+            nodes = np.concatenate([nodes, -np.ones((nodes.shape[0], 1), np.int64)], 1)
+        faces.append(nodes)
+        c0 = np.broadcast_to(c0, (nodes.shape[0],)).ravel()
+        c1 = np.broadcast_to(c1, (nodes.shape[0],)).ravel()
+        cv.append(np.stack([c0, c1], 1))
+        zone.extend([name] * nodes.shape[0])
+
+    # y-faces (constant j).  Node order (i,k) (i+1,k) (i+1,k+1) [(i,k+1)] gives the normal -y:
+    # c0 is the cell above, c1 the one below; on the upper boundary the order is reversed.
+    Ii, Kk = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    Ii, Kk = Ii.ravel(), Kk.ravel()
+    for j in range(ny + 1):
+        above = j < ny
+        below = j > 0
+        if j <= npr and npr > 0:
+            fl = flip(Ii, Kk)[:, None]
+            ta = np.where(fl, np.stack([nid(Ii, j, Kk), nid(Ii + 1, j, Kk), nid(Ii, j, Kk + 1)], 1),
+                          np.stack([nid(Ii, j, Kk), nid(Ii + 1, j, Kk), nid(Ii + 1, j, Kk + 1)], 1))
+            tb = np.where(fl, np.stack([nid(Ii + 1, j, Kk), nid(Ii + 1, j, Kk + 1), nid(Ii, j, Kk + 1)], 1),
+                          np.stack([nid(Ii, j, Kk), nid(Ii + 1, j, Kk + 1), nid(Ii, j, Kk + 1)], 1))
+            for t, tri in ((0, ta), (1, tb)):
+                if above and below:
+                    add(tri, cell(Ii, j, Kk, t), prism(Ii, j - 1, Kk, t), None)
+                elif above:
+                    add(tri, cell(Ii, j, Kk, t), -1, "lower")
+                else:
+                    add(tri[:, ::-1], prism(Ii, j - 1, Kk, t), -1, "upper")
+        else:
+            q = np.stack([nid(Ii, j, Kk), nid(Ii + 1, j, Kk), nid(Ii + 1, j, Kk + 1), nid(Ii, j, Kk + 1)], 1)
+            if above and below:
+                add(q, hexa(Ii, j, Kk), hexa(Ii, j - 1, Kk), None)
+            elif above:
+                add(q, hexa(Ii, j, Kk), -1, "lower")
+            else:
+                add(q[:, ::-1], hexa(Ii, j - 1, Kk), -1, "upper")
+    # x-faces (constant i): order (i,j,k) (i,j+1,k) (i,j+1,k+1) (i,j,k+1) gives +x: c0 left, c1 right.
+    # Left of column i is triangle A of quad i-1 (its i+1 edge), right is triangle B of quad i.
+    Jj, Kk2 = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+    Jj, Kk2 = Jj.ravel(), Kk2.ravel()
+    for i in range(nx + 1):
+        q = np.stack([nid(i, Jj, Kk2), nid(i, Jj + 1, Kk2), nid(i, Jj + 1, Kk2 + 1), nid(i, Jj, Kk2 + 1)], 1)
+        if i == 0:
+            add(q[:, ::-1], cell(0, Jj, Kk2, t_i0(0, Kk2)), -1, "inlet")
+        elif i == nx:
+            add(q, cell(nx - 1, Jj, Kk2, t_i1(nx - 1, Kk2)), -1, "outlet")
+        else:
+            add(q, cell(i - 1, Jj, Kk2, t_i1(i - 1, Kk2)), cell(i, Jj, Kk2, t_i0(i, Kk2)), None)
+    # z-faces (constant k): order (i,j,k) (i+1,j,k) (i+1,j+1,k) (i,j+1,k) gives +z: c0 the cell at k-1
+    # (triangle B, its k+1 edge), c1 the cell at k (triangle A, its k edge).
+    Ii3, Jj3 = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    Ii3, Jj3 = Ii3.ravel(), Jj3.ravel()
+    for k in range(nz + 1):
+        q = np.stack([nid(Ii3, Jj3, k), nid(Ii3 + 1, Jj3, k), nid(Ii3 + 1, Jj3 + 1, k), nid(Ii3, Jj3 + 1, k)], 1)
+        if k == 0:
+            add(q[:, ::-1], cell(Ii3, Jj3, 0, 0), -1, "sides")
+        elif k == nz:
+            add(q, cell(Ii3, Jj3, nz - 1, 1), -1, "sides")
+        else:
+            add(q, cell(Ii3, Jj3, k - 1, 1), cell(Ii3, Jj3, k, 0), None)
+    # diagonal faces inside the prism quads: (i,j,k) (i+1,j,k+1) (i+1,j+1,k+1) (i,j+1,k) points from A to B;
+    # on a flipped quad (i+1,j,k) (i,j,k+1) (i,j+1,k+1) (i+1,j+1,k) points from B' to A'
+    if npr:
+        Ii4, Jj4, Kk4 = (a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(npr), np.arange(nz), indexing="ij"))
+        fl = flip(Ii4, Kk4)
+        q = np.where(fl[:, None],
+                     np.stack([nid(Ii4 + 1, Jj4, Kk4), nid(Ii4, Jj4, Kk4 + 1), nid(Ii4, Jj4 + 1, Kk4 + 1),
+                               nid(Ii4 + 1, Jj4 + 1, Kk4)], 1),
+                     np.stack([nid(Ii4, Jj4, Kk4), nid(Ii4 + 1, Jj4, Kk4 + 1), nid(Ii4 + 1, Jj4 + 1, Kk4 + 1),
+                               nid(Ii4, Jj4 + 1, Kk4)], 1))
+        add(q, prism(Ii4, Jj4, Kk4, np.where(fl, 1, 0)), prism(Ii4, Jj4, Kk4, np.where(fl, 0, 1)), None)
+    fa_nodes = np.concatenate(faces).astype(np.int64)
+    fa_nno = np.where(fa_nodes[:, 3] >= 0, 4, 3).astype(np.int64)
+    cvofa = np.concatenate(cv).astype(np.int64)
+    names = np.array([z if z is not None else "" for z in zone], dtype=object)
+    zones = [(zname, np.nonzero(names == zname)[0]) for zname in ("inlet", "outlet", "lower", "upper", "sides")]
+    cell_types = np.concatenate([np.full(P, 6), np.full(ncv - P, 4)])
+    return RawMesh(x_no=x_no, fa_nodes=fa_nodes, fa_nno=fa_nno, cvofa=cvofa, ncv=ncv, zones=zones,
+                   cell_type=0 if npr else 4, cell_types=cell_types if npr else None)

@@ -44,6 +44,7 @@ def lib():
         L.jg_version.restype = I
         L.jg_device_count.argtypes = [C.POINTER(I)]
         L.jg_create.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
+        L.jg_renumber_cells.argtypes = [C.POINTER(jg_mesh), I, C.POINTER(I)]
         L.jg_destroy.argtypes = [P]
         L.jg_get_stream.argtypes = [P, C.POINTER(P)]
         L.jg_set_state.argtypes = [P, D, D, D]
@@ -107,10 +108,10 @@ class JoeGpu:
     """One case on the GPU.  ``mesh_src`` is a ``geometry.CvMesh`` or a dict of
     reference-layout arrays; ``params`` a ``case.JoeParams``."""
 
-    def __init__(self, mesh_src, params: JoeParams, precision: int = 0):
+    def __init__(self, mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False):
         self.params = params
         self.ma = MeshArrays(mesh_src, params)
-        self.jp = make_params(params, precision)
+        self.jp = make_params(params, precision, renumber)
         self.ncv = self.ma.ncv
         h = C.c_void_p()
         _ck(lib().jg_create(C.byref(self.ma.mesh), C.byref(self.jp), C.byref(h)))
@@ -379,10 +380,19 @@ class JoeServer:
         return {"resident": r.value, "queued": q.value, "unfetched": f.value, "bytes_resident": b.value}
 
 
-def case_footprint(mesh_src, params: JoeParams, precision: int = 0) -> float:
+def case_footprint(mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False) -> float:
     """Device bytes jg_create + jg_set_state allocate for this case."""
     ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
-    jp = make_params(params, precision)
+    jp = make_params(params, precision, renumber)
     b = C.c_double()
     _ck(lib().jg_case_footprint(C.byref(ma.mesh), C.byref(jp), C.byref(b)))
     return b.value
+
+
+def renumber_cells(mesh_src, params: JoeParams) -> np.ndarray:
+    """The cell order a handle made with ``renumber=True`` uses: the caller's id
+    of each cell (reverse Cuthill-McKee; host only, no GPU needed)."""
+    ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
+    out = np.empty(ma.ncv, np.int32)
+    _ck(lib().jg_renumber_cells(C.byref(ma.mesh), 1, out.ctypes.data_as(C.POINTER(C.c_int))))
+    return out

@@ -8,7 +8,7 @@ and boundary-face states, local time step, gradients, RHS, the implicit
 matrix A, one linear solve, and the state + L1 residuals after a few
 runBackwardEuler steps.
 
-    python tests/golden/make_golden.py [segregated] [sa] [sst]    # needs the reference + g++
+    python tests/golden/make_golden.py [segregated] [sa] [sst] [--only=NAME_PART]   # needs the reference + g++
 """
 from __future__ import annotations
 
@@ -42,6 +42,8 @@ def cases():
     bc_iso = dict(visc.bcs)
     bc_iso["lower"] = BC("WALL", (350.0,))
     rawp, _, prmp = case.plate_case(12, 8, 2)
+    # prism rows on the wall (triangulated wall surface extruded wall-normal), hexahedra above
+    rawm = meshgen.channel_bump_mixed(12, 6, 2, n_prism=2, stretch=1.2, jitter=0.1, seed=4)
     yield "bump_hllc", raw, prm
     yield "bump_roe", raw, dataclasses.replace(prm, SPACE_INTEGRATION="ROE")
     yield "bump_ausm_first_order", raw, dataclasses.replace(prm, SPACE_INTEGRATION="AUSM", SECOND_ORDER=False)
@@ -55,6 +57,8 @@ def cases():
                                                                           SPACE_INTEGRATION="HLLC",
                                                                           VISC_LIMITER=False)
     yield "plate_roe", rawp, prmp
+    yield "mixed_bump_hllc", rawm, prm
+    yield "mixed_bump_roe_laminar_isothermal", rawm, dataclasses.replace(visc, bcs=bc_iso)
 
 
 def sa_cases():
@@ -65,6 +69,8 @@ def sa_cases():
     bc_n["outlet"] = BC("NEUMANN")
     yield "sa_bump_farfield", raw, prm
     yield "sa_bump_cbc_symm_original", rawc, dataclasses.replace(prmc, SYMM_BC="ORIGINAL_NUMERIC")
+    rawm, _, prmm = case.sa_bump_case(12, 8, 2, stretch=1.2, jitter=0.1, seed=6, n_prism=3, alternate=True)
+    yield "sa_mixed_bump_farfield", rawm, prmm
     yield "sa_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
 
@@ -77,6 +83,8 @@ def sst_cases():
     bc_n["outlet"] = BC("NEUMANN")
     yield "sst_bump_farfield", raw, prm
     yield "sst_bump_cbc_symm_original", rawc, dataclasses.replace(prmc, SYMM_BC="ORIGINAL_NUMERIC")
+    rawm, _, prmm = case.sst_bump_case(12, 8, 2, stretch=1.2, jitter=0.1, seed=6, n_prism=3, alternate=True)
+    yield "sst_mixed_bump_farfield", rawm, prmm
     yield "sst_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
 
@@ -95,8 +103,11 @@ def params_from_json(s: str):
     return case.JoeParams(bcs=bcs, **d)
 
 
-def main(which=("segregated", "sa")):
+def main(which=("segregated", "sa"), only=""):
+    """``only``: regenerate just the fixtures whose name contains it."""
     for name, raw, prm in (cases() if "segregated" in which else ()):
+        if only not in name:
+            continue
         extra = "HARNESS_PERTURB = %g" % PERTURB
         d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "dump")
         prm_run = dataclasses.replace(prm, NSTEPS=NSTEPS)
@@ -117,6 +128,8 @@ def main(which=("segregated", "sa")):
     turb = [(n, r, p, 1) for n, r, p in (sa_cases() if "sa" in which else ())]
     turb += [(n, r, p, 2) for n, r, p in (sst_cases() if "sst" in which else ())]
     for name, raw, prm, run_kind in turb:
+        if only not in name:
+            continue
         extra = "HARNESS_PERTURB = %g" % PERTURB
         d = refrun.run(lambda p: meshgen.write_msh(p, raw), prm.joe_in("mesh.msh", extra), "coupled",
                        run_kind=run_kind)
@@ -142,4 +155,6 @@ def load(path):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("segregated", "sa", "sst"))
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = [a[len("--only="):] for a in sys.argv[1:] if a.startswith("--only=")]
+    main(tuple(args) or ("segregated", "sa", "sst"), only[0] if only else "")

@@ -50,7 +50,11 @@ enum { JG_TS_CFL = 0, JG_TS_CFL_MIN = 1, JG_TS_DT = 2 };
 enum { JG_DT_MAX_BASED = 0, JG_DT_SUM_BASED = 1 };
 /* linear solvers: BCGSTAB and LUSGS follow the reference (UgpWithCv.cpp:2660, 3172);
  * JACOBI / SGS are block point relaxation (fixed sweep count) */
-enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3 };
+enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3,
+       /* BCGSTAB_LINELET: BiCGSTAB preconditioned by block-tridiagonal solves along the
+        * wall-normal lines of initializeLinelet (JoeWithModels.cpp:7471-7559) and the
+        * block diagonal elsewhere, solveCvVectorR5BcgstabLine (UgpWithCv.cpp:3627-3992) */
+       JG_LS_BCGSTAB_LINELET = 4 };
 enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
 
 typedef struct jg_zone {

@@ -82,6 +82,7 @@ struct jg_case {
   int bs = 5;               // block size: 5, or 6 on the coupled SA path
   Turb turb{};              // SA arrays (coupled path)
   Renumbering rn;           // caller's id of each internal cell / face / nbocv entry (empty: same order)
+  Lines lines{};            // BCGSTAB_LINELET lines (nlines 0 otherwise)
   int* d_cell_old = nullptr;  // rn.cell_old on the device (state staging)
 };
 
@@ -183,6 +184,34 @@ static int upload_rows(jg_case* h, double* dev, const double* host, const std::v
   return JG_OK;
 }
 
+// the faces of each WALL zone, zone by zone, each zone in the caller's face order
+static std::vector<std::vector<int>> wall_zone_faces(const jg_mesh* mesh, const std::vector<int>& face_old) {
+  std::vector<std::vector<int>> zs;
+  for (int z = 0; z < mesh->nzones; z++)
+    if (mesh->zones[z].kind == JG_BC_WALL) {
+      std::vector<int> f;
+      for (int i = mesh->zones[z].ifa_f; i <= mesh->zones[z].ifa_l; i++) f.push_back(i);
+      if (!face_old.empty())
+        std::sort(f.begin(), f.end(), [&](int a, int b) { return face_old[a] < face_old[b]; });
+      zs.push_back(std::move(f));
+    }
+  return zs;
+}
+
+// the lines of two or more cells of initializeLinelet
+static void multi_cell_lines(const jg_mesh* mesh, const std::vector<int>& face_old, std::vector<int>& off,
+                             std::vector<int>& cv) {
+  std::vector<int> o, c;
+  build_lines(*mesh, wall_zone_faces(mesh, face_old), o, c);
+  off.assign(1, 0);
+  cv.clear();
+  for (size_t l = 0; l + 1 < o.size(); l++)
+    if (o[l + 1] - o[l] >= 2) {
+      cv.insert(cv.end(), c.begin() + o[l], c.begin() + o[l + 1]);
+      off.push_back((int)cv.size());
+    }
+}
+
 static Params make_params(const jg_params& q) {
   Params p;
   memset(&p, 0, sizeof(p));
@@ -219,10 +248,11 @@ static int check_params(const jg_params* q) {
   if (!q) return set_err(JG_ERR_ARG, "null params");
   if (q->flux < 0 || q->flux > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
   if (q->symm_bc < 0 || q->symm_bc > 2) return set_err(JG_ERR_ARG, "unsupported SYMM_BC %d", q->symm_bc);
-  if (q->lin_solver < 0 || q->lin_solver > 3) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
+  if (q->lin_solver < 0 || q->lin_solver > 4) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
   if (q->precision != JG_PREC_FP64 && q->precision != JG_PREC_MIXED)
     return set_err(JG_ERR_ARG, "unsupported precision %d", q->precision);
-  if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS))
+  if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS ||
+                                        q->lin_solver == JG_LS_BCGSTAB_LINELET))
     return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI or SGS sweeps");
   if (q->turb_model == JG_TURB_SA || q->turb_model == JG_TURB_SST) {
     if (q->nscal != (q->turb_model == JG_TURB_SA ? 1 : 2))
@@ -510,6 +540,19 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     launch_wall_distance(h->m, t, h->stream);
     CKL();
   }
+  if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
+    std::vector<int> off, cv;
+    multi_cell_lines(mesh, h->rn.face_old, off, cv);
+    Lines& L = h->lines;
+    L.nlines = (int)off.size() - 1;
+    const size_t nc = cv.size();
+    RC(upload(h, &L.off, off.data(), off.size()));
+    RC(upload(h, &L.cv, cv.data(), std::max<size_t>(nc, 1)));
+    RC(dmalloc(h, &L.inv, 25 * std::max<size_t>(nc, 1)));
+    RC(dmalloc(h, &L.low, 25 * std::max<size_t>(nc, 1)));
+    RC(dmalloc(h, &L.up, 25 * std::max<size_t>(nc, 1)));
+    RC(dmalloc(h, &L.v, 5 * std::max<size_t>(nc, 1)));
+  }
   double ctrl0[16] = {0};
   ctrl0[0] = q->cfl;
   CK(cudaMemcpyAsync(st.ctrl, ctrl0, sizeof(ctrl0), cudaMemcpyHostToDevice, h->stream));
@@ -556,7 +599,7 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
 // Device bytes a handle made by jg_create holds once its state is set: the
 // allocations of build() plus the state staging buffer, each rounded like
 // dmalloc_bytes rounds it.  CUDA-graph and event storage is not included.
-static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
+static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vector<int>& face_old) {
   const size_t N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b, nbs = mesh->nbocv_s;
   const size_t e = q->precision == JG_PREC_MIXED ? 4 : 8;
   const size_t bs = q->turb_model == JG_TURB_NONE ? 5 : 5 + q->nscal, b2 = bs * bs;
@@ -605,6 +648,12 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q) {
     for (size_t x : t) b += alloc_round(x);
     if (q->turb_model == JG_TURB_SST) b += 4 * alloc_round(N * d);
   }
+  if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
+    std::vector<int> off, cv;
+    multi_cell_lines(mesh, face_old, off, cv);
+    const size_t nc = std::max<size_t>(cv.size(), 1);
+    b += alloc_round(off.size() * i) + alloc_round(nc * i) + 3 * alloc_round(25 * nc * d) + alloc_round(5 * nc * d);
+  }
   return b;
 }
 
@@ -618,10 +667,10 @@ extern "C" int jg_case_footprint(const jg_mesh* mesh, const jg_params* params, d
     MeshOwned mo;
     Renumbering rn;
     RC(renumber_mesh(*mesh, params->renumber, mo, rn));
-    *bytes = (double)(footprint(&mo.m, params) + alloc_round((size_t)mesh->ncv * sizeof(int)));
+    *bytes = (double)(footprint(&mo.m, params, rn.face_old) + alloc_round((size_t)mesh->ncv * sizeof(int)));
     return JG_OK;
   }
-  *bytes = (double)footprint(mesh, params);
+  *bytes = (double)footprint(mesh, params, {});
   return JG_OK;
 }
 
@@ -715,7 +764,7 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   RC(check_params(params));
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "batches hold laminar / inviscid cases");
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
-  if (params->lin_solver == JG_LS_BCGSTAB)
+  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
   if (params->time_step_mode == JG_TS_CFL_MIN)
     return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
@@ -1000,7 +1049,8 @@ static size_t red_size(int N) { return (size_t)std::max(1024, grid_for(N, 256)) 
 
 // BiCGSTAB with the block-diagonal preconditioner, solveCvVectorR5Bcgstab
 // (UgpWithCv.cpp:2660-2876); operates on [5][N] vectors, phi in/out in d_tmp.
-static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, double zeroRel, int maxiter, int* iters) {
+static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, double zeroRel, int maxiter, int* iters,
+                   bool lines = false) {
   const int N = h->ncv;
   const long n5 = 5L * N;
   if (!h->d_tmp) {
@@ -1028,6 +1078,12 @@ static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, d
   };
   CK(cudaMemsetAsync(p, 0, n5 * sizeof(double), S));
   CK(cudaMemsetAsync(v, 0, n5 * sizeof(double), S));
+  // the preconditioner: block diagonal, or line-implicit (the lines' elimination once per solve)
+  if (lines) launch_line_factor(h->m, h->st, h->lines, S);
+  auto precond = [&](const double* x, double* y) {
+    if (lines) launch_line_precond(h->m, h->st, h->lines, x, y, S);
+    else launch_precond(h->m, h->st, x, y, S);
+  };
   double rho = 1.0, alpha = 1.0, omega = 1.0;
   launch_spmv(h->m, h->st, phi, res, S);
   launch_lin3(n5, res, 1.0, rhs, -1.0, res, 0.0, nullptr, S);
@@ -1043,14 +1099,14 @@ static int bcgstab(jg_case* h, double* phi, const double* rhs, double zeroAbs, d
     double beta = alpha * rho / rho_prime;
     // p = res - beta*(p - omega*v)
     launch_lin3(n5, p, 1.0, res, -beta, p, beta * omega, v, S);
-    launch_precond(h->m, h->st, p, phat, S);
+    precond(p, phat);
     launch_spmv(h->m, h->st, phat, v, S);
     double gamma;
     RC(dot(v, res0, gamma));
     if (fabs(gamma) < 1.0E-20) gamma = 1.0E-20;
     alpha = rho / gamma;
     launch_lin3(n5, s, 1.0, res, -alpha, v, 0.0, nullptr, S);
-    launch_precond(h->m, h->st, s, shat, S);
+    precond(s, shat);
     launch_spmv(h->m, h->st, shat, t, S);
     double st_, tt_;
     RC(dot(s, t, st_));
@@ -1087,7 +1143,8 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
   CKL();
   int it = 0;
   switch (h->hp.lin_solver) {
-    case JG_LS_BCGSTAB: {
+    case JG_LS_BCGSTAB:
+    case JG_LS_BCGSTAB_LINELET: {
       if (!h->d_tmp) {
         RC(dmalloc(h, &h->d_tmp, 8 * 5 * (size_t)N));
         RC(dmalloc(h, &h->d_red, red_size(N)));
@@ -1099,7 +1156,7 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
       CK(cudaMemcpyAsync(phi, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
       to_soa(rhs, soa, N, h->rn.cell_old);
       CK(cudaMemcpyAsync(b, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-      RC(bcgstab(h, phi, b, zeroAbs, zeroRel, maxIter, &it));
+      RC(bcgstab(h, phi, b, zeroAbs, zeroRel, maxIter, &it, h->hp.lin_solver == JG_LS_BCGSTAB_LINELET));
       launch_dq_from_x(h->m, h->p, h->st, phi, h->stream);
     } break;
     case JG_LS_LUSGS:
@@ -1175,20 +1232,14 @@ static int enqueue_step(jg_case* h, int for_graph) {
     launch_dq_from_x(h->m, h->p, h->st, h->st.x0, S);
   } else {
     if (for_graph) return set_err(JG_ERR_ARG, "BCGSTAB is not captured");
-    // host-driven BiCGSTAB on the assembled system, zero initial guess
+    // host-driven BiCGSTAB on the assembled system, zero initial guess; the rhs ([N][5] in st.b) as [5][N]
     const long n5 = 5L * h->ncv;
     double* phi = (double*)h->st.x0;
     double* b = (double*)h->st.x1;
     CK(cudaMemsetAsync(phi, 0, n5 * sizeof(double), S));
-    // b is [N][5] in st.b; the solver wants [5][N]: transpose via dq_from_x's inverse on the host side is costly,
-    // so reuse the device: copy b into x1 as [5][N]
-    std::vector<double> tmp(n5), soa;
-    CK(cudaMemcpyAsync(tmp.data(), h->st.b, n5 * sizeof(double), cudaMemcpyDeviceToHost, S));
-    CK(cudaStreamSynchronize(S));
-    to_soa(tmp.data(), soa, h->ncv, {});  // already in the handle's order
-    CK(cudaMemcpyAsync(b, soa.data(), n5 * sizeof(double), cudaMemcpyHostToDevice, S));
+    launch_aos_to_soa5(h->ncv, h->st.b, b, S);
     int it;
-    RC(bcgstab(h, phi, b, h->hp.ls_abs, h->hp.ls_rel, h->hp.ls_max_iter, &it));
+    RC(bcgstab(h, phi, b, h->hp.ls_abs, h->hp.ls_rel, h->hp.ls_max_iter, &it, solver == JG_LS_BCGSTAB_LINELET));
     launch_dq_from_x(h->m, h->p, h->st, phi, S);
   }
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
@@ -1249,7 +1300,7 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   CK(cudaStreamSynchronize(h->stream));
   ctrl[4] = ctrl[1];
   CK(cudaMemcpyAsync(h->st.ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
-  bool use_graph = h->hp.lin_solver != JG_LS_BCGSTAB;
+  bool use_graph = h->hp.lin_solver != JG_LS_BCGSTAB && h->hp.lin_solver != JG_LS_BCGSTAB_LINELET;
   if (use_graph) RC(ensure_graph(h));
   for (int k = 0; k < nsteps; k++) {
     if (use_graph) CK(cudaGraphLaunch(h->graph, h->stream));
@@ -1308,7 +1359,8 @@ int jg_batch_step(jg_case_t* h, int nsteps, double* resid) {
 // enqueue nsteps without synchronising (device-resident throughput runs)
 int jg_step_async(jg_case_t* h, int nsteps) {
   if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
-  if (h->hp.lin_solver == JG_LS_BCGSTAB) return set_err(JG_ERR_ARG, "jg_step_async needs a captured solver");
+  if (h->hp.lin_solver == JG_LS_BCGSTAB || h->hp.lin_solver == JG_LS_BCGSTAB_LINELET)
+    return set_err(JG_ERR_ARG, "jg_step_async needs a captured solver");
   if (!h->primed) RC(prime(h));
   RC(ensure_graph(h));
   for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(h->graph, h->stream));
@@ -1452,7 +1504,7 @@ int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** ou
   if (!mesh || !out) return set_err(JG_ERR_ARG, "null argument");
   *out = nullptr;
   RC(check_params(params));
-  if (params->lin_solver == JG_LS_BCGSTAB)
+  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "served cases are laminar / inviscid");
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "served cases keep their own order");
@@ -1540,7 +1592,8 @@ extern "C" int jg_get_profile(jg_case_t* h, double* ms) {
 // kernels launched by one captured step
 extern "C" int jg_step_kernel_count(jg_case_t* h, int* n) {
   if (!h || !n) return set_err(JG_ERR_ARG, "null argument");
-  if (h->hp.lin_solver == JG_LS_BCGSTAB) return set_err(JG_ERR_ARG, "BCGSTAB steps are not captured");
+  if (h->hp.lin_solver == JG_LS_BCGSTAB || h->hp.lin_solver == JG_LS_BCGSTAB_LINELET)
+    return set_err(JG_ERR_ARG, "BCGSTAB steps are not captured");
   if (!h->primed) RC(prime(h));
   RC(ensure_graph(h));
   *n = (int)h->graph_kernels;

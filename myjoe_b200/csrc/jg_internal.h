@@ -191,6 +191,30 @@ void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t
 }  // namespace jg
 
 namespace jg {
+// Lines of the BCGSTAB_LINELET preconditioner (jg_linelet.cu): the lines of
+// two or more cells, cells in line order; per line cell the inverse of its
+// eliminated diagonal block, the multiplier A(c_i, c_{i-1}) inv_{i-1} and the
+// upper block A(c_{i-1}, c_i) (row-major 5x5), and the forward-substitution
+// vector.
+struct Lines {
+  int nlines;
+  const int* off;  // [nlines+1]
+  const int* cv;   // [off[nlines]]
+  double* inv;     // [off[nlines]][25]
+  double* low;     // [off[nlines]][25] (position 0 of a line unused)
+  double* up;      // [off[nlines]][25] (position 0 of a line unused)
+  double* v;       // [off[nlines]][5]
+};
+// initializeLinelet on a mesh: wall_zones holds the faces of each WALL zone in zone order
+int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zones, std::vector<int>& off,
+                std::vector<int>& cv);
+void launch_line_factor(const Mesh& m, const State& st, const Lines& L, cudaStream_t s);
+// y = the line-implicit preconditioner applied to x ([5][N] both)
+void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const double* x, double* y,
+                         cudaStream_t s);
+// [N][5] -> [5][N]
+void launch_aos_to_soa5(int n, const double* aos, double* soa, cudaStream_t s);
+
 // A mesh in jg_mesh's layout whose arrays the struct owns (concatenated
 // batches, renumbered cases); bind() points m at the vectors.
 struct MeshOwned {

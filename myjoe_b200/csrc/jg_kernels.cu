@@ -1141,9 +1141,18 @@ __global__ void k_unpack_state(int n, const double* q, double* io, const int* pe
   io[4 * n + r] = q[5 * c + 4];
 }
 
+__global__ void k_aos_to_soa5(int n, const double* aos, double* soa) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int i = 0; i < 5; i++) soa[(size_t)i * n + c] = aos[5 * (size_t)c + i];
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+void launch_aos_to_soa5(int n, const double* aos, double* soa, cudaStream_t s) {
+  k_aos_to_soa5<<<grid_for(n, 256), 256, 0, s>>>(n, aos, soa);
+}
 void launch_pack_state(int n, const double* io, double* q, const int* perm, cudaStream_t s) {
   k_pack_state<<<grid_for(n, 256), 256, 0, s>>>(n, io, q, perm);
 }

@@ -1,0 +1,255 @@
+// jg_linelet.cu -- the line-implicit preconditioner of BCGSTAB_LINELET.
+//
+// initializeLinelet (src/joe/JoeWithModels.cpp:7471-7559) grows, from each
+// cell on a WALL face, a line of cells in the direction of strong coupling;
+// solveCvVectorR5BcgstabLine (src/common/UgpWithCv.cpp:3627-3992) is
+// BiCGSTAB whose preconditioner solves the block-tridiagonal system of each
+// line exactly (block Thomas elimination) and the block diagonal elsewhere.
+//
+// Here the lines are built once per handle on the host.  On the device the
+// elimination is split in two: k_line_factor runs once per linear solve (the
+// matrix does not change inside BiCGSTAB) and keeps, per line cell, the
+// inverse of the eliminated diagonal block, the multiplier
+// A(c_i, c_{i-1}) inv_{i-1} and the upper block A(c_{i-1}, c_i); k_line_apply
+// then does the forward and backward substitutions for one right-hand side
+// (twice per BiCGSTAB iteration).  The reference recomputes the elimination
+// inside every application; the factors are the same numbers.  One warp per
+// line: the lines are independent, and inside a line the work is a chain of
+// 5x5 block operations, so the warp's lanes hold the 25 entries (factor) or
+// the 5 rows (substitutions) of one block step.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "jg_internal.h"
+
+namespace jg {
+
+namespace {
+
+// findFace (JoeWithModels.cpp:7572-7587): the first face of a's list that b also has
+int find_face(const jg_mesh& m, int a, int b) {
+  if (a == b) return -1;
+  for (int i = m.faocv_i[a]; i < m.faocv_i[a + 1]; i++)
+    for (int j = m.faocv_i[b]; j < m.faocv_i[b + 1]; j++)
+      if (m.faocv_v[i] == m.faocv_v[j]) return m.faocv_v[i];
+  return -1;
+}
+
+double coupling(const jg_mesh& m, int a, int b) {
+  int f = find_face(m, a, b);
+  const double* n = &m.fa_normal[3 * f];
+  double area = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  return 0.5 * area * ((1.0 / m.cv_volume[a]) + (1.0 / m.cv_volume[b]));
+}
+
+}  // namespace
+
+int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zones, std::vector<int>& off,
+                std::vector<int>& cv) {
+  const int N = m.ncv;
+  std::vector<char> free_cv(N, 1);
+  // each WALL zone replaces the sources of the one before it; all of their cells leave the pool
+  std::vector<int> src;
+  for (const auto& z : wall_zones) {
+    src.clear();
+    for (int f : z) {
+      src.push_back(m.cvofa[2 * f]);
+      free_cv[m.cvofa[2 * f]] = 0;
+    }
+  }
+  off.assign(1, 0);
+  cv.clear();
+  for (int s : src) {
+    const size_t first = cv.size();
+    cv.push_back(s);
+    for (;;) {
+      const int icv = cv.back();
+      double wmax = 0.0;
+      for (int k = m.nbocv_i[icv] + 1; k < m.nbocv_i[icv + 1]; k++)
+        wmax = std::max(wmax, coupling(m, icv, m.nbocv_v[k]));
+      // the one free neighbour (not the cell the line came from) with more than half the largest coupling
+      int next = -1, count = 0;
+      const int prev = cv.size() - first >= 2 ? cv[cv.size() - 2] : -1;
+      for (int k = m.nbocv_i[icv] + 1; k < m.nbocv_i[icv + 1]; k++) {
+        const int nb = m.nbocv_v[k];
+        if (free_cv[nb] && coupling(m, icv, nb) / wmax > 0.5 && nb != prev) {
+          next = nb;
+          count++;
+        }
+      }
+      if (count != 1) break;  // no candidate, or an isotropic region
+      cv.push_back(next);
+      free_cv[next] = 0;
+    }
+    off.push_back((int)cv.size());
+  }
+  return JG_OK;
+}
+
+namespace {
+
+constexpr int LW = 4;  // warps (lines) per block
+
+// ludeco (UgpWithCv.cpp:2489-2516) on a row-major 5x5 block
+__device__ void ludeco5(double* A) {
+#pragma unroll
+  for (int jc = 1; jc < 5; jc++) A[jc] /= A[0];
+#pragma unroll
+  for (int jrjc = 1; jrjc < 5; jrjc++) {
+#pragma unroll
+    for (int jr = jrjc; jr < 5; jr++) {
+      double sum = A[5 * jr + jrjc];
+#pragma unroll
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jr + jm] * A[5 * jm + jrjc];
+      A[5 * jr + jrjc] = sum;
+    }
+    if (jrjc == 4) break;
+#pragma unroll
+    for (int jc = jrjc + 1; jc < 5; jc++) {
+      double sum = A[5 * jrjc + jc];
+#pragma unroll
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jrjc + jm] * A[5 * jm + jc];
+      A[5 * jrjc + jc] = sum / A[5 * jrjc + jrjc];
+    }
+  }
+}
+
+// column `col` of the inverse from the ludeco factors, as luinv (UgpWithCv.cpp:2542-2577)
+__device__ void luinv_col(const double* A, int col, double* c) {
+#pragma unroll
+  for (int i = 0; i < 5; i++) c[i] = (i == col) ? 1.0 : 0.0;
+  c[0] = c[0] / A[0];
+#pragma unroll
+  for (int jr = 1; jr < 5; jr++) {
+    double sum = c[jr];
+#pragma unroll
+    for (int jm = 0; jm < jr; jm++) sum -= A[5 * jr + jm] * c[jm];
+    c[jr] = sum / A[5 * jr + jr];
+  }
+#pragma unroll
+  for (int jr = 3; jr >= 0; jr--) {
+    double sum = c[jr];
+#pragma unroll
+    for (int jm = 4; jm > jr; jm--) sum -= A[5 * jr + jm] * c[jm];
+    c[jr] = sum;
+  }
+}
+
+// entry e of the matrix block A(row, col): the ELL columns of `row` whose neighbour is `col`
+__device__ double ell_block(const Mesh& m, const double* O, int row, int col, int e) {
+  const int s = row / SLICE, lane = row % SLICE;
+  double v = 0.0;
+  for (int j = m.ell_off[s]; j < m.ell_off[s + 1]; j++)
+    if (m.ell_nb[(size_t)j * SLICE + lane] == col) v += O[((size_t)j * 25 + e) * SLICE + lane];
+  return v;
+}
+
+__global__ void __launch_bounds__(32 * LW) k_line_factor(Mesh m, State st, Lines L) {
+  __shared__ double sh[LW][5][25];
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int line = blockIdx.x * LW + w;
+  if (line >= L.nlines) return;
+  double *b = sh[w][0], *inv = sh[w][1], *lo = sh[w][2], *up = sh[w][3], *mh = sh[w][4];
+  const int p0 = L.off[line], n = L.off[line + 1] - p0;
+  const int N = m.ncv;
+  const double* D = (const double*)st.D;
+  const double* O = (const double*)st.O;
+  const int e = lane < 25 ? lane : 24, r = e / 5, k = e % 5;
+  if (lane < 25) b[e] = D[(size_t)e * N + L.cv[p0]];
+  __syncwarp();
+  for (int i = 1;; i++) {
+    // inverse of the eliminated diagonal block of position i-1
+    if (lane < 5) {
+      double A[25], c[5];
+#pragma unroll
+      for (int q = 0; q < 25; q++) A[q] = b[q];
+      ludeco5(A);
+      luinv_col(A, lane, c);
+#pragma unroll
+      for (int q = 0; q < 5; q++) inv[5 * q + lane] = c[q];
+    }
+    __syncwarp();
+    if (lane < 25) L.inv[(size_t)(p0 + i - 1) * 25 + e] = inv[e];
+    if (i == n) break;
+    const int cp = L.cv[p0 + i - 1], c = L.cv[p0 + i];
+    if (lane < 25) {
+      lo[e] = ell_block(m, O, c, cp, e);
+      up[e] = ell_block(m, O, cp, c, e);
+      L.up[(size_t)(p0 + i) * 25 + e] = up[e];
+    }
+    __syncwarp();
+    // mhat = A(c, cp) inv (getMultMatrix order: sums from 0.0 over q)
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s += lo[5 * r + q] * inv[5 * q + k];
+    if (lane < 25) {
+      mh[e] = s;
+      L.low[(size_t)(p0 + i) * 25 + e] = s;
+    }
+    __syncwarp();
+    // next diagonal: A(c, c) - mhat A(cp, c)
+    double a0 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) a0 += mh[5 * r + q] * up[5 * q + k];
+    const double bn = D[(size_t)e * N + c] - a0;
+    __syncwarp();
+    if (lane < 25) b[e] = bn;
+    __syncwarp();
+  }
+}
+
+// y (cells of the lines) = the block-tridiagonal solve of x along each line; x, y are [5][N]
+__global__ void __launch_bounds__(32 * LW) k_line_apply(Mesh m, Lines L, const double* x, double* y) {
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int line = blockIdx.x * LW + w;
+  if (line >= L.nlines) return;
+  const int p0 = L.off[line], n = L.off[line + 1] - p0;
+  const size_t N = m.ncv;
+  const int r = lane % 5;
+  const bool row = lane < 5;
+  // forward: v_0 = x_0, v_i = x_i - mhat_i v_{i-1}
+  double v = x[r * N + L.cv[p0]];
+  if (row) L.v[(size_t)p0 * 5 + r] = v;
+  for (int i = 1; i < n; i++) {
+    const double* Mi = &L.low[(size_t)(p0 + i) * 25 + 5 * r];
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s += Mi[q] * __shfl_sync(0xffffffffu, v, q);
+    v = x[r * N + L.cv[p0 + i]] - s;
+    if (row) L.v[(size_t)(p0 + i) * 5 + r] = v;
+  }
+  // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - A(c_i, c_{i+1}) y_{i+1})
+  const double* I = &L.inv[(size_t)(p0 + n - 1) * 25 + 5 * r];
+  double yv = 0.0;
+#pragma unroll
+  for (int q = 0; q < 5; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
+  if (row) y[r * N + L.cv[p0 + n - 1]] = yv;
+  for (int i = n - 2; i >= 0; i--) {
+    const double* U = &L.up[(size_t)(p0 + i + 1) * 25 + 5 * r];
+    double s2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s2 += U[q] * __shfl_sync(0xffffffffu, yv, q);
+    const double a1 = L.v[(size_t)(p0 + i) * 5 + r] - s2;
+    const double* Ii = &L.inv[(size_t)(p0 + i) * 25 + 5 * r];
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s += Ii[q] * __shfl_sync(0xffffffffu, a1, q);
+    yv = s;
+    if (row) y[r * N + L.cv[p0 + i]] = yv;
+  }
+}
+
+}  // namespace
+
+void launch_line_factor(const Mesh& m, const State& st, const Lines& L, cudaStream_t s) {
+  if (L.nlines) k_line_factor<<<(L.nlines + LW - 1) / LW, 32 * LW, 0, s>>>(m, st, L);
+}
+
+void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const double* x, double* y,
+                         cudaStream_t s) {
+  launch_precond(m, st, x, y, s);  // the block diagonal everywhere, then the lines overwrite their cells
+  if (L.nlines) k_line_apply<<<(L.nlines + LW - 1) / LW, 32 * LW, 0, s>>>(m, L, x, y);
+}
+
+}  // namespace jg

@@ -32,6 +32,9 @@ struct jo_case {
   int dt_fixed_done;
   double dt_fixed;
   double *kine;     /* turbulent kinetic energy per cell (SST), NULL otherwise */
+  int nlines;       /* linelets (initializeLinelet): cells line_cv[line_off[l] .. line_off[l+1]) */
+  int *line_off, *line_cv;
+  unsigned char *linelet;  /* [N] the reference's Linelet flag: the cell is on a line of >= 2 cells */
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -78,6 +81,9 @@ void jo_destroy(jo_case *h) {
                     h->lamOcp_fa, h->mut_fa, h->grad_u, h->grad_rho, h->grad_p, h->grad_h, h->alpha_rho,
                     h->local_dt, h->fscale};
   for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); i++) free(arrs[i]);
+  free(h->line_off);
+  free(h->line_cv);
+  free(h->linelet);
   free(h);
 }
 
@@ -1321,9 +1327,195 @@ static void matvec(jo_case *h, double *res, const double *A, const double *x) {
   }
 }
 
+/* findFace (JoeWithModels.cpp:7572-7587): the first face of cell a's list that cell b also has */
+static int find_face(const jg_mesh *m, int a, int b) {
+  if (a == b) return -1;
+  for (int i = m->faocv_i[a]; i < m->faocv_i[a + 1]; i++)
+    for (int j = m->faocv_i[b]; j < m->faocv_i[b + 1]; j++)
+      if (m->faocv_v[i] == m->faocv_v[j]) return m->faocv_v[i];
+  return -1;
+}
+
+/* initializeLinelet (JoeWithModels.cpp:7471-7559).  Sources are the cells of
+ * the WALL faces; as in the reference, each WALL zone replaces the sources of
+ * the previous one (only the last WALL zone starts lines) while every WALL
+ * zone's cells are taken out of later lines.  From each source a line grows
+ * to the one unused neighbour (not the cell it came from) whose weight
+ * 0.5 |A_f| (1/V_cell + 1/V_nb) exceeds half the cell's largest neighbour
+ * weight; two or more candidates (an isotropic region) or none end it. */
+void jo_build_linelets(jo_case *h) {
+  const jg_mesh *m = &h->m;
+  const int N = h->ncv;
+  unsigned char *check = (unsigned char *)malloc(N ? N : 1);
+  memset(check, 1, N);
+  int nsrc = 0, *src = NULL;
+  for (int z = 0; z < m->nzones; z++) {
+    if (m->zones[z].kind != JG_BC_WALL) continue;
+    free(src);
+    nsrc = m->zones[z].ifa_l - m->zones[z].ifa_f + 1;
+    src = (int *)malloc(sizeof(int) * (nsrc ? nsrc : 1));
+    for (int f = m->zones[z].ifa_f, i = 0; f <= m->zones[z].ifa_l; f++, i++) {
+      src[i] = m->cvofa[2 * f];
+      check[src[i]] = 0;
+    }
+  }
+  int cap = nsrc + 16, len = 0;
+  int *cv = (int *)malloc(sizeof(int) * cap);
+  int *off = (int *)malloc(sizeof(int) * (nsrc + 1));
+  off[0] = 0;
+  for (int l = 0; l < nsrc; l++) {
+    if (len + 1 > cap) { cap *= 2; cv = (int *)realloc(cv, sizeof(int) * cap); }
+    cv[len++] = src[l];
+    int index_cv = 0, add;
+    do {
+      int icv = cv[off[l] + index_cv];
+      double max_weight = 0.0, nv[3];
+      for (int k = m->nbocv_i[icv] + 1; k < m->nbocv_i[icv + 1]; k++) {
+        int ino = m->nbocv_v[k];
+        int f = find_face(m, icv, ino);
+        double area = norm3(nv, &m->fa_normal[3 * f]);
+        double w = 0.5 * area * ((1.0 / m->cv_volume[icv]) + (1.0 / m->cv_volume[ino]));
+        max_weight = dmax(max_weight, w);
+      }
+      add = 0;
+      int counter = 0, next_cv = -1;
+      for (int k = m->nbocv_i[icv] + 1; k < m->nbocv_i[icv + 1]; k++) {
+        int ino = m->nbocv_v[k];
+        int f = find_face(m, icv, ino);
+        double area = norm3(nv, &m->fa_normal[3 * f]);
+        double w = 0.5 * area * ((1.0 / m->cv_volume[icv]) + (1.0 / m->cv_volume[ino]));
+        if (check[ino] && w / max_weight > 0.5 && (index_cv == 0 || ino != cv[off[l] + index_cv - 1])) {
+          add = 1;
+          next_cv = ino;
+          counter++;
+        }
+      }
+      if (counter > 1) add = 0;
+      if (add) {
+        if (len + 1 > cap) { cap *= 2; cv = (int *)realloc(cv, sizeof(int) * cap); }
+        cv[len++] = next_cv;
+        check[next_cv] = 0;
+        index_cv++;
+      }
+    } while (add);
+    off[l + 1] = len;
+  }
+  free(h->line_off); free(h->line_cv); free(h->linelet);
+  h->nlines = nsrc;
+  h->line_off = off;
+  h->line_cv = cv;
+  h->linelet = (unsigned char *)calloc(N ? N : 1, 1);
+  for (int l = 0; l < nsrc; l++)
+    if (off[l + 1] - off[l] >= 2)
+      for (int i = off[l]; i < off[l + 1]; i++) h->linelet[cv[i]] = 1;
+  free(src);
+  free(check);
+}
+
+int jo_linelets(jo_case *h, int *off, int *cv) {
+  if (!h->line_off) jo_build_linelets(h);
+  if (off) memcpy(off, h->line_off, sizeof(int) * (h->nlines + 1));
+  if (cv) memcpy(cv, h->line_cv, sizeof(int) * h->line_off[h->nlines]);
+  return h->nlines;
+}
+
+/* luinv (UgpWithCv.cpp:2542-2577): the inverse from the ludeco factors, column by column */
+static void luinv(double (*A)[5], double Ainv[5][5]) {
+  for (int i = 0; i < 5; i++) {
+    double c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    c[i] = 1.0;
+    c[0] = c[0] / A[0][0];
+    for (int jr = 1; jr < 5; jr++) {
+      double sum = c[jr];
+      for (int jm = 0; jm <= jr - 1; jm++) sum -= A[jr][jm] * c[jm];
+      c[jr] = sum / A[jr][jr];
+    }
+    for (int jrjr = 1; jrjr < 5; jrjr++) {
+      int jr = 4 - jrjr;
+      double sum = c[jr];
+      for (int jmjm = jr + 1; jmjm < 5; jmjm++) {
+        int jm = 4 - jmjm + jr + 1;
+        sum -= A[jr][jm] * c[jm];
+      }
+      c[jr] = sum;
+    }
+    for (int r = 0; r < 5; r++) Ainv[r][i] = c[r];
+  }
+}
+
+/* getMultMatrix (UgpWithCv.cpp:3994-4026): c = a b, sums from 0.0 in k order */
+static void mat_mul(double c[5][5], const double *a, const double b[5][5]) {
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) {
+      c[i][j] = 0.0;
+      for (int k = 0; k < 5; k++) c[i][j] += a[5 * i + k] * b[k][j];
+    }
+}
+static void mat_vec(double c[5], const double *a, const double *b) {
+  for (int i = 0; i < 5; i++) {
+    c[i] = 0.0;
+    for (int j = 0; j < 5; j++) c[i] += a[5 * i + j] * b[j];
+  }
+}
+
+/* getImplDependencyIndex (UgpWithCv.h:745-755): CSR entry of column b in row a */
+static int csr_entry(const jg_mesh *m, int a, int b) {
+  int k = m->nbocv_i[a];
+  while (m->nbocv_v[++k] != b);
+  return k;
+}
+
+/* the LINE IMPLICIT preconditioner of solveCvVectorR5BcgstabLine
+ * (UgpWithCv.cpp:3729-3810): the block diagonal (LU) off the lines, a
+ * block-tridiagonal Thomas solve along each line (every line, single cells
+ * included, overwrites its cells) */
+static void line_precond(jo_case *h, const double *A, const double *LU, const double *pv, double *phat,
+                         double (*bhat)[5][5], double (*invbhat)[5][5], double (*vhat)[5]) {
+  const jg_mesh *m = &h->m;
+  for (int c = 0; c < h->ncv; c++)
+    if (!h->linelet[c]) {
+      memcpy(&phat[5 * c], &pv[5 * c], 5 * sizeof(double));
+      lusolv((double(*)[5]) & LU[25 * c], &phat[5 * c], 5);
+    }
+  double LUb[5][5], mhat[5][5], aux0[5][5], aux1[5], aux2[5];
+  for (int l = 0; l < h->nlines; l++) {
+    const int *cv = &h->line_cv[h->line_off[l]];
+    int n = h->line_off[l + 1] - h->line_off[l];
+    for (int i = 0; i < 5; i++) {
+      vhat[0][i] = pv[5 * cv[0] + i];
+      for (int j = 0; j < 5; j++) bhat[0][i][j] = A[25 * m->nbocv_i[cv[0]] + 5 * i + j];
+    }
+    for (int i = 1; i < n; i++) {
+      int noc01 = csr_entry(m, cv[i - 1], cv[i]), noc11 = m->nbocv_i[cv[i]], noc10 = csr_entry(m, cv[i], cv[i - 1]);
+      memcpy(LUb, bhat[i - 1], sizeof(LUb));
+      ludeco(LUb, 5);
+      luinv(LUb, invbhat[i - 1]);
+      mat_mul(mhat, &A[25 * noc10], invbhat[i - 1]);
+      double a01[5][5];
+      memcpy(a01, &A[25 * noc01], sizeof(a01));
+      mat_mul(aux0, &mhat[0][0], a01);
+      for (int r = 0; r < 5; r++)
+        for (int c = 0; c < 5; c++) bhat[i][r][c] = A[25 * noc11 + 5 * r + c] - aux0[r][c];
+      mat_vec(aux1, &mhat[0][0], vhat[i - 1]);
+      for (int r = 0; r < 5; r++) vhat[i][r] = pv[5 * cv[i] + r] - aux1[r];
+    }
+    memcpy(LUb, bhat[n - 1], sizeof(LUb));
+    ludeco(LUb, 5);
+    luinv(LUb, invbhat[n - 1]);
+    mat_vec(&phat[5 * cv[n - 1]], &invbhat[n - 1][0][0], vhat[n - 1]);
+    for (int i = n - 2; i >= 0; i--) {
+      int noc01 = csr_entry(m, cv[i], cv[i + 1]);
+      mat_vec(aux2, &A[25 * noc01], &phat[5 * cv[i + 1]]);
+      for (int r = 0; r < 5; r++) aux1[r] = vhat[i][r] - aux2[r];
+      mat_vec(&phat[5 * cv[i]], &invbhat[i][0][0], aux1);
+    }
+  }
+}
+
 static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double *rhs, double zeroAbs, double zeroRel,
-                         int maxiter) {
-  /* solveCvVectorR5Bcgstab, UgpWithCv.cpp:2660-2876 */
+                         int maxiter, int line) {
+  /* solveCvVectorR5Bcgstab, UgpWithCv.cpp:2660-2876; with `line` its
+   * line-implicit twin solveCvVectorR5BcgstabLine, UgpWithCv.cpp:3627-3992 */
   int n = h->ncv;
   const jg_mesh *m = &h->m;
   double *res = dalloc(5 * n), *res0 = dalloc(5 * n), *pv = dalloc(5 * n), *v = dalloc(5 * n), *t = dalloc(5 * n),
@@ -1332,6 +1524,14 @@ static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double 
     memcpy(&LU[25 * c], &A[25 * m->nbocv_i[c]], 25 * sizeof(double));
     ludeco((double(*)[5]) & LU[25 * c], 5);
   }
+  int lmax = 1;
+  if (line) {
+    if (!h->line_off) jo_build_linelets(h);
+    for (int l = 0; l < h->nlines; l++) lmax = lmax > h->line_off[l + 1] - h->line_off[l] ? lmax : h->line_off[l + 1] - h->line_off[l];
+  }
+  double(*bhat)[5][5] = (double(*)[5][5])dalloc(25 * (size_t)lmax);
+  double(*invbhat)[5][5] = (double(*)[5][5])dalloc(25 * (size_t)lmax);
+  double(*vhat)[5] = (double(*)[5])dalloc(5 * (size_t)lmax);
   double rho = 1.0, alpha = 1.0, omega = 1.0;
   matvec(h, res, A, phi);
   for (int k = 0; k < 5 * n; k++) { res[k] = rhs[k] - res[k]; res0[k] = res[k]; }
@@ -1353,9 +1553,13 @@ static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double 
     if (fabs(rho_prime) < 1.0E-20) rho_prime = 1.0E-20;
     double beta = alpha * rho / rho_prime;
     for (int k = 0; k < 5 * n; k++) pv[k] = res[k] - beta * (pv[k] - omega * v[k]);
-    for (int c = 0; c < n; c++) {
-      memcpy(&phat[5 * c], &pv[5 * c], 5 * sizeof(double));
-      lusolv((double(*)[5]) & LU[25 * c], &phat[5 * c], 5);
+    if (line) {
+      line_precond(h, A, LU, pv, phat, bhat, invbhat, vhat);
+    } else {
+      for (int c = 0; c < n; c++) {
+        memcpy(&phat[5 * c], &pv[5 * c], 5 * sizeof(double));
+        lusolv((double(*)[5]) & LU[25 * c], &phat[5 * c], 5);
+      }
     }
     matvec(h, v, A, phat);
     double gamma = 0.0;
@@ -1363,9 +1567,13 @@ static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double 
     if (fabs(gamma) < 1.0E-20) gamma = 1.0E-20;
     alpha = rho / gamma;
     for (int k = 0; k < 5 * n; k++) s[k] = res[k] - alpha * v[k];
-    for (int c = 0; c < n; c++) {
-      memcpy(&shat[5 * c], &s[5 * c], 5 * sizeof(double));
-      lusolv((double(*)[5]) & LU[25 * c], &shat[5 * c], 5);
+    if (line) {
+      line_precond(h, A, LU, s, shat, bhat, invbhat, vhat);
+    } else {
+      for (int c = 0; c < n; c++) {
+        memcpy(&shat[5 * c], &s[5 * c], 5 * sizeof(double));
+        lusolv((double(*)[5]) & LU[25 * c], &shat[5 * c], 5);
+      }
     }
     matvec(h, t, A, shat);
     double b0 = 0.0, b1 = 0.0;
@@ -1385,6 +1593,7 @@ static int solve_bcgstab(jo_case *h, double *phi, const double *A, const double 
     else if (iter > maxiter) done = 2;
   }
   free(res); free(res0); free(pv); free(v); free(t); free(s); free(phat); free(shat); free(LU);
+  free(bhat); free(invbhat); free(vhat);
   return iter;
 }
 
@@ -1505,7 +1714,8 @@ static int solve_sgs(jo_case *h, double *phi, const double *A, const double *rhs
 int jo_solve(jo_case *h, double *dq, const double *A, const double *rhs, double zeroAbs, double zeroRel, int maxIter,
              int solver) {
   switch (solver) {
-    case JG_LS_BCGSTAB: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter);
+    case JG_LS_BCGSTAB: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, 0);
+    case JG_LS_BCGSTAB_LINELET: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, 1);
     case JG_LS_LUSGS: return solve_lusgs(h, dq, A, rhs);
     case JG_LS_JACOBI: return solve_jacobi(h, dq, A, rhs, maxIter);
     case JG_LS_SGS: return solve_sgs(h, dq, A, rhs, maxIter);

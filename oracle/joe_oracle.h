@@ -30,6 +30,9 @@ int jo_step(jo_case *h, int nsteps, double *resid);
  * "h_bfa","gam_bfa","RoM_bfa","mul_fa","lamOcp_fa","mut_fa","grad_u","grad_rho","grad_p",
  * "grad_enthalpy","alpha_rho","local_dt" */
 double *jo_array(jo_case *h, const char *name);
+/* initializeLinelet's lines: off[nlines+1], cv[off[nlines]]; returns nlines (NULL arrays: count only) */
+int jo_linelets(jo_case *h, int *off, int *cv);
+void jo_build_linelets(jo_case *h);
 double jo_cfl(jo_case *h);
 int jo_step_count(jo_case *h);
 

@@ -59,6 +59,8 @@ def lib():
         L.jo_sa_array.argtypes = [P, C.c_char_p]
         L.jo_sa_array.restype = D
         L.jo_sa_release.argtypes = [P]
+        L.jo_linelets.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.jo_linelets.restype = C.c_int
         _lib = L
     return _lib
 
@@ -124,6 +126,15 @@ class Oracle:
         rhs = np.ascontiguousarray(rhs, np.float64)
         it = lib().jo_solve(self.h, dptr(dq), dptr(A), dptr(rhs), zero_abs, zero_rel, max_iter, solver)
         return dq, it
+
+    def linelets(self):
+        """initializeLinelet's lines: (off[nlines+1], cells)"""
+        n = lib().jo_linelets(self.h, None, None)
+        off = np.zeros(n + 1, np.int32)
+        lib().jo_linelets(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), None)
+        cv = np.zeros(max(int(off[-1]), 1), np.int32)
+        lib().jo_linelets(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), cv.ctypes.data_as(C.POINTER(C.c_int)))
+        return off, cv[:off[-1]]
 
     def step(self, nsteps=1):
         r = np.zeros(5)

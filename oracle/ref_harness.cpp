@@ -100,11 +100,30 @@ public:
     }
   }
 
+  bool lines = false;
+
+  // JoeWithModels::run's preamble (JoeWithModels.cpp:20-31), up to the time integration
   void setup() {
     this->initializeFromRestartFile(this->getStringParam("RESTART"));
     this->initialHook();
     this->initialHookScalarRansTurbModel();
     this->initialHookScalarRansCombModel();
+    if (this->getStringParam("LINEAR_SOLVER_NS") == "BCGSTAB_LINELET") {
+      this->initializeLinelet();
+      lines = true;
+    }
+  }
+
+  // the lines initializeLinelet built: line_off[nSources+1], line_cv (cells of the lines in order)
+  void dumpLinelets() {
+    if (!lines) return;
+    std::vector<int> off(1, 0), cv;
+    for (int l = 0; l < this->nSources; l++) {
+      for (size_t i = 0; i < this->linelet_cv[l].size(); i++) cv.push_back(this->linelet_cv[l][i]);
+      off.push_back((int)cv.size());
+    }
+    DUMPI("line_off", off.data(), off.size());
+    DUMPI("line_cv", cv.data(), cv.size());
   }
 
   void writeMeta() {
@@ -139,6 +158,7 @@ public:
     DUMPD("x_fa", this->x_fa, 3 * nfa);
     DUMPD("fa_normal", this->fa_normal, 3 * nfa);
     DUMPD("cv_volume", this->cv_volume, ncv);
+    dumpLinelets();
     DUMPD("nbocv_lsg_coeff", this->nbocv_lsg_coeff, 3 * nbocv_s);
     DUMPD("boundary_fa_lsg_coeff", this->boundary_fa_lsg_coeff, 3 * nfa_b);
     dumpState("init");

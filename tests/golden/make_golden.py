@@ -59,6 +59,11 @@ def cases():
     yield "plate_roe", rawp, prmp
     yield "mixed_bump_hllc", rawm, prm
     yield "mixed_bump_roe_laminar_isothermal", rawm, dataclasses.replace(visc, bcs=bc_iso)
+    # BCGSTAB_LINELET: lines from the wall through the stretched rows (and through prisms into hexahedra)
+    rawl, _, prml = case.plate_case(24, 16, 2)
+    yield "plate_roe_linelet", rawl, dataclasses.replace(prml, LINEAR_SOLVER_NS="BCGSTAB_LINELET", LS_MAX_ITER=10)
+    yield "mixed_bump_roe_laminar_linelet", rawm, dataclasses.replace(visc, bcs=bc_iso,
+                                                                      LINEAR_SOLVER_NS="BCGSTAB_LINELET")
 
 
 def sa_cases():
@@ -116,7 +121,7 @@ def main(which=("segregated", "sa"), only=""):
                 "nbocv_lsg_coeff", "boundary_fa_lsg_coeff", "init_rho", "init_rhou", "init_rhoE",
                 "press", "temp", "enthalpy", "sos", "vel", "rho_bfa", "T_bfa", "vel_bfa", "p_bfa", "h_bfa",
                 "mul_fa", "lamOcp_fa", "local_dt", "grad_u", "grad_rho", "grad_p", "grad_enthalpy",
-                "rhs_rho", "rhs_rhou", "rhs_rhoE", "A", "rhs_sys", "dq"]
+                "rhs_rho", "rhs_rhou", "rhs_rhoE", "A", "rhs_sys", "dq", "line_off", "line_cv"]
         out = {k: d[k] for k in keep if k in d}
         out["final_rho"], out["final_rhou"], out["final_rhoE"] = r["final_rho"], r["final_rhou"], r["final_rhoE"]
         out["resid"] = r["resid"]

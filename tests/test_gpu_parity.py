@@ -138,11 +138,33 @@ def test_linear_solve_reference_solvers(golden):
     assert nrel(dq_g, dq_o) <= TOL
     # the reference's own default-threshold solve (BiCGSTAB, rel 1e-2) is matched by the oracle bit-exactly;
     # the GPU reaches the same iterate up to rounding
-    if g["params"].LINEAR_SOLVER_NS == "BCGSTAB":
-        j = gpu_case(g, "BCGSTAB")
+    if g["params"].LINEAR_SOLVER_NS in ("BCGSTAB", "BCGSTAB_LINELET"):
+        j = gpu_case(g, g["params"].LINEAR_SOLVER_NS)
         p = g["params"]
         dq_g, _ = j.solveCoupledLinSysNS(A, rhs, p.LS_ABS_RESID, p.LS_REL_RESID, p.LS_MAX_ITER)
         assert nrel(dq_g, g["dq"].reshape(-1, 5)) <= 1e-10
+
+
+def test_linelet_solve_converged(golden):
+    """BCGSTAB_LINELET driven to convergence on the reference's system
+    against the oracle, and fewer iterations than the block-diagonal
+    preconditioner where the lines are long."""
+    g = golden
+    if "line_off" not in g:
+        pytest.skip("not a BCGSTAB_LINELET fixture")
+    A = g["A"].copy()
+    vol_dt = g["cv_volume"] / g["local_dt"]
+    for i in range(5):
+        A[g["nbocv_i"][:-1], i, i] += vol_dt
+    rhs = g["rhs_sys"].reshape(-1, 5)
+    o = Oracle(dict(g), g["params"])
+    dq_o, it_o = o.solve(A, rhs, 1e-15, 1e-13, 400, SOLVER_KINDS["BCGSTAB_LINELET"])
+    j = gpu_case(g, "BCGSTAB_LINELET")
+    dq_g, it_g = j.solveCoupledLinSysNS(A, rhs, 1e-15, 1e-13, 400)
+    assert nrel(dq_g, dq_o) <= 1e-10
+    assert abs(it_g - it_o) <= 1
+    _, it_b = gpu_case(g, "BCGSTAB").solveCoupledLinSysNS(A, rhs, 1e-15, 1e-13, 400)
+    assert it_g <= it_b
 
 
 @pytest.mark.parametrize("relax", ["JACOBI", "SGS"])

@@ -141,12 +141,12 @@ def test_renumbered_golden_mixed_mesh_matches_reference():
 def test_renumbered_sgs_converges_to_the_same_field():
     from myjoe_b200 import case
     g, prm = _euler_mixed()
-    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=2.0, CFL_RAMP=(10, 5, 1.5, 100.0))
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=2.0, CFL_RAMP=(10, 5, 1.2, 20.0))
     a, b = _pair(g, prm)
     st = case.perturbed_state(g.x_cv, prm, 0.0)
     for j in (a, b):
         j.set_state(*st)
-    ra, rb = a.runBackwardEuler(1500), b.runBackwardEuler(1500)
+    ra, rb = a.runBackwardEuler(3200), b.runBackwardEuler(3200)
     assert ra[-1, 4] / ra[0, 4] < 1e-9 and rb[-1, 4] / rb[0, 4] < 1e-9
     for x, y in zip(a.get_state(), b.get_state()):
         assert np.linalg.norm(x - y) <= 1e-8 * np.linalg.norm(x)

@@ -76,3 +76,13 @@ def test_backward_euler_steps(golden):
     np.testing.assert_array_equal(rhou.ravel(), golden["final_rhou"].ravel())
     np.testing.assert_array_equal(rhoE, golden["final_rhoE"])
     np.testing.assert_allclose(res, golden["resid"], rtol=6e-5, atol=0)
+
+
+def test_linelets(golden):
+    """initializeLinelet's lines (fixtures solved with BCGSTAB_LINELET)."""
+    if "line_off" not in golden:
+        pytest.skip("not a BCGSTAB_LINELET fixture")
+    off, cv = _oracle(golden).linelets()
+    np.testing.assert_array_equal(off, golden["line_off"])
+    np.testing.assert_array_equal(cv, golden["line_cv"])
+    assert (np.diff(off) >= 2).any()

@@ -54,7 +54,12 @@ enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3,
        /* BCGSTAB_LINELET: BiCGSTAB preconditioned by block-tridiagonal solves along the
         * wall-normal lines of initializeLinelet (JoeWithModels.cpp:7471-7559) and the
         * block diagonal elsewhere, solveCvVectorR5BcgstabLine (UgpWithCv.cpp:3627-3992) */
-       JG_LS_BCGSTAB_LINELET = 4 };
+       JG_LS_BCGSTAB_LINELET = 4,
+       /* LINE (no reference counterpart; the reference's coupled solve is PETSc): ls_max_iter
+        * block line-Jacobi sweeps from zero: the block-tridiagonal system of every line of
+        * initializeLinelet solved exactly (block Thomas), the block diagonal on the other
+        * cells, the couplings across lines lagged.  5x5 and coupled paths, FP64 or mixed. */
+       JG_LS_LINE = 5 };
 enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
 
 typedef struct jg_zone {

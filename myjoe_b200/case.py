@@ -23,7 +23,7 @@ BC_KINDS = {
 }
 FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2}
 SYMM_BC_KINDS = {"ORIGINAL_NUMERIC": 0, "NEW_NUMERIC": 1, "ANALYTICAL": 2}
-SOLVER_KINDS = {"BCGSTAB": 0, "LUSGS": 1, "JACOBI": 2, "SGS": 3, "BCGSTAB_LINELET": 4}
+SOLVER_KINDS = {"BCGSTAB": 0, "LUSGS": 1, "JACOBI": 2, "SGS": 3, "BCGSTAB_LINELET": 4, "LINE": 5}
 
 
 @dataclasses.dataclass

@@ -248,19 +248,19 @@ static int check_params(const jg_params* q) {
   if (!q) return set_err(JG_ERR_ARG, "null params");
   if (q->flux < 0 || q->flux > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
   if (q->symm_bc < 0 || q->symm_bc > 2) return set_err(JG_ERR_ARG, "unsupported SYMM_BC %d", q->symm_bc);
-  if (q->lin_solver < 0 || q->lin_solver > 4) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
+  if (q->lin_solver < 0 || q->lin_solver > 5) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
   if (q->precision != JG_PREC_FP64 && q->precision != JG_PREC_MIXED)
     return set_err(JG_ERR_ARG, "unsupported precision %d", q->precision);
   if (q->precision == JG_PREC_MIXED && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_LUSGS ||
                                         q->lin_solver == JG_LS_BCGSTAB_LINELET))
-    return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI or SGS sweeps");
+    return set_err(JG_ERR_ARG, "the mixed-precision form relaxes with JACOBI, SGS or LINE sweeps");
   if (q->turb_model == JG_TURB_SA || q->turb_model == JG_TURB_SST) {
     if (q->nscal != (q->turb_model == JG_TURB_SA ? 1 : 2))
       return set_err(JG_ERR_ARG, "SA transports one scalar (nscal = 1), SST two (nscal = 2)");
     if (!(q->mu_ref > 0.0)) return set_err(JG_ERR_ARG, "a turbulence model needs a viscous case (mu_ref > 0)");
     if (q->flux != JG_FLUX_HLLC) return set_err(JG_ERR_ARG, "the coupled path uses the HLLC flux");
-    if (q->lin_solver != JG_LS_JACOBI && q->lin_solver != JG_LS_SGS)
-      return set_err(JG_ERR_ARG, "the coupled path relaxes with JACOBI or SGS sweeps");
+    if (q->lin_solver != JG_LS_JACOBI && q->lin_solver != JG_LS_SGS && q->lin_solver != JG_LS_LINE)
+      return set_err(JG_ERR_ARG, "the coupled path relaxes with JACOBI, SGS or LINE sweeps");
   } else if (q->turb_model != JG_TURB_NONE) {
     return set_err(JG_ERR_ARG, "unsupported turbulence model %d", q->turb_model);
   } else if (q->nscal != 0) {
@@ -540,18 +540,44 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     launch_wall_distance(h->m, t, h->stream);
     CKL();
   }
-  if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
+  if (q->lin_solver == JG_LS_BCGSTAB_LINELET || q->lin_solver == JG_LS_LINE) {
     std::vector<int> off, cv;
     multi_cell_lines(mesh, h->rn.face_old, off, cv);
     Lines& L = h->lines;
     L.nlines = (int)off.size() - 1;
-    const size_t nc = cv.size();
+    const size_t nc = std::max<size_t>(cv.size(), 1);
     RC(upload(h, &L.off, off.data(), off.size()));
-    RC(upload(h, &L.cv, cv.data(), std::max<size_t>(nc, 1)));
-    RC(dmalloc(h, &L.inv, 25 * std::max<size_t>(nc, 1)));
-    RC(dmalloc(h, &L.low, 25 * std::max<size_t>(nc, 1)));
-    RC(dmalloc(h, &L.up, 25 * std::max<size_t>(nc, 1)));
-    RC(dmalloc(h, &L.v, 5 * std::max<size_t>(nc, 1)));
+    RC(upload(h, &L.cv, cv.data(), nc));
+    if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
+      RC(dmalloc(h, &L.inv, 25 * nc));
+      RC(dmalloc(h, &L.low, 25 * nc));
+      RC(dmalloc(h, &L.up, 25 * nc));
+      RC(dmalloc(h, &L.v, 5 * nc));
+    } else {
+      // the line cells and, per ELL entry, whether it couples a cell to its predecessor or successor on its line
+      std::vector<uint8_t> on_line(N, 0), inl((size_t)rows * SLICE, 0);
+      std::vector<int> prev(N, -1), next(N, -1);
+      for (int l = 0; l < L.nlines; l++)
+        for (int k = off[l]; k < off[l + 1]; k++) {
+          on_line[cv[k]] = 1;
+          if (k > off[l]) prev[cv[k]] = cv[k - 1];
+          if (k + 1 < off[l + 1]) next[cv[k]] = cv[k + 1];
+        }
+      for (int c = 0; c < N; c++) {
+        if (!on_line[c]) continue;
+        const int sl = c / SLICE, lane = c % SLICE;
+        for (int j = 0; j < ncols[c]; j++) {
+          const size_t e = (size_t)(h->ell_off[sl] + j) * SLICE + lane;
+          if (ell_nb[e] == prev[c] || ell_nb[e] == next[c]) inl[e] = 1;
+        }
+      }
+      RC(upload(h, &L.on_line, on_line.data(), on_line.size()));
+      RC(upload(h, &L.ell_inline, inl.data(), inl.size()));
+      RC(dmalloc_bytes(h, &L.binv, (size_t)bs * bs * nc * h->eltsz));
+      RC(dmalloc_bytes(h, &L.blow, (size_t)bs * bs * nc * h->eltsz));
+      RC(dmalloc_bytes(h, &L.bup, (size_t)bs * bs * nc * h->eltsz));
+      RC(dmalloc_bytes(h, &L.bv, (size_t)bs * nc * h->eltsz));
+    }
   }
   double ctrl0[16] = {0};
   ctrl0[0] = q->cfl;
@@ -648,11 +674,15 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
     for (size_t x : t) b += alloc_round(x);
     if (q->turb_model == JG_TURB_SST) b += 4 * alloc_round(N * d);
   }
-  if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
+  if (q->lin_solver == JG_LS_BCGSTAB_LINELET || q->lin_solver == JG_LS_LINE) {
     std::vector<int> off, cv;
     multi_cell_lines(mesh, face_old, off, cv);
     const size_t nc = std::max<size_t>(cv.size(), 1);
-    b += alloc_round(off.size() * i) + alloc_round(nc * i) + 3 * alloc_round(25 * nc * d) + alloc_round(5 * nc * d);
+    b += alloc_round(off.size() * i) + alloc_round(nc * i);
+    if (q->lin_solver == JG_LS_BCGSTAB_LINELET)
+      b += 3 * alloc_round(25 * nc * d) + alloc_round(5 * nc * d);
+    else
+      b += alloc_round(N) + alloc_round(rows * SLICE) + 3 * alloc_round(b2 * nc * e) + alloc_round(bs * nc * e);
   }
   return b;
 }
@@ -766,6 +796,7 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
   if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
+  if (params->lin_solver == JG_LS_LINE) return set_err(JG_ERR_ARG, "LINE relaxation runs one case per handle");
   if (params->time_step_mode == JG_TS_CFL_MIN)
     return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
   int ndev = 0;
@@ -1176,6 +1207,12 @@ int jg_solve_lin_sys(jg_case_t* h, double* dq, const double* A, const double* rh
       launch_dq_from_x(h->m, h->p, h->st, h->st.x0, h->stream);
       it = sweeps;
     } break;
+    case JG_LS_LINE: {
+      int sweeps = std::max(1, maxIter);
+      launch_line_relax(h->m, h->p, h->st, h->lines, 5, sweeps, h->stream);
+      launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, h->stream);
+      it = sweeps;
+    } break;
   }
   CKL();
   RC(download_rows(h, h->st.dq, dq, h->rn.cell_old, N, 5));
@@ -1196,7 +1233,8 @@ static int enqueue_step_coupled(jg_case* h) {
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
   int sgs = h->hp.lin_solver == JG_LS_SGS;
   int sweeps = std::max(1, h->hp.ls_max_iter);
-  launch_relax6(h->m, h->p, h->st, sgs, sweeps, h->bs, S);
+  if (h->hp.lin_solver == JG_LS_LINE) launch_line_relax(h->m, h->p, h->st, h->lines, h->bs, sweeps, S);
+  else launch_relax6(h->m, h->p, h->st, sgs, sweeps, h->bs, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
   launch_update6(h->m, h->p, h->st, h->turb, (sgs || sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
   launch_state(h->m, h->p, h->st, S);
@@ -1230,6 +1268,10 @@ static int enqueue_step(jg_case* h, int for_graph) {
   } else if (solver == JG_LS_SGS) {
     launch_sgs(h->m, h->p, h->st, std::max(1, h->hp.ls_max_iter), S);
     launch_dq_from_x(h->m, h->p, h->st, h->st.x0, S);
+  } else if (solver == JG_LS_LINE) {
+    int sweeps = std::max(1, h->hp.ls_max_iter);
+    launch_line_relax(h->m, h->p, h->st, h->lines, 5, sweeps, S);
+    launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
   } else {
     if (for_graph) return set_err(JG_ERR_ARG, "BCGSTAB is not captured");
     // host-driven BiCGSTAB on the assembled system, zero initial guess; the rhs ([N][5] in st.b) as [5][N]
@@ -1504,7 +1546,8 @@ int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** ou
   if (!mesh || !out) return set_err(JG_ERR_ARG, "null argument");
   *out = nullptr;
   RC(check_params(params));
-  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
+  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET ||
+      params->lin_solver == JG_LS_LINE)
     return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "served cases are laminar / inviscid");
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "served cases keep their own order");

@@ -200,10 +200,18 @@ struct Lines {
   int nlines;
   const int* off;  // [nlines+1]
   const int* cv;   // [off[nlines]]
+  // BCGSTAB_LINELET (5x5, FP64)
   double* inv;     // [off[nlines]][25]
   double* low;     // [off[nlines]][25] (position 0 of a line unused)
   double* up;      // [off[nlines]][25] (position 0 of a line unused)
   double* v;       // [off[nlines]][5]
+  // LINE relaxation (B x B blocks in the matrix precision)
+  const uint8_t* on_line;     // [N] 1 on the cells of the lines
+  const uint8_t* ell_inline;  // [ell_rows*32] 1 where the ELL entry couples a cell to its line neighbour
+  void* binv;      // [off[nlines]][B*B]
+  void* blow;      // [off[nlines]][B*B]
+  void* bup;       // [off[nlines]][B*B]
+  void* bv;        // [off[nlines]][B]
 };
 // initializeLinelet on a mesh: wall_zones holds the faces of each WALL zone in zone order
 int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zones, std::vector<int>& off,
@@ -214,6 +222,11 @@ void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const d
                          cudaStream_t s);
 // [N][5] -> [5][N]
 void launch_aos_to_soa5(int n, const double* aos, double* soa, cudaStream_t s);
+// LINE relaxation of the assembled system (block size bs, matrix precision of p): the
+// block-tridiagonal factors of every line, then `sweeps` line-Jacobi sweeps from x = 0;
+// the result is in st.x0 (odd sweeps) or st.x1 (even)
+void launch_line_relax(const Mesh& m, const Params& p, State& st, const Lines& L, int bs, int sweeps,
+                       cudaStream_t s);
 
 // A mesh in jg_mesh's layout whose arrays the struct owns (concatenated
 // batches, renumbered cases); bind() points m at the vectors.

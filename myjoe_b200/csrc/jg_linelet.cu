@@ -253,3 +253,247 @@ void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const d
 }
 
 }  // namespace jg
+
+// ---------------------------------------------------------------------------
+// LINE relaxation: block line-Jacobi sweeps for B x B blocks (B = 5, 6, 7) in
+// the matrix precision BT.  A sweep is x' = T^-1 (b - (A - T) x), T the
+// block-tridiagonal part of A along the lines (the block diagonal elsewhere):
+//   k_lrelax_rhs: per cell r = b - sum of the off-diagonal blocks that are not
+//                 a line coupling times x; off the lines x' = Dinv r, on the
+//                 lines r is left in x' for
+//   k_lsolve:     the block Thomas substitutions of each line, in place.
+// k_lfactor computes the line factors once per step from D and the ELL
+// blocks, in FP64 arithmetic, and stores them in BT.
+// ---------------------------------------------------------------------------
+namespace jg {
+namespace {
+
+// inverse of a B x B block by the reference's LU (ludeco / luinv pattern), column `col`
+template <int B>
+__device__ void lu_inverse_col(const double* M, int col, double* out) {
+  double A[B * B];
+#pragma unroll
+  for (int q = 0; q < B * B; q++) A[q] = M[q];
+#pragma unroll
+  for (int jc = 1; jc < B; jc++) A[jc] /= A[0];
+#pragma unroll
+  for (int jrjc = 1; jrjc < B; jrjc++) {
+#pragma unroll
+    for (int jr = jrjc; jr < B; jr++) {
+      double sum = A[B * jr + jrjc];
+#pragma unroll
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jr + jm] * A[B * jm + jrjc];
+      A[B * jr + jrjc] = sum;
+    }
+    if (jrjc == B - 1) break;
+#pragma unroll
+    for (int jc = jrjc + 1; jc < B; jc++) {
+      double sum = A[B * jrjc + jc];
+#pragma unroll
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jrjc + jm] * A[B * jm + jc];
+      A[B * jrjc + jc] = sum / A[B * jrjc + jrjc];
+    }
+  }
+  double c[B];
+#pragma unroll
+  for (int i = 0; i < B; i++) c[i] = (i == col) ? 1.0 : 0.0;
+  c[0] = c[0] / A[0];
+#pragma unroll
+  for (int jr = 1; jr < B; jr++) {
+    double sum = c[jr];
+#pragma unroll
+    for (int jm = 0; jm < jr; jm++) sum -= A[B * jr + jm] * c[jm];
+    c[jr] = sum / A[B * jr + jr];
+  }
+#pragma unroll
+  for (int jr = B - 2; jr >= 0; jr--) {
+    double sum = c[jr];
+#pragma unroll
+    for (int jm = B - 1; jm > jr; jm--) sum -= A[B * jr + jm] * c[jm];
+    c[jr] = sum;
+  }
+#pragma unroll
+  for (int i = 0; i < B; i++) out[i] = c[i];
+}
+
+template <typename BT, int B>
+__device__ double ell_block_b(const Mesh& m, const BT* O, int row, int col, int e) {
+  const int s = row / SLICE, lane = row % SLICE;
+  double v = 0.0;
+  for (int j = m.ell_off[s]; j < m.ell_off[s + 1]; j++)
+    if (m.ell_nb[(size_t)j * SLICE + lane] == col) v += (double)O[((size_t)j * B * B + e) * SLICE + lane];
+  return v;
+}
+
+template <typename BT, int B>
+__global__ void __launch_bounds__(32 * LW) k_lfactor(Mesh m, State st, Lines L) {
+  constexpr int BB = B * B;
+  __shared__ double sh[LW][5][BB];
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int line = blockIdx.x * LW + w;
+  if (line >= L.nlines) return;
+  double *b = sh[w][0], *inv = sh[w][1], *lo = sh[w][2], *up = sh[w][3], *mh = sh[w][4];
+  const int p0 = L.off[line], n = L.off[line + 1] - p0;
+  const int N = m.ncv;
+  const BT* D = (const BT*)st.D;
+  const BT* O = (const BT*)st.O;
+  BT* Linv = (BT*)L.binv;
+  BT* Llow = (BT*)L.blow;
+  BT* Lup = (BT*)L.bup;
+  for (int e = lane; e < BB; e += 32) b[e] = (double)D[(size_t)e * N + L.cv[p0]];
+  __syncwarp();
+  for (int i = 1;; i++) {
+    if (lane < B) {
+      double col[B];
+      lu_inverse_col<B>(b, lane, col);
+#pragma unroll
+      for (int q = 0; q < B; q++) inv[B * q + lane] = col[q];
+    }
+    __syncwarp();
+    for (int e = lane; e < BB; e += 32) Linv[(size_t)(p0 + i - 1) * BB + e] = (BT)inv[e];
+    if (i == n) break;
+    const int cp = L.cv[p0 + i - 1], c = L.cv[p0 + i];
+    for (int e = lane; e < BB; e += 32) {
+      lo[e] = ell_block_b<BT, B>(m, O, c, cp, e);
+      up[e] = ell_block_b<BT, B>(m, O, cp, c, e);
+      Lup[(size_t)(p0 + i) * BB + e] = (BT)up[e];
+    }
+    __syncwarp();
+    for (int e = lane; e < BB; e += 32) {
+      const int r = e / B, k = e % B;
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < B; q++) s += lo[B * r + q] * inv[B * q + k];
+      mh[e] = s;
+      Llow[(size_t)(p0 + i) * BB + e] = (BT)s;
+    }
+    __syncwarp();
+    double bn[2];
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int e = lane + 32 * t;
+      bn[t] = 0.0;
+      if (e < BB) {
+        const int r = e / B, k = e % B;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < B; q++) s += mh[B * r + q] * up[B * q + k];
+        bn[t] = (double)D[(size_t)e * N + c] - s;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 2; t++)
+      if (lane + 32 * t < BB) b[lane + 32 * t] = bn[t];
+    __syncwarp();
+  }
+}
+
+// one block per 32-cell slice, B rows x 32 lanes (the k_jacobi_c layout)
+template <typename BT, int B>
+__global__ void __launch_bounds__(B * 32) k_lrelax_rhs(Mesh m, State st, Lines L, const BT* __restrict__ xin,
+                                                       BT* __restrict__ xout, int first) {
+  __shared__ BT sacc[B][SLICE];
+  const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
+  const int slice = blockIdx.x;
+  const int c = slice * SLICE + lane;
+  const bool active = c < m.ncv;
+  const int N = m.ncv;
+  BT acc = active ? (BT)st.b[(size_t)B * c + row] : (BT)0;
+  if (!first && active) {
+    const BT* O = (const BT*)st.O;
+    for (int j = m.ell_off[slice]; j < m.ell_off[slice + 1]; j++) {
+      if (L.ell_inline[(size_t)j * SLICE + lane]) continue;
+      int nb = m.ell_nb[(size_t)j * SLICE + lane];
+      const BT* Ob = O + ((size_t)j * B * B + B * row) * SLICE + lane;
+      BT s = 0;
+#pragma unroll
+      for (int k = 0; k < B; k++) s += Ob[k * SLICE] * xin[(size_t)k * N + nb];
+      acc -= s;
+    }
+  }
+  sacc[row][lane] = acc;
+  __syncthreads();
+  if (active) {
+    if (L.on_line[c]) {
+      xout[(size_t)row * N + c] = acc;
+    } else {
+      const BT* Di = (const BT*)st.Dinv;
+      BT s = 0;
+#pragma unroll
+      for (int k = 0; k < B; k++) s += Di[(size_t)(B * row + k) * N + c] * sacc[k][lane];
+      xout[(size_t)row * N + c] = s;
+    }
+  }
+}
+
+// x (cells of a line) = T_line^-1 r, r read from x; one warp per line, lanes < B hold the rows
+template <typename BT, int B>
+__global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restrict__ x) {
+  constexpr int BB = B * B;
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int line = blockIdx.x * LW + w;
+  if (line >= L.nlines) return;
+  const int p0 = L.off[line], n = L.off[line + 1] - p0;
+  const size_t N = m.ncv;
+  const int r = lane % B;
+  const bool row = lane < B;
+  const BT* Linv = (const BT*)L.binv;
+  const BT* Llow = (const BT*)L.blow;
+  const BT* Lup = (const BT*)L.bup;
+  BT* Lv = (BT*)L.bv;
+  BT v = x[r * N + L.cv[p0]];
+  if (row) Lv[(size_t)p0 * B + r] = v;
+  for (int i = 1; i < n; i++) {
+    const BT* Mi = &Llow[(size_t)(p0 + i) * BB + B * r];
+    BT s = 0;
+#pragma unroll
+    for (int q = 0; q < B; q++) s += Mi[q] * __shfl_sync(0xffffffffu, v, q);
+    v = x[r * N + L.cv[p0 + i]] - s;
+    if (row) Lv[(size_t)(p0 + i) * B + r] = v;
+  }
+  const BT* I = &Linv[(size_t)(p0 + n - 1) * BB + B * r];
+  BT yv = 0;
+#pragma unroll
+  for (int q = 0; q < B; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
+  if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
+  for (int i = n - 2; i >= 0; i--) {
+    const BT* U = &Lup[(size_t)(p0 + i + 1) * BB + B * r];
+    BT s2 = 0;
+#pragma unroll
+    for (int q = 0; q < B; q++) s2 += U[q] * __shfl_sync(0xffffffffu, yv, q);
+    const BT a1 = Lv[(size_t)(p0 + i) * B + r] - s2;
+    const BT* Ii = &Linv[(size_t)(p0 + i) * BB + B * r];
+    BT s = 0;
+#pragma unroll
+    for (int q = 0; q < B; q++) s += Ii[q] * __shfl_sync(0xffffffffu, a1, q);
+    yv = s;
+    if (row) x[r * N + L.cv[p0 + i]] = yv;
+  }
+}
+
+template <typename BT, int B>
+void line_relax(const Mesh& m, State& st, const Lines& L, int sweeps, cudaStream_t s) {
+  const int lb = (L.nlines + LW - 1) / LW;
+  if (L.nlines) k_lfactor<BT, B><<<lb, 32 * LW, 0, s>>>(m, st, L);
+  for (int it = 0; it < sweeps; it++) {
+    BT* xin = (BT*)((it % 2 == 0) ? st.x1 : st.x0);
+    BT* xout = (BT*)((it % 2 == 0) ? st.x0 : st.x1);
+    k_lrelax_rhs<BT, B><<<m.nslices, B * SLICE, 0, s>>>(m, st, L, xin, xout, it == 0);
+    if (L.nlines) k_lsolve<BT, B><<<lb, 32 * LW, 0, s>>>(m, L, xout);
+  }
+}
+
+}  // namespace
+
+void launch_line_relax(const Mesh& m, const Params& p, State& st, const Lines& L, int bs, int sweeps,
+                       cudaStream_t s) {
+  sweeps = sweeps < 1 ? 1 : sweeps;
+  switch (bs) {
+    case 5: p.fp32 ? line_relax<float, 5>(m, st, L, sweeps, s) : line_relax<double, 5>(m, st, L, sweeps, s); break;
+    case 6: p.fp32 ? line_relax<float, 6>(m, st, L, sweeps, s) : line_relax<double, 6>(m, st, L, sweeps, s); break;
+    default: p.fp32 ? line_relax<float, 7>(m, st, L, sweeps, s) : line_relax<double, 7>(m, st, L, sweeps, s); break;
+  }
+}
+
+}  // namespace jg

@@ -297,7 +297,8 @@ int jg_serve_now(jg_server_t* s, double* t) {
 int jg_serve_submit(jg_server_t* s, const jg_mesh* mesh, const jg_params* params, const double* rho,
                     const double* rhou, const double* rhoE, double t_arrival, long long* id) {
   if (!s || !mesh || !params || !rho || !rhou || !rhoE) return fail(JG_ERR_ARG, "null argument");
-  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
+  if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET ||
+      params->lin_solver == JG_LS_LINE)
     return fail(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
   double fp = 0.0;
   SRC(jg_case_footprint(mesh, params, &fp));

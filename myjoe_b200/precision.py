@@ -10,7 +10,9 @@ bump chord, far-field inlet/outlet/top, viscous WALL below) meshed by
 ``meshgen.channel_bump_mixed`` (prism rows on the wall, hexahedra above),
 cells and faces shuffled from the seed, solved through a handle that
 renumbers them itself (reverse Cuthill-McKee).  The shuffled order without
-renumbering is timed over a few hundred steps beside it.
+renumbering is timed over a few hundred steps beside it.  The linear solve
+is the LINE relaxation by default (block-tridiagonal solves along the
+wall-normal lines, which the stretched wall rows need), 10 sweeps per step.
 
     python -m myjoe_b200.precision [--nx 512 --ny 400 --nz 8 --n-prism 88] [--first-order] [--out f.json]
 """
@@ -85,6 +87,7 @@ def main(argv=None):
     ap.add_argument("--re", type=float, default=3.0e6)
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--first-order", action="store_true")
+    ap.add_argument("--solver", default="LINE", choices=["LINE", "SGS", "JACOBI"])
     ap.add_argument("--sweeps", type=int, default=10)
     ap.add_argument("--cfl-max", type=float, default=50.0)
     ap.add_argument("--max-steps", type=int, default=6000)
@@ -97,13 +100,14 @@ def main(argv=None):
     t = time.perf_counter()
     raw, g, prm = case.sa_bump_case(a.nx, a.ny, a.nz, mach=a.mach, re=a.re, bump_h=a.bump_h, seed=a.seed,
                                     stretch=a.stretch, n_prism=a.n_prism, alternate=True, shuffle=True)
-    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=a.sweeps, CFL=1.0,
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS=a.solver, LS_MAX_ITER=a.sweeps, CFL=1.0,
                               CFL_RAMP=(10, 5, 1.2, a.cfl_max), SECOND_ORDER=not a.first_order)
     t_mesh = time.perf_counter() - t
     nprism = 2 * a.nx * a.nz * a.n_prism
     res = {"workload": "SA bump, shuffled mixed prism/hex mesh", "ncv": g.ncv, "prisms": nprism,
            "hexahedra": g.ncv - nprism, "nfa": g.nfa, "mach": a.mach, "re": a.re, "bump_h": a.bump_h,
-           "second_order": not a.first_order, "sweeps": a.sweeps, "cfl_max": a.cfl_max, "drop": a.drop,
+           "second_order": not a.first_order, "solver": a.solver, "sweeps": a.sweeps, "cfl_max": a.cfl_max,
+           "drop": a.drop,
            "mesh_seconds": t_mesh}
     if not a.skip_order_timing:
         res["order_timing"] = [time_order(g, prm, False), time_order(g, prm, True)]

@@ -1716,6 +1716,7 @@ int jo_solve(jo_case *h, double *dq, const double *A, const double *rhs, double 
   switch (solver) {
     case JG_LS_BCGSTAB: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, 0);
     case JG_LS_BCGSTAB_LINELET: return solve_bcgstab(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, 1);
+    case JG_LS_LINE: return jo_line_relax(h, 5, dq, A, rhs, maxIter);
     case JG_LS_LUSGS: return solve_lusgs(h, dq, A, rhs);
     case JG_LS_JACOBI: return solve_jacobi(h, dq, A, rhs, maxIter);
     case JG_LS_SGS: return solve_sgs(h, dq, A, rhs, maxIter);
@@ -2723,6 +2724,125 @@ static void lusolv_n(const double *A, double *c, int n) {
   }
 }
 
+/* LINE relaxation as the GPU runs it (no reference counterpart): `sweeps`
+ * block line-Jacobi sweeps of the B x B system from x = 0.  On the lines of
+ * initializeLinelet (two or more cells) the block-tridiagonal system is
+ * solved exactly by block Thomas elimination; the other cells take a block
+ * Jacobi step; every coupling that is not between line neighbours uses the
+ * previous sweep's x. */
+int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps) {
+  const jg_mesh *m = &h->m;
+  const int n = h->ncv, BB = B * B;
+  if (!h->line_off) jo_build_linelets(h);
+  int *prev = (int *)malloc(sizeof(int) * n), *next = (int *)malloc(sizeof(int) * n);
+  char *on = (char *)calloc(n, 1);
+  for (int c = 0; c < n; c++) prev[c] = next[c] = -1;
+  int ncl = 0;
+  for (int l = 0; l < h->nlines; l++) {
+    int a = h->line_off[l], b = h->line_off[l + 1];
+    if (b - a < 2) continue;
+    for (int k = a; k < b; k++) {
+      int c = h->line_cv[k];
+      on[c] = 1;
+      ncl++;
+      if (k > a) prev[c] = h->line_cv[k - 1];
+      if (k + 1 < b) next[c] = h->line_cv[k + 1];
+    }
+  }
+  double *LU = dalloc((size_t)BB * n), *xn = dalloc((size_t)B * n), *r = dalloc((size_t)B * n);
+  double *inv = dalloc((size_t)BB * n), *low = dalloc((size_t)BB * n), *vv = dalloc((size_t)B * n);
+  for (int c = 0; c < n; c++) {
+    memcpy(&LU[(size_t)BB * c], &A[(size_t)BB * m->nbocv_i[c]], sizeof(double) * BB);
+    ludeco_n(&LU[(size_t)BB * c], B);
+  }
+  /* line factors: inv_i of the eliminated diagonal, low_i = A(c_i, c_{i-1}) inv_{i-1}, indexed by cell */
+  double bh[MAXB * MAXB], lu[MAXB * MAXB], col[MAXB];
+  for (int l = 0; l < h->nlines; l++) {
+    int a = h->line_off[l], b = h->line_off[l + 1];
+    if (b - a < 2) continue;
+    memcpy(bh, &A[(size_t)BB * m->nbocv_i[h->line_cv[a]]], sizeof(double) * BB);
+    for (int k = a; k < b; k++) {
+      int c = h->line_cv[k];
+      memcpy(lu, bh, sizeof(double) * BB);
+      ludeco_n(lu, B);
+      for (int j = 0; j < B; j++) {
+        for (int i = 0; i < B; i++) col[i] = (i == j) ? 1.0 : 0.0;
+        lusolv_n(lu, col, B);
+        for (int i = 0; i < B; i++) inv[(size_t)BB * c + B * i + j] = col[i];
+      }
+      if (k + 1 == b) break;
+      int cn = h->line_cv[k + 1];
+      const double *Alo = &A[(size_t)BB * csr_entry(m, cn, c)];
+      const double *Aup = &A[(size_t)BB * csr_entry(m, c, cn)];
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) {
+          double t = 0.0;
+          for (int q = 0; q < B; q++) t += Alo[B * i + q] * inv[(size_t)BB * c + B * q + j];
+          low[(size_t)BB * cn + B * i + j] = t;
+        }
+      const double *Dn = &A[(size_t)BB * m->nbocv_i[cn]];
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++) {
+          double t = 0.0;
+          for (int q = 0; q < B; q++) t += low[(size_t)BB * cn + B * i + q] * Aup[B * q + j];
+          bh[B * i + j] = Dn[B * i + j] - t;
+        }
+    }
+  }
+  memset(x, 0, sizeof(double) * B * n);
+  for (int s = 0; s < sweeps; s++) {
+    for (int c = 0; c < n; c++) {
+      double *rc = &r[(size_t)B * c];
+      for (int i = 0; i < B; i++) rc[i] = rhs[(size_t)B * c + i];
+      for (int k = m->nbocv_i[c] + 1; k < m->nbocv_i[c + 1]; k++) {
+        int nb = m->nbocv_v[k];
+        if (nb == prev[c] || nb == next[c]) continue;
+        for (int i = 0; i < B; i++)
+          for (int j = 0; j < B; j++) rc[i] -= A[(size_t)BB * k + B * i + j] * x[(size_t)B * nb + j];
+      }
+      if (!on[c]) {
+        memcpy(&xn[(size_t)B * c], rc, sizeof(double) * B);
+        lusolv_n(&LU[(size_t)BB * c], &xn[(size_t)B * c], B);
+      }
+    }
+    for (int l = 0; l < h->nlines; l++) {
+      int a = h->line_off[l], b = h->line_off[l + 1];
+      if (b - a < 2) continue;
+      for (int k = a; k < b; k++) {
+        int c = h->line_cv[k];
+        for (int i = 0; i < B; i++) {
+          double t = 0.0;
+          if (k > a)
+            for (int q = 0; q < B; q++) t += low[(size_t)BB * c + B * i + q] * vv[(size_t)B * h->line_cv[k - 1] + q];
+          vv[(size_t)B * c + i] = r[(size_t)B * c + i] - t;
+        }
+      }
+      for (int k = b - 1; k >= a; k--) {
+        int c = h->line_cv[k];
+        double a1[MAXB];
+        for (int i = 0; i < B; i++) {
+          double t = 0.0;
+          if (k + 1 < b) {
+            int cn = h->line_cv[k + 1];
+            const double *Aup = &A[(size_t)BB * csr_entry(m, c, cn)];
+            for (int q = 0; q < B; q++) t += Aup[B * i + q] * xn[(size_t)B * cn + q];
+          }
+          a1[i] = vv[(size_t)B * c + i] - t;
+        }
+        for (int i = 0; i < B; i++) {
+          double t = 0.0;
+          for (int q = 0; q < B; q++) t += inv[(size_t)BB * c + B * i + q] * a1[q];
+          xn[(size_t)B * c + i] = t;
+        }
+      }
+    }
+    memcpy(x, xn, sizeof(double) * B * n);
+  }
+  (void)ncl;
+  free(prev); free(next); free(on); free(LU); free(xn); free(r); free(inv); free(low); free(vv);
+  return sweeps;
+}
+
 /* block Jacobi (sgs = 0) or multicolour block Gauss-Seidel (sgs = 1) sweeps
  * of the B x B system from x = 0, as the GPU runs them */
 int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps, int sgs) {
@@ -2790,7 +2910,8 @@ int jo_step_coupled(jo_case *h, int nsteps, double *resid) {
       double tmp = h->m.cv_volume[c] / (h->local_dt[c]);
       for (int i = 0; i < B; i++) A[(size_t)B * B * h->m.nbocv_i[c] + (B + 1) * i] += tmp;
     }
-    jo_solve_blocks(h, B, dq, A, rhs, p->ls_max_iter, p->lin_solver == JG_LS_SGS);
+    if (p->lin_solver == JG_LS_LINE) jo_line_relax(h, B, dq, A, rhs, p->ls_max_iter);
+    else jo_solve_blocks(h, B, dq, A, rhs, p->ls_max_iter, p->lin_solver == JG_LS_SGS);
     for (int c = 0; c < n; c++) {
       h->rho[c] += dq[B * c];
       for (int i = 0; i < 3; i++) h->rhou[3 * c + i] += dq[B * c + 1 + i];

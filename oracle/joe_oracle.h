@@ -55,6 +55,8 @@ void jo_wall_distance(jo_case *h);
 int jo_calc_state_coupled(jo_case *h);
 void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit);
 int jo_solve_blocks(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps, int sgs);
+/* LINE relaxation (the GPU's JG_LS_LINE): block line-Jacobi sweeps from x = 0 */
+int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps);
 int jo_step_coupled(jo_case *h, int nsteps, double *resid);
 double *jo_sa_array(jo_case *h, const char *name);
 void jo_sa_release(jo_case *h);

@@ -60,6 +60,7 @@ def lib():
         L.jo_sa_array.restype = D
         L.jo_sa_release.argtypes = [P]
         L.jo_linelets.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.jo_line_relax.argtypes = [P, C.c_int, D, D, D, C.c_int]
         L.jo_linelets.restype = C.c_int
         _lib = L
     return _lib
@@ -182,11 +183,14 @@ class OracleSA(Oracle):
         lib().jo_calc_rhs_coupled(self.h, dptr(rhs), dptr(A), int(implicit))
         return rhs, A
 
-    def solve_blocks(self, A, rhs, sweeps, sgs=True):
+    def solve_blocks(self, A, rhs, sweeps, sgs=True, line=False):
         x = np.zeros((self.ncv, self.B))
         A = np.ascontiguousarray(A, np.float64)
         rhs = np.ascontiguousarray(rhs, np.float64)
-        lib().jo_solve_blocks(self.h, self.B, dptr(x), dptr(A), dptr(rhs), int(sweeps), int(sgs))
+        if line:
+            lib().jo_line_relax(self.h, self.B, dptr(x), dptr(A), dptr(rhs), int(sweeps))
+        else:
+            lib().jo_solve_blocks(self.h, self.B, dptr(x), dptr(A), dptr(rhs), int(sweeps), int(sgs))
         return x
 
     def step(self, nsteps=1):

@@ -56,9 +56,12 @@ enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3,
         * block diagonal elsewhere, solveCvVectorR5BcgstabLine (UgpWithCv.cpp:3627-3992) */
        JG_LS_BCGSTAB_LINELET = 4,
        /* LINE (no reference counterpart; the reference's coupled solve is PETSc): ls_max_iter
-        * block line-Jacobi sweeps from zero: the block-tridiagonal system of every line of
-        * initializeLinelet solved exactly (block Thomas), the block diagonal on the other
-        * cells, the couplings across lines lagged.  5x5 and coupled paths, FP64 or mixed. */
+        * block line-Jacobi sweeps from zero: the block-tridiagonal system of every line solved
+        * exactly (block Thomas), the block diagonal on the other cells, the couplings across
+        * lines lagged.  The lines follow initializeLinelet's rule from the WALL faces, except
+        * that where several neighbours pass a line goes on to the strongest coupling if it is
+        * 1.1 times the next (so it crosses prism/hexahedron interfaces).  5x5 and coupled
+        * paths, FP64 or mixed. */
        JG_LS_LINE = 5 };
 enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
 
@@ -218,15 +221,20 @@ int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
  * values, concatenated into one block-diagonal system so that every stage of
  * the iteration is one launch over all cases.  Each case keeps its own
  * residual reduction and never reads another case's data, so its results are
- * bit-identical alone and in any batch.  Linear solver JACOBI, SGS or LUSGS;
- * time step CFL or DT.  The batch handle accepts every single-case call
- * (jg_step reports the residual summed over the cases). */
+ * bit-identical alone and in any batch.  Linear solver JACOBI, SGS or LUSGS
+ * (JACOBI or SGS with a turbulence model); time step CFL or DT.  All cases
+ * share one model: none, SA or SST (each case's wall distance is taken to its
+ * own WALL faces).  The batch handle accepts every single-case call (jg_step
+ * reports the residual summed over the cases). */
 int jg_batch_create(int ncases, const jg_mesh *meshes, const jg_params *params, jg_case_t **out);
 int jg_batch_info(jg_case_t *h, int *ncases, int *cell_offsets /* [ncases+1], may be NULL */);
 /* sets one case's state; the state/BC preamble runs at the next step (set every case first) */
 int jg_batch_set_state(jg_case_t *h, int case_id, const double *rho, const double *rhou, const double *rhoE);
 int jg_batch_get_state(jg_case_t *h, int case_id, double *rho, double *rhou, double *rhoE);
-/* resid[nsteps][ncases][5]: the L1 residual of every case at every step.  A
+/* a turbulence-model batch: one case's transported scalars phi[ncv_k][nscal] in/out */
+int jg_batch_set_scalars(jg_case_t *h, int case_id, const double *phi);
+int jg_batch_get_scalars(jg_case_t *h, int case_id, double *phi);
+/* resid[nsteps][ncases][5 + nscal]: the L1 residual of every case at every step.  A
  * case that goes non-physical does not stop the batch: see jg_batch_status. */
 int jg_batch_step(jg_case_t *h, int nsteps, double *resid);
 /* status[ncases]: error flags of each case since the last call (1: density or

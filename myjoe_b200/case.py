@@ -249,7 +249,8 @@ def plate_case(nx=256, ny=96, nz=2, mach=0.3, re_l=1.0e5, p=1.0e5, T=300.0, flux
 
 
 def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
-                 stretch=1.0, inlet="FARFIELD", nu_factor=3.0, n_prism=0, shuffle=False, alternate=False):
+                 stretch=1.0, inlet="FARFIELD", nu_factor=3.0, n_prism=0, shuffle=False, alternate=False,
+                 aoa_deg=0.0, mu_ref=None):
     """Turbulent (SA) flow over the channel bump: viscous WALL lower (nuSA = 0),
     HLLC, Sutherland viscosity with MU_REF set so that the Reynolds number on
     the bump chord (length 1) is ``re``; inflow nuSA = ``nu_factor`` x the
@@ -257,16 +258,21 @@ def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_
     outlet and top (or CBC inlet with ``inlet="CBC"``), SYMMETRY z planes.
     ``stretch`` > 1 clusters the rows towards the lower wall.  ``n_prism`` > 0
     meshes that many wall rows with triangular prisms (``channel_bump_mixed``);
-    ``shuffle`` permutes cells and faces from ``seed``."""
+    ``shuffle`` permutes cells and faces from ``seed``; ``aoa_deg`` tilts the
+    inflow (far-field inlet).  ``mu_ref`` given fixes the fluid instead (``re``
+    is then unused): cases of one batch share it."""
     gam, R = 1.4, 287.0
     rho = p / (R * T)
     c = math.sqrt(gam * R * T)
     U = mach * c
     tref, sref = 273.15, 110.4
-    mu = rho * U * 1.0 / re
-    mu_ref = mu / ((T / tref) ** 1.5 * (tref + sref) / (T + sref))
+    sutherland = (T / tref) ** 1.5 * (tref + sref) / (T + sref)
+    if mu_ref is None:
+        mu_ref = rho * U * 1.0 / re / sutherland
+    mu = mu_ref * sutherland
     nu_inf = nu_factor * mu / rho
-    u = (U, 0.0, 0.0)
+    a = math.radians(aoa_deg)
+    u = (U * math.cos(a), U * math.sin(a), 0.0)
     if n_prism > 0:
         raw = meshgen.channel_bump_mixed(nx, ny, nz, n_prism=n_prism, bump_h=bump_h, jitter=jitter, seed=seed,
                                          stretch=stretch, alternate=alternate)
@@ -288,14 +294,15 @@ def sa_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_
 
 def sst_bump_case(nx=64, ny=32, nz=2, mach=0.7, re=3.0e6, p=1.0e5, T=300.0, bump_h=0.1, jitter=0.0, seed=0,
                   stretch=1.0, inlet="FARFIELD", tu=0.005, visc_ratio=0.1, n_prism=0, shuffle=False,
-                  alternate=False):
+                  alternate=False, aoa_deg=0.0, mu_ref=None):
     """Turbulent (Menter SST) flow over the channel bump, set up like
     ``sa_bump_case``: free-stream k = 1.5 (tu U)^2 and omega from the
     free-stream eddy-viscosity ratio mu_t/mu = ``visc_ratio``; at the wall
     k = 0 and omega from the model's wall hook (60 nu / (beta_1 d^2))."""
     raw, g, prm = sa_bump_case(nx, ny, nz, mach=mach, re=re, p=p, T=T, bump_h=bump_h, jitter=jitter, seed=seed,
-                               stretch=stretch, inlet=inlet, n_prism=n_prism, shuffle=shuffle, alternate=alternate)
-    U = prm.U_INITIAL[0]
+                               stretch=stretch, inlet=inlet, n_prism=n_prism, shuffle=shuffle, alternate=alternate,
+                               aoa_deg=aoa_deg, mu_ref=mu_ref)
+    U = math.hypot(prm.U_INITIAL[0], prm.U_INITIAL[1])
     rho = prm.RHO_INITIAL
     tref, sref = 273.15, 110.4
     mu = prm.MU_REF * (T / tref) ** 1.5 * (tref + sref) / (T + sref)

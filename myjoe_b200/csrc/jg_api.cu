@@ -200,9 +200,9 @@ static std::vector<std::vector<int>> wall_zone_faces(const jg_mesh* mesh, const 
 
 // the lines of two or more cells of initializeLinelet
 static void multi_cell_lines(const jg_mesh* mesh, const std::vector<int>& face_old, std::vector<int>& off,
-                             std::vector<int>& cv) {
+                             std::vector<int>& cv, bool relaxed) {
   std::vector<int> o, c;
-  build_lines(*mesh, wall_zone_faces(mesh, face_old), o, c);
+  build_lines(*mesh, wall_zone_faces(mesh, face_old), o, c, relaxed);
   off.assign(1, 0);
   cv.clear();
   for (size_t l = 0; l + 1 < o.size(); l++)
@@ -532,17 +532,25 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
           std::sort(wall.begin() + w0, wall.end(),
                     [&](int a, int b) { return h->rn.face_old[a] < h->rn.face_old[b]; });
       }
-    if (wall.empty()) return set_err(JG_ERR_ARG, "a turbulence model needs a WALL zone (wall distance)");
+    // the cases of a batch are concatenated zone by zone: the WALL faces of case k are one segment
+    std::vector<int> woff(h->ncases + 1, 0);
+    for (int k = 0, w = 0; k < h->ncases; k++) {
+      while (w < (int)wall.size() && wall[w] < h->case_nfa_b_off[k + 1]) w++;
+      woff[k + 1] = w;
+      if (woff[k + 1] == woff[k])
+        return set_err(JG_ERR_ARG, "case %d: a turbulence model needs a WALL zone (wall distance)", k);
+    }
     const int* dw = nullptr;
     RC(upload(h, &dw, wall.data(), wall.size()));
     t.wall_f = dw;
     t.nwall = (int)wall.size();
-    launch_wall_distance(h->m, t, h->stream);
+    for (int k = 0; k < h->ncases; k++)
+      launch_wall_distance(h->m, t, h->case_off[k], h->case_off[k + 1], woff[k], woff[k + 1], h->stream);
     CKL();
   }
   if (q->lin_solver == JG_LS_BCGSTAB_LINELET || q->lin_solver == JG_LS_LINE) {
     std::vector<int> off, cv;
-    multi_cell_lines(mesh, h->rn.face_old, off, cv);
+    multi_cell_lines(mesh, h->rn.face_old, off, cv, q->lin_solver == JG_LS_LINE);
     Lines& L = h->lines;
     L.nlines = (int)off.size() - 1;
     const size_t nc = std::max<size_t>(cv.size(), 1);
@@ -676,7 +684,7 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
   }
   if (q->lin_solver == JG_LS_BCGSTAB_LINELET || q->lin_solver == JG_LS_LINE) {
     std::vector<int> off, cv;
-    multi_cell_lines(mesh, face_old, off, cv);
+    multi_cell_lines(mesh, face_old, off, cv, q->lin_solver == JG_LS_LINE);
     const size_t nc = std::max<size_t>(cv.size(), 1);
     b += alloc_round(off.size() * i) + alloc_round(nc * i);
     if (q->lin_solver == JG_LS_BCGSTAB_LINELET)
@@ -792,7 +800,6 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (ncases <= 0 || !meshes || !out) return set_err(JG_ERR_ARG, "bad argument");
   *out = nullptr;
   RC(check_params(params));
-  if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "batches hold laminar / inviscid cases");
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
   if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
@@ -851,19 +858,54 @@ int jg_batch_get_state(jg_case_t* h, int k, double* rho, double* rhou, double* r
   return JG_OK;
 }
 
+int jg_batch_set_scalars(jg_case_t* h, int k, const double* phi) {
+  if (!h || !phi || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the batch transports no scalar");
+  const size_t N = h->ncv, ns = h->turb.ns, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
+  std::vector<double> cm(ns * n);  // [n][ns] -> [ns][n]
+  for (size_t c = 0; c < n; c++)
+    for (size_t q = 0; q < ns; q++) cm[q * n + c] = phi[ns * c + q];
+  for (size_t q = 0; q < ns; q++)
+    CK(cudaMemcpyAsync(h->turb.phi + q * N + c0, cm.data() + q * n, n * sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->primed = 0;
+  return JG_OK;
+}
+
+int jg_batch_get_scalars(jg_case_t* h, int k, double* phi) {
+  if (!h || !phi || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
+  if (h->bs == 5) return set_err(JG_ERR_ARG, "the batch transports no scalar");
+  const size_t N = h->ncv, ns = h->turb.ns, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
+  std::vector<double> cm(ns * n);
+  for (size_t q = 0; q < ns; q++)
+    CK(cudaMemcpyAsync(cm.data() + q * n, h->turb.phi + q * N + c0, n * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t c = 0; c < n; c++)
+    for (size_t q = 0; q < ns; q++) phi[ns * c + q] = cm[q * n + c];
+  return JG_OK;
+}
+
 int jg_get_stream(jg_case_t* h, void** stream) {
   if (!h || !stream) return set_err(JG_ERR_ARG, "null argument");
   *stream = (void*)h->stream;
   return JG_OK;
 }
 
-static int check_err_flags(jg_case* h) {
+// The handle's error flags.  Per-case state errors count for a single case,
+// and for every case of a batch with all_cases (the preamble: a bad input
+// state); during batch steps they stay per case (jg_batch_status).
+static int check_err_flags(jg_case* h, bool all_cases = false) {
   int e = 0, ec = 0;
+  const int nc = (h->ncases == 1 || all_cases) ? h->ncases : 0;
+  std::vector<int> ce(std::max(nc, 1), 0);
   CK(cudaMemcpyAsync(&e, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  if (h->ncases == 1) CK(cudaMemcpyAsync(&ec, h->st.case_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (nc) CK(cudaMemcpyAsync(ce.data(), h->st.case_err, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < nc; k++) ec |= ce[k];
   if (ec) {
-    CK(cudaMemsetAsync(h->st.case_err, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->st.case_err, 0, nc * sizeof(int), h->stream));
     e |= ec;
   }
   if (e) {
@@ -886,7 +928,7 @@ static int prime(jg_case* h) {
   }
   CKL();
   h->primed = 1;
-  return check_err_flags(h);
+  return check_err_flags(h, true);
 }
 
 int jg_set_state(jg_case_t* h, const double* rho, const double* rhou, const double* rhoE) {
@@ -1355,13 +1397,14 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
       CK(cudaMemcpy(resid, h->st.resid, h->bs * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
     } else {
       // the sum over the cases of the batch, per step
-      std::vector<double> all(5 * (size_t)nsteps * h->ncases);
+      const int bs = h->bs;
+      std::vector<double> all(bs * (size_t)nsteps * h->ncases);
       CK(cudaMemcpy(all.data(), h->st.resid, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
       for (int k = 0; k < nsteps; k++)
-        for (int i = 0; i < 5; i++) {
+        for (int i = 0; i < bs; i++) {
           double v = 0.0;
-          for (int c = 0; c < h->ncases; c++) v += all[((size_t)k * h->ncases + c) * 5 + i];
-          resid[5 * k + i] = v;
+          for (int c = 0; c < h->ncases; c++) v += all[((size_t)k * h->ncases + c) * bs + i];
+          resid[(size_t)bs * k + i] = v;
         }
     }
   }
@@ -1393,7 +1436,7 @@ int jg_batch_step(jg_case_t* h, int nsteps, double* resid) {
   RC(jg_step(h, nsteps, nullptr));
   if (resid && nsteps > 0) {
     // jg_step sized the ring buffer to hold nsteps entries starting at index 0
-    CK(cudaMemcpy(resid, h->st.resid, 5 * (size_t)nsteps * h->ncases * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(resid, h->st.resid, (size_t)h->bs * nsteps * h->ncases * sizeof(double), cudaMemcpyDeviceToHost));
   }
   return JG_OK;
 }

@@ -45,21 +45,23 @@ __device__ __forceinline__ double sq(double x) { return x * x; }  // pow(x, 2.0)
 // calcWallDistance (UgpWithCvCompFlow.h:1395-1535): nearest WALL face centroid
 // (first in zone order on ties), then the normal distance when the cell lies
 // over that face.  Wall-face centroids are staged through shared memory.
+// Cells [c0, c1) against the WALL faces wall_f[w0 .. w1) (a batch: one case).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_wall_dist(Mesh m, Turb t) {
+__global__ void __launch_bounds__(256) k_wall_dist(Mesh m, Turb t, int c0, int c1, int w0, int w1) {
   __shared__ double sx[256][3];
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int nwall = w1 - w0;
   double x[3] = {0.0, 0.0, 0.0};
-  if (c < m.ncv)
+  if (c < c1)
     for (int i = 0; i < 3; i++) x[i] = m.x_cv[3 * c + i];
   double minD = 1.0e20;
   int save = 0;
-  for (int k0 = 0; k0 < t.nwall; k0 += 256) {
+  for (int k0 = 0; k0 < nwall; k0 += 256) {
     int k = k0 + threadIdx.x;
-    if (k < t.nwall)
-      for (int i = 0; i < 3; i++) sx[threadIdx.x][i] = m.x_fa[3 * t.wall_f[k] + i];
+    if (k < nwall)
+      for (int i = 0; i < 3; i++) sx[threadIdx.x][i] = m.x_fa[3 * t.wall_f[w0 + k] + i];
     __syncthreads();
-    int n = min(256, t.nwall - k0);
+    int n = min(256, nwall - k0);
     for (int j = 0; j < n; j++) {
       double d = sqrt(sq(x[0] - sx[j][0]) + sq(x[1] - sx[j][1]) + sq(x[2] - sx[j][2]));
       if (d < minD) {
@@ -69,8 +71,8 @@ __global__ void __launch_bounds__(256) k_wall_dist(Mesh m, Turb t) {
     }
     __syncthreads();
   }
-  if (c >= m.ncv || t.nwall == 0) return;
-  int f = t.wall_f[save];
+  if (c >= c1 || nwall == 0) return;
+  int f = t.wall_f[w0 + save];
   double n[3], sh[3], nmag;
   unit_normal_c(m, f, n, nmag);
   for (int i = 0; i < 3; i++) sh[i] = m.x_fa[3 * f + i] - x[i];
@@ -1075,6 +1077,7 @@ __global__ void k_update_c(Mesh m, State st, Turb t, const BT* __restrict__ x, d
   constexpr int B = 5 + NS;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ncv) return;
+  if (!st.case_active[m.case_of[c]]) return;  // a frozen (retired) case of a batch keeps its state
   const int N = m.ncv;
   double dq[B];
   for (int i = 0; i < B; i++) {
@@ -1095,8 +1098,8 @@ __global__ void k_update_c(Mesh m, State st, Turb t, const BT* __restrict__ x, d
 // ---------------------------------------------------------------------------
 constexpr int TBC = 128;
 
-void launch_wall_distance(const Mesh& m, Turb& t, cudaStream_t s) {
-  k_wall_dist<<<grid_for(m.ncv, 256), 256, 0, s>>>(m, t);
+void launch_wall_distance(const Mesh& m, Turb& t, int c0, int c1, int w0, int w1, cudaStream_t s) {
+  if (c1 > c0) k_wall_dist<<<grid_for(c1 - c0, 256), 256, 0, s>>>(m, t, c0, c1, w0, w1);
 }
 void launch_scalar_bc(const Mesh& m, const Params& p, State& st, Turb& t, cudaStream_t s) {
   if (m.nfa_b) k_scalar_bc<<<grid_for(m.nfa_b, TBC), TBC, 0, s>>>(m, p, st, t);

@@ -176,7 +176,8 @@ int record_error(int code, const char* msg);  // sets the jg_last_error message
 
 namespace jg {
 // coupled turbulence-model path (jg_coupled.cu), block size 5 + ns
-void launch_wall_distance(const Mesh& m, Turb& t, cudaStream_t s);
+// wall distance of cells [c0, c1) to the WALL faces t.wall_f[w0 .. w1)
+void launch_wall_distance(const Mesh& m, Turb& t, int c0, int c1, int w0, int w1, cudaStream_t s);
 void launch_scalar_bc(const Mesh& m, const Params& p, State& st, Turb& t, cudaStream_t s);
 // gradients of the flow (limited, as calcFluxCoupled takes them) and of nuSA,
 // strain/vorticity magnitudes, turbulent viscosity and scalar diffusivity
@@ -214,8 +215,9 @@ struct Lines {
   void* bv;        // [off[nlines]][B]
 };
 // initializeLinelet on a mesh: wall_zones holds the faces of each WALL zone in zone order
+// (relaxed: the LINE relaxation's rule, which also crosses prism/hexahedron interfaces)
 int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zones, std::vector<int>& off,
-                std::vector<int>& cv);
+                std::vector<int>& cv, bool relaxed);
 void launch_line_factor(const Mesh& m, const State& st, const Lines& L, cudaStream_t s);
 // y = the line-implicit preconditioner applied to x ([5][N] both)
 void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const double* x, double* y,

@@ -44,13 +44,16 @@ __device__ __forceinline__ void state_from_q(const Params& p, const double* q, d
   prim[6] = sqrt(p.gamma * pp / r);
 }
 
+// state errors are recorded per case (a batch keeps going); a frozen case keeps its primitives
 __global__ void k_state(Mesh m, Params p, State st) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ncv) return;
+  const int k = m.case_of[c];
+  if (!st.case_active[k]) return;
   double q[5], prim[8];
   for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i];
   for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
-  state_from_q(p, q, prim, st.err, st.kine ? st.kine[c] : 0.0);
+  state_from_q(p, q, prim, st.case_err + k, st.kine ? st.kine[c] : 0.0);
   for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
 }
 
@@ -471,22 +474,28 @@ __device__ inline void block_inverse(double* A, double* Ai) {
   }
 }
 
-template <typename BT, int KIND, int VISC>
+// CL lanes per cell: lane l of a cell evaluates the cell's face slots l,
+// l+CL, ...; each lane accumulates its own partial diagonal block (shared
+// memory) and residual, summed over the lanes in a fixed order.  Two lanes
+// per cell halve the dependent chain of each thread and give the scheduler
+// twice the warps to balance over the SMs (a one-wave-and-a-bit grid at the
+// register-limited occupancy otherwise leaves most SMs idle in its tail).
+template <typename BT, int KIND, int VISC, int CL>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
   // FP32 for the mixed form's preconditioner (the residual is FP64 in both)
   using JT = BT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  JT* sD = reinterpret_cast<JT*>(smem_raw);  // [25][blockDim.x] diagonal-block accumulators
-  __shared__ double sres[5][128];
+  JT* sD = reinterpret_cast<JT*>(smem_raw);  // [25][blockDim.x] partial diagonal blocks, one per thread
   const int t = threadIdx.x, bd = blockDim.x;
-  int c = blockIdx.x * bd + t;
+  const int lane = t % CL;
+  int c = blockIdx.x * (bd / CL) + t / CL;
   bool active = c < m.ncv;
   double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (active) {
     for (int e = 0; e < 25; e++) sD[e * bd + t] = JT(0);
     BT* O = (BT*)st.O;
-    for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+    for (int k = m.slot_i[c] + lane; k < m.slot_i[c + 1]; k += CL) {
       const Slot s = m.slots[k];
       const int f = s.f;
       double nV[3], area;
@@ -619,11 +628,27 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         }
       }
     }
-    // ---------------- epilogue ----------------
+  }
+  // ---------------- epilogue ----------------
+  // the lanes' partial residuals and diagonal blocks, summed in lane order (lanes of a cell share
+  // its activity, so the whole warp reaches the shuffles)
+  if (CL > 1) {
+    for (int i = 0; i < 5; i++) {
+      double tot = 0.0;
+      for (int l = 0; l < CL; l++) tot += __shfl_sync(0xffffffffu, rhs[i], (t & 31) - lane + l);
+      rhs[i] = tot;
+    }
+    __syncwarp();
+  }
+  if (active && lane == 0) {
     for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
     if (implicit) {
       double Dm[25];
-      for (int e = 0; e < 25; e++) Dm[e] = (double)sD[e * bd + t];
+      for (int e = 0; e < 25; e++) {
+        JT d = sD[e * bd + t];
+        for (int l = 1; l < CL; l++) d += sD[e * bd + t + l];
+        Dm[e] = (double)d;
+      }
       if (for_step) {
         double tmp = m.vol[c] / st.local_dt[c];
         for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;
@@ -638,18 +663,6 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         for (int e = 0; e < 25; e++) Dig[(size_t)e * m.ncv + c] = (BT)Di[e];
       }
     }
-  }
-  // residual partial sums (|RHS|, runBackwardEuler JoeWithModels.cpp:1125-1136), fixed order
-  if (for_step) {
-    for (int i = 0; i < 5; i++) sres[i][t] = active ? fabs(rhs[i]) : 0.0;
-    __syncthreads();
-    for (int w = bd / 2; w > 0; w >>= 1) {
-      if (t < w)
-        for (int i = 0; i < 5; i++) sres[i][t] += sres[i][t + w];
-      __syncthreads();
-    }
-    if (t == 0)
-      for (int i = 0; i < 5; i++) st.blk[5 * blockIdx.x + i] = sres[i][0];
   }
 }
 
@@ -1210,11 +1223,13 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
   else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
+constexpr int FLUX_CL = 2;  // lanes per cell of the implicit face loop
 template <typename BT, int KIND>
 static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
   size_t shm = 25 * TB * sizeof(BT);
-  if (p.viscous) k_flux<BT, KIND, 1><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
-  else k_flux<BT, KIND, 0><<<grid_for(m.ncv, TB), TB, shm, s>>>(m, p, st, 1, for_step);
+  const int g = grid_for(m.ncv, TB / FLUX_CL);
+  if (p.viscous) k_flux<BT, KIND, 1, FLUX_CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+  else k_flux<BT, KIND, 0, FLUX_CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
 }
 template <typename BT>
 static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {

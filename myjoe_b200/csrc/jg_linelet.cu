@@ -6,7 +6,11 @@
 // BiCGSTAB whose preconditioner solves the block-tridiagonal system of each
 // line exactly (block Thomas elimination) and the block diagonal elsewhere.
 //
-// Here the lines are built once per handle on the host.  On the device the
+// Here the lines are built once per handle on the host.  The LINE relaxation
+// (below) uses the same rule with one relaxation: where several neighbours
+// pass, the line goes on to the strongest if it is 1.1 times the next one,
+// so that a line crosses from the last prism row into the hexahedron above
+// (whose other lower neighbour is the quad's second prism).  On the device the
 // elimination is split in two: k_line_factor runs once per linear solve (the
 // matrix does not change inside BiCGSTAB) and keeps, per line cell, the
 // inverse of the eliminated diagonal block, the multiplier
@@ -46,7 +50,7 @@ double coupling(const jg_mesh& m, int a, int b) {
 }  // namespace
 
 int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zones, std::vector<int>& off,
-                std::vector<int>& cv) {
+                std::vector<int>& cv, bool relaxed) {
   const int N = m.ncv;
   std::vector<char> free_cv(N, 1);
   // each WALL zone replaces the sources of the one before it; all of their cells leave the pool
@@ -68,17 +72,26 @@ int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zone
       double wmax = 0.0;
       for (int k = m.nbocv_i[icv] + 1; k < m.nbocv_i[icv + 1]; k++)
         wmax = std::max(wmax, coupling(m, icv, m.nbocv_v[k]));
-      // the one free neighbour (not the cell the line came from) with more than half the largest coupling
+      // the one free neighbour (not the cell the line came from) with more than half the largest
+      // coupling; relaxed: or, among several, the strongest when it is 1.1 times the next one
       int next = -1, count = 0;
+      double best_w = 0.0, second_w = 0.0;
       const int prev = cv.size() - first >= 2 ? cv[cv.size() - 2] : -1;
       for (int k = m.nbocv_i[icv] + 1; k < m.nbocv_i[icv + 1]; k++) {
         const int nb = m.nbocv_v[k];
-        if (free_cv[nb] && coupling(m, icv, nb) / wmax > 0.5 && nb != prev) {
-          next = nb;
+        const double w = coupling(m, icv, nb);
+        if (free_cv[nb] && w / wmax > 0.5 && nb != prev) {
           count++;
+          if (w > best_w) {
+            second_w = best_w;
+            best_w = w;
+            next = nb;
+          } else if (w > second_w) {
+            second_w = w;
+          }
         }
       }
-      if (count != 1) break;  // no candidate, or an isotropic region
+      if (count == 0 || (count > 1 && !(relaxed && best_w > 1.1 * second_w))) break;
       cv.push_back(next);
       free_cv[next] = 0;
     }

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import types
 
 import numpy as np
 
@@ -63,6 +64,8 @@ def lib():
         L.jg_batch_create.argtypes = [I, C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
         L.jg_batch_info.argtypes = [P, C.POINTER(I), C.POINTER(I)]
         L.jg_batch_set_state.argtypes = [P, I, D, D, D]
+        L.jg_batch_set_scalars.argtypes = [P, I, D]
+        L.jg_batch_get_scalars.argtypes = [P, I, D]
         L.jg_batch_get_state.argtypes = [P, I, D, D, D]
         L.jg_batch_step.argtypes = [P, I, D]
         L.jg_batch_status.argtypes = [P, C.POINTER(I)]
@@ -278,13 +281,20 @@ def euler_flux_faces(kind, L, R, area, nvec, matrices=True):
 class JoeGpuBatch(JoeGpu):
     """Many independent cases advanced together (jg_batch_create): one launch
     per stage over all cases.  ``cases`` is a list of (mesh, JoeParams); the
-    solver settings (flux, precision, linear solver, CFL ramp) come from the
-    first case, the boundary values from each case's own parameters."""
+    cases share one jg_params (the fluid: gamma, R, viscosity law and MU_REF,
+    Pr; the solver settings: flux, linear solver, CFL ramp, turbulence model)
+    and each brings its own boundary values.  Cases whose shared settings
+    differ (two fluids, say) are refused."""
 
     def __init__(self, cases, precision: int = 0):
         self.params = cases[0][1]
         self.mas = [MeshArrays(m, p) for m, p in cases]
         self.jp = make_params(self.params, precision)
+        for k, (_, prm) in enumerate(cases[1:], 1):
+            q = make_params(prm, precision)
+            diff = [f for f, _ in jg_params._fields_ if getattr(q, f) != getattr(self.jp, f)]
+            if diff:
+                raise ValueError("case %d differs from case 0 in the batch-wide settings %s" % (k, diff))
         arr = (jg_mesh * len(cases))(*[ma.mesh for ma in self.mas])
         h = C.c_void_p()
         _ck(lib().jg_batch_create(len(cases), arr, C.byref(self.jp), C.byref(h)))
@@ -292,6 +302,10 @@ class JoeGpuBatch(JoeGpu):
         self.ncases = len(cases)
         self.sizes = [ma.ncv for ma in self.mas]
         self.ncv = sum(self.sizes)
+        # the concatenated system's sizes (the single-case calls of the base class use them)
+        self.ma = types.SimpleNamespace(ncv=self.ncv, nfa=sum(ma.nfa for ma in self.mas),
+                                        nfa_b=sum(ma.nfa_b for ma in self.mas),
+                                        nbocv_s=sum(ma.nbocv_s for ma in self.mas))
 
     def set_case_state(self, k, rho, rhou, rhoE):
         rho, rhou, rhoE = (np.ascontiguousarray(a, np.float64) for a in (rho, rhou, rhoE))
@@ -303,6 +317,17 @@ class JoeGpuBatch(JoeGpu):
         _ck(lib().jg_batch_get_state(self.h, int(k), dptr(rho), dptr(rhou), dptr(rhoE)))
         return rho, rhou, rhoE
 
+    def set_case_scalars(self, k, phi):
+        """case k's transported scalars, phi[ncv_k] (SA) or phi[ncv_k][2] (SST)"""
+        phi = np.ascontiguousarray(np.asarray(phi, np.float64).reshape(self.sizes[k], self.params.nscal))
+        _ck(lib().jg_batch_set_scalars(self.h, int(k), dptr(phi)))
+
+    def get_case_scalars(self, k):
+        ns = self.params.nscal
+        phi = np.empty((self.sizes[k], ns))
+        _ck(lib().jg_batch_get_scalars(self.h, int(k), dptr(phi)))
+        return phi[:, 0] if ns == 1 else phi
+
     def status(self):
         st = (C.c_int * self.ncases)()
         _ck(lib().jg_batch_status(self.h, st))
@@ -312,8 +337,8 @@ class JoeGpuBatch(JoeGpu):
         _ck(lib().jg_batch_set_active(self.h, int(k), int(bool(active))))
 
     def runBackwardEulerCases(self, nsteps):
-        """residuals [nsteps][ncases][5]"""
-        r = np.zeros((max(nsteps, 1), self.ncases, 5))
+        """residuals [nsteps][ncases][5 + nscal]"""
+        r = np.zeros((max(nsteps, 1), self.ncases, self.nvar))
         _ck(lib().jg_batch_step(self.h, int(nsteps), dptr(r)))
         return r[:nsteps]
 

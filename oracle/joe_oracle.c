@@ -35,6 +35,8 @@ struct jo_case {
   int nlines;       /* linelets (initializeLinelet): cells line_cv[line_off[l] .. line_off[l+1]) */
   int *line_off, *line_cv;
   unsigned char *linelet;  /* [N] the reference's Linelet flag: the cell is on a line of >= 2 cells */
+  int rnlines;      /* the LINE relaxation's lines (crossing prism/hexahedron interfaces) */
+  int *rline_off, *rline_cv;
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -84,6 +86,8 @@ void jo_destroy(jo_case *h) {
   free(h->line_off);
   free(h->line_cv);
   free(h->linelet);
+  free(h->rline_off);
+  free(h->rline_cv);
   free(h);
 }
 
@@ -1342,8 +1346,12 @@ static int find_face(const jg_mesh *m, int a, int b) {
  * zone's cells are taken out of later lines.  From each source a line grows
  * to the one unused neighbour (not the cell it came from) whose weight
  * 0.5 |A_f| (1/V_cell + 1/V_nb) exceeds half the cell's largest neighbour
- * weight; two or more candidates (an isotropic region) or none end it. */
-void jo_build_linelets(jo_case *h) {
+ * weight; two or more candidates (an isotropic region) or none end it.
+ * With `relaxed` (the lines of the LINE relaxation, not the reference's), a
+ * line also goes on when several candidates pass but the strongest is more
+ * than 1.1 times the next: so it crosses from a prism row into the hexahedron
+ * above, whose other lower neighbour is the second prism of the quad. */
+static void build_lines(jo_case *h, int relaxed, int *nlines_out, int **off_out, int **cv_out) {
   const jg_mesh *m = &h->m;
   const int N = h->ncv;
   unsigned char *check = (unsigned char *)malloc(N ? N : 1);
@@ -1378,7 +1386,8 @@ void jo_build_linelets(jo_case *h) {
         max_weight = dmax(max_weight, w);
       }
       add = 0;
-      int counter = 0, next_cv = -1;
+      int counter = 0, next_cv = -1, best = -1;
+      double best_w = 0.0, second_w = 0.0;
       for (int k = m->nbocv_i[icv] + 1; k < m->nbocv_i[icv + 1]; k++) {
         int ino = m->nbocv_v[k];
         int f = find_face(m, icv, ino);
@@ -1388,9 +1397,19 @@ void jo_build_linelets(jo_case *h) {
           add = 1;
           next_cv = ino;
           counter++;
+          if (w > best_w) {
+            second_w = best_w;
+            best_w = w;
+            best = ino;
+          } else if (w > second_w) {
+            second_w = w;
+          }
         }
       }
-      if (counter > 1) add = 0;
+      if (counter > 1) {
+        add = relaxed && best_w > 1.1 * second_w;
+        next_cv = best;
+      }
       if (add) {
         if (len + 1 > cap) { cap *= 2; cv = (int *)realloc(cv, sizeof(int) * cap); }
         cv[len++] = next_cv;
@@ -1400,16 +1419,28 @@ void jo_build_linelets(jo_case *h) {
     } while (add);
     off[l + 1] = len;
   }
-  free(h->line_off); free(h->line_cv); free(h->linelet);
-  h->nlines = nsrc;
-  h->line_off = off;
-  h->line_cv = cv;
-  h->linelet = (unsigned char *)calloc(N ? N : 1, 1);
-  for (int l = 0; l < nsrc; l++)
-    if (off[l + 1] - off[l] >= 2)
-      for (int i = off[l]; i < off[l + 1]; i++) h->linelet[cv[i]] = 1;
+  *nlines_out = nsrc;
+  *off_out = off;
+  *cv_out = cv;
   free(src);
   free(check);
+}
+
+void jo_build_linelets(jo_case *h) {
+  free(h->line_off); free(h->line_cv); free(h->linelet);
+  build_lines(h, 0, &h->nlines, &h->line_off, &h->line_cv);
+  const int N = h->ncv;
+  h->linelet = (unsigned char *)calloc(N ? N : 1, 1);
+  for (int l = 0; l < h->nlines; l++)
+    if (h->line_off[l + 1] - h->line_off[l] >= 2)
+      for (int i = h->line_off[l]; i < h->line_off[l + 1]; i++) h->linelet[h->line_cv[i]] = 1;
+}
+
+int jo_relax_lines(jo_case *h, int *off, int *cv) {
+  if (!h->rline_off) build_lines(h, 1, &h->rnlines, &h->rline_off, &h->rline_cv);
+  if (off) memcpy(off, h->rline_off, sizeof(int) * (h->rnlines + 1));
+  if (cv) memcpy(cv, h->rline_cv, sizeof(int) * h->rline_off[h->rnlines]);
+  return h->rnlines;
 }
 
 int jo_linelets(jo_case *h, int *off, int *cv) {
@@ -2726,27 +2757,27 @@ static void lusolv_n(const double *A, double *c, int n) {
 
 /* LINE relaxation as the GPU runs it (no reference counterpart): `sweeps`
  * block line-Jacobi sweeps of the B x B system from x = 0.  On the lines of
- * initializeLinelet (two or more cells) the block-tridiagonal system is
+ * build_lines' relaxed rule (two or more cells) the block-tridiagonal system is
  * solved exactly by block Thomas elimination; the other cells take a block
  * Jacobi step; every coupling that is not between line neighbours uses the
  * previous sweep's x. */
 int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *rhs, int sweeps) {
   const jg_mesh *m = &h->m;
   const int n = h->ncv, BB = B * B;
-  if (!h->line_off) jo_build_linelets(h);
+  if (!h->rline_off) build_lines(h, 1, &h->rnlines, &h->rline_off, &h->rline_cv);
   int *prev = (int *)malloc(sizeof(int) * n), *next = (int *)malloc(sizeof(int) * n);
   char *on = (char *)calloc(n, 1);
   for (int c = 0; c < n; c++) prev[c] = next[c] = -1;
   int ncl = 0;
-  for (int l = 0; l < h->nlines; l++) {
-    int a = h->line_off[l], b = h->line_off[l + 1];
+  for (int l = 0; l < h->rnlines; l++) {
+    int a = h->rline_off[l], b = h->rline_off[l + 1];
     if (b - a < 2) continue;
     for (int k = a; k < b; k++) {
-      int c = h->line_cv[k];
+      int c = h->rline_cv[k];
       on[c] = 1;
       ncl++;
-      if (k > a) prev[c] = h->line_cv[k - 1];
-      if (k + 1 < b) next[c] = h->line_cv[k + 1];
+      if (k > a) prev[c] = h->rline_cv[k - 1];
+      if (k + 1 < b) next[c] = h->rline_cv[k + 1];
     }
   }
   double *LU = dalloc((size_t)BB * n), *xn = dalloc((size_t)B * n), *r = dalloc((size_t)B * n);
@@ -2757,12 +2788,12 @@ int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *r
   }
   /* line factors: inv_i of the eliminated diagonal, low_i = A(c_i, c_{i-1}) inv_{i-1}, indexed by cell */
   double bh[MAXB * MAXB], lu[MAXB * MAXB], col[MAXB];
-  for (int l = 0; l < h->nlines; l++) {
-    int a = h->line_off[l], b = h->line_off[l + 1];
+  for (int l = 0; l < h->rnlines; l++) {
+    int a = h->rline_off[l], b = h->rline_off[l + 1];
     if (b - a < 2) continue;
-    memcpy(bh, &A[(size_t)BB * m->nbocv_i[h->line_cv[a]]], sizeof(double) * BB);
+    memcpy(bh, &A[(size_t)BB * m->nbocv_i[h->rline_cv[a]]], sizeof(double) * BB);
     for (int k = a; k < b; k++) {
-      int c = h->line_cv[k];
+      int c = h->rline_cv[k];
       memcpy(lu, bh, sizeof(double) * BB);
       ludeco_n(lu, B);
       for (int j = 0; j < B; j++) {
@@ -2771,7 +2802,7 @@ int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *r
         for (int i = 0; i < B; i++) inv[(size_t)BB * c + B * i + j] = col[i];
       }
       if (k + 1 == b) break;
-      int cn = h->line_cv[k + 1];
+      int cn = h->rline_cv[k + 1];
       const double *Alo = &A[(size_t)BB * csr_entry(m, cn, c)];
       const double *Aup = &A[(size_t)BB * csr_entry(m, c, cn)];
       for (int i = 0; i < B; i++)
@@ -2805,25 +2836,25 @@ int jo_line_relax(jo_case *h, int B, double *x, const double *A, const double *r
         lusolv_n(&LU[(size_t)BB * c], &xn[(size_t)B * c], B);
       }
     }
-    for (int l = 0; l < h->nlines; l++) {
-      int a = h->line_off[l], b = h->line_off[l + 1];
+    for (int l = 0; l < h->rnlines; l++) {
+      int a = h->rline_off[l], b = h->rline_off[l + 1];
       if (b - a < 2) continue;
       for (int k = a; k < b; k++) {
-        int c = h->line_cv[k];
+        int c = h->rline_cv[k];
         for (int i = 0; i < B; i++) {
           double t = 0.0;
           if (k > a)
-            for (int q = 0; q < B; q++) t += low[(size_t)BB * c + B * i + q] * vv[(size_t)B * h->line_cv[k - 1] + q];
+            for (int q = 0; q < B; q++) t += low[(size_t)BB * c + B * i + q] * vv[(size_t)B * h->rline_cv[k - 1] + q];
           vv[(size_t)B * c + i] = r[(size_t)B * c + i] - t;
         }
       }
       for (int k = b - 1; k >= a; k--) {
-        int c = h->line_cv[k];
+        int c = h->rline_cv[k];
         double a1[MAXB];
         for (int i = 0; i < B; i++) {
           double t = 0.0;
           if (k + 1 < b) {
-            int cn = h->line_cv[k + 1];
+            int cn = h->rline_cv[k + 1];
             const double *Aup = &A[(size_t)BB * csr_entry(m, c, cn)];
             for (int q = 0; q < B; q++) t += Aup[B * i + q] * xn[(size_t)B * cn + q];
           }

@@ -33,6 +33,8 @@ double *jo_array(jo_case *h, const char *name);
 /* initializeLinelet's lines: off[nlines+1], cv[off[nlines]]; returns nlines (NULL arrays: count only) */
 int jo_linelets(jo_case *h, int *off, int *cv);
 void jo_build_linelets(jo_case *h);
+/* the lines of the LINE relaxation (initializeLinelet's rule, crossing prism/hexahedron interfaces) */
+int jo_relax_lines(jo_case *h, int *off, int *cv);
 double jo_cfl(jo_case *h);
 int jo_step_count(jo_case *h);
 

@@ -61,6 +61,8 @@ def lib():
         L.jo_sa_release.argtypes = [P]
         L.jo_linelets.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.jo_line_relax.argtypes = [P, C.c_int, D, D, D, C.c_int]
+        L.jo_relax_lines.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.jo_relax_lines.restype = C.c_int
         L.jo_linelets.restype = C.c_int
         _lib = L
     return _lib
@@ -135,6 +137,15 @@ class Oracle:
         lib().jo_linelets(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), None)
         cv = np.zeros(max(int(off[-1]), 1), np.int32)
         lib().jo_linelets(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), cv.ctypes.data_as(C.POINTER(C.c_int)))
+        return off, cv[:off[-1]]
+
+    def relax_lines(self):
+        """the LINE relaxation's lines: (off[nlines+1], cells)"""
+        n = lib().jo_relax_lines(self.h, None, None)
+        off = np.zeros(n + 1, np.int32)
+        lib().jo_relax_lines(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), None)
+        cv = np.zeros(max(int(off[-1]), 1), np.int32)
+        lib().jo_relax_lines(self.h, off.ctypes.data_as(C.POINTER(C.c_int)), cv.ctypes.data_as(C.POINTER(C.c_int)))
         return off, cv[:off[-1]]
 
     def step(self, nsteps=1):

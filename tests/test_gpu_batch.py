@@ -75,3 +75,71 @@ def test_diverging_case_is_retired_without_disturbing_the_batch():
             np.testing.assert_array_equal(a, c)
     assert np.all(np.isfinite(r[:, 1:, :]))
     b.close()
+
+
+def turb_cases(model):
+    make = case.sa_bump_case if model == "sa" else case.sst_bump_case
+    out = []
+    for k, (nx, ny, npr, mach, bump) in enumerate([(24, 12, 0, 0.5, 0.08), (32, 16, 4, 0.6, 0.05),
+                                                   (16, 10, 0, 0.4, 0.1)]):
+        # one fluid for the whole batch: Re grows with the Mach number at a fixed viscosity
+        _, g, prm = make(nx, ny, 2, mach=mach, mu_ref=2.0e-3, bump_h=bump, stretch=1.15, jitter=0.05, seed=k,
+                         n_prism=npr, alternate=True)
+        prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=1.0, CFL_RAMP=(3, 2, 1.2, 10.0))
+        out.append((g, prm))
+    return out
+
+
+def _phi0(g, prm):
+    vals = [prm.NUSA_INITIAL] if prm.TURB_MODEL == "SA" else [prm.KINE_INITIAL, prm.OMEGA_INITIAL]
+    return np.stack([case.perturbed_scalar(g.x_cv, v, 0.05) for v in vals], 1)
+
+
+@pytest.mark.parametrize("model", ["sa", "sst"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_turbulence_batch_is_bitwise_equal_to_alone(model, precision):
+    """SA (6x6) and SST (7x7) cases of different sizes, hex and mixed
+    prism/hex meshes, in one batch: per case the state, the transported
+    scalars and the residual history are those of the case run alone (each
+    case's wall distance is taken to its own walls)."""
+    cs = turb_cases(model)
+    nsteps = 10
+    alone = []
+    for g, prm in cs:
+        j = solver.JoeGpu(g, prm, precision=precision)
+        j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
+        j.set_scalars(_phi0(g, prm))
+        wd = j.turb_array("wallDist")
+        r = j.runBackwardEuler(nsteps)
+        alone.append((j.get_state(), j.get_scalars(), r, wd))
+        j.close()
+    b = solver.JoeGpuBatch(cs, precision=precision)
+    for k, (g, prm) in enumerate(cs):
+        b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
+        b.set_case_scalars(k, _phi0(g, prm))
+    wd = b.turb_array("wallDist")
+    off = np.concatenate([[0], np.cumsum(b.sizes)])
+    for k in range(len(cs)):
+        np.testing.assert_array_equal(wd[off[k]:off[k + 1]], alone[k][3])
+    rb = b.runBackwardEulerCases(nsteps)
+    assert rb.shape == (nsteps, len(cs), 5 + cs[0][1].nscal)
+    for k in range(len(cs)):
+        for a, c in zip(b.get_case_state(k), alone[k][0]):
+            np.testing.assert_array_equal(a, c)
+        np.testing.assert_array_equal(b.get_case_scalars(k), alone[k][1])
+        np.testing.assert_array_equal(rb[:, k, :], alone[k][2])
+    # a frozen case keeps its state while the others advance
+    b.set_active(1, False)
+    frozen = b.get_case_state(1)
+    b.runBackwardEulerCases(3)
+    for a, c in zip(b.get_case_state(1), frozen):
+        np.testing.assert_array_equal(a, c)
+    b.close()
+
+
+def test_batch_refuses_cases_with_different_fluids():
+    cs = turb_cases("sa")
+    g, prm = cs[1]
+    cs[1] = (g, dataclasses.replace(prm, MU_REF=2.0 * prm.MU_REF))
+    with pytest.raises(ValueError):
+        solver.JoeGpuBatch(cs)

@@ -58,10 +58,10 @@ enum { JG_LS_BCGSTAB = 0, JG_LS_LUSGS = 1, JG_LS_JACOBI = 2, JG_LS_SGS = 3,
        /* LINE (no reference counterpart; the reference's coupled solve is PETSc): ls_max_iter
         * block line-Jacobi sweeps from zero: the block-tridiagonal system of every line solved
         * exactly (block Thomas), the block diagonal on the other cells, the couplings across
-        * lines lagged.  The lines follow initializeLinelet's rule from the WALL faces, except
-        * that where several neighbours pass a line goes on to the strongest coupling if it is
-        * 1.1 times the next (so it crosses prism/hexahedron interfaces).  5x5 and coupled
-        * paths, FP64 or mixed. */
+        * lines lagged.  The lines follow initializeLinelet's rule from the faces of every
+        * WALL zone, except that where several neighbours pass a line goes on to the strongest
+        * coupling if it is 1.1 times the next (so it crosses prism/hexahedron interfaces).
+        * 5x5 and coupled paths, FP64 or mixed, single cases and batches. */
        JG_LS_LINE = 5 };
 enum { JG_PREC_FP64 = 0, JG_PREC_MIXED = 1 };
 
@@ -221,8 +221,8 @@ int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
  * values, concatenated into one block-diagonal system so that every stage of
  * the iteration is one launch over all cases.  Each case keeps its own
  * residual reduction and never reads another case's data, so its results are
- * bit-identical alone and in any batch.  Linear solver JACOBI, SGS or LUSGS
- * (JACOBI or SGS with a turbulence model); time step CFL or DT.  All cases
+ * bit-identical alone and in any batch.  Linear solver JACOBI, SGS, LINE or
+ * LUSGS (JACOBI, SGS or LINE with a turbulence model); time step CFL or DT.  All cases
  * share one model: none, SA or SST (each case's wall distance is taken to its
  * own WALL faces).  The batch handle accepts every single-case call (jg_step
  * reports the residual summed over the cases). */

@@ -130,6 +130,9 @@ def main(argv=None):
     ap.add_argument("--cfl-ramp", default="10,5,1.2,20",
                     help="CFL_RAMP AFTER_ITER,INTERVAL_ITER,FACTOR_CFL,MAX_CFL")
     ap.add_argument("--under-relax", type=float, default=0.3)
+    ap.add_argument("--sst-solver", default="LINE", choices=["LINE", "SGS", "JACOBI"],
+                    help="relaxation of the SST cases (their wall rows are stretched)")
+    ap.add_argument("--sst-cfl-ramp", default="10,5,1.2,200")
     ap.add_argument("--drop", type=float, default=1e-8)
     ap.add_argument("--max-steps", type=int, default=3000)
     ap.add_argument("--chunk", type=int, default=50)
@@ -148,12 +151,15 @@ def main(argv=None):
     ramp = (int(ra), int(ri), float(rf), float(rm))
     precision = 1 if args.precision == "mixed" else 0
     groups = []
+    sa, si, sf, sm = args.sst_cfl_ramp.split(",")
+    sst_ramp = (int(sa), int(si), float(sf), float(sm))
     for model in ("EULER", "SST"):
         idx = [k for k, sp in enumerate(specs) if sp["model"] == model]
         if not idx:
             continue
-        cases = [(built[k][0], dataclasses.replace(built[k][1], LINEAR_SOLVER_NS=args.solver,
-                                                   LS_MAX_ITER=args.sweeps, CFL=1.0, CFL_RAMP=ramp,
+        solver_name, r = (args.sst_solver, sst_ramp) if model == "SST" else (args.solver, ramp)
+        cases = [(built[k][0], dataclasses.replace(built[k][1], LINEAR_SOLVER_NS=solver_name,
+                                                   LS_MAX_ITER=args.sweeps, CFL=1.0, CFL_RAMP=r,
                                                    UNDER_RELAXATION=args.under_relax)) for k in idx]
         groups.append(Group(model, idx, cases, precision))
     # the handles step concurrently: one host thread each (the C calls release the GIL)
@@ -188,8 +194,10 @@ def main(argv=None):
     nconv = len(all_conv)
     out = {
         "form": "batch", "cases": args.cases, "cells": int(sum(gr.b.ncv for gr in groups)),
-        "precision": args.precision, "solver": "%s x%d" % (args.solver, args.sweeps), "drop": args.drop,
-        "cfl_ramp": list(ramp), "under_relax": args.under_relax, "sst_fraction": args.sst_fraction,
+        "precision": args.precision, "solver": "%s x%d" % (args.solver, args.sweeps),
+        "sst_solver": "%s x%d" % (args.sst_solver, args.sweeps), "drop": args.drop,
+        "cfl_ramp": list(ramp), "sst_cfl_ramp": list(sst_ramp), "under_relax": args.under_relax,
+        "sst_fraction": args.sst_fraction,
         "cell_iters_per_s": cell_iters / wall, "wall_s": wall, "mesh_setup_s": t_mesh,
         "converged": nconv, "failed": int(sum(gr.failed.sum() for gr in groups)),
         "converged_solves_per_hour": nconv / wall * 3600.0,

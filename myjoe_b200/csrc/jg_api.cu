@@ -803,7 +803,6 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
   if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
-  if (params->lin_solver == JG_LS_LINE) return set_err(JG_ERR_ARG, "LINE relaxation runs one case per handle");
   if (params->time_step_mode == JG_TS_CFL_MIN)
     return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
   int ndev = 0;

@@ -53,10 +53,11 @@ int build_lines(const jg_mesh& m, const std::vector<std::vector<int>>& wall_zone
                 std::vector<int>& cv, bool relaxed) {
   const int N = m.ncv;
   std::vector<char> free_cv(N, 1);
-  // each WALL zone replaces the sources of the one before it; all of their cells leave the pool
+  // each WALL zone replaces the sources of the one before it (relaxed: every WALL zone's cells are
+  // sources, so that each case of a batch grows its own lines); all of their cells leave the pool
   std::vector<int> src;
   for (const auto& z : wall_zones) {
-    src.clear();
+    if (!relaxed) src.clear();
     for (int f : z) {
       src.push_back(m.cvofa[2 * f]);
       free_cv[m.cvofa[2 * f]] = 0;

@@ -1347,7 +1347,8 @@ static int find_face(const jg_mesh *m, int a, int b) {
  * to the one unused neighbour (not the cell it came from) whose weight
  * 0.5 |A_f| (1/V_cell + 1/V_nb) exceeds half the cell's largest neighbour
  * weight; two or more candidates (an isotropic region) or none end it.
- * With `relaxed` (the lines of the LINE relaxation, not the reference's), a
+ * With `relaxed` (the lines of the LINE relaxation, not the reference's),
+ * every WALL zone's cells start lines, and a
  * line also goes on when several candidates pass but the strongest is more
  * than 1.1 times the next: so it crosses from a prism row into the hexahedron
  * above, whose other lower neighbour is the second prism of the quad. */
@@ -1359,10 +1360,11 @@ static void build_lines(jo_case *h, int relaxed, int *nlines_out, int **off_out,
   int nsrc = 0, *src = NULL;
   for (int z = 0; z < m->nzones; z++) {
     if (m->zones[z].kind != JG_BC_WALL) continue;
-    free(src);
-    nsrc = m->zones[z].ifa_l - m->zones[z].ifa_f + 1;
-    src = (int *)malloc(sizeof(int) * (nsrc ? nsrc : 1));
-    for (int f = m->zones[z].ifa_f, i = 0; f <= m->zones[z].ifa_l; f++, i++) {
+    int nz = m->zones[z].ifa_l - m->zones[z].ifa_f + 1;
+    int base = relaxed ? nsrc : 0;  /* relaxed: every WALL zone's cells are sources */
+    src = (int *)realloc(src, sizeof(int) * (base + nz + 1));
+    nsrc = base + nz;
+    for (int f = m->zones[z].ifa_f, i = base; f <= m->zones[z].ifa_l; f++, i++) {
       src[i] = m->cvofa[2 * f];
       check[src[i]] = 0;
     }

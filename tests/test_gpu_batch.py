@@ -77,7 +77,7 @@ def test_diverging_case_is_retired_without_disturbing_the_batch():
     b.close()
 
 
-def turb_cases(model):
+def turb_cases(model, solver_name="SGS"):
     make = case.sa_bump_case if model == "sa" else case.sst_bump_case
     out = []
     for k, (nx, ny, npr, mach, bump) in enumerate([(24, 12, 0, 0.5, 0.08), (32, 16, 4, 0.6, 0.05),
@@ -85,7 +85,8 @@ def turb_cases(model):
         # one fluid for the whole batch: Re grows with the Mach number at a fixed viscosity
         _, g, prm = make(nx, ny, 2, mach=mach, mu_ref=2.0e-3, bump_h=bump, stretch=1.15, jitter=0.05, seed=k,
                          n_prism=npr, alternate=True)
-        prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=1.0, CFL_RAMP=(3, 2, 1.2, 10.0))
+        prm = dataclasses.replace(prm, LINEAR_SOLVER_NS=solver_name, LS_MAX_ITER=6, CFL=1.0,
+                                  CFL_RAMP=(3, 2, 1.2, 10.0))
         out.append((g, prm))
     return out
 
@@ -95,14 +96,15 @@ def _phi0(g, prm):
     return np.stack([case.perturbed_scalar(g.x_cv, v, 0.05) for v in vals], 1)
 
 
-@pytest.mark.parametrize("model", ["sa", "sst"])
+@pytest.mark.parametrize("model,solver_name", [("sa", "SGS"), ("sst", "SGS"), ("sa", "LINE"), ("sst", "LINE")])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_turbulence_batch_is_bitwise_equal_to_alone(model, precision):
+def test_turbulence_batch_is_bitwise_equal_to_alone(model, solver_name, precision):
     """SA (6x6) and SST (7x7) cases of different sizes, hex and mixed
-    prism/hex meshes, in one batch: per case the state, the transported
+    prism/hex meshes, in one batch, relaxed by SGS or LINE (every case grows
+    its own lines from its own walls): per case the state, the transported
     scalars and the residual history are those of the case run alone (each
     case's wall distance is taken to its own walls)."""
-    cs = turb_cases(model)
+    cs = turb_cases(model, solver_name)
     nsteps = 10
     alone = []
     for g, prm in cs:

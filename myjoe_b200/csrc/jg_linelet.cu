@@ -299,9 +299,8 @@ __device__ void lu_inverse_col(const double* M, int col, double* out) {
       for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jr + jm] * A[B * jm + jrjc];
       A[B * jr + jrjc] = sum;
     }
-    if (jrjc == B - 1) break;
 #pragma unroll
-    for (int jc = jrjc + 1; jc < B; jc++) {
+    for (int jc = jrjc + 1; jc < B; jc++) {  // empty on the last row
       double sum = A[B * jrjc + jc];
 #pragma unroll
       for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jrjc + jm] * A[B * jm + jc];
@@ -444,6 +443,9 @@ __global__ void __launch_bounds__(B * 32) k_lrelax_rhs(Mesh m, State st, Lines L
 // x (cells of a line) = T_line^-1 r, r read from x; one warp per line, lanes < B hold the rows
 template <typename BT, int B>
 __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restrict__ x) {
+  // The chain along a line is serial; the operands of step i+1 (a matrix row,
+  // the cell id, the right-hand side) do not depend on it, so each is loaded
+  // one step ahead to overlap its latency with the current step.
   constexpr int BB = B * B;
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int line = blockIdx.x * LW + w;
@@ -456,33 +458,77 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
   const BT* Llow = (const BT*)L.blow;
   const BT* Lup = (const BT*)L.bup;
   BT* Lv = (BT*)L.bv;
+  // forward: v_0 = r_0, v_i = r_i - low_i v_{i-1}
   BT v = x[r * N + L.cv[p0]];
   if (row) Lv[(size_t)p0 * B + r] = v;
+  BT mn[B], xn = 0;
+  if (n > 1) {
+#pragma unroll
+    for (int q = 0; q < B; q++) mn[q] = Llow[(size_t)(p0 + 1) * BB + B * r + q];
+    xn = x[r * N + L.cv[p0 + 1]];
+  }
   for (int i = 1; i < n; i++) {
-    const BT* Mi = &Llow[(size_t)(p0 + i) * BB + B * r];
+    BT mi[B];
+#pragma unroll
+    for (int q = 0; q < B; q++) mi[q] = mn[q];
+    const BT xi = xn;
+    if (i + 1 < n) {
+#pragma unroll
+      for (int q = 0; q < B; q++) mn[q] = Llow[(size_t)(p0 + i + 1) * BB + B * r + q];
+      xn = x[r * N + L.cv[p0 + i + 1]];
+    }
     BT s = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s += Mi[q] * __shfl_sync(0xffffffffu, v, q);
-    v = x[r * N + L.cv[p0 + i]] - s;
+    for (int q = 0; q < B; q++) s += mi[q] * __shfl_sync(0xffffffffu, v, q);
+    v = xi - s;
     if (row) Lv[(size_t)(p0 + i) * B + r] = v;
   }
-  const BT* I = &Linv[(size_t)(p0 + n - 1) * BB + B * r];
+  // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - up_{i+1} y_{i+1})
   BT yv = 0;
+  {
+    const BT* I = &Linv[(size_t)(p0 + n - 1) * BB + B * r];
 #pragma unroll
-  for (int q = 0; q < B; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
+    for (int q = 0; q < B; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
+  }
   if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
+  BT un[B], in[B], vn = 0;
+  int cn = 0;
+  if (n > 1) {
+#pragma unroll
+    for (int q = 0; q < B; q++) {
+      un[q] = Lup[(size_t)(p0 + n - 1) * BB + B * r + q];
+      in[q] = Linv[(size_t)(p0 + n - 2) * BB + B * r + q];
+    }
+    vn = Lv[(size_t)(p0 + n - 2) * B + r];
+    cn = L.cv[p0 + n - 2];
+  }
   for (int i = n - 2; i >= 0; i--) {
-    const BT* U = &Lup[(size_t)(p0 + i + 1) * BB + B * r];
+    BT ui[B], ii[B];
+#pragma unroll
+    for (int q = 0; q < B; q++) {
+      ui[q] = un[q];
+      ii[q] = in[q];
+    }
+    const BT vi = vn;
+    const int ci = cn;
+    if (i > 0) {
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        un[q] = Lup[(size_t)(p0 + i) * BB + B * r + q];
+        in[q] = Linv[(size_t)(p0 + i - 1) * BB + B * r + q];
+      }
+      vn = Lv[(size_t)(p0 + i - 1) * B + r];
+      cn = L.cv[p0 + i - 1];
+    }
     BT s2 = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s2 += U[q] * __shfl_sync(0xffffffffu, yv, q);
-    const BT a1 = Lv[(size_t)(p0 + i) * B + r] - s2;
-    const BT* Ii = &Linv[(size_t)(p0 + i) * BB + B * r];
+    for (int q = 0; q < B; q++) s2 += ui[q] * __shfl_sync(0xffffffffu, yv, q);
+    const BT a1 = vi - s2;
     BT s = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s += Ii[q] * __shfl_sync(0xffffffffu, a1, q);
+    for (int q = 0; q < B; q++) s += ii[q] * __shfl_sync(0xffffffffu, a1, q);
     yv = s;
-    if (row) x[r * N + L.cv[p0 + i]] = yv;
+    if (row) x[r * N + ci] = yv;
   }
 }
 

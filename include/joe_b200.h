@@ -243,6 +243,20 @@ int jg_batch_status(jg_case_t *h, int *status);
 /* freeze (0) or resume (1) a case: a frozen case keeps its state (retired) */
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
+/* Launch shapes (no reference counterpart): the lanes per cell of the 5x5
+ * face loop (1, 2 or 4; default 2) and the kernel of the 5x5 Jacobi sweep (0:
+ * a block per 32-cell slice, a thread per block row, the default; 1: a thread
+ * per cell).  jg_autotune times each candidate on the handle's own mesh
+ * (trials launches, CUDA events) and keeps the fastest; ms[5] (may be NULL)
+ * gets the face loop time per launch for 1, 2, 4 lanes and the sweep time for
+ * kernels 0, 1.  The sweep kernels give bit-identical results; the lanes per
+ * cell change the order of each cell's diagonal-block and residual sums
+ * (rounding-level differences).  Handles without a turbulence model; others
+ * keep their single shape.  A batch handle tunes for all its cases. */
+int jg_set_launch_config(jg_case_t *h, int flux_cl, int relax_variant);
+int jg_get_launch_config(jg_case_t *h, int *flux_cl, int *relax_variant);
+int jg_autotune(jg_case_t *h, int trials, int *flux_cl, int *relax_variant, float *ms);
+
 /* Device bytes jg_create + jg_set_state allocate for a case (exact, before
  * creating it) and the bytes a live handle holds. */
 int jg_case_footprint(const jg_mesh *mesh, const jg_params *params, double *bytes);

@@ -10,7 +10,8 @@ cell layers in z), inflow Mach uniform on 0.3-0.8, angle of attack uniform on
 (one fluid: Re on the bump chord 1e6 x Mach / 0.55, rows stretched towards
 the wall, 7x7 coupled blocks), the rest inviscid HLLC (5x5).  The cases of each model run in one
 jg_batch handle (one launch per stage over all its cases, CUDA graph per
-step); the two handles step concurrently on their own streams until every
+step, launch shapes autotuned on the batch: jg_autotune); the two handles
+step concurrently on their own streams until every
 case reaches the residual drop.  Prints one JSON line: cell-iters/s over all
 cases, converged solves/hour, per-case steps and time-to-converge percentiles,
 per model.
@@ -133,6 +134,7 @@ def main(argv=None):
     ap.add_argument("--sst-solver", default="LINE", choices=["LINE", "SGS", "JACOBI"],
                     help="relaxation of the SST cases (their wall rows are stretched)")
     ap.add_argument("--sst-cfl-ramp", default="10,5,1.2,200")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--drop", type=float, default=1e-8)
     ap.add_argument("--max-steps", type=int, default=3000)
     ap.add_argument("--chunk", type=int, default=50)
@@ -161,7 +163,9 @@ def main(argv=None):
         cases = [(built[k][0], dataclasses.replace(built[k][1], LINEAR_SOLVER_NS=solver_name,
                                                    LS_MAX_ITER=args.sweeps, CFL=1.0, CFL_RAMP=r,
                                                    UNDER_RELAXATION=args.under_relax)) for k in idx]
-        groups.append(Group(model, idx, cases, precision))
+        gr = Group(model, idx, cases, precision)
+        gr.shape = None if args.no_autotune else gr.b.autotune(3)
+        groups.append(gr)
     # the handles step concurrently: one host thread each (the C calls release the GIL)
     from concurrent.futures import ThreadPoolExecutor
     t_run = time.perf_counter()
@@ -183,6 +187,7 @@ def main(argv=None):
         all_ttc.extend(ttc.tolist())
         per_model[gr.name] = {
             "cases": len(gr.idx), "cells": int(gr.b.ncv), "steps": gr.steps, "ms_per_step": step_ms,
+            "launch_shape": gr.shape,
             "cell_iters_per_s_alone_on_stream": gr.b.ncv / (step_ms / 1000.0),
             "converged": int(done.sum()), "failed": int(gr.failed.sum()),
             "failed_cases": [dict(specs[gr.idx[k]], cells=int(gr.b.sizes[k]))

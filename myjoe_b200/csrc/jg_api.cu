@@ -241,6 +241,8 @@ static Params make_params(const jg_params& q) {
   p.under_relax = q.under_relax;
   p.viscous = q.mu_ref > 0.0;
   p.fp32 = q.precision == JG_PREC_MIXED;
+  p.flux_cl = 2;
+  p.relax_variant = 0;
   return p;
 }
 
@@ -1671,6 +1673,91 @@ extern "C" int jg_get_profile(jg_case_t* h, double* ms) {
   CK(cudaEventElapsedTime(&b, h->ev[2], h->ev[3]));
   ms[0] = a;
   ms[1] = b;
+  return JG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch shapes: the lanes per cell of the 5x5 face loop and the Jacobi sweep kernel
+// ---------------------------------------------------------------------------
+static void drop_graph(jg_case* h) {
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->graph_sweeps = -1;
+}
+
+extern "C" int jg_set_launch_config(jg_case_t* h, int flux_cl, int relax_variant) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4) return set_err(JG_ERR_ARG, "lanes per cell must be 1, 2 or 4");
+  if (relax_variant != 0 && relax_variant != 1) return set_err(JG_ERR_ARG, "sweep kernel must be 0 or 1");
+  CK(cudaStreamSynchronize(h->stream));
+  h->p.flux_cl = flux_cl;
+  h->p.relax_variant = relax_variant;
+  drop_graph(h);  // the next step captures the new shapes
+  return JG_OK;
+}
+
+extern "C" int jg_get_launch_config(jg_case_t* h, int* flux_cl, int* relax_variant) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (flux_cl) *flux_cl = h->p.flux_cl;
+  if (relax_variant) *relax_variant = h->p.relax_variant;
+  return JG_OK;
+}
+
+// Times every candidate shape on the handle's own mesh and state (trials
+// launches each, CUDA events on the case stream) and keeps the fastest.  The
+// timed launches only overwrite work arrays that the next step recomputes.
+extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_variant, float* ms) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (!h->primed) RC(prime(h));
+  if (h->bs == 5) {
+    trials = std::max(1, trials);
+    cudaStream_t S = h->stream;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    launch_dt(h->m, h->p, h->st, 1, 0.0, S);
+    launch_grad(h->m, h->p, h->st, S);
+    Params p = h->p;
+    const int cls[3] = {1, 2, 4};
+    float best = 1e30f;
+    int best_cl = h->p.flux_cl, best_v = h->p.relax_variant;
+    for (int i = 0; i < 3; i++) {
+      p.flux_cl = cls[i];
+      launch_flux(h->m, p, h->st, 1, 1, S);  // warm-up
+      CK(cudaEventRecord(e0, S));
+      for (int t = 0; t < trials; t++) launch_flux(h->m, p, h->st, 1, 1, S);
+      CK(cudaEventRecord(e1, S));
+      CK(cudaEventSynchronize(e1));
+      float t_ms = 0.0f;
+      CK(cudaEventElapsedTime(&t_ms, e0, e1));
+      if (ms) ms[i] = t_ms / trials;
+      if (t_ms < best) { best = t_ms; best_cl = cls[i]; }
+    }
+    p.flux_cl = best_cl;
+    best = 1e30f;
+    for (int v = 0; v < 2; v++) {
+      p.relax_variant = v;
+      launch_jacobi(h->m, p, h->st, 2, S);  // warm-up
+      CK(cudaEventRecord(e0, S));
+      launch_jacobi(h->m, p, h->st, 2 * trials, S);
+      CK(cudaEventRecord(e1, S));
+      CK(cudaEventSynchronize(e1));
+      float t_ms = 0.0f;
+      CK(cudaEventElapsedTime(&t_ms, e0, e1));
+      if (ms) ms[3 + v] = t_ms / (2 * trials);
+      if (t_ms < best) { best = t_ms; best_v = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CKL();
+    h->p.flux_cl = best_cl;
+    h->p.relax_variant = best_v;
+    drop_graph(h);
+  }
+  if (flux_cl) *flux_cl = h->p.flux_cl;
+  if (relax_variant) *relax_variant = h->p.relax_variant;
   return JG_OK;
 }
 

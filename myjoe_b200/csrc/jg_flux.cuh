@@ -480,8 +480,17 @@ __device__ inline void visc_flux(double Fu[3], double& FE, VFace& vf, const VSid
 // dF/dU x dU/dQ of the viscous flux (UgpWithCvCompFlow.cpp:717-745, 1692-1760) for
 // side 0 (A0) or side 1 (A1), scaled by sgn and added into the 5x5 row-major
 // accumulator acc (rows 1..4; the other entries are zero).
+// a 5x5 block seen through a stride (one thread's column of a [25][n] array)
 template <typename T>
-__device__ inline void visc_jac_add(T* acc, T sgn, int side, const VFace& vf, const VSide& s,
+struct StridedBlock {
+  T* p;
+  int stride;
+  __device__ T& operator[](int e) const { return p[e * stride]; }
+};
+
+// acc: a T* (a block in registers) or a StridedBlock<T> (accumulated in place)
+template <typename T, typename Acc>
+__device__ inline void visc_jac_add(Acc acc, T sgn, int side, const VFace& vf, const VSide& s,
                                     const double* u_fa) {
   // inputs rounded to T once, the arithmetic in T (FP64: the reference's expressions term by term)
   const T mm = (T)(vf.mul + vf.mut), alpha = (T)vf.alpha, smag = (T)vf.smag, area = (T)vf.area, keff = (T)vf.keff;

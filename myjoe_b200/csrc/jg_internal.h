@@ -130,6 +130,11 @@ struct Params {
   int viscous;      // mu_ref > 0
   int fp32;         // matrix + relaxation in FP32
   int turb;         // JG_TURB_*
+  // launch shapes (jg_autotune / jg_set_launch_config): lanes per cell of the 5x5 face loop
+  // (1, 2 or 4), and the 5x5 Jacobi sweep's kernel (0: a block per 32-cell slice with a
+  // thread per block row, 1: a thread per cell)
+  int flux_cl;
+  int relax_variant;
 };
 
 // launchers (jg_kernels.cu); all enqueue on stream s

@@ -537,17 +537,16 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           for (int i = 0; i < 3; i++) rhs[1 + i] += sg * Fu[i];
           rhs[4] += sg * FE;
           if (implicit) {
-            // row of c0: D -= A0, O -= A1 ; row of c1: D += A1, O += A0  (calcViscousFluxNS 3678-3696)
-            JT Dv[25];
-            for (int e = 0; e < 25; e++) Dv[e] = JT(0);
+            // row of c0: D -= A0, O -= A1 ; row of c1: D += A1, O += A0  (calcViscousFluxNS 3678-3696);
+            // the diagonal part goes straight into the cell's shared-memory block
+            const StridedBlock<JT> Ds{sD + t, bd};
             if (s.side == 0) {
-              visc_jac_add<JT>(Dv, JT(-1.0), 0, vf, v0, ufa);
+              visc_jac_add<JT>(Ds, JT(-1.0), 0, vf, v0, ufa);
               visc_jac_add<JT>(Ob, JT(-1.0), 1, vf, v1, ufa);
             } else {
-              visc_jac_add<JT>(Dv, JT(1.0), 1, vf, v1, ufa);
+              visc_jac_add<JT>(Ds, JT(1.0), 1, vf, v1, ufa);
               visc_jac_add<JT>(Ob, JT(1.0), 0, vf, v0, ufa);
             }
-            for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
           }
         }
         if (implicit)
@@ -619,12 +618,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
           for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
           rhs[4] -= FE;
-          if (implicit) {
-            JT Dv[25];
-            for (int e = 0; e < 25; e++) Dv[e] = JT(0);
-            visc_jac_add<JT>(Dv, JT(-1.0), 0, vf, v0, v1.u);
-            for (int e = 5; e < 25; e++) sD[e * bd + t] += Dv[e];
-          }
+          if (implicit) visc_jac_add<JT>(StridedBlock<JT>{sD + t, bd}, JT(-1.0), 0, vf, v0, v1.u);
         }
       }
     }
@@ -1223,13 +1217,19 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
   else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
-constexpr int FLUX_CL = 2;  // lanes per cell of the implicit face loop
+template <typename BT, int KIND, int CL>
+static void launch_flux_cell_cl(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
+  size_t shm = 25 * TB * sizeof(BT);
+  const int g = grid_for(m.ncv, TB / CL);
+  if (p.viscous) k_flux<BT, KIND, 1, CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+  else k_flux<BT, KIND, 0, CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+}
+// lanes per cell of the implicit face loop: p.flux_cl (1, 2 or 4)
 template <typename BT, int KIND>
 static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  size_t shm = 25 * TB * sizeof(BT);
-  const int g = grid_for(m.ncv, TB / FLUX_CL);
-  if (p.viscous) k_flux<BT, KIND, 1, FLUX_CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
-  else k_flux<BT, KIND, 0, FLUX_CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+  if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1>(m, p, st, for_step, s);
+  else if (p.flux_cl == 4) launch_flux_cell_cl<BT, KIND, 4>(m, p, st, for_step, s);
+  else launch_flux_cell_cl<BT, KIND, 2>(m, p, st, for_step, s);
 }
 template <typename BT>
 static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
@@ -1254,14 +1254,21 @@ int flux_partials(const Mesh& m, int implicit) { return implicit ? grid_for(m.nc
 void launch_resid(const Mesh& m, State& st, int hist_from_ctrl, cudaStream_t s) {
   k_resid_final<<<1, 256, 0, s>>>(st, flux_partials(m, 1), hist_from_ctrl);
 }
+// both sweep kernels do the same arithmetic in the same order (bit-identical results)
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {
   for (int it = 0; it < sweeps; it++) {
     void* xin = (it % 2 == 0) ? st.x1 : st.x0;
     void* xout = (it % 2 == 0) ? st.x0 : st.x1;
-    if (p.fp32)
+    if (p.relax_variant == 1) {
+      if (p.fp32)
+        k_jacobi<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const float*)xin, (float*)xout, it == 0);
+      else
+        k_jacobi<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
+    } else if (p.fp32) {
       k_jacobi2<float><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (const float*)xin, (float*)xout, it == 0);
-    else
+    } else {
       k_jacobi2<double><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (const double*)xin, (double*)xout, it == 0);
+    }
   }
 }
 void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {

@@ -46,6 +46,9 @@ def lib():
         L.jg_device_count.argtypes = [C.POINTER(I)]
         L.jg_create.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
         L.jg_renumber_cells.argtypes = [C.POINTER(jg_mesh), I, C.POINTER(I)]
+        L.jg_set_launch_config.argtypes = [P, I, I]
+        L.jg_get_launch_config.argtypes = [P, C.POINTER(I), C.POINTER(I)]
+        L.jg_autotune.argtypes = [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)]
         L.jg_destroy.argtypes = [P]
         L.jg_get_stream.argtypes = [P, C.POINTER(P)]
         L.jg_set_state.argtypes = [P, D, D, D]
@@ -260,6 +263,23 @@ class JoeGpu:
         b = C.c_double()
         _ck(lib().jg_case_device_bytes(self.h, C.byref(b)))
         return b.value
+
+    def autotune(self, trials=5):
+        """time the launch shapes on this handle and keep the fastest: returns
+        (lanes per cell of the face loop, sweep kernel, {shape: ms per launch})"""
+        cl, rv = C.c_int(0), C.c_int(0)
+        ms = (C.c_float * 5)()
+        _ck(lib().jg_autotune(self.h, int(trials), C.byref(cl), C.byref(rv), ms))
+        times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4]}
+        return cl.value, rv.value, times
+
+    def set_launch_config(self, flux_cl, relax_variant):
+        _ck(lib().jg_set_launch_config(self.h, int(flux_cl), int(relax_variant)))
+
+    def launch_config(self):
+        cl, rv = C.c_int(0), C.c_int(0)
+        _ck(lib().jg_get_launch_config(self.h, C.byref(cl), C.byref(rv)))
+        return cl.value, rv.value
 
     def cfl_step(self):
         cfl = C.c_double(0.0)

@@ -43,7 +43,10 @@ enum {
   JG_BC_NEUMANN = 6,              /* v: -                                    */
   JG_BC_FARFIELD = 7              /* v[0..2] = u, v[3] = p, v[4] = rho, v[5] = gamma */
 };
-enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2 };
+/* SPACE_INTEGRATION: HLLC, ROE, AUSM (implicit side: the HLLC matrices) and HAENEL
+ * (Haenel & Schwane, calcEulerFlux_HAENEL / calcEulerFluxMatrices_HAENEL,
+ * UgpWithCvCompFlow.cpp:1329-1505; also AUSMDV with SHOCK_FIX_TYPE = HAENEL) */
+enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2, JG_FLUX_HAENEL = 3 };
 enum { JG_MU_POWERLAW = 0, JG_MU_SUTHERLAND = 1 };
 enum { JG_SYMM_ORIGINAL_NUMERIC = 0, JG_SYMM_NEW_NUMERIC = 1, JG_SYMM_ANALYTICAL = 2 };
 enum { JG_TS_CFL = 0, JG_TS_CFL_MIN = 1, JG_TS_DT = 2 };

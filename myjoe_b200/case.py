@@ -21,7 +21,7 @@ BC_KINDS = {
     "SYMMETRY": 1, "WALL": 2, "CBC": 3, "CBC_SUBSONIC_INLET": 4,
     "CBC_SUBSONIC_OUTLET": 5, "NEUMANN": 6, "FARFIELD": 7, "NOTHING": 8,
 }
-FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2}
+FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2, "HAENEL": 3}
 SYMM_BC_KINDS = {"ORIGINAL_NUMERIC": 0, "NEW_NUMERIC": 1, "ANALYTICAL": 2}
 SOLVER_KINDS = {"BCGSTAB": 0, "LUSGS": 1, "JACOBI": 2, "SGS": 3, "BCGSTAB_LINELET": 4, "LINE": 5}
 

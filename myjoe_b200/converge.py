@@ -1,0 +1,77 @@
+"""Time to converge one case on the GPU: the Euler bump (SURVEY-style
+config 1: 64x32x4 hex, 8,192 cells, HLLC, M 0.5, second order with the
+limiter, CFL 1 ramped to 100) or the laminar plate (config 2: 256x96x2,
+49,152 cells, Roe + Sutherland), run to a residual drop of the L1 energy
+residual, FP64 or mixed.  Prints one JSON line: steps, device seconds,
+cell-iters/s, converged solves per hour of one GPU.
+
+    python -m myjoe_b200.converge --config 1 [--precision mixed] [--solver SGS] [--drop 1e-10]
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import time
+
+import numpy as np
+
+from . import build, case, solver
+
+
+def make(config):
+    if config == 1:
+        _, g, prm = case.bump_case(64, 32, 4)
+        return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 100.0)), "Euler bump 64x32x4 (8,192 cells), HLLC"
+    _, g, prm = case.plate_case(256, 96, 2)
+    return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 100.0)), \
+        "laminar plate 256x96x2 (49,152 cells), Roe + Sutherland"
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--solver", default="SGS", choices=["SGS", "JACOBI", "LINE", "BCGSTAB", "BCGSTAB_LINELET"])
+    ap.add_argument("--sweeps", type=int, default=10)
+    ap.add_argument("--drop", type=float, default=1e-10)
+    ap.add_argument("--max-steps", type=int, default=4000)
+    ap.add_argument("--chunk", type=int, default=50)
+    a = ap.parse_args(argv)
+    build.build()
+    g, prm, name = make(a.config)
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS=a.solver, LS_MAX_ITER=a.sweeps)
+    j = solver.JoeGpu(g, prm, precision=1 if a.precision == "mixed" else 0)
+    j.set_state(*case.perturbed_state(g.x_cv, prm, 0.0))
+    j.runBackwardEuler(1)
+    j.close()
+    # the timed solve: a fresh handle from the uniform start
+    j = solver.JoeGpu(g, prm, precision=1 if a.precision == "mixed" else 0)
+    j.set_state(*case.perturbed_state(g.x_cv, prm, 0.0))
+    steps, ran, r0, t, drop = 0, 0, None, 0.0, 1.0
+    while steps < a.max_steps:
+        t0 = time.perf_counter()
+        r = j.runBackwardEuler(a.chunk)
+        t += time.perf_counter() - t0
+        ran += a.chunk
+        if r0 is None:
+            r0 = r[0, 4]
+        d = r[:, 4] / r0
+        hit = np.nonzero(d <= a.drop)[0]
+        if hit.size:
+            steps += int(hit[0]) + 1
+            drop = float(d[hit[0]])
+            break
+        steps += a.chunk
+        drop = float(d[-1])
+        if not np.isfinite(drop):
+            break
+    t *= steps / max(ran, 1)  # the steps after the drop inside the last chunk do not count
+    out = {"workload": name, "cells": g.ncv, "precision": a.precision, "solver": "%s x%d" % (a.solver, a.sweeps),
+           "drop_target": a.drop, "drop": drop, "converged": bool(drop <= a.drop), "steps": steps,
+           "seconds": t, "cell_iters_per_s": g.ncv * steps / t, "solves_per_hour": 3600.0 / t}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

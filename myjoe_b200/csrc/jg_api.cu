@@ -248,7 +248,7 @@ static Params make_params(const jg_params& q) {
 
 static int check_params(const jg_params* q) {
   if (!q) return set_err(JG_ERR_ARG, "null params");
-  if (q->flux < 0 || q->flux > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
+  if (q->flux < 0 || q->flux > 3) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
   if (q->symm_bc < 0 || q->symm_bc > 2) return set_err(JG_ERR_ARG, "unsupported SYMM_BC %d", q->symm_bc);
   if (q->lin_solver < 0 || q->lin_solver > 5) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
   if (q->precision != JG_PREC_FP64 && q->precision != JG_PREC_MIXED)
@@ -1466,7 +1466,7 @@ int jg_get_cfl_step(jg_case_t* h, double* cfl, int* step) {
 int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
                         double* F, double* AL, double* AR) {
   if (n < 0 || !L || !R || !area || !nvec || !F) return set_err(JG_ERR_ARG, "bad argument");
-  if (kind < 0 || kind > 2) return set_err(JG_ERR_ARG, "unsupported flux %d", kind);
+  if (kind < 0 || kind > 3) return set_err(JG_ERR_ARG, "unsupported flux %d", kind);
   if (n == 0) return JG_OK;
   double *dL, *dR, *dA, *dN, *dF, *dAL = nullptr, *dAR = nullptr;
   size_t b6 = 6 * (size_t)n * 8, b3 = 3 * (size_t)n * 8;

@@ -14,6 +14,7 @@ namespace jg {
 template <typename T>
 struct FStateT {
   T rho, u[3], p, gam;
+  T h;  // static enthalpy (the HAENEL flux reads it; the others derive what they need from p, rho)
 };
 using FState = FStateT<double>;
 
@@ -32,6 +33,7 @@ __device__ __forceinline__ FStateT<T> fstate_as(const FState& s) {
   for (int i = 0; i < 3; i++) o.u[i] = (T)s.u[i];
   o.p = (T)s.p;
   o.gam = (T)s.gam;
+  o.h = (T)s.h;
   return o;
 }
 
@@ -408,11 +410,121 @@ __device__ inline void flux_ausm(double F[5], const FState& L, const FState& R, 
   for (int i = 0; i < 5; i++) F[i] *= area;
 }
 
+// ---------------------------------------------------------------------------
+// Haenel & Schwane (AUSM family with a common speed of sound), calcEulerFlux_HAENEL
+// and calcEulerFluxMatrices_HAENEL, UgpWithCvCompFlow.cpp:1329-1505, with the split
+// Mach-number polynomials p_plusminus / u_plusminus and their derivatives (753-877)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T hs_p_pm(T p, T un, T c, T sign) {
+  T M = sign * un / c;
+  if (T(1.0) <= M) return p;
+  if (T(-1.0) <= M) return T(0.25) * p * (M + T(1.0)) * (M + T(1.0)) * (T(2.0) - M);
+  return T(0.0);
+}
+
+template <typename T>
+__device__ __forceinline__ T hs_u_pm(T un, T c, T sign) {  // alpha = 1
+  T M = sign * un / c;
+  if (T(1.0) <= M) return un;
+  if (T(0.0) <= M) return sign * T(1.0) * c * T(0.25) * (M + T(1.0)) * (M + T(1.0)) + (T(1.0) - T(1.0)) * un;
+  if (T(-1.0) <= M) return sign * T(1.0) * c * T(0.25) * (M + T(1.0)) * (M + T(1.0));
+  return T(0.0);
+}
+
+// d(rho u^+-)/dQ, alpha = 1 (entry 5, the scalar's, is not needed here)
+template <typename T>
+__device__ __forceinline__ void hs_drhou_pm(T b[5], T un, T c, const T* n, T sign) {
+  T M = sign * un / c;
+  if (T(1.0) <= M) {
+    b[0] = T(0.0);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i];
+  } else if (T(0.0) <= M) {
+    b[0] = sign * T(0.25) * T(1.0) * c * (T(1.0) - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (T(0.5) * T(1.0) * (M + T(1.0)) + (T(1.0) - T(1.0)));
+  } else if (T(-1.0) <= M) {
+    b[0] = sign * T(0.25) * T(1.0) * c * (T(1.0) - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (T(0.5) * T(1.0) * (M + T(1.0)));
+  } else {
+    b[0] = T(0.0);
+    for (int i = 0; i < 3; i++) b[1 + i] = T(0.0);
+  }
+  b[4] = T(0.0);
+}
+
+// dp^+-/dQ
+template <typename T>
+__device__ __forceinline__ void hs_dp_pm(T d[5], const T* u, T rho, T p, T un, T uu, T ht, T c, T gam, const T* n,
+                                         T sign) {
+  T M = sign * un / c;
+  T dpdrho = gam * p / rho + (T(1.0) - gam) * (ht - uu);
+  if (T(1.0) <= M) {
+    d[0] = dpdrho;
+    for (int i = 0; i < 3; i++) d[1 + i] = (T(1.0) - gam) * u[i];
+    d[4] = gam - T(1.0);
+  } else if (T(-1.0) <= M) {
+    T w = T(0.25) * (M + T(1.0)) * (M + T(1.0)) * (T(2.0) - M);
+    d[0] = w * dpdrho - T(0.75) * p / rho * (T(1.0) + M) * (T(1.0) - M) * M;
+    for (int i = 0; i < 3; i++)
+      d[1 + i] = w * (T(1.0) - gam) * u[i] + T(0.75) * p / (rho * c) * (T(1.0) + M) * (T(1.0) - M) * sign * n[i];
+    d[4] = w * (gam - T(1.0));
+  } else {
+    for (int i = 0; i < 5; i++) d[i] = T(0.0);
+  }
+}
+
+__device__ inline void flux_haenel(double F[5], const FState& L, const FState& R, double area, const double nV[3]) {
+  double unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u), cL = sqrt(L.gam * L.p / L.rho), hL = L.h + 0.5 * uLuL + 0.0;
+  double unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u), cR = sqrt(R.gam * R.p / R.rho), hR = R.h + 0.5 * uRuR + 0.0;
+  double cLR = fmax(cL, cR);
+  double p_half = hs_p_pm(L.p, unL, cLR, 1.0) + hs_p_pm(R.p, unR, cLR, -1.0);
+  double uLp = hs_u_pm(unL, cLR, 1.0), uRm = hs_u_pm(unR, cLR, -1.0);
+  F[0] = L.rho * uLp + R.rho * uRm;
+  for (int i = 0; i < 3; i++) F[1 + i] = L.rho * uLp * L.u[i] + R.rho * uRm * R.u[i] + p_half * nV[i];
+  F[4] = L.rho * uLp * hL + R.rho * uRm * hR;
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+// one side's matrix: the side's u^+- (upm), its derivative blocks (beta, delta)
+template <typename T>
+__device__ __forceinline__ void haenel_side(T* A, const FStateT<T>& S, T un, T uu, T hS, T upm, const T beta[5],
+                                            const T delta[5], T area, const T nV[3]) {
+  for (int j = 0; j < 5; j++) {
+    A[j] = beta[j];
+    for (int i = 0; i < 3; i++) A[5 * (1 + i) + j] = beta[j] * S.u[i] + delta[j] * nV[i];
+    A[20 + j] = beta[j] * hS;
+  }
+  for (int i = 0; i < 3; i++) {
+    A[5 * (1 + i)] += -upm * S.u[i];
+    A[5 * (1 + i) + 1 + i] += upm;
+  }
+  A[20] += upm * ((S.gam - T(1.0)) * uu - S.gam * hS + S.gam * S.p / S.rho);
+  for (int j = 0; j < 3; j++) A[21 + j] += upm * (T(1.0) - S.gam) * S.u[j];
+  A[24] += upm * S.gam;
+  for (int e = 0; e < 25; e++) A[e] *= area;
+}
+
+template <typename T>
+__device__ inline void matrices_haenel(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area, const T nV[3]) {
+  T unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u), cL = sqrt(L.gam * L.p / L.rho), hL = L.h + T(0.5) * uLuL + T(0.0);
+  T unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u), cR = sqrt(R.gam * R.p / R.rho), hR = R.h + T(0.5) * uRuR + T(0.0);
+  T cLR = fmax(cL, cR);
+  T uLp = hs_u_pm(unL, cLR, T(1.0)), uRm = hs_u_pm(unR, cLR, T(-1.0));
+  T bp[5], bm[5], dp[5], dm[5];
+  hs_drhou_pm(bp, unL, cLR, nV, T(1.0));
+  hs_drhou_pm(bm, unR, cLR, nV, T(-1.0));
+  hs_dp_pm(dp, L.u, L.rho, L.p, unL, uLuL, hL, cLR, L.gam, nV, T(1.0));
+  hs_dp_pm(dm, R.u, R.rho, R.p, unR, uRuR, hR, cLR, R.gam, nV, T(-1.0));
+  if (AL) haenel_side(AL, L, unL, uLuL, hL, uLp, bp, dp, area, nV);
+  if (AR) haenel_side(AR, R, unR, uRuR, hR, uRm, bm, dm, area, nV);
+}
+
 template <int KIND>
 __device__ __forceinline__ void euler_flux_t(double F[5], const FState& L, const FState& R, double area,
                                              const double nV[3]) {
   if (KIND == 1) flux_roe(F, L, R, area, nV);
   else if (KIND == 2) flux_ausm(F, L, R, area, nV);
+  else if (KIND == 3) flux_haenel(F, L, R, area, nV);
   else flux_hllc(F, L, R, area, nV);
 }
 
@@ -420,6 +532,7 @@ template <int KIND, typename T>
 __device__ __forceinline__ void euler_matrices_t(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area,
                                                  const T nV[3]) {
   if (KIND == 1) matrices_roe<T>(AL, AR, L, R, area, nV);
+  else if (KIND == 3) matrices_haenel<T>(AL, AR, L, R, area, nV);
   else matrices_hllc<T>(AL, AR, L, R, area, nV);
 }
 
@@ -427,13 +540,15 @@ __device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& 
                                            const double nV[3]) {
   if (kind == 1) flux_roe(F, L, R, area, nV);
   else if (kind == 2) flux_ausm(F, L, R, area, nV);
+  else if (kind == 3) flux_haenel(F, L, R, area, nV);
   else flux_hllc(F, L, R, area, nV);
 }
 
-// implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061)
+// implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061), HAENEL its own
 __device__ __forceinline__ void euler_matrices(int kind, double* AL, double* AR, const FState& L, const FState& R,
                                                double area, const double nV[3]) {
   if (kind == 1) matrices_roe<double>(AL, AR, L, R, area, nV);
+  else if (kind == 3) matrices_haenel<double>(AL, AR, L, R, area, nV);
   else matrices_hllc<double>(AL, AR, L, R, area, nV);
 }
 

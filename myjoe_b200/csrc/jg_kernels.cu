@@ -403,6 +403,7 @@ __device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, 
   for (int i = 0; i < 3; i++) s.u[i] = st.prim[8 * c + i];
   s.p = st.prim[8 * c + 3];
   s.gam = p.gamma;
+  s.h = st.prim[8 * c + 5];
   return s;
 }
 
@@ -414,10 +415,12 @@ __device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const St
   for (int i = 0; i < 3; i++) r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
   double rr = s.rho + dot3(r0, &st.grho[3 * c]);
   double pp = s.p + dot3(r0, &st.gp[3 * c]);
-  if ((pp <= 0.0) || (rr <= 0.0)) return s;
+  if ((pp <= 0.0) || (rr <= 0.0)) return s;  // first order: the cell's own h is calcThermoProp_p of (p, rho)
   s.rho = rr;
   s.p = pp;
   for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
+  const double T = pp / (rr * p.R);  // calcThermoProp_p at the face
+  s.h = p.gamma * p.R / (p.gamma - 1.0) * T;
   return s;
 }
 
@@ -556,7 +559,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         const DevZone z = m.zones[m.bzone[f]];
         const double* bb = &st.bfa[8 * f];
         FState B;
-        B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
+        B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
         const FStateT<JT> Bt = fstate_as<JT>(B);
         const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
         double F[5];
@@ -715,7 +718,7 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
       const DevZone z = m.zones[m.bzone[f]];
       const double* bb = &st.bfa[8 * f];
       FState B;
-      B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma;
+      B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
       double F[5];
       if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
         euler_flux_t<KIND>(F, B, B, area, nV);
@@ -1115,6 +1118,9 @@ __global__ void k_flux_faces(int kind, int n, const double* L, const double* R, 
   FState sl, sr;
   sl.rho = L[6 * f]; sl.u[0] = L[6 * f + 1]; sl.u[1] = L[6 * f + 2]; sl.u[2] = L[6 * f + 3]; sl.p = L[6 * f + 4]; sl.gam = L[6 * f + 5];
   sr.rho = R[6 * f]; sr.u[0] = R[6 * f + 1]; sr.u[1] = R[6 * f + 2]; sr.u[2] = R[6 * f + 3]; sr.p = R[6 * f + 4]; sr.gam = R[6 * f + 5];
+  // ideal-gas enthalpy from the state (HAENEL)
+  sl.h = sl.gam * sl.p / ((sl.gam - 1.0) * sl.rho);
+  sr.h = sr.gam * sr.p / ((sr.gam - 1.0) * sr.rho);
   double nV[3] = {nvec[3 * f], nvec[3 * f + 1], nvec[3 * f + 2]};
   double Fl[5];
   euler_flux(kind, Fl, sl, sr, area[f], nV);
@@ -1215,6 +1221,7 @@ template <typename BT>
 static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
   if (p.flux == JG_FLUX_ROE) launch_flux_k<BT, 1>(m, p, st, implicit, for_step, s);
   else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
+  else if (p.flux == JG_FLUX_HAENEL) launch_flux_k<BT, 3>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
 template <typename BT, int KIND, int CL>
@@ -1235,6 +1242,7 @@ template <typename BT>
 static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
   if (p.flux == JG_FLUX_ROE) launch_flux_cell_k<BT, 1>(m, p, st, for_step, s);
   else if (p.flux == JG_FLUX_AUSM) launch_flux_cell_k<BT, 2>(m, p, st, for_step, s);
+  else if (p.flux == JG_FLUX_HAENEL) launch_flux_cell_k<BT, 3>(m, p, st, for_step, s);
   else launch_flux_cell_k<BT, 0>(m, p, st, for_step, s);
 }
 // residual + Jacobian: one thread per cell, so that the 32 lanes of a warp

@@ -499,7 +499,7 @@ static void grad_vector(jo_case *h, double *g, const double *u, const double *u_
 /* ------------------------------------------------------------------------ */
 /* Euler fluxes and their implicit matrices                                  */
 /* ------------------------------------------------------------------------ */
-typedef struct { double rho, u[3], p, gam, k; } fstate;
+typedef struct { double rho, u[3], p, gam, k, h; } fstate;  /* h: static enthalpy */
 
 /* calcEulerFlux_HLLC, UgpWithCvCompFlow.cpp:120-235 */
 static void flux_hllc(double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
@@ -944,9 +944,108 @@ static void flux_ausm(double F[5], const fstate *L, const fstate *R, double area
   for (int i = 0; i < 5; i++) F[i] *= area;
 }
 
+/* Haenel & Schwane: calcEulerFlux_HAENEL and calcEulerFluxMatrices_HAENEL
+ * (UgpWithCvCompFlow.cpp:1329-1505) with p_plusminus, u_plusminus (alpha 1),
+ * drhou_plusminus_dQ and dp_plusminus_dQ (753-877) */
+static double hs_p_pm(double p, double un, double c, double sign) {
+  double M = sign * un / c;
+  if (1.0 <= M) return p;
+  else if (-1.0 <= M) return 0.25 * p * (M + 1.0) * (M + 1.0) * (2.0 - M);
+  return 0.0;
+}
+static double hs_u_pm(double alpha, double un, double c, double sign) {
+  double M = sign * un / c;
+  if (1.0 <= M) return un;
+  else if (0.0 <= M) return sign * alpha * c * 0.25 * (M + 1.0) * (M + 1.0) + (1.0 - alpha) * un;
+  else if (-1.0 <= M) return sign * alpha * c * 0.25 * (M + 1.0) * (M + 1.0);
+  return 0.0;
+}
+static void hs_drhou_pm(double *b, double alpha, double un, double c, const double *n, double sign) {
+  double M = sign * un / c;
+  if (1.0 <= M) {
+    b[0] = 0.0;
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i];
+  } else if (0.0 <= M) {
+    b[0] = sign * 0.25 * alpha * c * (1.0 - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (0.5 * alpha * (M + 1.0) + (1.0 - alpha));
+  } else if (-1.0 <= M) {
+    b[0] = sign * 0.25 * alpha * c * (1.0 - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (0.5 * alpha * (M + 1.0));
+  } else {
+    b[0] = 0.0;
+    for (int i = 0; i < 3; i++) b[1 + i] = 0.0;
+  }
+  b[4] = 0.0;
+}
+static void hs_dp_pm(double *d, const double *u, double rho, double p, double un, double uu, double ht, double c,
+                     double gam, const double *n, double sign) {
+  double M = sign * un / c;
+  double dpdrho = gam * p / rho + (1.0 - gam) * (ht - uu);
+  if (1.0 <= M) {
+    d[0] = dpdrho;
+    for (int i = 0; i < 3; i++) d[1 + i] = (1.0 - gam) * u[i];
+    d[4] = (gam - 1.0);
+  } else if (-1.0 <= M) {
+    d[0] = 0.25 * (M + 1.0) * (M + 1.0) * (2.0 - M) * dpdrho - 0.75 * p / rho * (1.0 + M) * (1.0 - M) * M;
+    for (int i = 0; i < 3; i++)
+      d[1 + i] = 0.25 * (M + 1.0) * (M + 1.0) * (2.0 - M) * (1.0 - gam) * u[i] +
+                 0.75 * p / (rho * c) * (1.0 + M) * (1.0 - M) * sign * n[i];
+    d[4] = 0.25 * (M + 1.0) * (M + 1.0) * (2.0 - M) * (gam - 1.0);
+  } else {
+    for (int i = 0; i < 5; i++) d[i] = 0.0;
+  }
+}
+static void flux_haenel(double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+  double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->h + 0.5 * uLuL + L->k;
+  double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->h + 0.5 * uRuR + R->k;
+  double cLR = dmax(cL, cR);
+  double p_half = hs_p_pm(L->p, unL, cLR, +1.0) + hs_p_pm(R->p, unR, cLR, -1.0);
+  double uLp = hs_u_pm(1.0, unL, cLR, +1.0), uRm = hs_u_pm(1.0, unR, cLR, -1.0);
+  F[0] = L->rho * uLp + R->rho * uRm;
+  for (int i = 0; i < 3; i++) F[1 + i] = L->rho * uLp * L->u[i] + R->rho * uRm * R->u[i] + p_half * nV[i];
+  F[4] = L->rho * uLp * hL + R->rho * uRm * hR;
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+static void haenel_side(double (*A)[5], const fstate *S, double uu, double hS, double upm, const double *beta,
+                        const double *delta, double area, const double *nV) {
+  for (int j = 0; j < 5; j++) {
+    A[0][j] = beta[j];
+    for (int i = 0; i < 3; i++) A[1 + i][j] = beta[j] * S->u[i] + delta[j] * nV[i];
+    A[4][j] = beta[j] * hS;
+  }
+  for (int i = 0; i < 3; i++) {
+    A[1 + i][0] += -upm * S->u[i];
+    A[1 + i][1 + i] += upm;
+  }
+  A[4][0] += upm * ((S->gam - 1.0) * uu - S->gam * hS + S->gam * S->p / S->rho);
+  for (int j = 0; j < 3; j++) A[4][1 + j] += upm * (1.0 - S->gam) * S->u[j];
+  A[4][4] += upm * S->gam;
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) A[i][j] *= area;
+}
+static void matrices_haenel(double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
+                            const double *nV) {
+  double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->h + 0.5 * uLuL + L->k;
+  double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->h + 0.5 * uRuR + R->k;
+  double cLR = dmax(cL, cR);
+  double uLp = hs_u_pm(1.0, unL, cLR, 1.0), uRm = hs_u_pm(1.0, unR, cLR, -1.0);
+  double bp[5], bm[5], dp[5], dm[5];
+  hs_drhou_pm(bp, 1.0, unL, cLR, nV, +1.0);
+  hs_drhou_pm(bm, 1.0, unR, cLR, nV, -1.0);
+  hs_dp_pm(dp, L->u, L->rho, L->p, unL, uLuL, hL, cLR, L->gam, nV, +1.0);
+  hs_dp_pm(dm, R->u, R->rho, R->p, unR, uRuR, hR, cLR, R->gam, nV, -1.0);
+  if (AL) haenel_side(AL, L, uLuL, hL, uLp, bp, dp, area, nV);
+  if (AR) haenel_side(AR, R, uRuR, hR, uRm, bm, dm, area, nV);
+}
+
 static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
   if (kind == JG_FLUX_ROE) flux_roe(F, L, R, area, nV);
   else if (kind == JG_FLUX_AUSM) flux_ausm(F, L, R, area, nV);
+  else if (kind == JG_FLUX_HAENEL) flux_haenel(F, L, R, area, nV);
   else flux_hllc(F, L, R, area, nV);
 }
 
@@ -954,14 +1053,18 @@ static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, 
 static void euler_matrices(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
                            const double *nV) {
   if (kind == JG_FLUX_ROE) matrices_roe(AL, AR, L, R, area, nV);
+  else if (kind == JG_FLUX_HAENEL) matrices_haenel(AL, AR, L, R, area, nV);
   else matrices_hllc(AL, AR, L, R, area, nV);
 }
 
 void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
                          double *F, double *AL, double *AR) {
   for (int f = 0; f < n; f++) {
-    fstate sl = {L[6 * f], {L[6 * f + 1], L[6 * f + 2], L[6 * f + 3]}, L[6 * f + 4], L[6 * f + 5], 0.0};
-    fstate sr = {R[6 * f], {R[6 * f + 1], R[6 * f + 2], R[6 * f + 3]}, R[6 * f + 4], R[6 * f + 5], 0.0};
+    fstate sl = {L[6 * f], {L[6 * f + 1], L[6 * f + 2], L[6 * f + 3]}, L[6 * f + 4], L[6 * f + 5], 0.0, 0.0};
+    fstate sr = {R[6 * f], {R[6 * f + 1], R[6 * f + 2], R[6 * f + 3]}, R[6 * f + 4], R[6 * f + 5], 0.0, 0.0};
+    /* ideal-gas enthalpy from the state */
+    sl.h = sl.gam * sl.p / ((sl.gam - 1.0) * sl.rho);
+    sr.h = sr.gam * sr.p / ((sr.gam - 1.0) * sr.rho);
     euler_flux(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f]);
     if (AL || AR)
       euler_matrices(kind, AL ? (double(*)[5]) & AL[25 * f] : NULL, AR ? (double(*)[5]) & AR[25 * f] : NULL, &sl, &sr,
@@ -980,12 +1083,13 @@ static int csr_slot(const jg_mesh *m, int row, int col) {
 }
 
 static fstate cell_state(jo_case *h, int c) {
-  fstate s = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->press[c], h->gam[c], 0.0};
+  fstate s = {h->rho[c], {h->vel[3 * c], h->vel[3 * c + 1], h->vel[3 * c + 2]}, h->press[c], h->gam[c], 0.0,
+              h->enthalpy[c]};
   return s;
 }
 static fstate bfa_state(jo_case *h, int f) {
   fstate s = {h->rho_bfa[f], {h->vel_bfa[3 * f], h->vel_bfa[3 * f + 1], h->vel_bfa[3 * f + 2]}, h->p_bfa[f],
-              h->gam_bfa[f], 0.0};
+              h->gam_bfa[f], 0.0, h->h_bfa[f]};
   return s;
 }
 
@@ -995,17 +1099,20 @@ static int reconstruct(jo_case *h, int c, int f, fstate *s) {
   for (int i = 0; i < 3; i++) r0[i] = h->m.x_fa[3 * f + i] - h->m.x_cv[3 * c + i];
   double rho0 = h->rho[c] + dot3(r0, &h->grad_rho[3 * c]);
   double p0 = h->press[c] + dot3(r0, &h->grad_p[3 * c]);
-  if ((p0 <= 0.0) || (rho0 <= 0.0)) {
+  int fallback = (p0 <= 0.0) || (rho0 <= 0.0);
+  if (fallback) {
     s->rho = h->rho[c];
     s->p = h->press[c];
-    return 1;
+  } else {
+    s->rho = rho0;
+    s->p = p0;
+    for (int i = 0; i < 3; i++) s->u[i] = h->vel[3 * c + i] + dot3(r0, &h->grad_u[9 * c + 3 * i]);
   }
-  s->rho = rho0;
-  s->p = p0;
-  for (int i = 0; i < 3; i++) s->u[i] = h->vel[3 * c + i] + dot3(r0, &h->grad_u[9 * c + 3 * i]);
-  /* calcThermoProp_p: gamma = GAMMA (ideal gas) */
+  /* calcThermoProp_p at the face (ideal gas: gamma = GAMMA, R = R_gas) */
   s->gam = h->p.gamma;
-  return 0;
+  double T = s->p / (s->rho * h->p.R_gas);
+  s->h = h->p.gamma * h->p.R_gas / (h->p.gamma - 1.0) * T;
+  return fallback;
 }
 
 static void add_block(double *A, int slot, double (*B)[5], double sgn) {

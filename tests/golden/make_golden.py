@@ -57,6 +57,11 @@ def cases():
                                                                           SPACE_INTEGRATION="HLLC",
                                                                           VISC_LIMITER=False)
     yield "plate_roe", rawp, prmp
+    # Haenel & Schwane (SPACE_INTEGRATION = HAENEL): second order, laminar, first order with NEW_NUMERIC symmetry
+    yield "bump_haenel", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
+    yield "bump_haenel_laminar_isothermal", raw, dataclasses.replace(visc, SPACE_INTEGRATION="HAENEL", bcs=bc_iso)
+    yield "bump_haenel_first_order_symm_new", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL",
+                                                                      SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
     yield "mixed_bump_hllc", rawm, prm
     yield "mixed_bump_roe_laminar_isothermal", rawm, dataclasses.replace(visc, bcs=bc_iso)
     # BCGSTAB_LINELET: lines from the wall through the stretched rows (and through prisms into hexahedra)

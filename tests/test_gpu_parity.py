@@ -194,7 +194,7 @@ def test_backward_euler_steps_match_reference(golden):
     np.testing.assert_allclose(res, g["resid"], rtol=6e-5)
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
 def test_per_face_fluxes(kind):
     """calcEulerFlux_{HLLC,Roe,AUSM} + matrices over random subsonic and
     supersonic face states, GPU vs oracle."""

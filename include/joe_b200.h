@@ -247,7 +247,7 @@ int jg_batch_status(jg_case_t *h, int *status);
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
 /* Launch shapes (no reference counterpart): the lanes per cell of the 5x5
- * face loop (1, 2 or 4; default 2) and the kernel of the 5x5 Jacobi sweep (0:
+ * face loop (1, 2 or 4; default 1) and the kernel of the 5x5 Jacobi sweep (0:
  * a block per 32-cell slice, a thread per block row, the default; 1: a thread
  * per cell).  jg_autotune times each candidate on the handle's own mesh
  * (trials launches, CUDA events) and keeps the fastest; ms[5] (may be NULL)

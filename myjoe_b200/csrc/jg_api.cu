@@ -241,7 +241,7 @@ static Params make_params(const jg_params& q) {
   p.under_relax = q.under_relax;
   p.viscous = q.mu_ref > 0.0;
   p.fp32 = q.precision == JG_PREC_MIXED;
-  p.flux_cl = 2;
+  p.flux_cl = 1;
   p.relax_variant = 0;
   return p;
 }

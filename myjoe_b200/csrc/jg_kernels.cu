@@ -477,12 +477,15 @@ __device__ inline void block_inverse(double* A, double* Ai) {
   }
 }
 
-// CL lanes per cell: lane l of a cell evaluates the cell's face slots l,
-// l+CL, ...; each lane accumulates its own partial diagonal block (shared
-// memory) and residual, summed over the lanes in a fixed order.  Two lanes
-// per cell halve the dependent chain of each thread and give the scheduler
-// twice the warps to balance over the SMs (a one-wave-and-a-bit grid at the
-// register-limited occupancy otherwise leaves most SMs idle in its tail).
+// CL lanes per cell (a launch shape chosen per handle, jg_autotune): lane l
+// of a cell evaluates the cell's face slots l, l+CL, ...; each lane
+// accumulates its own partial diagonal block (shared memory) and residual,
+// summed over the lanes in a fixed order.  More lanes shorten each thread's
+// dependent chain and give the scheduler more warps to spread over the SMs
+// (a small mesh is otherwise a one-and-a-bit-wave grid at the
+// register-limited occupancy); they cost repeated reads of the cell's data.
+// Measured: the viscous Roe plate (49k cells) is 2% faster with two lanes,
+// inviscid HLLC bumps (430k cells) 1.4x faster with one.
 template <typename BT, int KIND, int VISC, int CL>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,

@@ -115,7 +115,13 @@ typedef struct jg_params {
   int turb_model;      /* JG_TURB_*: with a model the case runs runBackwardEulerCoupled's
                           (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
   int renumber;        /* JG_RENUMBER_*: the handle's own cell/face order (jg_create only) */
+  int grad_scheme;     /* GRAD_RECONSTRUCTION SCHEME: JG_GRAD_* (the flow gradients of calcEulerFlux) */
 } jg_params;
+/* JG_GRAD_LSQ: least squares (calcCvScalarGrad / calcCvVectorGrad, UgpWithCv.h:1009-1083);
+ * JG_GRAD_GREENGAUSS: Green-Gauss with distance-weighted face values
+ * (calcCvScalarGradGreenGauss / calcCvVectorGradGreenGauss, UgpWithCv.h:1091-1184, GG_WITH_DIST);
+ * both followed by the same Barth-Jespersen limiter.  Green-Gauss: cases without a turbulence model. */
+enum { JG_GRAD_LSQ = 0, JG_GRAD_GREENGAUSS = 1 };
 /* Cell and face order inside a handle.  JG_RENUMBER_NONE keeps the caller's
  * order (a mesh the reference loaded is already in reverse Cuthill-McKee
  * order, Ugp::init, src/common/Ugp.cpp:3389-3399).  JG_RENUMBER_RCM renumbers

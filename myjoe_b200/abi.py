@@ -42,7 +42,8 @@ class jg_params(C.Structure):
                 ("under_relax", C.c_double),
                 ("lin_solver", C.c_int), ("ls_max_iter", C.c_int),
                 ("ls_abs", C.c_double), ("ls_rel", C.c_double),
-                ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int)]
+                ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int),
+                ("grad_scheme", C.c_int)]
 
 
 class jg_serve_config(C.Structure):
@@ -101,6 +102,7 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_
     q.nscal = p.nscal
     q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
     q.renumber = 1 if renumber else 0
+    q.grad_scheme = 1 if p.GRAD_SCHEME == "GREENGAUSS" else 0
     return q
 
 

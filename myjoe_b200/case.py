@@ -56,6 +56,7 @@ class JoeParams:
     SPACE_INTEGRATION: str = "HLLC"
     LIMITER: bool = True
     EPS: float = 0.01
+    GRAD_SCHEME: str = "LEASTSQUARES"   # GRAD_RECONSTRUCTION SCHEME: LEASTSQUARES or GREENGAUSS
     VISC_LIMITER: bool = True
     SYMM_BC: str = "ORIGINAL_NUMERIC"
     TIME_STEP: str = "MAX_BASED"
@@ -116,7 +117,7 @@ class JoeParams:
             "MU_POWER_LAW = %.17g" % self.MU_POWER_LAW, "SL_TREF = %.17g" % self.SL_TREF,
             "SL_SREF = %.17g" % self.SL_SREF,
             "SPACE_INTEGRATION = %s" % self.SPACE_INTEGRATION,
-            "GRAD_RECONSTRUCTION  SCHEME=LEASTSQUARES  LIMITER=%s  EPS=%.17g" % (
+            "GRAD_RECONSTRUCTION  SCHEME=%s  LIMITER=%s  EPS=%.17g" % (self.GRAD_SCHEME,
                 "YES" if self.LIMITER else "NO", self.EPS),
             "VISC_LIMITER = %s" % ("YES" if self.VISC_LIMITER else "NO"),
             "SYMM_BC = %s" % self.SYMM_BC,

@@ -19,12 +19,14 @@ import numpy as np
 from . import build, case, solver
 
 
-def make(config):
+def make(config, cfl_max):
     if config == 1:
+        # the settings of the reference's own converged run of this case (tests/golden/make_converged.py)
         _, g, prm = case.bump_case(64, 32, 4)
-        return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 100.0)), "Euler bump 64x32x4 (8,192 cells), HLLC"
+        return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, cfl_max or 20.0), EPS=0.01), \
+            "Euler bump 64x32x4 (8,192 cells), HLLC"
     _, g, prm = case.plate_case(256, 96, 2)
-    return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 100.0)), \
+    return g, dataclasses.replace(prm, CFL=1.0, CFL_RAMP=(10, 5, 1.2, cfl_max or 100.0)), \
         "laminar plate 256x96x2 (49,152 cells), Roe + Sutherland"
 
 
@@ -36,10 +38,11 @@ def main(argv=None):
     ap.add_argument("--sweeps", type=int, default=10)
     ap.add_argument("--drop", type=float, default=1e-10)
     ap.add_argument("--max-steps", type=int, default=4000)
+    ap.add_argument("--cfl-max", type=float, default=0.0, help="MAX_CFL of the ramp (0: the config's)")
     ap.add_argument("--chunk", type=int, default=50)
     a = ap.parse_args(argv)
     build.build()
-    g, prm, name = make(a.config)
+    g, prm, name = make(a.config, a.cfl_max)
     prm = dataclasses.replace(prm, LINEAR_SOLVER_NS=a.solver, LS_MAX_ITER=a.sweeps)
     j = solver.JoeGpu(g, prm, precision=1 if a.precision == "mixed" else 0)
     j.set_state(*case.perturbed_state(g.x_cv, prm, 0.0))
@@ -68,6 +71,7 @@ def main(argv=None):
             break
     t *= steps / max(ran, 1)  # the steps after the drop inside the last chunk do not count
     out = {"workload": name, "cells": g.ncv, "precision": a.precision, "solver": "%s x%d" % (a.solver, a.sweeps),
+           "cfl_ramp": list(prm.CFL_RAMP),
            "drop_target": a.drop, "drop": drop, "converged": bool(drop <= a.drop), "steps": steps,
            "seconds": t, "cell_iters_per_s": g.ncv * steps / t, "solves_per_hour": 3600.0 / t}
     print(json.dumps(out))

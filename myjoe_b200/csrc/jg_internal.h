@@ -135,6 +135,7 @@ struct Params {
   // thread per block row, 1: a thread per cell)
   int flux_cl;
   int relax_variant;
+  int grad_scheme;  // JG_GRAD_*
 };
 
 // launchers (jg_kernels.cu); all enqueue on stream s

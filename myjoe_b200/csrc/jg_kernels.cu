@@ -350,6 +350,69 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
       gh[j] += w[j] * b[6];
     }
   }
+  if (p.grad_scheme == JG_GRAD_GREENGAUSS) {
+    // calcCv{Scalar,Vector}GradGreenGauss (UgpWithCv.h:1091-1184, GG_WITH_DIST): the cell's internal
+    // faces in face order with the distance-weighted face value, then its boundary faces, over V
+    for (int j = 0; j < 9; j++) gu[j] = 0.0;
+    for (int j = 0; j < 3; j++) gr[j] = gpr[j] = gh[j] = 0.0;
+    for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+      const Slot s = m.slots[k];
+      if (s.nb < 0) continue;
+      const int f = s.f, c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
+      double d0[3], d1[3];
+      for (int j = 0; j < 3; j++) {
+        d0[j] = m.x_fa[3 * f + j] - m.x_cv[3 * c0 + j];
+        d1[j] = m.x_fa[3 * f + j] - m.x_cv[3 * c1 + j];
+      }
+      const double w0 = sqrt(dot3(d0, d0)), w1 = sqrt(dot3(d1, d1));
+      const double* p0 = &st.prim[8 * c0];
+      const double* p1 = &st.prim[8 * c1];
+      const double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
+      const double fr = (w1 * st.q[5 * c0] + w0 * st.q[5 * c1]) / (w0 + w1);
+      const double fp = (w1 * p0[3] + w0 * p1[3]) / (w0 + w1);
+      const double fh = (w1 * p0[5] + w0 * p1[5]) / (w0 + w1);
+      if (s.side == 0) {
+        for (int i = 0; i < 3; i++) {
+          const double fu = (w1 * p0[i] + w0 * p1[i]) / (w0 + w1);
+          for (int j = 0; j < 3; j++) gu[3 * i + j] += fu * n[j];
+        }
+        for (int j = 0; j < 3; j++) {
+          gr[j] += fr * n[j];
+          gpr[j] += fp * n[j];
+          gh[j] += fh * n[j];
+        }
+      } else {
+        for (int i = 0; i < 3; i++) {
+          const double fu = (w1 * p0[i] + w0 * p1[i]) / (w0 + w1);
+          for (int j = 0; j < 3; j++) gu[3 * i + j] -= fu * n[j];
+        }
+        for (int j = 0; j < 3; j++) {
+          gr[j] -= fr * n[j];
+          gpr[j] -= fp * n[j];
+          gh[j] -= fh * n[j];
+        }
+      }
+    }
+    for (int k = m.bf_i[c]; k < m.bf_i[c + 1]; k++) {
+      const int f = m.bf_v[k];
+      const double* b = &st.bfa[8 * f];
+      const double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) gu[3 * i + j] += b[1 + i] * n[j];
+      for (int j = 0; j < 3; j++) {
+        gr[j] += b[0] * n[j];
+        gpr[j] += b[4] * n[j];
+        gh[j] += b[6] * n[j];
+      }
+    }
+    const double V = m.vol[c];
+    for (int j = 0; j < 9; j++) gu[j] /= V;
+    for (int j = 0; j < 3; j++) {
+      gr[j] /= V;
+      gpr[j] /= V;
+      gh[j] /= V;
+    }
+  }
   // limiter factors over the internal faces of the cell
   double au[3] = {1.0, 1.0, 1.0}, ar = 1.0, ap = 1.0, ah = 1.0;
   const double eps = p.eps;

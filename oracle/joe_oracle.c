@@ -400,10 +400,71 @@ double jo_calc_dt(jo_case *h, double cfl_target) {
 /* ------------------------------------------------------------------------ */
 #define SDWLS_CLIP_SCALAR 1.0e-8 /* SDWLSClippingScalar, UgpWithCv.h:20 */
 
+/* distance weights of face f (GG_WITH_DIST): w0 = |x_fa - x_cv0|, w1 = |x_fa - x_cv1| */
+static void gg_weights(const jg_mesh *m, int f, double *w0, double *w1) {
+  int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+  double d0[3], d1[3];
+  for (int i = 0; i < 3; i++) {
+    d0[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c0 + i];
+    d1[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c1 + i];
+  }
+  *w0 = sqrt(dot3(d0, d0));
+  *w1 = sqrt(dot3(d1, d1));
+}
+
+/* calcCvScalarGradGreenGauss (UgpWithCv.h:1091-1128) with GG_WITH_DIST */
+static void grad_scalar_gg(jo_case *h, double *g, const double *phi, const double *phi_bfa) {
+  const jg_mesh *m = &h->m;
+  for (int k = 0; k < 3 * h->ncv; k++) g[k] = 0.0;
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double w0, w1;
+    gg_weights(m, f, &w0, &w1);
+    double fv = (w1 * phi[c0] + w0 * phi[c1]) / (w0 + w1);
+    for (int i = 0; i < 3; i++) {
+      g[3 * c0 + i] += fv * m->fa_normal[3 * f + i];
+      g[3 * c1 + i] -= fv * m->fa_normal[3 * f + i];
+    }
+  }
+  for (int f = 0; f < h->nfa_b; f++) {
+    int c = m->cvofa[2 * f];
+    for (int i = 0; i < 3; i++) g[3 * c + i] += phi_bfa[f] * m->fa_normal[3 * f + i];
+  }
+  for (int c = 0; c < h->ncv; c++)
+    for (int i = 0; i < 3; i++) g[3 * c + i] /= m->cv_volume[c];
+}
+
+/* calcCvVectorGradGreenGauss (UgpWithCv.h:1133-1184) with GG_WITH_DIST */
+static void grad_vector_gg(jo_case *h, double *g, const double *u, const double *u_bfa) {
+  const jg_mesh *m = &h->m;
+  for (int k = 0; k < 9 * h->ncv; k++) g[k] = 0.0;
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double w0, w1;
+    gg_weights(m, f, &w0, &w1);
+    for (int i = 0; i < 3; i++) {
+      double fv = (w1 * u[3 * c0 + i] + w0 * u[3 * c1 + i]) / (w0 + w1);
+      for (int j = 0; j < 3; j++) {
+        g[9 * c0 + 3 * i + j] += fv * m->fa_normal[3 * f + j];
+        g[9 * c1 + 3 * i + j] -= fv * m->fa_normal[3 * f + j];
+      }
+    }
+  }
+  for (int f = 0; f < h->nfa_b; f++) {
+    int c = m->cvofa[2 * f];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += u_bfa[3 * f + i] * m->fa_normal[3 * f + j];
+  }
+  for (int c = 0; c < h->ncv; c++)
+    for (int k = 0; k < 9; k++) g[9 * c + k] /= m->cv_volume[c];
+}
+
 static void grad_scalar(jo_case *h, double *g, const double *phi, const double *phi_bfa, int limit,
                         const double *ref, double *alpha) {
   const jg_mesh *m = &h->m;
-  /* calcCvScalarGrad(grad, phi) + boundary part, UgpWithCv.h:1009-1056 */
+  /* calcCvScalarGrad(grad, phi) + boundary part, UgpWithCv.h:1009-1056 (or Green-Gauss) */
+  if (h->p.grad_scheme == JG_GRAD_GREENGAUSS) grad_scalar_gg(h, g, phi, phi_bfa);
+  else
   for (int c = 0; c < h->ncv; c++) {
     int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
     for (int i = 0; i < 3; i++) g[3 * c + i] = m->nbocv_lsg_coeff[3 * nf + i] * phi[c];
@@ -412,10 +473,11 @@ static void grad_scalar(jo_case *h, double *g, const double *phi, const double *
       for (int i = 0; i < 3; i++) g[3 * c + i] += m->nbocv_lsg_coeff[3 * k + i] * phi[nb];
     }
   }
-  for (int f = 0; f < h->nfa_b; f++) {
-    int c = m->cvofa[2 * f];
-    for (int i = 0; i < 3; i++) g[3 * c + i] += m->boundary_fa_lsg_coeff[3 * f + i] * phi_bfa[f];
-  }
+  if (h->p.grad_scheme != JG_GRAD_GREENGAUSS)
+    for (int f = 0; f < h->nfa_b; f++) {
+      int c = m->cvofa[2 * f];
+      for (int i = 0; i < 3; i++) g[3 * c + i] += m->boundary_fa_lsg_coeff[3 * f + i] * phi_bfa[f];
+    }
   if (!limit) return;
   /* limitCvScalarGradBJ (smooth form), UgpWithCv.h:881-938 */
   for (int c = 0; c < h->ncv; c++) {
@@ -450,6 +512,8 @@ static void grad_scalar(jo_case *h, double *g, const double *phi, const double *
 static void grad_vector(jo_case *h, double *g, const double *u, const double *u_bfa, int limit, const double *ref) {
   const jg_mesh *m = &h->m;
   /* calcCvVectorGrad(grad, u) + boundary part, UgpWithCv.h:1031-1083; g[c][i][j] = d u_i / d x_j */
+  if (h->p.grad_scheme == JG_GRAD_GREENGAUSS) grad_vector_gg(h, g, u, u_bfa);
+  else
   for (int c = 0; c < h->ncv; c++) {
     int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
     for (int i = 0; i < 3; i++)
@@ -460,11 +524,12 @@ static void grad_vector(jo_case *h, double *g, const double *u, const double *u_
         for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += m->nbocv_lsg_coeff[3 * k + j] * u[3 * nb + i];
     }
   }
-  for (int f = 0; f < h->nfa_b; f++) {
-    int c = m->cvofa[2 * f];
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += m->boundary_fa_lsg_coeff[3 * f + j] * u_bfa[3 * f + i];
-  }
+  if (h->p.grad_scheme != JG_GRAD_GREENGAUSS)
+    for (int f = 0; f < h->nfa_b; f++) {
+      int c = m->cvofa[2 * f];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) g[9 * c + 3 * i + j] += m->boundary_fa_lsg_coeff[3 * f + j] * u_bfa[3 * f + i];
+    }
   if (!limit) return;
   /* limitCvVectorGradBJ, UgpWithCv.h:943-1000 */
   for (int c = 0; c < h->ncv; c++) {

@@ -58,6 +58,11 @@ def cases():
                                                                           VISC_LIMITER=False)
     yield "plate_roe", rawp, prmp
     # Haenel & Schwane (SPACE_INTEGRATION = HAENEL): second order, laminar, first order with NEW_NUMERIC symmetry
+    # Green-Gauss gradients (GRAD_RECONSTRUCTION SCHEME=GREENGAUSS, the reference's default scheme)
+    yield "bump_hllc_greengauss", raw, dataclasses.replace(prm, GRAD_SCHEME="GREENGAUSS")
+    yield "plate_roe_greengauss", rawp, dataclasses.replace(prmp, GRAD_SCHEME="GREENGAUSS")
+    yield "bump_roe_laminar_greengauss_novisclim", raw, dataclasses.replace(visc, bcs=bc_iso, GRAD_SCHEME="GREENGAUSS",
+                                                                          VISC_LIMITER=False)
     yield "bump_haenel", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
     yield "bump_haenel_laminar_isothermal", raw, dataclasses.replace(visc, SPACE_INTEGRATION="HAENEL", bcs=bc_iso)
     yield "bump_haenel_first_order_symm_new", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL",

@@ -196,8 +196,8 @@ def test_backward_euler_steps_match_reference(golden):
 
 @pytest.mark.parametrize("kind", [0, 1, 2, 3])
 def test_per_face_fluxes(kind):
-    """calcEulerFlux_{HLLC,Roe,AUSM} + matrices over random subsonic and
-    supersonic face states, GPU vs oracle."""
+    """calcEulerFlux_{HLLC,Roe,AUSM,HAENEL} + matrices over random subsonic
+    and supersonic face states, GPU vs oracle."""
     rng = np.random.default_rng(11 + kind)
     n = 4096
     def states(n):
@@ -217,6 +217,7 @@ def test_per_face_fluxes(kind):
     fs = np.column_stack([scale / np.sqrt(1.4 * L[:, 4] / L[:, 0]), scale, scale, scale, cscale])
     assert (np.abs(Fg - Fo) / fs).max() <= TOL
     ms = np.abs(ALo).reshape(n, -1).max(1) + np.abs(ARo).reshape(n, -1).max(1)
+    ms = np.where(ms > 0.0, ms, 1.0)  # HAENEL: both blocks vanish between diverging supersonic states
     assert (np.abs(ALg - ALo).reshape(n, -1).max(1) / ms).max() <= TOL
     assert (np.abs(ARg - ARo).reshape(n, -1).max(1) / ms).max() <= TOL
 

@@ -32,6 +32,7 @@ extern "C" {
 #define JG_ERR_NOMEM (-3)     /* device allocation failed */
 #define JG_ERR_STATE (-4)     /* non-physical state (NaN, rho<=0) detected */
 #define JG_ERR_NODEVICE (-5)  /* no CUDA device */
+#define JG_ERR_IO (-6)        /* file cannot be opened, read or written, or is not in the expected format */
 
 /* boundary kinds: setBC, src/joe/JoeWithModels.cpp:3857-4300 */
 enum {
@@ -225,6 +226,9 @@ int jg_step(jg_case_t *h, int nsteps, double *resid);
 /* the same steps enqueued on the case stream without synchronising */
 int jg_step_async(jg_case_t *h, int nsteps);
 int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
+/* sets the CFL and the step count the next step's ramp starts from (the
+ * reference's `cfl` and `step` members, e.g. after reading a restart) */
+int jg_set_cfl_step(jg_case_t *h, double cfl, int step);
 /* Batching form (no reference counterpart; the reference runs one case per
  * process): ncases independent cases, each with its own mesh and boundary
  * values, concatenated into one block-diagonal system so that every stage of
@@ -364,6 +368,64 @@ int jg_step_kernel_count(jg_case_t *h, int *n);
 #define JG_NOALLOC_MAX_CELLS 65536
 int jg_relax_csr_noalloc(int ncv, const int *nbocv_i, const int *nbocv_v, const double *A, const double *rhs,
                          double *dq, int sweeps, void *stream);
+
+/* Restart files: the reference's binary restart format (Ugp::writeRestart,
+ * Ugp::readRestart, src/common/Ugp.cpp:9792-13240; header Ugp.h:3423-3446),
+ * so that a solution can move between the reference and this library in
+ * either direction.  Host-only code, no GPU needed except for the two state
+ * calls.  A jg_restart_t holds a whole file in host memory: the mesh (node
+ * coordinates x_no[nno][3]; face nodes noofa_i[nfa+1] / noofa_v, ordered so
+ * that the face normal points from cvofa[f][0] to cvofa[f][1]; cvofa[nfa][2]
+ * with -1 for a boundary face and -(partner)-2 for a periodic one; the face
+ * zones, each a contiguous face range, in face order; the partition cv_part)
+ * and the data records in the order they were read or put.  Cells, faces and
+ * nodes are numbered in the file's global order.  jg_restart_write lays the
+ * records out as the reference does with one process: the file the reference
+ * wrote is written back byte for byte.  Names are at most 51 characters. */
+typedef struct jg_restart jg_restart_t;
+/* data record kinds: the reference's UGP_IO_* ids (Ugp.cpp:9797-9820) */
+enum { JG_RS_I0 = 11, JG_RS_D0 = 12, JG_RS_FA_D1 = 24, JG_RS_NO_D1 = 32, JG_RS_NO_D3 = 33,
+       JG_RS_CV_D1 = 42, JG_RS_CV_D3 = 43, JG_RS_CV_D33 = 44 };
+/* face zone kinds: FA_ZONE_* (Ugp.h:41-55) */
+enum { JG_FA_ZONE_BOUNDARY = 1, JG_FA_ZONE_PERIODIC_CART = 2, JG_FA_ZONE_INTERNAL = 6 };
+int jg_restart_new(jg_restart_t **out);
+int jg_restart_free(jg_restart_t *r);
+/* whole file; byte-swapped files are recognised and swapped.  JG_ERR_IO on a
+ * missing, truncated or malformed file (the message says which record). */
+int jg_restart_read(const char *path, jg_restart_t **out);
+int jg_restart_write(const jg_restart_t *r, const char *path);
+int jg_restart_counts(const jg_restart_t *r, int *nno, int *nfa, int *ncv, int *noofa_count, int *nzones,
+                      int *nrecords);
+/* any pointer may be NULL; sizes from jg_restart_counts */
+int jg_restart_get_mesh(const jg_restart_t *r, double *x_no, int *noofa_i, int *noofa_v, int *cvofa, int *cv_part);
+/* name: 52 bytes; periodic[3] (FaZone::getPeriodicData) may be NULL */
+int jg_restart_get_zone(const jg_restart_t *r, int izone, char *name, int *kind, int *ifa_f, int *ifa_l,
+                        double *periodic);
+/* replaces the mesh (and clears the zones; one partition); records already
+ * held must fit the new counts */
+int jg_restart_set_mesh(jg_restart_t *r, int nno, int nfa, int ncv, const double *x_no, const int *noofa_i,
+                        const int *noofa_v, const int *cvofa);
+/* appends a zone; zones are added in face order and must end up covering every face */
+int jg_restart_add_zone(jg_restart_t *r, const char *name, int kind, int ifa_f, int ifa_l, const double *periodic);
+/* irec = -1 when no record has that name */
+int jg_restart_find(const jg_restart_t *r, const char *name, int *irec);
+/* count = items (cells, nodes or faces; 0 for I0 / D0), width = doubles per
+ * item (1, 3, 9); data[count*width] may be NULL; any other pointer may be NULL */
+int jg_restart_get_record(const jg_restart_t *r, int irec, char *name, int *kind, int *count, int *width,
+                          double *data, int *ivalue, double *dvalue);
+/* replaces the record of that name in place, or appends it; array kinds take
+ * one item per cell / node / face of the mesh */
+int jg_restart_put_record(jg_restart_t *r, const char *name, int kind, const double *data, int ivalue,
+                          double dvalue);
+/* the handle's state into the restart (its mesh must have the handle's cells, in
+ * the handle's caller order): STEP, RHO, RHOE, the model's scalars (nuSA; kine,
+ * omega) and RHOU; the other records are left as they are. */
+int jg_restart_save_state(jg_restart_t *r, jg_case_t *h);
+/* the handle's state from the restart as readRestart + initialHook leave the
+ * reference (JoeWithModels.cpp:20-31, 201-213): RHO, RHOU, RHOE, the model's
+ * scalars, and STEP (0 when absent) with the CFL back at jg_params.cfl, as
+ * runBackwardEuler resumes after a restart (JoeWithModels.cpp:975-978). */
+int jg_restart_load_state(jg_case_t *h, const jg_restart_t *r);
 
 /* Per-face Euler fluxes and implicit matrices, batched over n faces on the
  * GPU: calcEulerFlux_{HLLC,Roe,AUSM} and calcEulerFluxMatrices_{HLLC,Roe}

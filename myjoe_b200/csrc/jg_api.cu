@@ -1468,6 +1468,19 @@ int jg_get_cfl_step(jg_case_t* h, double* cfl, int* step) {
   return JG_OK;
 }
 
+int jg_set_cfl_step(jg_case_t* h, double cfl, int step) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (step < 0 || !(cfl >= 0.0)) return set_err(JG_ERR_ARG, "bad cfl or step");
+  double ctrl[16];
+  CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  ctrl[0] = cfl;
+  ctrl[1] = (double)step;
+  CK(cudaMemcpyAsync(h->st.ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return JG_OK;
+}
+
 int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
                         double* F, double* AL, double* AR) {
   if (n < 0 || !L || !R || !area || !nvec || !F) return set_err(JG_ERR_ARG, "bad argument");
@@ -1651,6 +1664,15 @@ int serve_case_launch(jg_case* h, int nsteps, double* h_ring, int* h_err, cudaEv
 size_t serve_case_bytes(jg_case* h) { return h->bytes; }
 int serve_case_ncv(jg_case* h) { return h->ncv; }
 int serve_set_err(int code, const char* msg) { return set_err(code, "%s", msg); }
+int case_restart_info(jg_case* h, int* ncv, int* nscal, int* turb_model, int* ncases, double* cfl0) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  *ncv = h->ncv;
+  *nscal = h->hp.turb_model == JG_TURB_NONE ? 0 : h->hp.nscal;
+  *turb_model = h->hp.turb_model;
+  *ncases = h->ncases;
+  *cfl0 = h->hp.cfl;
+  return JG_OK;
+}
 
 }  // namespace jg
 

@@ -263,4 +263,7 @@ int serve_case_ring(jg_case* h);
 size_t serve_case_bytes(jg_case* h);
 int serve_case_ncv(jg_case* h);
 int serve_set_err(int code, const char* msg);
+// what the restart bridge needs of a handle: caller cells, transported
+// scalars, turbulence model, cases, the CFL the ramp starts from
+int case_restart_info(jg_case* h, int* ncv, int* nscal, int* turb_model, int* ncases, double* cfl0);
 }  // namespace jg

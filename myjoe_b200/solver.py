@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(HERE, "libjoe_b200.so")
 _lib = None
 
 JG_ERR = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory", -4: "non-physical state",
-          -5: "no CUDA device"}
+          -5: "no CUDA device", -6: "file error"}
 
 
 class JoeGpuError(RuntimeError):
@@ -63,6 +63,7 @@ def lib():
         L.jg_step.argtypes = [P, I, D]
         L.jg_step_async.argtypes = [P, I]
         L.jg_get_cfl_step.argtypes = [P, D, C.POINTER(I)]
+        L.jg_set_cfl_step.argtypes = [P, C.c_double, I]
         L.jg_euler_flux_faces.argtypes = [I, I, D, D, D, D, D, D, D]
         L.jg_batch_create.argtypes = [I, C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
         L.jg_batch_info.argtypes = [P, C.POINTER(I), C.POINTER(I)]
@@ -286,6 +287,10 @@ class JoeGpu:
         step = C.c_int(0)
         _ck(lib().jg_get_cfl_step(self.h, C.byref(cfl), C.byref(step)))
         return cfl.value, step.value
+
+    def set_cfl_step(self, cfl, step):
+        """the CFL and step count the next step's ramp starts from (jg_set_cfl_step)"""
+        _ck(lib().jg_set_cfl_step(self.h, float(cfl), int(step)))
 
 
 def euler_flux_faces(kind, L, R, area, nvec, matrices=True):

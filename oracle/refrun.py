@@ -57,13 +57,21 @@ def _load(d):
     return out
 
 
-def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout: float = 600.0):
-    """Write the mesh (``mesh_writer(path)``) and ``Joe.in`` into a temp
-    directory, run the harness there, return (dumps, stdout)."""
+def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout: float = 600.0,
+        files: dict | None = None, collect: tuple = ()):
+    """Write the mesh (``mesh_writer(path)``, may be None) and ``Joe.in`` into a
+    temp directory, plus ``files`` (name -> bytes), run the harness there and
+    return its dumps; the files named in ``collect`` that the run wrote (e.g.
+    the restart.out runBackwardEuler leaves) come back as bytes in
+    dumps["files"]."""
     if not available():
         raise FileNotFoundError("reference harness not built: make -C oracle")
     with tempfile.TemporaryDirectory(prefix="joe_ref_") as d:
-        mesh_writer(os.path.join(d, "mesh.msh"))
+        if mesh_writer is not None:
+            mesh_writer(os.path.join(d, "mesh.msh"))
+        for name, data in (files or {}).items():
+            with open(os.path.join(d, name), "wb") as f:
+                f.write(data)
         with open(os.path.join(d, "Joe.in"), "w") as f:
             f.write(joe_in)
         out = os.path.join(d, "out")
@@ -74,6 +82,12 @@ def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout
             raise RuntimeError("reference harness failed (%d):\n%s\n%s" % (
                 p.returncode, p.stdout[-3000:], p.stderr[-3000:]))
         dumps = _load(out)
+        dumps["files"] = {}
+        for name in collect:
+            fp = os.path.join(d, name)
+            if os.path.exists(fp):
+                with open(fp, "rb") as f:
+                    dumps["files"][name] = f.read()
         dumps["stdout"] = p.stdout
         m = re.search(r"HARNESS_SECONDS ([0-9.eE+-]+)", p.stdout)
         if m:

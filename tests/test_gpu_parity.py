@@ -27,7 +27,7 @@ from tests.golden.make_golden import load
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith(("converged_", "sa_", "sst_")))
+                if not os.path.basename(p).startswith(("converged_", "sa_", "sst_", "restart_")))
 TOL = 1e-12
 
 

@@ -13,7 +13,7 @@ from myjoe_b200.case import SOLVER_KINDS
 from tests.golden.make_golden import load
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith(("converged_", "sa_", "sst_")))
+                if not os.path.basename(p).startswith(("converged_", "sa_", "sst_", "restart_")))
 
 
 @pytest.fixture(params=GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])

@@ -121,8 +121,13 @@ typedef struct jg_params {
 /* JG_GRAD_LSQ: least squares (calcCvScalarGrad / calcCvVectorGrad, UgpWithCv.h:1009-1083);
  * JG_GRAD_GREENGAUSS: Green-Gauss with distance-weighted face values
  * (calcCvScalarGradGreenGauss / calcCvVectorGradGreenGauss, UgpWithCv.h:1091-1184, GG_WITH_DIST);
- * both followed by the same Barth-Jespersen limiter.  Green-Gauss: cases without a turbulence model. */
-enum { JG_GRAD_LSQ = 0, JG_GRAD_GREENGAUSS = 1 };
+ * both followed by the same Barth-Jespersen limiter.
+ * JG_GRAD_SDWLS: solution-dependent weighted least squares (calcCvScalarGradSDWLS /
+ * calcCvVectorGradSDWLS, UgpWithCv.h:1418-1800): per cell and per quantity, the neighbours and
+ * boundary faces weighted 1 / (|dx|^2 (|dphi| + eps ref)), ref = rho, p, h, and the speed of sound
+ * for the velocity; no limiter (limiter must be 0, as the reference sets it).
+ * Green-Gauss and SDWLS: cases without a turbulence model. */
+enum { JG_GRAD_LSQ = 0, JG_GRAD_GREENGAUSS = 1, JG_GRAD_SDWLS = 2 };
 /* Cell and face order inside a handle.  JG_RENUMBER_NONE keeps the caller's
  * order (a mesh the reference loaded is already in reverse Cuthill-McKee
  * order, Ugp::init, src/common/Ugp.cpp:3389-3399).  JG_RENUMBER_RCM renumbers

@@ -102,7 +102,9 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_
     q.nscal = p.nscal
     q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
     q.renumber = 1 if renumber else 0
-    q.grad_scheme = 1 if p.GRAD_SCHEME == "GREENGAUSS" else 0
+    q.grad_scheme = {"LEASTSQUARES": 0, "GREENGAUSS": 1, "SDWLS": 2}[p.GRAD_SCHEME]
+    if q.grad_scheme == 2:
+        q.limiter = 0   # SDWLS applies no limiter (limiterNavierS = 0, UgpWithCvCompFlow.h:275-280)
     return q
 
 

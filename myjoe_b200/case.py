@@ -56,7 +56,7 @@ class JoeParams:
     SPACE_INTEGRATION: str = "HLLC"
     LIMITER: bool = True
     EPS: float = 0.01
-    GRAD_SCHEME: str = "LEASTSQUARES"   # GRAD_RECONSTRUCTION SCHEME: LEASTSQUARES or GREENGAUSS
+    GRAD_SCHEME: str = "LEASTSQUARES"   # GRAD_RECONSTRUCTION SCHEME: LEASTSQUARES, GREENGAUSS or SDWLS
     VISC_LIMITER: bool = True
     SYMM_BC: str = "ORIGINAL_NUMERIC"
     TIME_STEP: str = "MAX_BASED"

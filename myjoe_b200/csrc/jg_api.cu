@@ -270,10 +270,12 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "transported scalars need a turbulence model");
   }
   if (q->time_step_mode < 0 || q->time_step_mode > 2) return set_err(JG_ERR_ARG, "bad time step mode");
-  if (q->grad_scheme != JG_GRAD_LSQ && q->grad_scheme != JG_GRAD_GREENGAUSS)
+  if (q->grad_scheme != JG_GRAD_LSQ && q->grad_scheme != JG_GRAD_GREENGAUSS && q->grad_scheme != JG_GRAD_SDWLS)
     return set_err(JG_ERR_ARG, "unsupported gradient scheme %d", q->grad_scheme);
-  if (q->grad_scheme == JG_GRAD_GREENGAUSS && q->turb_model != JG_TURB_NONE)
-    return set_err(JG_ERR_ARG, "Green-Gauss gradients: cases without a turbulence model");
+  if (q->grad_scheme != JG_GRAD_LSQ && q->turb_model != JG_TURB_NONE)
+    return set_err(JG_ERR_ARG, "Green-Gauss and SDWLS gradients: cases without a turbulence model");
+  if (q->grad_scheme == JG_GRAD_SDWLS && q->limiter)
+    return set_err(JG_ERR_ARG, "SDWLS gradients take no limiter (limiter = 0)");
   if (q->renumber != JG_RENUMBER_NONE && q->renumber != JG_RENUMBER_RCM)
     return set_err(JG_ERR_ARG, "unsupported renumbering %d", q->renumber);
   if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");

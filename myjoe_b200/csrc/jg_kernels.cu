@@ -298,6 +298,101 @@ __device__ __forceinline__ double bj_factor(double phi_c, double phifa, double p
   return (dp * dp + 2.0 * dm * dp + eps2) / (dp * dp + 2 * dm * dm + dm * dp + eps2);
 }
 
+// calcCvScalarGradSDWLS / calcCvVectorGradSDWLS (UgpWithCv.h:1418-1800) for one cell.  Each quantity
+// weighs its neighbours and boundary faces by 1 / (|dx|^2 (|dphi| + e)) (van Leer weight, geomWeighting
+// |dx|^2, UgpWithCv.h:16-23; the velocity by |du|), so each has its own moment matrix: a first pass
+// sums the four matrices, a second applies their adjugates.  e = max(EPS ref, 1e-8) for rho, p, h
+// (ref = the quantity itself), EPS c for the velocity.
+struct Sdwls {
+  double sw[6];  // xx yy zz xy xz yz
+  __device__ void add(double w, const double* dx) {
+    sw[0] += w * dx[0] * dx[0];
+    sw[1] += w * dx[1] * dx[1];
+    sw[2] += w * dx[2] * dx[2];
+    sw[3] += w * dx[0] * dx[1];
+    sw[4] += w * dx[0] * dx[2];
+    sw[5] += w * dx[1] * dx[2];
+  }
+  __device__ double denom() const {
+    return 2.0 * sw[3] * sw[4] * sw[5] + sw[0] * sw[1] * sw[2] - sw[0] * sw[5] * sw[5] - sw[1] * sw[4] * sw[4] -
+           sw[2] * sw[3] * sw[3];
+  }
+  // adjugate row j . dx
+  __device__ double row(int j, const double* dx) const {
+    if (j == 0)
+      return (sw[1] * sw[2] - sw[5] * sw[5]) * dx[0] + (sw[4] * sw[5] - sw[3] * sw[2]) * dx[1] +
+             (sw[3] * sw[5] - sw[4] * sw[1]) * dx[2];
+    if (j == 1)
+      return (sw[4] * sw[5] - sw[3] * sw[2]) * dx[0] + (sw[0] * sw[2] - sw[4] * sw[4]) * dx[1] +
+             (sw[3] * sw[4] - sw[5] * sw[0]) * dx[2];
+    return (sw[3] * sw[5] - sw[4] * sw[1]) * dx[0] + (sw[3] * sw[4] - sw[5] * sw[0]) * dx[1] +
+           (sw[0] * sw[1] - sw[3] * sw[3]) * dx[2];
+  }
+};
+
+// one neighbour (or boundary face) at offset dx with values (u, rho, p, h) = v: pass 0 adds to the
+// moments, pass 1 to the gradients
+__device__ __forceinline__ void sdwls_visit(int pass, const double* dx, const double* vc, const double* v,
+                                            const double* e, Sdwls* M, const double* den, double* gu, double* gr,
+                                            double* gpr, double* gh) {
+  const double dist2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+  double du[3], du2 = 0.0;
+  for (int i = 0; i < 3; i++) {
+    du[i] = v[i] - vc[i];
+    du2 += du[i] * du[i];
+  }
+  const double d[3] = {v[3] - vc[3], v[4] - vc[4], v[5] - vc[5]};  // rho, p, h
+  const double wu = 1.0 / (dist2 * (sqrt(du2) + e[0]));
+  double ws[3];
+  for (int q = 0; q < 3; q++) ws[q] = 1.0 / (dist2 * (fabs(d[q]) + e[1 + q]));
+  if (pass == 0) {
+    M[0].add(wu, dx);
+    for (int q = 0; q < 3; q++) M[1 + q].add(ws[q], dx);
+    return;
+  }
+  for (int j = 0; j < 3; j++) {
+    const double t = wu * M[0].row(j, dx) / den[0];
+    for (int i = 0; i < 3; i++) gu[3 * i + j] += du[i] * t;
+  }
+  double* gs[3] = {gr, gpr, gh};
+  for (int q = 0; q < 3; q++)
+    for (int j = 0; j < 3; j++) gs[q][j] += d[q] * ws[q] * M[1 + q].row(j, dx) / den[1 + q];
+}
+
+__device__ void grad_sdwls(const Mesh& m, const Params& p, const State& st, int c, double* gu, double* gr,
+                           double* gpr, double* gh) {
+  const double* pc = &st.prim[8 * c];
+  const double vc[6] = {pc[0], pc[1], pc[2], st.q[5 * c], pc[3], pc[5]};
+  const double e[4] = {p.eps * pc[6], fmax(p.eps * vc[3], 1.0e-8), fmax(p.eps * vc[4], 1.0e-8),
+                       fmax(p.eps * vc[5], 1.0e-8)};
+  Sdwls M[4];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) M[q].sw[k] = 0.0;
+  double den[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = 0; j < 9; j++) gu[j] = 0.0;
+  for (int j = 0; j < 3; j++) gr[j] = gpr[j] = gh[j] = 0.0;
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 1)
+      for (int q = 0; q < 4; q++) den[q] = M[q].denom();
+    for (int k = m.nb_i[c] + 1; k < m.nb_i[c + 1]; k++) {
+      const int nb = m.nb_v[k];
+      const double* pn = &st.prim[8 * nb];
+      const double v[6] = {pn[0], pn[1], pn[2], st.q[5 * nb], pn[3], pn[5]};
+      double dx[3];
+      for (int i = 0; i < 3; i++) dx[i] = m.x_cv[3 * nb + i] - m.x_cv[3 * c + i];
+      sdwls_visit(pass, dx, vc, v, e, M, den, gu, gr, gpr, gh);
+    }
+    for (int k = m.bf_i[c]; k < m.bf_i[c + 1]; k++) {
+      const int f = m.bf_v[k];
+      const double* b = &st.bfa[8 * f];
+      const double v[6] = {b[1], b[2], b[3], b[0], b[4], b[6]};
+      double dx[3];
+      for (int i = 0; i < 3; i++) dx[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+      sdwls_visit(pass, dx, vc, v, e, M, den, gu, gr, gpr, gh);
+    }
+  }
+}
+
 __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, int visc_lim_u, int visc_lim_h,
                        int separate_guv) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -413,6 +508,7 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
       gh[j] /= V;
     }
   }
+  if (p.grad_scheme == JG_GRAD_SDWLS) grad_sdwls(m, p, st, c, gu, gr, gpr, gh);
   // limiter factors over the internal faces of the cell
   double au[3] = {1.0, 1.0, 1.0}, ar = 1.0, ap = 1.0, ah = 1.0;
   const double eps = p.eps;

@@ -459,10 +459,135 @@ static void grad_vector_gg(jo_case *h, double *g, const double *u, const double 
     for (int k = 0; k < 9; k++) g[9 * c + k] /= m->cv_volume[c];
 }
 
+/* SDWLS weight of one neighbour or boundary face: 1 / (|dx|^2 (limiterWeight(d) + e)) with the van
+ * Leer weight limiterWeight(a) = |a| and geomWeighting's |dx|^2 (UgpWithCv.h:16-23) */
+static double sdwls_weight(const double dx[3], double dphi_abs, double e) {
+  double dist2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+  return 1.0 / (dist2 * (dphi_abs + e));
+}
+
+/* the weighted moments sw[6] = {xx, yy, zz, xy, xz, yz} */
+static void sdwls_moment_add(double sw[6], double w, const double dx[3]) {
+  sw[0] += w * dx[0] * dx[0];
+  sw[1] += w * dx[1] * dx[1];
+  sw[2] += w * dx[2] * dx[2];
+  sw[3] += w * dx[0] * dx[1];
+  sw[4] += w * dx[0] * dx[2];
+  sw[5] += w * dx[1] * dx[2];
+}
+
+/* the determinant of the moment matrix */
+static double sdwls_denom(const double sw[6]) {
+  return 2.0 * sw[3] * sw[4] * sw[5] + sw[0] * sw[1] * sw[2] - sw[0] * sw[5] * sw[5] - sw[1] * sw[4] * sw[4] -
+         sw[2] * sw[3] * sw[3];
+}
+
+/* row j of the adjugate of the moment matrix applied to dx */
+static double sdwls_row(const double sw[6], int j, const double dx[3]) {
+  if (j == 0)
+    return (sw[1] * sw[2] - sw[5] * sw[5]) * dx[0] + (sw[4] * sw[5] - sw[3] * sw[2]) * dx[1] +
+           (sw[3] * sw[5] - sw[4] * sw[1]) * dx[2];
+  if (j == 1)
+    return (sw[4] * sw[5] - sw[3] * sw[2]) * dx[0] + (sw[0] * sw[2] - sw[4] * sw[4]) * dx[1] +
+           (sw[3] * sw[4] - sw[5] * sw[0]) * dx[2];
+  return (sw[3] * sw[5] - sw[4] * sw[1]) * dx[0] + (sw[3] * sw[4] - sw[5] * sw[0]) * dx[1] +
+         (sw[0] * sw[1] - sw[3] * sw[3]) * dx[2];
+}
+
+/* calcCvScalarGradSDWLS (UgpWithCv.h:1418-1585): per cell, least squares over the neighbours and the
+ * boundary faces with solution-dependent weights; e = max(EPS ref, SDWLSClippingScalar); no limiter */
+static void grad_scalar_sdwls(jo_case *h, double *g, const double *phi, const double *phi_bfa, const double *ref) {
+  const jg_mesh *m = &h->m;
+  for (int c = 0; c < h->ncv; c++) {
+    double sw[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double e = dmax(h->p.eps * ref[c], SDWLS_CLIP_SCALAR);
+    const int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
+    for (int pass = 0; pass < 2; pass++) {
+      double denom = pass ? sdwls_denom(sw) : 0.0;
+      if (pass)
+        for (int i = 0; i < 3; i++) g[3 * c + i] = 0.0;
+      for (int k = nf + 1; k <= nl; k++) {
+        int nb = m->nbocv_v[k];
+        double dp = phi[nb] - phi[c], dx[3];
+        for (int i = 0; i < 3; i++) dx[i] = m->x_cv[3 * nb + i] - m->x_cv[3 * c + i];
+        double w = sdwls_weight(dx, fabs(dp), e);
+        if (!pass) sdwls_moment_add(sw, w, dx);
+        else
+          for (int i = 0; i < 3; i++) g[3 * c + i] += dp * w * sdwls_row(sw, i, dx) / denom;
+      }
+      for (int k = m->faocv_i[c]; k < m->faocv_i[c + 1]; k++) {
+        int f = m->faocv_v[k];
+        if (f >= h->nfa_b) continue;
+        double dp = phi_bfa[f] - phi[c], dx[3];
+        for (int i = 0; i < 3; i++) dx[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c + i];
+        double w = sdwls_weight(dx, fabs(dp), e);
+        if (!pass) sdwls_moment_add(sw, w, dx);
+        else
+          for (int i = 0; i < 3; i++) g[3 * c + i] += dp * w * sdwls_row(sw, i, dx) / denom;
+      }
+    }
+  }
+}
+
+/* calcCvVectorGradSDWLS (UgpWithCv.h:1589-1800): the weight from |du|, e = EPS ref (no clipping) */
+static void grad_vector_sdwls(jo_case *h, double *g, const double *u, const double *u_bfa, const double *ref) {
+  const jg_mesh *m = &h->m;
+  for (int c = 0; c < h->ncv; c++) {
+    double sw[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double e = h->p.eps * ref[c];
+    const int nf = m->nbocv_i[c], nl = m->nbocv_i[c + 1] - 1;
+    for (int pass = 0; pass < 2; pass++) {
+      double denom = pass ? sdwls_denom(sw) : 0.0;
+      if (pass)
+        for (int k = 0; k < 9; k++) g[9 * c + k] = 0.0;
+      for (int k = nf + 1; k <= nl; k++) {
+        int nb = m->nbocv_v[k];
+        double du[3], du2 = 0.0, dx[3];
+        for (int i = 0; i < 3; i++) {
+          du[i] = u[3 * nb + i] - u[3 * c + i];
+          du2 += du[i] * du[i];
+        }
+        for (int i = 0; i < 3; i++) dx[i] = m->x_cv[3 * nb + i] - m->x_cv[3 * c + i];
+        double w = sdwls_weight(dx, fabs(sqrt(du2)), e);
+        if (!pass) sdwls_moment_add(sw, w, dx);
+        else
+          for (int j = 0; j < 3; j++) {
+            double t = w * sdwls_row(sw, j, dx) / denom;
+            for (int i = 0; i < 3; i++) g[9 * c + 3 * i + j] += du[i] * t;
+          }
+      }
+      for (int k = m->faocv_i[c]; k < m->faocv_i[c + 1]; k++) {
+        int f = m->faocv_v[k];
+        if (f >= h->nfa_b) continue;
+        double du[3], du2 = 0.0, dx[3];
+        for (int i = 0; i < 3; i++) {
+          du[i] = u_bfa[3 * f + i] - u[3 * c + i];
+          du2 += du[i] * du[i];
+        }
+        for (int i = 0; i < 3; i++) dx[i] = m->x_fa[3 * f + i] - m->x_cv[3 * c + i];
+        double w = sdwls_weight(dx, fabs(sqrt(du2)), e);
+        if (!pass) sdwls_moment_add(sw, w, dx);
+        else
+          for (int j = 0; j < 3; j++) {
+            double t = w * sdwls_row(sw, j, dx) / denom;
+            for (int i = 0; i < 3; i++) g[9 * c + 3 * i + j] += du[i] * t;
+          }
+      }
+    }
+  }
+}
+
 static void grad_scalar(jo_case *h, double *g, const double *phi, const double *phi_bfa, int limit,
                         const double *ref, double *alpha) {
   const jg_mesh *m = &h->m;
-  /* calcCvScalarGrad(grad, phi) + boundary part, UgpWithCv.h:1009-1056 (or Green-Gauss) */
+  /* calcCvScalarGrad(grad, phi) + boundary part, UgpWithCv.h:1009-1056 (or Green-Gauss); SDWLS
+   * takes no limiter (calcCvScalarGrad's GRAD_SDWLS case, UgpWithCv.h:826-828) */
+  if (h->p.grad_scheme == JG_GRAD_SDWLS) {
+    grad_scalar_sdwls(h, g, phi, phi_bfa, ref);
+    if (alpha)
+      for (int c = 0; c < h->ncv; c++) alpha[c] = 1.0;
+    return;
+  }
   if (h->p.grad_scheme == JG_GRAD_GREENGAUSS) grad_scalar_gg(h, g, phi, phi_bfa);
   else
   for (int c = 0; c < h->ncv; c++) {
@@ -512,6 +637,10 @@ static void grad_scalar(jo_case *h, double *g, const double *phi, const double *
 static void grad_vector(jo_case *h, double *g, const double *u, const double *u_bfa, int limit, const double *ref) {
   const jg_mesh *m = &h->m;
   /* calcCvVectorGrad(grad, u) + boundary part, UgpWithCv.h:1031-1083; g[c][i][j] = d u_i / d x_j */
+  if (h->p.grad_scheme == JG_GRAD_SDWLS) {
+    grad_vector_sdwls(h, g, u, u_bfa, ref);
+    return;
+  }
   if (h->p.grad_scheme == JG_GRAD_GREENGAUSS) grad_vector_gg(h, g, u, u_bfa);
   else
   for (int c = 0; c < h->ncv; c++) {

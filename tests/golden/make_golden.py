@@ -63,6 +63,10 @@ def cases():
     yield "plate_roe_greengauss", rawp, dataclasses.replace(prmp, GRAD_SCHEME="GREENGAUSS")
     yield "bump_roe_laminar_greengauss_novisclim", raw, dataclasses.replace(visc, bcs=bc_iso, GRAD_SCHEME="GREENGAUSS",
                                                                           VISC_LIMITER=False)
+    # SDWLS gradients (GRAD_RECONSTRUCTION SCHEME=SDWLS): inviscid second order, laminar plate, isothermal wall
+    yield "bump_hllc_sdwls", raw, dataclasses.replace(prm, GRAD_SCHEME="SDWLS")
+    yield "plate_roe_sdwls", rawp, dataclasses.replace(prmp, GRAD_SCHEME="SDWLS")
+    yield "bump_roe_laminar_sdwls_isothermal", raw, dataclasses.replace(visc, bcs=bc_iso, GRAD_SCHEME="SDWLS")
     yield "bump_haenel", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
     yield "bump_haenel_laminar_isothermal", raw, dataclasses.replace(visc, SPACE_INTEGRATION="HAENEL", bcs=bc_iso)
     yield "bump_haenel_first_order_symm_new", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL",

@@ -47,7 +47,7 @@ enum {
 /* SPACE_INTEGRATION: HLLC, ROE, AUSM (implicit side: the HLLC matrices) and HAENEL
  * (Haenel & Schwane, calcEulerFlux_HAENEL / calcEulerFluxMatrices_HAENEL,
  * UgpWithCvCompFlow.cpp:1329-1505; also AUSMDV with SHOCK_FIX_TYPE = HAENEL) */
-enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2, JG_FLUX_HAENEL = 3 };
+enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2, JG_FLUX_HAENEL = 3, JG_FLUX_AUSMDV = 4 };
 enum { JG_MU_POWERLAW = 0, JG_MU_SUTHERLAND = 1 };
 enum { JG_SYMM_ORIGINAL_NUMERIC = 0, JG_SYMM_NEW_NUMERIC = 1, JG_SYMM_ANALYTICAL = 2 };
 enum { JG_TS_CFL = 0, JG_TS_CFL_MIN = 1, JG_TS_DT = 2 };
@@ -117,7 +117,24 @@ typedef struct jg_params {
                           (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
   int renumber;        /* JG_RENUMBER_*: the handle's own cell/face order (jg_create only) */
   int grad_scheme;     /* GRAD_RECONSTRUCTION SCHEME: JG_GRAD_* (the flow gradients of calcEulerFlux) */
+  /* AUSMDV family (flux = JG_FLUX_AUSMDV; UgpWithCvCompFlow.h:198-234): */
+  int ausm_type;       /* SPACE_INTEGRATION AUSMDV / AUSMV / AUSMD: JG_AUSM_* */
+  int shock_fix;       /* SHOCK_FIX_TYPE: JG_SHOCK_FIX_* */
+  int shock_flag;      /* SHOCK_FIX_FLAG: JG_SHOCK_FLAG_* */
+  int entropy_fix;     /* ENTROPY_FIX EXPANSION_FAN: 1, NONE: 0 */
 } jg_params;
+/* AUSMDV (Wada & Liou, calcEulerFlux_AUSMDV / calcEulerFluxMatrices_AUSMDV,
+ * UgpWithCvCompFlow.cpp:879-1322): the AUSMD / AUSMV blend, the entropy fix for
+ * single expansion waves, and the shock fix of JoeWithModels.cpp:2753-2781 and
+ * 2933-2957: every step the cells beside a sonic internal face are flagged; an
+ * internal face whose two cells are flagged (JG_SHOCK_FLAG_HEX; either cell:
+ * JG_SHOCK_FLAG_TET), sonic faces included (the reference defines
+ * SHOCKFIX_ACROSS_SHOCK), takes the Haenel & Schwane flux (JG_SHOCK_FIX_HAENEL)
+ * or AUSMDV with alpha from the densities (JG_SHOCK_FIX_ALPHA_LR).
+ * Boundary faces take AUSMDV without the shock fix.  Cases without a turbulence model. */
+enum { JG_AUSM_DV = 0, JG_AUSM_V = 1, JG_AUSM_D = 2 };
+enum { JG_SHOCK_FIX_NONE = 0, JG_SHOCK_FIX_HAENEL = 1, JG_SHOCK_FIX_ALPHA_LR = 2 };
+enum { JG_SHOCK_FLAG_HEX = 0, JG_SHOCK_FLAG_TET = 1 };
 /* JG_GRAD_LSQ: least squares (calcCvScalarGrad / calcCvVectorGrad, UgpWithCv.h:1009-1083);
  * JG_GRAD_GREENGAUSS: Green-Gauss with distance-weighted face values
  * (calcCvScalarGradGreenGauss / calcCvVectorGradGreenGauss, UgpWithCv.h:1091-1184, GG_WITH_DIST);

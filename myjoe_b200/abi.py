@@ -7,7 +7,8 @@ import ctypes as C
 
 import numpy as np
 
-from .case import BC_KINDS, FLUX_KINDS, SOLVER_KINDS, SYMM_BC_KINDS, JoeParams
+from .case import (AUSM_TYPES, BC_KINDS, FLUX_KINDS, SHOCK_FIX_KINDS, SHOCK_FLAG_KINDS, SOLVER_KINDS, SYMM_BC_KINDS,
+                   JoeParams)
 
 
 class jg_zone(C.Structure):
@@ -43,7 +44,8 @@ class jg_params(C.Structure):
                 ("lin_solver", C.c_int), ("ls_max_iter", C.c_int),
                 ("ls_abs", C.c_double), ("ls_rel", C.c_double),
                 ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int),
-                ("grad_scheme", C.c_int)]
+                ("grad_scheme", C.c_int),
+                ("ausm_type", C.c_int), ("shock_fix", C.c_int), ("shock_flag", C.c_int), ("entropy_fix", C.c_int)]
 
 
 class jg_serve_config(C.Structure):
@@ -78,6 +80,11 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_
     q.PrTurb = p.PRTURB
     q.mu_mode = 1 if p.MU_MODE == "SUTHERLAND" else 0
     q.flux = FLUX_KINDS[p.SPACE_INTEGRATION]
+    if q.flux == 4:
+        q.ausm_type = AUSM_TYPES[p.SPACE_INTEGRATION]
+        q.shock_fix = SHOCK_FIX_KINDS[p.SHOCK_FIX_TYPE]
+        q.shock_flag = SHOCK_FLAG_KINDS[p.SHOCK_FIX_FLAG]
+        q.entropy_fix = int(p.ENTROPY_FIX == "EXPANSION_FAN")
     q.mu_ref = p.MU_REF
     q.mu_power_law = p.MU_POWER_LAW
     q.SL_Tref = p.SL_TREF

@@ -21,7 +21,10 @@ BC_KINDS = {
     "SYMMETRY": 1, "WALL": 2, "CBC": 3, "CBC_SUBSONIC_INLET": 4,
     "CBC_SUBSONIC_OUTLET": 5, "NEUMANN": 6, "FARFIELD": 7, "NOTHING": 8,
 }
-FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2, "HAENEL": 3}
+FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2, "HAENEL": 3, "AUSMDV": 4, "AUSMV": 4, "AUSMD": 4}
+AUSM_TYPES = {"AUSMDV": 0, "AUSMV": 1, "AUSMD": 2}
+SHOCK_FIX_KINDS = {"NONE": 0, "HAENEL": 1, "ALPHA_LR": 2}
+SHOCK_FLAG_KINDS = {"CELL_FLAG_HEX": 0, "CELL_FLAG_TET": 1}
 SYMM_BC_KINDS = {"ORIGINAL_NUMERIC": 0, "NEW_NUMERIC": 1, "ANALYTICAL": 2}
 SOLVER_KINDS = {"BCGSTAB": 0, "LUSGS": 1, "JACOBI": 2, "SGS": 3, "BCGSTAB_LINELET": 4, "LINE": 5}
 
@@ -57,6 +60,10 @@ class JoeParams:
     LIMITER: bool = True
     EPS: float = 0.01
     GRAD_SCHEME: str = "LEASTSQUARES"   # GRAD_RECONSTRUCTION SCHEME: LEASTSQUARES, GREENGAUSS or SDWLS
+    # AUSMDV / AUSMV / AUSMD only (the reference's defaults)
+    SHOCK_FIX_TYPE: str = "HAENEL"      # NONE, HAENEL or ALPHA_LR
+    SHOCK_FIX_FLAG: str = "CELL_FLAG_HEX"   # or CELL_FLAG_TET
+    ENTROPY_FIX: str = "EXPANSION_FAN"  # or NONE
     VISC_LIMITER: bool = True
     SYMM_BC: str = "ORIGINAL_NUMERIC"
     TIME_STEP: str = "MAX_BASED"
@@ -117,6 +124,8 @@ class JoeParams:
             "MU_POWER_LAW = %.17g" % self.MU_POWER_LAW, "SL_TREF = %.17g" % self.SL_TREF,
             "SL_SREF = %.17g" % self.SL_SREF,
             "SPACE_INTEGRATION = %s" % self.SPACE_INTEGRATION,
+            "SHOCK_FIX_TYPE = %s" % self.SHOCK_FIX_TYPE, "SHOCK_FIX_FLAG = %s" % self.SHOCK_FIX_FLAG,
+            "ENTROPY_FIX = %s" % self.ENTROPY_FIX,
             "GRAD_RECONSTRUCTION  SCHEME=%s  LIMITER=%s  EPS=%.17g" % (self.GRAD_SCHEME,
                 "YES" if self.LIMITER else "NO", self.EPS),
             "VISC_LIMITER = %s" % ("YES" if self.VISC_LIMITER else "NO"),

@@ -244,12 +244,21 @@ static Params make_params(const jg_params& q) {
   p.flux_cl = 1;
   p.relax_variant = 0;
   p.grad_scheme = q.grad_scheme;
+  p.ausm_type = q.ausm_type;
+  p.entropy_fix = q.entropy_fix ? 1 : 0;
+  p.shock_fix = q.flux == JG_FLUX_AUSMDV ? q.shock_fix : JG_SHOCK_FIX_NONE;
+  p.shock_flag_sum = q.shock_flag == JG_SHOCK_FLAG_TET ? 0.9 : 1.1;
   return p;
 }
 
 static int check_params(const jg_params* q) {
   if (!q) return set_err(JG_ERR_ARG, "null params");
-  if (q->flux < 0 || q->flux > 3) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
+  if (q->flux < 0 || q->flux > 4) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
+  if (q->flux == JG_FLUX_AUSMDV) {
+    if (q->ausm_type < 0 || q->ausm_type > 2) return set_err(JG_ERR_ARG, "unsupported AUSM type %d", q->ausm_type);
+    if (q->shock_fix < 0 || q->shock_fix > 2) return set_err(JG_ERR_ARG, "unsupported shock fix %d", q->shock_fix);
+    if (q->shock_flag < 0 || q->shock_flag > 1) return set_err(JG_ERR_ARG, "unsupported shock flag %d", q->shock_flag);
+  }
   if (q->symm_bc < 0 || q->symm_bc > 2) return set_err(JG_ERR_ARG, "unsupported SYMM_BC %d", q->symm_bc);
   if (q->lin_solver < 0 || q->lin_solver > 5) return set_err(JG_ERR_ARG, "unsupported linear solver %d", q->lin_solver);
   if (q->precision != JG_PREC_FP64 && q->precision != JG_PREC_MIXED)
@@ -464,6 +473,9 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(dmalloc(h, &st.gh, 3 * (size_t)N));
   RC(dmalloc(h, &st.local_dt, (size_t)N));
   RC(dmalloc(h, &st.rhs, bs * (size_t)N));
+  st.shock_flag = nullptr;
+  if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE)
+    RC(dmalloc(h, &st.shock_flag, (size_t)N));
   RC(dmalloc(h, &st.b, bs * (size_t)N));
   RC(dmalloc_bytes(h, &st.D, bs * bs * (size_t)N * h->eltsz));
   RC(dmalloc_bytes(h, &st.Dinv, bs * bs * (size_t)N * h->eltsz));
@@ -1486,7 +1498,7 @@ int jg_set_cfl_step(jg_case_t* h, double cfl, int step) {
 int jg_euler_flux_faces(int kind, int n, const double* L, const double* R, const double* area, const double* nvec,
                         double* F, double* AL, double* AR) {
   if (n < 0 || !L || !R || !area || !nvec || !F) return set_err(JG_ERR_ARG, "bad argument");
-  if (kind < 0 || kind > 3) return set_err(JG_ERR_ARG, "unsupported flux %d", kind);
+  if (kind < 0 || kind > 4) return set_err(JG_ERR_ARG, "unsupported flux %d", kind);
   if (n == 0) return JG_OK;
   double *dL, *dR, *dA, *dN, *dF, *dAL = nullptr, *dAR = nullptr;
   size_t b6 = 6 * (size_t)n * 8, b3 = 3 * (size_t)n * 8;

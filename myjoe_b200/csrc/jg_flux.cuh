@@ -519,36 +519,251 @@ __device__ inline void matrices_haenel(T* AL, T* AR, const FStateT<T>& L, const 
   if (AR) haenel_side(AR, R, unR, uRuR, hR, uRm, bm, dm, area, nV);
 }
 
+// ---------------------------------------------------------------------------
+// AUSMDV (Wada & Liou), calcEulerFlux_AUSMDV and calcEulerFluxMatrices_AUSMDV,
+// UgpWithCvCompFlow.cpp:879-1322, with the split polynomials of a general alpha
+// (u_plusminus, drhou_plusminus_dQ, 753-877).  The face options `fo`:
+// bits 0-1 the blend (FO_DV 0: AUSMDV, 1: AUSMV, 2: AUSMD), bit 2 the entropy fix
+// for single expansion waves, bit 3 alpha from the densities alone (the ALPHA_LR
+// shock fix), bit 4 the Haenel & Schwane flux instead (the HAENEL shock fix).
+// ---------------------------------------------------------------------------
+enum { FO_TYPE = 3, FO_EFIX = 4, FO_ALPHA_LR = 8, FO_HAENEL = 16 };
+
+template <typename T>
+__device__ __forceinline__ T ausm_u_pm(T alpha, T un, T c, T sign) {
+  T M = sign * un / c;
+  if (T(1.0) <= M) return un;
+  if (T(0.0) <= M) return sign * alpha * c * T(0.25) * (M + T(1.0)) * (M + T(1.0)) + (T(1.0) - alpha) * un;
+  if (T(-1.0) <= M) return sign * alpha * c * T(0.25) * (M + T(1.0)) * (M + T(1.0));
+  return T(0.0);
+}
+
+template <typename T>
+__device__ __forceinline__ void ausm_drhou_pm(T b[5], T alpha, T un, T c, const T* n, T sign) {
+  T M = sign * un / c;
+  if (T(1.0) <= M) {
+    b[0] = T(0.0);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i];
+  } else if (T(0.0) <= M) {
+    b[0] = sign * T(0.25) * alpha * c * (T(1.0) - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (T(0.5) * alpha * (M + T(1.0)) + (T(1.0) - alpha));
+  } else if (T(-1.0) <= M) {
+    b[0] = sign * T(0.25) * alpha * c * (T(1.0) - M * M);
+    for (int i = 0; i < 3; i++) b[1 + i] = n[i] * (T(0.5) * alpha * (M + T(1.0)));
+  } else {
+    b[0] = T(0.0);
+    for (int i = 0; i < 3; i++) b[1 + i] = T(0.0);
+  }
+  b[4] = T(0.0);
+}
+
+// alpha_LR_L (753-759)
+template <typename T>
+__device__ __forceinline__ T ausm_alpha_L(T pL, T rhoL, T pR, T rhoR, int fo) {
+  if (fo & FO_ALPHA_LR) return T(2.0) * (T(1.0) / rhoL) / ((T(1.0) / rhoL) + (T(1.0) / rhoR));
+  return T(2.0) * (pL / rhoL) / ((pL / rhoL) + (pR / rhoR));
+}
+
+// the AUSMD / AUSMV blend weight s
+template <typename T>
+__device__ __forceinline__ T ausm_s(T pL, T pR, int fo) {
+  const int type = fo & FO_TYPE;
+  if (type == 0) return T(0.5) * fmin(T(1.0), (T(10.0) * fabs(pR - pL)) / fmin(pL, pR));
+  return type == 1 ? T(0.5) : T(-0.5);
+}
+
+// the entropy fix's wave-speed jump (cases A and B of Wada & Liou); 0 where it does not apply
+template <typename T>
+__device__ __forceinline__ T ausm_dlambda(T unL, T cL, T unR, T cR) {
+  if ((unL <= -cL) && (unR >= cR)) return T(0.0);
+  if (((unL - cL) < T(0.0)) && ((unR - cR) > T(0.0))) return (unR - cR) - (unL - cL);
+  if (((unL + cL) < T(0.0)) && ((unR + cR) > T(0.0))) return (unR + cR) - (unL + cL);
+  return T(0.0);
+}
+
+__device__ inline void flux_ausmdv(double F[5], const FState& L, const FState& R, double area, const double nV[3],
+                                   int fo) {
+  const double unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u), cL = sqrt(L.gam * L.p / L.rho);
+  const double hL = L.h + 0.5 * uLuL + 0.0;
+  const double alphaL = ausm_alpha_L(L.p, L.rho, R.p, R.rho, fo);
+  const double unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u), cR = sqrt(R.gam * R.p / R.rho);
+  const double hR = R.h + 0.5 * uRuR + 0.0;
+  const double alphaR = 2.0 - alphaL;
+  const double cLR = fmax(cL, cR);
+  const double p_half = hs_p_pm(L.p, unL, cLR, 1.0) + hs_p_pm(R.p, unR, cLR, -1.0);
+  const double uLp = ausm_u_pm(alphaL, unL, cLR, 1.0), uRm = ausm_u_pm(alphaR, unR, cLR, -1.0);
+  const double rhou_half = L.rho * uLp + R.rho * uRm;
+  const double s = ausm_s(L.p, R.p, fo);
+  const double pn = (0.5 + s) * (L.rho * unL * uLp + R.rho * unR * uRm);
+  F[0] = rhou_half;
+  if (rhou_half >= 0.0) {
+    for (int i = 0; i < 3; i++)
+      F[1 + i] = rhou_half * (L.u[i] - unL * nV[i]) + nV[i] * (p_half + pn + (0.5 - s) * rhou_half * unL);
+    F[4] = rhou_half * hL;
+  } else {
+    for (int i = 0; i < 3; i++)
+      F[1 + i] = rhou_half * (R.u[i] - unR * nV[i]) + nV[i] * (p_half + pn + (0.5 - s) * rhou_half * unR);
+    F[4] = rhou_half * hR;
+  }
+  if (fo & FO_EFIX) {
+    const double dl = 0.125 * ausm_dlambda(unL, cL, unR, cR);
+    if (dl != 0.0) {
+      F[0] -= dl * (R.rho - L.rho);
+      for (int i = 0; i < 3; i++) F[1 + i] -= dl * (R.rho * R.u[i] - L.rho * L.u[i]);
+      F[4] -= dl * (R.rho * hR - L.rho * hL);
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+// one side's convective part of the AUSMDV matrix: d(rho u_half)/dQ times the upwind side's
+// (tangential velocity, total enthalpy), plus rho u_half times their derivatives when this side is
+// the upwind one (`own`); ut / hu: the upwind side's tangential velocity and total enthalpy
+template <typename T>
+__device__ __forceinline__ void ausmdv_side(T* A, const FStateT<T>& S, bool own, T uu, T hS, T rhou_half,
+                                            const T beta[5], const T* ut, T hu, const T nV[3]) {
+  for (int e = 0; e < 25; e++) A[e] = T(0.0);
+  A[0] += beta[0];
+  for (int j = 0; j < 3; j++) A[1 + j] += beta[1 + j];
+  if (own) {
+    const T eS = hS - S.p / S.rho;
+    for (int i = 0; i < 3; i++) {
+      A[5 * (1 + i)] += beta[0] * ut[i] - rhou_half * ut[i] / S.rho;
+      for (int j = 0; j < 3; j++) A[5 * (1 + i) + 1 + j] += beta[1 + j] * ut[i] - rhou_half * nV[i] * nV[j] / S.rho;
+      A[5 * (1 + i) + 1 + i] += rhou_half / S.rho;
+    }
+    A[20] += beta[0] * hS + rhou_half * ((S.gam - T(1.0)) * uu - S.gam * eS) / S.rho;
+    for (int j = 0; j < 3; j++) A[21 + j] += beta[1 + j] * hS - rhou_half * (S.gam - T(1.0)) * S.u[j] / S.rho;
+    A[24] += rhou_half * S.gam / S.rho;
+  } else {
+    for (int i = 0; i < 3; i++) {
+      A[5 * (1 + i)] += beta[0] * ut[i];
+      for (int j = 0; j < 3; j++) A[5 * (1 + i) + 1 + j] += beta[1 + j] * ut[i];
+    }
+    A[20] += beta[0] * hu;
+    for (int j = 0; j < 3; j++) A[21 + j] += beta[1 + j] * hu;
+  }
+}
+
+template <typename T>
+__device__ inline void matrices_ausmdv(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area, const T nV[3],
+                                       int fo) {
+  const T unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u), cL = sqrt(L.gam * L.p / L.rho);
+  const T hL = L.h + T(0.5) * uLuL + T(0.0);
+  const T alphaL = ausm_alpha_L(L.p, L.rho, R.p, R.rho, fo);
+  T utL[3], utR[3];
+  for (int i = 0; i < 3; i++) utL[i] = L.u[i] - unL * nV[i];
+  const T unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u), cR = sqrt(R.gam * R.p / R.rho);
+  const T hR = R.h + T(0.5) * uRuR + T(0.0);
+  const T alphaR = T(2.0) - alphaL;
+  for (int i = 0; i < 3; i++) utR[i] = R.u[i] - unR * nV[i];
+  const T cLR = fmax(cL, cR);
+  const T uLp = ausm_u_pm(alphaL, unL, cLR, T(1.0)), uRm = ausm_u_pm(alphaR, unR, cLR, T(-1.0));
+  const T rhou_half = L.rho * uLp + R.rho * uRm;
+  const T s = ausm_s(L.p, R.p, fo);
+  T bp[5], bm[5], dp[5], dm[5];
+  ausm_drhou_pm(bp, alphaL, unL, cLR, nV, T(1.0));
+  ausm_drhou_pm(bm, alphaR, unR, cLR, nV, T(-1.0));
+  hs_dp_pm(dp, L.u, L.rho, L.p, unL, uLuL, hL, cLR, L.gam, nV, T(1.0));
+  hs_dp_pm(dm, R.u, R.rho, R.p, unR, uRuR, hR, cLR, R.gam, nV, T(-1.0));
+  T dl = T(0.0);
+  if (fo & FO_EFIX) dl = ausm_dlambda(unL, cL, unR, cR);
+  for (int side = 0; side < 2; side++) {
+    T* A = side == 0 ? AL : AR;
+    if (!A) continue;
+    const FStateT<T>& S = side == 0 ? L : R;
+    const T un = side == 0 ? unL : unR, uu = side == 0 ? uLuL : uRuR, hS = side == 0 ? hL : hR;
+    const T upm = side == 0 ? uLp : uRm;
+    const T* beta = side == 0 ? bp : bm;
+    const T* delta = side == 0 ? dp : dm;
+    const bool own = side == 0 ? (rhou_half >= T(0.0)) : (rhou_half < T(0.0));
+    ausmdv_side<T>(A, S, own, uu, hS, rhou_half, beta, side == 0 ? (own ? utL : utR) : (own ? utR : utL),
+                   side == 0 ? hR : hL, nV);
+    // P_half: u* is the upwind side's normal velocity, its derivative this side's when upwind
+    const T unstar = own ? un : (side == 0 ? unR : unL);
+    T dun[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
+    if (own) {
+      dun[0] = -un / S.rho;
+      for (int j = 0; j < 3; j++) dun[1 + j] = nV[j] / S.rho;
+    }
+    for (int i = 0; i < 3; i++) {
+      for (int j = 0; j < 4; j++)
+        A[5 * (1 + i) + j] +=
+            nV[i] * (beta[j] * ((T(0.5) + s) * un + (T(0.5) - s) * unstar) + (T(0.5) - s) * rhou_half * dun[j]);
+      A[5 * (1 + i)] += -nV[i] * (T(0.5) + s) * upm * un;
+      for (int j = 0; j < 3; j++) A[5 * (1 + i) + 1 + j] += nV[i] * (T(0.5) + s) * upm * nV[j];
+      for (int j = 0; j < 5; j++) A[5 * (1 + i) + j] += nV[i] * delta[j];
+    }
+  }
+  if (dl != T(0.0)) {
+    for (int side = 0; side < 2; side++) {
+      T* A = side == 0 ? AL : AR;
+      if (!A) continue;
+      const FStateT<T>& S = side == 0 ? L : R;
+      const T sg = side == 0 ? T(1.0) : T(-1.0);
+      const T un = side == 0 ? unL : unR, uu = side == 0 ? uLuL : uRuR, hS = side == 0 ? hL : hR;
+      // A_L += 0.125 (...), A_R -= 0.125 (...) with the side's own state
+      T a[25];
+      for (int e = 0; e < 25; e++) a[e] = T(0.0);
+      a[0] = T(0.125) * (dl + un / S.rho * (L.rho - R.rho));
+      for (int i = 0; i < 3; i++) a[5 * (1 + i)] = T(0.125) * un / S.rho * (L.rho * L.u[i] - R.rho * R.u[i]);
+      a[20] = T(0.125) * (dl * ((T(1.0) - S.gam) * (hS - uu) + S.gam * S.p / S.rho) +
+                          un / S.rho * (L.rho * hL - R.rho * hR));
+      for (int j = 0; j < 3; j++) {
+        a[1 + j] = -T(0.125) * nV[j] / S.rho * (L.rho - R.rho);
+        a[5 * (1 + j) + 1 + j] += T(0.125) * dl;
+        for (int i = 0; i < 3; i++) a[5 * (1 + i) + 1 + j] += -T(0.125) * nV[j] / S.rho * (L.rho * L.u[i] - R.rho * R.u[i]);
+        a[21 + j] = T(0.125) * (dl * (T(1.0) - S.gam) * S.u[j] - nV[j] / S.rho * (L.rho * hL - R.rho * hR));
+      }
+      a[24] = T(0.125) * dl * S.gam;
+      for (int e = 0; e < 25; e++) A[e] += sg * a[e];
+    }
+  }
+  if (AL)
+    for (int e = 0; e < 25; e++) AL[e] *= area;
+  if (AR)
+    for (int e = 0; e < 25; e++) AR[e] *= area;
+}
+
 template <int KIND>
 __device__ __forceinline__ void euler_flux_t(double F[5], const FState& L, const FState& R, double area,
-                                             const double nV[3]) {
+                                             const double nV[3], int fo = 0) {
   if (KIND == 1) flux_roe(F, L, R, area, nV);
   else if (KIND == 2) flux_ausm(F, L, R, area, nV);
   else if (KIND == 3) flux_haenel(F, L, R, area, nV);
-  else flux_hllc(F, L, R, area, nV);
+  else if (KIND == 4) {
+    if (fo & FO_HAENEL) flux_haenel(F, L, R, area, nV);
+    else flux_ausmdv(F, L, R, area, nV, fo);
+  } else flux_hllc(F, L, R, area, nV);
 }
 
 template <int KIND, typename T>
 __device__ __forceinline__ void euler_matrices_t(T* AL, T* AR, const FStateT<T>& L, const FStateT<T>& R, T area,
-                                                 const T nV[3]) {
+                                                 const T nV[3], int fo = 0) {
   if (KIND == 1) matrices_roe<T>(AL, AR, L, R, area, nV);
   else if (KIND == 3) matrices_haenel<T>(AL, AR, L, R, area, nV);
-  else matrices_hllc<T>(AL, AR, L, R, area, nV);
+  else if (KIND == 4) {
+    if (fo & FO_HAENEL) matrices_haenel<T>(AL, AR, L, R, area, nV);
+    else matrices_ausmdv<T>(AL, AR, L, R, area, nV, fo);
+  } else matrices_hllc<T>(AL, AR, L, R, area, nV);
 }
 
+// per-face entry (jg_euler_flux_faces): kind 4 is AUSMDV with the entropy fix and no shock fix
 __device__ __forceinline__ void euler_flux(int kind, double F[5], const FState& L, const FState& R, double area,
                                            const double nV[3]) {
   if (kind == 1) flux_roe(F, L, R, area, nV);
   else if (kind == 2) flux_ausm(F, L, R, area, nV);
   else if (kind == 3) flux_haenel(F, L, R, area, nV);
+  else if (kind == 4) flux_ausmdv(F, L, R, area, nV, FO_EFIX);
   else flux_hllc(F, L, R, area, nV);
 }
 
-// implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061), HAENEL its own
+// implicit side: AUSM uses the HLLC matrices (src/joe/JoeWithModels.cpp:3057-3061), HAENEL and AUSMDV their own
 __device__ __forceinline__ void euler_matrices(int kind, double* AL, double* AR, const FState& L, const FState& R,
                                                double area, const double nV[3]) {
   if (kind == 1) matrices_roe<double>(AL, AR, L, R, area, nV);
   else if (kind == 3) matrices_haenel<double>(AL, AR, L, R, area, nV);
+  else if (kind == 4) matrices_ausmdv<double>(AL, AR, L, R, area, nV, FO_EFIX);
   else matrices_hllc<double>(AL, AR, L, R, area, nV);
 }
 

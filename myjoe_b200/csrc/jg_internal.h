@@ -73,6 +73,7 @@ struct State {
   double* gh;       // [N][3]
   double* local_dt; // [N]
   double* rhs;      // [N][5] RHS of calcRhs (rho, rhou, rhoE)
+  unsigned char* shock_flag;  // [N] AUSMDV shock fix: the cell touches a sonic internal face
   double* b;        // [N][5] under-relaxed rhs of the linear system
   void* D;          // [25][N] diagonal block (double or float), component-major
   void* Dinv;       // [25][N] its inverse
@@ -136,6 +137,10 @@ struct Params {
   int flux_cl;
   int relax_variant;
   int grad_scheme;  // JG_GRAD_*
+  // AUSMDV: the blend (JG_AUSM_*), entropy fix, shock fix (JG_SHOCK_FIX_*) and the flag
+  // sum a face's two cells must exceed for it (1.1: both flagged, 0.9: either)
+  int ausm_type, entropy_fix, shock_fix;
+  double shock_flag_sum;
 };
 
 // launchers (jg_kernels.cu); all enqueue on stream s

@@ -645,6 +645,49 @@ __device__ inline void block_inverse(double* A, double* Ai) {
 // register-limited occupancy); they cost repeated reads of the cell's data.
 // Measured: the viscous Roe plate (49k cells) is 2% faster with two lanes,
 // inviscid HLLC bumps (430k cells) 1.4x faster with one.
+// AUSMDV shock sensor (JoeWithModels.cpp:2753-2781): is internal face f sonic between its
+// cells' centre states, a compression through u_n - c or u_n + c
+__device__ __forceinline__ bool face_sonic(const Mesh& m, const Params& p, const State& st, int f) {
+  const int c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
+  double nV[3], area;
+  unit_normal(m, f, nV, area);
+  const double* p0 = &st.prim[8 * c0];
+  const double* p1 = &st.prim[8 * c1];
+  const double unL = dot3(p0, nV), unR = dot3(p1, nV);
+  const double cL = sqrt(p.gamma * p0[3] / st.q[5 * c0]), cR = sqrt(p.gamma * p1[3] / st.q[5 * c1]);
+  return (((unL - cL) > 0.0) && ((unR - cR) < 0.0)) || (((unL + cL) > 0.0) && ((unR + cR) < 0.0));
+}
+
+// the cells beside a sonic internal face; cell-centric, so no two threads write one flag
+__global__ void k_shock_flag(Mesh m, Params p, State st) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  unsigned char flag = 0;
+  for (int k = m.slot_i[c]; k < m.slot_i[c + 1] && !flag; k++) {
+    const Slot s = m.slots[k];
+    if (s.nb >= 0 && face_sonic(m, p, st, s.f)) flag = 1;
+  }
+  st.shock_flag[c] = flag;
+}
+
+// the AUSMDV options of an internal face (JoeWithModels.cpp:2933-2957): the shock fix where the
+// cells' flags add up past the threshold, sonic faces included (SHOCKFIX_ACROSS_SHOCK is defined,
+// JoeWithModels.cpp:4)
+template <int KIND>
+__device__ __forceinline__ int face_opts(const Params& p, const State& st, int c0, int c1) {
+  if (KIND != 4) return 0;
+  int fo = p.ausm_type | (p.entropy_fix ? FO_EFIX : 0);
+  if (p.shock_fix != JG_SHOCK_FIX_NONE && double(st.shock_flag[c0]) + double(st.shock_flag[c1]) > p.shock_flag_sum)
+    fo |= p.shock_fix == JG_SHOCK_FIX_HAENEL ? FO_HAENEL : FO_ALPHA_LR;
+  return fo;
+}
+
+// boundary faces: AUSMDV without the shock fix (JoeWithModels.cpp:3149-3153)
+template <int KIND>
+__device__ __forceinline__ int bnd_opts(const Params& p) {
+  return KIND == 4 ? (p.ausm_type | (p.entropy_fix ? FO_EFIX : 0)) : 0;
+}
+
 template <typename BT, int KIND, int VISC, int CL>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
@@ -670,10 +713,11 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         const int c0 = s.side == 0 ? c : s.nb;
         const int c1 = s.side == 0 ? s.nb : c;
         const double sg = s.side == 0 ? -1.0 : 1.0;  // residual sign of this cell
+        const int fo = face_opts<KIND>(p, st, c0, c1);
         {
           FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
           double F[5];
-          euler_flux_t<KIND>(F, L, R, area, nV);
+          euler_flux_t<KIND>(F, L, R, area, nV, fo);
           for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
         }
         JT Ob[25];
@@ -681,7 +725,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         if (implicit) {
           FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c0)), R0 = fstate_as<JT>(cell_fstate(p, st, c1));
           JT Apl[25], Ami[25];
-          euler_matrices_t<KIND, JT>(Apl, Ami, L0, R0, (JT)area, nVt);
+          euler_matrices_t<KIND, JT>(Apl, Ami, L0, R0, (JT)area, nVt, fo);
           // row of c0: D += Apl, O(c0,c1) = Ami ; row of c1: D -= Ami, O(c1,c0) = -Apl
           if (s.side == 0) {
             for (int e = 0; e < 25; e++) { sD[e * bd + t] += Apl[e]; Ob[e] = Ami[e]; }
@@ -725,8 +769,9 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         const FStateT<JT> Bt = fstate_as<JT>(B);
         const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
         double F[5];
+        const int fob = bnd_opts<KIND>(p);
         if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-          euler_flux_t<KIND>(F, B, B, area, nV);
+          euler_flux_t<KIND>(F, B, B, area, nV, fob);
           if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
             for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
           } else {
@@ -744,22 +789,22 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
               }
             } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
               JT Apl[25], Ami[25];
-              euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt);
+              euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt, fob);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
             } else {
               JT Apl[25];
-              euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt);
+              euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt, fob);
               for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
             }
           }
         } else {
           FState L = recon(m, p, st, c, f);
-          euler_flux_t<KIND>(F, L, B, area, nV);
+          euler_flux_t<KIND>(F, L, B, area, nV, fob);
           for (int i = 0; i < 5; i++) rhs[i] -= F[i];
           if (implicit) {
             FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
             JT Apl[25];
-            euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt);
+            euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt, fob);
             for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
           }
         }
@@ -860,7 +905,7 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
       {
         FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
         double F[5];
-        euler_flux_t<KIND>(F, L, R, area, nV);
+        euler_flux_t<KIND>(F, L, R, area, nV, face_opts<KIND>(p, st, c0, c1));
         for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
       }
       if (VISC) {
@@ -882,8 +927,9 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
       FState B;
       B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
       double F[5];
+      const int fob = bnd_opts<KIND>(p);
       if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-        euler_flux_t<KIND>(F, B, B, area, nV);
+        euler_flux_t<KIND>(F, B, B, area, nV, fob);
         if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
           for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
         } else {
@@ -891,7 +937,7 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
         }
       } else {
         FState L = recon(m, p, st, c, f);
-        euler_flux_t<KIND>(F, L, B, area, nV);
+        euler_flux_t<KIND>(F, L, B, area, nV, fob);
         for (int i = 0; i < 5; i++) rhs[i] -= F[i];
       }
       if (VISC && z.kind != JG_BC_SYMMETRY) {
@@ -1384,6 +1430,7 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
   if (p.flux == JG_FLUX_ROE) launch_flux_k<BT, 1>(m, p, st, implicit, for_step, s);
   else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
   else if (p.flux == JG_FLUX_HAENEL) launch_flux_k<BT, 3>(m, p, st, implicit, for_step, s);
+  else if (p.flux == JG_FLUX_AUSMDV) launch_flux_k<BT, 4>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
 template <typename BT, int KIND, int CL>
@@ -1405,12 +1452,15 @@ static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_
   if (p.flux == JG_FLUX_ROE) launch_flux_cell_k<BT, 1>(m, p, st, for_step, s);
   else if (p.flux == JG_FLUX_AUSM) launch_flux_cell_k<BT, 2>(m, p, st, for_step, s);
   else if (p.flux == JG_FLUX_HAENEL) launch_flux_cell_k<BT, 3>(m, p, st, for_step, s);
+  else if (p.flux == JG_FLUX_AUSMDV) launch_flux_cell_k<BT, 4>(m, p, st, for_step, s);
   else launch_flux_cell_k<BT, 0>(m, p, st, for_step, s);
 }
 // residual + Jacobian: one thread per cell, so that the 32 lanes of a warp
 // walk the same face position of 32 neighbouring cells (coherent branches);
 // residual only: the light 8-lanes-per-cell kernel
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
+  if (p.flux == JG_FLUX_AUSMDV && p.shock_fix != JG_SHOCK_FIX_NONE)
+    k_shock_flag<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
   if (!implicit) {
     if (p.fp32) launch_flux_t<float>(m, p, st, 0, for_step, s);
     else launch_flux_t<double>(m, p, st, 0, for_step, s);

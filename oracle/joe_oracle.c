@@ -1236,19 +1236,232 @@ static void matrices_haenel(double (*AL)[5], double (*AR)[5], const fstate *L, c
   if (AR) haenel_side(AR, R, uRuR, hR, uRm, bm, dm, area, nV);
 }
 
-static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV) {
+/* AUSMDV options of one face: the blend (JG_AUSM_*), the entropy fix, the face's shock fix
+ * (JG_SHOCK_FIX_*: HAENEL selects the Haenel & Schwane flux, ALPHA_LR alpha from the densities) */
+typedef struct { int type, efix, shock; } ausm_opt;
+
+/* alpha_LR_L (UgpWithCvCompFlow.cpp:753-759) */
+static double ausm_alpha_L(double pL, double rhoL, double pR, double rhoR, int shock) {
+  if (shock == JG_SHOCK_FIX_ALPHA_LR) return 2.0 * (1.0 / rhoL) / ((1.0 / rhoL) + (1.0 / rhoR));
+  return 2.0 * (pL / rhoL) / ((pL / rhoL) + (pR / rhoR));
+}
+
+static double ausm_s(double pL, double pR, int type) {
+  if (type == JG_AUSM_DV) return 0.5 * dmin(1.0, (10.0 * fabs(pR - pL)) / dmin(pL, pR));
+  if (type == JG_AUSM_V) return 0.5;
+  return -0.5;
+}
+
+/* calcEulerFlux_AUSMDV (UgpWithCvCompFlow.cpp:879-971) */
+static void flux_ausmdv(double F[5], const fstate *L, const fstate *R, double area, const double *nV, ausm_opt o) {
+  double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->h + 0.5 * uLuL + L->k;
+  double alphaL = ausm_alpha_L(L->p, L->rho, R->p, R->rho, o.shock);
+  double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->h + 0.5 * uRuR + R->k;
+  double alphaR = 2.0 - alphaL;
+  double cLR = dmax(cL, cR);
+  double p_half = hs_p_pm(L->p, unL, cLR, +1.0) + hs_p_pm(R->p, unR, cLR, -1.0);
+  double unL_plus = hs_u_pm(alphaL, unL, cLR, +1.0);
+  double unR_minus = hs_u_pm(alphaR, unR, cLR, -1.0);
+  double rhou_half = L->rho * unL_plus + R->rho * unR_minus;
+  double s = ausm_s(L->p, R->p, o.type);
+  F[0] = rhou_half;
+  if (rhou_half >= 0.0) {
+    for (int i = 0; i < 3; i++)
+      F[1 + i] = rhou_half * (L->u[i] - unL * nV[i]) +
+                 nV[i] * (p_half + (0.5 + s) * (L->rho * unL * unL_plus + R->rho * unR * unR_minus) +
+                          (0.5 - s) * rhou_half * unL);
+    F[4] = rhou_half * hL;
+  } else {
+    for (int i = 0; i < 3; i++)
+      F[1 + i] = rhou_half * (R->u[i] - unR * nV[i]) +
+                 nV[i] * (p_half + (0.5 + s) * (L->rho * unL * unL_plus + R->rho * unR * unR_minus) +
+                          (0.5 - s) * rhou_half * unR);
+    F[4] = rhou_half * hR;
+  }
+  if (o.efix) {
+    double dl;
+    if ((unL <= -cL) && (unR >= cR)) dl = 0.0;
+    else if (((unL - cL) < 0.0) && ((unR - cR) > 0.0)) dl = 0.125 * ((unR - cR) - (unL - cL));
+    else if (((unL + cL) < 0.0) && ((unR + cR) > 0.0)) dl = 0.125 * ((unR + cR) - (unL + cL));
+    else dl = 0.0;
+    if (dl != 0.0) {
+      F[0] -= dl * (R->rho - L->rho);
+      for (int i = 0; i < 3; i++) F[1 + i] -= dl * (R->rho * R->u[i] - L->rho * L->u[i]);
+      F[4] -= dl * (R->rho * hR - L->rho * hL);
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] *= area;
+}
+
+/* one side of calcEulerFluxMatrices_AUSMDV (UgpWithCvCompFlow.cpp:978-1183): S this side, own: the
+ * side is upwind (rho u_half's sign), ut / hu the upwind side's tangential velocity and total
+ * enthalpy, un_o the other side's normal velocity */
+static void ausmdv_side(double (*A)[5], const fstate *S, int own, double un, double uu, double hS, double upm,
+                        double rhou_half, double s, const double *beta, const double *delta, const double *ut,
+                        double hu, double un_o, const double *nV) {
+  double unstar, dun[4];
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) A[i][j] = 0.0;
+  if (own) {
+    double eS = hS - S->p / S->rho;
+    A[0][0] += beta[0];
+    for (int j = 0; j < 3; j++) A[0][1 + j] += beta[1 + j];
+    for (int i = 0; i < 3; i++) {
+      A[1 + i][0] += beta[0] * ut[i] - rhou_half * ut[i] / S->rho;
+      for (int j = 0; j < 3; j++) A[1 + i][1 + j] += beta[1 + j] * ut[i] - rhou_half * nV[i] * nV[j] / S->rho;
+      A[1 + i][1 + i] += rhou_half / S->rho;
+    }
+    A[4][0] += beta[0] * hS + rhou_half * ((S->gam - 1.0) * uu - S->gam * eS) / S->rho;
+    for (int j = 0; j < 3; j++) A[4][1 + j] += beta[1 + j] * hS - rhou_half * (S->gam - 1.0) * S->u[j] / S->rho;
+    A[4][4] += rhou_half * S->gam / S->rho;
+    unstar = un;
+    dun[0] = -un / S->rho;
+    for (int j = 0; j < 3; j++) dun[1 + j] = nV[j] / S->rho;
+  } else {
+    A[0][0] += beta[0];
+    for (int j = 0; j < 3; j++) A[0][1 + j] += beta[1 + j];
+    for (int i = 0; i < 3; i++) {
+      A[1 + i][0] += beta[0] * ut[i];
+      for (int j = 0; j < 3; j++) A[1 + i][1 + j] += beta[1 + j] * ut[i];
+    }
+    A[4][0] += beta[0] * hu;
+    for (int j = 0; j < 3; j++) A[4][1 + j] += beta[1 + j] * hu;
+    unstar = un_o;
+    for (int j = 0; j < 4; j++) dun[j] = 0.0;
+  }
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 4; j++)
+      A[1 + i][j] += nV[i] * (beta[j] * ((0.5 + s) * un + (0.5 - s) * unstar) + (0.5 - s) * rhou_half * dun[j]);
+    A[1 + i][0] += -nV[i] * (0.5 + s) * upm * un;
+    for (int j = 0; j < 3; j++) A[1 + i][1 + j] += nV[i] * (0.5 + s) * upm * nV[j];
+    for (int j = 0; j < 5; j++) A[1 + i][j] += nV[i] * delta[j];
+  }
+}
+
+/* the entropy fix's part of one side (UgpWithCvCompFlow.cpp:1185-1283): sg = +1 for A_L, -1 for A_R */
+static void ausmdv_efix_side(double (*A)[5], const fstate *S, const fstate *L, const fstate *R, double sg, double dl,
+                             double un, double uu, double hS, double hL, double hR, const double *nV) {
+  if (sg > 0.0) {
+    A[0][0] += 0.125 * (dl + un / S->rho * (L->rho - R->rho));
+    for (int i = 0; i < 3; i++) A[1 + i][0] += 0.125 * un / S->rho * (L->rho * L->u[i] - R->rho * R->u[i]);
+    A[4][0] += 0.125 * (dl * ((1.0 - S->gam) * (hS - uu) + S->gam * S->p / S->rho) +
+                        un / S->rho * (L->rho * hL - R->rho * hR));
+    for (int j = 0; j < 3; j++) {
+      A[0][1 + j] += -0.125 * nV[j] / S->rho * (L->rho - R->rho);
+      A[1 + j][1 + j] += 0.125 * dl;
+      for (int i = 0; i < 3; i++) A[1 + i][1 + j] += -0.125 * nV[j] / S->rho * (L->rho * L->u[i] - R->rho * R->u[i]);
+      A[4][1 + j] += 0.125 * (dl * (1.0 - S->gam) * S->u[j] - nV[j] / S->rho * (L->rho * hL - R->rho * hR));
+    }
+    A[4][4] += 0.125 * dl * S->gam;
+  } else {
+    A[0][0] -= 0.125 * (dl + un / S->rho * (L->rho - R->rho));
+    for (int i = 0; i < 3; i++) A[1 + i][0] -= 0.125 * un / S->rho * (L->rho * L->u[i] - R->rho * R->u[i]);
+    A[4][0] -= 0.125 * (dl * ((1.0 - S->gam) * (hS - uu) + S->gam * S->p / S->rho) +
+                        un / S->rho * (L->rho * hL - R->rho * hR));
+    for (int j = 0; j < 3; j++) {
+      A[0][1 + j] -= -0.125 * nV[j] / S->rho * (L->rho - R->rho);
+      A[1 + j][1 + j] -= 0.125 * dl;
+      for (int i = 0; i < 3; i++) A[1 + i][1 + j] -= -0.125 * nV[j] / S->rho * (L->rho * L->u[i] - R->rho * R->u[i]);
+      A[4][1 + j] -= 0.125 * (dl * (1.0 - S->gam) * S->u[j] - nV[j] / S->rho * (L->rho * hL - R->rho * hR));
+    }
+    A[4][4] -= 0.125 * dl * S->gam;
+  }
+}
+
+/* calcEulerFluxMatrices_AUSMDV (UgpWithCvCompFlow.cpp:978-1322) */
+static void matrices_ausmdv(double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
+                            const double *nV, ausm_opt o) {
+  double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->h + 0.5 * uLuL + L->k;
+  double alphaL = ausm_alpha_L(L->p, L->rho, R->p, R->rho, o.shock);
+  double utL[3], utR[3];
+  for (int i = 0; i < 3; i++) utL[i] = L->u[i] - unL * nV[i];
+  double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->h + 0.5 * uRuR + R->k;
+  double alphaR = 2.0 - alphaL;
+  for (int i = 0; i < 3; i++) utR[i] = R->u[i] - unR * nV[i];
+  double cLR = dmax(cL, cR);
+  double unL_plus = hs_u_pm(alphaL, unL, cLR, +1.0);
+  double unR_minus = hs_u_pm(alphaR, unR, cLR, -1.0);
+  double rhou_half = L->rho * unL_plus + R->rho * unR_minus;
+  double s = ausm_s(L->p, R->p, o.type);
+  double bp[5], bm[5], dp[5], dm[5];
+  hs_drhou_pm(bp, alphaL, unL, cLR, nV, +1.0);
+  hs_drhou_pm(bm, alphaR, unR, cLR, nV, -1.0);
+  hs_dp_pm(dp, L->u, L->rho, L->p, unL, uLuL, hL, cLR, L->gam, nV, +1.0);
+  hs_dp_pm(dm, R->u, R->rho, R->p, unR, uRuR, hR, cLR, R->gam, nV, -1.0);
+  int ownL = rhou_half >= 0.0;
+  if (AL) ausmdv_side(AL, L, ownL, unL, uLuL, hL, unL_plus, rhou_half, s, bp, dp, ownL ? utL : utR, hR, unR, nV);
+  if (AR) ausmdv_side(AR, R, !ownL, unR, uRuR, hR, unR_minus, rhou_half, s, bm, dm, !ownL ? utR : utL, hL, unL, nV);
+  if (o.efix) {
+    double dl;
+    if ((unL <= -cL) && (unR >= cR)) dl = 0.0;
+    else if (((unL - cL) < 0.0) && ((unR - cR) > 0.0)) dl = ((unR - cR) - (unL - cL));
+    else if (((unL + cL) < 0.0) && ((unR + cR) > 0.0)) dl = ((unR + cR) - (unL + cL));
+    else dl = 0.0;
+    if (dl != 0.0) {
+      if (AL) ausmdv_efix_side(AL, L, L, R, +1.0, dl, unL, uLuL, hL, hL, hR, nV);
+      if (AR) ausmdv_efix_side(AR, R, L, R, -1.0, dl, unR, uRuR, hR, hL, hR, nV);
+    }
+  }
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++) {
+      if (AL) AL[i][j] *= area;
+      if (AR) AR[i][j] *= area;
+    }
+}
+
+/* the face options: fo.shock = JG_SHOCK_FIX_HAENEL selects calcEulerFlux_HAENEL
+ * (JoeWithModels.cpp:2970-2979, 3041-3050) */
+static void euler_flux_o(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV,
+                         ausm_opt o) {
   if (kind == JG_FLUX_ROE) flux_roe(F, L, R, area, nV);
   else if (kind == JG_FLUX_AUSM) flux_ausm(F, L, R, area, nV);
   else if (kind == JG_FLUX_HAENEL) flux_haenel(F, L, R, area, nV);
-  else flux_hllc(F, L, R, area, nV);
+  else if (kind == JG_FLUX_AUSMDV) {
+    if (o.shock == JG_SHOCK_FIX_HAENEL) flux_haenel(F, L, R, area, nV);
+    else flux_ausmdv(F, L, R, area, nV, o);
+  } else flux_hllc(F, L, R, area, nV);
 }
 
 /* implicit matrices per flux choice: AUSM uses the HLLC matrices (JoeWithModels.cpp:3057-3061) */
-static void euler_matrices(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
-                           const double *nV) {
+static void euler_matrices_o(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R,
+                             double area, const double *nV, ausm_opt o) {
   if (kind == JG_FLUX_ROE) matrices_roe(AL, AR, L, R, area, nV);
   else if (kind == JG_FLUX_HAENEL) matrices_haenel(AL, AR, L, R, area, nV);
-  else matrices_hllc(AL, AR, L, R, area, nV);
+  else if (kind == JG_FLUX_AUSMDV) {
+    if (o.shock == JG_SHOCK_FIX_HAENEL) matrices_haenel(AL, AR, L, R, area, nV);
+    else matrices_ausmdv(AL, AR, L, R, area, nV, o);
+  } else matrices_hllc(AL, AR, L, R, area, nV);
+}
+
+/* boundary faces and the per-face entry: AUSMDV without the shock fix */
+static ausm_opt bnd_opt(const jg_params *p) {
+  ausm_opt o = {p->ausm_type, p->entropy_fix, JG_SHOCK_FIX_NONE};
+  return o;
+}
+
+static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV,
+                       const jg_params *p) {
+  euler_flux_o(kind, F, L, R, area, nV, bnd_opt(p));
+}
+
+static void euler_matrices(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
+                           const double *nV, const jg_params *p) {
+  euler_matrices_o(kind, AL, AR, L, R, area, nV, bnd_opt(p));
+}
+
+/* AUSMDV's sonic test of an internal face at its cells' centre states (JoeWithModels.cpp:2765-2776) */
+static int face_sonic(jo_case *h, int f) {
+  const jg_mesh *m = &h->m;
+  int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+  double nV[3];
+  norm3(nV, &m->fa_normal[3 * f]);
+  double unL = dot3(&h->vel[3 * c0], nV), unR = dot3(&h->vel[3 * c1], nV);
+  double cL = sqrt(h->gam[c0] * h->press[c0] / h->rho[c0]), cR = sqrt(h->gam[c1] * h->press[c1] / h->rho[c1]);
+  return (((unL - cL) > 0.0) && ((unR - cR) < 0.0)) || (((unL + cL) > 0.0) && ((unR + cR) < 0.0));
 }
 
 void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
@@ -1259,10 +1472,12 @@ void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, cons
     /* ideal-gas enthalpy from the state */
     sl.h = sl.gam * sl.p / ((sl.gam - 1.0) * sl.rho);
     sr.h = sr.gam * sr.p / ((sr.gam - 1.0) * sr.rho);
-    euler_flux(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f]);
+    /* kind 4: AUSMDV with the entropy fix, no shock fix */
+    ausm_opt o = {JG_AUSM_DV, 1, JG_SHOCK_FIX_NONE};
+    euler_flux_o(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f], o);
     if (AL || AR)
-      euler_matrices(kind, AL ? (double(*)[5]) & AL[25 * f] : NULL, AR ? (double(*)[5]) & AR[25 * f] : NULL, &sl, &sr,
-                     area[f], &nvec[3 * f]);
+      euler_matrices_o(kind, AL ? (double(*)[5]) & AL[25 * f] : NULL, AR ? (double(*)[5]) & AR[25 * f] : NULL, &sl,
+                       &sr, area[f], &nvec[3 * f], o);
   }
 }
 
@@ -1325,6 +1540,17 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
     grad_scalar(h, h->grad_rho, h->rho, h->rho_bfa, p->limiter, h->rho, h->alpha_rho);
     grad_scalar(h, h->grad_p, h->press, h->p_bfa, p->limiter, h->press, NULL);
   }
+  /* AUSMDV shock sensor: flag the cells beside a sonic internal face (JoeWithModels.cpp:2753-2781) */
+  double *flag = NULL;
+  if (kind == JG_FLUX_AUSMDV && p->shock_fix != JG_SHOCK_FIX_NONE) {
+    flag = dalloc(h->ncv);
+    for (int f = h->nfa_b; f < h->nfa; f++)
+      if (face_sonic(h, f)) {
+        flag[m->cvofa[2 * f]] = 1.0;
+        flag[m->cvofa[2 * f + 1]] = 1.0;
+      }
+  }
+  const double flag_sum = p->shock_flag == JG_SHOCK_FLAG_TET ? 0.9 : 1.1;
   double Apl[5][5], Ami[5][5], F[5];
   for (int f = h->nfa_b; f < h->nfa; f++) {
     int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
@@ -1335,13 +1561,17 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
       reconstruct(h, c0, f, &L);
       reconstruct(h, c1, f, &R);
     }
-    euler_flux(kind, F, &L, &R, area, nV);
+    /* the face's shock fix (JoeWithModels.cpp:2933-2957): both (or either) cells flagged; with
+     * SHOCKFIX_ACROSS_SHOCK defined (JoeWithModels.cpp:4) also on the sonic faces themselves */
+    ausm_opt o = bnd_opt(p);
+    if (flag && (flag[c0] + flag[c1]) > flag_sum) o.shock = p->shock_fix;
+    euler_flux_o(kind, F, &L, &R, area, nV, o);
     rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
     rr[c1] += F[0]; for (int i = 0; i < 3; i++) ru[3 * c1 + i] += F[1 + i]; rE[c1] += F[4];
     for (int i = 0; i < 5; i++) { h->fscale[5 * c0 + i] += fabs(F[i]); h->fscale[5 * c1 + i] += fabs(F[i]); }
     if (implicit) {
       fstate L0 = cell_state(h, c0), R0 = cell_state(h, c1);
-      euler_matrices(kind, Apl, Ami, &L0, &R0, area, nV);
+      euler_matrices_o(kind, Apl, Ami, &L0, &R0, area, nV, o);
       int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
       add_block(A, n00, Apl, 1.0);
       add_block(A, n01, Ami, 1.0);
@@ -1358,7 +1588,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
       int n00 = m->nbocv_i[c0];
       if (zn->kind == JG_BC_SYMMETRY) {
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &B, &B, area, nV);
+        euler_flux(kind, F, &B, &B, area, nV, p);
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (p->symm_bc == JG_SYMM_ANALYTICAL) {
           for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= h->p_bfa[f] * nV[i] * area;
@@ -1366,7 +1596,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
           rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
         }
         if (implicit) {
-          euler_matrices(kind, Apl, Ami, &B, &B, area, nV);
+          euler_matrices(kind, Apl, Ami, &B, &B, area, nV, p);
           if (p->symm_bc == JG_SYMM_ORIGINAL_NUMERIC) add_block(A, n00, Apl, 1.0);
           else if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
             double S[5][5];
@@ -1391,28 +1621,29 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
         }
       } else if (zn->kind == JG_BC_WALL) {
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &B, &B, area, nV);
+        euler_flux(kind, F, &B, &B, area, nV, p);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {
-          euler_matrices(kind, Apl, NULL, &B, &B, area, nV);
+          euler_matrices(kind, Apl, NULL, &B, &B, area, nV, p);
           add_block(A, n00, Apl, 1.0);
         }
       } else {
         fstate L = cell_state(h, c0);
         if (p->second_order) reconstruct(h, c0, f, &L);
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &L, &B, area, nV);
+        euler_flux(kind, F, &L, &B, area, nV, p);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {
           fstate L0 = cell_state(h, c0);
-          euler_matrices(kind, Apl, NULL, &L0, &B, area, nV);
+          euler_matrices(kind, Apl, NULL, &L0, &B, area, nV, p);
           add_block(A, n00, Apl, 1.0);
         }
       }
     }
   }
+  free(flag);
 }
 
 /* ------------------------------------------------------------------------ */

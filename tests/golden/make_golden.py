@@ -67,6 +67,17 @@ def cases():
     yield "bump_hllc_sdwls", raw, dataclasses.replace(prm, GRAD_SCHEME="SDWLS")
     yield "plate_roe_sdwls", rawp, dataclasses.replace(prmp, GRAD_SCHEME="SDWLS")
     yield "bump_roe_laminar_sdwls_isothermal", raw, dataclasses.replace(visc, bcs=bc_iso, GRAD_SCHEME="SDWLS")
+    # AUSMDV family: sonic faces from a sonic inflow, the HAENEL shock fix on faces between flagged
+    # cells (CELL_FLAG_HEX), ALPHA_LR with CELL_FLAG_TET, the entropy fix on an expansion; AUSMD and AUSMV
+    rawt, _, prmt = case.bump_case(8, 4, 2, jitter=0.15, seed=7, mach=1.0)
+    rawt5, _, prmt5 = case.bump_case(8, 4, 2, jitter=0.15, seed=7, mach=1.05)
+    yield "bump_ausmdv_m1", rawt, dataclasses.replace(prmt, SPACE_INTEGRATION="AUSMDV")
+    yield "bump_ausmdv_alpha_tet_m105", rawt5, dataclasses.replace(prmt5, SPACE_INTEGRATION="AUSMDV",
+                                                                   SHOCK_FIX_TYPE="ALPHA_LR",
+                                                                   SHOCK_FIX_FLAG="CELL_FLAG_TET")
+    yield "bump_ausmv_m105", rawt5, dataclasses.replace(prmt5, SPACE_INTEGRATION="AUSMV", SHOCK_FIX_TYPE="NONE")
+    yield "bump_ausmd_first_order", raw, dataclasses.replace(prm, SPACE_INTEGRATION="AUSMD", SECOND_ORDER=False,
+                                                             ENTROPY_FIX="NONE", SHOCK_FIX_TYPE="NONE")
     yield "bump_haenel", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
     yield "bump_haenel_laminar_isothermal", raw, dataclasses.replace(visc, SPACE_INTEGRATION="HAENEL", bcs=bc_iso)
     yield "bump_haenel_first_order_symm_new", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL",

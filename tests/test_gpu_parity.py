@@ -194,10 +194,11 @@ def test_backward_euler_steps_match_reference(golden):
     np.testing.assert_allclose(res, g["resid"], rtol=6e-5)
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 def test_per_face_fluxes(kind):
-    """calcEulerFlux_{HLLC,Roe,AUSM,HAENEL} + matrices over random subsonic
-    and supersonic face states, GPU vs oracle."""
+    """calcEulerFlux_{HLLC,Roe,AUSM,HAENEL,AUSMDV} + matrices over random
+    subsonic and supersonic face states, GPU vs oracle (AUSMDV with the
+    entropy fix)."""
     rng = np.random.default_rng(11 + kind)
     n = 4096
     def states(n):

@@ -47,7 +47,11 @@ enum {
 /* SPACE_INTEGRATION: HLLC, ROE, AUSM (implicit side: the HLLC matrices) and HAENEL
  * (Haenel & Schwane, calcEulerFlux_HAENEL / calcEulerFluxMatrices_HAENEL,
  * UgpWithCvCompFlow.cpp:1329-1505; also AUSMDV with SHOCK_FIX_TYPE = HAENEL) */
-enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2, JG_FLUX_HAENEL = 3, JG_FLUX_AUSMDV = 4 };
+/* JST: Jameson-Schmidt-Turkel central flux with blended second / fourth difference dissipation
+ * (calcEulerFlux_JST, UgpWithCvCompFlow.cpp:4050-4160; the pressure sensor, spectral radii and
+ * undivided Laplacian of calcJSTCoeff_Const / calcJSTCoeff_Var, JoeWithModels.cpp:13380-13492,
+ * recomputed every residual); implicit side: the HLLC matrices (JoeWithModels.cpp:3067-3071) */
+enum { JG_FLUX_HLLC = 0, JG_FLUX_ROE = 1, JG_FLUX_AUSM = 2, JG_FLUX_HAENEL = 3, JG_FLUX_AUSMDV = 4, JG_FLUX_JST = 5 };
 enum { JG_MU_POWERLAW = 0, JG_MU_SUTHERLAND = 1 };
 enum { JG_SYMM_ORIGINAL_NUMERIC = 0, JG_SYMM_NEW_NUMERIC = 1, JG_SYMM_ANALYTICAL = 2 };
 enum { JG_TS_CFL = 0, JG_TS_CFL_MIN = 1, JG_TS_DT = 2 };

@@ -21,7 +21,7 @@ BC_KINDS = {
     "SYMMETRY": 1, "WALL": 2, "CBC": 3, "CBC_SUBSONIC_INLET": 4,
     "CBC_SUBSONIC_OUTLET": 5, "NEUMANN": 6, "FARFIELD": 7, "NOTHING": 8,
 }
-FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2, "HAENEL": 3, "AUSMDV": 4, "AUSMV": 4, "AUSMD": 4}
+FLUX_KINDS = {"HLLC": 0, "ROE": 1, "AUSM": 2, "HAENEL": 3, "AUSMDV": 4, "AUSMV": 4, "AUSMD": 4, "JST": 5}
 AUSM_TYPES = {"AUSMDV": 0, "AUSMV": 1, "AUSMD": 2}
 SHOCK_FIX_KINDS = {"NONE": 0, "HAENEL": 1, "ALPHA_LR": 2}
 SHOCK_FLAG_KINDS = {"CELL_FLAG_HEX": 0, "CELL_FLAG_TET": 1}

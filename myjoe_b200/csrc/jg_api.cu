@@ -253,7 +253,7 @@ static Params make_params(const jg_params& q) {
 
 static int check_params(const jg_params* q) {
   if (!q) return set_err(JG_ERR_ARG, "null params");
-  if (q->flux < 0 || q->flux > 4) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
+  if (q->flux < 0 || q->flux > 5) return set_err(JG_ERR_ARG, "unsupported flux %d", q->flux);
   if (q->flux == JG_FLUX_AUSMDV) {
     if (q->ausm_type < 0 || q->ausm_type > 2) return set_err(JG_ERR_ARG, "unsupported AUSM type %d", q->ausm_type);
     if (q->shock_fix < 0 || q->shock_fix > 2) return set_err(JG_ERR_ARG, "unsupported shock fix %d", q->shock_fix);
@@ -476,6 +476,16 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   st.shock_flag = nullptr;
   if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE)
     RC(dmalloc(h, &st.shock_flag, (size_t)N));
+  st.jst = nullptr;
+  st.jst_bcv = nullptr;
+  if (q->flux == JG_FLUX_JST) {
+    // calcJSTCoeff_Const (JoeWithModels.cpp:13380-13395): BoundaryCV marks the first cell of every
+    // internal face (the reference's rule, kept as it changes the dissipation)
+    RC(dmalloc(h, &st.jst, 8 * (size_t)N));
+    std::vector<unsigned char> bcv((size_t)N, 0);
+    for (int f = nfa_b; f < nfa; f++) bcv[mesh->cvofa[2 * f]] = 1;
+    RC(upload(h, &st.jst_bcv, bcv.data(), bcv.size()));
+  }
   RC(dmalloc(h, &st.b, bs * (size_t)N));
   RC(dmalloc_bytes(h, &st.D, bs * bs * (size_t)N * h->eltsz));
   RC(dmalloc_bytes(h, &st.Dinv, bs * bs * (size_t)N * h->eltsz));

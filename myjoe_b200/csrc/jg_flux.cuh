@@ -725,10 +725,47 @@ __device__ inline void matrices_ausmdv(T* AL, T* AR, const FStateT<T>& L, const 
     for (int e = 0; e < 25; e++) AR[e] *= area;
 }
 
+// ---------------------------------------------------------------------------
+// JST, calcEulerFlux_JST (UgpWithCvCompFlow.cpp:4050-4160): the central flux of
+// the arithmetic-mean state plus the blended second / fourth difference
+// dissipation; JL / JR = {pressure sensor, spectral radius, internal faces,
+// undivided Laplacian[5]} of the two cells (the boundary cell's on both sides
+// at a boundary face)
+// ---------------------------------------------------------------------------
+__device__ inline void flux_jst(double F[5], const FState& L, const FState& R, double area, const double nV[3],
+                                const double* JL, const double* JR) {
+  const double unL = dot3(L.u, nV), uLuL = dot3(L.u, L.u), cL = sqrt(L.gam * L.p / L.rho);
+  const double hL = L.gam / (L.gam - 1.0) * L.p / L.rho + 0.5 * uLuL + 0.0;
+  const double unR = dot3(R.u, nV), uRuR = dot3(R.u, R.u), cR = sqrt(R.gam * R.p / R.rho);
+  const double hR = R.gam / (R.gam - 1.0) * R.p / R.rho + 0.5 * uRuR + 0.0;
+  const double md = 0.5 * (L.rho + R.rho), mp = 0.5 * (L.p + R.p), mh = 0.5 * (hL + hR);
+  double mv[3];
+  for (int i = 0; i < 3; i++) mv[i] = 0.5 * (L.u[i] + R.u[i]);
+  const double mun = md * dot3(mv, nV);  // the mean mass flux through the face
+  F[0] = mun;
+  for (int i = 0; i < 3; i++) F[1 + i] = mun * mv[i] + mp * nV[i];
+  F[4] = mun * mh;
+  for (int i = 0; i < 5; i++) F[i] *= area;
+  double dU[5];
+  dU[0] = L.rho - R.rho;
+  for (int i = 0; i < 3; i++) dU[1 + i] = L.rho * L.u[i] - R.rho * R.u[i];
+  dU[4] = L.rho * hL - R.rho * hR;
+  const double mlam = 0.5 * ((fabs(unL) + cL) * area + (fabs(unR) + cR) * area);
+  const double phiL = pow(JL[1] / (4.0 * mlam), 0.3), phiR = pow(JR[1] / (4.0 * mlam), 0.3);
+  const double stretch = 4.0 * phiL * phiR / (phiL + phiR);
+  const double nL = JL[2], nR = JR[2];
+  const double sc2 = 3.0 * (nL + nR) / (nL * nR), sc4 = sc2 * sc2 / 4.0;
+  const double e2 = 0.5 * 0.5 * (JL[0] + JR[0]) * sc2;
+  const double e4 = fmax(0.0, 0.02 - e2) * sc4;
+  for (int i = 0; i < 5; i++) F[i] += (e2 * dU[i] - e4 * (JL[3 + i] - JR[3 + i])) * stretch * mlam;
+}
+
 template <int KIND>
 __device__ __forceinline__ void euler_flux_t(double F[5], const FState& L, const FState& R, double area,
-                                             const double nV[3], int fo = 0) {
-  if (KIND == 1) flux_roe(F, L, R, area, nV);
+                                             const double nV[3], int fo = 0, const double* JL = nullptr,
+                                             const double* JR = nullptr) {
+  if (KIND == 5) flux_jst(F, L, R, area, nV, JL, JR);
+  else if (KIND == 1) flux_roe(F, L, R, area, nV);
   else if (KIND == 2) flux_ausm(F, L, R, area, nV);
   else if (KIND == 3) flux_haenel(F, L, R, area, nV);
   else if (KIND == 4) {

@@ -74,6 +74,8 @@ struct State {
   double* local_dt; // [N]
   double* rhs;      // [N][5] RHS of calcRhs (rho, rhou, rhoE)
   unsigned char* shock_flag;  // [N] AUSMDV shock fix: the cell touches a sonic internal face
+  double* jst;                // [N][8] JST: pressure sensor, spectral radius, internal faces, undivided Laplacian[5]
+  const unsigned char* jst_bcv;  // [N] JST's BoundaryCV: the cell is the first cell of an internal face
   double* b;        // [N][5] under-relaxed rhs of the linear system
   void* D;          // [25][N] diagonal block (double or float), component-major
   void* Dinv;       // [25][N] its inverse

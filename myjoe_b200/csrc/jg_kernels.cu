@@ -682,6 +682,54 @@ __device__ __forceinline__ int face_opts(const Params& p, const State& st, int c
   return fo;
 }
 
+// JST coefficients of the current state, calcJSTCoeff_Var (JoeWithModels.cpp:13435-13492), per
+// cell over its internal faces (each face in its own orientation, as the reference's face loop
+// sees it): the spectral radius sum, the pressure sensor |sum dp| / sum (p0 + p1) and the
+// undivided Laplacian of (rho, rhou, rhoE + p), a face counting for a cell unless the cell is
+// interior-flagged and the other one not (the reference's BoundaryCV rule)
+__global__ void k_jst(Mesh m, Params p, State st) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  double lam = 0.0, p1 = 0.0, p2 = 0.0, lap[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int nint = 0;
+  for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+    const Slot s = m.slots[k];
+    if (s.nb < 0) continue;
+    nint++;
+    const int f = s.f, c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
+    double nV[3], area;
+    unit_normal(m, f, nV, area);
+    const double r0 = st.q[5 * c0], r1 = st.q[5 * c1];
+    const double P0 = st.prim[8 * c0 + 3], P1 = st.prim[8 * c1 + 3];
+    double u0[3], u1[3];
+    for (int i = 0; i < 3; i++) {
+      u0[i] = st.q[5 * c0 + 1 + i] / r0;
+      u1[i] = st.q[5 * c1 + 1 + i] / r1;
+    }
+    const double l0 = 0.5 * (fabs(dot3(u0, nV)) + sqrt(p.gamma * P0 / r0)) * area;
+    const double l1 = 0.5 * (fabs(dot3(u1, nV)) + sqrt(p.gamma * P1 / r1)) * area;
+    lam += l0;
+    lam += l1;
+    const bool first = c == c0;
+    p1 += first ? (P1 - P0) : (P0 - P1);
+    p2 += (P0 + P1);
+    const bool b0 = st.jst_bcv[c0] != 0, b1 = st.jst_bcv[c1] != 0;
+    const bool take = first ? !(b0 && !b1) : !(!b0 && b1);
+    if (take) {
+      double d[5];
+      d[0] = r0 - r1;
+      for (int i = 0; i < 3; i++) d[1 + i] = st.q[5 * c0 + 1 + i] - st.q[5 * c1 + 1 + i];
+      d[4] = (st.q[5 * c0 + 4] + P0) - (st.q[5 * c1 + 4] + P1);
+      for (int i = 0; i < 5; i++) lap[i] += first ? -d[i] : d[i];
+    }
+  }
+  double* J = &st.jst[8 * c];
+  J[0] = fabs(p1) / p2;
+  J[1] = lam;
+  J[2] = (double)nint;
+  for (int i = 0; i < 5; i++) J[3 + i] = lap[i];
+}
+
 // boundary faces: AUSMDV without the shock fix (JoeWithModels.cpp:3149-3153)
 template <int KIND>
 __device__ __forceinline__ int bnd_opts(const Params& p) {
@@ -717,7 +765,8 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         {
           FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
           double F[5];
-          euler_flux_t<KIND>(F, L, R, area, nV, fo);
+          euler_flux_t<KIND>(F, L, R, area, nV, fo, KIND == 5 ? &st.jst[8 * c0] : nullptr,
+                             KIND == 5 ? &st.jst[8 * c1] : nullptr);
           for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
         }
         JT Ob[25];
@@ -770,8 +819,9 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
         double F[5];
         const int fob = bnd_opts<KIND>(p);
+        const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
         if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-          euler_flux_t<KIND>(F, B, B, area, nV, fob);
+          euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
           if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
             for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
           } else {
@@ -799,7 +849,7 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
           }
         } else {
           FState L = recon(m, p, st, c, f);
-          euler_flux_t<KIND>(F, L, B, area, nV, fob);
+          euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
           for (int i = 0; i < 5; i++) rhs[i] -= F[i];
           if (implicit) {
             FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
@@ -905,7 +955,8 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
       {
         FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
         double F[5];
-        euler_flux_t<KIND>(F, L, R, area, nV, face_opts<KIND>(p, st, c0, c1));
+        euler_flux_t<KIND>(F, L, R, area, nV, face_opts<KIND>(p, st, c0, c1), KIND == 5 ? &st.jst[8 * c0] : nullptr,
+                           KIND == 5 ? &st.jst[8 * c1] : nullptr);
         for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
       }
       if (VISC) {
@@ -928,8 +979,9 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
       B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
       double F[5];
       const int fob = bnd_opts<KIND>(p);
+      const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
       if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-        euler_flux_t<KIND>(F, B, B, area, nV, fob);
+        euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
         if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
           for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
         } else {
@@ -937,7 +989,7 @@ __global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int fo
         }
       } else {
         FState L = recon(m, p, st, c, f);
-        euler_flux_t<KIND>(F, L, B, area, nV, fob);
+        euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
         for (int i = 0; i < 5; i++) rhs[i] -= F[i];
       }
       if (VISC && z.kind != JG_BC_SYMMETRY) {
@@ -1431,6 +1483,7 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
   else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
   else if (p.flux == JG_FLUX_HAENEL) launch_flux_k<BT, 3>(m, p, st, implicit, for_step, s);
   else if (p.flux == JG_FLUX_AUSMDV) launch_flux_k<BT, 4>(m, p, st, implicit, for_step, s);
+  else if (p.flux == JG_FLUX_JST) launch_flux_k<BT, 5>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
 template <typename BT, int KIND, int CL>
@@ -1453,6 +1506,7 @@ static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_
   else if (p.flux == JG_FLUX_AUSM) launch_flux_cell_k<BT, 2>(m, p, st, for_step, s);
   else if (p.flux == JG_FLUX_HAENEL) launch_flux_cell_k<BT, 3>(m, p, st, for_step, s);
   else if (p.flux == JG_FLUX_AUSMDV) launch_flux_cell_k<BT, 4>(m, p, st, for_step, s);
+  else if (p.flux == JG_FLUX_JST) launch_flux_cell_k<BT, 5>(m, p, st, for_step, s);
   else launch_flux_cell_k<BT, 0>(m, p, st, for_step, s);
 }
 // residual + Jacobian: one thread per cell, so that the 32 lanes of a warp
@@ -1461,6 +1515,7 @@ static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
   if (p.flux == JG_FLUX_AUSMDV && p.shock_fix != JG_SHOCK_FIX_NONE)
     k_shock_flag<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
+  if (p.flux == JG_FLUX_JST) k_jst<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
   if (!implicit) {
     if (p.fp32) launch_flux_t<float>(m, p, st, 0, for_step, s);
     else launch_flux_t<double>(m, p, st, 0, for_step, s);

@@ -37,6 +37,10 @@ struct jo_case {
   unsigned char *linelet;  /* [N] the reference's Linelet flag: the cell is on a line of >= 2 cells */
   int rnlines;      /* the LINE relaxation's lines (crossing prism/hexahedron interfaces) */
   int *rline_off, *rline_cv;
+  /* JST: per cell {PressSensor, Lambda, NeighborCV, Conserv_Und_Lapl[5]}, BoundaryCV, p1/p2_Und_Lapl */
+  double *jst;
+  unsigned char *bcv;
+  double *p1_lapl, *p2_lapl;
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -70,6 +74,17 @@ jo_case *jo_create(const jg_mesh *m, const jg_params *p) {
   h->grad_u = dalloc(9 * n); h->grad_rho = dalloc(3 * n); h->grad_p = dalloc(3 * n);
   h->grad_h = dalloc(3 * n); h->alpha_rho = dalloc(n); h->local_dt = dalloc(n);
   h->fscale = dalloc(5 * n);
+  h->jst = dalloc(8 * n);
+  h->p1_lapl = dalloc(n);
+  h->p2_lapl = dalloc(n);
+  h->bcv = (unsigned char *)calloc(n ? n : 1, 1);
+  /* calcJSTCoeff_Const (JoeWithModels.cpp:13380-13395): BoundaryCV is set on the first cell of every
+   * internal face (as the reference writes it), NeighborCV counts the internal faces of each cell */
+  for (int f = m->nfa_b; f < m->nfa; f++) {
+    h->bcv[m->cvofa[2 * f]] = 1;
+    h->jst[8 * m->cvofa[2 * f] + 2] += 1.0;
+    h->jst[8 * m->cvofa[2 * f + 1] + 2] += 1.0;
+  }
   /* initialHookScalarRansCombModel: RoM = R_gas, gamma = GAMMA (UgpWithCvCompFlow.h:1630-1640) */
   for (int i = 0; i < n; i++) { h->gam[i] = p->gamma; h->RoM[i] = p->R_gas; }
   h->cfl = p->cfl;
@@ -81,8 +96,9 @@ void jo_destroy(jo_case *h) {
   double *arrs[] = {h->rho, h->rhou, h->rhoE, h->vel, h->press, h->temp, h->enthalpy, h->sos, h->gam, h->RoM,
                     h->rho_bfa, h->T_bfa, h->vel_bfa, h->p_bfa, h->h_bfa, h->gam_bfa, h->RoM_bfa, h->mul_fa,
                     h->lamOcp_fa, h->mut_fa, h->grad_u, h->grad_rho, h->grad_p, h->grad_h, h->alpha_rho,
-                    h->local_dt, h->fscale};
+                    h->local_dt, h->fscale, h->jst, h->p1_lapl, h->p2_lapl};
   for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); i++) free(arrs[i]);
+  free(h->bcv);
   free(h->line_off);
   free(h->line_cv);
   free(h->linelet);
@@ -1413,11 +1429,105 @@ static void matrices_ausmdv(double (*AL)[5], double (*AR)[5], const fstate *L, c
     }
 }
 
+/* calcEulerFlux_JST (UgpWithCvCompFlow.cpp:4050-4160): central flux of the mean state plus the
+ * blended second / fourth difference dissipation; J = {PressSensor, Lambda, NeighborCV,
+ * Conserv_Und_Lapl[5]} of each side's cell (transported scalars: none) */
+static void flux_jst(double F[5], const fstate *L, const fstate *R, double area, const double *nV, const double *JL,
+                     const double *JR) {
+  double Param_p = 0.3, Param_Kappa_2 = 0.5, Param_Kappa_4 = 0.02;
+  double unL = dot3(L->u, nV), uLuL = dot3(L->u, L->u), cL = sqrt(L->gam * L->p / L->rho);
+  double hL = L->gam / (L->gam - 1.0) * L->p / L->rho + 0.5 * uLuL + L->k;
+  double unR = dot3(R->u, nV), uRuR = dot3(R->u, R->u), cR = sqrt(R->gam * R->p / R->rho);
+  double hR = R->gam / (R->gam - 1.0) * R->p / R->rho + 0.5 * uRuR + R->k;
+  double md = 0.5 * (L->rho + R->rho), mp = 0.5 * (L->p + R->p), mh = 0.5 * (hL + hR), mv[3];
+  for (int i = 0; i < 3; i++) mv[i] = 0.5 * (L->u[i] + R->u[i]);
+  double ru = md * mv[0], rv = md * mv[1], rw = md * mv[2], pf[5];
+  pf[0] = ru * nV[0];
+  pf[1] = (ru * mv[0] + mp) * nV[0];
+  pf[2] = ru * mv[1] * nV[0];
+  pf[3] = ru * mv[2] * nV[0];
+  pf[4] = ru * mh * nV[0];
+  pf[0] += rv * nV[1];
+  pf[1] += rv * mv[0] * nV[1];
+  pf[2] += (rv * mv[1] + mp) * nV[1];
+  pf[3] += rv * mv[2] * nV[1];
+  pf[4] += rv * mh * nV[1];
+  pf[0] += rw * nV[2];
+  pf[1] += rw * mv[0] * nV[2];
+  pf[2] += rw * mv[1] * nV[2];
+  pf[3] += (rw * mv[2] + mp) * nV[2];
+  pf[4] += rw * mh * nV[2];
+  for (int i = 0; i < 5; i++) F[i] = pf[i] * area;
+  double dU[5], dL[5];
+  dU[0] = L->rho - R->rho;
+  for (int i = 0; i < 3; i++) dU[1 + i] = L->rho * L->u[i] - R->rho * R->u[i];
+  dU[4] = L->rho * hL - R->rho * hR;
+  for (int i = 0; i < 5; i++) dL[i] = JL[3 + i] - JR[3 + i];
+  double lamL = (fabs(unL) + cL) * area, lamR = (fabs(unR) + cR) * area;
+  double mlam = 0.5 * (lamL + lamR);
+  double phiL = pow(JL[1] / (4.0 * mlam), Param_p), phiR = pow(JR[1] / (4.0 * mlam), Param_p);
+  double stretch = 4.0 * phiL * phiR / (phiL + phiR);
+  int nL = (int)JL[2], nR = (int)JR[2];
+  double sc2 = 3.0 * ((double)nL + (double)nR) / ((double)nL * (double)nR);
+  double sc4 = sc2 * sc2 / 4.0;
+  double e2 = Param_Kappa_2 * 0.5 * (JL[0] + JR[0]) * sc2;
+  double e4 = dmax(0.0, Param_Kappa_4 - e2) * sc4;
+  for (int i = 0; i < 5; i++) F[i] += (e2 * dU[i] - e4 * dL[i]) * stretch * mlam;
+}
+
+/* calcJSTCoeff_Var (JoeWithModels.cpp:13435-13492): spectral radii, the pressure sensor and the
+ * undivided Laplacian of the conserved state (rhoE + p for the energy) over the internal faces */
+static void calc_jst_var(jo_case *h) {
+  const jg_mesh *m = &h->m;
+  for (int c = 0; c < h->ncv; c++) {
+    h->p1_lapl[c] = 0.0;
+    h->p2_lapl[c] = 0.0;
+    for (int k = 0; k < 5; k++) h->jst[8 * c + 3 + k] = 0.0;
+    h->jst[8 * c + 1] = 0.0;
+  }
+  for (int f = h->nfa_b; f < h->nfa; f++) {
+    int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
+    double nV[3];
+    double area = norm3(nV, &m->fa_normal[3 * f]);
+    double P0 = h->press[c0], P1 = h->press[c1];
+    double a0 = sqrt(h->gam[c0] * P0 / h->rho[c0]), a1 = sqrt(h->gam[c1] * P1 / h->rho[c1]);
+    double u0[3], u1[3];
+    for (int i = 0; i < 3; i++) {
+      u0[i] = h->rhou[3 * c0 + i] / h->rho[c0];
+      u1[i] = h->rhou[3 * c1 + i] / h->rho[c1];
+    }
+    double l0 = 0.5 * (fabs(dot3(u0, nV)) + a0) * area, l1 = 0.5 * (fabs(dot3(u1, nV)) + a1) * area;
+    h->jst[8 * c0 + 1] += l0;
+    h->jst[8 * c0 + 1] += l1;
+    h->jst[8 * c1 + 1] += l0;
+    h->jst[8 * c1 + 1] += l1;
+    h->p1_lapl[c0] += (P1 - P0);
+    h->p1_lapl[c1] += (P0 - P1);
+    h->p2_lapl[c0] += (P0 + P1);
+    h->p2_lapl[c1] += (P0 + P1);
+    double d[5];
+    d[0] = h->rho[c0] - h->rho[c1];
+    for (int i = 0; i < 3; i++) d[1 + i] = h->rhou[3 * c0 + i] - h->rhou[3 * c1 + i];
+    d[4] = (h->rhoE[c0] + P0) - (h->rhoE[c1] + P1);
+    int b0 = h->bcv[c0], b1 = h->bcv[c1];
+    if ((!b0 && !b1) || (b0 && b1)) {
+      for (int k = 0; k < 5; k++) h->jst[8 * c0 + 3 + k] -= d[k];
+      for (int k = 0; k < 5; k++) h->jst[8 * c1 + 3 + k] += d[k];
+    }
+    if (!b0 && b1)
+      for (int k = 0; k < 5; k++) h->jst[8 * c0 + 3 + k] -= d[k];
+    if (b0 && !b1)
+      for (int k = 0; k < 5; k++) h->jst[8 * c1 + 3 + k] += d[k];
+  }
+  for (int c = 0; c < h->ncv; c++) h->jst[8 * c] = fabs(h->p1_lapl[c]) / h->p2_lapl[c];
+}
+
 /* the face options: fo.shock = JG_SHOCK_FIX_HAENEL selects calcEulerFlux_HAENEL
  * (JoeWithModels.cpp:2970-2979, 3041-3050) */
 static void euler_flux_o(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV,
-                         ausm_opt o) {
-  if (kind == JG_FLUX_ROE) flux_roe(F, L, R, area, nV);
+                         ausm_opt o, const double *JL, const double *JR) {
+  if (kind == JG_FLUX_JST) flux_jst(F, L, R, area, nV, JL, JR);
+  else if (kind == JG_FLUX_ROE) flux_roe(F, L, R, area, nV);
   else if (kind == JG_FLUX_AUSM) flux_ausm(F, L, R, area, nV);
   else if (kind == JG_FLUX_HAENEL) flux_haenel(F, L, R, area, nV);
   else if (kind == JG_FLUX_AUSMDV) {
@@ -1443,9 +1553,10 @@ static ausm_opt bnd_opt(const jg_params *p) {
   return o;
 }
 
+/* boundary faces: JST takes the sensors of the boundary cell on both sides (JoeWithModels.cpp:3169-3178) */
 static void euler_flux(int kind, double F[5], const fstate *L, const fstate *R, double area, const double *nV,
-                       const jg_params *p) {
-  euler_flux_o(kind, F, L, R, area, nV, bnd_opt(p));
+                       const jg_params *p, const double *J) {
+  euler_flux_o(kind, F, L, R, area, nV, bnd_opt(p), J, J);
 }
 
 static void euler_matrices(int kind, double (*AL)[5], double (*AR)[5], const fstate *L, const fstate *R, double area,
@@ -1474,7 +1585,7 @@ void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, cons
     sr.h = sr.gam * sr.p / ((sr.gam - 1.0) * sr.rho);
     /* kind 4: AUSMDV with the entropy fix, no shock fix */
     ausm_opt o = {JG_AUSM_DV, 1, JG_SHOCK_FIX_NONE};
-    euler_flux_o(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f], o);
+    euler_flux_o(kind, &F[5 * f], &sl, &sr, area[f], &nvec[3 * f], o, NULL, NULL);
     if (AL || AR)
       euler_matrices_o(kind, AL ? (double(*)[5]) & AL[25 * f] : NULL, AR ? (double(*)[5]) & AR[25 * f] : NULL, &sl,
                        &sr, area[f], &nvec[3 * f], o);
@@ -1534,6 +1645,8 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
   const jg_mesh *m = &h->m;
   const jg_params *p = &h->p;
   int kind = p->flux;
+  /* JST: its coefficients of the current state first (JoeWithModels.cpp:2663-2664) */
+  if (kind == JG_FLUX_JST) calc_jst_var(h);
   if (p->second_order) {
     grad_vector(h, h->grad_u, h->vel, h->vel_bfa, p->limiter, h->sos);
     for (int c = 0; c < h->ncv; c++) h->alpha_rho[c] = 1.0;
@@ -1565,7 +1678,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
      * SHOCKFIX_ACROSS_SHOCK defined (JoeWithModels.cpp:4) also on the sonic faces themselves */
     ausm_opt o = bnd_opt(p);
     if (flag && (flag[c0] + flag[c1]) > flag_sum) o.shock = p->shock_fix;
-    euler_flux_o(kind, F, &L, &R, area, nV, o);
+    euler_flux_o(kind, F, &L, &R, area, nV, o, &h->jst[8 * c0], &h->jst[8 * c1]);
     rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
     rr[c1] += F[0]; for (int i = 0; i < 3; i++) ru[3 * c1 + i] += F[1 + i]; rE[c1] += F[4];
     for (int i = 0; i < 5; i++) { h->fscale[5 * c0 + i] += fabs(F[i]); h->fscale[5 * c1 + i] += fabs(F[i]); }
@@ -1588,7 +1701,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
       int n00 = m->nbocv_i[c0];
       if (zn->kind == JG_BC_SYMMETRY) {
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &B, &B, area, nV, p);
+        euler_flux(kind, F, &B, &B, area, nV, p, &h->jst[8 * c0]);
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (p->symm_bc == JG_SYMM_ANALYTICAL) {
           for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= h->p_bfa[f] * nV[i] * area;
@@ -1621,7 +1734,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
         }
       } else if (zn->kind == JG_BC_WALL) {
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &B, &B, area, nV, p);
+        euler_flux(kind, F, &B, &B, area, nV, p, &h->jst[8 * c0]);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {
@@ -1632,7 +1745,7 @@ static void calc_euler_flux(jo_case *h, double *rr, double *ru, double *rE, doub
         fstate L = cell_state(h, c0);
         if (p->second_order) reconstruct(h, c0, f, &L);
         fstate B = bfa_state(h, f);
-        euler_flux(kind, F, &L, &B, area, nV, p);
+        euler_flux(kind, F, &L, &B, area, nV, p, &h->jst[8 * c0]);
         rr[c0] -= F[0]; for (int i = 0; i < 3; i++) ru[3 * c0 + i] -= F[1 + i]; rE[c0] -= F[4];
         for (int i = 0; i < 5; i++) h->fscale[5 * c0 + i] += fabs(F[i]);
         if (implicit) {

@@ -146,8 +146,24 @@ public:
     sprintf(nm, "%s_rhoE.f64", tag); dumpRaw(nm, this->rhoE, sizeof(double) * this->ncv);
   }
 
+  // the JST arrays runBackwardEuler allocates before its loop (JoeWithModels.cpp:932-937),
+  // so that calcRhs can run outside it
+  void prepareJST() {
+    if (this->getStringParam("SPACE_INTEGRATION", "HLLC") != "JST") return;
+    int n = this->ncv_g;
+    this->PressSensor = new double[n];
+    this->Conserv_Und_Lapl = new double[n][5];
+    this->Lambda = new double[n];
+    this->BoundaryCV = new bool[n];
+    this->NeighborCV = new int[n];
+    this->p1_Und_Lapl = new double[n];
+    this->p2_Und_Lapl = new double[n];
+    this->calcJSTCoeff_Const(0);
+  }
+
   void dumpAll() {
     int ncv = this->ncv, nfa = this->nfa, nfa_b = this->nfa_b, nbocv_s = this->nbocv_s;
+    prepareJST();
     writeMeta();
     DUMPI("cvofa", this->cvofa, 2 * nfa);
     DUMPI("faocv_i", this->faocv_i, ncv + 1);

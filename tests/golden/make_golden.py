@@ -78,6 +78,10 @@ def cases():
     yield "bump_ausmv_m105", rawt5, dataclasses.replace(prmt5, SPACE_INTEGRATION="AUSMV", SHOCK_FIX_TYPE="NONE")
     yield "bump_ausmd_first_order", raw, dataclasses.replace(prm, SPACE_INTEGRATION="AUSMD", SECOND_ORDER=False,
                                                              ENTROPY_FIX="NONE", SHOCK_FIX_TYPE="NONE")
+    # JST: first and second order, and the laminar plate
+    yield "bump_jst_first_order", raw, dataclasses.replace(prm, SPACE_INTEGRATION="JST", SECOND_ORDER=False)
+    yield "bump_jst", raw, dataclasses.replace(prm, SPACE_INTEGRATION="JST")
+    yield "plate_jst", rawp, dataclasses.replace(prmp, SPACE_INTEGRATION="JST")
     yield "bump_haenel", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
     yield "bump_haenel_laminar_isothermal", raw, dataclasses.replace(visc, SPACE_INTEGRATION="HAENEL", bcs=bc_iso)
     yield "bump_haenel_first_order_symm_new", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL",

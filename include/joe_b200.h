@@ -282,21 +282,16 @@ int jg_batch_status(jg_case_t *h, int *status);
 /* freeze (0) or resume (1) a case: a frozen case keeps its state (retired) */
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
-/* Launch shapes (no reference counterpart): the 5x5 face loop's shape,
- * flux_cl = 1, 2 or 4 lanes per cell (default 1: each cell evaluates its own
- * faces, every internal face twice) or 0, face-centric (one thread per internal
- * face evaluates it once and writes its flux and off-diagonal blocks; a cell
- * pass sums them and its boundary faces into the residual and the diagonal
- * block), and the kernel of the 5x5 Jacobi sweep (0: a block per 32-cell
- * slice, a thread per block row, the default; 1: a thread per cell).
- * jg_autotune times each candidate on the handle's own mesh (trials launches,
- * CUDA events) and keeps the fastest; ms[6] (may be NULL) gets the face loop
- * time per launch for 1, 2, 4 lanes (ms[0..2]), the sweep time for kernels 0, 1
- * (ms[3..4]) and the face-centric loop's time (ms[5]).  The sweep kernels give
- * bit-identical results; the face loop shapes change the order of each cell's
- * diagonal-block and residual sums (rounding-level differences).  Handles
- * without a turbulence model; others keep their single shape.  A batch handle
- * tunes for all its cases. */
+/* Launch shapes (no reference counterpart): the lanes per cell of the 5x5
+ * face loop (1, 2 or 4; default 1) and the kernel of the 5x5 Jacobi sweep (0:
+ * a block per 32-cell slice, a thread per block row, the default; 1: a thread
+ * per cell).  jg_autotune times each candidate on the handle's own mesh
+ * (trials launches, CUDA events) and keeps the fastest; ms[5] (may be NULL)
+ * gets the face loop time per launch for 1, 2, 4 lanes and the sweep time for
+ * kernels 0, 1.  The sweep kernels give bit-identical results; the lanes per
+ * cell change the order of each cell's diagonal-block and residual sums
+ * (rounding-level differences).  Handles without a turbulence model; others
+ * keep their single shape.  A batch handle tunes for all its cases. */
 int jg_set_launch_config(jg_case_t *h, int flux_cl, int relax_variant);
 int jg_get_launch_config(jg_case_t *h, int *flux_cl, int *relax_variant);
 int jg_autotune(jg_case_t *h, int trials, int *flux_cl, int *relax_variant, float *ms);

@@ -66,7 +66,6 @@ struct jg_case {
   int graph_sweeps = -1;
   int primed = 0;           // state + BC computed since the last set_state
   int ncolors = 1;
-  bool face_centric_ok = false;  // every internal face is listed by both its cells (faocv)
   int ncases = 1;           // independent cases concatenated in this handle (jg_batch_create)
   std::vector<int> case_off;        // [ncases+1] first cell of each case
   std::vector<int> case_nfa_b_off;  // [ncases+1] first boundary face of each case
@@ -444,16 +443,6 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(upload(h, &m.cvofa, mesh->cvofa, 2 * (size_t)nfa));
   RC(upload(h, &m.slot_i, fi, (size_t)N + 1));
   RC(upload(h, &m.slots, slots.data(), slots.size()));
-  {
-    // the face-centric face loop's ELL columns: internal face f in the row of each of its cells
-    std::vector<int> fcol(2 * (size_t)std::max(nfa - nfa_b, 1), -1);
-    for (const Slot& sl : slots)
-      if (sl.nb >= 0) fcol[2 * (size_t)(sl.f - nfa_b) + sl.side] = sl.col;
-    h->face_centric_ok = true;
-    for (int f = nfa_b; f < nfa; f++)
-      if (fcol[2 * (size_t)(f - nfa_b)] < 0 || fcol[2 * (size_t)(f - nfa_b) + 1] < 0) h->face_centric_ok = false;
-    RC(upload(h, &m.fcol, fcol.data(), fcol.size()));
-  }
   RC(upload(h, &m.nb_i, mesh->nbocv_i, (size_t)N + 1));
   RC(upload(h, &m.nb_v, mesh->nbocv_v, (size_t)mesh->nbocv_s));
   RC(upload(h, &m.lsq, mesh->nbocv_lsg_coeff, 3 * (size_t)mesh->nbocv_s));
@@ -487,7 +476,6 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   st.shock_flag = nullptr;
   if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE)
     RC(dmalloc(h, &st.shock_flag, (size_t)N));
-  RC(dmalloc(h, &st.ff, 5 * (size_t)std::max(nfa - nfa_b, 1)));
   st.jst = nullptr;
   st.jst_bcv = nullptr;
   if (q->flux == JG_FLUX_JST) {
@@ -713,11 +701,6 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
   size_t b = 0;
   for (size_t x : a)
     if (x) b += alloc_round(x);
-  // the face-centric loop's columns and face fluxes; AUSMDV shock flags; JST coefficients
-  const size_t nint = std::max<size_t>(nfa - nfa_b, 1);
-  b += alloc_round(2 * nint * i) + alloc_round(5 * nint * d);
-  if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE) b += alloc_round(N);
-  if (q->flux == JG_FLUX_JST) b += alloc_round(8 * N * d) + alloc_round(N);
   if (bs > 5) {
     // model arrays: phi, phi_bfa, grad_phi, diff (per scalar), wall distance, strain, vorticity
     // (+ divergence, cross-diffusion, F1, F2 for SST), mut_fa, the wall faces
@@ -1757,10 +1740,7 @@ static void drop_graph(jg_case* h) {
 
 extern "C" int jg_set_launch_config(jg_case_t* h, int flux_cl, int relax_variant) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
-  if (flux_cl != 0 && flux_cl != 1 && flux_cl != 2 && flux_cl != 4)
-    return set_err(JG_ERR_ARG, "face loop shape must be 0 (face-centric) or 1, 2, 4 lanes per cell");
-  if (flux_cl == 0 && !h->face_centric_ok)
-    return set_err(JG_ERR_ARG, "the face-centric face loop needs every internal face in both cells' faocv");
+  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4) return set_err(JG_ERR_ARG, "lanes per cell must be 1, 2 or 4");
   if (relax_variant != 0 && relax_variant != 1) return set_err(JG_ERR_ARG, "sweep kernel must be 0 or 1");
   CK(cudaStreamSynchronize(h->stream));
   h->p.flux_cl = flux_cl;
@@ -1791,16 +1771,10 @@ extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_va
     launch_dt(h->m, h->p, h->st, 1, 0.0, S);
     launch_grad(h->m, h->p, h->st, S);
     Params p = h->p;
-    // ms[0..2]: 1, 2, 4 lanes per cell; ms[5]: face-centric (flux_cl 0)
-    const int cls[4] = {1, 2, 4, 0};
-    const int slot[4] = {0, 1, 2, 5};
+    const int cls[3] = {1, 2, 4};
     float best = 1e30f;
     int best_cl = h->p.flux_cl, best_v = h->p.relax_variant;
-    for (int i = 0; i < 4; i++) {
-      if (cls[i] == 0 && !h->face_centric_ok) {
-        if (ms) ms[5] = -1.0f;
-        continue;
-      }
+    for (int i = 0; i < 3; i++) {
       p.flux_cl = cls[i];
       launch_flux(h->m, p, h->st, 1, 1, S);  // warm-up
       CK(cudaEventRecord(e0, S));
@@ -1809,7 +1783,7 @@ extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_va
       CK(cudaEventSynchronize(e1));
       float t_ms = 0.0f;
       CK(cudaEventElapsedTime(&t_ms, e0, e1));
-      if (ms) ms[slot[i]] = t_ms / trials;
+      if (ms) ms[i] = t_ms / trials;
       if (t_ms < best) { best = t_ms; best_cl = cls[i]; }
     }
     p.flux_cl = best_cl;

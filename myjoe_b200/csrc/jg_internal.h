@@ -33,7 +33,6 @@ struct Slot {
 
 struct Mesh {
   int ncv, nfa, nfa_b, nzones;
-  const int* fcol;  // [nfa - nfa_b][2] ELL column of internal face f in the row of cvofa[f][0], [1]
   int nslices;
   const double* x_cv;      // [N][3]
   const double* vol;       // [N]
@@ -75,7 +74,6 @@ struct State {
   double* local_dt; // [N]
   double* rhs;      // [N][5] RHS of calcRhs (rho, rhou, rhoE)
   unsigned char* shock_flag;  // [N] AUSMDV shock fix: the cell touches a sonic internal face
-  double* ff;                 // [nfa - nfa_b][5] face-centric face loop: each internal face's residual flux
   double* jst;                // [N][8] JST: pressure sensor, spectral radius, internal faces, undivided Laplacian[5]
   const unsigned char* jst_bcv;  // [N] JST's BoundaryCV: the cell is the first cell of an internal face
   double* b;        // [N][5] under-relaxed rhs of the linear system

@@ -636,6 +636,15 @@ __device__ inline void block_inverse(double* A, double* Ai) {
   }
 }
 
+// CL lanes per cell (a launch shape chosen per handle, jg_autotune): lane l
+// of a cell evaluates the cell's face slots l, l+CL, ...; each lane
+// accumulates its own partial diagonal block (shared memory) and residual,
+// summed over the lanes in a fixed order.  More lanes shorten each thread's
+// dependent chain and give the scheduler more warps to spread over the SMs
+// (a small mesh is otherwise a one-and-a-bit-wave grid at the
+// register-limited occupancy); they cost repeated reads of the cell's data.
+// Measured: the viscous Roe plate (49k cells) is 2% faster with two lanes,
+// inviscid HLLC bumps (430k cells) 1.4x faster with one.
 // AUSMDV shock sensor (JoeWithModels.cpp:2753-2781): is internal face f sonic between its
 // cells' centre states, a compression through u_n - c or u_n + c
 __device__ __forceinline__ bool face_sonic(const Mesh& m, const Params& p, const State& st, int f) {
@@ -727,94 +736,6 @@ __device__ __forceinline__ int bnd_opts(const Params& p) {
   return KIND == 4 ? (p.ausm_type | (p.entropy_fix ? FO_EFIX : 0)) : 0;
 }
 
-// one boundary face of cell c (the cell is cvofa[f][0]): the Euler and viscous boundary fluxes
-// into rhs and, when implicit, their diagonal-block part into Ds (JoeWithModels.cpp:3112-3569, 3764-3784)
-template <typename BT, int KIND, int VISC>
-__device__ __forceinline__ void boundary_face(const Mesh& m, const Params& p, const State& st, int c, int f,
-                                              const double nV[3], double area, int implicit, double rhs[5],
-                                              StridedBlock<BT> Ds) {
-  using JT = BT;
-  // ---------------- boundary face (the cell is cvofa[f][0]) ----------------
-  const DevZone z = m.zones[m.bzone[f]];
-  const double* bb = &st.bfa[8 * f];
-  FState B;
-  B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
-  const FStateT<JT> Bt = fstate_as<JT>(B);
-  const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
-  double F[5];
-  const int fob = bnd_opts<KIND>(p);
-  const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
-  if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-    euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
-    if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
-      for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
-    } else {
-      for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-    }
-    if (implicit) {
-      if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
-        // analytical pressure Jacobian, JoeWithModels.cpp:3231-3251
-        double a2 = p.gamma - 1.0;
-        double phi = 0.5 * a2 * (B.u[0] * B.u[0] + B.u[1] * B.u[1] + B.u[2] * B.u[2]);
-        for (int i = 0; i < 3; i++) {
-          Ds[5 * (i + 1) + 0] += (JT)(phi * nV[i] * area);
-          for (int j = 0; j < 3; j++) Ds[5 * (i + 1) + 1 + j] += (JT)(-a2 * B.u[j] * nV[i] * area);
-          Ds[5 * (i + 1) + 4] += (JT)(a2 * nV[i] * area);
-        }
-      } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
-        JT Apl[25], Ami[25];
-        euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt, fob);
-        for (int e = 0; e < 25; e++) Ds[e] += Apl[e] + Ami[e];
-      } else {
-        JT Apl[25];
-        euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt, fob);
-        for (int e = 0; e < 25; e++) Ds[e] += Apl[e];
-      }
-    }
-  } else {
-    FState L = recon(m, p, st, c, f);
-    euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
-    for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-    if (implicit) {
-      FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
-      JT Apl[25];
-      euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt, fob);
-      for (int e = 0; e < 25; e++) Ds[e] += Apl[e];
-    }
-  }
-  if (VISC && z.kind != JG_BC_SYMMETRY) {
-    VSide v0 = cell_vside(p, st, c);
-    VSide v1;
-    v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
-    v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
-    v1.gu = v0.gu; v1.gh = v0.gh;
-    double sV[3], smag;
-    for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
-    if (z.kind == JG_BC_WALL) {
-      smag = fabs(dot3(sV, nV));  // projected on the wall normal; nVec is used as sVec
-      for (int i = 0; i < 3; i++) sV[i] = nV[i];
-    } else {
-      smag = sqrt(dot3(sV, sV));
-      for (int i = 0; i < 3; i++) sV[i] /= smag;
-    }
-    double Fu[3], FE;
-    VFace vf;
-    visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
-    for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
-    rhs[4] -= FE;
-    if (implicit) visc_jac_add<JT>(Ds, JT(-1.0), 0, vf, v0, v1.u);
-  }
-}
-
-// CL lanes per cell (a launch shape chosen per handle, jg_autotune): lane l
-// of a cell evaluates the cell's face slots l, l+CL, ...; each lane
-// accumulates its own partial diagonal block (shared memory) and residual,
-// summed over the lanes in a fixed order.  More lanes shorten each thread's
-// dependent chain and give the scheduler more warps to spread over the SMs
-// (a small mesh is otherwise a one-and-a-bit-wave grid at the
-// register-limited occupancy); they cost repeated reads of the cell's data.
-// Measured: the viscous Roe plate (49k cells) is 2% faster with two lanes,
-// inviscid HLLC bumps (430k cells) 1.4x faster with one.
 template <typename BT, int KIND, int VISC, int CL>
 __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
@@ -889,7 +810,76 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         if (implicit)
           for (int e = 0; e < 25; e++) O[ell_index<BT>(m, c, s.col, e)] = (BT)Ob[e];
       } else {
-        boundary_face<BT, KIND, VISC>(m, p, st, c, f, nV, area, implicit, rhs, StridedBlock<JT>{sD + t, bd});
+        // ---------------- boundary face (the cell is cvofa[f][0]) ----------------
+        const DevZone z = m.zones[m.bzone[f]];
+        const double* bb = &st.bfa[8 * f];
+        FState B;
+        B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
+        const FStateT<JT> Bt = fstate_as<JT>(B);
+        const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
+        double F[5];
+        const int fob = bnd_opts<KIND>(p);
+        const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
+        if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
+          euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
+          if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
+            for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
+          } else {
+            for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+          }
+          if (implicit) {
+            if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
+              // analytical pressure Jacobian, JoeWithModels.cpp:3231-3251
+              double a2 = p.gamma - 1.0;
+              double phi = 0.5 * a2 * (B.u[0] * B.u[0] + B.u[1] * B.u[1] + B.u[2] * B.u[2]);
+              for (int i = 0; i < 3; i++) {
+                sD[(5 * (i + 1) + 0) * bd + t] += (JT)(phi * nV[i] * area);
+                for (int j = 0; j < 3; j++) sD[(5 * (i + 1) + 1 + j) * bd + t] += (JT)(-a2 * B.u[j] * nV[i] * area);
+                sD[(5 * (i + 1) + 4) * bd + t] += (JT)(a2 * nV[i] * area);
+              }
+            } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
+              JT Apl[25], Ami[25];
+              euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt, fob);
+              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
+            } else {
+              JT Apl[25];
+              euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt, fob);
+              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
+            }
+          }
+        } else {
+          FState L = recon(m, p, st, c, f);
+          euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
+          for (int i = 0; i < 5; i++) rhs[i] -= F[i];
+          if (implicit) {
+            FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
+            JT Apl[25];
+            euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt, fob);
+            for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
+          }
+        }
+        if (VISC && z.kind != JG_BC_SYMMETRY) {
+          VSide v0 = cell_vside(p, st, c);
+          VSide v1;
+          v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
+          v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
+          v1.gu = v0.gu; v1.gh = v0.gh;
+          double sV[3], smag;
+          for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+          if (z.kind == JG_BC_WALL) {
+            smag = fabs(dot3(sV, nV));  // projected on the wall normal; nVec is used as sVec
+            for (int i = 0; i < 3; i++) sV[i] = nV[i];
+          } else {
+            smag = sqrt(dot3(sV, sV));
+            for (int i = 0; i < 3; i++) sV[i] /= smag;
+          }
+          double Fu[3], FE;
+          VFace vf;
+          visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
+          for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
+          rhs[4] -= FE;
+          if (implicit) visc_jac_add<JT>(StridedBlock<JT>{sD + t, bd}, JT(-1.0), 0, vf, v0, v1.u);
+        }
       }
     }
   }
@@ -926,116 +916,6 @@ __global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int im
         BT* Dig = (BT*)st.Dinv;
         for (int e = 0; e < 25; e++) Dig[(size_t)e * m.ncv + c] = (BT)Di[e];
       }
-    }
-  }
-}
-
-// Face-centric implicit face loop (launch shape flux_cl = 0), two kernels.  The cell-centric
-// kernel above evaluates every internal face twice, once for each of its cells; here k_face
-// evaluates each internal face once (one thread per face): its residual flux (Euler on the
-// reconstructed states + viscous) goes to ff[face], its blocks straight into the two
-// off-diagonal slots, O(c0,c1) = Ami - A1 and O(c1,c0) = -Apl + A0.  k_cell_sum then forms
-// each cell's residual from ff, its boundary faces, and its diagonal block
-//   D(c) = boundary part - sum over internal faces of O(neighbour, c),
-// which is the cell-centric D term by term (the face flux Jacobians are conservative: what
-// a face adds to one row's diagonal it subtracts from the other row's off-diagonal).
-template <typename BT, int KIND, int VISC>
-__global__ void __launch_bounds__(128) k_face(Mesh m, Params p, State st, int implicit) {
-  using JT = BT;
-  const int fi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (fi >= m.nfa - m.nfa_b) return;
-  const int f = m.nfa_b + fi;
-  const int c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
-  double nV[3], area;
-  unit_normal(m, f, nV, area);
-  const int fo = face_opts<KIND>(p, st, c0, c1);
-  double F[5];
-  {
-    FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
-    euler_flux_t<KIND>(F, L, R, area, nV, fo, KIND == 5 ? &st.jst[8 * c0] : nullptr,
-                       KIND == 5 ? &st.jst[8 * c1] : nullptr);
-  }
-  JT O0[25], O1[25];  // O(c0,c1), O(c1,c0)
-  if (implicit) {
-    const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
-    FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c0)), R0 = fstate_as<JT>(cell_fstate(p, st, c1));
-    JT Apl[25], Ami[25];
-    euler_matrices_t<KIND, JT>(Apl, Ami, L0, R0, (JT)area, nVt, fo);
-    for (int e = 0; e < 25; e++) {
-      O0[e] = Ami[e];
-      O1[e] = -Apl[e];
-    }
-  }
-  if (VISC) {
-    VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-    double sV[3];
-    for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-    double smag = sqrt(dot3(sV, sV));
-    for (int i = 0; i < 3; i++) sV[i] /= smag;
-    double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
-    double Fu[3], FE;
-    VFace vf;
-    visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, ufa, area, nV, smag, sV);
-    for (int i = 0; i < 3; i++) F[1 + i] += Fu[i];
-    F[4] += FE;
-    if (implicit) {
-      visc_jac_add<JT>(O0, JT(-1.0), 1, vf, v1, ufa);
-      visc_jac_add<JT>(O1, JT(1.0), 0, vf, v0, ufa);
-    }
-  }
-  for (int i = 0; i < 5; i++) st.ff[5 * (size_t)fi + i] = F[i];
-  if (implicit) {
-    BT* O = (BT*)st.O;
-    const int col0 = m.fcol[2 * fi], col1 = m.fcol[2 * fi + 1];
-    for (int e = 0; e < 25; e++) O[ell_index<BT>(m, c0, col0, e)] = (BT)O0[e];
-    for (int e = 0; e < 25; e++) O[ell_index<BT>(m, c1, col1, e)] = (BT)O1[e];
-  }
-}
-
-template <typename BT, int KIND, int VISC>
-__global__ void __launch_bounds__(128) k_cell_sum(Mesh m, Params p, State st, int implicit, int for_step) {
-  using JT = BT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  JT* sD = reinterpret_cast<JT*>(smem_raw);  // [25][blockDim.x]
-  const int t = threadIdx.x, bd = blockDim.x;
-  const int c = blockIdx.x * bd + t;
-  if (c >= m.ncv) return;
-  double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int e = 0; e < 25; e++) sD[e * bd + t] = JT(0);
-  const BT* O = (const BT*)st.O;
-  for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
-    const Slot s = m.slots[k];
-    const int f = s.f;
-    if (s.nb >= 0) {
-      const int fi = f - m.nfa_b;
-      const double sg = s.side == 0 ? -1.0 : 1.0;
-      for (int i = 0; i < 5; i++) rhs[i] += sg * st.ff[5 * (size_t)fi + i];
-      if (implicit) {
-        const int ocol = m.fcol[2 * fi + (s.side == 0 ? 1 : 0)];  // c's column in the neighbour's row
-        for (int e = 0; e < 25; e++) sD[e * bd + t] -= (JT)O[ell_index<BT>(m, s.nb, ocol, e)];
-      }
-    } else {
-      double nV[3], area;
-      unit_normal(m, f, nV, area);
-      boundary_face<BT, KIND, VISC>(m, p, st, c, f, nV, area, implicit, rhs, StridedBlock<JT>{sD + t, bd});
-    }
-  }
-  for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
-  if (implicit) {
-    double Dm[25];
-    for (int e = 0; e < 25; e++) Dm[e] = (double)sD[e * bd + t];
-    if (for_step) {
-      double tmp = m.vol[c] / st.local_dt[c];
-      for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;
-      for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
-    }
-    BT* Dg = (BT*)st.D;
-    for (int e = 0; e < 25; e++) Dg[(size_t)e * m.ncv + c] = (BT)Dm[e];
-    if (for_step) {
-      double Di[25];
-      block_inverse(Dm, Di);
-      BT* Dig = (BT*)st.Dinv;
-      for (int e = 0; e < 25; e++) Dig[(size_t)e * m.ncv + c] = (BT)Di[e];
     }
   }
 }
@@ -1614,18 +1494,9 @@ static void launch_flux_cell_cl(const Mesh& m, const Params& p, State& st, int f
   else k_flux<BT, KIND, 0, CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
 }
 // lanes per cell of the implicit face loop: p.flux_cl (1, 2 or 4)
-template <typename BT, int KIND, int VISC>
-static void launch_face_centric(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  const int nint = m.nfa - m.nfa_b;
-  if (nint > 0) k_face<BT, KIND, VISC><<<grid_for(nint, TB), TB, 0, s>>>(m, p, st, 1);
-  k_cell_sum<BT, KIND, VISC><<<grid_for(m.ncv, TB), TB, 25 * TB * sizeof(BT), s>>>(m, p, st, 1, for_step);
-}
 template <typename BT, int KIND>
 static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  if (p.flux_cl == 0) {
-    if (p.viscous) launch_face_centric<BT, KIND, 1>(m, p, st, for_step, s);
-    else launch_face_centric<BT, KIND, 0>(m, p, st, for_step, s);
-  } else if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1>(m, p, st, for_step, s);
+  if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1>(m, p, st, for_step, s);
   else if (p.flux_cl == 4) launch_flux_cell_cl<BT, KIND, 4>(m, p, st, for_step, s);
   else launch_flux_cell_cl<BT, KIND, 2>(m, p, st, for_step, s);
 }

@@ -267,12 +267,11 @@ class JoeGpu:
 
     def autotune(self, trials=5):
         """time the launch shapes on this handle and keep the fastest: returns
-        (face loop shape: 0 face-centric or lanes per cell, sweep kernel, {shape: ms per launch})"""
+        (lanes per cell of the face loop, sweep kernel, {shape: ms per launch})"""
         cl, rv = C.c_int(0), C.c_int(0)
-        ms = (C.c_float * 6)()
+        ms = (C.c_float * 5)()
         _ck(lib().jg_autotune(self.h, int(trials), C.byref(cl), C.byref(rv), ms))
-        times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4],
-                 "flux_cl0": ms[5]}
+        times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4]}
         return cl.value, rv.value, times
 
     def set_launch_config(self, flux_cl, relax_variant):

@@ -2,9 +2,8 @@
 
 The two Jacobi sweep kernels do the same arithmetic in the same order, so a
 step gives bit-identical results with either; the lanes per cell of the face
-loop (1, 2, 4 lanes per cell, or face-centric) change only the order of each
-cell's diagonal-block and residual sums, so steps agree to rounding (1e-12
-relative after 10 steps).  The autotuner
+loop change only the order of each cell's diagonal-block and residual sums,
+so steps agree to rounding (1e-12 relative after 10 steps).  The autotuner
 returns a valid shape and per-shape times, and a batch and its cases alone
 stay bit-identical under a shared shape."""
 import dataclasses
@@ -43,7 +42,7 @@ def test_sweep_kernels_are_bitwise_equal():
         np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("cl", [1, 4, 0])
+@pytest.mark.parametrize("cl", [1, 4])
 def test_lanes_per_cell_agree_to_rounding(cl):
     g, prm = _plate("SGS")
     a = _run(g, prm, (2, 0))
@@ -53,34 +52,14 @@ def test_lanes_per_cell_agree_to_rounding(cl):
     np.testing.assert_allclose(b[1], a[1], rtol=1e-10)
 
 
-@pytest.mark.parametrize("flux", ["HLLC", "AUSMDV", "JST", "HAENEL"])
-@pytest.mark.parametrize("precision", [0, 1])
-def test_face_centric_matches_cell_centric(flux, precision):
-    """The face-centric loop against one lane per cell on a sonic inflow (the
-    AUSMDV shock fix active), inviscid, both precisions."""
-    _, g, prm = case.bump_case(24, 12, 2, jitter=0.1, seed=3, mach=1.0)
-    prm = dataclasses.replace(prm, SPACE_INTEGRATION=flux, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=2.0)
-    out = []
-    for shape in ((1, 0), (0, 0)):
-        j = solver.JoeGpu(g, prm, precision=precision)
-        j.set_launch_config(*shape)
-        j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
-        r = j.runBackwardEuler(6)
-        out.append((j.get_state(), r))
-        j.close()
-    tol = 1e-12 if precision == 0 else 1e-6   # mixed: FP32 blocks summed in another order
-    for x, y in zip(out[1][0], out[0][0]):
-        assert np.abs(x - y).max() <= tol * np.abs(y).max()
-
-
 def test_autotune_picks_a_valid_shape_and_keeps_results():
     g, prm = _plate("SGS")
     j = solver.JoeGpu(g, prm)
     j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
     cl, rv, ms = j.autotune(3)
-    assert cl in (0, 1, 2, 4) and rv in (0, 1)
+    assert cl in (1, 2, 4) and rv in (0, 1)
     assert all(v > 0.0 for v in ms.values())
-    assert ms["flux_cl%d" % cl] == min(ms["flux_cl1"], ms["flux_cl2"], ms["flux_cl4"], ms["flux_cl0"])
+    assert ms["flux_cl%d" % cl] == min(ms["flux_cl1"], ms["flux_cl2"], ms["flux_cl4"])
     r = j.runBackwardEuler(10)   # the tuned shape is captured at the next step
     assert np.all(np.isfinite(r))
     ref = _run(g, prm, (cl, rv))
@@ -89,19 +68,18 @@ def test_autotune_picks_a_valid_shape_and_keeps_results():
     j.close()
 
 
-@pytest.mark.parametrize("shape", [(4, 1), (0, 0)])
-def test_batch_bitwise_under_a_shared_shape(shape):
+def test_batch_bitwise_under_a_shared_shape():
     cs = []
     for k, (nx, ny) in enumerate([(24, 12), (40, 16)]):
         _, g, prm = case.bump_case(nx, ny, 2, jitter=0.1, seed=k)
         cs.append((g, dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=2.0)))
     b = solver.JoeGpuBatch(cs)
-    b.set_launch_config(*shape)
+    b.set_launch_config(4, 1)
     for k, (g, prm) in enumerate(cs):
         b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
     b.runBackwardEulerCases(8)
     for k, (g, prm) in enumerate(cs):
-        st, _, _ = _run(g, prm, shape, nsteps=8)
+        st, _, _ = _run(g, prm, (4, 1), nsteps=8)
         for x, y in zip(b.get_case_state(k), st):
             np.testing.assert_array_equal(x, y)
     b.close()

@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--face-loop", default="auto", choices=["auto", "1", "2", "4"],
+                    help="face loop lanes per cell: autotuned, or 1, 2, 4")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -203,6 +205,9 @@ def main():
     j.set_state(*st0)
     # launch shapes picked on this mesh before any timing (jg_autotune; a set-up step of the API)
     tuned_cl, tuned_sweep, _ = j.autotune(5)
+    if args.face_loop != "auto":
+        tuned_cl = int(args.face_loop)
+        j.set_launch_config(tuned_cl, tuned_sweep)
     j.set_state(*st0)
     j.set_profiling(True)
     kernels_per_step = j.step_kernel_count()

@@ -701,6 +701,9 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
   size_t b = 0;
   for (size_t x : a)
     if (x) b += alloc_round(x);
+  // AUSMDV shock flags; JST coefficients and BoundaryCV
+  if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE) b += alloc_round(N);
+  if (q->flux == JG_FLUX_JST) b += alloc_round(8 * N * d) + alloc_round(N);
   if (bs > 5) {
     // model arrays: phi, phi_bfa, grad_phi, diff (per scalar), wall distance, strain, vorticity
     // (+ divergence, cross-diffusion, F1, F2 for SST), mut_fa, the wall faces
@@ -1408,12 +1411,8 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
       h->graph = nullptr;
     }
   }
-  // history base: residual k of this call goes to resid[k]
-  double ctrl[16];
-  CK(cudaMemcpyAsync(ctrl, h->st.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  ctrl[4] = ctrl[1];
-  CK(cudaMemcpyAsync(h->st.ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, h->stream));
+  // history base: residual k of this call goes to resid[k] (set on the device, no round trip)
+  launch_hist_base(h->st, h->stream);
   bool use_graph = h->hp.lin_solver != JG_LS_BCGSTAB && h->hp.lin_solver != JG_LS_BCGSTAB_LINELET;
   if (use_graph) RC(ensure_graph(h));
   for (int k = 0; k < nsteps; k++) {

@@ -147,6 +147,7 @@ struct Params {
 
 // launchers (jg_kernels.cu); all enqueue on stream s
 void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_hist_base(State& st, cudaStream_t s);
 void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s);

@@ -1449,6 +1449,9 @@ void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   k_bc<<<grid_for(m.nfa_b, TB), TB, 0, s>>>(m, p, st);
 }
 void launch_ctrl_step(const Params& p, State& st, cudaStream_t s) { k_ctrl_step<<<1, 1, 0, s>>>(p, st); }
+// the residual history of the steps that follow starts at entry 0: ctrl[4] = the step count now
+__global__ void k_hist_base(State st) { st.ctrl[4] = st.ctrl[1]; }
+void launch_hist_base(State& st, cudaStream_t s) { k_hist_base<<<1, 1, 0, s>>>(st); }
 void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl, double cfl, cudaStream_t s) {
   int nb = grid_for(m.ncv, 256);
   k_dt<<<nb, 256, 0, s>>>(m, p, st, use_ctrl, cfl);

@@ -1420,11 +1420,14 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
     else RC(enqueue_step(h, 0));
   }
   CKL();
+  // a single case's residual history rides on the error-flag read's synchronisation
+  const bool direct = resid && nsteps > 0 && h->ncases == 1;
+  if (direct)
+    CK(cudaMemcpyAsync(resid, h->st.resid, h->bs * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
   RC(check_err_flags(h));
-  if (resid && nsteps > 0) {
-    if (h->ncases == 1) {
-      CK(cudaMemcpy(resid, h->st.resid, h->bs * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
-    } else {
+  if (resid && nsteps > 0 && !direct) {
+    {
       // the sum over the cases of the batch, per step
       const int bs = h->bs;
       std::vector<double> all(bs * (size_t)nsteps * h->ncases);

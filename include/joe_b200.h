@@ -454,10 +454,13 @@ int jg_restart_save_state(jg_restart_t *r, jg_case_t *h);
 int jg_restart_load_state(jg_case_t *h, const jg_restart_t *r);
 
 /* Per-face Euler fluxes and implicit matrices, batched over n faces on the
- * GPU: calcEulerFlux_{HLLC,Roe,AUSM} and calcEulerFluxMatrices_{HLLC,Roe}
- * (src/joe/UgpWithCvCompFlow.cpp:120-709, 3281-3641).  L/R[n][6] =
- * (rho, u, v, w, p, gamma), area[n], nvec[n][3] unit normals; F[n][5];
- * AL/AR[n][5][5] may be NULL. */
+ * GPU: kind = JG_FLUX_HLLC, ROE, AUSM (HLLC matrices), HAENEL or AUSMDV (the
+ * AUSMDV blend with the expansion-fan entropy fix, no shock fix: that needs
+ * the cells' sonic flags); calcEulerFlux_* and calcEulerFluxMatrices_*
+ * (src/joe/UgpWithCvCompFlow.cpp:120-709, 879-1505, 3281-3641).  JST needs
+ * its cells' sensors and is not offered per face.  L/R[n][6] = (rho, u, v,
+ * w, p, gamma), area[n], nvec[n][3] unit normals; F[n][5]; AL/AR[n][5][5] may
+ * be NULL. */
 int jg_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
                         double *F, double *AL, double *AR);
 

@@ -301,7 +301,12 @@ def main():
             tr = json.load(f)
         key = "k_jacobi" if dom["kernel"].startswith("k_jacobi") else "k_flux"
         if key in tr and args.precision in tr[key]:
-            dom["traffic"] = tr[key][args.precision]["bytes_per_cell"] * n
+            entry = tr[key][args.precision]
+            if key == "k_flux":  # per launch shape: lanes per cell
+                entry = entry.get(str(tuned_cl))
+            if entry:
+                dom["traffic"] = entry["bytes_per_cell"] * n
+                dom["traffic_source"] = entry["source"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -393,6 +393,9 @@ __device__ void grad_sdwls(const Mesh& m, const Params& p, const State& st, int 
   }
 }
 
+// SCHEME: the gradient scheme (JG_GRAD_*) as a template parameter, so that each
+// scheme's kernel holds only its own registers
+template <int SCHEME>
 __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, int visc_lim_u, int visc_lim_h,
                        int separate_guv) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -445,7 +448,7 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
       gh[j] += w[j] * b[6];
     }
   }
-  if (p.grad_scheme == JG_GRAD_GREENGAUSS) {
+  if (SCHEME == JG_GRAD_GREENGAUSS) {
     // calcCv{Scalar,Vector}GradGreenGauss (UgpWithCv.h:1091-1184, GG_WITH_DIST): the cell's internal
     // faces in face order with the distance-weighted face value, then its boundary faces, over V
     for (int j = 0; j < 9; j++) gu[j] = 0.0;
@@ -508,7 +511,7 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
       gh[j] /= V;
     }
   }
-  if (p.grad_scheme == JG_GRAD_SDWLS) grad_sdwls(m, p, st, c, gu, gr, gpr, gh);
+  if (SCHEME == JG_GRAD_SDWLS) grad_sdwls(m, p, st, c, gu, gr, gpr, gh);
   // limiter factors over the internal faces of the cell
   double au[3] = {1.0, 1.0, 1.0}, ar = 1.0, ap = 1.0, ah = 1.0;
   const double eps = p.eps;
@@ -1458,6 +1461,16 @@ void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl, double c
   k_dt_final<<<1, 256, 0, s>>>(m, p, st, nb);
   if (p.ts_mode == JG_TS_CFL_MIN) k_dt_min_all<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st);
 }
+static void launch_grad_k(const Mesh& m, const Params& p, State& st, int do_euler, int do_visc, int lim_u, int lim_h,
+                          int separate, cudaStream_t s) {
+  const int g = grid_for(m.ncv, TB);
+  if (p.grad_scheme == JG_GRAD_GREENGAUSS)
+    k_grad<JG_GRAD_GREENGAUSS><<<g, TB, 0, s>>>(m, p, st, do_euler, do_visc, lim_u, lim_h, separate);
+  else if (p.grad_scheme == JG_GRAD_SDWLS)
+    k_grad<JG_GRAD_SDWLS><<<g, TB, 0, s>>>(m, p, st, do_euler, do_visc, lim_u, lim_h, separate);
+  else
+    k_grad<JG_GRAD_LSQ><<<g, TB, 0, s>>>(m, p, st, do_euler, do_visc, lim_u, lim_h, separate);
+}
 void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   int do_euler = p.second_order;
   int do_visc = p.viscous;
@@ -1465,12 +1478,12 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   // viscous velocity gradient: limited like the Euler one when VISC_LIMITER=YES
   int visc_lim = p.visc_limiter && p.limiter;
   int separate = do_visc && do_euler && !p.visc_limiter && p.limiter;
-  k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate);
+  launch_grad_k(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate, s);
 }
 // calcFluxCoupled (JoeWithModels.cpp:4683-4702): grad_u (second order or viscous), grad_rho,
 // grad_p (second order) and grad_enthalpy (viscous), all with the flow limiter; one grad_u
 void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
-  k_grad<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, p.second_order, 1, p.limiter, p.limiter, 0);
+  launch_grad_k(m, p, st, p.second_order, 1, p.limiter, p.limiter, 0, s);
 }
 constexpr int FLUX_CELLS = 128 / FL;  // cells per k_flux2 block
 // residual only: 8 lanes per cell (light kernel, many warps)

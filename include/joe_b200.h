@@ -233,6 +233,9 @@ int jg_get_turb_array(jg_case_t *h, const char *name, double *out);
  * grad_u is what the reference holds after calcRhs: the viscous gradient when
  * MU_REF > 0 (unlimited under VISC_LIMITER=NO), else the Euler one. */
 int jg_get_gradients(jg_case_t *h, double *grad_u, double *grad_rho, double *grad_p, double *grad_h);
+/* the same gradients of the current state computed on their own (calcRhs's
+ * first pass), without the face loop; 5x5 handles, second order or viscous */
+int jg_calc_grad(jg_case_t *h, double *grad_u, double *grad_rho, double *grad_p, double *grad_h);
 
 /* UgpWithCvCompFlow::solveCoupledLinSysNS (src/joe/UgpWithCvCompFlow.h:899-950):
  * solves A dq = rhs with the solver of jg_params.lin_solver; dq is the initial
@@ -255,6 +258,18 @@ int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
 /* sets the CFL and the step count the next step's ramp starts from (the
  * reference's `cfl` and `step` members, e.g. after reading a restart) */
 int jg_set_cfl_step(jg_case_t *h, double cfl, int step);
+/* runBackwardEuler until doneSolver stops it (JoeWithModels.h:42-95): the energy
+ * residual at or below resid_drop x the first step's, or max_steps steps; the
+ * residual is checked every check_every steps (1: exactly as the reference;
+ * more: fewer host round trips, the state then up to check_every - 1 steps past
+ * the step that met the drop).  steps / drop (may be NULL): steps run and the
+ * last step's drop.  Single-case handles. */
+int jg_run_to(jg_case_t *h, double resid_drop, int max_steps, int check_every, int *steps, double *drop);
+/* new run-time settings for a live handle: CFL / DT and the ramp,
+ * under-relaxation, linear-solver thresholds and sweeps, limiter EPS,
+ * time-step mode.  Any other field must equal the handle's (JG_ERR_ARG).  The
+ * CFL the ramp stands at is unchanged (jg_set_cfl_step). */
+int jg_set_params(jg_case_t *h, const jg_params *params);
 /* Batching form (no reference counterpart; the reference runs one case per
  * process): ncases independent cases, each with its own mesh and boundary
  * values, concatenated into one block-diagonal system so that every stage of

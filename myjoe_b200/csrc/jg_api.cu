@@ -1829,3 +1829,81 @@ extern "C" int solveLinSysNSCoupled(jg_case_t* h, double* dq, const double* A, c
                                     double zeroRel, int maxIter, int* iters) {
   return jg_solve_lin_sys(h, dq, A, rhs, zeroAbs, zeroRel, maxIter, iters);
 }
+
+// calcCvVectorGrad / calcCvScalarGrad of the handle's current state on their own (UgpWithCv.h:803-1083),
+// the pass calcRhs starts with: the same kernel, so the arrays equal those of jg_calc_rhs
+extern "C" int jg_calc_grad(jg_case_t* h, double* grad_u, double* grad_rho, double* grad_p, double* grad_h) {
+  if (!h) return set_err(JG_ERR_ARG, "null handle");
+  if (h->bs != 5) return set_err(JG_ERR_ARG, "the coupled path's gradients come with jg_calc_rhs_coupled");
+  if (!h->p.second_order && !h->p.viscous)
+    return set_err(JG_ERR_ARG, "a first-order inviscid case computes no gradients");
+  if (!h->primed) RC(prime(h));
+  launch_grad(h->m, h->p, h->st, h->stream);
+  CKL();
+  return jg_get_gradients(h, grad_u, grad_rho, grad_p, grad_h);
+}
+
+// runBackwardEuler until doneSolver stops it (JoeWithModels.h:42-95): the energy residual at or below
+// resid_drop x the first step's, or max_steps steps.  The residual is checked every check_every
+// steps (1: exactly as the reference; more: fewer host round trips, the state then ends up to
+// check_every - 1 steps past the one that met the drop).  steps / drop (may be NULL): the steps run
+// and the drop of the last step run.
+extern "C" int jg_run_to(jg_case_t* h, double resid_drop, int max_steps, int check_every, int* steps, double* drop) {
+  if (!h || max_steps < 0 || check_every < 1 || !(resid_drop >= 0.0)) return set_err(JG_ERR_ARG, "bad argument");
+  if (h->ncases != 1) return set_err(JG_ERR_ARG, "a batch handle: run its cases with jg_batch_step");
+  const int bs = h->bs;
+  std::vector<double> r((size_t)bs * check_every);
+  double r0 = -1.0, last = 1.0;
+  int done = 0;
+  while (done < max_steps) {
+    const int n = std::min(check_every, max_steps - done);
+    int rc = jg_step(h, n, r.data());
+    if (rc) {
+      if (steps) *steps = done;
+      if (drop) *drop = last;
+      return rc;
+    }
+    bool met = false;
+    for (int k = 0; k < n; k++) {
+      const double e = r[(size_t)k * bs + 4];
+      if (r0 < 0.0) r0 = e;
+      last = r0 > 0.0 ? e / r0 : 0.0;
+      if (last <= resid_drop) met = true;
+    }
+    done += n;
+    if (met) break;
+  }
+  if (steps) *steps = done;
+  if (drop) *drop = last;
+  return JG_OK;
+}
+
+// new run-time settings for a live handle (the reference re-reads its parameters between runs):
+// the CFL / DT settings and ramp, under-relaxation, linear-solver thresholds and sweeps, limiter
+// EPS and the time-step mode.  Settings that shape the handle's arrays (flux, order, limiter on /
+// off, viscosity, model, precision, solver kind, renumbering, gradient scheme, boundary kinds) must
+// not change.  The CFL the ramp stands at is left as it is (jg_set_cfl_step sets it).
+extern "C" int jg_set_params(jg_case_t* h, const jg_params* q) {
+  if (!h || !q) return set_err(JG_ERR_ARG, "null argument");
+  RC(check_params(q));
+  const jg_params& o = h->hp;
+  if (q->flux != o.flux || q->second_order != o.second_order || q->limiter != o.limiter ||
+      q->mu_mode != o.mu_mode || q->mu_ref != o.mu_ref || q->mu_power_law != o.mu_power_law ||
+      q->SL_Tref != o.SL_Tref || q->SL_Sref != o.SL_Sref || q->gamma != o.gamma || q->R_gas != o.R_gas ||
+      q->Pr != o.Pr || q->PrTurb != o.PrTurb || q->T_ref != o.T_ref || q->visc_limiter != o.visc_limiter ||
+      q->symm_bc != o.symm_bc || q->lin_solver != o.lin_solver || q->precision != o.precision ||
+      q->nscal != o.nscal || q->turb_model != o.turb_model || q->renumber != o.renumber ||
+      q->grad_scheme != o.grad_scheme || q->ausm_type != o.ausm_type || q->shock_fix != o.shock_fix ||
+      q->shock_flag != o.shock_flag || q->entropy_fix != o.entropy_fix)
+    return set_err(JG_ERR_ARG, "jg_set_params changes run-time settings only (CFL, DT, ramp, under-relaxation, "
+                               "solver thresholds and sweeps, EPS, time-step mode)");
+  CK(cudaStreamSynchronize(h->stream));
+  const int cl = h->p.flux_cl, rv = h->p.relax_variant;
+  h->hp = *q;
+  h->p = make_params(*q);
+  h->p.flux_cl = cl;
+  h->p.relax_variant = rv;
+  drop_graph(h);
+  return JG_OK;
+}
+

@@ -64,6 +64,9 @@ def lib():
         L.jg_step_async.argtypes = [P, I]
         L.jg_get_cfl_step.argtypes = [P, D, C.POINTER(I)]
         L.jg_set_cfl_step.argtypes = [P, C.c_double, I]
+        L.jg_run_to.argtypes = [P, C.c_double, I, I, C.POINTER(I), D]
+        L.jg_set_params.argtypes = [P, C.POINTER(jg_params)]
+        L.jg_calc_grad.argtypes = [P, D, D, D, D]
         L.jg_euler_flux_faces.argtypes = [I, I, D, D, D, D, D, D, D]
         L.jg_batch_create.argtypes = [I, C.POINTER(jg_mesh), C.POINTER(jg_params), C.POINTER(P)]
         L.jg_batch_info.argtypes = [P, C.POINTER(I), C.POINTER(I)]
@@ -287,6 +290,28 @@ class JoeGpu:
         step = C.c_int(0)
         _ck(lib().jg_get_cfl_step(self.h, C.byref(cfl), C.byref(step)))
         return cfl.value, step.value
+
+    def run_to(self, resid_drop, max_steps, check_every=1):
+        """runBackwardEuler until the energy residual drops to resid_drop x the first
+        step's or max_steps (jg_run_to): returns (steps run, last drop)"""
+        n, d = C.c_int(0), C.c_double(0.0)
+        _ck(lib().jg_run_to(self.h, float(resid_drop), int(max_steps), int(check_every), C.byref(n), C.byref(d)))
+        return n.value, d.value
+
+    def set_params(self, params: JoeParams):
+        """new run-time settings (CFL, ramp, under-relaxation, solver thresholds, EPS) for this handle"""
+        jp = make_params(params, self.jp.precision, bool(self.jp.renumber))
+        _ck(lib().jg_set_params(self.h, C.byref(jp)))
+        self.jp = jp
+        self.params = params
+
+    def calcGrad(self):
+        """calcCvVectorGrad / calcCvScalarGrad of the current state on their own
+        (jg_calc_grad), keyed as ``gradients()``"""
+        n = self.ncv
+        gu, gr, gp, gh = np.empty((n, 3, 3)), np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        _ck(lib().jg_calc_grad(self.h, dptr(gu), dptr(gr), dptr(gp), dptr(gh)))
+        return {"grad_u": gu, "grad_rho": gr, "grad_p": gp, "grad_enthalpy": gh}
 
     def set_cfl_step(self, cfl, step):
         """the CFL and step count the next step's ramp starts from (jg_set_cfl_step)"""

@@ -1,0 +1,89 @@
+"""The driver-level entry points: jg_run_to (runBackwardEuler until the
+energy-residual drop, as doneSolver stops it), jg_set_params (run-time
+settings of a live handle) and jg_calc_grad (the gradient pass on its own).
+Each is checked against the plain calls it must agree with, bit for bit."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from myjoe_b200 import case, solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _bump(**kw):
+    _, g, prm = case.bump_case(24, 12, 2, jitter=0.1, seed=4)
+    return g, dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=10, CFL=1.0,
+                                  CFL_RAMP=(10, 5, 1.2, 20.0), **kw)
+
+
+def _fresh(g, prm):
+    j = solver.JoeGpu(g, prm)
+    j.set_state(*case.perturbed_state(g.x_cv, prm, 0.0))
+    return j
+
+
+@pytest.mark.parametrize("check_every", [1, 25])
+def test_run_to_stops_where_the_drop_is_met(check_every):
+    g, prm = _bump()
+    a = _fresh(g, prm)
+    n, d = a.run_to(1e-6, 4000, check_every)
+    b = _fresh(g, prm)
+    r = b.runBackwardEuler(n)
+    drops = r[:, 4] / r[0, 4]
+    assert d == drops[-1]
+    first = int(np.nonzero(drops <= 1e-6)[0][0]) + 1
+    if check_every == 1:
+        assert n == first
+    else:
+        assert first <= n < first + check_every and n % check_every == 0
+    for x, y in zip(a.get_state(), b.get_state()):
+        np.testing.assert_array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_run_to_max_steps():
+    g, prm = _bump()
+    j = _fresh(g, prm)
+    n, d = j.run_to(0.0, 30, 7)
+    assert n == 30 and 0.0 < d
+    assert j.cfl_step()[1] == 30
+    j.close()
+
+
+def test_set_params_equals_a_handle_made_with_them():
+    g, prm = _bump()
+    new = dataclasses.replace(prm, CFL=2.0, CFL_RAMP=(5, 3, 1.3, 40.0), UNDER_RELAXATION=0.5, LS_MAX_ITER=6,
+                              EPS=0.02)
+    a = _fresh(g, prm)
+    a.runBackwardEuler(3)   # a captured step with the old settings, then the new ones
+    a.set_params(new)
+    a.set_cfl_step(new.CFL, 0)
+    a.set_state(*case.perturbed_state(g.x_cv, prm, 0.0))
+    ra = a.runBackwardEuler(20)
+    b = _fresh(g, new)
+    rb = b.runBackwardEuler(20)
+    np.testing.assert_array_equal(ra, rb)
+    for x, y in zip(a.get_state(), b.get_state()):
+        np.testing.assert_array_equal(x, y)
+    with pytest.raises(solver.JoeGpuError) as e:
+        a.set_params(dataclasses.replace(new, SPACE_INTEGRATION="ROE"))
+    assert e.value.code == -1
+    a.close()
+    b.close()
+
+
+def test_calc_grad_equals_the_gradients_of_calc_rhs():
+    g, prm = _bump()
+    prm = dataclasses.replace(prm, MU_MODE="SUTHERLAND", MU_REF=1.716e-5 * 2000.0)
+    j = solver.JoeGpu(g, prm)
+    j.set_state(*case.perturbed_state(g.x_cv, prm, 0.05))
+    got = j.calcGrad()
+    j.calcDt()
+    j.calcRhs()
+    ref = j.gradients()
+    for k in ("grad_u", "grad_rho", "grad_p", "grad_enthalpy"):
+        np.testing.assert_array_equal(got[k], ref[k])
+    j.close()

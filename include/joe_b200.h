@@ -478,6 +478,18 @@ int jg_restart_load_state(jg_case_t *h, const jg_restart_t *r);
  * be NULL. */
 int jg_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area, const double *nvec,
                         double *F, double *AL, double *AR);
+/* Per-face viscous fluxes and implicit blocks, batched over n faces on the GPU:
+ * addViscFlux (src/joe/UgpWithCvCompFlow.cpp:1521-1763), laminar (no turbulent
+ * viscosity).  S0/S1[n][8] = (rho, u, v, w, h, T, R, gamma) of the two sides,
+ * gu0/gu1[n][3][3] velocity gradients, gh0/gh1[n][3] enthalpy gradients,
+ * mul/lamOcp[n] at the face, u_fa[n][3], area[n], nvec/svec[n][3] the unit
+ * normal and unit cell-to-cell vector, smag[n] the distance; F[n][4] = (Frhou,
+ * FrhoE); A0/A1[n][5][5] (may be NULL): the blocks calcViscousFluxNS
+ * subtracts from the first cell's row (JoeWithModels.cpp:3678-3696). */
+int jg_visc_flux_faces(int n, const double *S0, const double *S1, const double *gu0, const double *gu1,
+                       const double *gh0, const double *gh1, const double *mul, const double *lamOcp,
+                       const double *u_fa, const double *area, const double *nvec, const double *svec,
+                       const double *smag, double *F, double *A0, double *A1);
 
 #ifdef __cplusplus
 }

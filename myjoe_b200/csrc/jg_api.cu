@@ -1907,3 +1907,43 @@ extern "C" int jg_set_params(jg_case_t* h, const jg_params* q) {
   return JG_OK;
 }
 
+// addViscFlux per face on the GPU (per-face parity), laminar: no turbulent viscosity
+extern "C" int jg_visc_flux_faces(int n, const double* S0, const double* S1, const double* gu0, const double* gu1,
+                                  const double* gh0, const double* gh1, const double* mul, const double* lamOcp,
+                                  const double* u_fa, const double* area, const double* nvec, const double* svec,
+                                  const double* smag, double* F, double* A0, double* A1) {
+  const double* host[13] = {S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec, svec, smag};
+  const size_t width[13] = {8, 8, 9, 9, 3, 3, 1, 1, 3, 1, 3, 3, 1};
+  if (n < 0 || !F) return set_err(JG_ERR_ARG, "bad argument");
+  for (int k = 0; k < 13; k++)
+    if (!host[k]) return set_err(JG_ERR_ARG, "null input array %d", k);
+  if (n == 0) return JG_OK;
+  double* dev[13] = {nullptr};
+  double *dF = nullptr, *dA0 = nullptr, *dA1 = nullptr;
+  int rc = JG_OK;
+  auto fail = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == JG_OK) rc = set_err(JG_ERR_CUDA, "%s", cudaGetErrorString(e));
+  };
+  for (int k = 0; k < 13 && rc == JG_OK; k++) {
+    fail(cudaMalloc(&dev[k], width[k] * n * sizeof(double)));
+    if (rc == JG_OK) fail(cudaMemcpy(dev[k], host[k], width[k] * n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (rc == JG_OK) fail(cudaMalloc(&dF, 4 * (size_t)n * sizeof(double)));
+  if (rc == JG_OK && A0) fail(cudaMalloc(&dA0, 25 * (size_t)n * sizeof(double)));
+  if (rc == JG_OK && A1) fail(cudaMalloc(&dA1, 25 * (size_t)n * sizeof(double)));
+  if (rc == JG_OK) {
+    const double* in[13];
+    for (int k = 0; k < 13; k++) in[k] = dev[k];
+    launch_visc_faces(n, in, dF, dA0, dA1, 0);
+    fail(cudaGetLastError());
+  }
+  if (rc == JG_OK) fail(cudaMemcpy(F, dF, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (rc == JG_OK && A0) fail(cudaMemcpy(A0, dA0, 25 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (rc == JG_OK && A1) fail(cudaMemcpy(A1, dA1, 25 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 13; k++) cudaFree(dev[k]);
+  cudaFree(dF);
+  cudaFree(dA0);
+  cudaFree(dA1);
+  return rc;
+}
+

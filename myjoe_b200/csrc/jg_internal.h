@@ -148,6 +148,8 @@ struct Params {
 // launchers (jg_kernels.cu); all enqueue on stream s
 void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_hist_base(State& st, cudaStream_t s);
+// in[13]: S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec, svec, smag (device arrays)
+void launch_visc_faces(int n, const double* const* in, double* F, double* A0, double* A1, cudaStream_t s);
 void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s);

@@ -1615,4 +1615,53 @@ void launch_flux_faces(int kind, int n, const double* L, const double* R, const 
   k_flux_faces<<<grid_for(n, 64), 64, 0, s>>>(kind, n, L, R, area, nvec, F, AL, AR);
 }
 
+// addViscFlux per face (jg_visc_flux_faces): the face-loop's visc_flux and visc_jac_add on given
+// side states; A0 / A1 are the blocks calcViscousFluxNS subtracts from the first cell's row
+// (JoeWithModels.cpp:3678-3696)
+__global__ void k_visc_faces(int n, const double* S0, const double* S1, const double* gu0, const double* gu1,
+                             const double* gh0, const double* gh1, const double* mul, const double* lam,
+                             const double* ufa, const double* area, const double* nvec, const double* svec,
+                             const double* smag, double* F, double* A0, double* A1) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  VSide v[2];
+  const double* S[2] = {S0 + 8 * (size_t)f, S1 + 8 * (size_t)f};
+  const double* gu[2] = {gu0 + 9 * (size_t)f, gu1 + 9 * (size_t)f};
+  const double* gh[2] = {gh0 + 3 * (size_t)f, gh1 + 3 * (size_t)f};
+  for (int k = 0; k < 2; k++) {
+    v[k].rho = S[k][0];
+    for (int i = 0; i < 3; i++) v[k].u[i] = S[k][1 + i];
+    v[k].h = S[k][4];
+    v[k].T = S[k][5];
+    v[k].R = S[k][6];
+    v[k].gam = S[k][7];
+    v[k].gu = gu[k];
+    v[k].gh = gh[k];
+  }
+  const double nV[3] = {nvec[3 * f], nvec[3 * f + 1], nvec[3 * f + 2]};
+  const double sV[3] = {svec[3 * f], svec[3 * f + 1], svec[3 * f + 2]};
+  const double u_fa[3] = {ufa[3 * f], ufa[3 * f + 1], ufa[3 * f + 2]};
+  double Fu[3], FE;
+  VFace vf;
+  visc_flux(Fu, FE, vf, v[0], v[1], mul[f], 0.0, lam[f], 0.9, u_fa, area[f], nV, smag[f], sV);
+  for (int i = 0; i < 3; i++) F[4 * (size_t)f + i] = Fu[i];
+  F[4 * (size_t)f + 3] = FE;
+  if (A0) {
+    double a[25];
+    for (int e = 0; e < 25; e++) a[e] = 0.0;
+    visc_jac_add<double>(a, 1.0, 0, vf, v[0], u_fa);
+    for (int e = 0; e < 25; e++) A0[25 * (size_t)f + e] = a[e];
+  }
+  if (A1) {
+    double a[25];
+    for (int e = 0; e < 25; e++) a[e] = 0.0;
+    visc_jac_add<double>(a, 1.0, 1, vf, v[1], u_fa);
+    for (int e = 0; e < 25; e++) A1[25 * (size_t)f + e] = a[e];
+  }
+}
+void launch_visc_faces(int n, const double* const* in, double* F, double* A0, double* A1, cudaStream_t s) {
+  k_visc_faces<<<grid_for(n, 64), 64, 0, s>>>(n, in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8],
+                                               in[9], in[10], in[11], in[12], F, A0, A1);
+}
+
 }  // namespace jg

@@ -328,6 +328,20 @@ def euler_flux_faces(kind, L, R, area, nvec, matrices=True):
     return F, AL, AR
 
 
+def visc_flux_faces(S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec, svec, smag, matrices=True):
+    """addViscFlux per face on the GPU (jg_visc_flux_faces): (F[n,4], A0[n,5,5], A1[n,5,5])"""
+    a = [np.ascontiguousarray(x, np.float64) for x in (S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec,
+                                                        svec, smag)]
+    n = a[0].shape[0]
+    F = np.zeros((n, 4))
+    A0 = np.zeros((n, 5, 5)) if matrices else None
+    A1 = np.zeros((n, 5, 5)) if matrices else None
+    L = lib()
+    L.jg_visc_flux_faces.argtypes = [C.c_int] + [C.POINTER(C.c_double)] * 16
+    _ck(L.jg_visc_flux_faces(n, *[dptr(x) for x in a], dptr(F), _p(A0), _p(A1)))
+    return F, A0, A1
+
+
 class JoeGpuBatch(JoeGpu):
     """Many independent cases advanced together (jg_batch_create): one launch
     per stage over all cases.  ``cases`` is a list of (mesh, JoeParams); the

@@ -1829,6 +1829,29 @@ static void add_visc_flux(jo_case *h, double Fu[3], double *FE, double (*A0)[5],
   }
 }
 
+/* addViscFlux per face, batched (test entry): S0/S1[n][8] = (rho, u, v, w, h, T, R, gamma) of the two
+ * sides, gu0/gu1[n][9] velocity gradients, gh0/gh1[n][3] enthalpy gradients, mul/lamOcp[n] at the
+ * face, u_fa[n][3], area[n], nV/sV[n][3] unit normal and unit cell-to-cell vector, smag[n];
+ * F[n][4] = (Frhou, FrhoE), A0/A1[n][5][5] (may be NULL).  No turbulent viscosity. */
+void jo_visc_flux_faces(int n, const double *S0, const double *S1, const double *gu0, const double *gu1,
+                        const double *gh0, const double *gh1, const double *mul, const double *lamOcp,
+                        const double *u_fa, const double *area, const double *nV, const double *sV,
+                        const double *smag, double *F, double *A0, double *A1) {
+  jo_case tmp;
+  memset(&tmp, 0, sizeof(tmp));
+  tmp.p.PrTurb = 0.9;
+  for (int f = 0; f < n; f++) {
+    const double *a = &S0[8 * f], *b = &S1[8 * f];
+    double Fu[3], FE;
+    add_visc_flux(&tmp, Fu, &FE, A0 ? (double(*)[5]) & A0[25 * f] : NULL, A1 ? (double(*)[5]) & A1[25 * f] : NULL,
+                  a[0], &a[1], &gu0[9 * f], a[4], &gh0[3 * f], a[5], a[6], a[7], b[0], &b[1], &gu1[9 * f], b[4],
+                  &gh1[3 * f], b[5], b[6], b[7], mul[f], 0.0, lamOcp[f], &u_fa[3 * f], area[f], &nV[3 * f], smag[f],
+                  &sV[3 * f]);
+    for (int i = 0; i < 3; i++) F[4 * f + i] = Fu[i];
+    F[4 * f + 3] = FE;
+  }
+}
+
 /* calcViscousFluxNS, JoeWithModels.cpp:3591-3855 */
 static void calc_viscous_flux(jo_case *h, double *ru, double *rE, double *A, int implicit) {
   const jg_mesh *m = &h->m;

@@ -42,6 +42,10 @@ int jo_step_count(jo_case *h);
  * area[n], nvec[n][3]; F[n][5]; AL/AR[n][25] (may be NULL) */
 void jo_euler_flux_faces(int kind, int n, const double *L, const double *R, const double *area,
                          const double *nvec, double *F, double *AL, double *AR);
+void jo_visc_flux_faces(int n, const double *S0, const double *S1, const double *gu0, const double *gu1,
+                        const double *gh0, const double *gh1, const double *mul, const double *lamOcp,
+                        const double *u_fa, const double *area, const double *nV, const double *sV,
+                        const double *smag, double *F, double *A0, double *A1);
 
 /* Coupled path with a turbulence model (jg_params.turb_model SA: nscal 1, block
  * 6; SST: nscal 2 (kine, omega), block 7): scalars phi[ncv][nscal] in/out,

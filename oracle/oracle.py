@@ -31,6 +31,7 @@ def lib():
         L.jo_create.restype = P
         L.jo_create.argtypes = [C.POINTER(jg_mesh), C.POINTER(jg_params)]
         L.jo_destroy.argtypes = [P]
+        L.jo_visc_flux_faces.argtypes = [C.c_int] + [D] * 16
         L.jo_set_state.argtypes = [P, D, D, D]
         L.jo_get_state.argtypes = [P, D, D, D]
         L.jo_calc_state.argtypes = [P]
@@ -209,6 +210,19 @@ class OracleSA(Oracle):
         if lib().jo_step_coupled(self.h, nsteps, dptr(r)):
             raise ValueError("oracle step failed")
         return r
+
+
+def visc_flux_faces(S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec, svec, smag, matrices=True):
+    """addViscFlux per face (jo_visc_flux_faces): (F[n,4], A0[n,5,5], A1[n,5,5])"""
+    a = [np.ascontiguousarray(x, np.float64) for x in (S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec,
+                                                        svec, smag)]
+    n = a[0].shape[0]
+    F = np.zeros((n, 4))
+    A0 = np.zeros((n, 5, 5)) if matrices else None
+    A1 = np.zeros((n, 5, 5)) if matrices else None
+    lib().jo_visc_flux_faces(n, *[dptr(x) for x in a], dptr(F), dptr(A0) if matrices else None,
+                             dptr(A1) if matrices else None)
+    return F, A0, A1
 
 
 def euler_flux_faces(kind, L, R, area, nvec, matrices=True):

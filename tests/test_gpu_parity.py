@@ -223,6 +223,41 @@ def test_per_face_fluxes(kind):
     assert (np.abs(ARg - ARo).reshape(n, -1).max(1) / ms).max() <= TOL
 
 
+def test_per_face_viscous_fluxes():
+    """addViscFlux + its blocks over random face states and gradients, GPU vs
+    oracle (the oracle's viscous flux is pinned through the laminar fixtures'
+    calcRhs)."""
+    from oracle.oracle import visc_flux_faces as oracle_visc
+    rng = np.random.default_rng(29)
+    n = 4096
+    def side():
+        rho = rng.uniform(0.3, 2.0, n)
+        T = rng.uniform(200.0, 400.0, n)
+        u = rng.normal(0.0, 50.0, (n, 3))
+        h = 1.4 * 287.0 / 0.4 * T
+        return np.column_stack([rho, u, h, T, np.full(n, 287.0), np.full(n, 1.4)])
+    S0, S1 = side(), side()
+    gu0, gu1 = rng.normal(0.0, 100.0, (n, 9)), rng.normal(0.0, 100.0, (n, 9))
+    gh0, gh1 = rng.normal(0.0, 1e5, (n, 3)), rng.normal(0.0, 1e5, (n, 3))
+    mul = rng.uniform(1e-5, 1e-3, n)
+    lam = mul / 0.72
+    nv = rng.normal(size=(n, 3))
+    nv /= np.linalg.norm(nv, axis=1)[:, None]
+    sv = nv + 0.3 * rng.normal(size=(n, 3))
+    sv /= np.linalg.norm(sv, axis=1)[:, None]
+    smag = rng.uniform(1e-3, 0.1, n)
+    ufa = 0.5 * (S0[:, 1:4] + S1[:, 1:4])
+    area = rng.uniform(1e-3, 1.0, n)
+    args = (S0, S1, gu0, gu1, gh0, gh1, mul, lam, ufa, area, nv, sv, smag)
+    Fo, A0o, A1o = oracle_visc(*args)
+    Fg, A0g, A1g = solver.visc_flux_faces(*args)
+    fs = np.abs(Fo).max(axis=0)
+    assert (np.abs(Fg - Fo).max(axis=0) / fs).max() <= TOL
+    for g, o in ((A0g, A0o), (A1g, A1o)):
+        sc = np.abs(o).reshape(n, -1).max(1)
+        assert (np.abs(g - o).reshape(n, -1).max(1) / sc).max() <= TOL
+
+
 @pytest.mark.parametrize("which", ["bump_64x32x4_hllc", "plate_256x96x2_roe"])
 def test_full_size_calc_rhs(which):
     """calcRhs at the benchmark sizes (8,192 and 49,152 cells) against the oracle."""

@@ -176,8 +176,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--face-loop", default="auto", choices=["auto", "1", "2", "4"],
-                    help="face loop lanes per cell: autotuned, or 1, 2, 4")
+    ap.add_argument("--face-loop", default="auto", choices=["auto", "1", "2", "4", "17"],
+                    help="face loop shape: autotuned, 1/2/4 lanes per cell, or 17 (one lane, 3 blocks per SM)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -325,7 +325,9 @@ def main():
                 "config": {"workload": WORKLOAD, "cells": n, "internal_faces_per_cell": round(f_int, 4),
                            "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": "replicas" if world > 1 else "single case",
-                           "launch_shape": {"face_loop_lanes_per_cell": tuned_cl, "sweep_kernel": tuned_sweep}},
+                           "launch_shape": {"face_loop": ("1 lane per cell, 3 blocks per SM" if tuned_cl == 17
+                                                          else "%d lanes per cell" % tuned_cl),
+                                            "sweep_kernel": tuned_sweep}},
                 "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": 5 * 8 * n,
                         "d2h_bytes_per_step": 5 * 8 * n + 40},
                 "gpu_launches": kernels_per_step * args.steps,

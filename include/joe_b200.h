@@ -298,15 +298,19 @@ int jg_batch_status(jg_case_t *h, int *status);
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
 /* Launch shapes (no reference counterpart): the lanes per cell of the 5x5
- * face loop (1, 2 or 4; default 1) and the kernel of the 5x5 Jacobi sweep (0:
- * a block per 32-cell slice, a thread per block row, the default; 1: a thread
- * per cell).  jg_autotune times each candidate on the handle's own mesh
- * (trials launches, CUDA events) and keeps the fastest; ms[5] (may be NULL)
- * gets the face loop time per launch for 1, 2, 4 lanes and the sweep time for
- * kernels 0, 1.  The sweep kernels give bit-identical results; the lanes per
+ * face loop (flux_cl = 1, 2 or 4, with registers for two 128-thread blocks
+ * per SM; default 1; or JG_FLUX_CL1_3BLK: one lane, registers capped for three
+ * blocks per SM, more warps to hide FP64 latency at the price of some spills)
+ * and the kernel of the 5x5 Jacobi sweep (0: a block per 32-cell slice, a
+ * thread per block row, the default; 1: a thread per cell).  jg_autotune
+ * times each candidate on the handle's own mesh (trials launches, CUDA
+ * events) and keeps the fastest; ms[6] (may be NULL) gets the face loop time
+ * per launch for 1, 2, 4 lanes (ms[0..2]), the sweep time for kernels 0, 1
+ * (ms[3..4]) and the face loop time for JG_FLUX_CL1_3BLK (ms[5]).  The sweep kernels give bit-identical results; the lanes per
  * cell change the order of each cell's diagonal-block and residual sums
  * (rounding-level differences).  Handles without a turbulence model; others
  * keep their single shape.  A batch handle tunes for all its cases. */
+#define JG_FLUX_CL1_3BLK 17
 int jg_set_launch_config(jg_case_t *h, int flux_cl, int relax_variant);
 int jg_get_launch_config(jg_case_t *h, int *flux_cl, int *relax_variant);
 int jg_autotune(jg_case_t *h, int trials, int *flux_cl, int *relax_variant, float *ms);

@@ -1742,7 +1742,8 @@ static void drop_graph(jg_case* h) {
 
 extern "C" int jg_set_launch_config(jg_case_t* h, int flux_cl, int relax_variant) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
-  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4) return set_err(JG_ERR_ARG, "lanes per cell must be 1, 2 or 4");
+  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4 && flux_cl != JG_FLUX_CL1_3BLK)
+    return set_err(JG_ERR_ARG, "face loop shape must be 1, 2, 4 lanes per cell or JG_FLUX_CL1_3BLK");
   if (relax_variant != 0 && relax_variant != 1) return set_err(JG_ERR_ARG, "sweep kernel must be 0 or 1");
   CK(cudaStreamSynchronize(h->stream));
   h->p.flux_cl = flux_cl;
@@ -1773,10 +1774,12 @@ extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_va
     launch_dt(h->m, h->p, h->st, 1, 0.0, S);
     launch_grad(h->m, h->p, h->st, S);
     Params p = h->p;
-    const int cls[3] = {1, 2, 4};
+    // ms[0..2]: 1, 2, 4 lanes per cell; ms[5]: one lane with three blocks per SM
+    const int cls[4] = {1, 2, 4, JG_FLUX_CL1_3BLK};
+    const int slot[4] = {0, 1, 2, 5};
     float best = 1e30f;
     int best_cl = h->p.flux_cl, best_v = h->p.relax_variant;
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < 4; i++) {
       p.flux_cl = cls[i];
       launch_flux(h->m, p, h->st, 1, 1, S);  // warm-up
       CK(cudaEventRecord(e0, S));
@@ -1785,7 +1788,7 @@ extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_va
       CK(cudaEventSynchronize(e1));
       float t_ms = 0.0f;
       CK(cudaEventElapsedTime(&t_ms, e0, e1));
-      if (ms) ms[i] = t_ms / trials;
+      if (ms) ms[slot[i]] = t_ms / trials;
       if (t_ms < best) { best = t_ms; best_cl = cls[i]; }
     }
     p.flux_cl = best_cl;

@@ -739,8 +739,11 @@ __device__ __forceinline__ int bnd_opts(const Params& p) {
   return KIND == 4 ? (p.ausm_type | (p.entropy_fix ? FO_EFIX : 0)) : 0;
 }
 
-template <typename BT, int KIND, int VISC, int CL>
-__global__ void __launch_bounds__(128) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
+// MINB: resident blocks per SM the register allocation must allow (__launch_bounds__): 2 lets the
+// compiler use all 255 registers; 3 caps it near 168 (some spills to L1-cached local memory) for
+// 12 instead of 8 warps per SM, which hides more FP64 latency on some meshes (jg_autotune decides)
+template <typename BT, int KIND, int VISC, int CL, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
   // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
   // FP32 for the mixed form's preconditioner (the residual is FP64 in both)
   using JT = BT;
@@ -1502,19 +1505,22 @@ static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implici
   else if (p.flux == JG_FLUX_JST) launch_flux_k<BT, 5>(m, p, st, implicit, for_step, s);
   else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
 }
-template <typename BT, int KIND, int CL>
+template <typename BT, int KIND, int CL, int MINB>
 static void launch_flux_cell_cl(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
   size_t shm = 25 * TB * sizeof(BT);
   const int g = grid_for(m.ncv, TB / CL);
-  if (p.viscous) k_flux<BT, KIND, 1, CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
-  else k_flux<BT, KIND, 0, CL><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+  if (p.viscous) k_flux<BT, KIND, 1, CL, MINB><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
+  else k_flux<BT, KIND, 0, CL, MINB><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
 }
 // lanes per cell of the implicit face loop: p.flux_cl (1, 2 or 4)
+// p.flux_cl: lanes per cell 1, 2 or 4 (two 128-thread blocks per SM), or JG_FLUX_CL1_3BLK
+// (one lane, three blocks per SM)
 template <typename BT, int KIND>
 static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1>(m, p, st, for_step, s);
-  else if (p.flux_cl == 4) launch_flux_cell_cl<BT, KIND, 4>(m, p, st, for_step, s);
-  else launch_flux_cell_cl<BT, KIND, 2>(m, p, st, for_step, s);
+  if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1, 2>(m, p, st, for_step, s);
+  else if (p.flux_cl == JG_FLUX_CL1_3BLK) launch_flux_cell_cl<BT, KIND, 1, 3>(m, p, st, for_step, s);
+  else if (p.flux_cl == 4) launch_flux_cell_cl<BT, KIND, 4, 2>(m, p, st, for_step, s);
+  else launch_flux_cell_cl<BT, KIND, 2, 2>(m, p, st, for_step, s);
 }
 template <typename BT>
 static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {

@@ -272,9 +272,10 @@ class JoeGpu:
         """time the launch shapes on this handle and keep the fastest: returns
         (lanes per cell of the face loop, sweep kernel, {shape: ms per launch})"""
         cl, rv = C.c_int(0), C.c_int(0)
-        ms = (C.c_float * 5)()
+        ms = (C.c_float * 6)()
         _ck(lib().jg_autotune(self.h, int(trials), C.byref(cl), C.byref(rv), ms))
-        times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4]}
+        times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4],
+                 "flux_cl17": ms[5]}
         return cl.value, rv.value, times
 
     def set_launch_config(self, flux_cl, relax_variant):

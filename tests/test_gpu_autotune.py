@@ -42,7 +42,7 @@ def test_sweep_kernels_are_bitwise_equal():
         np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("cl", [1, 4])
+@pytest.mark.parametrize("cl", [1, 4, 17])
 def test_lanes_per_cell_agree_to_rounding(cl):
     g, prm = _plate("SGS")
     a = _run(g, prm, (2, 0))
@@ -57,9 +57,9 @@ def test_autotune_picks_a_valid_shape_and_keeps_results():
     j = solver.JoeGpu(g, prm)
     j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
     cl, rv, ms = j.autotune(3)
-    assert cl in (1, 2, 4) and rv in (0, 1)
+    assert cl in (1, 2, 4, 17) and rv in (0, 1)
     assert all(v > 0.0 for v in ms.values())
-    assert ms["flux_cl%d" % cl] == min(ms["flux_cl1"], ms["flux_cl2"], ms["flux_cl4"])
+    assert ms["flux_cl%d" % cl] == min(ms["flux_cl1"], ms["flux_cl2"], ms["flux_cl4"], ms["flux_cl17"])
     r = j.runBackwardEuler(10)   # the tuned shape is captured at the next step
     assert np.all(np.isfinite(r))
     ref = _run(g, prm, (cl, rv))

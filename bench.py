@@ -67,46 +67,57 @@ def algorithmic_bytes(g, precision):
 
 
 class ClockSampler:
-    def __init__(self, index):
-        self.proc = None
-        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Read-only NVML samples of the SM clock and the clock-event reasons of the
+    GPU this process runs on, every `period` seconds in a thread, until stop().
+    The GPU is found by its UUID (from the CUDA device this process uses), so a
+    remapping by CUDA_VISIBLE_DEVICES cannot point the query at another GPU."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, device_index, period=0.02):
+        import threading
+        self.samples, self.uuid, self.error = [], None, None
+        self._stop = threading.Event()
+        self._thread = None
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            u = str(torch.cuda.get_device_properties(device_index).uuid)
+            self.uuid = u if u.startswith("GPU-") else "GPU-" + u
+            self._nvml = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(self.uuid)
+            self._max = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: the line says why
+            self.error = "%s: %s" % (type(e).__name__, e)
+            return
+        self._thread = threading.Thread(target=self._run, args=(period,), daemon=True)
+        self._thread.start()
+
+    def _run(self, period):
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+                self.samples.append((sm, rs))
+            except Exception as e:
+                self.error = "%s: %s" % (type(e).__name__, e)
+                return
+            self._stop.wait(period)
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = max(smax, float(parts[2]))
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if parts[5 + k].lower() == "active":
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
-            return None
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        if self._thread is None:
+            return {"error": self.error} if self.error else None
+        self._stop.set()
+        self._thread.join(timeout=5)
+        if not self.samples:
+            return {"gpu_uuid": self.uuid, "samples": 0, "error": self.error}
+        sm = sorted(x for x, _ in self.samples)
+        reasons = sorted({nm for _, rs in self.samples for nm, bit in self.REASONS if rs & bit})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self._max, "reasons": reasons,
+                "samples": len(sm), "gpu_uuid": self.uuid}
 
 
 def reference_run(raw, prm, nsteps, nproc):

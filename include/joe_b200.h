@@ -258,12 +258,15 @@ int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
 /* sets the CFL and the step count the next step's ramp starts from (the
  * reference's `cfl` and `step` members, e.g. after reading a restart) */
 int jg_set_cfl_step(jg_case_t *h, double cfl, int step);
-/* runBackwardEuler until doneSolver stops it (JoeWithModels.h:42-95): the energy
- * residual at or below resid_drop x the first step's, or max_steps steps; the
- * residual is checked every check_every steps (1: exactly as the reference;
- * more: fewer host round trips, the state then up to check_every - 1 steps past
- * the step that met the drop).  steps / drop (may be NULL): steps run and the
- * last step's drop.  Single-case handles. */
+/* runBackwardEuler until a residual rule stops it, or max_steps steps.
+ * resid_drop >= 0: a RELATIVE drop, the energy residual at or below
+ * resid_drop x the first step's (not the reference's rule).  resid_drop < 0:
+ * the reference's doneSolver rule (JoeWithModels.h:64, RESID_ENERG_TH): the
+ * absolute energy residual strictly below -resid_drop.  The residual is checked
+ * every check_every steps (1: step by step as the reference; more: fewer host
+ * round trips, the state then up to check_every - 1 steps past the step that
+ * met the rule).  steps / drop (may be NULL): steps run and the last step's
+ * relative drop.  Single-case handles. */
 int jg_run_to(jg_case_t *h, double resid_drop, int max_steps, int check_every, int *steps, double *drop);
 /* new run-time settings for a live handle: CFL / DT and the ramp,
  * under-relaxation, linear-solver thresholds and sweeps, limiter EPS,
@@ -346,7 +349,9 @@ typedef struct jg_server jg_server_t;
 typedef struct {
   int device;                /* CUDA device */
   int max_resident;          /* cases on the device at once (>= 1) */
-  double hbm_budget;         /* device bytes the resident cases may hold; <= 0: 90% of the free memory */
+  double hbm_budget;         /* device bytes the resident cases may hold; <= 0: 90% of the free memory.
+                              * A case whose footprint is above it is retired as JG_SERVE_FAILED
+                              * (with its initial state) without being started. */
   int steps_per_poll;        /* steps launched per case between residual checks (1..64) */
   double resid_drop;         /* convergence: energy residual / first-step energy residual */
   int max_steps;             /* retire unconverged after this many steps */
@@ -402,7 +407,9 @@ int jg_step_kernel_count(jg_case_t *h, int *n);
  * All pointers are DEVICE memory owned by the caller, in the reference's
  * layouts: nbocv_i[ncv+1], nbocv_v[nnz] (CSR, diagonal first), A[nnz][5][5],
  * rhs[ncv][5]; dq[ncv][5] receives the result of `sweeps` block Jacobi sweeps
- * from zero (the iteration of jg_solve_lin_sys with JG_LS_JACOBI).  Work
+ * from zero (the iteration of jg_solve_lin_sys with JG_LS_JACOBI, equal to it
+ * to rounding: the diagonal block is applied through its LU factors, as the
+ * reference's lusolv does, not through a stored inverse).  Work
  * memory is a fixed array of JG_NOALLOC_MAX_CELLS x 5 doubles (2.5 MiB) inside
  * the library, held by every GPU that loads it until the process exits;
  * ncv > JG_NOALLOC_MAX_CELLS is rejected with JG_ERR_ARG.  The first call on

@@ -1846,13 +1846,15 @@ extern "C" int jg_calc_grad(jg_case_t* h, double* grad_u, double* grad_rho, doub
   return jg_get_gradients(h, grad_u, grad_rho, grad_p, grad_h);
 }
 
-// runBackwardEuler until doneSolver stops it (JoeWithModels.h:42-95): the energy residual at or below
-// resid_drop x the first step's, or max_steps steps.  The residual is checked every check_every
-// steps (1: exactly as the reference; more: fewer host round trips, the state then ends up to
-// check_every - 1 steps past the one that met the drop).  steps / drop (may be NULL): the steps run
-// and the drop of the last step run.
+// runBackwardEuler until a residual rule stops it, or max_steps steps.  resid_drop >= 0: the energy
+// residual at or below resid_drop x the first step's (a relative drop); resid_drop < 0: doneSolver's
+// rule (JoeWithModels.h:64), the absolute energy residual strictly below -resid_drop.  The residual
+// is checked every check_every steps (1: step by step; more: fewer host round trips, the state then
+// ends up to check_every - 1 steps past the one that met the rule).  steps / drop (may be NULL): the
+// steps run and the relative drop of the last step run.
 extern "C" int jg_run_to(jg_case_t* h, double resid_drop, int max_steps, int check_every, int* steps, double* drop) {
-  if (!h || max_steps < 0 || check_every < 1 || !(resid_drop >= 0.0)) return set_err(JG_ERR_ARG, "bad argument");
+  if (!h || max_steps < 0 || check_every < 1 || !(resid_drop == resid_drop)) return set_err(JG_ERR_ARG, "bad argument");
+  const bool absolute = resid_drop < 0.0;
   if (h->ncases != 1) return set_err(JG_ERR_ARG, "a batch handle: run its cases with jg_batch_step");
   const int bs = h->bs;
   std::vector<double> r((size_t)bs * check_every);
@@ -1871,7 +1873,7 @@ extern "C" int jg_run_to(jg_case_t* h, double resid_drop, int max_steps, int che
       const double e = r[(size_t)k * bs + 4];
       if (r0 < 0.0) r0 = e;
       last = r0 > 0.0 ? e / r0 : 0.0;
-      if (last <= resid_drop) met = true;
+      if (absolute ? (e < -resid_drop) : (last <= resid_drop)) met = true;
     }
     done += n;
     if (met) break;
@@ -1900,6 +1902,9 @@ extern "C" int jg_set_params(jg_case_t* h, const jg_params* q) {
       q->shock_flag != o.shock_flag || q->entropy_fix != o.entropy_fix)
     return set_err(JG_ERR_ARG, "jg_set_params changes run-time settings only (CFL, DT, ramp, under-relaxation, "
                                "solver thresholds and sweeps, EPS, time-step mode)");
+  // a batch keeps the promise jg_batch_create makes: no setting that couples its cases
+  if (h->ncases > 1 && q->time_step_mode == JG_TS_CFL_MIN)
+    return set_err(JG_ERR_ARG, "CFL_MIN would couple the cases of a batch");
   CK(cudaStreamSynchronize(h->stream));
   const int cl = h->p.flux_cl, rv = h->p.relax_variant;
   h->hp = *q;

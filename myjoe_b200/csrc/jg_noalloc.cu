@@ -10,8 +10,10 @@
 //
 // jg_relax_csr_noalloc runs block Jacobi sweeps on a system given in the
 // reference's own layout (CSR over nbocv, diagonal block first, A[nnz][5][5],
-// rhs/dq[ncv][5]) -- the same iteration as jg_solve_lin_sys with
-// lin_solver = JG_LS_JACOBI.  Its only working memory is one vector of
+// rhs/dq[ncv][5]) -- the iteration of jg_solve_lin_sys with lin_solver =
+// JG_LS_JACOBI, agreeing with it to rounding (here each sweep solves with the
+// LU factors, as lusolv does; that path multiplies by the stored inverse).
+// Its only working memory is one vector of
 // JG_NOALLOC_MAX_CELLS x 5 doubles (2.5 MiB) in a file-scope __device__ array,
 // which every GPU that loads the library holds until the process exits.
 #include <cuda_runtime.h>
@@ -80,9 +82,9 @@ __device__ void lu_solve5(double* A, double* c) {
     for (int jm = 0; jm < jr; jm++) sum -= A[5 * jr + jm] * c[jm];
     c[jr] = sum / A[5 * jr + jr];
   }
-  for (int jr = 3; jr >= 0; jr--) {
+  for (int jr = 3; jr >= 0; jr--) {  // lusolv subtracts from the last column back
     double sum = c[jr];
-    for (int jm = jr + 1; jm < 5; jm++) sum -= A[5 * jr + jm] * c[jm];
+    for (int jm = 4; jm > jr; jm--) sum -= A[5 * jr + jm] * c[jm];
     c[jr] = sum;
   }
 }

@@ -232,7 +232,13 @@ static int finish(jg_server* s, Request* r, int status) {
   f.rho.resize(N);
   f.rhou.resize(3 * (size_t)N);
   f.rhoE.resize(N);
-  if (r->h) SRC(jg_get_state(r->h, f.rho.data(), f.rhou.data(), f.rhoE.data()));
+  if (r->h) {
+    SRC(jg_get_state(r->h, f.rho.data(), f.rhou.data(), f.rhoE.data()));
+  } else {  // never started: its initial state
+    f.rho = r->rho;
+    f.rhou = r->rhou;
+    f.rhoE = r->rhoE;
+  }
   jg_serve_result& o = f.res;
   o.id = r->id;
   o.status = status;
@@ -370,15 +376,26 @@ int jg_serve_poll(jg_server_t* s, double max_wait_s, jg_serve_result* out, int c
       if (!s->resident.empty() && s->bytes_resident + r->footprint > s->budget) break;
       std::unique_ptr<Request> own = std::move(s->queue[pick]);
       s->queue.erase(s->queue.begin() + pick);
-      int rc = start_case(s, r);
+      // a case that cannot fit even an empty device (its footprint above the budget, or its
+      // allocation failing with nothing else resident) is retired as failed, so that poll
+      // reports it, and the server goes on with the others
+      int rc = r->footprint > s->budget ? JG_ERR_NOMEM : start_case(s, r);
       if (rc == JG_ERR_NOMEM && !s->resident.empty()) {
         // the pool is fuller than the estimate says: wait for a retirement
         release_case(s, r);
         s->queue.insert(s->queue.begin() + pick, std::move(own));
         break;
       }
-      if (rc != JG_OK) {
+      if (rc == JG_ERR_NOMEM || rc == JG_ERR_ARG) {
         release_case(s, r);
+        SRC(finish(s, r, JG_SERVE_FAILED));
+        progressed = true;
+        continue;
+      }
+      if (rc != JG_OK) {
+        // a CUDA error: the request goes back to the queue (not lost) and the error to the caller
+        release_case(s, r);
+        s->queue.insert(s->queue.begin() + pick, std::move(own));
         return rc;
       }
       r->t_admit = r->t_admit < 0.0 ? s->now() : r->t_admit;

@@ -294,7 +294,9 @@ class JoeGpu:
 
     def run_to(self, resid_drop, max_steps, check_every=1):
         """runBackwardEuler until the energy residual drops to resid_drop x the first
-        step's or max_steps (jg_run_to): returns (steps run, last drop)"""
+        step's (resid_drop >= 0), or falls strictly below -resid_drop (resid_drop < 0:
+        the reference's RESID_ENERG_TH rule), or max_steps (jg_run_to): returns
+        (steps run, last relative drop)"""
         n, d = C.c_int(0), C.c_double(0.0)
         _ck(lib().jg_run_to(self.h, float(resid_drop), int(max_steps), int(check_every), C.byref(n), C.byref(d)))
         return n.value, d.value

@@ -65,7 +65,7 @@ def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout
     the restart.out runBackwardEuler leaves) come back as bytes in
     dumps["files"]."""
     if not available():
-        raise FileNotFoundError("reference harness not built: make -C oracle")
+        raise FileNotFoundError("reference harness not built: make -C oracle ref REF=<the reference src directory>")
     with tempfile.TemporaryDirectory(prefix="joe_ref_") as d:
         if mesh_writer is not None:
             mesh_writer(os.path.join(d, "mesh.msh"))

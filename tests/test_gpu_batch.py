@@ -149,3 +149,19 @@ def test_batch_refuses_cases_with_different_fluids():
     cs[1] = (g, dataclasses.replace(prm, MU_REF=2.0 * prm.MU_REF))
     with pytest.raises(ValueError):
         solver.JoeGpuBatch(cs)
+
+
+def test_batch_refuses_a_coupling_time_step_mode_after_creation():
+    """jg_set_params on a batch handle refuses CFL_MIN (one minimum over the
+    cells of every case would couple them), as jg_batch_create does; the
+    handle keeps stepping with its old settings."""
+    import ctypes as C
+    from myjoe_b200.abi import jg_params
+    b = solver.JoeGpuBatch(cases())
+    q = jg_params()
+    C.memmove(C.byref(q), C.byref(b.jp), C.sizeof(jg_params))
+    q.time_step_mode = 1  # JG_TS_CFL_MIN
+    assert solver.lib().jg_set_params(b.h, C.byref(q)) == -1  # JG_ERR_ARG
+    r = b.runBackwardEulerCases(2)
+    assert np.all(np.isfinite(r))
+    b.close()

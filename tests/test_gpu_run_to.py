@@ -44,6 +44,21 @@ def test_run_to_stops_where_the_drop_is_met(check_every):
     b.close()
 
 
+def test_run_to_absolute_threshold_is_strict():
+    """resid_drop < 0: the reference's doneSolver rule, the absolute energy
+    residual strictly below the threshold (RESID_ENERG_TH)."""
+    g, prm = _bump()
+    b = _fresh(g, prm)
+    r = b.runBackwardEuler(400)
+    th = float(r[250, 4])           # a residual the run reaches exactly
+    first = int(np.nonzero(r[:, 4] < th)[0][0]) + 1
+    a = _fresh(g, prm)
+    n, _ = a.run_to(-th, 400, 1)
+    assert n == first and n != 251   # step 251's residual equals the threshold: not below it
+    b.close()
+    a.close()
+
+
 def test_run_to_max_steps():
     g, prm = _bump()
     j = _fresh(g, prm)

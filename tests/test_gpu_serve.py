@@ -99,3 +99,31 @@ def test_footprint_is_exact(precision):
         j.set_state(*case.perturbed_state(mesh.x_cv, p, 0.0))
         assert j.device_bytes() == est
         j.close()
+
+
+def test_case_above_the_budget_is_reported_failed():
+    """A case whose footprint exceeds the whole memory budget can never be
+    admitted: poll reports it as failed, with its initial state, and the
+    cases that fit are served as usual."""
+    from myjoe_b200 import solver
+    cases = _cases()
+    fp = [solver.case_footprint(c[0], c[1], 0) for c in cases]
+    small = int(np.argmin(fp))
+    big = int(np.argmax(fp))
+    assert fp[big] > 1.2 * fp[small]
+    srv = solver.JoeServer(steps_per_poll=25, resid_drop=DROP, max_steps=3000, max_restarts=0,
+                           hbm_budget=1.1 * fp[small])
+    g, prm, st = cases[big]
+    id_big = srv.submit(g, prm, st)
+    g, prm, st = cases[small]
+    id_small = srv.submit(g, prm, st)
+    res = {}
+    while len(res) < 2:
+        for r in srv.poll(max_wait=0.01):
+            res[r["id"]] = (r, srv.fetch(r["id"]))
+    srv.close()
+    r, state = res[id_big]
+    assert r["status"] == 2 and r["steps"] == 0
+    for a, b in zip(state, cases[big][2]):
+        np.testing.assert_array_equal(np.asarray(a).reshape(np.shape(b)), b)
+    assert res[id_small][0]["status"] == 0

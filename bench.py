@@ -179,6 +179,36 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+CONVERGE_WORKLOAD = ("burst of seeded channel-bump cases (hex, 2 cell layers; cells log-uniform, Mach U(0.3,0.8), "
+                     "AoA U(+-4 deg), bump U(0.05,0.12)), inviscid HLLC, second order, far field, SGS x10, "
+                     "CFL 1 -> 20, each retired at a 1e-8 drop of its L1 energy residual")
+
+
+def build_converge_cases(args, rank):
+    import multiprocessing as mp
+    from myjoe_b200 import serve
+    lo, hi = (int(x) for x in args.converge_cells.split(","))
+    specs = serve.case_specs(args.converge_cases, lo, hi, seed=1000 + rank)
+    with mp.get_context("spawn").Pool(min(len(specs), os.cpu_count() or 1)) as pool:
+        return pool.map(serve.build_request, specs)
+
+
+def converge_leg(cases, args):
+    """The north-star comparison on one GPU: the same case list through the plain FP64 drop-in
+    (one case at a time, Jacobian every step) and through the serving form (mixed precision,
+    lagged Jacobian, many cases resident)."""
+    from myjoe_b200 import serve
+    cfg = serve.BurstConfig(jac_lag=args.jac_lag)
+    plain = serve.run_burst("plain", cases, cfg)
+    served = serve.run_burst("serve", cases, cfg)
+    return {"workload": CONVERGE_WORKLOAD, "cases": len(cases), "cells": args.converge_cells,
+            "cells_total": int(sum(c[0].ncv for c in cases)),
+            "solves_per_hour": served["solves_per_hour"], "p50_s": served["p50_s"], "p99_s": served["p99_s"],
+            "plain_fp64": plain, "serving": served,
+            "ratio_vs_plain_fp64": served["solves_per_hour"] / plain["solves_per_hour"]
+            if plain["solves_per_hour"] > 0 else None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -187,8 +217,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--face-loop", default="auto", choices=["auto", "1", "2", "4", "17"],
-                    help="face loop shape: autotuned, 1/2/4 lanes per cell, or 17 (one lane, 3 blocks per SM)")
+    ap.add_argument("--face-loop", default="auto", choices=["auto", "1", "2", "4", "17", "33", "34", "36", "40"],
+                    help="face loop shape: autotuned; fused 1/2/4 lanes per cell or 17 (one lane, 3 blocks per SM); "
+                         "split 32 + lanes per cell of the residual kernel")
+    ap.add_argument("--converge-cases", type=int, default=24,
+                    help="cases of the time-to-converge leg (0: skip it)")
+    ap.add_argument("--converge-cells", default="5000,500000", help="cells log-uniform on lo,hi")
+    ap.add_argument("--jac-lag", type=int, default=4, help="serving arm: flux Jacobian every k-th step")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -201,6 +236,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the time-to-converge cases are meshed by a spawn pool on the host cores, outside every timed region
+    conv_cases = build_converge_cases(args, rank) if args.converge_cases > 0 else None
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
@@ -249,7 +286,6 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clk = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_s = sum(step_ms) / 1000.0
     if world > 1:
@@ -285,6 +321,34 @@ def main():
         e2e_s = float(t.item())
     e2e = world * n * args.steps / e2e_s
 
+    # like for like with the reference arm: the same case with the GPU's BiCGSTAB x10 (the
+    # reference's LINEAR_SOLVER_NS_TRESHOLDS MAX_ITER=10), FP64, host-driven iterations
+    jb = solver.JoeGpu(g, dataclasses.replace(prm, LINEAR_SOLVER_NS="BCGSTAB", LS_MAX_ITER=SWEEPS), precision=0)
+    jb.set_state(*st0)
+    jb.runBackwardEuler(max(args.warmup, 3))
+    nb = max(5, min(args.steps, 50))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    jb.runBackwardEuler(nb)
+    torch.cuda.synchronize()
+    bcg_s = time.perf_counter() - t0
+    jb.close()
+    bicgstab = {"value": g.ncv * nb / bcg_s, "unit": "cell-iters/s", "steps": nb,
+                "linear_solver": "BCGSTAB MAX_ITER=%d (the reference arm's solver), FP64" % SWEEPS,
+                "timing": "wall clock around synchronised host-driven steps"}
+
+    conv = converge_leg(conv_cases, args) if conv_cases else None
+    if world > 1 and conv is not None:
+        allc = [None] * world
+        dist.all_gather_object(allc, conv)
+        conv["solves_per_hour"] = sum(c["solves_per_hour"] for c in allc)
+        conv["ratio_vs_plain_fp64"] = conv["solves_per_hour"] / max(
+            1e-300, sum(c["plain_fp64"]["solves_per_hour"] for c in allc))
+        conv["replicas"] = world
+    clk = clocks.stop()
+    if clk is not None:
+        clk["window"] = "the timed steps, the e2e, BiCGSTAB and time-to-converge legs"
+
     # roofline of the dominant kernel, from the live in-graph events
     face_b, sweep_b, f_int, m_blk = algorithmic_bytes(g, args.precision)
     peak, peak_kind = measured_peaks()
@@ -293,14 +357,17 @@ def main():
     sweep_avg = solve_avg / SWEEPS
     sweep_gbs = sweep_b * n / (sweep_avg * 1e-3) / 1e9
     face_gbs = face_b * n / (face_avg * 1e-3) / 1e9
+    split = tuned_cl >= 32
+    face_name = ("face loop: k_res (residual, %d lanes per cell) beside k_jac (Jacobian blocks) on a second stream"
+                 % (tuned_cl - 32) if split else "k_flux (fused face loop + Jacobian assembly)")
     if solve_avg >= face_avg:
         dom = {"kernel": "k_jacobi (block point-relaxation sweep)", "bound": "hbm", "achieved": sweep_gbs,
                "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak, "traffic": None,
                "bytes_per_cell": sweep_b, "launch_ms": sweep_avg}
-        other = {"kernel": "k_flux (face loop + Jacobian assembly)", "achieved": face_gbs, "frac": face_gbs / peak,
+        other = {"kernel": face_name, "achieved": face_gbs, "frac": face_gbs / peak,
                  "bytes_per_cell": face_b, "launch_ms": face_avg}
     else:
-        dom = {"kernel": "k_flux (face loop + Jacobian assembly)", "bound": "hbm", "achieved": face_gbs,
+        dom = {"kernel": face_name, "bound": "hbm", "achieved": face_gbs,
                "peak": peak, "unit": "GB/s", "frac": face_gbs / peak, "traffic": None,
                "bytes_per_cell": face_b, "launch_ms": face_avg}
         other = {"kernel": "k_jacobi (block point-relaxation sweep)", "achieved": sweep_gbs, "frac": sweep_gbs / peak,
@@ -310,10 +377,10 @@ def main():
     if os.path.exists(prof_path):
         with open(prof_path) as f:
             tr = json.load(f)
-        key = "k_jacobi" if dom["kernel"].startswith("k_jacobi") else "k_flux"
+        key = "k_jacobi" if dom["kernel"].startswith("k_jacobi") else "face_loop"
         if key in tr and args.precision in tr[key]:
             entry = tr[key][args.precision]
-            if key == "k_flux":  # per launch shape: lanes per cell
+            if key == "face_loop":  # per launch shape
                 entry = entry.get(str(tuned_cl))
             if entry:
                 dom["traffic"] = entry["bytes_per_cell"] * n
@@ -336,15 +403,19 @@ def main():
                 "config": {"workload": WORKLOAD, "cells": n, "internal_faces_per_cell": round(f_int, 4),
                            "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": "replicas" if world > 1 else "single case",
-                           "launch_shape": {"face_loop": ("1 lane per cell, 3 blocks per SM" if tuned_cl == 17
-                                                          else "%d lanes per cell" % tuned_cl),
-                                            "sweep_kernel": tuned_sweep}},
+                           "launch_shape": {"face_loop": (("split: residual %d lanes per cell + Jacobian kernel"
+                                                           % (tuned_cl - 32)) if split else
+                                                          "fused, 1 lane per cell, 3 blocks per SM" if tuned_cl == 17
+                                                          else "fused, %d lanes per cell" % tuned_cl),
+                                            "code": tuned_cl, "sweep_kernel": tuned_sweep}},
                 "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": 5 * 8 * n,
                         "d2h_bytes_per_step": 5 * 8 * n + 40},
                 "gpu_launches": kernels_per_step * args.steps,
                 "roofline": dom, "roofline_other": other,
                 "face_loop_ms": face_avg, "relaxation_ms": solve_avg,
                 "finite_residual": finite,
+                "bicgstab_like_for_like": bicgstab,
+                "time_to_converge": conv,
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     j.close()

@@ -126,6 +126,13 @@ typedef struct jg_params {
   int shock_fix;       /* SHOCK_FIX_TYPE: JG_SHOCK_FIX_* */
   int shock_flag;      /* SHOCK_FIX_FLAG: JG_SHOCK_FLAG_* */
   int entropy_fix;     /* ENTROPY_FIX EXPANSION_FAN: 1, NONE: 0 */
+  /* Lagged Jacobian (no reference counterpart; the reference forms the blocks every
+   * step): 0 or 1 forms the flux Jacobian blocks every step; k > 1 forms them every
+   * k-th step of each case (and at its first step after a new state), adding each
+   * step's own vol/dt to the kept diagonal.  The residual and the update are exact
+   * every step, so the converged field does not depend on it.  Cases without a
+   * turbulence model, captured linear solvers (JACOBI, SGS, LINE, LUSGS). */
+  int jac_lag;
 } jg_params;
 /* AUSMDV (Wada & Liou, calcEulerFlux_AUSMDV / calcEulerFluxMatrices_AUSMDV,
  * UgpWithCvCompFlow.cpp:879-1322): the AUSMD / AUSMV blend, the entropy fix for
@@ -157,7 +164,10 @@ enum { JG_GRAD_LSQ = 0, JG_GRAD_GREENGAUSS = 1, JG_GRAD_SDWLS = 2 };
  * order (cells, faces and nbocv entries), so only the speed changes.  Block
  * Jacobi steps and calcRhs give bit-identical results either way; the L1
  * residual sum and the Gauss-Seidel colouring follow the internal order. */
-enum { JG_RENUMBER_NONE = 0, JG_RENUMBER_RCM = 1 };
+/* JG_RENUMBER_RCM_COLOR: the RCM order grouped by Gauss-Seidel colour, so that each colour
+ * pass of the SGS relaxation reads a contiguous part of the matrix; the same colour classes,
+ * so SGS gives the same bits as with JG_RENUMBER_RCM. */
+enum { JG_RENUMBER_NONE = 0, JG_RENUMBER_RCM = 1, JG_RENUMBER_RCM_COLOR = 2 };
 /* turbulence models, with the reference's default constants:
  *   JG_TURB_SA  Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h): nscal 1, nuSA (1e-10 .. 1)
  *   JG_TURB_SST Menter k-omega SST (TurbModel_KOMSST.h): nscal 2, kine (1e-10 .. 1e10) and
@@ -300,20 +310,26 @@ int jg_batch_status(jg_case_t *h, int *status);
 /* freeze (0) or resume (1) a case: a frozen case keeps its state (retired) */
 int jg_batch_set_active(jg_case_t *h, int case_id, int active);
 
-/* Launch shapes (no reference counterpart): the lanes per cell of the 5x5
- * face loop (flux_cl = 1, 2 or 4, with registers for two 128-thread blocks
- * per SM; default 1; or JG_FLUX_CL1_3BLK: one lane, registers capped for three
- * blocks per SM, more warps to hide FP64 latency at the price of some spills)
- * and the kernel of the 5x5 Jacobi sweep (0: a block per 32-cell slice, a
- * thread per block row, the default; 1: a thread per cell).  jg_autotune
- * times each candidate on the handle's own mesh (trials launches, CUDA
- * events) and keeps the fastest; ms[6] (may be NULL) gets the face loop time
- * per launch for 1, 2, 4 lanes (ms[0..2]), the sweep time for kernels 0, 1
- * (ms[3..4]) and the face loop time for JG_FLUX_CL1_3BLK (ms[5]).  The sweep kernels give bit-identical results; the lanes per
- * cell change the order of each cell's diagonal-block and residual sums
+/* Launch shapes (no reference counterpart).  The 5x5 face loop runs either
+ * fused -- residual and Jacobian blocks in one kernel, flux_cl = 1, 2 or 4
+ * lanes per cell with registers for two 128-thread blocks per SM, or
+ * JG_FLUX_CL1_3BLK: one lane, registers capped for three blocks per SM -- or
+ * split (flux_cl = JG_FLUX_SPLIT + FL, FL = 1, 2, 4 or 8; the default is
+ * JG_FLUX_SPLIT + 4): a residual kernel with FL lanes per cell and a Jacobian
+ * kernel (one thread per cell, the face matrices formed row by row) on two
+ * streams.  Second: the kernel of the 5x5 Jacobi sweep (0: a block per 32-cell
+ * slice, a thread per block row, the default; 1: a thread per cell).
+ * jg_autotune times each candidate on the handle's own mesh (trials launches,
+ * CUDA events) and keeps the fastest; ms[10] (may be NULL) gets the face loop
+ * time per launch: fused 1, 2, 4 lanes (ms[0..2]), fused JG_FLUX_CL1_3BLK
+ * (ms[5]), split FL = 1, 2, 4, 8 (ms[6..9]); and the sweep time for kernels 0,
+ * 1 (ms[3..4]).  A handle with a lagged Jacobian (jac_lag > 1) runs split
+ * shapes only.  The sweep kernels give bit-identical results; the face-loop
+ * shapes change the order of each cell's diagonal-block and residual sums
  * (rounding-level differences).  Handles without a turbulence model; others
  * keep their single shape.  A batch handle tunes for all its cases. */
 #define JG_FLUX_CL1_3BLK 17
+#define JG_FLUX_SPLIT 32
 int jg_set_launch_config(jg_case_t *h, int flux_cl, int relax_variant);
 int jg_get_launch_config(jg_case_t *h, int *flux_cl, int *relax_variant);
 int jg_autotune(jg_case_t *h, int trials, int *flux_cl, int *relax_variant, float *ms);

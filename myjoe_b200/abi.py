@@ -45,7 +45,8 @@ class jg_params(C.Structure):
                 ("ls_abs", C.c_double), ("ls_rel", C.c_double),
                 ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int),
                 ("grad_scheme", C.c_int),
-                ("ausm_type", C.c_int), ("shock_fix", C.c_int), ("shock_flag", C.c_int), ("entropy_fix", C.c_int)]
+                ("ausm_type", C.c_int), ("shock_fix", C.c_int), ("shock_flag", C.c_int), ("entropy_fix", C.c_int),
+                ("jac_lag", C.c_int)]
 
 
 class jg_serve_config(C.Structure):
@@ -72,8 +73,10 @@ def iptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int))
 
 
-def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_params:
+def make_params(p: JoeParams, precision: int = 0, renumber: bool = False, jac_lag: int = 1) -> jg_params:
+    """jac_lag: form the flux Jacobian blocks every jac_lag-th step (1: every step, as the reference)"""
     q = jg_params()
+    q.jac_lag = int(jac_lag)
     q.gamma = p.GAMMA
     q.R_gas = p.R_gas
     q.Pr = p.PR
@@ -108,7 +111,7 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False) -> jg_
     q.precision = precision
     q.nscal = p.nscal
     q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
-    q.renumber = 1 if renumber else 0
+    q.renumber = int(renumber)   # False/True: none/RCM; 2: RCM grouped by Gauss-Seidel colour
     q.grad_scheme = {"LEASTSQUARES": 0, "GREENGAUSS": 1, "SDWLS": 2}[p.GRAD_SCHEME]
     if q.grad_scheme == 2:
         q.limiter = 0   # SDWLS applies no limiter (limiterNavierS = 0, UgpWithCvCompFlow.h:275-280)

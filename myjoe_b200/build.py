@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libjoe_b200.so")
-SOURCES = ["jg_kernels.cu", "jg_api.cu", "jg_noalloc.cu", "jg_serve.cu", "jg_coupled.cu", "jg_renumber.cu", "jg_linelet.cu", "jg_restart.cu"]
+SOURCES = ["jg_kernels.cu", "jg_faceloop.cu", "jg_fused.cu", "jg_api.cu", "jg_noalloc.cu", "jg_serve.cu", "jg_coupled.cu", "jg_renumber.cu", "jg_linelet.cu", "jg_restart.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 

@@ -241,7 +241,7 @@ static Params make_params(const jg_params& q) {
   p.under_relax = q.under_relax;
   p.viscous = q.mu_ref > 0.0;
   p.fp32 = q.precision == JG_PREC_MIXED;
-  p.flux_cl = 1;
+  p.flux_cl = JG_FLUX_SPLIT + 4;  // the split face loop, 4 lanes per cell in the residual
   p.relax_variant = 0;
   p.grad_scheme = q.grad_scheme;
   p.ausm_type = q.ausm_type;
@@ -285,9 +285,14 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "Green-Gauss and SDWLS gradients: cases without a turbulence model");
   if (q->grad_scheme == JG_GRAD_SDWLS && q->limiter)
     return set_err(JG_ERR_ARG, "SDWLS gradients take no limiter (limiter = 0)");
-  if (q->renumber != JG_RENUMBER_NONE && q->renumber != JG_RENUMBER_RCM)
+  if (q->renumber != JG_RENUMBER_NONE && q->renumber != JG_RENUMBER_RCM && q->renumber != JG_RENUMBER_RCM_COLOR)
     return set_err(JG_ERR_ARG, "unsupported renumbering %d", q->renumber);
   if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");
+  if (q->jac_lag < 0) return set_err(JG_ERR_ARG, "bad Jacobian lag %d", q->jac_lag);
+  if (q->jac_lag > 1 && q->turb_model != JG_TURB_NONE)
+    return set_err(JG_ERR_ARG, "a lagged Jacobian: cases without a turbulence model");
+  if (q->jac_lag > 1 && (q->lin_solver == JG_LS_BCGSTAB || q->lin_solver == JG_LS_BCGSTAB_LINELET))
+    return set_err(JG_ERR_ARG, "a lagged Jacobian: captured linear solvers (JACOBI, SGS, LINE, LUSGS)");
   return JG_OK;
 }
 
@@ -321,14 +326,72 @@ int jg_destroy(jg_case_t* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : h->allocs) cudaFree(p);
   }
+  if (h->st.aux) cudaStreamSynchronize(h->st.aux);
   if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->st.aux) cudaStreamDestroy(h->st.aux);
+  if (h->st.ev_fork) cudaEventDestroy(h->st.ev_fork);
+  if (h->st.ev_join) cudaEventDestroy(h->st.ev_join);
   delete h;
   return JG_OK;
+}
+
+// Greedy colouring of the cell graph (neighbours through internal faces) in cell order: each cell
+// takes the smallest colour none of its lower-numbered neighbours has.  With at most
+// MAX_COLOR_LISTS colours, also the slices holding a cell of each colour, colour by colour
+// (cslices[coff[q] .. coff[q+1])).  Returns the number of colours.
+static int color_cells(const jg_mesh* mesh, std::vector<uint8_t>& color, std::vector<int>& cslices,
+                       std::vector<int>& coff) {
+  const int N = mesh->ncv;
+  std::vector<int> adj_i(N + 1, 0), adj_v;
+  for (int f = mesh->nfa_b; f < mesh->nfa; f++) {
+    adj_i[mesh->cvofa[2 * f] + 1]++;
+    adj_i[mesh->cvofa[2 * f + 1] + 1]++;
+  }
+  for (int c = 0; c < N; c++) adj_i[c + 1] += adj_i[c];
+  adj_v.resize(adj_i[N]);
+  {
+    std::vector<int> fill(adj_i.begin(), adj_i.end() - 1);
+    for (int f = mesh->nfa_b; f < mesh->nfa; f++) {
+      const int a = mesh->cvofa[2 * f], b = mesh->cvofa[2 * f + 1];
+      adj_v[fill[a]++] = b;
+      adj_v[fill[b]++] = a;
+    }
+  }
+  color.assign(N, 0);
+  int ncolors = 1;
+  std::vector<int> mark(256, -1);
+  for (int c = 0; c < N; c++) {
+    for (int k = adj_i[c]; k < adj_i[c + 1]; k++)
+      if (adj_v[k] < c) mark[color[adj_v[k]]] = c;
+    int k = 0;
+    while (k < 255 && mark[k] == c) k++;
+    color[c] = (uint8_t)k;
+    ncolors = std::max(ncolors, k + 1);
+  }
+  cslices.clear();
+  coff.assign(1, 0);
+  if (ncolors <= MAX_COLOR_LISTS) {
+    const int nslices = (N + SLICE - 1) / SLICE;
+    std::vector<uint32_t> has(nslices, 0);  // bit q: the slice holds a cell of colour q
+    for (int c = 0; c < N; c++) has[c / SLICE] |= 1u << color[c];
+    for (int q = 0; q < ncolors; q++) {
+      for (int sl = 0; sl < nslices; sl++)
+        if (has[sl] & (1u << q)) cslices.push_back(sl);
+      coff.push_back((int)cslices.size());
+    }
+  }
+  return ncolors;
 }
 
 static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   const int N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b;
   if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (q->turb_model == JG_TURB_NONE && !h->st.aux) {
+    // the face loop's Jacobian kernel runs beside its residual kernel on a second stream
+    CK(cudaStreamCreateWithFlags(&h->st.aux, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->st.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->st.ev_join, cudaEventDisableTiming));
+  }
   h->ncv = N;
   h->nfa = nfa;
   h->nfa_b = nfa_b;
@@ -415,26 +478,19 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     }
   }
   h->ell_elems = (size_t)rows * bs * bs * SLICE;
-  // greedy colouring of the cell graph (neighbours through internal faces), in cell order
-  std::vector<uint8_t> color(N, 0);
-  int ncolors = 1;
-  {
-    std::vector<int> mark(256, -1);
-    for (int c = 0; c < N; c++) {
-      for (int j = h->cell_cols[c]; j < h->cell_cols[c + 1]; j++) {
-        int nb = h->col_nb[j];
-        if (nb < c) mark[color[nb]] = c;
-      }
-      int k = 0;
-      while (k < 255 && mark[k] == c) k++;
-      color[c] = (uint8_t)k;
-      ncolors = std::max(ncolors, k + 1);
-    }
-  }
+  // greedy colouring of the cell graph (neighbours through internal faces), in cell order, and per
+  // colour the slices that hold a cell of that colour (a colour pass launches over these only)
+  std::vector<uint8_t> color;
+  std::vector<int> cslices, coff;
+  const int ncolors = color_cells(mesh, color, cslices, coff);
   h->ncolors = ncolors;
   // device mesh
   Mesh& m = h->m;
   memset(&m, 0, sizeof(m));
+  if (ncolors <= MAX_COLOR_LISTS) {
+    RC(upload(h, &m.color_slices, cslices.data(), cslices.size()));
+    for (int c = 0; c <= ncolors; c++) m.color_slice_off[c] = coff[c];
+  }
   m.ncv = N; m.nfa = nfa; m.nfa_b = nfa_b; m.nzones = mesh->nzones; m.nslices = nslices; m.ell_rows = rows;
   RC(upload(h, &m.x_cv, mesh->x_cv, 3 * (size_t)N));
   RC(upload(h, &m.vol, mesh->cv_volume, (size_t)N));
@@ -494,6 +550,9 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(dmalloc_bytes(h, &st.x1, bs * (size_t)N * h->eltsz));
   RC(dmalloc(h, &st.dq, bs * (size_t)N));
   st.bs = bs;
+  st.jac_lag = bs == 5 ? std::max(q->jac_lag, 1) : 1;
+  st.D0 = nullptr;
+  st.jac_next = nullptr;
   // per-block partials: k_flux2 writes 5 per 16-cell block, k_dt 1 per 256-cell block
   RC(dmalloc(h, &st.blk, 5 * (size_t)grid_for(N, 16) + 5 * (size_t)grid_for(N, 256) + 16));
   RC(dmalloc(h, &st.ctrl, 16));
@@ -527,6 +586,11 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     RC(upload(h, &d, rblk_case.data(), rblk_case.size()));
     h->d_rblk_case = (int*)d;
     RC(dmalloc(h, &st.rpart, bs * (size_t)h->nrblk));
+    if (st.jac_lag > 1) {
+      // the kept face part of the diagonal blocks and each case's next refresh step (0: the next step)
+      RC(dmalloc_bytes(h, &st.D0, bs * bs * (size_t)N * h->eltsz));
+      RC(dmalloc(h, &st.jac_next, (size_t)h->ncases));
+    }
     std::vector<uint8_t> on(h->ncases, 1);
     const uint8_t* da = nullptr;
     RC(upload(h, &da, on.data(), on.size()));
@@ -625,6 +689,19 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   return JG_OK;
 }
 
+// build() on the caller's mesh, or on its renumbered copy (with the device copy of the cell order)
+static int build_case(jg_case* h, const jg_mesh* mesh, const jg_params* params) {
+  if (params->renumber == JG_RENUMBER_NONE) return build(h, mesh, params);
+  MeshOwned mo;
+  RC(renumber_mesh(*mesh, params->renumber, mo, h->rn));
+  RC(build(h, &mo.m, params));
+  const int* d = nullptr;
+  RC(upload(h, &d, h->rn.cell_old.data(), h->rn.cell_old.size()));
+  h->d_cell_old = (int*)d;
+  CK(cudaStreamSynchronize(h->stream));  // the renumbered host arrays go out of scope
+  return JG_OK;
+}
+
 int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
   if (!mesh || !out) return set_err(JG_ERR_ARG, "null argument");
   *out = nullptr;
@@ -634,23 +711,7 @@ int jg_create(const jg_mesh* mesh, const jg_params* params, jg_case_t** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
   jg_case* h = new jg_case();
-  int rc = JG_OK;
-  if (params->renumber == JG_RENUMBER_RCM) {
-    MeshOwned mo;
-    rc = renumber_mesh(*mesh, params->renumber, mo, h->rn);
-    if (rc == JG_OK) rc = build(h, &mo.m, params);
-    if (rc == JG_OK) {
-      const int* d = nullptr;
-      rc = upload(h, &d, h->rn.cell_old.data(), h->rn.cell_old.size());
-      h->d_cell_old = (int*)d;
-    }
-    if (rc == JG_OK) {
-      cudaError_t e = cudaStreamSynchronize(h->stream);  // the renumbered host arrays go out of scope
-      if (e != cudaSuccess) rc = set_err(JG_ERR_CUDA, "%s", cudaGetErrorString(e));
-    }
-  } else {
-    rc = build(h, mesh, params);
-  }
+  int rc = build_case(h, mesh, params);
   if (rc != JG_OK) {
     std::string keep = g_err;
     jg_destroy(h);
@@ -701,9 +762,18 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
   size_t b = 0;
   for (size_t x : a)
     if (x) b += alloc_round(x);
+  {
+    // the per-colour slice lists
+    std::vector<uint8_t> color;
+    std::vector<int> cslices, coff;
+    if (color_cells(mesh, color, cslices, coff) <= MAX_COLOR_LISTS)
+      b += alloc_round(std::max<size_t>(cslices.size(), 1) * i);
+  }
   // AUSMDV shock flags; JST coefficients and BoundaryCV
   if (q->flux == JG_FLUX_AUSMDV && q->shock_fix != JG_SHOCK_FIX_NONE) b += alloc_round(N);
   if (q->flux == JG_FLUX_JST) b += alloc_round(8 * N * d) + alloc_round(N);
+  // lagged Jacobian: the kept diagonal face part and the refresh step of the case
+  if (bs == 5 && q->jac_lag > 1) b += alloc_round(b2 * N * e) + alloc_round(sizeof(long long));
   if (bs > 5) {
     // model arrays: phi, phi_bfa, grad_phi, diff (per scalar), wall distance, strain, vorticity
     // (+ divergence, cross-diffusion, F1, F2 for SST), mut_fa, the wall faces
@@ -734,7 +804,7 @@ extern "C" int jg_case_footprint(const jg_mesh* mesh, const jg_params* params, d
   RC(check_params(params));
   if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
     return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
-  if (params->renumber == JG_RENUMBER_RCM) {
+  if (params->renumber != JG_RENUMBER_NONE) {
     // the sliced-ELL padding follows the renumbered order; plus the device copy of the cell order
     MeshOwned mo;
     Renumbering rn;
@@ -952,6 +1022,8 @@ static int check_err_flags(jg_case* h, bool all_cases = false) {
 // calcStateVariables + calcMaterialProperties + setBC (+ mut = 0), the
 // runBackwardEuler preamble (JoeWithModels.cpp:942-957)
 static int prime(jg_case* h) {
+  // a new state: every case forms its Jacobian blocks at its next step
+  if (h->st.jac_next) CK(cudaMemsetAsync(h->st.jac_next, 0, sizeof(long long) * h->ncases, h->stream));
   launch_state(h->m, h->p, h->st, h->stream);
   launch_face_props(h->m, h->p, h->st, h->stream);
   launch_bc(h->m, h->p, h->st, h->stream);
@@ -1638,12 +1710,11 @@ int serve_case_create(const jg_mesh* mesh, const jg_params* params, jg_case** ou
       params->lin_solver == JG_LS_LINE)
     return set_err(JG_ERR_ARG, "served cases relax with JACOBI, SGS or LUSGS (captured steps)");
   if (params->turb_model != JG_TURB_NONE) return set_err(JG_ERR_ARG, "served cases are laminar / inviscid");
-  if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "served cases keep their own order");
   if (mesh->ncv <= 0 || mesh->nfa < mesh->nfa_b || mesh->nfa_b < 0 || mesh->nbocv_s < mesh->ncv)
     return set_err(JG_ERR_ARG, "inconsistent mesh sizes");
   jg_case* h = new jg_case();
   h->async_alloc = 1;
-  int rc = build(h, mesh, params);
+  int rc = build_case(h, mesh, params);
   if (rc == JG_OK) rc = dmalloc(h, &h->d_io, 5 * (size_t)mesh->ncv);
   if (rc != JG_OK) {
     std::string keep = g_err;
@@ -1661,7 +1732,8 @@ int serve_case_start(jg_case* h, const double* rho, const double* rhou, const do
   CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  launch_pack_state((int)N, h->d_io, h->st.q, nullptr, h->stream);
+  launch_pack_state((int)N, h->d_io, h->st.q, h->d_cell_old, h->stream);
+  if (h->st.jac_next) CK(cudaMemsetAsync(h->st.jac_next, 0, sizeof(long long) * h->ncases, h->stream));
   launch_state(h->m, h->p, h->st, h->stream);
   launch_face_props(h->m, h->p, h->st, h->stream);
   launch_bc(h->m, h->p, h->st, h->stream);
@@ -1742,8 +1814,11 @@ static void drop_graph(jg_case* h) {
 
 extern "C" int jg_set_launch_config(jg_case_t* h, int flux_cl, int relax_variant) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
-  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4 && flux_cl != JG_FLUX_CL1_3BLK)
-    return set_err(JG_ERR_ARG, "face loop shape must be 1, 2, 4 lanes per cell or JG_FLUX_CL1_3BLK");
+  const bool split = flux_cl == JG_FLUX_SPLIT + 1 || flux_cl == JG_FLUX_SPLIT + 2 || flux_cl == JG_FLUX_SPLIT + 4 ||
+                     flux_cl == JG_FLUX_SPLIT + 8;
+  if (flux_cl != 1 && flux_cl != 2 && flux_cl != 4 && flux_cl != JG_FLUX_CL1_3BLK && !split)
+    return set_err(JG_ERR_ARG, "face loop shape must be 1, 2, 4 lanes per cell, JG_FLUX_CL1_3BLK or "
+                               "JG_FLUX_SPLIT + 1, 2, 4 or 8");
   if (relax_variant != 0 && relax_variant != 1) return set_err(JG_ERR_ARG, "sweep kernel must be 0 or 1");
   CK(cudaStreamSynchronize(h->stream));
   h->p.flux_cl = flux_cl;
@@ -1774,16 +1849,25 @@ extern "C" int jg_autotune(jg_case_t* h, int trials, int* flux_cl, int* relax_va
     launch_dt(h->m, h->p, h->st, 1, 0.0, S);
     launch_grad(h->m, h->p, h->st, S);
     Params p = h->p;
-    // ms[0..2]: 1, 2, 4 lanes per cell; ms[5]: one lane with three blocks per SM
-    const int cls[4] = {1, 2, 4, JG_FLUX_CL1_3BLK};
-    const int slot[4] = {0, 1, 2, 5};
+    // every shape is timed forming the whole Jacobian (a lag schedule would skip it)
+    State st = h->st;
+    st.jac_lag = 1;
+    // ms[0..2]: fused, 1, 2, 4 lanes per cell; ms[5]: fused, one lane with three blocks per SM;
+    // ms[6..9]: split, residual with 1, 2, 4, 8 lanes per cell.  A lagged handle runs split.
+    const int cls[8] = {1, 2, 4, JG_FLUX_CL1_3BLK, JG_FLUX_SPLIT + 1, JG_FLUX_SPLIT + 2, JG_FLUX_SPLIT + 4,
+                        JG_FLUX_SPLIT + 8};
+    const int slot[8] = {0, 1, 2, 5, 6, 7, 8, 9};
     float best = 1e30f;
     int best_cl = h->p.flux_cl, best_v = h->p.relax_variant;
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < 8; i++) {
+      if (h->st.jac_lag > 1 && cls[i] < JG_FLUX_SPLIT) {
+        if (ms) ms[slot[i]] = 0.0f;
+        continue;
+      }
       p.flux_cl = cls[i];
-      launch_flux(h->m, p, h->st, 1, 1, S);  // warm-up
+      launch_flux(h->m, p, st, 1, 1, S);  // warm-up
       CK(cudaEventRecord(e0, S));
-      for (int t = 0; t < trials; t++) launch_flux(h->m, p, h->st, 1, 1, S);
+      for (int t = 0; t < trials; t++) launch_flux(h->m, p, st, 1, 1, S);
       CK(cudaEventRecord(e1, S));
       CK(cudaEventSynchronize(e1));
       float t_ms = 0.0f;
@@ -1899,7 +1983,7 @@ extern "C" int jg_set_params(jg_case_t* h, const jg_params* q) {
       q->symm_bc != o.symm_bc || q->lin_solver != o.lin_solver || q->precision != o.precision ||
       q->nscal != o.nscal || q->turb_model != o.turb_model || q->renumber != o.renumber ||
       q->grad_scheme != o.grad_scheme || q->ausm_type != o.ausm_type || q->shock_fix != o.shock_fix ||
-      q->shock_flag != o.shock_flag || q->entropy_fix != o.entropy_fix)
+      q->shock_flag != o.shock_flag || q->entropy_fix != o.entropy_fix || std::max(q->jac_lag, 1) != std::max(o.jac_lag, 1))
     return set_err(JG_ERR_ARG, "jg_set_params changes run-time settings only (CFL, DT, ramp, under-relaxation, "
                                "solver thresholds and sweeps, EPS, time-step mode)");
   // a batch keeps the promise jg_batch_create makes: no setting that couples its cases

@@ -1,0 +1,133 @@
+// jg_cell.cuh -- per-cell and per-face helpers shared by the face-loop kernels:
+// face normals, cell-centre states, second-order reconstruction, the viscous
+// side state, the sliced-ELL index of an off-diagonal block entry, the 5x5
+// block inverse and the AUSMDV face options.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "jg_flux.cuh"
+#include "jg_internal.h"
+
+namespace jg {
+
+__device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
+  double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
+  area = sqrt(dot3(n, n));
+  for (int i = 0; i < 3; i++) nV[i] = n[i] / area;
+}
+
+__device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, int c) {
+  FState s;
+  s.rho = st.q[5 * c];
+  for (int i = 0; i < 3; i++) s.u[i] = st.prim[8 * c + i];
+  s.p = st.prim[8 * c + 3];
+  s.gam = p.gamma;
+  s.h = st.prim[8 * c + 5];
+  return s;
+}
+
+// second-order reconstruction at x_fa with the first-order fallback, JoeWithModels.cpp:2832-2921
+__device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const State& st, int c, int f) {
+  FState s = cell_fstate(p, st, c);
+  if (!p.second_order) return s;
+  double r0[3];
+  for (int i = 0; i < 3; i++) r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+  double rr = s.rho + dot3(r0, &st.grho[3 * c]);
+  double pp = s.p + dot3(r0, &st.gp[3 * c]);
+  if ((pp <= 0.0) || (rr <= 0.0)) return s;  // first order: the cell's own h is calcThermoProp_p of (p, rho)
+  s.rho = rr;
+  s.p = pp;
+  for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
+  const double T = pp / (rr * p.R);  // calcThermoProp_p at the face
+  s.h = p.gamma * p.R / (p.gamma - 1.0) * T;
+  return s;
+}
+
+__device__ __forceinline__ VSide cell_vside(const Params& p, const State& st, int c) {
+  VSide v;
+  v.rho = st.q[5 * c];
+  for (int i = 0; i < 3; i++) v.u[i] = st.prim[8 * c + i];
+  v.h = st.prim[8 * c + 5];
+  v.T = st.prim[8 * c + 4];
+  v.R = p.R;
+  v.gam = p.gamma;
+  v.gu = &st.guv[9 * c];
+  v.gh = &st.gh[3 * c];
+  return v;
+}
+
+template <typename BT>
+__device__ __forceinline__ size_t ell_index(const Mesh& m, int c, int col, int e) {
+  int slice = c / SLICE, lane = c % SLICE;
+  return ((size_t)(m.ell_off[slice] + col) * 25 + e) * SLICE + lane;
+}
+
+// 5x5 LU without pivoting + inverse, ludeco / luinv (UgpWithCv.cpp:2489-2577); the loops have
+// constant bounds so that they unroll and both blocks stay in registers
+__device__ __forceinline__ void block_inverse(double* A, double* Ai) {
+#pragma unroll
+  for (int jc = 1; jc < 5; jc++) A[jc] /= A[0];
+#pragma unroll
+  for (int jrjc = 1; jrjc < 5; jrjc++) {
+#pragma unroll
+    for (int jr = jrjc; jr < 5; jr++) {
+      double sum = A[5 * jr + jrjc];
+#pragma unroll
+      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jr + jm] * A[5 * jm + jrjc];
+      A[5 * jr + jrjc] = sum;
+    }
+    if (jrjc < 4) {
+#pragma unroll
+      for (int jc = jrjc + 1; jc < 5; jc++) {
+        double sum = A[5 * jrjc + jc];
+#pragma unroll
+        for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jrjc + jm] * A[5 * jm + jc];
+        A[5 * jrjc + jc] = sum / A[5 * jrjc + jrjc];
+      }
+    }
+  }
+#pragma unroll
+  for (int col = 0; col < 5; col++) {
+    double cv[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) cv[i] = (i == col) ? 1.0 : 0.0;
+    cv[0] = cv[0] / A[0];
+#pragma unroll
+    for (int jr = 1; jr < 5; jr++) {
+      double sum = cv[jr];
+#pragma unroll
+      for (int jm = 0; jm < jr; jm++) sum -= A[5 * jr + jm] * cv[jm];
+      cv[jr] = sum / A[5 * jr + jr];
+    }
+#pragma unroll
+    for (int jr = 3; jr >= 0; jr--) {
+      double sum = cv[jr];
+#pragma unroll
+      for (int jm = jr + 1; jm < 5; jm++) sum -= A[5 * jr + jm] * cv[jm];
+      cv[jr] = sum;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) Ai[5 * i + col] = cv[i];
+  }
+}
+
+// the AUSMDV options of an internal face (JoeWithModels.cpp:2933-2957): the shock fix where the
+// cells' flags add up past the threshold, sonic faces included (SHOCKFIX_ACROSS_SHOCK is defined,
+// JoeWithModels.cpp:4)
+template <int KIND>
+__device__ __forceinline__ int face_opts(const Params& p, const State& st, int c0, int c1) {
+  if (KIND != 4) return 0;
+  int fo = p.ausm_type | (p.entropy_fix ? FO_EFIX : 0);
+  if (p.shock_fix != JG_SHOCK_FIX_NONE && double(st.shock_flag[c0]) + double(st.shock_flag[c1]) > p.shock_flag_sum)
+    fo |= p.shock_fix == JG_SHOCK_FIX_HAENEL ? FO_HAENEL : FO_ALPHA_LR;
+  return fo;
+}
+
+// boundary faces: AUSMDV without the shock fix (JoeWithModels.cpp:3149-3153)
+template <int KIND>
+__device__ __forceinline__ int bnd_opts(const Params& p) {
+  return KIND == 4 ? (p.ausm_type | (p.entropy_fix ? FO_EFIX : 0)) : 0;
+}
+
+}  // namespace jg

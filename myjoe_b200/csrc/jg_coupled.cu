@@ -1040,10 +1040,11 @@ __global__ void __launch_bounds__(B * 32) k_jacobi_c(Mesh m, State st, const BT*
 }
 
 template <typename BT, int B>
-__global__ void __launch_bounds__(B * 32) k_gs_c(Mesh m, State st, BT* __restrict__ x, int color) {
+__global__ void __launch_bounds__(B * 32) k_gs_c(Mesh m, State st, BT* __restrict__ x, int color,
+                                                 const int* __restrict__ slices) {
   __shared__ BT sacc[B][SLICE];
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
-  const int slice = blockIdx.x;
+  const int slice = slices ? slices[blockIdx.x] : blockIdx.x;  // slices: those holding this colour
   const int c = slice * SLICE + lane;
   const bool active = c < m.ncv && m.color[c] == color;
   const int N = m.ncv;
@@ -1132,7 +1133,10 @@ static void relax_c(const Mesh& m, State& st, int sgs, int sweeps, cudaStream_t 
     for (int it = 0; it < sweeps; it++)
       for (int q = 0; q < m.ncolors; q++) {
         int col = (it % 2 == 0) ? q : m.ncolors - 1 - q;
-        k_gs_c<BT, B><<<m.nslices, B * SLICE, 0, s>>>(m, st, (BT*)st.x0, col);
+        const bool lists = m.color_slices != nullptr;
+        const int* sl = lists ? m.color_slices + m.color_slice_off[col] : nullptr;
+        const int g = lists ? m.color_slice_off[col + 1] - m.color_slice_off[col] : m.nslices;
+        if (g > 0) k_gs_c<BT, B><<<g, B * SLICE, 0, s>>>(m, st, (BT*)st.x0, col, sl);
       }
   } else {
     for (int it = 0; it < sweeps; it++) {

@@ -18,6 +18,7 @@
 namespace jg {
 
 constexpr int SLICE = 32;
+constexpr int MAX_COLOR_LISTS = 16;
 
 struct DevZone {
   int kind;
@@ -55,6 +56,11 @@ struct Mesh {
   int ell_rows;
   const uint8_t* color;    // [N] colour of the cell (no two neighbours share one)
   int ncolors;
+  // per colour q (q < MAX_COLOR_LISTS): the slices holding a cell of that colour are
+  // color_slices[color_slice_off[q] .. color_slice_off[q+1]) (host-side offsets; no lists when
+  // ncolors > MAX_COLOR_LISTS: every colour pass covers every slice)
+  const int* color_slices;
+  int color_slice_off[17];
   const int* case_of;      // [N] case of each cell (batches)
 };
 
@@ -94,6 +100,15 @@ struct State {
   double* mut_fa;   // [nfa] turbulent viscosity (coupled path), nullptr without a model
   const double* kine;  // [N] turbulent kinetic energy in the pressure recovery (SST), nullptr otherwise
   int bs;           // block size of the system: 5, or 6 with SA (rhs, b, dq, x, D, O, resid use it)
+  // lagged Jacobian (jac_lag > 1, 5x5 path): the flux blocks of case k are formed again at the
+  // step jac_next[k] (0: at the next step) and kept in between; D0 holds the face part of the
+  // diagonal block ([25][N], matrix precision) to which each step adds its own vol/dt
+  int jac_lag;
+  void* D0;
+  long long* jac_next;   // [ncases]
+  // the face loop's residual and Jacobian kernels run on two streams (host-side only)
+  cudaStream_t aux;
+  cudaEvent_t ev_fork, ev_join;
 };
 
 // Transported scalars and turbulence-model arrays (coupled path only).
@@ -133,9 +148,10 @@ struct Params {
   int viscous;      // mu_ref > 0
   int fp32;         // matrix + relaxation in FP32
   int turb;         // JG_TURB_*
-  // launch shapes (jg_autotune / jg_set_launch_config): lanes per cell of the 5x5 face loop
-  // (1, 2 or 4), and the 5x5 Jacobi sweep's kernel (0: a block per 32-cell slice with a
-  // thread per block row, 1: a thread per cell)
+  // launch shapes (jg_autotune / jg_set_launch_config): the 5x5 face loop (fused: 1, 2 or 4
+  // lanes per cell or JG_FLUX_CL1_3BLK; split: JG_FLUX_SPLIT + lanes per cell of the residual
+  // kernel), and the 5x5 Jacobi sweep's kernel (0: a block per 32-cell slice with a thread per
+  // block row, 1: a thread per cell)
   int flux_cl;
   int relax_variant;
   int grad_scheme;  // JG_GRAD_*
@@ -156,7 +172,16 @@ void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_ctrl_step(const Params& p, State& st, cudaStream_t s);
 void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl_cfl, double cfl, cudaStream_t s);
 void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+// the face loop: residual (+ Jacobian blocks when implicit; for_step adds vol/dt, inverts the
+// diagonal and writes the under-relaxed rhs) -- split into a residual and a Jacobian kernel
+// (jg_faceloop.cu) or fused (jg_fused.cu), by p.flux_cl
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
+void launch_flux_fused(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s);
+void launch_face_sensors(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+// face-loop launch shapes: split (residual kernel with FL lanes per cell + Jacobian kernel)
+// are JG_FLUX_SPLIT + FL; the others are the fused kernel's
+inline bool flux_split(const Params& p, const State& st) { return p.flux_cl >= JG_FLUX_SPLIT || st.jac_lag > 1; }
+inline int flux_split_lanes(const Params& p) { return p.flux_cl >= JG_FLUX_SPLIT ? p.flux_cl - JG_FLUX_SPLIT : 4; }
 void launch_resid(const Mesh& m, State& st, int hist_index_from_ctrl, cudaStream_t s);
 // per-case residual history, resid[(idx*ncases + case)*5 + i]
 // per-case L1 residual: RCHUNK-cell chunks counted from each case's first cell
@@ -260,6 +285,7 @@ struct Renumbering {
   std::vector<int> cell_old, face_old, nbs_old;
 };
 int rcm_order(const jg_mesh& m, std::vector<int>& cell_old);
+int rcm_color_order(const jg_mesh& m, std::vector<int>& cell_old);
 int renumber_mesh(const jg_mesh& in, int method, MeshOwned& out, Renumbering& r);
 }  // namespace jg
 

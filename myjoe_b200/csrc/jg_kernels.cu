@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "jg_cell.cuh"
 #include "jg_flux.cuh"
 #include "jg_internal.h"
 
@@ -88,12 +89,6 @@ __global__ void k_face_props(Mesh m, Params p, State st) {
   double mu = mu_law(p, T);
   st.mul_fa[f] = mu;
   st.lam_fa[f] = mu / p.Pr;
-}
-
-__device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
-  double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
-  area = sqrt(dot3(n, n));
-  for (int i = 0; i < 3; i++) nV[i] = n[i] / area;
 }
 
 // setBC + ComputeBCProperties_T/H + the EOS density, JoeWithModels.cpp:3857-4300,
@@ -559,95 +554,6 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
 // ---------------------------------------------------------------------------
 // face loop (calcEulerFlux + calcViscousFluxNS, JoeWithModels.cpp:2621-3855)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, int c) {
-  FState s;
-  s.rho = st.q[5 * c];
-  for (int i = 0; i < 3; i++) s.u[i] = st.prim[8 * c + i];
-  s.p = st.prim[8 * c + 3];
-  s.gam = p.gamma;
-  s.h = st.prim[8 * c + 5];
-  return s;
-}
-
-// second-order reconstruction at x_fa with the first-order fallback, JoeWithModels.cpp:2832-2921
-__device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const State& st, int c, int f) {
-  FState s = cell_fstate(p, st, c);
-  if (!p.second_order) return s;
-  double r0[3];
-  for (int i = 0; i < 3; i++) r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
-  double rr = s.rho + dot3(r0, &st.grho[3 * c]);
-  double pp = s.p + dot3(r0, &st.gp[3 * c]);
-  if ((pp <= 0.0) || (rr <= 0.0)) return s;  // first order: the cell's own h is calcThermoProp_p of (p, rho)
-  s.rho = rr;
-  s.p = pp;
-  for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
-  const double T = pp / (rr * p.R);  // calcThermoProp_p at the face
-  s.h = p.gamma * p.R / (p.gamma - 1.0) * T;
-  return s;
-}
-
-__device__ __forceinline__ VSide cell_vside(const Params& p, const State& st, int c) {
-  VSide v;
-  v.rho = st.q[5 * c];
-  for (int i = 0; i < 3; i++) v.u[i] = st.prim[8 * c + i];
-  v.h = st.prim[8 * c + 5];
-  v.T = st.prim[8 * c + 4];
-  v.R = p.R;
-  v.gam = p.gamma;
-  v.gu = &st.guv[9 * c];
-  v.gh = &st.gh[3 * c];
-  return v;
-}
-
-template <typename BT>
-__device__ __forceinline__ size_t ell_index(const Mesh& m, int c, int col, int e) {
-  int slice = c / SLICE, lane = c % SLICE;
-  return ((size_t)(m.ell_off[slice] + col) * 25 + e) * SLICE + lane;
-}
-
-// 5x5 LU without pivoting + inverse, ludeco / luinv (UgpWithCv.cpp:2489-2577)
-__device__ inline void block_inverse(double* A, double* Ai) {
-  for (int jc = 1; jc < 5; jc++) A[jc] /= A[0];
-  for (int jrjc = 1;; jrjc++) {
-    for (int jr = jrjc; jr < 5; jr++) {
-      double sum = A[5 * jr + jrjc];
-      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jr + jm] * A[5 * jm + jrjc];
-      A[5 * jr + jrjc] = sum;
-    }
-    if (jrjc == 4) break;
-    for (int jc = jrjc + 1; jc < 5; jc++) {
-      double sum = A[5 * jrjc + jc];
-      for (int jm = 0; jm < jrjc; jm++) sum -= A[5 * jrjc + jm] * A[5 * jm + jc];
-      A[5 * jrjc + jc] = sum / A[5 * jrjc + jrjc];
-    }
-  }
-  for (int col = 0; col < 5; col++) {
-    double cv[5];
-    for (int i = 0; i < 5; i++) cv[i] = (i == col) ? 1.0 : 0.0;
-    cv[0] = cv[0] / A[0];
-    for (int jr = 1; jr < 5; jr++) {
-      double sum = cv[jr];
-      for (int jm = 0; jm < jr; jm++) sum -= A[5 * jr + jm] * cv[jm];
-      cv[jr] = sum / A[5 * jr + jr];
-    }
-    for (int jr = 3; jr >= 0; jr--) {
-      double sum = cv[jr];
-      for (int jm = jr + 1; jm < 5; jm++) sum -= A[5 * jr + jm] * cv[jm];
-      cv[jr] = sum;
-    }
-    for (int i = 0; i < 5; i++) Ai[5 * i + col] = cv[i];
-  }
-}
-
-// CL lanes per cell (a launch shape chosen per handle, jg_autotune): lane l
-// of a cell evaluates the cell's face slots l, l+CL, ...; each lane
-// accumulates its own partial diagonal block (shared memory) and residual,
-// summed over the lanes in a fixed order.  More lanes shorten each thread's
-// dependent chain and give the scheduler more warps to spread over the SMs
-// (a small mesh is otherwise a one-and-a-bit-wave grid at the
-// register-limited occupancy); they cost repeated reads of the cell's data.
-// Measured: the viscous Roe plate (49k cells) is 2% faster with two lanes,
-// inviscid HLLC bumps (430k cells) 1.4x faster with one.
 // AUSMDV shock sensor (JoeWithModels.cpp:2753-2781): is internal face f sonic between its
 // cells' centre states, a compression through u_n - c or u_n + c
 __device__ __forceinline__ bool face_sonic(const Mesh& m, const Params& p, const State& st, int f) {
@@ -671,18 +577,6 @@ __global__ void k_shock_flag(Mesh m, Params p, State st) {
     if (s.nb >= 0 && face_sonic(m, p, st, s.f)) flag = 1;
   }
   st.shock_flag[c] = flag;
-}
-
-// the AUSMDV options of an internal face (JoeWithModels.cpp:2933-2957): the shock fix where the
-// cells' flags add up past the threshold, sonic faces included (SHOCKFIX_ACROSS_SHOCK is defined,
-// JoeWithModels.cpp:4)
-template <int KIND>
-__device__ __forceinline__ int face_opts(const Params& p, const State& st, int c0, int c1) {
-  if (KIND != 4) return 0;
-  int fo = p.ausm_type | (p.entropy_fix ? FO_EFIX : 0);
-  if (p.shock_fix != JG_SHOCK_FIX_NONE && double(st.shock_flag[c0]) + double(st.shock_flag[c1]) > p.shock_flag_sum)
-    fo |= p.shock_fix == JG_SHOCK_FIX_HAENEL ? FO_HAENEL : FO_ALPHA_LR;
-  return fo;
 }
 
 // JST coefficients of the current state, calcJSTCoeff_Var (JoeWithModels.cpp:13435-13492), per
@@ -731,312 +625,6 @@ __global__ void k_jst(Mesh m, Params p, State st) {
   J[1] = lam;
   J[2] = (double)nint;
   for (int i = 0; i < 5; i++) J[3 + i] = lap[i];
-}
-
-// boundary faces: AUSMDV without the shock fix (JoeWithModels.cpp:3149-3153)
-template <int KIND>
-__device__ __forceinline__ int bnd_opts(const Params& p) {
-  return KIND == 4 ? (p.ausm_type | (p.entropy_fix ? FO_EFIX : 0)) : 0;
-}
-
-// MINB: resident blocks per SM the register allocation must allow (__launch_bounds__): 2 lets the
-// compiler use all 255 registers; 3 caps it near 168 (some spills to L1-cached local memory) for
-// 12 instead of 8 warps per SM, which hides more FP64 latency on some meshes (jg_autotune decides)
-template <typename BT, int KIND, int VISC, int CL, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, int implicit, int for_step) {
-  // the Jacobian blocks are formed in BT arithmetic: FP64 for the plain form,
-  // FP32 for the mixed form's preconditioner (the residual is FP64 in both)
-  using JT = BT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  JT* sD = reinterpret_cast<JT*>(smem_raw);  // [25][blockDim.x] partial diagonal blocks, one per thread
-  const int t = threadIdx.x, bd = blockDim.x;
-  const int lane = t % CL;
-  int c = blockIdx.x * (bd / CL) + t / CL;
-  bool active = c < m.ncv;
-  double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  if (active) {
-    for (int e = 0; e < 25; e++) sD[e * bd + t] = JT(0);
-    BT* O = (BT*)st.O;
-    for (int k = m.slot_i[c] + lane; k < m.slot_i[c + 1]; k += CL) {
-      const Slot s = m.slots[k];
-      const int f = s.f;
-      double nV[3], area;
-      unit_normal(m, f, nV, area);
-      if (s.nb >= 0) {
-        // ---------------- internal face ----------------
-        const int c0 = s.side == 0 ? c : s.nb;
-        const int c1 = s.side == 0 ? s.nb : c;
-        const double sg = s.side == 0 ? -1.0 : 1.0;  // residual sign of this cell
-        const int fo = face_opts<KIND>(p, st, c0, c1);
-        {
-          FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
-          double F[5];
-          euler_flux_t<KIND>(F, L, R, area, nV, fo, KIND == 5 ? &st.jst[8 * c0] : nullptr,
-                             KIND == 5 ? &st.jst[8 * c1] : nullptr);
-          for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
-        }
-        JT Ob[25];
-        const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
-        if (implicit) {
-          FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c0)), R0 = fstate_as<JT>(cell_fstate(p, st, c1));
-          JT Apl[25], Ami[25];
-          euler_matrices_t<KIND, JT>(Apl, Ami, L0, R0, (JT)area, nVt, fo);
-          // row of c0: D += Apl, O(c0,c1) = Ami ; row of c1: D -= Ami, O(c1,c0) = -Apl
-          if (s.side == 0) {
-            for (int e = 0; e < 25; e++) { sD[e * bd + t] += Apl[e]; Ob[e] = Ami[e]; }
-          } else {
-            for (int e = 0; e < 25; e++) { sD[e * bd + t] -= Ami[e]; Ob[e] = -Apl[e]; }
-          }
-        }
-        if (VISC) {
-          VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-          double sV[3];
-          for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-          double smag = sqrt(dot3(sV, sV));
-          for (int i = 0; i < 3; i++) sV[i] /= smag;
-          double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
-          double Fu[3], FE;
-          VFace vf;
-          visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, ufa, area, nV, smag, sV);
-          for (int i = 0; i < 3; i++) rhs[1 + i] += sg * Fu[i];
-          rhs[4] += sg * FE;
-          if (implicit) {
-            // row of c0: D -= A0, O -= A1 ; row of c1: D += A1, O += A0  (calcViscousFluxNS 3678-3696);
-            // the diagonal part goes straight into the cell's shared-memory block
-            const StridedBlock<JT> Ds{sD + t, bd};
-            if (s.side == 0) {
-              visc_jac_add<JT>(Ds, JT(-1.0), 0, vf, v0, ufa);
-              visc_jac_add<JT>(Ob, JT(-1.0), 1, vf, v1, ufa);
-            } else {
-              visc_jac_add<JT>(Ds, JT(1.0), 1, vf, v1, ufa);
-              visc_jac_add<JT>(Ob, JT(1.0), 0, vf, v0, ufa);
-            }
-          }
-        }
-        if (implicit)
-          for (int e = 0; e < 25; e++) O[ell_index<BT>(m, c, s.col, e)] = (BT)Ob[e];
-      } else {
-        // ---------------- boundary face (the cell is cvofa[f][0]) ----------------
-        const DevZone z = m.zones[m.bzone[f]];
-        const double* bb = &st.bfa[8 * f];
-        FState B;
-        B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
-        const FStateT<JT> Bt = fstate_as<JT>(B);
-        const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};
-        double F[5];
-        const int fob = bnd_opts<KIND>(p);
-        const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
-        if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-          euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
-          if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
-            for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
-          } else {
-            for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-          }
-          if (implicit) {
-            if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
-              // analytical pressure Jacobian, JoeWithModels.cpp:3231-3251
-              double a2 = p.gamma - 1.0;
-              double phi = 0.5 * a2 * (B.u[0] * B.u[0] + B.u[1] * B.u[1] + B.u[2] * B.u[2]);
-              for (int i = 0; i < 3; i++) {
-                sD[(5 * (i + 1) + 0) * bd + t] += (JT)(phi * nV[i] * area);
-                for (int j = 0; j < 3; j++) sD[(5 * (i + 1) + 1 + j) * bd + t] += (JT)(-a2 * B.u[j] * nV[i] * area);
-                sD[(5 * (i + 1) + 4) * bd + t] += (JT)(a2 * nV[i] * area);
-              }
-            } else if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_NEW_NUMERIC) {
-              JT Apl[25], Ami[25];
-              euler_matrices_t<KIND, JT>(Apl, Ami, Bt, Bt, (JT)area, nVt, fob);
-              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e] + Ami[e];
-            } else {
-              JT Apl[25];
-              euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, Bt, Bt, (JT)area, nVt, fob);
-              for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
-            }
-          }
-        } else {
-          FState L = recon(m, p, st, c, f);
-          euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
-          for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-          if (implicit) {
-            FStateT<JT> L0 = fstate_as<JT>(cell_fstate(p, st, c));
-            JT Apl[25];
-            euler_matrices_t<KIND, JT>(Apl, (JT*)nullptr, L0, Bt, (JT)area, nVt, fob);
-            for (int e = 0; e < 25; e++) sD[e * bd + t] += Apl[e];
-          }
-        }
-        if (VISC && z.kind != JG_BC_SYMMETRY) {
-          VSide v0 = cell_vside(p, st, c);
-          VSide v1;
-          v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
-          v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
-          v1.gu = v0.gu; v1.gh = v0.gh;
-          double sV[3], smag;
-          for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
-          if (z.kind == JG_BC_WALL) {
-            smag = fabs(dot3(sV, nV));  // projected on the wall normal; nVec is used as sVec
-            for (int i = 0; i < 3; i++) sV[i] = nV[i];
-          } else {
-            smag = sqrt(dot3(sV, sV));
-            for (int i = 0; i < 3; i++) sV[i] /= smag;
-          }
-          double Fu[3], FE;
-          VFace vf;
-          visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
-          for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
-          rhs[4] -= FE;
-          if (implicit) visc_jac_add<JT>(StridedBlock<JT>{sD + t, bd}, JT(-1.0), 0, vf, v0, v1.u);
-        }
-      }
-    }
-  }
-  // ---------------- epilogue ----------------
-  // the lanes' partial residuals and diagonal blocks, summed in lane order (lanes of a cell share
-  // its activity, so the whole warp reaches the shuffles)
-  if (CL > 1) {
-    for (int i = 0; i < 5; i++) {
-      double tot = 0.0;
-      for (int l = 0; l < CL; l++) tot += __shfl_sync(0xffffffffu, rhs[i], (t & 31) - lane + l);
-      rhs[i] = tot;
-    }
-    __syncwarp();
-  }
-  if (active && lane == 0) {
-    for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
-    if (implicit) {
-      double Dm[25];
-      for (int e = 0; e < 25; e++) {
-        JT d = sD[e * bd + t];
-        for (int l = 1; l < CL; l++) d += sD[e * bd + t + l];
-        Dm[e] = (double)d;
-      }
-      if (for_step) {
-        double tmp = m.vol[c] / st.local_dt[c];
-        for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;
-        for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
-      }
-      BT* Dg = (BT*)st.D;
-      for (int e = 0; e < 25; e++) Dg[(size_t)e * m.ncv + c] = (BT)Dm[e];
-      if (for_step) {
-        double Di[25];
-        block_inverse(Dm, Di);
-        BT* Dig = (BT*)st.Dinv;
-        for (int e = 0; e < 25; e++) Dig[(size_t)e * m.ncv + c] = (BT)Di[e];
-      }
-    }
-  }
-}
-
-// 8 lanes per cell: lane l of a cell evaluates the cell's faces l, l+8, ...;
-// the contributions are summed over the lanes with an XOR butterfly (every
-// lane ends with the same order-fixed sum: deterministic).
-constexpr int FL = 8;  // lanes per cell
-
-__device__ __forceinline__ double lane_sum(double v) {
-  v += __shfl_xor_sync(0xffffffffu, v, 4);
-  v += __shfl_xor_sync(0xffffffffu, v, 2);
-  v += __shfl_xor_sync(0xffffffffu, v, 1);
-  return v;
-}
-
-// Residual-only face loop (calcRhs with flagImplicit = 0), 8 lanes per cell.
-// Without the Jacobian blocks the live set is small (~120 registers), so the
-// lanes-per-cell split pays: many warps per SM.
-template <int KIND, int VISC>
-__global__ void __launch_bounds__(128) k_rhs2(Mesh m, Params p, State st, int for_step) {
-  __shared__ double sres[5][128 / FL];
-  const int t = threadIdx.x, lane = t % FL, cl = t / FL;
-  const int c = blockIdx.x * (128 / FL) + cl;
-  const bool active = c < m.ncv;
-  double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  const int k0 = active ? m.slot_i[c] : 0, k1 = active ? m.slot_i[c + 1] : 0;
-  for (int k = k0 + lane; k < k1; k += FL) {
-    const Slot s = m.slots[k];
-    const int f = s.f;
-    double nV[3], area;
-    unit_normal(m, f, nV, area);
-    if (s.nb >= 0) {
-      const int c0 = s.side == 0 ? c : s.nb;
-      const int c1 = s.side == 0 ? s.nb : c;
-      const double sg = s.side == 0 ? -1.0 : 1.0;
-      {
-        FState L = recon(m, p, st, c0, f), R = recon(m, p, st, c1, f);
-        double F[5];
-        euler_flux_t<KIND>(F, L, R, area, nV, face_opts<KIND>(p, st, c0, c1), KIND == 5 ? &st.jst[8 * c0] : nullptr,
-                           KIND == 5 ? &st.jst[8 * c1] : nullptr);
-        for (int i = 0; i < 5; i++) rhs[i] += sg * F[i];
-      }
-      if (VISC) {
-        VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-        double sV[3];
-        for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-        double smag = sqrt(dot3(sV, sV));
-        for (int i = 0; i < 3; i++) sV[i] /= smag;
-        double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
-        double Fu[3], FE;
-        VFace vf;
-        visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, ufa, area, nV, smag, sV);
-        for (int i = 0; i < 3; i++) rhs[1 + i] += sg * Fu[i];
-        rhs[4] += sg * FE;
-      }
-    } else {
-      const DevZone z = m.zones[m.bzone[f]];
-      const double* bb = &st.bfa[8 * f];
-      FState B;
-      B.rho = bb[0]; B.u[0] = bb[1]; B.u[1] = bb[2]; B.u[2] = bb[3]; B.p = bb[4]; B.gam = p.gamma; B.h = bb[6];
-      double F[5];
-      const int fob = bnd_opts<KIND>(p);
-      const double* jb = KIND == 5 ? &st.jst[8 * c] : nullptr;
-      if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_WALL) {
-        euler_flux_t<KIND>(F, B, B, area, nV, fob, jb, jb);
-        if (z.kind == JG_BC_SYMMETRY && p.symm_bc == JG_SYMM_ANALYTICAL) {
-          for (int i = 0; i < 3; i++) rhs[1 + i] -= bb[4] * nV[i] * area;
-        } else {
-          for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-        }
-      } else {
-        FState L = recon(m, p, st, c, f);
-        euler_flux_t<KIND>(F, L, B, area, nV, fob, jb, jb);
-        for (int i = 0; i < 5; i++) rhs[i] -= F[i];
-      }
-      if (VISC && z.kind != JG_BC_SYMMETRY) {
-        VSide v0 = cell_vside(p, st, c);
-        VSide v1;
-        v1.rho = bb[0]; v1.u[0] = bb[1]; v1.u[1] = bb[2]; v1.u[2] = bb[3];
-        v1.h = bb[6]; v1.T = bb[5]; v1.R = p.R; v1.gam = p.gamma;
-        v1.gu = v0.gu; v1.gh = v0.gh;
-        double sV[3], smag;
-        for (int i = 0; i < 3; i++) sV[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
-        if (z.kind == JG_BC_WALL) {
-          smag = fabs(dot3(sV, nV));
-          for (int i = 0; i < 3; i++) sV[i] = nV[i];
-        } else {
-          smag = sqrt(dot3(sV, sV));
-          for (int i = 0; i < 3; i++) sV[i] /= smag;
-        }
-        double Fu[3], FE;
-        VFace vf;
-        visc_flux(Fu, FE, vf, v0, v1, st.mul_fa[f], 0.0, st.lam_fa[f], p.PrTurb, v1.u, area, nV, smag, sV);
-        for (int i = 0; i < 3; i++) rhs[1 + i] -= Fu[i];
-        rhs[4] -= FE;
-      }
-    }
-  }
-  for (int i = 0; i < 5; i++) rhs[i] = lane_sum(rhs[i]);
-  if (active && lane == 0) {
-    for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
-    if (for_step)
-      for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
-  }
-  if (for_step) {
-    if (lane == 0)
-      for (int i = 0; i < 5; i++) sres[i][cl] = active ? fabs(rhs[i]) : 0.0;
-    __syncthreads();
-    if (t < 5) {
-      double v = 0.0;
-      for (int q = 0; q < 128 / FL; q++) v += sres[t][q];
-      st.blk[5 * blockIdx.x + t] = v;
-    }
-  }
 }
 
 // Block point relaxation, one warp per block row: a 160-thread block handles
@@ -1134,6 +722,10 @@ __global__ void k_resid_cases(State st, const int* __restrict__ rblk_off, int nc
     idx = ((idx % st.hist_cap) + st.hist_cap) % st.hist_cap;  // ring buffer
     for (int i = 0; i < B; i++) st.resid[(idx * ncases + k) * B + i] = v[i];
     if (!(v[4] == v[4]) && st.case_active[k]) atomicOr(st.case_err + k, 4);  // NaN energy residual (doneSolver)
+    // a lagged Jacobian formed at this step is next due jac_lag steps later (the face loop, which
+    // read the schedule, ran before this kernel)
+    const long long step = (long long)st.ctrl[1];
+    if (hist_from_ctrl && st.jac_next && step >= st.jac_next[k]) st.jac_next[k] = step + st.jac_lag;
   }
 }
 void launch_resid_cases(State& st, const int* case_off, const int* rblk_off, const int* rblk_case, int nrblk,
@@ -1188,11 +780,13 @@ __global__ void __launch_bounds__(128) k_jacobi(Mesh m, State st, const BT* __re
 // Multicolour block Gauss-Seidel pass over one colour, in place: the cells of
 // a colour have no neighbours of the same colour, so each reads the latest
 // values of the others.  Same row-parallel layout as k_jacobi2.
+// slices (may be null: every slice): the slices that hold a cell of this colour
 template <typename BT>
-__global__ void __launch_bounds__(160) k_gs2(Mesh m, State st, BT* __restrict__ x, int color) {
+__global__ void __launch_bounds__(160) k_gs2(Mesh m, State st, BT* __restrict__ x, int color,
+                                             const int* __restrict__ slices) {
   __shared__ BT sacc[5][SLICE];
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
-  const int slice = blockIdx.x;
+  const int slice = slices ? slices[blockIdx.x] : blockIdx.x;
   const int c = slice * SLICE + lane;
   const bool active = c < m.ncv && m.color[c] == color;
   const int N = m.ncv;
@@ -1483,73 +1077,17 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   int separate = do_visc && do_euler && !p.visc_limiter && p.limiter;
   launch_grad_k(m, p, st, do_euler, do_visc, visc_lim, visc_lim, separate, s);
 }
+// per-cell sensors the face loop of some flux kinds reads: the AUSMDV shock-fix flags, the JST
+// coefficients (both before the face loop, cell-centric)
+void launch_face_sensors(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  if (p.flux == JG_FLUX_AUSMDV && p.shock_fix != JG_SHOCK_FIX_NONE)
+    k_shock_flag<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
+  if (p.flux == JG_FLUX_JST) k_jst<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
+}
 // calcFluxCoupled (JoeWithModels.cpp:4683-4702): grad_u (second order or viscous), grad_rho,
 // grad_p (second order) and grad_enthalpy (viscous), all with the flow limiter; one grad_u
 void launch_grad_coupled(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   launch_grad_k(m, p, st, p.second_order, 1, p.limiter, p.limiter, 0, s);
-}
-constexpr int FLUX_CELLS = 128 / FL;  // cells per k_flux2 block
-// residual only: 8 lanes per cell (light kernel, many warps)
-template <typename BT, int KIND>
-static void launch_flux_k(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
-  int g = grid_for(m.ncv, FLUX_CELLS);
-  if (p.viscous) k_rhs2<KIND, 1><<<g, 128, 0, s>>>(m, p, st, for_step);
-  else k_rhs2<KIND, 0><<<g, 128, 0, s>>>(m, p, st, for_step);
-}
-template <typename BT>
-static void launch_flux_t(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
-  if (p.flux == JG_FLUX_ROE) launch_flux_k<BT, 1>(m, p, st, implicit, for_step, s);
-  else if (p.flux == JG_FLUX_AUSM) launch_flux_k<BT, 2>(m, p, st, implicit, for_step, s);
-  else if (p.flux == JG_FLUX_HAENEL) launch_flux_k<BT, 3>(m, p, st, implicit, for_step, s);
-  else if (p.flux == JG_FLUX_AUSMDV) launch_flux_k<BT, 4>(m, p, st, implicit, for_step, s);
-  else if (p.flux == JG_FLUX_JST) launch_flux_k<BT, 5>(m, p, st, implicit, for_step, s);
-  else launch_flux_k<BT, 0>(m, p, st, implicit, for_step, s);
-}
-template <typename BT, int KIND, int CL, int MINB>
-static void launch_flux_cell_cl(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  size_t shm = 25 * TB * sizeof(BT);
-  const int g = grid_for(m.ncv, TB / CL);
-  if (p.viscous) k_flux<BT, KIND, 1, CL, MINB><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
-  else k_flux<BT, KIND, 0, CL, MINB><<<g, TB, shm, s>>>(m, p, st, 1, for_step);
-}
-// lanes per cell of the implicit face loop: p.flux_cl (1, 2 or 4)
-// p.flux_cl: lanes per cell 1, 2 or 4 (two 128-thread blocks per SM), or JG_FLUX_CL1_3BLK
-// (one lane, three blocks per SM)
-template <typename BT, int KIND>
-static void launch_flux_cell_k(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  if (p.flux_cl == 1) launch_flux_cell_cl<BT, KIND, 1, 2>(m, p, st, for_step, s);
-  else if (p.flux_cl == JG_FLUX_CL1_3BLK) launch_flux_cell_cl<BT, KIND, 1, 3>(m, p, st, for_step, s);
-  else if (p.flux_cl == 4) launch_flux_cell_cl<BT, KIND, 4, 2>(m, p, st, for_step, s);
-  else launch_flux_cell_cl<BT, KIND, 2, 2>(m, p, st, for_step, s);
-}
-template <typename BT>
-static void launch_flux_cell(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s) {
-  if (p.flux == JG_FLUX_ROE) launch_flux_cell_k<BT, 1>(m, p, st, for_step, s);
-  else if (p.flux == JG_FLUX_AUSM) launch_flux_cell_k<BT, 2>(m, p, st, for_step, s);
-  else if (p.flux == JG_FLUX_HAENEL) launch_flux_cell_k<BT, 3>(m, p, st, for_step, s);
-  else if (p.flux == JG_FLUX_AUSMDV) launch_flux_cell_k<BT, 4>(m, p, st, for_step, s);
-  else if (p.flux == JG_FLUX_JST) launch_flux_cell_k<BT, 5>(m, p, st, for_step, s);
-  else launch_flux_cell_k<BT, 0>(m, p, st, for_step, s);
-}
-// residual + Jacobian: one thread per cell, so that the 32 lanes of a warp
-// walk the same face position of 32 neighbouring cells (coherent branches);
-// residual only: the light 8-lanes-per-cell kernel
-void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s) {
-  if (p.flux == JG_FLUX_AUSMDV && p.shock_fix != JG_SHOCK_FIX_NONE)
-    k_shock_flag<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
-  if (p.flux == JG_FLUX_JST) k_jst<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
-  if (!implicit) {
-    if (p.fp32) launch_flux_t<float>(m, p, st, 0, for_step, s);
-    else launch_flux_t<double>(m, p, st, 0, for_step, s);
-    return;
-  }
-  if (p.fp32) launch_flux_cell<float>(m, p, st, for_step, s);
-  else launch_flux_cell<double>(m, p, st, for_step, s);
-}
-// number of per-block residual partials written by launch_flux
-int flux_partials(const Mesh& m, int implicit) { return implicit ? grid_for(m.ncv, TB) : grid_for(m.ncv, FLUX_CELLS); }
-void launch_resid(const Mesh& m, State& st, int hist_from_ctrl, cudaStream_t s) {
-  k_resid_final<<<1, 256, 0, s>>>(st, flux_partials(m, 1), hist_from_ctrl);
 }
 // both sweep kernels do the same arithmetic in the same order (bit-identical results)
 void launch_jacobi(const Mesh& m, const Params& p, State& st, int sweeps, cudaStream_t s) {
@@ -1574,8 +1112,12 @@ void launch_sgs(const Mesh& m, const Params& p, State& st, int sweeps, cudaStrea
   for (int it = 0; it < sweeps; it++)
     for (int q = 0; q < m.ncolors; q++) {
       int col = (it % 2 == 0) ? q : m.ncolors - 1 - q;  // forward, then backward colour order
-      if (p.fp32) k_gs2<float><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (float*)st.x0, col);
-      else k_gs2<double><<<m.nslices, 5 * SLICE, 0, s>>>(m, st, (double*)st.x0, col);
+      const bool lists = m.color_slices != nullptr;
+      const int* sl = lists ? m.color_slices + m.color_slice_off[col] : nullptr;
+      const int g = lists ? m.color_slice_off[col + 1] - m.color_slice_off[col] : m.nslices;
+      if (g == 0) continue;
+      if (p.fp32) k_gs2<float><<<g, 5 * SLICE, 0, s>>>(m, st, (float*)st.x0, col, sl);
+      else k_gs2<double><<<g, 5 * SLICE, 0, s>>>(m, st, (double*)st.x0, col, sl);
     }
 }
 void launch_dq_from_x(const Mesh& m, const Params& p, State& st, const void* x, cudaStream_t s) {

@@ -55,6 +55,19 @@ def request_stream(rate, horizon, lo, hi, seed):
     return out
 
 
+def case_specs(n, lo, hi, seed):
+    """n seeded cases with the stream's distributions (cells log-uniform on [lo, hi], Mach
+    U(0.3, 0.8), angle of attack U(+-4 deg), bump height U(0.05, 0.12)), all arriving at t = 0"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        cells = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        ny = max(4, int(round(math.sqrt(cells / 4.0))))
+        out.append(dict(t=0.0, nx=2 * ny, ny=ny, nz=2, mach=float(rng.uniform(0.3, 0.8)),
+                        aoa=float(rng.uniform(-4.0, 4.0)), bump=float(rng.uniform(0.05, 0.12)), seed=k))
+    return out
+
+
 def build_request(spec):
     from myjoe_b200 import case
     _, g, prm = case.bump_case(spec["nx"], spec["ny"], spec["nz"], mach=spec["mach"], aoa_deg=spec["aoa"],
@@ -71,6 +84,70 @@ def solver_params(prm, args):
 
 def pct(a, q):
     return float(np.percentile(a, q)) if len(a) else None
+
+
+@dataclasses.dataclass
+class BurstConfig:
+    """Settings of a burst: every case submitted at t = 0, the arm runs until all retire."""
+    drop: float = 1e-8
+    sweeps: int = 10
+    cfl_ramp: str = "10,5,1.2,20"
+    max_steps: int = 6000
+    chunk: int = 25
+    max_resident: int = 64
+    max_restarts: int = 2
+    restart_factor: float = 0.25
+    stall_steps: int = 1000
+    jac_lag: int = 4          # serving arms: flux Jacobian blocks every jac_lag-th step
+    hbm_budget: float = 0.0   # GB; 0: 90% of the free device memory
+    renumber: int = 2         # every arm: cells in RCM order grouped by Gauss-Seidel colour
+
+
+def run_burst(arm, cases, cfg: BurstConfig):
+    """One arm over a list of built cases (g, prm, state), all arriving at once.
+
+    * ``plain``: the plain FP64 GPU drop-in, one case at a time in list order, the
+      Jacobian formed every step;
+    * ``serve``: the serving form, mixed precision with a lagged Jacobian, up to
+      ``max_resident`` cases on the device at once, admitted in list order by footprint;
+    * ``serve-smallest``: the same, admitting the smallest queued footprint first.
+
+    Time-to-converge is arrival (t = 0) to retirement; solves/hour = converged cases /
+    makespan.  Same relaxation, CFL ramp, step limit, stall rule and restart policy in
+    every arm."""
+    from myjoe_b200 import solver
+    serving = arm.startswith("serve")
+    srv = solver.JoeServer(max_resident=cfg.max_resident if serving else 1, hbm_budget=cfg.hbm_budget * 1e9,
+                           steps_per_poll=cfg.chunk, resid_drop=cfg.drop, max_steps=cfg.max_steps,
+                           max_restarts=cfg.max_restarts, restart_cfl_factor=cfg.restart_factor,
+                           stall_steps=cfg.stall_steps, admission="smallest" if arm == "serve-smallest" else "fifo")
+
+    class _A:  # solver_params reads these
+        sweeps, cfl_ramp = cfg.sweeps, cfg.cfl_ramp
+    t0 = srv.now()
+    for g, prm, state in cases:
+        srv.submit(g, solver_params(prm, _A), state, precision=1 if serving else 0, t_arrival=t0,
+                   jac_lag=cfg.jac_lag if serving else 1, renumber=cfg.renumber)
+    results = []
+    while len(results) < len(cases):
+        for r in srv.poll(max_wait=0.05):
+            srv.fetch(r["id"])
+            results.append(r)
+    makespan = max(r["t_done"] for r in results) - t0
+    srv.close()
+    conv = [r for r in results if r["status"] == 0]
+    ttc = [r["t_done"] - t0 for r in conv]
+    cell_iters = sum(r["ncv"] * r["steps_total"] for r in results)
+    return {"arm": arm, "precision": "mixed" if serving else "fp64", "jac_lag": cfg.jac_lag if serving else 1,
+            "max_resident": cfg.max_resident if serving else 1, "cases": len(cases), "converged": len(conv),
+            "failed": sum(1 for r in results if r["status"] == 2),
+            "max_steps_hit": sum(1 for r in results if r["status"] == 1),
+            "stalled": sum(1 for r in results if r["status"] == 3),
+            "restarts": sum(r["restarts"] for r in results), "makespan_s": makespan,
+            "solves_per_hour": len(conv) / makespan * 3600.0,
+            "p50_s": pct(ttc, 50), "p99_s": pct(ttc, 99),
+            "steps_to_converge_p50": pct([r["conv_step"] for r in conv], 50),
+            "cell_iters_per_s": cell_iters / makespan}
 
 
 def run_arm(arm, stream, args):

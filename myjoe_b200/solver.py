@@ -21,6 +21,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libjoe_b200.so")
 _lib = None
 
+FLUX_SPLIT = 32        # JG_FLUX_SPLIT: face-loop shapes split into a residual and a Jacobian kernel
+FLUX_CL1_3BLK = 17     # JG_FLUX_CL1_3BLK
+RENUMBER_RCM, RENUMBER_RCM_COLOR = 1, 2   # jg_params.renumber
 JG_ERR = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory", -4: "non-physical state",
           -5: "no CUDA device", -6: "file error"}
 
@@ -118,10 +121,10 @@ class JoeGpu:
     """One case on the GPU.  ``mesh_src`` is a ``geometry.CvMesh`` or a dict of
     reference-layout arrays; ``params`` a ``case.JoeParams``."""
 
-    def __init__(self, mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False):
+    def __init__(self, mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False, jac_lag: int = 1):
         self.params = params
         self.ma = MeshArrays(mesh_src, params)
-        self.jp = make_params(params, precision, renumber)
+        self.jp = make_params(params, precision, renumber, jac_lag)
         self.ncv = self.ma.ncv
         h = C.c_void_p()
         _ck(lib().jg_create(C.byref(self.ma.mesh), C.byref(self.jp), C.byref(h)))
@@ -272,10 +275,12 @@ class JoeGpu:
         """time the launch shapes on this handle and keep the fastest: returns
         (lanes per cell of the face loop, sweep kernel, {shape: ms per launch})"""
         cl, rv = C.c_int(0), C.c_int(0)
-        ms = (C.c_float * 6)()
+        ms = (C.c_float * 10)()
         _ck(lib().jg_autotune(self.h, int(trials), C.byref(cl), C.byref(rv), ms))
         times = {"flux_cl1": ms[0], "flux_cl2": ms[1], "flux_cl4": ms[2], "sweep0": ms[3], "sweep1": ms[4],
                  "flux_cl17": ms[5]}
+        for k, fl in enumerate((1, 2, 4, 8)):
+            times["flux_cl%d" % (FLUX_SPLIT + fl)] = ms[6 + k]
         return cl.value, rv.value, times
 
     def set_launch_config(self, flux_cl, relax_variant):
@@ -303,7 +308,7 @@ class JoeGpu:
 
     def set_params(self, params: JoeParams):
         """new run-time settings (CFL, ramp, under-relaxation, solver thresholds, EPS) for this handle"""
-        jp = make_params(params, self.jp.precision, bool(self.jp.renumber))
+        jp = make_params(params, self.jp.precision, bool(self.jp.renumber), self.jp.jac_lag)
         _ck(lib().jg_set_params(self.h, C.byref(jp)))
         self.jp = jp
         self.params = params
@@ -353,12 +358,12 @@ class JoeGpuBatch(JoeGpu):
     and each brings its own boundary values.  Cases whose shared settings
     differ (two fluids, say) are refused."""
 
-    def __init__(self, cases, precision: int = 0):
+    def __init__(self, cases, precision: int = 0, jac_lag: int = 1):
         self.params = cases[0][1]
         self.mas = [MeshArrays(m, p) for m, p in cases]
-        self.jp = make_params(self.params, precision)
+        self.jp = make_params(self.params, precision, jac_lag=jac_lag)
         for k, (_, prm) in enumerate(cases[1:], 1):
-            q = make_params(prm, precision)
+            q = make_params(prm, precision, jac_lag=jac_lag)
             diff = [f for f, _ in jg_params._fields_ if getattr(q, f) != getattr(self.jp, f)]
             if diff:
                 raise ValueError("case %d differs from case 0 in the batch-wide settings %s" % (k, diff))
@@ -443,9 +448,10 @@ class JoeServer:
         _ck(lib().jg_serve_now(self.h, C.byref(t)))
         return t.value
 
-    def submit(self, mesh_src, params: JoeParams, state, precision: int = 0, t_arrival: float = -1.0) -> int:
+    def submit(self, mesh_src, params: JoeParams, state, precision: int = 0, t_arrival: float = -1.0,
+               jac_lag: int = 1, renumber: int = 0) -> int:
         ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
-        jp = make_params(params, precision)
+        jp = make_params(params, precision, renumber, jac_lag)
         rho, rhou, rhoE = (np.ascontiguousarray(a, np.float64) for a in state)
         i = C.c_longlong()
         _ck(lib().jg_serve_submit(self.h, C.byref(ma.mesh), C.byref(jp), dptr(rho), dptr(rhou), dptr(rhoE),
@@ -472,19 +478,21 @@ class JoeServer:
         return {"resident": r.value, "queued": q.value, "unfetched": f.value, "bytes_resident": b.value}
 
 
-def case_footprint(mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False) -> float:
+def case_footprint(mesh_src, params: JoeParams, precision: int = 0, renumber: bool = False,
+                   jac_lag: int = 1) -> float:
     """Device bytes jg_create + jg_set_state allocate for this case."""
     ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
-    jp = make_params(params, precision, renumber)
+    jp = make_params(params, precision, renumber, jac_lag)
     b = C.c_double()
     _ck(lib().jg_case_footprint(C.byref(ma.mesh), C.byref(jp), C.byref(b)))
     return b.value
 
 
-def renumber_cells(mesh_src, params: JoeParams) -> np.ndarray:
-    """The cell order a handle made with ``renumber=True`` uses: the caller's id
-    of each cell (reverse Cuthill-McKee; host only, no GPU needed)."""
+def renumber_cells(mesh_src, params: JoeParams, method: int = RENUMBER_RCM) -> np.ndarray:
+    """The cell order a handle made with ``renumber=method`` uses: the caller's id
+    of each cell (reverse Cuthill-McKee, or RCM grouped by Gauss-Seidel colour;
+    host only, no GPU needed)."""
     ma = mesh_src if isinstance(mesh_src, MeshArrays) else MeshArrays(mesh_src, params)
     out = np.empty(ma.ncv, np.int32)
-    _ck(lib().jg_renumber_cells(C.byref(ma.mesh), 1, out.ctypes.data_as(C.POINTER(C.c_int))))
+    _ck(lib().jg_renumber_cells(C.byref(ma.mesh), int(method), out.ctypes.data_as(C.POINTER(C.c_int))))
     return out

@@ -1,9 +1,10 @@
 """Launch shapes of the 5x5 path (jg_set_launch_config / jg_autotune).
 
 The two Jacobi sweep kernels do the same arithmetic in the same order, so a
-step gives bit-identical results with either; the lanes per cell of the face
-loop change only the order of each cell's diagonal-block and residual sums,
-so steps agree to rounding (1e-12 relative after 10 steps).  The autotuner
+step gives bit-identical results with either; the face-loop shapes (fused or
+split into residual and Jacobian kernels, lanes per cell) change only the
+order of each cell's diagonal-block and residual sums and the form of the Roe
+dissipation matrix, so steps agree to rounding (1e-12 relative after 10 steps).  The autotuner
 returns a valid shape and per-shape times, and a batch and its cases alone
 stay bit-identical under a shared shape."""
 import dataclasses
@@ -42,7 +43,8 @@ def test_sweep_kernels_are_bitwise_equal():
         np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("cl", [1, 4, 17])
+# fused shapes (1, 4, 17) and split shapes (residual and Jacobian kernels: 32 + lanes per cell)
+@pytest.mark.parametrize("cl", [1, 4, 17, 33, 34, 36, 40])
 def test_lanes_per_cell_agree_to_rounding(cl):
     g, prm = _plate("SGS")
     a = _run(g, prm, (2, 0))
@@ -57,9 +59,10 @@ def test_autotune_picks_a_valid_shape_and_keeps_results():
     j = solver.JoeGpu(g, prm)
     j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
     cl, rv, ms = j.autotune(3)
-    assert cl in (1, 2, 4, 17) and rv in (0, 1)
+    shapes = (1, 2, 4, 17, 33, 34, 36, 40)
+    assert cl in shapes and rv in (0, 1)
     assert all(v > 0.0 for v in ms.values())
-    assert ms["flux_cl%d" % cl] == min(ms["flux_cl1"], ms["flux_cl2"], ms["flux_cl4"], ms["flux_cl17"])
+    assert ms["flux_cl%d" % cl] == min(ms["flux_cl%d" % s] for s in shapes)
     r = j.runBackwardEuler(10)   # the tuned shape is captured at the next step
     assert np.all(np.isfinite(r))
     ref = _run(g, prm, (cl, rv))

@@ -157,7 +157,10 @@ def test_batch_refuses_a_coupling_time_step_mode_after_creation():
     handle keeps stepping with its old settings."""
     import ctypes as C
     from myjoe_b200.abi import jg_params
-    b = solver.JoeGpuBatch(cases())
+    cs = cases()
+    b = solver.JoeGpuBatch(cs)
+    for k, (g, prm) in enumerate(cs):
+        b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
     q = jg_params()
     C.memmove(C.byref(q), C.byref(b.jp), C.sizeof(jg_params))
     q.time_step_mode = 1  # JG_TS_CFL_MIN

@@ -150,3 +150,25 @@ def test_renumbered_sgs_converges_to_the_same_field():
     assert ra[-1, 4] / ra[0, 4] < 1e-9 and rb[-1, 4] / rb[0, 4] < 1e-9
     for x, y in zip(a.get_state(), b.get_state()):
         assert np.linalg.norm(x - y) <= 1e-8 * np.linalg.norm(x)
+
+
+def test_color_grouped_order_gives_the_rcm_sgs_bits():
+    """JG_RENUMBER_RCM_COLOR keeps the RCM order's colour classes, so multicolour
+    Gauss-Seidel steps give the RCM handle's states bit for bit (only the L1
+    residual sums run in another order); each colour pass now launches over the
+    slices of that colour only."""
+    from myjoe_b200 import case, solver
+    g, prm = _euler_mixed()
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="SGS", LS_MAX_ITER=6, CFL=2.0, CFL_RAMP=(10, 5, 1.2, 20.0))
+    for precision in (0, 1):
+        a = solver.JoeGpu(g, prm, precision=precision, renumber=solver.RENUMBER_RCM)
+        b = solver.JoeGpu(g, prm, precision=precision, renumber=solver.RENUMBER_RCM_COLOR)
+        st = case.perturbed_state(g.x_cv, prm, 0.02)
+        for j in (a, b):
+            j.set_state(*st)
+        ra, rb = a.runBackwardEuler(30), b.runBackwardEuler(30)
+        np.testing.assert_allclose(rb, ra, rtol=1e-13, atol=0.0)
+        for x, y in zip(a.get_state(), b.get_state()):
+            np.testing.assert_array_equal(x, y)
+        a.close()
+        b.close()

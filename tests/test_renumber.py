@@ -101,3 +101,45 @@ def test_rcm_order_handles_disconnected_components():
     comp = order2 >= n
     assert np.count_nonzero(np.diff(comp.astype(int))) == 1
     assert sorted(order.tolist()) == sorted((order2[comp] - n).tolist())
+
+
+def _greedy_colors(g, cell_old):
+    """greedy colouring of the cell graph in the order cell_old (a handle's own colouring)"""
+    new = _inverse(cell_old)
+    fa = g.cvofa[g.nfa_b:]
+    adj = [[] for _ in range(g.ncv)]
+    for a, b in fa:
+        adj[new[a]].append(new[b])
+        adj[new[b]].append(new[a])
+    col = np.zeros(g.ncv, int)
+    for c in range(g.ncv):
+        used = {col[nb] for nb in adj[c] if nb < c}
+        k = 0
+        while k in used:
+            k += 1
+        col[c] = k
+    return col
+
+
+def test_rcm_color_order_groups_the_rcm_colour_classes():
+    """JG_RENUMBER_RCM_COLOR: the RCM order stably grouped by the greedy colours of
+    the RCM order; colouring again in the new order gives the same classes, now
+    contiguous (so each Gauss-Seidel colour pass reads a contiguous range)."""
+    raw = meshgen.channel_bump_mixed(48, 24, 4, n_prism=6, stretch=1.1, jitter=0.1, seed=5)
+    g = geometry.build_cv_mesh(raw, seed=9, shuffle=True)
+    _, _, prm = case.bump_case(8, 4, 2)
+    rcm = solver.renumber_cells(g, prm, solver.RENUMBER_RCM)
+    rc = solver.renumber_cells(g, prm, solver.RENUMBER_RCM_COLOR)
+    assert np.array_equal(np.sort(rc), np.arange(g.ncv))
+    col_rcm = _greedy_colors(g, rcm)
+    col_rc = _greedy_colors(g, rc)
+    assert np.all(np.diff(col_rc) >= 0)                       # colours contiguous, in order
+    by_cell_rcm = np.empty(g.ncv, int)
+    by_cell_rcm[rcm] = col_rcm
+    by_cell_rc = np.empty(g.ncv, int)
+    by_cell_rc[rc] = col_rc
+    np.testing.assert_array_equal(by_cell_rcm, by_cell_rc)    # the same class of every cell
+    # inside a colour, the RCM order is kept
+    pos_rcm = _inverse(rcm)
+    for q in range(col_rc.max() + 1):
+        assert np.all(np.diff(pos_rcm[rc[col_rc == q]]) > 0)

@@ -184,6 +184,104 @@ CONVERGE_WORKLOAD = ("burst of seeded channel-bump cases (hex, 2 cell layers; ce
                      "CFL 1 -> 20, each retired at a 1e-8 drop of its L1 energy residual")
 
 
+HBM_WORKLOAD = ("channel bump 1400x700x2 hex (1,960,000 cells), HLLC, second order, far field, JACOBI x10, "
+                "cells grouped by Gauss-Seidel colour in RCM order; the working set (~4 GB FP64) is far above L2")
+
+
+def build_hbm_case():
+    from myjoe_b200 import case
+    _, g, prm = case.bump_case(1400, 700, 2, inlet="FARFIELD")
+    return g, prm, case.perturbed_state(g.x_cv, prm, 0.0)
+
+
+def hbm_leg(hcase, nsteps=20):
+    """The 5x5 path at HBM scale, FP64 and mixed: ms per step and the face-loop and sweep roofline
+    from the in-graph events (the matrix and the state do not fit L2, so no flush is needed)."""
+    import torch
+    from myjoe_b200 import solver
+    g, prm, st0 = hcase
+    peak, _ = measured_peaks()
+    out = {"workload": HBM_WORKLOAD, "cells": g.ncv, "l2": "working set above L2 (no flush)"}
+    p = dataclasses.replace(prm, LINEAR_SOLVER_NS="JACOBI", LS_MAX_ITER=SWEEPS, CFL=1.0, CFL_RAMP=(10, 5, 1.2, 20.0))
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        j = solver.JoeGpu(g, p, precision=prec, renumber=2)
+        j.set_state(*st0)
+        cl, rv, _ = j.autotune(3)
+        j.set_state(*st0)
+        j.set_profiling(True)
+        j.runBackwardEuler(3)
+        stream = torch.cuda.ExternalStream(j.stream)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        fm, sm = [], []
+        for e0, e1 in ev:
+            e0.record(stream)
+            j.step_async(1)
+            e1.record(stream)
+            pr = j.profile()
+            fm.append(pr["face_loop_ms"])
+            sm.append(pr["linear_solve_ms"])
+        torch.cuda.synchronize()
+        step_ms = sum(a.elapsed_time(b) for a, b in ev) / nsteps
+        face_b, sweep_b, f_int, _ = algorithmic_bytes(g, name)
+        face_ms, sweep_ms = sum(fm) / nsteps, sum(sm) / nsteps / SWEEPS
+        out[name] = {"ms_per_step": step_ms, "cell_iters_per_s": g.ncv / (step_ms * 1e-3),
+                     "launch_shape": {"face_loop": cl, "sweep_kernel": rv},
+                     "face_loop": {"ms": face_ms, "bytes_per_cell": face_b,
+                                   "achieved_gbs": face_b * g.ncv / (face_ms * 1e-3) / 1e9,
+                                   "frac": face_b * g.ncv / (face_ms * 1e-3) / 1e9 / peak},
+                     "sweep": {"ms": sweep_ms, "bytes_per_cell": sweep_b,
+                               "achieved_gbs": sweep_b * g.ncv / (sweep_ms * 1e-3) / 1e9,
+                               "frac": sweep_b * g.ncv / (sweep_ms * 1e-3) / 1e9 / peak}}
+        j.close()
+    out["peak_gbs"] = peak
+    return out
+
+
+CONFIG3_WORKLOAD = ("precision form: SA-RANS channel bump M 0.7, Re 3e6, shuffled mixed prism/hex mesh 512x400x8 "
+                    "(88 prism rows, stretch 1.02; 1,998,848 cells) renumbered by the handle, HLLC + viscous, "
+                    "6x6 coupled blocks, LINE x10, FP64 and mixed")
+
+
+def run_config3(args):
+    """--workload config3: the precision form's 2M-cell workload, FP64 and mixed, one JSON line."""
+    import numpy as np
+    import torch
+    from myjoe_b200 import build, case, solver
+    if build.needs_build():
+        build.build()
+    _, g, prm = case.sa_bump_case(512, 400, 8, mach=0.7, re=3.0e6, bump_h=0.05, stretch=1.02, n_prism=88,
+                                  shuffle=True, seed=0)
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="LINE", LS_MAX_ITER=SWEEPS, CFL=1.0,
+                              CFL_RAMP=(10, 5, 1.2, 1000.0), SECOND_ORDER=False)
+    st0 = case.perturbed_state(g.x_cv, prm, 0.0)
+    out = {"metric": "cell-iters/s", "unit": "cell-iters/s", "workload": CONFIG3_WORKLOAD, "cells": g.ncv,
+           "steps": args.steps, "l2": "working set above L2 (no flush)"}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        j = solver.JoeGpu(g, prm, precision=prec, renumber=True)
+        j.set_state(*st0)
+        j.set_scalars(np.full(g.ncv, prm.NUSA_INITIAL))
+        j.runBackwardEuler(max(args.warmup, 3))
+        j.set_profiling(True)
+        stream = torch.cuda.ExternalStream(j.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fm, sm = [], []
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            j.step_async(1)
+            pr = j.profile()
+            fm.append(pr["face_loop_ms"])
+            sm.append(pr["linear_solve_ms"])
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[name] = {"ms_per_step": ms, "cell_iters_per_s": g.ncv / (ms * 1e-3), "face_loop_ms": sum(fm) / len(fm),
+                     "relaxation_ms": sum(sm) / len(sm), "device_bytes": j.device_bytes()}
+        j.close()
+    out["value"] = out["mixed"]["cell_iters_per_s"]
+    print(json.dumps(out))
+
+
 def build_converge_cases(args, rank):
     import multiprocessing as mp
     from myjoe_b200 import serve
@@ -224,9 +322,16 @@ def main():
                     help="cases of the time-to-converge leg (0: skip it)")
     ap.add_argument("--converge-cells", default="5000,500000", help="cells log-uniform on lo,hi")
     ap.add_argument("--jac-lag", type=int, default=4, help="serving arm: flux Jacobian every k-th step")
+    ap.add_argument("--no-hbm-leg", dest="hbm_leg", action="store_false",
+                    help="skip the 2M-cell HBM-scale leg")
+    ap.add_argument("--workload", default="plate", choices=["plate", "config3"],
+                    help="plate: the headline line; config3: the 2M-cell precision-form workload (own line)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "config3":
+        run_config3(args)
         return
 
     import numpy as np
@@ -236,7 +341,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    # the time-to-converge cases are meshed by a spawn pool on the host cores, outside every timed region
+    # the HBM-scale case is meshed in a spawn process while the time-to-converge cases are meshed by a
+    # spawn pool on the host cores, all outside every timed region
+    import multiprocessing as mp
+    hpool = mp.get_context("spawn").Pool(1) if args.hbm_leg else None
+    hjob = hpool.apply_async(build_hbm_case) if hpool else None
     conv_cases = build_converge_cases(args, rank) if args.converge_cases > 0 else None
     torch.cuda.set_device(local)
     if world > 1:
@@ -338,6 +447,12 @@ def main():
                 "timing": "wall clock around synchronised host-driven steps"}
 
     conv = converge_leg(conv_cases, args) if conv_cases else None
+    hbm = None
+    if hjob is not None:
+        hcase = hjob.get()
+        hpool.close()
+        hbm = hbm_leg(hcase)
+        del hcase
     if world > 1 and conv is not None:
         allc = [None] * world
         dist.all_gather_object(allc, conv)
@@ -347,7 +462,7 @@ def main():
         conv["replicas"] = world
     clk = clocks.stop()
     if clk is not None:
-        clk["window"] = "the timed steps, the e2e, BiCGSTAB and time-to-converge legs"
+        clk["window"] = "the timed steps, the e2e, BiCGSTAB, time-to-converge and HBM-scale legs"
 
     # roofline of the dominant kernel, from the live in-graph events
     face_b, sweep_b, f_int, m_blk = algorithmic_bytes(g, args.precision)
@@ -416,6 +531,7 @@ def main():
                 "finite_residual": finite,
                 "bicgstab_like_for_like": bicgstab,
                 "time_to_converge": conv,
+                "hbm_scale": hbm,
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     j.close()

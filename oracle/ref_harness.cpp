@@ -7,6 +7,7 @@
 // runBackwardEuler as the CPU baseline.
 //
 // usage: ref_harness <Joe.in> <run 0|1|2> <dump|coupled|run> <outdir>
+//        joe_gpu_case <Joe.in> 0 gpu <outdir>   (the same harness built with the drop-in binding)
 //   run 0 : JoeWithModels (laminar / inviscid); run 1 : + RansTurbSA; run 2 : + RansTurbKOmSST
 //   dump    : init -> state/material/BC -> calcDt -> calcRhs(implicit) -> one
 //             linear solve (solveCoupledLinSysNS); every array written to outdir
@@ -15,6 +16,8 @@
 //             Jacobian of runBackwardEulerCoupled, plus the turbulence arrays
 //   run     : init -> runBackwardEuler (NSTEPS from the input); prints the
 //             wall-clock of the iteration loop and writes the final state
+//   gpu     : as run, with include/joe_gpu.hpp's JoeGpu in place of JoeWithModels:
+//             the loop on the GPU through libjoe_b200.so
 //
 // Extra input keys read only by this harness:
 //   HARNESS_PERTURB = a   smooth perturbation of the uniform initial state
@@ -29,6 +32,11 @@
 #include "JoeWithModels.h"
 #include "turbModels/TurbModel_SA.h"
 #include "turbModels/TurbModel_KOMSST.h"
+#ifdef JOE_GPU_BINDING
+// the drop-in binding (include/joe_gpu.hpp), built into oracle/_ref/joe_gpu_case with the
+// library linked: mode "gpu" runs the same case path as "run" with the loop on the GPU
+#include "joe_gpu.hpp"
+#endif
 
 static std::string g_out;
 
@@ -338,6 +346,19 @@ public:
     }
   }
 
+  // mode "gpu" (Base = JoeGpu): the binding's GPU loop in place of runBackwardEuler
+  void runTimedGpu() {
+    writeMeta();
+    DUMPD("x_cv", this->x_cv, 3 * this->ncv);
+    dumpState("init");
+    auto t0 = std::chrono::steady_clock::now();
+    this->runBackwardEulerGpu();
+    auto t1 = std::chrono::steady_clock::now();
+    double secs = std::chrono::duration<double>(t1 - t0).count();
+    dumpState("final");
+    printf("HARNESS_STEPS %d\nHARNESS_SECONDS %.6f\n", this->step, secs);
+  }
+
   void runTimed() {
     writeMeta();
     DUMPD("x_cv", this->x_cv, 3 * this->ncv);
@@ -362,6 +383,15 @@ int main(int argc, char *argv[]) {
   int run = atoi(argv[2]);
   std::string mode = argv[3];
   try {
+#ifdef JOE_GPU_BINDING
+    if (mode == "gpu" && run == 0) {
+      Harness<JoeGpu> *j = new Harness<JoeGpu>(argv[1]);
+      j->setup();
+      j->runTimedGpu();
+      MPI_Finalize();
+      return 0;
+    }
+#endif
     if (run == 0) {
       Harness<JoeWithModels> *j = new Harness<JoeWithModels>(argv[1]);
       j->setup();

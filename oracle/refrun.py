@@ -57,15 +57,19 @@ def _load(d):
     return out
 
 
+BINDING = os.path.join(HERE, "_ref", "joe_gpu_case")
+
+
 def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout: float = 600.0,
-        files: dict | None = None, collect: tuple = ()):
+        files: dict | None = None, collect: tuple = (), harness: str | None = None):
     """Write the mesh (``mesh_writer(path)``, may be None) and ``Joe.in`` into a
     temp directory, plus ``files`` (name -> bytes), run the harness there and
     return its dumps; the files named in ``collect`` that the run wrote (e.g.
     the restart.out runBackwardEuler leaves) come back as bytes in
     dumps["files"]."""
-    if not available():
-        raise FileNotFoundError("reference harness not built: make -C oracle ref REF=<the reference src directory>")
+    harness = harness or HARNESS
+    if not os.path.exists(harness):
+        raise FileNotFoundError("%s not built: make -C oracle ref binding REF=<the reference src directory>" % harness)
     with tempfile.TemporaryDirectory(prefix="joe_ref_") as d:
         if mesh_writer is not None:
             mesh_writer(os.path.join(d, "mesh.msh"))
@@ -76,7 +80,7 @@ def run(mesh_writer, joe_in: str, mode: str = "dump", run_kind: int = 0, timeout
             f.write(joe_in)
         out = os.path.join(d, "out")
         os.mkdir(out)
-        p = subprocess.run([HARNESS, "Joe.in", str(run_kind), mode, out], cwd=d,
+        p = subprocess.run([harness, "Joe.in", str(run_kind), mode, out], cwd=d,
                            capture_output=True, text=True, timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError("reference harness failed (%d):\n%s\n%s" % (

@@ -74,3 +74,49 @@ def test_converged_field_matches_reference(ref, form):
     assert l2rel(rho[m], ref["rho"]) <= 1e-8
     assert l2rel(rhou[m], ref["rhou"]) <= 1e-8
     assert l2rel(rhoE[m], ref["rhoE"]) <= 1e-8
+
+
+PLATE = os.path.join(os.path.dirname(__file__), "golden", "converged_plate_64x32x2.npz")
+
+
+def run_plate(g, prm, precision, jac_lag=1, max_steps=8000, chunk=200, drop=6e-10):
+    """From the uniform state until the L1 energy residual falls to `drop` x its peak (the
+    plate's residual is ~0 at the first step and grows before it falls)."""
+    j = solver.JoeGpu(g, prm, precision=precision, jac_lag=jac_lag)
+    rho0 = np.full(g.ncv, prm.RHO_INITIAL)
+    u0 = np.asarray(prm.U_INITIAL)
+    rhoE0 = np.full(g.ncv, prm.P_INITIAL / (prm.GAMMA - 1.0) + 0.5 * prm.RHO_INITIAL * float(u0 @ u0))
+    j.set_state(rho0, rho0[:, None] * u0[None, :], rhoE0)
+    hist = []
+    while len(hist) < max_steps:
+        hist.extend(j.runBackwardEuler(chunk))
+        e = np.array(hist)[:, 4]
+        if e[-1] <= drop * e.max():
+            break
+    st = j.get_state()
+    j.close()
+    return st, np.array(hist)
+
+
+# the laminar Roe / Sutherland plate (the plate benchmark's physics at 64x32x2) against the
+# reference's own steady state; any convergent linear solver reaches it, so the GPU forms use the
+# reference's BiCGSTAB (FP64) and the LINE relaxation (FP64 and mixed, the latter with a lagged Jacobian)
+@pytest.mark.parametrize("form", ["fp64_bcgstab", "fp64_line", "mixed_line", "mixed_line_lag5"])
+def test_converged_plate_matches_reference(form):
+    from scipy.spatial import cKDTree
+    from tests.golden.make_converged import plate_config
+    if not os.path.exists(PLATE):
+        pytest.fail("missing golden %s" % PLATE)
+    z = np.load(PLATE)
+    _, g, prm = plate_config()
+    if form != "fp64_bcgstab":
+        prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="LINE", LS_MAX_ITER=10)
+    precision = 1 if form.startswith("mixed") else 0
+    (rho, rhou, rhoE), hist = run_plate(g, prm, precision, jac_lag=5 if form.endswith("lag5") else 1)
+    e = hist[:, 4]
+    assert e[-1] <= 1e-9 * e.max(), (len(e), e[-1] / e.max())
+    dist, m = cKDTree(g.x_cv).query(z["x_cv"])
+    assert dist.max() < 1e-12
+    assert l2rel(rho[m], z["rho"]) <= 1e-8
+    assert l2rel(rhou[m], z["rhou"]) <= 1e-8
+    assert l2rel(rhoE[m], z["rhoE"]) <= 1e-8

@@ -119,7 +119,7 @@ typedef struct jg_params {
   int nscal;           /* transported scalars: 0 (laminar / inviscid), 1 (SA), 2 (SST) */
   int turb_model;      /* JG_TURB_*: with a model the case runs runBackwardEulerCoupled's
                           (5+nscal)^2 block system (JoeWithModels.cpp:4326-4611) */
-  int renumber;        /* JG_RENUMBER_*: the handle's own cell/face order (jg_create only) */
+  int renumber;        /* JG_RENUMBER_*: the handle's own cell/face order (a batch renumbers each case on its own) */
   int grad_scheme;     /* GRAD_RECONSTRUCTION SCHEME: JG_GRAD_* (the flow gradients of calcEulerFlux) */
   /* AUSMDV family (flux = JG_FLUX_AUSMDV; UgpWithCvCompFlow.h:198-234): */
   int ausm_type;       /* SPACE_INTEGRATION AUSMDV / AUSMV / AUSMD: JG_AUSM_* */

@@ -45,6 +45,21 @@ def case_specs(n, lo, hi, seed, sst_fraction=0.0):
     return specs
 
 
+def wall_stretch(ny, first=1.0e-6, height=1.0):
+    """Geometric ratio r of ny wall-normal rows over `height` whose first row is `first` high:
+    first = height (r - 1) / (r^ny - 1), by bisection (at most 1.1)"""
+    lo, hi = 1.0 + 1e-9, 1.1
+    if height * (hi - 1.0) / (hi ** ny - 1.0) >= first:
+        return hi
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if height * (mid - 1.0) / (mid ** ny - 1.0) > first:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
 def build_case(spec):
     from myjoe_b200 import case
     if spec.get("model") == "SST":
@@ -53,7 +68,7 @@ def build_case(spec):
         _, g, prm = case.sst_bump_case(spec["nx"], spec["ny"], spec["nz"], mach=spec["mach"],
                                        mu_ref=SST_MU_REF,
                                        aoa_deg=spec["aoa"], bump_h=spec["bump"], seed=spec["seed"],
-                                       stretch=spec.get("stretch", 1.1))
+                                       stretch=spec.get("stretch", wall_stretch(spec["ny"])))
         return g, prm
     _, g, prm = case.bump_case(spec["nx"], spec["ny"], spec["nz"], mach=spec["mach"], aoa_deg=spec["aoa"],
                                bump_h=spec["bump"], seed=spec["seed"], inlet=spec.get("inlet", "FARFIELD"))
@@ -76,10 +91,10 @@ def build_cases(specs, workers):
 class Group:
     """The cases of one model in one batch handle, with their progress."""
 
-    def __init__(self, name, idx, cases, precision):
+    def __init__(self, name, idx, cases, precision, jac_lag=1, renumber=0):
         from myjoe_b200 import case, solver
         self.name, self.idx = name, idx
-        self.b = solver.JoeGpuBatch(cases, precision=precision)
+        self.b = solver.JoeGpuBatch(cases, precision=precision, jac_lag=jac_lag, renumber=renumber)
         for k, (g, prm) in enumerate(cases):
             self.b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.0))
             if prm.TURB_MODEL != "NONE":
@@ -139,6 +154,8 @@ def main(argv=None):
     ap.add_argument("--max-steps", type=int, default=3000)
     ap.add_argument("--chunk", type=int, default=50)
     ap.add_argument("--workers", type=int, default=min(32, mp.cpu_count()))
+    ap.add_argument("--jac-lag", type=int, default=4, help="inviscid cases: flux Jacobian every k-th step")
+    ap.add_argument("--renumber", type=int, default=2, help="each case's cell order: 0 its own, 1 RCM, 2 RCM by colour")
     args = ap.parse_args(argv)
 
     specs = case_specs(args.cases, args.min_cells, args.max_cells, args.seed, args.sst_fraction)
@@ -163,7 +180,8 @@ def main(argv=None):
         cases = [(built[k][0], dataclasses.replace(built[k][1], LINEAR_SOLVER_NS=solver_name,
                                                    LS_MAX_ITER=args.sweeps, CFL=1.0, CFL_RAMP=r,
                                                    UNDER_RELAXATION=args.under_relax)) for k in idx]
-        gr = Group(model, idx, cases, precision)
+        gr = Group(model, idx, cases, precision, jac_lag=args.jac_lag if model == "EULER" else 1,
+                   renumber=args.renumber)
         gr.shape = None if args.no_autotune else gr.b.autotune(3)
         groups.append(gr)
     # the handles step concurrently: one host thread each (the C calls release the GIL)
@@ -202,7 +220,7 @@ def main(argv=None):
         "precision": args.precision, "solver": "%s x%d" % (args.solver, args.sweeps),
         "sst_solver": "%s x%d" % (args.sst_solver, args.sweeps), "drop": args.drop,
         "cfl_ramp": list(ramp), "sst_cfl_ramp": list(sst_ramp), "under_relax": args.under_relax,
-        "sst_fraction": args.sst_fraction,
+        "sst_fraction": args.sst_fraction, "jac_lag": args.jac_lag, "renumber": args.renumber,
         "cell_iters_per_s": cell_iters / wall, "wall_s": wall, "mesh_setup_s": t_mesh,
         "converged": nconv, "failed": int(sum(gr.failed.sum() for gr in groups)),
         "converged_solves_per_hour": nconv / wall * 3600.0,

@@ -84,6 +84,9 @@ struct jg_case {
   Renumbering rn;           // caller's id of each internal cell / face / nbocv entry (empty: same order)
   Lines lines{};            // BCGSTAB_LINELET lines (nlines 0 otherwise)
   int* d_cell_old = nullptr;  // rn.cell_old on the device (state staging)
+  // a renumbered batch: each case's caller-order id of its cells (case-local), host and device
+  std::vector<int> case_cell_old;
+  int* d_case_cell_old = nullptr;
 };
 
 // Rows between the handle's order and the caller's: an array of nblk blocks
@@ -904,7 +907,6 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (ncases <= 0 || !meshes || !out) return set_err(JG_ERR_ARG, "bad argument");
   *out = nullptr;
   RC(check_params(params));
-  if (params->renumber != JG_RENUMBER_NONE) return set_err(JG_ERR_ARG, "batched cases keep their own order");
   if (params->lin_solver == JG_LS_BCGSTAB || params->lin_solver == JG_LS_BCGSTAB_LINELET)
     return set_err(JG_ERR_ARG, "a batch relaxes with JACOBI, SGS or LUSGS (BiCGSTAB's dot products would couple the cases)");
   if (params->time_step_mode == JG_TS_CFL_MIN)
@@ -913,8 +915,33 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(JG_ERR_NODEVICE, "no CUDA device");
   MeshOwned cat;
   jg_case* h = new jg_case();
-  int rc = concat_meshes(ncases, meshes, cat, h->case_off, h->case_nfa_b_off);
-  if (rc == JG_OK) rc = build(h, &cat.m, params);
+  int rc = JG_OK;
+  if (params->renumber != JG_RENUMBER_NONE) {
+    // each case renumbered on its own (cells never leave their case), then concatenated; the
+    // case-local cell order of every case is kept for the per-case state and scalar calls
+    std::vector<MeshOwned> mo(ncases);
+    std::vector<jg_mesh> rm(ncases);
+    for (int k = 0; k < ncases && rc == JG_OK; k++) {
+      Renumbering r;
+      rc = renumber_mesh(meshes[k], params->renumber, mo[k], r);
+      if (rc == JG_OK) {
+        mo[k].bind();
+        rm[k] = mo[k].m;
+        h->case_cell_old.insert(h->case_cell_old.end(), r.cell_old.begin(), r.cell_old.end());
+      }
+    }
+    if (rc == JG_OK) rc = concat_meshes(ncases, rm.data(), cat, h->case_off, h->case_nfa_b_off);
+    if (rc == JG_OK) rc = build(h, &cat.m, params);
+    if (rc == JG_OK) {
+      const int* d = nullptr;
+      rc = upload(h, &d, h->case_cell_old.data(), h->case_cell_old.size());
+      h->d_case_cell_old = (int*)d;
+    }
+    if (rc == JG_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = set_err(JG_ERR_CUDA, "batch upload");
+  } else {
+    rc = concat_meshes(ncases, meshes, cat, h->case_off, h->case_nfa_b_off);
+    if (rc == JG_OK) rc = build(h, &cat.m, params);
+  }
   if (rc != JG_OK) {
     std::string keep = g_err;
     jg_destroy(h);
@@ -940,7 +967,8 @@ int jg_batch_set_state(jg_case_t* h, int k, const double* rho, const double* rho
   CK(cudaMemcpyAsync(h->d_io, rho, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + n, rhou, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * n, rhoE, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  launch_pack_state((int)n, h->d_io, h->st.q + 5 * c0, nullptr, h->stream);
+  launch_pack_state((int)n, h->d_io, h->st.q + 5 * c0, h->d_case_cell_old ? h->d_case_cell_old + c0 : nullptr,
+                    h->stream);
   CK(cudaMemsetAsync(h->st.prim + 8 * c0, 0, 8 * n * sizeof(double), h->stream));
   CKL();
   // the state/BC preamble runs at the next operator call, once every case has its state
@@ -952,7 +980,8 @@ int jg_batch_get_state(jg_case_t* h, int k, double* rho, double* rhou, double* r
   if (!h || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
   const size_t N = h->ncv, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
   if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
-  launch_unpack_state((int)n, h->st.q + 5 * c0, h->d_io, nullptr, h->stream);
+  launch_unpack_state((int)n, h->st.q + 5 * c0, h->d_io, h->d_case_cell_old ? h->d_case_cell_old + c0 : nullptr,
+                      h->stream);
   CKL();
   if (rho) CK(cudaMemcpyAsync(rho, h->d_io, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -965,9 +994,10 @@ int jg_batch_set_scalars(jg_case_t* h, int k, const double* phi) {
   if (!h || !phi || k < 0 || k >= h->ncases) return set_err(JG_ERR_ARG, "bad argument");
   if (h->bs == 5) return set_err(JG_ERR_ARG, "the batch transports no scalar");
   const size_t N = h->ncv, ns = h->turb.ns, n = h->case_off[k + 1] - h->case_off[k], c0 = h->case_off[k];
-  std::vector<double> cm(ns * n);  // [n][ns] -> [ns][n]
+  std::vector<double> cm(ns * n);  // [n][ns] -> [ns][n], in the batch's cell order
+  const int* perm = h->case_cell_old.empty() ? nullptr : h->case_cell_old.data() + c0;
   for (size_t c = 0; c < n; c++)
-    for (size_t q = 0; q < ns; q++) cm[q * n + c] = phi[ns * c + q];
+    for (size_t q = 0; q < ns; q++) cm[q * n + c] = phi[ns * (perm ? (size_t)perm[c] : c) + q];
   for (size_t q = 0; q < ns; q++)
     CK(cudaMemcpyAsync(h->turb.phi + q * N + c0, cm.data() + q * n, n * sizeof(double), cudaMemcpyHostToDevice,
                        h->stream));
@@ -985,8 +1015,9 @@ int jg_batch_get_scalars(jg_case_t* h, int k, double* phi) {
     CK(cudaMemcpyAsync(cm.data() + q * n, h->turb.phi + q * N + c0, n * sizeof(double), cudaMemcpyDeviceToHost,
                        h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  const int* perm = h->case_cell_old.empty() ? nullptr : h->case_cell_old.data() + c0;
   for (size_t c = 0; c < n; c++)
-    for (size_t q = 0; q < ns; q++) phi[ns * c + q] = cm[q * n + c];
+    for (size_t q = 0; q < ns; q++) phi[ns * (perm ? (size_t)perm[c] : c) + q] = cm[q * n + c];
   return JG_OK;
 }
 

@@ -750,7 +750,7 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
   extern __shared__ double sD[];  // [BB][blockDim.x]
   const int tid = threadIdx.x, bd = blockDim.x;
   const int c = blockIdx.x * bd + tid;
-  if (c >= m.ncv) return;
+  if (c >= m.ncv || !st.case_active[m.case_of[c]]) return;  // a frozen case keeps its arrays
   const int N = m.ncv, nf = m.nfa;
   const bool only_p = p.symm_bc == JG_SYMM_ANALYTICAL;
   double rhs[B];
@@ -1016,7 +1016,7 @@ __global__ void __launch_bounds__(B * 32) k_jacobi_c(Mesh m, State st, const BT*
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
   const int slice = blockIdx.x;
   const int c = slice * SLICE + lane;
-  const bool active = c < m.ncv;
+  const bool active = c < m.ncv && st.case_active[m.case_of[c]];
   const int N = m.ncv;
   BT acc = active ? (BT)st.b[(size_t)B * c + row] : (BT)0;
   if (!first && active) {
@@ -1046,7 +1046,7 @@ __global__ void __launch_bounds__(B * 32) k_gs_c(Mesh m, State st, BT* __restric
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
   const int slice = slices ? slices[blockIdx.x] : blockIdx.x;  // slices: those holding this colour
   const int c = slice * SLICE + lane;
-  const bool active = c < m.ncv && m.color[c] == color;
+  const bool active = c < m.ncv && m.color[c] == color && st.case_active[m.case_of[c]];
   const int N = m.ncv;
   BT acc = 0;
   if (active) {

@@ -55,7 +55,7 @@ template <int KIND, int VISC, int FL>
 __global__ void __launch_bounds__(TB) k_res(Mesh m, Params p, State st, int for_step) {
   const int t = threadIdx.x, lane = t % FL;
   const int c = blockIdx.x * (TB / FL) + t / FL;
-  const bool active = c < m.ncv;
+  const bool active = c < m.ncv && st.case_active[m.case_of[c]];  // a frozen case keeps its arrays
   double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const int k0 = active ? m.slot_i[c] : 0, k1 = active ? m.slot_i[c + 1] : 0;
   for (int k = k0 + lane; k < k1; k += FL) {
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(TB, jac_min_blocks<BT, KIND>()) k_jac(Mesh m, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x;
   const int c = blockIdx.x * TB + t;
-  if (c >= m.ncv) return;
+  if (c >= m.ncv || !st.case_active[m.case_of[c]]) return;
   if (sched && !jac_due(st, m.case_of[c])) return;
   JT* sd = reinterpret_cast<JT*>(smem_raw) + t;  // this cell's diagonal block: entry e at sd[e * TB]
   for (int e = 0; e < 25; e++) sd[e * TB] = JT(0);
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(TB, jac_min_blocks<BT, KIND>()) k_jac(Mesh m, 
 template <typename BT>
 __global__ void __launch_bounds__(TB) k_diag(Mesh m, State st) {
   const int c = blockIdx.x * TB + threadIdx.x;
-  if (c >= m.ncv) return;
+  if (c >= m.ncv || !st.case_active[m.case_of[c]]) return;
   if (jac_due(st, m.case_of[c])) return;  // k_jac formed this case's blocks at this step
   const int N = m.ncv;
   const BT* D0 = (const BT*)st.D0;

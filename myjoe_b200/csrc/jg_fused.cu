@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, 
   const int t = threadIdx.x, bd = blockDim.x;
   const int lane = t % CL;
   int c = blockIdx.x * (bd / CL) + t / CL;
-  bool active = c < m.ncv;
+  bool active = c < m.ncv && st.case_active[m.case_of[c]];
   double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (active) {
     for (int e = 0; e < 25; e++) sD[e * bd + t] = JT(0);

@@ -212,7 +212,7 @@ __global__ void k_dt(Mesh m, Params p, State st, int use_ctrl, double cfl_arg) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   double dtc = 1.0e20;
   double cfl = use_ctrl ? st.ctrl[0] : cfl_arg;
-  if (c < m.ncv) {
+  if (c < m.ncv && st.case_active[m.case_of[c]]) {
     if (p.ts_mode == JG_TS_DT) {
       dtc = p.dt_fixed;
     } else {
@@ -394,7 +394,7 @@ template <int SCHEME>
 __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, int visc_lim_u, int visc_lim_h,
                        int separate_guv) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.ncv) return;
+  if (c >= m.ncv || !st.case_active[m.case_of[c]]) return;  // a frozen case keeps its arrays
   const double* pc = &st.prim[8 * c];
   double rc = st.q[5 * c];
   // raw LSQ sums: diagonal, neighbours (nbocv order), then boundary faces
@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(160) k_jacobi2(Mesh m, State st, const BT* __r
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
   const int slice = blockIdx.x;
   const int c = slice * SLICE + lane;
-  const bool active = c < m.ncv;
+  const bool active = c < m.ncv && st.case_active[m.case_of[c]];
   const int N = m.ncv;
   BT acc = active ? (BT)st.b[5 * c + row] : (BT)0;
   if (!first && active) {
@@ -749,7 +749,7 @@ template <typename BT>
 __global__ void __launch_bounds__(128) k_jacobi(Mesh m, State st, const BT* __restrict__ xin, BT* __restrict__ xout,
                                                 int first) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.ncv) return;
+  if (c >= m.ncv || !st.case_active[m.case_of[c]]) return;
   const int N = m.ncv;
   BT acc[5];
   for (int i = 0; i < 5; i++) acc[i] = (BT)st.b[5 * c + i];
@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(160) k_gs2(Mesh m, State st, BT* __restrict__ 
   const int row = threadIdx.x / SLICE, lane = threadIdx.x % SLICE;
   const int slice = slices ? slices[blockIdx.x] : blockIdx.x;
   const int c = slice * SLICE + lane;
-  const bool active = c < m.ncv && m.color[c] == color;
+  const bool active = c < m.ncv && m.color[c] == color && st.case_active[m.case_of[c]];
   const int N = m.ncv;
   BT acc = 0;
   if (active) {

@@ -15,8 +15,9 @@ drop of its energy residual.
 Two arms see the same arrival stream:
 
 * ``serve``: the serving form -- mixed precision (FP32 Jacobian and
-  relaxation inside FP64 defect correction), up to ``--max-resident`` cases on
-  the device at once, admitted by device-memory footprint (jg_serve_*);
+  relaxation inside FP64 defect correction) with the flux Jacobian formed every
+  ``--jac-lag``-th step, up to ``--max-resident`` cases on the device at once,
+  admitted by device-memory footprint (jg_serve_*);
 * ``serve-smallest``: the same, admitting the smallest queued footprint first;
 * ``plain``: the plain FP64 GPU path, one case at a time in arrival order
   (the same server with one resident case and FP64 throughout).
@@ -186,7 +187,8 @@ def run_arm(arm, stream, args):
                 break       # the client is still building this mesh: keep the device busy meanwhile
             g, prm, state = pending.popleft().get()
             top_up()
-            srv.submit(g, solver_params(prm, args), state, precision=precision, t_arrival=t0 + stream[nxt]["t"])
+            srv.submit(g, solver_params(prm, args), state, precision=precision, t_arrival=t0 + stream[nxt]["t"],
+                       jac_lag=args.jac_lag if serving else 1, renumber=args.renumber)
             nxt += 1
             st["queued"] += 1
         for r in srv.poll(max_wait=0.02):
@@ -217,6 +219,7 @@ def run_arm(arm, stream, args):
         "steps_to_converge_p50": pct([r["conv_step"] for r in conv], 50),
         "cell_iters_per_s": cell_iters / horizon,
         "drop": args.drop, "solver": "SGS x%d" % args.sweeps, "cfl_ramp": args.cfl_ramp,
+        "jac_lag": args.jac_lag if serving else 1, "renumber": args.renumber,
         "cells": [args.min_cells, args.max_cells],
     }
 
@@ -243,6 +246,8 @@ def main(argv=None):
                     help="retire a case whose best residual drop has not halved in this many steps (0: off)")
     ap.add_argument("--workers", type=int, default=min(32, mp.cpu_count()))
     ap.add_argument("--lookahead", type=int, default=48, help="mesh builds in flight")
+    ap.add_argument("--jac-lag", type=int, default=4, help="serving arms: flux Jacobian every k-th step")
+    ap.add_argument("--renumber", type=int, default=2, help="cell order of every arm (0 none, 1 RCM, 2 RCM by colour)")
     args = ap.parse_args(argv)
 
     from myjoe_b200 import build

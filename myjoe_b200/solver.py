@@ -358,12 +358,12 @@ class JoeGpuBatch(JoeGpu):
     and each brings its own boundary values.  Cases whose shared settings
     differ (two fluids, say) are refused."""
 
-    def __init__(self, cases, precision: int = 0, jac_lag: int = 1):
+    def __init__(self, cases, precision: int = 0, jac_lag: int = 1, renumber: int = 0):
         self.params = cases[0][1]
         self.mas = [MeshArrays(m, p) for m, p in cases]
-        self.jp = make_params(self.params, precision, jac_lag=jac_lag)
+        self.jp = make_params(self.params, precision, renumber, jac_lag)
         for k, (_, prm) in enumerate(cases[1:], 1):
-            q = make_params(prm, precision, jac_lag=jac_lag)
+            q = make_params(prm, precision, renumber, jac_lag)
             diff = [f for f, _ in jg_params._fields_ if getattr(q, f) != getattr(self.jp, f)]
             if diff:
                 raise ValueError("case %d differs from case 0 in the batch-wide settings %s" % (k, diff))

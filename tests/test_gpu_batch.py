@@ -168,3 +168,53 @@ def test_batch_refuses_a_coupling_time_step_mode_after_creation():
     r = b.runBackwardEulerCases(2)
     assert np.all(np.isfinite(r))
     b.close()
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_renumbered_batch_is_bitwise_equal_to_renumbered_alone(method):
+    """A batch renumbers each case on its own (RCM, or RCM grouped by colour):
+    each case's state and residual history equal the same case renumbered on
+    its own handle, and states come back in the caller's cell order."""
+    cs = cases()
+    nsteps = 10
+    alone = []
+    for g, prm in cs:
+        j = solver.JoeGpu(g, prm, precision=1, renumber=method)
+        j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
+        r = j.runBackwardEuler(nsteps)
+        alone.append((j.get_state(), r))
+        j.close()
+    b = solver.JoeGpuBatch(cs, precision=1, renumber=method)
+    for k, (g, prm) in enumerate(cs):
+        b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
+    rb = b.runBackwardEulerCases(nsteps)
+    for k in range(len(cs)):
+        for x, y in zip(b.get_case_state(k), alone[k][0]):
+            np.testing.assert_array_equal(x, y)
+        np.testing.assert_array_equal(rb[:, k, :], alone[k][1])
+    b.close()
+
+
+def test_renumbered_turbulence_batch_scalars_in_caller_order():
+    """SST cases renumbered inside a batch: scalars go in and come out in each
+    case's own cell order, and equal the same case renumbered alone."""
+    cs = turb_cases("sst")
+    nsteps = 6
+    alone = []
+    for g, prm in cs:
+        j = solver.JoeGpu(g, prm, renumber=1)
+        j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
+        j.set_scalars(_phi0(g, prm))
+        j.runBackwardEuler(nsteps)
+        alone.append((j.get_state(), np.asarray(j.get_scalars()).reshape(g.ncv, -1)))
+        j.close()
+    b = solver.JoeGpuBatch(cs, renumber=1)
+    for k, (g, prm) in enumerate(cs):
+        b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
+        b.set_case_scalars(k, _phi0(g, prm))
+    b.runBackwardEulerCases(nsteps)
+    for k in range(len(cs)):
+        for x, y in zip(b.get_case_state(k), alone[k][0]):
+            np.testing.assert_array_equal(x, y)
+        np.testing.assert_array_equal(np.asarray(b.get_case_scalars(k)).reshape(alone[k][1].shape), alone[k][1])
+    b.close()

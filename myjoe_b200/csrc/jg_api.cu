@@ -1416,8 +1416,7 @@ static int enqueue_step_coupled(jg_case* h) {
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
   launch_update6(h->m, h->p, h->st, h->turb, (sgs || sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
   launch_state(h->m, h->p, h->st, S);
-  launch_face_props(h->m, h->p, h->st, S);
-  launch_bc(h->m, h->p, h->st, S);
+  launch_faces_after_update(h->m, h->p, h->st, S);
   launch_scalar_bc(h->m, h->p, h->st, h->turb, S);
   launch_turb_props(h->m, h->p, h->st, h->turb, S);
   CKL();
@@ -1436,20 +1435,24 @@ static int enqueue_step(jg_case* h, int for_graph) {
   launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, S);
   int solver = h->hp.lin_solver;
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
+  // the relaxation's result (x, [5][N]); the update reads it directly
+  const void* x = nullptr;
+  int x_fp32 = h->p.fp32;
   if (solver == JG_LS_LUSGS) {
     launch_lusgs(h->m, h->p, h->st, S);
-    launch_dq_from_x(h->m, h->p, h->st, h->st.x1, S);
+    x = h->st.x1;
+    x_fp32 = 0;  // LU-SGS is FP64
   } else if (solver == JG_LS_JACOBI) {
     int sweeps = std::max(1, h->hp.ls_max_iter);
     launch_jacobi(h->m, h->p, h->st, sweeps, S);
-    launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
+    x = (sweeps % 2 == 1) ? h->st.x0 : h->st.x1;
   } else if (solver == JG_LS_SGS) {
     launch_sgs(h->m, h->p, h->st, std::max(1, h->hp.ls_max_iter), S);
-    launch_dq_from_x(h->m, h->p, h->st, h->st.x0, S);
+    x = h->st.x0;
   } else if (solver == JG_LS_LINE) {
     int sweeps = std::max(1, h->hp.ls_max_iter);
     launch_line_relax(h->m, h->p, h->st, h->lines, 5, sweeps, S);
-    launch_dq_from_x(h->m, h->p, h->st, (sweeps % 2 == 1) ? h->st.x0 : h->st.x1, S);
+    x = (sweeps % 2 == 1) ? h->st.x0 : h->st.x1;
   } else {
     if (for_graph) return set_err(JG_ERR_ARG, "BCGSTAB is not captured");
     // host-driven BiCGSTAB on the assembled system, zero initial guess; the rhs ([N][5] in st.b) as [5][N]
@@ -1460,12 +1463,12 @@ static int enqueue_step(jg_case* h, int for_graph) {
     launch_aos_to_soa5(h->ncv, h->st.b, b, S);
     int it;
     RC(bcgstab(h, phi, b, h->hp.ls_abs, h->hp.ls_rel, h->hp.ls_max_iter, &it, solver == JG_LS_BCGSTAB_LINELET));
-    launch_dq_from_x(h->m, h->p, h->st, phi, S);
+    x = phi;
+    x_fp32 = 0;  // BiCGSTAB is FP64
   }
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
-  launch_update_state(h->m, h->p, h->st, S);
-  launch_face_props(h->m, h->p, h->st, S);
-  launch_bc(h->m, h->p, h->st, S);
+  launch_update_state_x(h->m, h->p, h->st, x, x_fp32, S);
+  launch_faces_after_update(h->m, h->p, h->st, S);
   CKL();
   return JG_OK;
 }

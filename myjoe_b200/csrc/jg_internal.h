@@ -167,6 +167,10 @@ void launch_hist_base(State& st, cudaStream_t s);
 // in[13]: S0, S1, gu0, gu1, gh0, gh1, mul, lamOcp, u_fa, area, nvec, svec, smag (device arrays)
 void launch_visc_faces(int n, const double* const* in, double* F, double* A0, double* A1, cudaStream_t s);
 void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+// the update from the relaxation's result x ([5][N], FP32 when x_fp32) without the dq copy
+void launch_update_state_x(const Mesh& m, const Params& p, State& st, const void* x, int x_fp32, cudaStream_t s);
+// launch_bc and launch_face_props in one launch
+void launch_faces_after_update(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_bc(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_ctrl_step(const Params& p, State& st, cudaStream_t s);

@@ -74,10 +74,23 @@ __global__ void k_update_state(Mesh m, Params p, State st) {
   for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
 }
 
+// the same with the relaxation's result x ([5][N], matrix precision) in place of dq = (double) x
+template <typename BT>
+__global__ void k_update_state_x(Mesh m, Params p, State st, const BT* __restrict__ x) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ncv) return;
+  int k = m.case_of[c];
+  if (!st.case_active[k]) return;
+  double q[5], prim[8];
+  for (int i = 0; i < 5; i++) q[i] = st.q[5 * c + i] + (double)x[(size_t)i * m.ncv + c];
+  for (int i = 0; i < 5; i++) st.q[5 * c + i] = q[i];
+  for (int i = 0; i < 8; i++) prim[i] = st.prim[8 * c + i];
+  state_from_q(p, q, prim, st.case_err + k);
+  for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
+}
+
 // calcMaterialProperties on internal faces: distance-weighted face temperature
-__global__ void k_face_props(Mesh m, Params p, State st) {
-  int f = m.nfa_b + blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= m.nfa) return;
+__device__ __forceinline__ void face_props(const Mesh& m, const Params& p, State& st, int f) {
   int c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
   double d0[3], d1[3];
   for (int i = 0; i < 3; i++) {
@@ -90,12 +103,15 @@ __global__ void k_face_props(Mesh m, Params p, State st) {
   st.mul_fa[f] = mu;
   st.lam_fa[f] = mu / p.Pr;
 }
+__global__ void k_face_props(Mesh m, Params p, State st) {
+  int f = m.nfa_b + blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nfa) return;
+  face_props(m, p, st, f);
+}
 
 // setBC + ComputeBCProperties_T/H + the EOS density, JoeWithModels.cpp:3857-4300,
-// UgpWithCvCompFlow.h:1783-1839.  One thread per boundary face.
-__global__ void k_bc(Mesh m, Params p, State st) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= m.nfa_b) return;
+// UgpWithCvCompFlow.h:1783-1839, for boundary face f.
+__device__ __forceinline__ void bc_face(const Mesh& m, const Params& p, State& st, int f) {
   const DevZone z = m.zones[m.bzone[f]];
   int c0 = m.cvofa[2 * f];
   const double* pc = &st.prim[8 * c0];
@@ -195,6 +211,19 @@ __global__ void k_bc(Mesh m, Params p, State st) {
     st.mul_fa[f] = mu;
     st.lam_fa[f] = mu / p.Pr;
   }
+}
+// one thread per boundary face
+__global__ void k_bc(Mesh m, Params p, State st) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nfa_b) return;
+  bc_face(m, p, st, f);
+}
+// both passes that follow a state update in one launch: boundary faces take setBC, internal
+// faces (viscous cases) the face properties; the faces are independent
+__global__ void k_faces_after_update(Mesh m, Params p, State st) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < m.nfa_b) bc_face(m, p, st, f);
+  else if (p.viscous && f < m.nfa) face_props(m, p, st, f);
 }
 
 // CFL ramp of runBackwardEuler (JoeWithModels.cpp:977-978), on the device so a
@@ -1040,6 +1069,14 @@ void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
 void launch_update_state(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   k_update_state<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
 }
+void launch_update_state_x(const Mesh& m, const Params& p, State& st, const void* x, int x_fp32, cudaStream_t s) {
+  if (x_fp32) k_update_state_x<float><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, (const float*)x);
+  else k_update_state_x<double><<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st, (const double*)x);
+}
+void launch_faces_after_update(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
+  const int n = p.viscous ? m.nfa : m.nfa_b;
+  if (n > 0) k_faces_after_update<<<grid_for(n, TB), TB, 0, s>>>(m, p, st);
+}
 void launch_face_props(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   if (!p.viscous || m.nfa == m.nfa_b) return;
   k_face_props<<<grid_for(m.nfa - m.nfa_b, TB), TB, 0, s>>>(m, p, st);
@@ -1055,7 +1092,8 @@ void launch_hist_base(State& st, cudaStream_t s) { k_hist_base<<<1, 1, 0, s>>>(s
 void launch_dt(const Mesh& m, const Params& p, State& st, int use_ctrl, double cfl, cudaStream_t s) {
   int nb = grid_for(m.ncv, 256);
   k_dt<<<nb, 256, 0, s>>>(m, p, st, use_ctrl, cfl);
-  k_dt_final<<<1, 256, 0, s>>>(m, p, st, nb);
+  // the minimum over the cells: asked for by jg_calc_dt and by CFL_MIN; a step needs it only then
+  if (!use_ctrl || p.ts_mode == JG_TS_CFL_MIN) k_dt_final<<<1, 256, 0, s>>>(m, p, st, nb);
   if (p.ts_mode == JG_TS_CFL_MIN) k_dt_min_all<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, st);
 }
 static void launch_grad_k(const Mesh& m, const Params& p, State& st, int do_euler, int do_visc, int lim_u, int lim_h,

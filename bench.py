@@ -366,7 +366,6 @@ def main():
         tuned_cl = int(args.face_loop)
         j.set_launch_config(tuned_cl, tuned_sweep)
     j.set_state(*st0)
-    j.set_profiling(True)
     kernels_per_step = j.step_kernel_count()
     stream = torch.cuda.ExternalStream(j.stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -377,7 +376,6 @@ def main():
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    face_ms, solve_ms = [], []
     clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
@@ -387,15 +385,27 @@ def main():
             starts[k].record(stream)
             j.step_async(1)
             ends[k].record(stream)
-        prof = j.profile()
-        face_ms.append(prof["face_loop_ms"])
-        solve_ms.append(prof["linear_solve_ms"])
-        with torch.cuda.stream(stream):
             flush.add_(1.0)   # > L2: evict the case before the next timed step
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # the face loop and the relaxation, from CUDA events inside the step graph, over a second pass
+    # of the same K steps under the same L2 flush: event nodes between the kernels lengthen a step
+    # (they split the graph's launch stream), so the timed steps above run without them
+    face_ms, solve_ms = [], []
+    j.set_profiling(True)
+    j.step_async(2)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            j.step_async(1)
+        prof = j.profile()
+        face_ms.append(prof["face_loop_ms"])
+        solve_ms.append(prof["linear_solve_ms"])
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)
+    torch.cuda.synchronize()
+    j.set_profiling(False)
     total_s = sum(step_ms) / 1000.0
     if world > 1:
         t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
@@ -487,6 +497,8 @@ def main():
                "bytes_per_cell": face_b, "launch_ms": face_avg}
         other = {"kernel": "k_jacobi (block point-relaxation sweep)", "achieved": sweep_gbs, "frac": sweep_gbs / peak,
                  "bytes_per_cell": sweep_b, "launch_ms": sweep_avg}
+    dom["launch_ms_source"] = ("CUDA events inside the step graph, averaged over a second pass of the same "
+                               "steps (the timed steps run without the event nodes)")
     dom["peak_source"] = peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind
     prof_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof_path):

@@ -77,6 +77,10 @@ struct jg_case {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t graph_kernels = 0;
   double* d_io = nullptr;   // [5][N] staging for direct host<->device state copies
+  // pinned host staging for the error flags and a call's residual history: the reads of a call
+  // are asynchronous copies that one synchronisation completes
+  void* hpin = nullptr;
+  size_t hpin_bytes = 0;
   int async_alloc = 0;      // stream-ordered allocation (serving): no device-wide sync on free
   size_t bytes = 0;         // device bytes held by this handle
   int bs = 5;               // block size: 5, or 6 on the coupled SA path
@@ -273,7 +277,9 @@ static int check_params(const jg_params* q) {
     if (q->nscal != (q->turb_model == JG_TURB_SA ? 1 : 2))
       return set_err(JG_ERR_ARG, "SA transports one scalar (nscal = 1), SST two (nscal = 2)");
     if (!(q->mu_ref > 0.0)) return set_err(JG_ERR_ARG, "a turbulence model needs a viscous case (mu_ref > 0)");
-    if (q->flux != JG_FLUX_HLLC) return set_err(JG_ERR_ARG, "the coupled path uses the HLLC flux");
+    // calcFluxCoupled's flux choices (JoeWithModels.cpp:4987-5057)
+    if (q->flux != JG_FLUX_HLLC && q->flux != JG_FLUX_AUSMDV && q->flux != JG_FLUX_HAENEL)
+      return set_err(JG_ERR_ARG, "the coupled path takes the HLLC, AUSMDV (AUSMV, AUSMD) or HAENEL flux");
     if (q->lin_solver != JG_LS_JACOBI && q->lin_solver != JG_LS_SGS && q->lin_solver != JG_LS_LINE)
       return set_err(JG_ERR_ARG, "the coupled path relaxes with JACOBI, SGS or LINE sweeps");
   } else if (q->turb_model != JG_TURB_NONE) {
@@ -334,6 +340,9 @@ int jg_destroy(jg_case_t* h) {
   if (h->st.aux) cudaStreamDestroy(h->st.aux);
   if (h->st.ev_fork) cudaEventDestroy(h->st.ev_fork);
   if (h->st.ev_join) cudaEventDestroy(h->st.ev_join);
+  if (h->hpin) cudaFreeHost(h->hpin);
+  if (h->st.ev_pre) cudaEventDestroy(h->st.ev_pre);
+  if (h->st.ev_dt) cudaEventDestroy(h->st.ev_dt);
   delete h;
   return JG_OK;
 }
@@ -390,10 +399,13 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   const int N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b;
   if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   if (q->turb_model == JG_TURB_NONE && !h->st.aux) {
-    // the face loop's Jacobian kernel runs beside its residual kernel on a second stream
+    // the face loop's Jacobian kernel runs beside its residual kernel on a second stream, and
+    // the time step beside the gradients
     CK(cudaStreamCreateWithFlags(&h->st.aux, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->st.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->st.ev_join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->st.ev_pre, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->st.ev_dt, cudaEventDisableTiming));
   }
   h->ncv = N;
   h->nfa = nfa;
@@ -1030,14 +1042,38 @@ int jg_get_stream(jg_case_t* h, void** stream) {
 // The handle's error flags.  Per-case state errors count for a single case,
 // and for every case of a batch with all_cases (the preamble: a bad input
 // state); during batch steps they stay per case (jg_batch_status).
-static int check_err_flags(jg_case* h, bool all_cases = false) {
-  int e = 0, ec = 0;
+// the handle's pinned staging area, at least `bytes` long (grown on demand; every call that
+// copies into it synchronises before it returns, so no copy into an old area is in flight)
+static int pinned(jg_case* h, size_t bytes, void** out) {
+  if (bytes > h->hpin_bytes) {
+    if (h->hpin) CK(cudaFreeHost(h->hpin));
+    h->hpin = nullptr;
+    h->hpin_bytes = 0;
+    const size_t b = std::max<size_t>(bytes, 4096);
+    CK(cudaHostAlloc(&h->hpin, b, cudaHostAllocDefault));
+    h->hpin_bytes = b;
+  }
+  *out = h->hpin;
+  return JG_OK;
+}
+
+// Reads (and clears) the error flags; with nres > 0 also copies nres doubles from the device
+// array dres to res_out, in the same synchronisation (the copy is made whatever the flags say).
+static int check_err_flags(jg_case* h, bool all_cases = false, const double* dres = nullptr, size_t nres = 0,
+                           double* res_out = nullptr) {
   const int nc = (h->ncases == 1 || all_cases) ? h->ncases : 0;
-  std::vector<int> ce(std::max(nc, 1), 0);
-  CK(cudaMemcpyAsync(&e, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  if (nc) CK(cudaMemcpyAsync(ce.data(), h->st.case_err, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  const size_t off = (sizeof(int) * (1 + (size_t)nc) + 15) & ~(size_t)15;
+  void* hp = nullptr;
+  RC(pinned(h, off + nres * sizeof(double), &hp));
+  int* hi = (int*)hp;
+  double* hr = (double*)((char*)hp + off);
+  CK(cudaMemcpyAsync(hi, h->st.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (nc) CK(cudaMemcpyAsync(hi + 1, h->st.case_err, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (nres) CK(cudaMemcpyAsync(hr, dres, nres * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int k = 0; k < nc; k++) ec |= ce[k];
+  if (nres) memcpy(res_out, hr, nres * sizeof(double));
+  int e = hi[0], ec = 0;
+  for (int k = 0; k < nc; k++) ec |= hi[1 + k];
   if (ec) {
     CK(cudaMemsetAsync(h->st.case_err, 0, nc * sizeof(int), h->stream));
     e |= ec;
@@ -1056,11 +1092,13 @@ static int prime(jg_case* h) {
   // a new state: every case forms its Jacobian blocks at its next step
   if (h->st.jac_next) CK(cudaMemsetAsync(h->st.jac_next, 0, sizeof(long long) * h->ncases, h->stream));
   launch_state(h->m, h->p, h->st, h->stream);
-  launch_face_props(h->m, h->p, h->st, h->stream);
-  launch_bc(h->m, h->p, h->st, h->stream);
   if (h->bs > 5) {
+    launch_face_props(h->m, h->p, h->st, h->stream);
+    launch_bc(h->m, h->p, h->st, h->stream);
     launch_scalar_bc(h->m, h->p, h->st, h->turb, h->stream);
     launch_turb_props(h->m, h->p, h->st, h->turb, h->stream);
+  } else {
+    launch_faces_after_update(h->m, h->p, h->st, h->stream);  // setBC and the face properties, one launch
   }
   CKL();
   h->primed = 1;
@@ -1427,8 +1465,20 @@ static int enqueue_step(jg_case* h, int for_graph) {
   if (h->bs > 5) return enqueue_step_coupled(h);
   cudaStream_t S = h->stream;
   launch_ctrl_step(h->p, h->st, S);
-  launch_dt(h->m, h->p, h->st, 1, 0.0, S);
+  // calcDt on the second stream beside the gradients: neither reads what the other writes.  The
+  // split face loop's Jacobian kernel follows it on that stream (the join brings both back);
+  // the fused face loop waits for it here.
+  const bool dt_aside = h->st.aux && h->st.ev_pre && h->st.ev_dt;
+  if (dt_aside) {
+    CK(cudaEventRecord(h->st.ev_pre, S));
+    CK(cudaStreamWaitEvent(h->st.aux, h->st.ev_pre, 0));
+    launch_dt(h->m, h->p, h->st, 1, 0.0, h->st.aux);
+    CK(cudaEventRecord(h->st.ev_dt, h->st.aux));
+  } else {
+    launch_dt(h->m, h->p, h->st, 1, 0.0, S);
+  }
   launch_grad(h->m, h->p, h->st, S);
+  if (dt_aside && !flux_split(h->p, h->st)) CK(cudaStreamWaitEvent(S, h->st.ev_dt, 0));
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
   launch_flux(h->m, h->p, h->st, 1, 1, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
@@ -1528,10 +1578,7 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   CKL();
   // a single case's residual history rides on the error-flag read's synchronisation
   const bool direct = resid && nsteps > 0 && h->ncases == 1;
-  if (direct)
-    CK(cudaMemcpyAsync(resid, h->st.resid, h->bs * (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost,
-                       h->stream));
-  RC(check_err_flags(h));
+  RC(check_err_flags(h, false, direct ? h->st.resid : nullptr, direct ? h->bs * (size_t)nsteps : 0, resid));
   if (resid && nsteps > 0 && !direct) {
     {
       // the sum over the cases of the batch, per step

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "jg_cell.cuh"
 #include "jg_flux.cuh"
 #include "jg_internal.h"
 
@@ -517,6 +518,157 @@ __device__ void matrices_hllc_c(double* AL, double* AR, const CState<NS>& L, con
 }
 
 // ---------------------------------------------------------------------------
+// coupled AUSMDV / AUSMV / AUSMD and Haenel & Schwane (UgpWithCvCompFlow.cpp:2293-3036;
+// ConvTerm = 1, dp/dscal = 0): the flow part is the segregated scheme of jg_flux.cuh with the
+// state's k in the total enthalpy; the scalars ride on the mass flux of the upwind side (AUSMDV,
+// with the entropy fix acting on them as on the density) or of each split part (HAENEL).
+// fo: the face's AUSMDV options (FO_*); haenel: the Haenel & Schwane scheme (SPACE_INTEGRATION
+// HAENEL, or AUSMDV's HAENEL shock fix on this face)
+// ---------------------------------------------------------------------------
+template <int NS>
+__device__ __forceinline__ FState fstate_c(const CState<NS>& s) {
+  FState f;
+  f.rho = s.rho;
+  for (int i = 0; i < 3; i++) f.u[i] = s.u[i];
+  f.p = s.p;
+  f.gam = s.gam;
+  f.h = s.h + s.k;
+  return f;
+}
+
+template <int NS>
+__device__ void flux_ausm_c(double* F, const CState<NS>& L, const CState<NS>& R, double area, const double* nV,
+                            bool only_p, bool haenel, int fo) {
+  if (only_p) {
+    flux_hllc_c<NS>(F, L, R, area, nV, true);  // the same pressure-only flux
+    return;
+  }
+  const FState fL = fstate_c(L), fR = fstate_c(R);
+  double F5[5];
+  const double unL = dot3(L.u, nV), cL = sqrt(L.gam * L.p / L.rho);
+  const double unR = dot3(R.u, nV), cR = sqrt(R.gam * R.p / R.rho);
+  const double cLR = fmax(cL, cR);
+  if (haenel) {
+    flux_haenel(F5, fL, fR, area, nV);
+    const double mL = L.rho * hs_u_pm(unL, cLR, 1.0), mR = R.rho * hs_u_pm(unR, cLR, -1.0);
+    for (int s = 0; s < NS; s++) F[5 + s] = (mL * L.sc[s] + mR * R.sc[s]) * area;
+  } else {
+    flux_ausmdv(F5, fL, fR, area, nV, fo);
+    const double aL = ausm_alpha_L(L.p, L.rho, R.p, R.rho, fo);
+    const double rh = L.rho * ausm_u_pm(aL, unL, cLR, 1.0) + R.rho * ausm_u_pm(2.0 - aL, unR, cLR, -1.0);
+    const double dl = (fo & FO_EFIX) ? 0.125 * ausm_dlambda(unL, cL, unR, cR) : 0.0;
+    for (int s = 0; s < NS; s++) {
+      double fs = rh * (rh >= 0.0 ? L.sc[s] : R.sc[s]);
+      if (dl != 0.0) fs -= dl * (R.rho * R.sc[s] - L.rho * L.sc[s]);
+      F[5 + s] = fs * area;
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] = F5[i];
+}
+
+template <int NS>
+__device__ void matrices_ausm_c(double* AL, double* AR, const CState<NS>& L, const CState<NS>& R, double area,
+                                const double* nV, bool only_p, bool haenel, int fo) {
+  constexpr int B = 5 + NS, BB = B * B;
+  if (only_p) {
+    if (AL) {
+      const double uLuL = dot3(L.u, L.u), g = L.gam, hL = L.h + 0.5 * uLuL + L.k;
+      const double dpdrho = (1.0 - g) * (hL - uLuL) + g * L.p / L.rho;
+      for (int e = 0; e < BB; e++) AL[e] = 0.0;
+      for (int r = 0; r < 3; r++) {
+        double* a = AL + B * (1 + r);
+        a[0] = dpdrho * nV[r] * area;
+        for (int c = 0; c < 3; c++) a[1 + c] = (1.0 - g) * L.u[c] * nV[r] * area;
+        a[4] = (g - 1.0) * nV[r] * area;
+      }
+    }
+    if (AR)
+      for (int e = 0; e < BB; e++) AR[e] = 0.0;
+  } else {
+    const FState fL = fstate_c(L), fR = fstate_c(R);
+    double A5L[25], A5R[25];
+    if (haenel) matrices_haenel<double>(AL ? A5L : nullptr, AR ? A5R : nullptr, fL, fR, area, nV);
+    else matrices_ausmdv<double>(AL ? A5L : nullptr, AR ? A5R : nullptr, fL, fR, area, nV, fo);
+    const double unL = dot3(L.u, nV), cL = sqrt(L.gam * L.p / L.rho);
+    const double unR = dot3(R.u, nV), cR = sqrt(R.gam * R.p / R.rho);
+    const double cLR = fmax(cL, cR);
+    double bp[5], bm[5], rh = 0.0, dl = 0.0, uLp = 0.0, uRm = 0.0;
+    if (haenel) {
+      uLp = hs_u_pm(unL, cLR, 1.0);
+      uRm = hs_u_pm(unR, cLR, -1.0);
+      hs_drhou_pm(bp, unL, cLR, nV, 1.0);
+      hs_drhou_pm(bm, unR, cLR, nV, -1.0);
+    } else {
+      const double aL = ausm_alpha_L(L.p, L.rho, R.p, R.rho, fo);
+      rh = L.rho * ausm_u_pm(aL, unL, cLR, 1.0) + R.rho * ausm_u_pm(2.0 - aL, unR, cLR, -1.0);
+      if (fo & FO_EFIX) dl = ausm_dlambda(unL, cL, unR, cR);
+      ausm_drhou_pm(bp, aL, unL, cLR, nV, 1.0);
+      ausm_drhou_pm(bm, 2.0 - aL, unR, cLR, nV, -1.0);
+    }
+    for (int side = 0; side < 2; side++) {
+      double* A = side ? AR : AL;
+      if (!A) continue;
+      const CState<NS>& S = side ? R : L;
+      const CState<NS>& O = side ? L : R;
+      const double* A5 = side ? A5R : A5L;
+      const double* beta = side ? bm : bp;
+      for (int e = 0; e < BB; e++) A[e] = 0.0;
+      for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) A[B * i + j] = A5[5 * i + j];
+      for (int q = 0; q < NS; q++) {
+        double* a = A + B * (5 + q);
+        if (haenel) {
+          for (int j = 0; j < 5; j++) a[j] = beta[j] * S.sc[q] * area;
+          a[5 + q] = S.rho * (side ? uRm : uLp) * area;
+        } else {
+          // the upwind side: d(rho u_1/2)/dQ phi plus rho u_1/2 on the diagonal; else the other side's phi
+          const bool own = side ? (rh < 0.0) : (rh >= 0.0);
+          const double ph = own ? S.sc[q] : O.sc[q];
+          double v0 = beta[0] * ph, v[3], vd = own ? rh : 0.0;
+          for (int j = 0; j < 3; j++) v[j] = beta[1 + j] * ph;
+          if (dl != 0.0) {
+            const double jump = L.rho * L.sc[q] - R.rho * R.sc[q], sg = side ? -1.0 : 1.0;
+            const double un = side ? unR : unL;
+            v0 += sg * 0.125 * (dl * S.sc[q] + un / S.rho * jump);
+            for (int j = 0; j < 3; j++) v[j] += sg * (-0.125 * nV[j] / S.rho * jump);
+            vd += sg * 0.125 * dl * S.rho;
+          }
+          a[0] = v0 * area;
+          for (int j = 0; j < 3; j++) a[1 + j] = v[j] * area;
+          a[5 + q] = vd * area;
+        }
+      }
+    }
+  }
+  // dF/dQ times dQ/dU for the scalar columns
+  for (int side = 0; side < 2; side++) {
+    double* A = side ? AR : AL;
+    if (!A) continue;
+    const CState<NS>& S = side ? R : L;
+    for (int j = 0; j < B; j++)
+      for (int s = 0; s < NS; s++) {
+        A[B * j] -= S.sc[s] / S.rho * A[B * j + 5 + s];
+        A[B * j + 5 + s] /= S.rho;
+      }
+  }
+}
+
+// the coupled path's flux choice (calcFluxCoupled, JoeWithModels.cpp:4987-5057 and the boundary
+// branches 5139-5799): FK 0 HLLC, FK 1 the AUSM family (haenel / fo as above)
+template <int NS, int FK>
+__device__ __forceinline__ void cflux(double* F, const CState<NS>& L, const CState<NS>& R, double area,
+                                      const double* nV, bool only_p, bool haenel, int fo) {
+  if (FK == 0) flux_hllc_c<NS>(F, L, R, area, nV, only_p);
+  else flux_ausm_c<NS>(F, L, R, area, nV, only_p, haenel, fo);
+}
+template <int NS, int FK>
+__device__ __forceinline__ void cmatrices(double* AL, double* AR, const CState<NS>& L, const CState<NS>& R,
+                                          double area, const double* nV, bool only_p, bool haenel, int fo) {
+  if (FK == 0) matrices_hllc_c<NS>(AL, AR, L, R, area, nV, only_p);
+  else matrices_ausm_c<NS>(AL, AR, L, R, area, nV, only_p, haenel, fo);
+}
+
+// ---------------------------------------------------------------------------
 // calcViscousFluxCoupled (UgpWithCvCompFlow.cpp:3040-3276) with the model's k
 // ---------------------------------------------------------------------------
 template <int NS>
@@ -743,7 +895,7 @@ __device__ void block_inverse_n(double* A, double* Ai) {
 // face loop: calcRhsCoupled (fluxes, boundary zones, model sources) + the
 // implicit-step epilogue (vol/dt, under-relaxed rhs, D^-1)
 // ---------------------------------------------------------------------------
-template <typename BT, int MODEL>
+template <typename BT, int MODEL, int FK>
 __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb t, int implicit, int for_step) {
   constexpr int NS = TM<MODEL>::NS, B = TM<MODEL>::B, BB = TM<MODEL>::BB;
   constexpr bool SST = MODEL == JG_TURB_SST;
@@ -760,6 +912,9 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
   double F[B];
   double one[NS], dfa[NS], dterm[NS];
   for (int q = 0; q < NS; q++) one[q] = 1.0;
+  // boundary faces: AUSMDV without the shock fix (JoeWithModels.cpp:5177-5182)
+  const bool ausmdv = FK && p.flux == JG_FLUX_AUSMDV, hz_b = FK && p.flux == JG_FLUX_HAENEL;
+  const int fob = ausmdv ? bnd_opts<4>(p) : 0;
   for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
     const Slot s = m.slots[k];
     const int f = s.f;
@@ -770,16 +925,19 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
       const int c0 = s.side == 0 ? c : s.nb;
       const int c1 = s.side == 0 ? s.nb : c;
       const double sg = s.side == 0 ? -1.0 : 1.0;
+      // the face's shock fix (JoeWithModels.cpp:4956-4982)
+      const int fo = ausmdv ? face_opts<4>(p, st, c0, c1) : 0;
+      const bool hz = hz_b || (fo & FO_HAENEL);
       {
         CState<NS> L = recon_c<NS>(m, p, st, t, c0, f, SST), R = recon_c<NS>(m, p, st, t, c1, f, SST);
-        flux_hllc_c<NS>(F, L, R, area, nV, false);
+        cflux<NS, FK>(F, L, R, area, nV, false, hz, fo);
         for (int i = 0; i < B; i++) rhs[i] += sg * F[i];
       }
       double Ob[BB];
       if (implicit) {
         CState<NS> L0 = cell_c<NS>(m, p, st, t, c0, SST), R0 = cell_c<NS>(m, p, st, t, c1, SST);
         double Apl[BB], Ami[BB];
-        matrices_hllc_c<NS>(Apl, Ami, L0, R0, area, nV, false);
+        cmatrices<NS, FK>(Apl, Ami, L0, R0, area, nV, false, hz, fo);
         // row of c0: D += Apl, O = Ami ; row of c1: D -= Ami, O = -Apl
         if (s.side == 0) {
           for (int e = 0; e < BB; e++) { sD[e * bd + tid] += Apl[e]; Ob[e] = Ami[e]; }
@@ -834,16 +992,16 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
       if (z.kind == JG_BC_SYMMETRY || z.kind == JG_BC_NEUMANN) {
         if (SST) Bs.k = Bs.sc[0];
         const bool op = (z.kind == JG_BC_SYMMETRY) && only_p;
-        flux_hllc_c<NS>(F, Bs, Bs, area, nV, op);
+        cflux<NS, FK>(F, Bs, Bs, area, nV, op, hz_b, fob);
         for (int i = 0; i < B; i++) rhs[i] -= F[i];
         if (implicit) {
           if (z.kind == JG_BC_NEUMANN || p.symm_bc == JG_SYMM_NEW_NUMERIC) {
             double Apl[BB], Ami[BB];
-            matrices_hllc_c<NS>(Apl, Ami, Bs, Bs, area, nV, false);
+            cmatrices<NS, FK>(Apl, Ami, Bs, Bs, area, nV, false, hz_b, fob);
             for (int e = 0; e < BB; e++)
               sD[e * bd + tid] += (p.symm_bc == JG_SYMM_NEW_NUMERIC) ? Apl[e] + Ami[e] : Apl[e];
           } else {
-            matrices_hllc_c<NS>(Dv, nullptr, Bs, Bs, area, nV, only_p);
+            cmatrices<NS, FK>(Dv, nullptr, Bs, Bs, area, nV, only_p, hz_b, fob);
             for (int e = 0; e < BB; e++) sD[e * bd + tid] += Dv[e];
           }
         }
@@ -870,15 +1028,15 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
         }
       } else if (z.kind == JG_BC_WALL) {
         // the wall keeps the face kinetic energy at 0 (JoeWithModels.cpp:5448-5452)
-        flux_hllc_c<NS>(F, Bs, Bs, area, nV, only_p);
+        cflux<NS, FK>(F, Bs, Bs, area, nV, only_p, hz_b, fob);
         for (int i = 0; i < B; i++) rhs[i] -= F[i];
         if (implicit) {
           if (p.symm_bc == JG_SYMM_NEW_NUMERIC) {
             double Apl[BB], Ami[BB];
-            matrices_hllc_c<NS>(Apl, Ami, Bs, Bs, area, nV, false);
+            cmatrices<NS, FK>(Apl, Ami, Bs, Bs, area, nV, false, hz_b, fob);
             for (int e = 0; e < BB; e++) sD[e * bd + tid] += Apl[e] + Ami[e];
           } else {
-            matrices_hllc_c<NS>(Dv, nullptr, Bs, Bs, area, nV, only_p);
+            cmatrices<NS, FK>(Dv, nullptr, Bs, Bs, area, nV, only_p, hz_b, fob);
             for (int e = 0; e < BB; e++) sD[e * bd + tid] += Dv[e];
           }
         }
@@ -904,11 +1062,11 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
         // CBC, CBC_SUBSONIC_INLET/OUTLET, FARFIELD (JoeWithModels.cpp:5624-5788)
         CState<NS> L = recon_c<NS>(m, p, st, t, c, f, SST);
         if (SST) Bs.k = Bs.sc[0];
-        flux_hllc_c<NS>(F, L, Bs, area, nV, false);
+        cflux<NS, FK>(F, L, Bs, area, nV, false, hz_b, fob);
         for (int i = 0; i < B; i++) rhs[i] -= F[i];
         if (implicit) {
           CState<NS> L0 = cell_c<NS>(m, p, st, t, c, SST);
-          matrices_hllc_c<NS>(Dv, nullptr, L0, Bs, area, nV, false);
+          cmatrices<NS, FK>(Dv, nullptr, L0, Bs, area, nV, false, hz_b, fob);
           for (int e = 0; e < BB; e++) sD[e * bd + tid] += Dv[e];
         }
         VSideC<NS> v0 = vcell_c<NS>(m, st, t, p, c, SST);
@@ -1115,14 +1273,26 @@ void launch_turb_props(const Mesh& m, const Params& p, State& st, Turb& t, cudaS
 template <typename BT>
 static void launch_flux_c_t(const Mesh& m, const Params& p, State& st, Turb& t, int implicit, int for_step,
                             cudaStream_t s) {
-  if (t.model == JG_TURB_SST)  // 64-cell blocks keep the 7x7 accumulators (49 x 64 doubles) within 48 KB
-    k_flux_c<BT, JG_TURB_SST><<<grid_for(m.ncv, 64), 64, 49 * 64 * sizeof(double), s>>>(m, p, st, t, implicit,
-                                                                                        for_step);
-  else
-    k_flux_c<BT, JG_TURB_SA><<<grid_for(m.ncv, TBC), TBC, 36 * TBC * sizeof(double), s>>>(m, p, st, t, implicit,
-                                                                                         for_step);
+  // 64-cell blocks keep the 7x7 accumulators (49 x 64 doubles) within 48 KB
+  const bool ausm = p.flux == JG_FLUX_AUSMDV || p.flux == JG_FLUX_HAENEL;
+  if (t.model == JG_TURB_SST) {
+    if (ausm)
+      k_flux_c<BT, JG_TURB_SST, 1><<<grid_for(m.ncv, 64), 64, 49 * 64 * sizeof(double), s>>>(m, p, st, t, implicit,
+                                                                                             for_step);
+    else
+      k_flux_c<BT, JG_TURB_SST, 0><<<grid_for(m.ncv, 64), 64, 49 * 64 * sizeof(double), s>>>(m, p, st, t, implicit,
+                                                                                             for_step);
+  } else {
+    if (ausm)
+      k_flux_c<BT, JG_TURB_SA, 1><<<grid_for(m.ncv, TBC), TBC, 36 * TBC * sizeof(double), s>>>(m, p, st, t,
+                                                                                              implicit, for_step);
+    else
+      k_flux_c<BT, JG_TURB_SA, 0><<<grid_for(m.ncv, TBC), TBC, 36 * TBC * sizeof(double), s>>>(m, p, st, t,
+                                                                                              implicit, for_step);
+  }
 }
 void launch_flux6(const Mesh& m, const Params& p, State& st, Turb& t, int implicit, int for_step, cudaStream_t s) {
+  launch_face_sensors(m, p, st, s);  // AUSMDV's shock sensor
   if (p.fp32) launch_flux_c_t<float>(m, p, st, t, implicit, for_step, s);
   else launch_flux_c_t<double>(m, p, st, t, implicit, for_step, s);
 }

@@ -2991,6 +2991,179 @@ static void matrices_hllc_coupled(double *AL, double *AR, int ns, const cstate *
   }
 }
 
+/* ---- coupled AUSMDV and Haenel & Schwane (UgpWithCvCompFlow.cpp:2293-3036), ConvTerm = 1,
+ * dp/dscal = 0 (no model here sets dpress_dphi).  The five flow entries are the segregated
+ * schemes' (their total enthalpy h + u.u/2 + k in the same order); the scalars ride on the mass
+ * flux of the upwind side (AUSMDV) or of each split part (HAENEL), and the entropy fix acts on
+ * them as on the density. ---- */
+static fstate fstate_of(const cstate *c) {
+  fstate f = {c->rho, {c->u[0], c->u[1], c->u[2]}, c->p, c->gam, c->k, c->h};
+  return f;
+}
+
+/* the AUSMDV mass flux rho u_1/2 and the entropy fix's unscaled wave-speed jump (0: no fix) */
+static void ausmdv_mass(const cstate *L, const cstate *R, const double *nV, ausm_opt o, double *rhou_half,
+                        double *dl, double *unL_o, double *unR_o, double *alphaL_o, double *cLR_o) {
+  double unL = dot3(L->u, nV), cL = sqrt(L->gam * L->p / L->rho);
+  double alphaL = ausm_alpha_L(L->p, L->rho, R->p, R->rho, o.shock);
+  double unR = dot3(R->u, nV), cR = sqrt(R->gam * R->p / R->rho);
+  double alphaR = 2.0 - alphaL;
+  double cLR = dmax(cL, cR);
+  *rhou_half = L->rho * hs_u_pm(alphaL, unL, cLR, +1.0) + R->rho * hs_u_pm(alphaR, unR, cLR, -1.0);
+  double d = 0.0;
+  if (o.efix) {
+    if ((unL <= -cL) && (unR >= cR)) d = 0.0;
+    else if (((unL - cL) < 0.0) && ((unR - cR) > 0.0)) d = ((unR - cR) - (unL - cL));
+    else if (((unL + cL) < 0.0) && ((unR + cR) > 0.0)) d = ((unR + cR) - (unL + cL));
+  }
+  *dl = d;
+  *unL_o = unL;
+  *unR_o = unR;
+  *alphaL_o = alphaL;
+  *cLR_o = cLR;
+}
+
+/* calcEulerFluxCoupled_AUSMDV (:2293-2399) and calcEulerFluxCoupled_HAENEL (:2802-2850);
+ * haenel selects the latter */
+static void flux_ausm_coupled(double *F, int ns, const cstate *L, const cstate *R, double area, const double *nV,
+                              int only_pressure, int haenel, ausm_opt o) {
+  if (only_pressure) {
+    flux_hllc_coupled(F, ns, L, R, area, nV, 1);  /* the same pressure-only flux */
+    return;
+  }
+  fstate fL = fstate_of(L), fR = fstate_of(R);
+  double F5[5];
+  if (haenel) {
+    flux_haenel(F5, &fL, &fR, area, nV);
+    double unL = dot3(L->u, nV), cL = sqrt(L->gam * L->p / L->rho);
+    double unR = dot3(R->u, nV), cR = sqrt(R->gam * R->p / R->rho);
+    double cLR = dmax(cL, cR);
+    double uLp = hs_u_pm(1.0, unL, cLR, 1.0), uRm = hs_u_pm(1.0, unR, cLR, -1.0);
+    for (int s = 0; s < ns; s++) F[5 + s] = (L->rho * uLp * L->sc[s] + R->rho * uRm * R->sc[s]) * area;
+  } else {
+    flux_ausmdv(F5, &fL, &fR, area, nV, o);
+    double rh, dl, unL, unR, aL, cLR;
+    ausmdv_mass(L, R, nV, o, &rh, &dl, &unL, &unR, &aL, &cLR);
+    dl *= 0.125;
+    for (int s = 0; s < ns; s++) {
+      double fs = 1.0 * rh * (rh >= 0.0 ? L->sc[s] : R->sc[s]);
+      if (dl != 0.0) fs -= dl * (R->rho * R->sc[s] - L->rho * L->sc[s]);
+      F[5 + s] = fs * area;
+    }
+  }
+  for (int i = 0; i < 5; i++) F[i] = F5[i];
+}
+
+/* calcEulerFluxMatricesCoupled_AUSMDV (:2405-2796) and calcEulerFluxMatricesCoupled_HAENEL
+ * (:2858-3034), then dQ/dU of the scalar columns */
+static void matrices_ausm_coupled(double *AL, double *AR, int ns, const cstate *L, const cstate *R, double area,
+                                  const double *nV, int only_pressure, int haenel, ausm_opt o) {
+  int B = 5 + ns, BB = B * B;
+  if (only_pressure) {
+    if (AL) {
+      double uLuL = dot3(L->u, L->u), g = L->gam;
+      double hL = L->h + 0.5 * uLuL + L->k;
+      double dpdrho = (1.0 - g) * (hL - uLuL) + g * L->p / L->rho;
+      for (int e = 0; e < BB; e++) AL[e] = 0.0;
+      for (int r = 0; r < 3; r++) {
+        double *a = AL + B * (1 + r);
+        a[0] = dpdrho * nV[r];
+        for (int c = 0; c < 3; c++) a[1 + c] = (1.0 - g) * L->u[c] * nV[r];
+        a[4] = (g - 1.0) * nV[r];
+      }
+      for (int e = 0; e < BB; e++) AL[e] *= area;
+    }
+    if (AR) memset(AR, 0, sizeof(double) * BB);
+  } else {
+    fstate fL = fstate_of(L), fR = fstate_of(R);
+    double L5[5][5], R5[5][5];
+    if (haenel) matrices_haenel(AL ? L5 : NULL, AR ? R5 : NULL, &fL, &fR, area, nV);
+    else matrices_ausmdv(AL ? L5 : NULL, AR ? R5 : NULL, &fL, &fR, area, nV, o);
+    double unL = dot3(L->u, nV), cL = sqrt(L->gam * L->p / L->rho);
+    double unR = dot3(R->u, nV), cR = sqrt(R->gam * R->p / R->rho);
+    double cLR = dmax(cL, cR);
+    double bp[5], bm[5];
+    double rh = 0.0, dl = 0.0, uLp, uRm;
+    if (haenel) {
+      uLp = hs_u_pm(1.0, unL, cLR, 1.0);
+      uRm = hs_u_pm(1.0, unR, cLR, -1.0);
+      hs_drhou_pm(bp, 1.0, unL, cLR, nV, +1.0);
+      hs_drhou_pm(bm, 1.0, unR, cLR, nV, -1.0);
+    } else {
+      double aL;
+      ausmdv_mass(L, R, nV, o, &rh, &dl, &unL, &unR, &aL, &cLR);
+      uLp = uRm = 0.0;
+      hs_drhou_pm(bp, aL, unL, cLR, nV, +1.0);
+      hs_drhou_pm(bm, 2.0 - aL, unR, cLR, nV, -1.0);
+    }
+    for (int side = 0; side < 2; side++) {
+      double *A = side ? AR : AL;
+      if (!A) continue;
+      const cstate *S = side ? R : L, *O = side ? L : R;
+      double (*A5)[5] = side ? R5 : L5;
+      const double *beta = side ? bm : bp;
+      for (int e = 0; e < BB; e++) A[e] = 0.0;
+      for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) A[B * i + j] = A5[i][j];
+      for (int q = 0; q < ns; q++) {
+        double *a = A + B * (5 + q);
+        if (haenel) {
+          for (int j = 0; j < 5; j++) a[j] = beta[j] * S->sc[q] * area;
+          a[5 + q] = S->rho * (side ? uRm : uLp) * area;
+        } else {
+          /* upwind side: d(rho u_1/2)/dQ phi + rho u_1/2 on the diagonal; else the other side's phi */
+          int own = side ? (rh < 0.0) : (rh >= 0.0);
+          double ph = own ? S->sc[q] : O->sc[q];
+          double v0 = beta[0] * ph, v[3], vd = own ? rh : 0.0;
+          for (int j = 0; j < 3; j++) v[j] = beta[1 + j] * ph;
+          if (dl != 0.0) {
+            double jump = L->rho * L->sc[q] - R->rho * R->sc[q];
+            double un = side ? unR : unL;
+            if (!side) {
+              v0 += 0.125 * (dl * S->sc[q] + un / S->rho * jump);
+              for (int j = 0; j < 3; j++) v[j] += -0.125 * nV[j] / S->rho * jump;
+              vd += 0.125 * dl * S->rho;
+            } else {
+              v0 -= 0.125 * (dl * S->sc[q] + un / S->rho * jump);
+              for (int j = 0; j < 3; j++) v[j] -= -0.125 * nV[j] / S->rho * jump;
+              vd -= 0.125 * dl * S->rho;
+            }
+          }
+          a[0] = v0 * area;
+          for (int j = 0; j < 3; j++) a[1 + j] = v[j] * area;
+          a[5 + q] = vd * area;
+        }
+      }
+    }
+  }
+  for (int side = 0; side < 2; side++) {
+    double *A = side ? AR : AL;
+    const cstate *S = side ? R : L;
+    if (!A) continue;
+    for (int j = 0; j < B; j++)
+      for (int s = 0; s < ns; s++) {
+        A[B * j] -= S->sc[s] / S->rho * A[B * j + 5 + s];
+        A[B * j + 5 + s] /= S->rho;
+      }
+  }
+}
+
+/* the coupled path's flux choice (calcFluxCoupled, JoeWithModels.cpp:4987-5057 and the boundary
+ * branches 5139-5799): HLLC, AUSMDV (the face's shock fix o.shock; HAENEL there selects the Haenel &
+ * Schwane scheme) or HAENEL */
+static void cflux(const jg_params *p, ausm_opt o, double *F, int ns, const cstate *L, const cstate *R, double area,
+                  const double *nV, int only_pressure) {
+  if (p->flux == JG_FLUX_HLLC) flux_hllc_coupled(F, ns, L, R, area, nV, only_pressure);
+  else flux_ausm_coupled(F, ns, L, R, area, nV, only_pressure,
+                         p->flux == JG_FLUX_HAENEL || o.shock == JG_SHOCK_FIX_HAENEL, o);
+}
+static void cmatrices(const jg_params *p, ausm_opt o, double *AL, double *AR, int ns, const cstate *L,
+                      const cstate *R, double area, const double *nV, int only_pressure) {
+  if (p->flux == JG_FLUX_HLLC) matrices_hllc_coupled(AL, AR, ns, L, R, area, nV, only_pressure);
+  else matrices_ausm_coupled(AL, AR, ns, L, R, area, nV, only_pressure,
+                             p->flux == JG_FLUX_HAENEL || o.shock == JG_SHOCK_FIX_HAENEL, o);
+}
+
 /* calcViscousFluxCoupled (UgpWithCvCompFlow.cpp:3040-3276), turbulence model on */
 typedef struct {
   double rho, u[3], h, T, R, gam, sc[MAXS], k;
@@ -3177,6 +3350,18 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
   memset(A0, 0, sizeof(A0));
   memset(A1, 0, sizeof(A1));
   double ones[MAXS] = {1.0, 1.0}, dterm[MAXS], dfa[MAXS];
+  /* AUSMDV shock sensor at the cell-centre states (JoeWithModels.cpp:4763-4792) */
+  double *flag = NULL;
+  if (p->flux == JG_FLUX_AUSMDV && p->shock_fix != JG_SHOCK_FIX_NONE) {
+    flag = dalloc(h->ncv);
+    for (int f = h->nfa_b; f < h->nfa; f++)
+      if (face_sonic(h, f)) {
+        flag[m->cvofa[2 * f]] = 1.0;
+        flag[m->cvofa[2 * f + 1]] = 1.0;
+      }
+  }
+  const double flag_sum = p->shock_flag == JG_SHOCK_FLAG_TET ? 0.9 : 1.1;
+  const ausm_opt ob = bnd_opt(p);  /* boundary faces: AUSMDV without the shock fix */
   /* internal faces, JoeWithModels.cpp:4797-5132 */
   for (int f = h->nfa_b; f < h->nfa; f++) {
     int c0 = m->cvofa[2 * f], c1 = m->cvofa[2 * f + 1];
@@ -3195,13 +3380,16 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
       face_weights(h, f, c0, c1, &w0, &w1);
       kine_fa = (w1 * t->phi[0][c0] + w0 * t->phi[0][c1]) / (w0 + w1);
     }
-    flux_hllc_coupled(F, ns, &L, &R, area, nV, 0);
+    /* the face's shock fix (JoeWithModels.cpp:4956-4982) */
+    ausm_opt o = bnd_opt(p);
+    if (flag && (flag[c0] + flag[c1]) > flag_sum) o.shock = p->shock_fix;
+    cflux(p, o, F, ns, &L, &R, area, nV, 0);
     for (int i = 0; i < B; i++) { rhs[B * c0 + i] -= F[i]; rhs[B * c1 + i] += F[i]; }
     int n00 = m->nbocv_i[c0], n01 = csr_slot(m, c0, c1), n11 = m->nbocv_i[c1], n10 = csr_slot(m, c1, c0);
     if (implicit) {
       cstate L0 = cell_cstate(h, t, c0), R0 = cell_cstate(h, t, c1);
       if (sst) { L0.k = t->phi[0][c0]; R0.k = t->phi[0][c1]; }
-      matrices_hllc_coupled(Apl, Ami, ns, &L0, &R0, area, nV, 0);
+      cmatrices(p, o, Apl, Ami, ns, &L0, &R0, area, nV, 0);
       add_blk(A, B, n00, Apl, 1.0);
       add_blk(A, B, n01, Ami, 1.0);
       add_blk(A, B, n11, Ami, -1.0);
@@ -3241,15 +3429,15 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
       if (zn->kind == JG_BC_SYMMETRY || zn->kind == JG_BC_NEUMANN) {
         if (sst) Bs.k = t->phi_bfa[0][f];
         int op = (zn->kind == JG_BC_SYMMETRY) ? only_p : 0;
-        flux_hllc_coupled(F, ns, &Bs, &Bs, area, nV, op);
+        cflux(p, ob, F, ns, &Bs, &Bs, area, nV, op);
         for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
           if (zn->kind == JG_BC_NEUMANN || p->symm_bc == JG_SYMM_NEW_NUMERIC) {
-            matrices_hllc_coupled(Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
+            cmatrices(p, ob, Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
             for (int e = 0; e < BB; e++)
               A[(size_t)BB * n00 + e] += (p->symm_bc == JG_SYMM_NEW_NUMERIC) ? Apl[e] + Ami[e] : Apl[e];
           } else {
-            matrices_hllc_coupled(Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
+            cmatrices(p, ob, Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
             add_blk(A, B, n00, Apl, 1.0);
           }
         }
@@ -3272,14 +3460,14 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
         }
       } else if (zn->kind == JG_BC_WALL) {
         /* the wall branch keeps the face kinetic energy at 0 (JoeWithModels.cpp:5448-5452) */
-        flux_hllc_coupled(F, ns, &Bs, &Bs, area, nV, only_p);
+        cflux(p, ob, F, ns, &Bs, &Bs, area, nV, only_p);
         for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
           if (p->symm_bc == JG_SYMM_NEW_NUMERIC) {
-            matrices_hllc_coupled(Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
+            cmatrices(p, ob, Apl, Ami, ns, &Bs, &Bs, area, nV, 0);
             for (int e = 0; e < BB; e++) A[(size_t)BB * n00 + e] += Apl[e] + Ami[e];
           } else {
-            matrices_hllc_coupled(Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
+            cmatrices(p, ob, Apl, NULL, ns, &Bs, &Bs, area, nV, only_p);
             add_blk(A, B, n00, Apl, 1.0);
           }
         }
@@ -3304,12 +3492,12 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
         cstate L = cell_cstate(h, t, c0);
         if (p->second_order) reconstruct_c(h, t, c0, f, &L);
         if (sst) { L.k = L.sc[0]; Bs.k = t->phi_bfa[0][f]; }
-        flux_hllc_coupled(F, ns, &L, &Bs, area, nV, 0);
+        cflux(p, ob, F, ns, &L, &Bs, area, nV, 0);
         for (int i = 0; i < B; i++) rhs[B * c0 + i] -= F[i];
         if (implicit) {
           cstate L0 = cell_cstate(h, t, c0);
           if (sst) L0.k = t->phi[0][c0];
-          matrices_hllc_coupled(Apl, NULL, ns, &L0, &Bs, area, nV, 0);
+          cmatrices(p, ob, Apl, NULL, ns, &L0, &Bs, area, nV, 0);
           add_blk(A, B, n00, Apl, 1.0);
         }
         if (visc) {
@@ -3333,6 +3521,7 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
       }
     }
   }
+  free(flag);
   /* source terms: sourceHookRansTurbCoupled (TurbModel_SA.h:359-434; TurbModel_KOMSST.h:306-340) */
   for (int c = 0; c < h->ncv; c++) {
     size_t d0 = (size_t)BB * m->nbocv_i[c];

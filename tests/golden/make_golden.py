@@ -107,6 +107,22 @@ def sa_cases():
     yield "sa_mixed_bump_farfield", rawm, prmm
     yield "sa_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
+    # the coupled AUSMDV family and HAENEL (calcFluxCoupled's other flux choices): sonic inflows for the
+    # shock sensor (the HAENEL shock fix with CELL_FLAG_HEX, ALPHA_LR with CELL_FLAG_TET), the entropy
+    # fix, every boundary branch; HAENEL is not combined with NEW_NUMERIC symmetry, whose matrices the
+    # reference leaves unset (it compares the name "Haenel" there)
+    rawt, _, prmt = case.sa_bump_case(16, 8, 2, stretch=1.2, jitter=0.1, seed=7, mach=1.0)
+    rawt5, _, prmt5 = case.sa_bump_case(16, 8, 2, stretch=1.15, jitter=0.1, seed=8, inlet="CBC", mach=1.05)
+    yield "sa_bump_ausmdv_m1", rawt, dataclasses.replace(prmt, SPACE_INTEGRATION="AUSMDV")
+    yield "sa_bump_ausmv_alpha_tet_m105_symm_original", rawt5, dataclasses.replace(
+        prmt5, SPACE_INTEGRATION="AUSMV", SHOCK_FIX_TYPE="ALPHA_LR", SHOCK_FIX_FLAG="CELL_FLAG_TET",
+        SYMM_BC="ORIGINAL_NUMERIC")
+    yield "sa_bump_ausmd_neumann_first_order_new_numeric", rawc, dataclasses.replace(
+        prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC", SPACE_INTEGRATION="AUSMD",
+        SHOCK_FIX_TYPE="NONE", ENTROPY_FIX="NONE")
+    yield "sa_bump_haenel_farfield", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
+    yield "sa_mixed_bump_haenel_symm_original", rawm, dataclasses.replace(prmm, SPACE_INTEGRATION="HAENEL",
+                                                                          SYMM_BC="ORIGINAL_NUMERIC")
 
 
 def sst_cases():
@@ -121,6 +137,11 @@ def sst_cases():
     yield "sst_mixed_bump_farfield", rawm, prmm
     yield "sst_bump_neumann_first_order_new_numeric", rawc, dataclasses.replace(
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC")
+    # the coupled AUSMDV and HAENEL with k in the total enthalpy
+    rawt, _, prmt = case.sst_bump_case(16, 8, 2, stretch=1.2, jitter=0.1, seed=7, mach=1.0)
+    yield "sst_bump_ausmdv_m1", rawt, dataclasses.replace(prmt, SPACE_INTEGRATION="AUSMDV")
+    yield "sst_bump_haenel_neumann_first_order", rawc, dataclasses.replace(
+        prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="ORIGINAL_NUMERIC", SPACE_INTEGRATION="HAENEL")
 
 
 def params_json(prm) -> str:

@@ -264,6 +264,13 @@ int solveLinSysNSCoupled(jg_case_t *h, double *dq, const double *A, const double
 int jg_step(jg_case_t *h, int nsteps, double *resid);
 /* the same steps enqueued on the case stream without synchronising */
 int jg_step_async(jg_case_t *h, int nsteps);
+/* A host-resident state stepped in place: jg_set_state(rho, rhou, rhoE) + jg_step(nsteps, resid)
+ * + jg_get_state into the same arrays, with one synchronisation (the three calls make three); for
+ * a caller that keeps the state on the host between steps, as the reference's loop does.  Pinned
+ * host arrays make the copies asynchronous DMA.  A single case (not a batch handle).  Returns
+ * JG_ERR_STATE if the uploaded or a stepped state is non-physical (the arrays then hold the last
+ * state the device computed). */
+int jg_step_host(jg_case_t *h, double *rho, double *rhou, double *rhoE, int nsteps, double *resid);
 int jg_get_cfl_step(jg_case_t *h, double *cfl, int *step);
 /* sets the CFL and the step count the next step's ramp starts from (the
  * reference's `cfl` and `step` members, e.g. after reading a restart) */

@@ -343,6 +343,8 @@ int jg_destroy(jg_case_t* h) {
   if (h->hpin) cudaFreeHost(h->hpin);
   if (h->st.ev_pre) cudaEventDestroy(h->st.ev_pre);
   if (h->st.ev_dt) cudaEventDestroy(h->st.ev_dt);
+  if (h->st.ev_res) cudaEventDestroy(h->st.ev_res);
+  if (h->st.ev_resid) cudaEventDestroy(h->st.ev_resid);
   delete h;
   return JG_OK;
 }
@@ -399,13 +401,15 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   const int N = mesh->ncv, nfa = mesh->nfa, nfa_b = mesh->nfa_b;
   if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   if (q->turb_model == JG_TURB_NONE && !h->st.aux) {
-    // the face loop's Jacobian kernel runs beside its residual kernel on a second stream, and
-    // the time step beside the gradients
+    // the face loop's Jacobian kernel runs beside its residual kernel on a second stream; the
+    // step control and time step beside the gradients, the residual norms beside the relaxation
     CK(cudaStreamCreateWithFlags(&h->st.aux, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->st.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->st.ev_join, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->st.ev_pre, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->st.ev_dt, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->st.ev_res, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->st.ev_resid, cudaEventDisableTiming));
   }
   h->ncv = N;
   h->nfa = nfa;
@@ -1088,7 +1092,7 @@ static int check_err_flags(jg_case* h, bool all_cases = false, const double* dre
 
 // calcStateVariables + calcMaterialProperties + setBC (+ mut = 0), the
 // runBackwardEuler preamble (JoeWithModels.cpp:942-957)
-static int prime(jg_case* h) {
+static int prime_enqueue(jg_case* h) {
   // a new state: every case forms its Jacobian blocks at its next step
   if (h->st.jac_next) CK(cudaMemsetAsync(h->st.jac_next, 0, sizeof(long long) * h->ncases, h->stream));
   launch_state(h->m, h->p, h->st, h->stream);
@@ -1102,19 +1106,39 @@ static int prime(jg_case* h) {
   }
   CKL();
   h->primed = 1;
+  return JG_OK;
+}
+static int prime(jg_case* h) {
+  RC(prime_enqueue(h));
   return check_err_flags(h, true);
 }
 
-int jg_set_state(jg_case_t* h, const double* rho, const double* rhou, const double* rhoE) {
-  if (!h || !rho || !rhou || !rhoE) return set_err(JG_ERR_ARG, "null argument");
+// the caller's state -> the handle (enqueued; pinned host memory makes the copies asynchronous DMA)
+static int stage_state_in(jg_case* h, const double* rho, const double* rhou, const double* rhoE) {
   const size_t N = h->ncv;
   if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
-  // direct copies from the caller's arrays (pinned host memory makes them asynchronous DMA)
   CK(cudaMemcpyAsync(h->d_io, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + N, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_io + 4 * N, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   launch_pack_state((int)N, h->d_io, h->st.q, h->d_cell_old, h->stream);
   CK(cudaMemsetAsync(h->st.prim, 0, 8 * N * sizeof(double), h->stream));
+  return JG_OK;
+}
+// the handle's state -> the caller's arrays (enqueued; any pointer may be NULL)
+static int stage_state_out(jg_case* h, double* rho, double* rhou, double* rhoE) {
+  const size_t N = h->ncv;
+  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
+  launch_unpack_state((int)N, h->st.q, h->d_io, h->d_cell_old, h->stream);
+  CKL();
+  if (rho) CK(cudaMemcpyAsync(rho, h->d_io, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (rhoE) CK(cudaMemcpyAsync(rhoE, h->d_io + 4 * N, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return JG_OK;
+}
+
+int jg_set_state(jg_case_t* h, const double* rho, const double* rhou, const double* rhoE) {
+  if (!h || !rho || !rhou || !rhoE) return set_err(JG_ERR_ARG, "null argument");
+  RC(stage_state_in(h, rho, rhou, rhoE));
   return prime(h);
 }
 
@@ -1125,13 +1149,7 @@ int jg_calc_state(jg_case_t* h) {
 
 int jg_get_state(jg_case_t* h, double* rho, double* rhou, double* rhoE) {
   if (!h) return set_err(JG_ERR_ARG, "null handle");
-  const size_t N = h->ncv;
-  if (!h->d_io) RC(dmalloc(h, &h->d_io, 5 * N));
-  launch_unpack_state((int)N, h->st.q, h->d_io, h->d_cell_old, h->stream);
-  CKL();
-  if (rho) CK(cudaMemcpyAsync(rho, h->d_io, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (rhou) CK(cudaMemcpyAsync(rhou, h->d_io + N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (rhoE) CK(cudaMemcpyAsync(rhoE, h->d_io + 4 * N, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  RC(stage_state_out(h, rho, rhou, rhoE));
   CK(cudaStreamSynchronize(h->stream));
   return JG_OK;
 }
@@ -1464,26 +1482,37 @@ static int enqueue_step_coupled(jg_case* h) {
 static int enqueue_step(jg_case* h, int for_graph) {
   if (h->bs > 5) return enqueue_step_coupled(h);
   cudaStream_t S = h->stream;
-  launch_ctrl_step(h->p, h->st, S);
-  // calcDt on the second stream beside the gradients: neither reads what the other writes.  The
-  // split face loop's Jacobian kernel follows it on that stream (the join brings both back);
-  // the fused face loop waits for it here.
-  const bool dt_aside = h->st.aux && h->st.ev_pre && h->st.ev_dt;
-  if (dt_aside) {
+  // Off the critical path on the second stream: the CFL ramp and calcDt beside the gradients
+  // (neither reads what the other writes; the split face loop's Jacobian kernel follows them on
+  // that stream and its join brings them back, the fused face loop waits for them here), and the
+  // residual norms beside the relaxation (joined before the update).
+  const int solver = h->hp.lin_solver;
+  const bool aside = h->st.aux && h->st.ev_pre && h->st.ev_dt && h->st.ev_res && h->st.ev_resid;
+  const bool resid_aside = aside && solver != JG_LS_BCGSTAB && solver != JG_LS_BCGSTAB_LINELET;
+  if (aside) {
     CK(cudaEventRecord(h->st.ev_pre, S));
     CK(cudaStreamWaitEvent(h->st.aux, h->st.ev_pre, 0));
+    launch_ctrl_step(h->p, h->st, h->st.aux);
     launch_dt(h->m, h->p, h->st, 1, 0.0, h->st.aux);
     CK(cudaEventRecord(h->st.ev_dt, h->st.aux));
   } else {
+    launch_ctrl_step(h->p, h->st, S);
     launch_dt(h->m, h->p, h->st, 1, 0.0, S);
   }
   launch_grad(h->m, h->p, h->st, S);
-  if (dt_aside && !flux_split(h->p, h->st)) CK(cudaStreamWaitEvent(S, h->st.ev_dt, 0));
+  if (aside && !flux_split(h->p, h->st)) CK(cudaStreamWaitEvent(S, h->st.ev_dt, 0));
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[0], S, cudaEventRecordExternal));
   launch_flux(h->m, h->p, h->st, 1, 1, S);
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[1], S, cudaEventRecordExternal));
-  launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, S);
-  int solver = h->hp.lin_solver;
+  if (resid_aside) {
+    CK(cudaEventRecord(h->st.ev_res, S));
+    CK(cudaStreamWaitEvent(h->st.aux, h->st.ev_res, 0));
+    launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, h->st.aux);
+    CK(cudaEventRecord(h->st.ev_resid, h->st.aux));
+  } else {
+    if (aside) CK(cudaStreamWaitEvent(S, h->st.ev_dt, 0));
+    launch_resid_cases(h->st, h->d_case_off, h->d_rblk_off, h->d_rblk_case, h->nrblk, h->ncases, 1, S);
+  }
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[2], S, cudaEventRecordExternal));
   // the relaxation's result (x, [5][N]); the update reads it directly
   const void* x = nullptr;
@@ -1517,6 +1546,7 @@ static int enqueue_step(jg_case* h, int for_graph) {
     x_fp32 = 0;  // BiCGSTAB is FP64
   }
   if (h->profiling) CK(cudaEventRecordWithFlags(h->ev[3], S, cudaEventRecordExternal));
+  if (resid_aside) CK(cudaStreamWaitEvent(S, h->st.ev_resid, 0));
   launch_update_state_x(h->m, h->p, h->st, x, x_fp32, S);
   launch_faces_after_update(h->m, h->p, h->st, S);
   CKL();
@@ -1552,9 +1582,8 @@ static int ensure_graph(jg_case* h) {
   return JG_OK;
 }
 
-int jg_step(jg_case_t* h, int nsteps, double* resid) {
-  if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
-  if (!h->primed) RC(prime(h));
+// nsteps steps enqueued on the case stream (the host-driven BiCGSTAB synchronises inside)
+static int enqueue_steps(jg_case* h, int nsteps) {
   if (nsteps > h->hist_cap) {
     int cap = std::max(nsteps, 2 * h->hist_cap);
     double* r = nullptr;
@@ -1576,24 +1605,45 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
     else RC(enqueue_step(h, 0));
   }
   CKL();
+  return JG_OK;
+}
+
+// the per-step residual history of the last call, summed over the cases of a batch
+static int batch_resid_sum(jg_case* h, int nsteps, double* resid) {
+  const int bs = h->bs;
+  std::vector<double> all(bs * (size_t)nsteps * h->ncases);
+  CK(cudaMemcpy(all.data(), h->st.resid, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < nsteps; k++)
+    for (int i = 0; i < bs; i++) {
+      double v = 0.0;
+      for (int c = 0; c < h->ncases; c++) v += all[((size_t)k * h->ncases + c) * bs + i];
+      resid[(size_t)bs * k + i] = v;
+    }
+  return JG_OK;
+}
+
+int jg_step(jg_case_t* h, int nsteps, double* resid) {
+  if (!h || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
+  if (!h->primed) RC(prime(h));
+  RC(enqueue_steps(h, nsteps));
   // a single case's residual history rides on the error-flag read's synchronisation
   const bool direct = resid && nsteps > 0 && h->ncases == 1;
   RC(check_err_flags(h, false, direct ? h->st.resid : nullptr, direct ? h->bs * (size_t)nsteps : 0, resid));
-  if (resid && nsteps > 0 && !direct) {
-    {
-      // the sum over the cases of the batch, per step
-      const int bs = h->bs;
-      std::vector<double> all(bs * (size_t)nsteps * h->ncases);
-      CK(cudaMemcpy(all.data(), h->st.resid, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
-      for (int k = 0; k < nsteps; k++)
-        for (int i = 0; i < bs; i++) {
-          double v = 0.0;
-          for (int c = 0; c < h->ncases; c++) v += all[((size_t)k * h->ncases + c) * bs + i];
-          resid[(size_t)bs * k + i] = v;
-        }
-    }
-  }
+  if (resid && nsteps > 0 && !direct) RC(batch_resid_sum(h, nsteps, resid));
   return JG_OK;
+}
+
+// set_state + step + get_state with one synchronisation: the state goes up, the preamble and the
+// steps run, the new state comes back into the same arrays
+int jg_step_host(jg_case_t* h, double* rho, double* rhou, double* rhoE, int nsteps, double* resid) {
+  if (!h || !rho || !rhou || !rhoE || nsteps < 0) return set_err(JG_ERR_ARG, "bad argument");
+  if (h->ncases != 1) return set_err(JG_ERR_ARG, "jg_step_host takes a single case (batches: jg_batch_*)");
+  RC(stage_state_in(h, rho, rhou, rhoE));
+  RC(prime_enqueue(h));
+  RC(enqueue_steps(h, nsteps));
+  RC(stage_state_out(h, rho, rhou, rhoE));
+  const size_t nres = resid && nsteps > 0 ? h->bs * (size_t)nsteps : 0;
+  return check_err_flags(h, true, nres ? h->st.resid : nullptr, nres, resid);
 }
 
 // per-case status of a batch: status[k] = error flags of case k since the last

@@ -106,10 +106,10 @@ struct State {
   int jac_lag;
   void* D0;
   long long* jac_next;   // [ncases]
-  // the face loop's residual and Jacobian kernels run on two streams, and a step's time step
-  // beside its gradients (host-side only)
+  // the face loop's residual and Jacobian kernels run on two streams; a step's control and time
+  // step run beside its gradients, its residual norms beside its relaxation (host-side only)
   cudaStream_t aux;
-  cudaEvent_t ev_fork, ev_join, ev_pre, ev_dt;
+  cudaEvent_t ev_fork, ev_join, ev_pre, ev_dt, ev_res, ev_resid;
 };
 
 // Transported scalars and turbulence-model arrays (coupled path only).

@@ -56,6 +56,7 @@ def lib():
         L.jg_get_stream.argtypes = [P, C.POINTER(P)]
         L.jg_set_state.argtypes = [P, D, D, D]
         L.jg_get_state.argtypes = [P, D, D, D]
+        L.jg_step_host.argtypes = [P, D, D, D, I, D]
         L.jg_calc_state.argtypes = [P]
         L.jg_get_primitives.argtypes = [P, D, D, D, D, D]
         L.jg_get_bfa.argtypes = [P, D, D, D, D, D, D, D]
@@ -252,6 +253,16 @@ class JoeGpu:
 
     def step_async(self, nsteps):
         _ck(lib().jg_step_async(self.h, int(nsteps)))
+
+    def step_host(self, rho, rhou, rhoE, nsteps, resid=None):
+        """``nsteps`` steps of a host-resident state, in place (jg_step_host): the arrays (C-contiguous
+        float64, ``rhou`` [ncv][3]) go up, the steps run, the new state comes back into them, with one
+        synchronisation.  ``resid`` ([nsteps][nvar] float64) receives the residual history."""
+        for a in (rho, rhou, rhoE):
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("step_host updates C-contiguous float64 arrays in place")
+        _ck(lib().jg_step_host(self.h, dptr(rho), dptr(rhou), dptr(rhoE), int(nsteps),
+                               dptr(resid) if resid is not None else None))
 
     def set_profiling(self, on=True):
         _ck(lib().jg_set_profiling(self.h, int(on)))

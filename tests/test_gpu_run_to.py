@@ -1,6 +1,7 @@
 """The driver-level entry points: jg_run_to (runBackwardEuler until the
 energy-residual drop, as doneSolver stops it), jg_set_params (run-time
-settings of a live handle) and jg_calc_grad (the gradient pass on its own).
+settings of a live handle), jg_calc_grad (the gradient pass on its own) and
+jg_step_host (a host-resident state stepped in place).
 Each is checked against the plain calls it must agree with, bit for bit."""
 import dataclasses
 
@@ -101,4 +102,39 @@ def test_calc_grad_equals_the_gradients_of_calc_rhs():
     ref = j.gradients()
     for k in ("grad_u", "grad_rho", "grad_p", "grad_enthalpy"):
         np.testing.assert_array_equal(got[k], ref[k])
+    j.close()
+
+
+@pytest.mark.parametrize("renumber", [0, 2])
+def test_step_host_is_set_step_get(renumber):
+    """jg_step_host (a host-resident state stepped in place, one synchronisation) gives, bit for
+    bit, what jg_set_state + jg_step + jg_get_state give, step after step, in the caller's order."""
+    g, prm = _bump()
+    st = case.perturbed_state(g.x_cv, prm, 0.0)
+    a = solver.JoeGpu(g, prm, renumber=renumber)
+    b = solver.JoeGpu(g, prm, renumber=renumber)
+    a.set_state(*st)
+    b.set_state(*st)
+    rho, rhou, rhoE = (np.array(x, dtype=np.float64, order="C") for x in st)
+    ra = np.zeros((3, 5))
+    for k in range(4):
+        a.step_host(rho, rhou, rhoE, 3, ra)
+        b.set_state(*b.get_state())
+        rb = b.runBackwardEuler(3)
+        np.testing.assert_array_equal(ra, rb)
+        for x, y in zip((rho, rhou, rhoE), b.get_state()):
+            np.testing.assert_array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_step_host_reports_a_nonphysical_state():
+    g, prm = _bump()
+    st = [np.array(x, dtype=np.float64, order="C") for x in case.perturbed_state(g.x_cv, prm, 0.0)]
+    j = solver.JoeGpu(g, prm)
+    j.set_state(*st)
+    st[2][7] = -abs(st[2][7])     # negative energy, so negative pressure, in one cell
+    with pytest.raises(solver.JoeGpuError) as e:
+        j.step_host(st[0], st[1], st[2], 1)
+    assert e.value.code == -4   # JG_ERR_STATE
     j.close()

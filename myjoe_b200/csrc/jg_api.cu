@@ -516,6 +516,13 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(upload(h, &m.x_fa, mesh->x_fa, 3 * (size_t)nfa));
   RC(upload(h, &m.fa_n, mesh->fa_normal, 3 * (size_t)nfa));
   RC(upload(h, &m.cvofa, mesh->cvofa, 2 * (size_t)nfa));
+  {
+    double *fu = nullptr, *fs = nullptr;
+    RC(dmalloc(h, &fu, 4 * (size_t)nfa));
+    RC(dmalloc(h, &fs, 4 * (size_t)(nfa - nfa_b)));
+    m.fa_u = fu;
+    m.fa_s = fs;
+  }
   RC(upload(h, &m.slot_i, fi, (size_t)N + 1));
   RC(upload(h, &m.slots, slots.data(), slots.size()));
   RC(upload(h, &m.nb_i, mesh->nbocv_i, (size_t)N + 1));
@@ -531,6 +538,8 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
   RC(upload(h, &m.ell_lower, ell_lower.data(), ell_lower.size()));
   RC(upload(h, &m.color, color.data(), color.size()));
   m.ncolors = ncolors;
+  launch_face_geo(m, (double*)m.fa_u, (double*)m.fa_s, h->stream);
+  CKL();
   // device state
   State& st = h->st;
   memset(&st, 0, sizeof(st));
@@ -765,7 +774,8 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
   const size_t nz = std::max(1, mesh->nzones);
   const size_t a[] = {
       // mesh
-      3 * N * d, N * d, 3 * nfa * d, 3 * nfa * d, 2 * nfa * i, (N + 1) * i, (size_t)fi[N] * sizeof(Slot),
+      3 * N * d, N * d, 3 * nfa * d, 3 * nfa * d, 2 * nfa * i, 4 * nfa * d, std::max<size_t>(4 * (nfa - nfa_b), 1) * d,
+      (N + 1) * i, (size_t)fi[N] * sizeof(Slot),
       (N + 1) * i, nbs * i, 3 * nbs * d, (N + 1) * i, std::max<size_t>(nbslot, 1) * i, 3 * nfa_b * d,
       nfa_b * i, nz * sizeof(DevZone), (nslices + 1) * i, rows * SLICE * i, rows * SLICE, N,
       // state

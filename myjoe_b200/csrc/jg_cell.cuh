@@ -11,10 +11,19 @@
 
 namespace jg {
 
+// the unit normal and area of face f (normVec3d of fa_normal, formed once per mesh by k_face_geo)
 __device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
-  double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
-  area = sqrt(dot3(n, n));
-  for (int i = 0; i < 3; i++) nV[i] = n[i] / area;
+  const double* u = &m.fa_u[4 * f];
+  for (int i = 0; i < 3; i++) nV[i] = u[i];
+  area = u[3];
+}
+
+// the unit vector from an internal face's cvofa[f][0] centre to its cvofa[f][1] centre and its
+// length (the viscous flux's sVec and smag, JoeWithModels.cpp:3626-3629)
+__device__ __forceinline__ void cell_to_cell(const Mesh& m, int f, double sV[3], double& smag) {
+  const double* s = &m.fa_s[4 * (f - m.nfa_b)];
+  for (int i = 0; i < 3; i++) sV[i] = s[i];
+  smag = s[3];
 }
 
 __device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, int c) {

@@ -36,9 +36,7 @@ struct TM {
 };
 
 __device__ __forceinline__ void unit_normal_c(const Mesh& m, int f, double nV[3], double& area) {
-  double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
-  area = sqrt(dot3(n, n));
-  for (int i = 0; i < 3; i++) nV[i] = n[i] / area;
+  unit_normal(m, f, nV, area);
 }
 __device__ __forceinline__ double sq(double x) { return x * x; }  // pow(x, 2.0) of the reference, exactly
 
@@ -947,10 +945,8 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
       }
       {
         VSideC<NS> v0 = vcell_c<NS>(m, st, t, p, c0, SST), v1 = vcell_c<NS>(m, st, t, p, c1, SST);
-        double sV[3];
-        for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-        double smag = sqrt(dot3(sV, sV));
-        for (int i = 0; i < 3; i++) sV[i] /= smag;
+        double sV[3], smag;
+        cell_to_cell(m, f, sV, smag);
         double alpha = dot3(nV, sV);
         double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
         double kine_fa = 0.0;

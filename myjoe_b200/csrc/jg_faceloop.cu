@@ -76,10 +76,8 @@ __global__ void __launch_bounds__(TB) k_res(Mesh m, Params p, State st, int for_
       }
       if (VISC) {
         VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-        double sV[3];
-        for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-        double smag = sqrt(dot3(sV, sV));
-        for (int i = 0; i < 3; i++) sV[i] /= smag;
+        double sV[3], smag;
+        cell_to_cell(m, f, sV, smag);
         double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
         double Fu[3], FE;
         VFace vf;
@@ -182,10 +180,8 @@ __global__ void __launch_bounds__(TB, jac_min_blocks<BT, KIND>()) k_jac(Mesh m, 
       JT vsg = JT(0);
       if (VISC) {
         VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-        double sV[3];
-        for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-        double smag = sqrt(dot3(sV, sV));
-        for (int i = 0; i < 3; i++) sV[i] /= smag;
+        double sV[3], smag;
+        cell_to_cell(m, f, sV, smag);
         double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
         double Fu[3], FE;
         VFace vf;

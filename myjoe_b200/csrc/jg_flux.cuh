@@ -816,6 +816,7 @@ struct VSide {
 // the "left hand side" momentum/energy fluxes and the face stress tau.
 struct VFace {
   double alpha, smag, area, mul, mut, keff;
+  double aos;  // alpha / smag
   double tau[3];
 };
 
@@ -823,13 +824,14 @@ __device__ inline void visc_flux(double Fu[3], double& FE, VFace& vf, const VSid
                                  double mut, double lamOcp, double PrTurb, const double* u_fa, double area,
                                  const double nV[3], double smag, const double sV[3]) {
   double alpha = dot3(nV, sV);
+  const double aos = alpha / smag;  // the normal-derivative weight, one division for all terms
   double g[9];
   for (int i = 0; i < 9; i++) g[i] = 0.5 * (s0.gu[i] + s1.gu[i]);
   double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
   double div = g[0] + g[4] + g[8];
   double tau[3];
   for (int i = 0; i < 3; i++) {
-    double b = alpha * (s1.u[i] - s0.u[i]) / smag + g[3 * i + 0] * fC[0] + g[0 + i] * nV[0] + g[3 * i + 1] * fC[1] +
+    double b = (s1.u[i] - s0.u[i]) * aos + g[3 * i + 0] * fC[0] + g[0 + i] * nV[0] + g[3 * i + 1] * fC[1] +
                g[3 + i] * nV[1] + g[3 * i + 2] * fC[2] + g[6 + i] * nV[2];
     double tl = mul * b - (2.0 / 3.0 * mul * div) * nV[i];
     double tt = mut * b - (2.0 / 3.0 * mut * div) * nV[i];
@@ -837,10 +839,10 @@ __device__ inline void visc_flux(double Fu[3], double& FE, VFace& vf, const VSid
   }
   for (int i = 0; i < 3; i++) Fu[i] = -area * tau[i];
   double keff = lamOcp + mut / PrTurb;
-  double enth = keff * (alpha * (s1.h - s0.h) / smag +
+  double enth = keff * ((s1.h - s0.h) * aos +
                         0.5 * ((s0.gh[0] + s1.gh[0]) * fC[0] + (s0.gh[1] + s1.gh[1]) * fC[1] + (s0.gh[2] + s1.gh[2]) * fC[2]));
   FE = -area * (enth + tau[0] * u_fa[0] + tau[1] * u_fa[1] + tau[2] * u_fa[2]);
-  vf.alpha = alpha; vf.smag = smag; vf.area = area; vf.mul = mul; vf.mut = mut; vf.keff = keff;
+  vf.alpha = alpha; vf.smag = smag; vf.area = area; vf.mul = mul; vf.mut = mut; vf.keff = keff; vf.aos = aos;
   for (int i = 0; i < 3; i++) vf.tau[i] = tau[i];
 }
 
@@ -860,13 +862,13 @@ template <typename T, typename Acc>
 __device__ inline void visc_jac_add(Acc acc, T sgn, int side, const VFace& vf, const VSide& s,
                                     const double* u_fa) {
   // inputs rounded to T once, the arithmetic in T (FP64: the reference's expressions term by term)
-  const T mm = (T)(vf.mul + vf.mut), alpha = (T)vf.alpha, smag = (T)vf.smag, area = (T)vf.area, keff = (T)vf.keff;
+  const T mm = (T)(vf.mul + vf.mut), aos = (T)vf.aos, area = (T)vf.area, keff = (T)vf.keff;
   const T tau[3] = {(T)vf.tau[0], (T)vf.tau[1], (T)vf.tau[2]};
   const T uf[3] = {(T)u_fa[0], (T)u_fa[1], (T)u_fa[2]};
   const T rho = (T)s.rho, hh = (T)s.h, RR = (T)s.R, TT = (T)s.T, gam = (T)s.gam;
   const T u[3] = {(T)s.u[0], (T)s.u[1], (T)s.u[2]};
-  T d = (side == 0) ? -mm * alpha / smag * area : mm * alpha / smag * area;
-  T f44 = (side == 0) ? -area * keff * alpha / smag : area * keff * alpha / smag;
+  T d = (side == 0) ? -mm * aos * area : mm * aos * area;
+  T f44 = (side == 0) ? -area * keff * aos : area * keff * aos;
   T f4[3] = {area * tau[0] * T(0.5) + uf[0] * d, area * tau[1] * T(0.5) + uf[1] * d,
              area * tau[2] * T(0.5) + uf[2] * d};
   T ir = T(1.0) / rho;

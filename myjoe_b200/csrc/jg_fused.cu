@@ -75,10 +75,8 @@ __global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, 
         }
         if (VISC) {
           VSide v0 = cell_vside(p, st, c0), v1 = cell_vside(p, st, c1);
-          double sV[3];
-          for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
-          double smag = sqrt(dot3(sV, sV));
-          for (int i = 0; i < 3; i++) sV[i] /= smag;
+          double sV[3], smag;
+          cell_to_cell(m, f, sV, smag);
           double ufa[3] = {0.5 * (v0.u[0] + v1.u[0]), 0.5 * (v0.u[1] + v1.u[1]), 0.5 * (v0.u[2] + v1.u[2])};
           double Fu[3], FE;
           VFace vf;

@@ -39,6 +39,11 @@ struct Mesh {
   const double* vol;       // [N]
   const double* x_fa;      // [nfa][3]
   const double* fa_n;      // [nfa][3] area-weighted normal
+  // static face geometry, formed once per mesh (k_face_geo) with the expressions the face loop used
+  // to evaluate per face: fa_u[nfa][4] the unit normal and the area; fa_s[nfa - nfa_b][4] the unit
+  // vector from cvofa[f][0]'s centre to cvofa[f][1]'s and its length (sVec, smag) of internal faces
+  const double* fa_u;
+  const double* fa_s;
   const int* cvofa;        // [nfa][2]
   const int* slot_i;       // [N+1] cell -> face slots (reference faocv order)
   const Slot* slots;       // [faocv_s]
@@ -183,6 +188,7 @@ void launch_grad(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int for_step, cudaStream_t s);
 void launch_flux_fused(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s);
 void launch_face_sensors(const Mesh& m, const Params& p, State& st, cudaStream_t s);
+void launch_face_geo(const Mesh& m, double* fa_u, double* fa_s, cudaStream_t s);
 // face-loop launch shapes: split (residual kernel with FL lanes per cell + Jacobian kernel)
 // are JG_FLUX_SPLIT + FL; the others are the fused kernel's
 inline bool flux_split(const Params& p, const State& st) { return p.flux_cl >= JG_FLUX_SPLIT || st.jac_lag > 1; }

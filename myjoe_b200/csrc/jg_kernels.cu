@@ -1063,6 +1063,29 @@ void launch_unpack_state(int n, const double* q, double* io, const int* perm, cu
 }
 constexpr int TB = 128;
 
+// static face geometry, once per mesh: the unit normal and area of every face; for internal
+// faces the unit vector between the cell centres and its length
+__global__ void k_face_geo(Mesh m, double* fa_u, double* fa_s) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nfa) return;
+  const double n[3] = {m.fa_n[3 * f], m.fa_n[3 * f + 1], m.fa_n[3 * f + 2]};
+  const double area = sqrt(dot3(n, n));
+  for (int i = 0; i < 3; i++) fa_u[4 * f + i] = n[i] / area;
+  fa_u[4 * f + 3] = area;
+  if (f >= m.nfa_b) {
+    const int c0 = m.cvofa[2 * f], c1 = m.cvofa[2 * f + 1];
+    double sV[3];
+    for (int i = 0; i < 3; i++) sV[i] = m.x_cv[3 * c1 + i] - m.x_cv[3 * c0 + i];
+    const double smag = sqrt(dot3(sV, sV));
+    double* o = &fa_s[4 * (f - m.nfa_b)];
+    for (int i = 0; i < 3; i++) o[i] = sV[i] / smag;
+    o[3] = smag;
+  }
+}
+void launch_face_geo(const Mesh& m, double* fa_u, double* fa_s, cudaStream_t s) {
+  if (m.nfa > 0) k_face_geo<<<grid_for(m.nfa, TB), TB, 0, s>>>(m, fa_u, fa_s);
+}
+
 void launch_state(const Mesh& m, const Params& p, State& st, cudaStream_t s) {
   k_state<<<grid_for(m.ncv, TB), TB, 0, s>>>(m, p, st);
 }

@@ -18,7 +18,7 @@ namespace jg {
 
 // row i of calcJacobianA (UgpWithCvCompFlow.cpp:666-709), nV carrying the face area
 template <typename T>
-__device__ __forceinline__ void jacobian_A_row(T* A, int i, const T* vel, T pp, T rrho, const T* nV, T gamma) {
+__device__ __forceinline__ void jacobian_A_row(T* A, int i, const T* vel, T c2, T ikm1, const T* nV, T gamma) {
   const T km1 = gamma - T(1.0);
   const T nVel[3] = {vel[0] * nV[0], vel[1] * nV[1], vel[2] * nV[2]};
   const T U_k = nVel[0] + nVel[1] + nVel[2];
@@ -49,10 +49,7 @@ __device__ __forceinline__ void jacobian_A_row(T* A, int i, const T* vel, T pp, 
       A[4] = km1 * nV[2];
       break;
     default: {
-      T c2 = gamma * pp / rrho;
-      const T c = sqrt(c2);
-      c2 = c * c;
-      const T ikm1 = T(1.0) / km1;
+      // c2: the square of c = sqrt(gamma p / rho) (the reference squares the root), ikm1 = 1 / (gamma - 1)
       A[0] = U_k * ((gamma - T(2.)) * vsh - c2 * ikm1);
       A[1] = c2 * ikm1 * nV[0] - km1 * vel[0] * (nVel[1] + nVel[2]) - (km1 * vel[0] * vel[0] - vsh) * nV[0];
       A[2] = c2 * ikm1 * nV[1] - km1 * vel[1] * (nVel[0] + nVel[2]) - (km1 * vel[1] * vel[1] - vsh) * nV[1];
@@ -80,16 +77,18 @@ __device__ __forceinline__ void roe_rows(const FStateT<T>& L, const FStateT<T>& 
   const T tmp = T(1.0) / (T(1.0) + Rrho);
   const T v[3] = {tmp * (L.u[0] + R.u[0] * Rrho), tmp * (L.u[1] + R.u[1] * Rrho), tmp * (L.u[2] + R.u[2] * Rrho)};
   const T uRoe = dot3(v, nV);
-  const T gpr = tmp * ((L.gam * L.p / L.rho + T(0.5) * (L.gam - T(1.0)) * uLuL) +
-                       (R.gam * R.p / R.rho + T(0.5) * (R.gam - T(1.0)) * uRuR) * Rrho);
+  // gamma p / rho of each side: in the Roe sound speed and (rooted and squared) in calcJacobianA
+  const T gpL = L.gam * L.p / L.rho, gpR = R.gam * R.p / R.rho;
+  const T gpr = tmp * ((gpL + T(0.5) * (L.gam - T(1.0)) * uLuL) + (gpR + T(0.5) * (R.gam - T(1.0)) * uRuR) * Rrho);
   const T c = sqrt(gpr - ((L.gam + R.gam) * T(0.5) - T(1.0)) * T(0.5) * dot3(v, v));
   const T gamma = T(0.5) * (L.gam + R.gam);
-  const T km1 = gamma - T(1.0);
-  const T c2 = c * c, vS = dot3(v, v);
+  const T km1 = gamma - T(1.0), ikm1 = T(1.0) / km1;
+  const T cL = sqrt(gpL), cR = sqrt(gpR), c2L = cL * cL, c2R = cR * cR;
+  const T c2 = c * c, vS = dot3(v, v), ic = T(1.0) / c;
   const T l1 = fabs(uRoe), l4 = fabs(uRoe + c), l5 = fabs(uRoe - c);
   const T a2 = T(0.5) * (l4 - l5), a3 = T(0.5) * (l4 + l5) - l1;
-  const T hA = c2 / km1 + T(0.5) * vS;
-  const T cgr = a3 * km1 / c2, cmr = -a2 / c, cgs = a2 * km1 / c, cms = -a3;
+  const T hA = c2 * ikm1 + T(0.5) * vS;
+  const T cgr = a3 * km1 * ic * ic, cmr = -a2 * ic, cgs = a2 * km1 * ic, cms = -a3;
   const T g[5] = {T(0.5) * vS, -v[0], -v[1], -v[2], T(1.0)};
   const T mv[5] = {uRoe, -nV[0], -nV[1], -nV[2], T(0.0)};
   T wr[5], ws[5];
@@ -103,8 +102,8 @@ __device__ __forceinline__ void roe_rows(const FStateT<T>& L, const FStateT<T>& 
 #pragma unroll
   for (int i = 0; i < 5; i++) {
     T aL[5], aR[5];
-    jacobian_A_row(aL, i, L.u, L.p, L.rho, nA, gamma);
-    jacobian_A_row(aR, i, R.u, R.p, R.rho, nA, gamma);
+    jacobian_A_row(aL, i, L.u, c2L, ikm1, nA, gamma);
+    jacobian_A_row(aR, i, R.u, c2R, ikm1, nA, gamma);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const T pm = rv[i] * wr[j] + sv[i] * ws[j] + (i == j ? l1 : T(0.0));
@@ -149,7 +148,8 @@ __device__ __forceinline__ void hllc_rows(const FStateT<T>& L, const FStateT<T>&
 #pragma unroll
     for (int i = 0; i < 5; i++) {
       T aj[5], az[5] = {T(0.0), T(0.0), T(0.0), T(0.0), T(0.0)};
-      jacobian_A_row(aj, i, Su, Sp, Srho, nA, gmean);
+      const T cS = sqrt(gmean * Sp / Srho);
+      jacobian_A_row(aj, i, Su, cS * cS, T(1.0) / (gmean - T(1.0)), nA, gmean);
       if (left) emit(i, aj, az);
       else emit(i, az, aj);
     }
@@ -276,13 +276,13 @@ struct VJacRows {
 
 template <typename T>
 __device__ __forceinline__ VJacRows<T> vjac_rows(int side, const VFace& vf, const VSide& s, const double* u_fa) {
-  const T mm = (T)(vf.mul + vf.mut), alpha = (T)vf.alpha, smag = (T)vf.smag, area = (T)vf.area, keff = (T)vf.keff;
+  const T mm = (T)(vf.mul + vf.mut), aos = (T)vf.aos, area = (T)vf.area, keff = (T)vf.keff;
   const T tau[3] = {(T)vf.tau[0], (T)vf.tau[1], (T)vf.tau[2]};
   const T uf[3] = {(T)u_fa[0], (T)u_fa[1], (T)u_fa[2]};
   const T rho = (T)s.rho, hh = (T)s.h, RR = (T)s.R, TT = (T)s.T, gam = (T)s.gam;
   const T u[3] = {(T)s.u[0], (T)s.u[1], (T)s.u[2]};
-  const T d = (side == 0) ? -mm * alpha / smag * area : mm * alpha / smag * area;
-  const T f44 = (side == 0) ? -area * keff * alpha / smag : area * keff * alpha / smag;
+  const T d = (side == 0) ? -mm * aos * area : mm * aos * area;
+  const T f44 = (side == 0) ? -area * keff * aos : area * keff * aos;
   const T f4[3] = {area * tau[0] * T(0.5) + uf[0] * d, area * tau[1] * T(0.5) + uf[1] * d,
                    area * tau[2] * T(0.5) + uf[2] * d};
   const T ir = T(1.0) / rho;

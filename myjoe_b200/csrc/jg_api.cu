@@ -224,6 +224,7 @@ static Params make_params(const jg_params& q) {
   memset(&p, 0, sizeof(p));
   p.gamma = q.gamma;
   p.R = q.R_gas;
+  p.cp = p.gamma * p.R / (p.gamma - 1.0);
   p.Pr = q.Pr;
   p.PrTurb = q.PrTurb;
   p.mu_mode = q.mu_mode;

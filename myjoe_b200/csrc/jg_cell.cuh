@@ -49,7 +49,7 @@ __device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const St
   s.p = pp;
   for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
   const double T = pp / (rr * p.R);  // calcThermoProp_p at the face
-  s.h = p.gamma * p.R / (p.gamma - 1.0) * T;
+  s.h = p.cp * T;
   return s;
 }
 

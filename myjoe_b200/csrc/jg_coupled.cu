@@ -806,7 +806,7 @@ __device__ __forceinline__ CState<NS> recon_c(const Mesh& m, const Params& p, co
   s.rho = rr;
   s.p = pp;
   s.T = pp / (rr * p.R);
-  s.h = p.gamma * p.R / (p.gamma - 1.0) * s.T;
+  s.h = p.cp * s.T;
   s.k = sst ? s.sc[0] : 0.0;
   return s;
 }

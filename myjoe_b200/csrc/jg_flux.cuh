@@ -257,10 +257,10 @@ __device__ inline void matrices_hllc(T* AL, T* AR, const FStateT<T>& L, const FS
 // c^2 < 1e-12 leaves only the central part, as in the reference's early return)
 __device__ inline void flux_roe(double F[5], const FState& L, const FState& R, double area, const double nV[3]) {
   double gamma = 0.5 * (L.gam + R.gam);
-  double gm1 = gamma - 1.0;
+  double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
   double run0 = L.rho * dot3(L.u, nV), run1 = R.rho * dot3(R.u, nV);
-  double rE0 = L.p / gm1 + 0.5 * L.rho * dot3(L.u, L.u);
-  double rE1 = R.p / gm1 + 0.5 * R.rho * dot3(R.u, R.u);
+  double rE0 = L.p * igm1 + 0.5 * L.rho * dot3(L.u, L.u);
+  double rE1 = R.p * igm1 + 0.5 * R.rho * dot3(R.u, R.u);
   double H0 = (rE0 + L.p) / L.rho, H1 = (rE1 + R.p) / R.rho;
   double ha = 0.5 * area;
   F[0] = ha * (run0 + run1);
@@ -273,7 +273,7 @@ __device__ inline void flux_roe(double F[5], const FState& L, const FState& R, d
   double alA = 0.5 * (ua * ua + va * va + wa * wa);
   double a2 = gm1 * (hA - alA);
   if (a2 < 1.0e-12) return;
-  double aA = sqrt(a2);
+  double aA = sqrt(a2), iaA = 1.0 / aA;
   double unA = ua * nV[0] + va * nV[1] + wa * nV[2];
   double dr = R.rho - L.rho;
   double dru = R.rho * R.u[0] - L.rho * L.u[0];
@@ -284,8 +284,8 @@ __device__ inline void flux_roe(double F[5], const FState& L, const FState& R, d
   double a1 = 0.5 * (l2 + l3), ab2 = 0.5 * (l2 - l3), ab3 = a1 - l1;
   double ab4 = gm1 * (alA * dr - ua * dru - va * drv - wa * drw + drE);
   double ab5 = unA * dr - nV[0] * dru - nV[1] * drv - nV[2] * drw;
-  double ab6 = ab3 * ab4 / a2 - ab2 * ab5 / aA;
-  double ab7 = ab3 * ab5 - ab2 * ab4 / aA;
+  double ab6 = ab3 * ab4 * (iaA * iaA) - ab2 * ab5 * iaA;
+  double ab7 = ab3 * ab5 - ab2 * ab4 * iaA;
   F[0] -= ha * (l1 * dr + ab6);
   F[1] -= ha * (l1 * dru + ua * ab6 - nV[0] * ab7);
   F[2] -= ha * (l1 * drv + va * ab6 - nV[1] * ab7);

@@ -141,6 +141,7 @@ struct Turb {
 
 struct Params {
   double gamma, R, Pr, PrTurb;
+  double cp;        // gamma R / (gamma - 1), the enthalpy per kelvin (set with gamma and R)
   int mu_mode, flux;
   double mu_ref, mu_pow, SL_T, SL_S, T_ref;
   int second_order, limiter;

@@ -41,7 +41,7 @@ __device__ __forceinline__ void state_from_q(const Params& p, const double* q, d
   prim[2] = u[2];
   prim[3] = pp;
   prim[4] = T;
-  prim[5] = p.gamma * p.R / (p.gamma - 1.0) * T;
+  prim[5] = p.cp * T;
   prim[6] = sqrt(p.gamma * pp / r);
 }
 
@@ -120,7 +120,7 @@ __device__ __forceinline__ void bc_face(const Mesh& m, const Params& p, State& s
   unit_normal(m, f, nV, area);
   double T = 0.0, v[3] = {0.0, 0.0, 0.0}, pb = 0.0, h;
   double rho_ff = 0.0;
-  double cp = p.gamma * p.R / (p.gamma - 1.0);
+  double cp = p.cp;
   switch (z.kind) {
     case JG_BC_CBC: {
       if (dot3(z.v, nV) > 0.0) {

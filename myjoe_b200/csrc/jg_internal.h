@@ -190,6 +190,11 @@ void launch_flux(const Mesh& m, const Params& p, State& st, int implicit, int fo
 void launch_flux_fused(const Mesh& m, const Params& p, State& st, int for_step, cudaStream_t s);
 void launch_face_sensors(const Mesh& m, const Params& p, State& st, cudaStream_t s);
 void launch_face_geo(const Mesh& m, double* fa_u, double* fa_s, cudaStream_t s);
+// jg_step_host's upload (pack + state + history base) and download (unpack + flags + residuals)
+void launch_state_in(const Mesh& m, const Params& p, State& st, const double* rho, const double* rhou,
+                     const double* rhoE, const int* perm, cudaStream_t s);
+void launch_state_out(const Mesh& m, State& st, double* rho, double* rhou, double* rhoE, const int* perm, double* out,
+                      int nres, cudaStream_t s);
 // face-loop launch shapes: split (residual kernel with FL lanes per cell + Jacobian kernel)
 // are JG_FLUX_SPLIT + FL; the others are the fused kernel's
 inline bool flux_split(const Params& p, const State& st) { return p.flux_cl >= JG_FLUX_SPLIT || st.jac_lag > 1; }

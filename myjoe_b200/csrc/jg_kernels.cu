@@ -1049,9 +1049,58 @@ __global__ void k_aos_to_soa5(int n, const double* aos, double* soa) {
   for (int i = 0; i < 5; i++) soa[(size_t)i * n + c] = aos[5 * (size_t)c + i];
 }
 
+// A host-resident state stepped in place (jg_step_host, one case, 5x5): the upload's pack fused
+// with calcStateVariables (the state preamble's memset of the primitives kept as prim[3] = 0,
+// the only entry state_from_q reads), the history base of the call and the lag schedule's reset
+// rho, rhou, rhoE: the staged copy of the caller's arrays in device memory
+__global__ void k_state_in(Mesh m, Params p, State st, const double* rho, const double* rhou, const double* rhoE,
+                           const int* perm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) {
+    st.ctrl[4] = st.ctrl[1];
+    if (st.jac_next) st.jac_next[0] = 0;
+  }
+  if (c >= m.ncv) return;
+  const int r = perm ? perm[c] : c;
+  double q[5], prim[8];
+  q[0] = rho[r];
+  for (int i = 0; i < 3; i++) q[1 + i] = rhou[3 * r + i];
+  q[4] = rhoE[r];
+  for (int i = 0; i < 5; i++) st.q[5 * c + i] = q[i];
+  for (int i = 0; i < 8; i++) prim[i] = 0.0;
+  state_from_q(p, q, prim, st.case_err + m.case_of[c]);
+  for (int i = 0; i < 8; i++) st.prim[8 * c + i] = prim[i];
+}
+// ... and the download's unpack with the call's error flags and residual history gathered into
+// out[0..2+nres) (err, case_err[0], resid), the flags cleared for the next call
+__global__ void k_state_out(Mesh m, State st, double* rho, double* rhou, double* rhoE, const int* perm, double* out,
+                            int nres) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) {
+    out[0] = (double)*st.err;
+    out[1] = (double)st.case_err[0];
+    *st.err = 0;
+    st.case_err[0] = 0;
+  }
+  if (c < nres) out[2 + c] = st.resid[c];
+  if (c >= m.ncv) return;
+  const int r = perm ? perm[c] : c;
+  rho[r] = st.q[5 * c];
+  for (int i = 0; i < 3; i++) rhou[3 * r + i] = st.q[5 * c + 1 + i];
+  rhoE[r] = st.q[5 * c + 4];
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+void launch_state_in(const Mesh& m, const Params& p, State& st, const double* rho, const double* rhou,
+                     const double* rhoE, const int* perm, cudaStream_t s) {
+  k_state_in<<<grid_for(m.ncv, 256), 256, 0, s>>>(m, p, st, rho, rhou, rhoE, perm);
+}
+void launch_state_out(const Mesh& m, State& st, double* rho, double* rhou, double* rhoE, const int* perm, double* out,
+                      int nres, cudaStream_t s) {
+  k_state_out<<<grid_for(m.ncv > nres ? m.ncv : nres, 256), 256, 0, s>>>(m, st, rho, rhou, rhoE, perm, out, nres);
+}
 void launch_aos_to_soa5(int n, const double* aos, double* soa, cudaStream_t s) {
   k_aos_to_soa5<<<grid_for(n, 256), 256, 0, s>>>(n, aos, soa);
 }

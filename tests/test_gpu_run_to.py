@@ -105,17 +105,24 @@ def test_calc_grad_equals_the_gradients_of_calc_rhs():
     j.close()
 
 
-@pytest.mark.parametrize("renumber", [0, 2])
-def test_step_host_is_set_step_get(renumber):
+@pytest.mark.parametrize("renumber,pinned", [(0, False), (2, False), (0, True), (2, True)])
+def test_step_host_is_set_step_get(renumber, pinned):
     """jg_step_host (a host-resident state stepped in place, one synchronisation) gives, bit for
-    bit, what jg_set_state + jg_step + jg_get_state give, step after step, in the caller's order."""
+    bit, what jg_set_state + jg_step + jg_get_state give, step after step, in the caller's order,
+    from pageable and from page-locked arrays."""
+    import torch
     g, prm = _bump()
     st = case.perturbed_state(g.x_cv, prm, 0.0)
     a = solver.JoeGpu(g, prm, renumber=renumber)
     b = solver.JoeGpu(g, prm, renumber=renumber)
     a.set_state(*st)
     b.set_state(*st)
-    rho, rhou, rhoE = (np.array(x, dtype=np.float64, order="C") for x in st)
+    if pinned:
+        rho, rhou, rhoE = (torch.empty(np.shape(x), dtype=torch.float64, pin_memory=True).numpy() for x in st)
+        for x, y in zip((rho, rhou, rhoE), st):
+            x[...] = y
+    else:
+        rho, rhou, rhoE = (np.array(x, dtype=np.float64, order="C") for x in st)
     ra = np.zeros((3, 5))
     for k in range(4):
         a.step_host(rho, rhou, rhoE, 3, ra)

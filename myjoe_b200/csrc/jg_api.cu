@@ -83,6 +83,13 @@ struct jg_case {
   size_t hpin_bytes = 0;
   double* d_out = nullptr;  // jg_step_host: the call's flags and residuals gathered on the device
   int d_out_cap = 0;
+  long graph_gen = 0;       // counts the step graph's instantiations
+  // jg_step_host on page-locked arrays, one step: the whole call (copies, state passes, the
+  // step, copies back) captured as one graph, for the arrays, staging and step graph it was made with
+  cudaGraphExec_t host_graph = nullptr;
+  const void* host_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  long host_gen = -1;
+  int host_nres = -1;
   int async_alloc = 0;      // stream-ordered allocation (serving): no device-wide sync on free
   size_t bytes = 0;         // device bytes held by this handle
   int bs = 5;               // block size: 5, or 6 on the coupled SA path
@@ -330,6 +337,7 @@ int jg_device_count(int* n) {
 int jg_destroy(jg_case_t* h) {
   if (!h) return JG_OK;
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
   for (int i = 0; i < 4; i++)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->async_alloc) {
@@ -1592,6 +1600,7 @@ static int ensure_graph(jg_case* h) {
   CK(cudaGraphInstantiate(&h->graph, g, 0));
   cudaGraphDestroy(g);
   h->graph_sweeps = sweeps;
+  h->graph_gen++;
   return JG_OK;
 }
 
@@ -1647,6 +1656,37 @@ int jg_step(jg_case_t* h, int nsteps, double* resid) {
   return JG_OK;
 }
 
+// jg_step_host's stream work on the 5x5 path: the copies up, one kernel (pack + state + history
+// base), one (setBC + face properties), the steps (recorded in place when captured), one kernel
+// (unpack + flags + residuals gathered), the copies down.  The kernels reading and writing
+// page-locked caller memory in place over the bus measured slower than the copy engines (495
+// against 381 us a step on a 49k-cell case), so the state is staged.
+static int host_step_enqueue(jg_case* h, double* rho, double* rhou, double* rhoE, int nsteps, int nres, void* hp,
+                             bool capture) {
+  const size_t N = h->ncv;
+  double* ir = h->d_io;
+  double* iu = h->d_io + N;
+  double* ie = h->d_io + 4 * N;
+  CK(cudaMemcpyAsync(ir, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(iu, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(ie, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_state_in(h->m, h->p, h->st, ir, iu, ie, h->d_cell_old, h->stream);
+  launch_faces_after_update(h->m, h->p, h->st, h->stream);
+  if (capture) {
+    for (int k = 0; k < nsteps; k++) RC(enqueue_step(h, 1));
+  } else {
+    h->primed = 1;
+    RC(enqueue_steps(h, nsteps, true));
+  }
+  launch_state_out(h->m, h->st, ir, iu, ie, h->d_cell_old, h->d_out, nres, h->stream);
+  CKL();
+  CK(cudaMemcpyAsync(rho, ir, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(rhou, iu, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(rhoE, ie, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(hp, h->d_out, (2 + (size_t)nres) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return JG_OK;
+}
+
 // set_state + step + get_state with one synchronisation: the state goes up, the preamble and the
 // steps run, the new state comes back into the same arrays
 int jg_step_host(jg_case_t* h, double* rho, double* rhou, double* rhoE, int nsteps, double* resid) {
@@ -1667,24 +1707,42 @@ int jg_step_host(jg_case_t* h, double* rho, double* rhou, double* rhoE, int nste
     }
     void* hp = nullptr;
     RC(pinned(h, (2 + (size_t)nres) * sizeof(double), &hp));
-    // the staging copies (the kernels reading and writing page-locked caller memory in place over
-    // the bus measured slower than the copy engines: 495 against 381 us a step on a 49k-cell case)
-    double* ir = h->d_io;
-    double* iu = h->d_io + N;
-    double* ie = h->d_io + 4 * N;
-    CK(cudaMemcpyAsync(ir, rho, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(iu, rhou, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(ie, rhoE, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    launch_state_in(h->m, h->p, h->st, ir, iu, ie, h->d_cell_old, h->stream);
-    launch_faces_after_update(h->m, h->p, h->st, h->stream);
-    h->primed = 1;
-    RC(enqueue_steps(h, nsteps, true));
-    launch_state_out(h->m, h->st, ir, iu, ie, h->d_cell_old, h->d_out, nres, h->stream);
-    CKL();
-    CK(cudaMemcpyAsync(rho, ir, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(rhou, iu, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(rhoE, ie, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(hp, h->d_out, (2 + (size_t)nres) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // one step on page-locked arrays: the whole call as one graph (made once for these arrays)
+    bool locked = nsteps == 1 && h->hp.lin_solver != JG_LS_BCGSTAB && h->hp.lin_solver != JG_LS_BCGSTAB_LINELET;
+    const double* arr[3] = {rho, rhou, rhoE};
+    for (int i = 0; i < 3 && locked; i++) {
+      cudaPointerAttributes a;
+      if (cudaPointerGetAttributes(&a, arr[i]) != cudaSuccess) {
+        cudaGetLastError();  // an unregistered pointer is not an error here
+        locked = false;
+      } else {
+        locked = a.type == cudaMemoryTypeHost;
+      }
+    }
+    if (locked) {
+      RC(ensure_graph(h));  // (the history holds 64 steps from the start)
+      const void* key[5] = {rho, rhou, rhoE, hp, h->d_out};
+      if (!h->host_graph || h->host_gen != h->graph_gen || memcmp(key, h->host_key, sizeof(key)) != 0 ||
+          h->host_nres != nres) {
+        if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
+        h->host_graph = nullptr;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = host_step_enqueue(h, rho, rhou, rhoE, 1, nres, hp, true);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (rc != JG_OK) return rc;
+        if (e != cudaSuccess) return set_err(JG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        CK(cudaGraphInstantiate(&h->host_graph, g, 0));
+        cudaGraphDestroy(g);
+        memcpy(h->host_key, key, sizeof(key));
+        h->host_gen = h->graph_gen;
+        h->host_nres = nres;
+      }
+      CK(cudaGraphLaunch(h->host_graph, h->stream));
+      h->primed = 1;
+    } else {
+      RC(host_step_enqueue(h, rho, rhou, rhoE, nsteps, nres, hp, false));
+    }
     CK(cudaStreamSynchronize(h->stream));
     const double* o = (const double*)hp;
     if (nres) memcpy(resid, o + 2, nres * sizeof(double));

@@ -123,11 +123,12 @@ def test_step_host_is_set_step_get(renumber, pinned):
             x[...] = y
     else:
         rho, rhou, rhoE = (np.array(x, dtype=np.float64, order="C") for x in st)
-    ra = np.zeros((3, 5))
+    ns = 1 if pinned else 3   # one step on page-locked arrays: the call's own captured graph
+    ra = np.zeros((ns, 5))
     for k in range(4):
-        a.step_host(rho, rhou, rhoE, 3, ra)
+        a.step_host(rho, rhou, rhoE, ns, ra)
         b.set_state(*b.get_state())
-        rb = b.runBackwardEuler(3)
+        rb = b.runBackwardEuler(ns)
         np.testing.assert_array_equal(ra, rb)
         for x, y in zip((rho, rhou, rhoE), b.get_state()):
             np.testing.assert_array_equal(x, y)

@@ -11,6 +11,32 @@
 
 namespace jg {
 
+// an L1 prefetch of the cache line holding p (a hint: no registers held, no wait)
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// the face loop's reads of a neighbour cell c, prefetched a face ahead: its state, primitives,
+// centre, gradients (and the viscous gradients)
+__device__ __forceinline__ void prefetch_cell(const State& st, const Mesh& m, int c, bool visc) {
+  prefetch_l1(&st.q[5 * c]);
+  prefetch_l1(&st.prim[8 * c]);
+  prefetch_l1(&m.x_cv[3 * c]);
+  prefetch_l1(&st.grho[3 * c]);
+  prefetch_l1(&st.gp[3 * c]);
+  prefetch_l1(&st.gu[9 * c]);
+  if (visc) {
+    prefetch_l1(&st.guv[9 * c]);
+    prefetch_l1(&st.gh[3 * c]);
+  }
+}
+
+// the Jacobian kernel's reads of a neighbour cell c: its state and primitives (and the viscous
+// gradient the viscous matrices' stress needs)
+__device__ __forceinline__ void prefetch_cell_jac(const State& st, int c, bool visc) {
+  prefetch_l1(&st.q[5 * c]);
+  prefetch_l1(&st.prim[8 * c]);
+  if (visc) prefetch_l1(&st.guv[9 * c]);
+}
+
 // the unit normal and area of face f (normVec3d of fa_normal, formed once per mesh by k_face_geo)
 __device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
   const double* u = &m.fa_u[4 * f];
@@ -36,18 +62,24 @@ __device__ __forceinline__ FState cell_fstate(const Params& p, const State& st, 
   return s;
 }
 
-// second-order reconstruction at x_fa with the first-order fallback, JoeWithModels.cpp:2832-2921
+// second-order reconstruction at x_fa with the first-order fallback, JoeWithModels.cpp:2832-2921;
+// every input is loaded before the fallback test, so the gathers are in flight together
 __device__ __forceinline__ FState recon(const Mesh& m, const Params& p, const State& st, int c, int f) {
   FState s = cell_fstate(p, st, c);
   if (!p.second_order) return s;
-  double r0[3];
-  for (int i = 0; i < 3; i++) r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
-  double rr = s.rho + dot3(r0, &st.grho[3 * c]);
-  double pp = s.p + dot3(r0, &st.gp[3 * c]);
+  double r0[3], gr[3], gp[3], gu[9];
+  for (int i = 0; i < 3; i++) {
+    r0[i] = m.x_fa[3 * f + i] - m.x_cv[3 * c + i];
+    gr[i] = st.grho[3 * c + i];
+    gp[i] = st.gp[3 * c + i];
+  }
+  for (int i = 0; i < 9; i++) gu[i] = st.gu[9 * c + i];
+  double rr = s.rho + dot3(r0, gr);
+  double pp = s.p + dot3(r0, gp);
   if ((pp <= 0.0) || (rr <= 0.0)) return s;  // first order: the cell's own h is calcThermoProp_p of (p, rho)
   s.rho = rr;
   s.p = pp;
-  for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &st.gu[9 * c + 3 * i]);
+  for (int i = 0; i < 3; i++) s.u[i] += dot3(r0, &gu[3 * i]);
   const double T = pp / (rr * p.R);  // calcThermoProp_p at the face
   s.h = p.cp * T;
   return s;

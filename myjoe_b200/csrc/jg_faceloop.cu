@@ -58,9 +58,17 @@ __global__ void __launch_bounds__(TB) k_res(Mesh m, Params p, State st, int for_
   const bool active = c < m.ncv && st.case_active[m.case_of[c]];  // a frozen case keeps its arrays
   double rhs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const int k0 = active ? m.slot_i[c] : 0, k1 = active ? m.slot_i[c + 1] : 0;
+  if (k0 + lane < k1) {
+    const int nb = m.slots[k0 + lane].nb;
+    if (nb >= 0) prefetch_cell(st, m, nb, VISC);
+  }
   for (int k = k0 + lane; k < k1; k += FL) {
     const Slot s = m.slots[k];
     const int f = s.f;
+    if (k + FL < k1) {  // the next face's neighbour, a face ahead
+      const int nb = m.slots[k + FL].nb;
+      if (nb >= 0) prefetch_cell(st, m, nb, VISC);
+    }
     double nV[3], area;
     unit_normal(m, f, nV, area);
     if (s.nb >= 0) {
@@ -164,9 +172,12 @@ __global__ void __launch_bounds__(TB, jac_min_blocks<BT, KIND>()) k_jac(Mesh m, 
   for (int e = 0; e < 25; e++) sd[e * TB] = JT(0);
   BT* O = (BT*)st.O;
   const int slice = c / SLICE, lane = c % SLICE;
-  for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
+  const int k0 = m.slot_i[c], k1 = m.slot_i[c + 1];
+  if (k0 < k1 && m.slots[k0].nb >= 0) prefetch_cell_jac(st, m.slots[k0].nb, VISC);
+  for (int k = k0; k < k1; k++) {
     const Slot s = m.slots[k];
     const int f = s.f;
+    if (k + 1 < k1 && m.slots[k + 1].nb >= 0) prefetch_cell_jac(st, m.slots[k + 1].nb, VISC);  // a face ahead
     double nV[3], area;
     unit_normal(m, f, nV, area);
     const JT nVt[3] = {(JT)nV[0], (JT)nV[1], (JT)nV[2]};

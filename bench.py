@@ -282,11 +282,13 @@ def run_config3(args):
     print(json.dumps(out))
 
 
-def build_converge_cases(args, rank):
+def build_converge_cases(args, rank, world):
+    """This rank's share of one seeded case list of converge_cases cases per GPU (weak scaling in
+    cases): each case runs whole on one GPU, balanced by cells (serve.partition_cases)."""
     import multiprocessing as mp
     from myjoe_b200 import serve
     lo, hi = (int(x) for x in args.converge_cells.split(","))
-    specs = serve.case_specs(args.converge_cases, lo, hi, seed=1000 + rank)
+    specs = serve.partition_cases(serve.case_specs(args.converge_cases * world, lo, hi, seed=1000), world, rank)
     with mp.get_context("spawn").Pool(min(len(specs), os.cpu_count() or 1)) as pool:
         return pool.map(serve.build_request, specs)
 
@@ -346,7 +348,7 @@ def main():
     import multiprocessing as mp
     hpool = mp.get_context("spawn").Pool(1) if args.hbm_leg else None
     hjob = hpool.apply_async(build_hbm_case) if hpool else None
-    conv_cases = build_converge_cases(args, rank) if args.converge_cases > 0 else None
+    conv_cases = build_converge_cases(args, rank, world) if args.converge_cases > 0 else None
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
@@ -464,12 +466,10 @@ def main():
         hbm = hbm_leg(hcase)
         del hcase
     if world > 1 and conv is not None:
+        from myjoe_b200 import serve
         allc = [None] * world
         dist.all_gather_object(allc, conv)
-        conv["solves_per_hour"] = sum(c["solves_per_hour"] for c in allc)
-        conv["ratio_vs_plain_fp64"] = conv["solves_per_hour"] / max(
-            1e-300, sum(c["plain_fp64"]["solves_per_hour"] for c in allc))
-        conv["replicas"] = world
+        conv = serve.merge_rank_results(allc)
     clk = clocks.stop()
     if clk is not None:
         clk["window"] = "the timed steps, the e2e, BiCGSTAB, time-to-converge and HBM-scale legs"

@@ -69,6 +69,40 @@ def case_specs(n, lo, hi, seed):
     return out
 
 
+def spec_cells(spec):
+    return spec["nx"] * spec["ny"] * spec["nz"]
+
+
+def partition_cases(specs, world, rank):
+    """The cases one GPU of `world` runs when a case list is spread over the GPUs of a node: every
+    case runs whole on one GPU (no collective on the data path, weak scaling in cases).  Longest
+    first by cells, each to the least-loaded GPU (ties: the lower rank), so every rank derives the
+    same assignment from the same list; the rank's cases keep their list order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank %d of %d" % (rank, world))
+    order = sorted(range(len(specs)), key=lambda k: (-spec_cells(specs[k]), k))
+    load = [0] * world
+    owner = [0] * len(specs)
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[k] = r
+        load[r] += spec_cells(specs[k])
+    return [specs[k] for k in range(len(specs)) if owner[k] == rank]
+
+
+def merge_rank_results(results):
+    """One time-to-converge record from the records of the GPUs of a node (each ran its own share of
+    the case list): solves per hour, cases and cells add up, the ratio is of the sums."""
+    out = dict(results[0])
+    out["solves_per_hour"] = sum(r["solves_per_hour"] for r in results)
+    plain = sum(r["plain_fp64"]["solves_per_hour"] for r in results)
+    out["ratio_vs_plain_fp64"] = out["solves_per_hour"] / max(1e-300, plain)
+    out["cases"] = sum(r.get("cases", 0) for r in results)
+    out["cells_total"] = sum(r.get("cells_total", 0) for r in results)
+    out["gpus"] = len(results)
+    return out
+
+
 def build_request(spec):
     from myjoe_b200 import case
     _, g, prm = case.bump_case(spec["nx"], spec["ny"], spec["nz"], mach=spec["mach"], aoa_deg=spec["aoa"],

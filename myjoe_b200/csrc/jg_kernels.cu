@@ -21,7 +21,10 @@ int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double mu_law(const Params& p, double T) {
   // calcMuLam / calcMaterialProperties, src/joe/UgpWithCvCompFlow.h:1601-1621, 1701-1753
-  if (p.mu_mode == JG_MU_SUTHERLAND) return p.mu_ref * pow(T / p.SL_T, 1.5) * (p.SL_T + p.SL_S) / (T + p.SL_S);
+  if (p.mu_mode == JG_MU_SUTHERLAND) {
+    const double t = T / p.SL_T;  // pow(t, 1.5) as t sqrt(t)
+    return p.mu_ref * (t * sqrt(t)) * (p.SL_T + p.SL_S) / (T + p.SL_S);
+  }
   return p.mu_ref * pow(T / p.T_ref, p.mu_pow);
 }
 
@@ -316,10 +319,20 @@ __global__ void k_dt_min_all(Mesh m, State st) {
 // LSQ gradients + smooth Barth-Jespersen limiter, UgpWithCv.h:803-1083.
 // Fields: velocity (ref = speed of sound), density, pressure, enthalpy.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double bj_factor(double phi_c, double phifa, double pmax, double pmin, double eps2) {
+// the limiter ratio of one face as a (numerator, denominator) pair: the denominator is positive
+// (dp^2 + dm dp + 2 dm^2 >= 0 for every dm, dp), so the smallest ratio over a cell's faces is
+// tracked by cross-multiplication and divided out once per cell (bj_min)
+struct BjRatio {
+  double n = 1.0, d = 1.0;
+};
+__device__ __forceinline__ void bj_min(BjRatio& r, double phi_c, double phifa, double pmax, double pmin, double eps2) {
   double dm = phifa - phi_c;
   double dp = ((phifa - phi_c) >= 0.0) ? pmax - phi_c : pmin - phi_c;
-  return (dp * dp + 2.0 * dm * dp + eps2) / (dp * dp + 2 * dm * dm + dm * dp + eps2);
+  const double n = dp * dp + 2.0 * dm * dp + eps2, d = dp * dp + 2 * dm * dm + dm * dp + eps2;
+  if (n * r.d < r.n * d) {
+    r.n = n;
+    r.d = d;
+  }
 }
 
 // calcCvScalarGradSDWLS / calcCvVectorGradSDWLS (UgpWithCv.h:1418-1800) for one cell.  Each quantity
@@ -539,24 +552,29 @@ __global__ void k_grad(Mesh m, Params p, State st, int do_euler, int do_visc, in
   // limiter factors over the internal faces of the cell
   double au[3] = {1.0, 1.0, 1.0}, ar = 1.0, ap = 1.0, ah = 1.0;
   const double eps = p.eps;
-  double e2u = pow(eps * pc[6], 2.0);
-  double e2r = pow(fmax(eps * fabs(rc), 1.0e-8), 2.0);
-  double e2p = pow(fmax(eps * fabs(pc[3]), 1.0e-8), 2.0);
-  double e2h = pow(fmax(eps * fabs(pc[5]), 1.0e-8), 2.0);
+  // pow(x, 2.0) of the reference, as x * x
+  const double vu = eps * pc[6], vr = fmax(eps * fabs(rc), 1.0e-8), vp = fmax(eps * fabs(pc[3]), 1.0e-8),
+               vh = fmax(eps * fabs(pc[5]), 1.0e-8);
+  const double e2u = vu * vu, e2r = vr * vr, e2p = vp * vp, e2h = vh * vh;
   bool lu[3], lr = (rmax - rmin) > 1.0e-12, lp = (pmax - pmin) > 1.0e-12, lh = (hmax - hmin) > 1.0e-12;
   for (int i = 0; i < 3; i++) lu[i] = (umax[i] - umin[i]) > 1.0e-8;
   if (p.limiter) {
+    BjRatio bu[3], br, bp, bh;
     for (int k = m.slot_i[c]; k < m.slot_i[c + 1]; k++) {
       Slot s = m.slots[k];
       if (s.nb < 0) continue;
       double r0[3];
       for (int j = 0; j < 3; j++) r0[j] = m.x_fa[3 * s.f + j] - m.x_cv[3 * c + j];
       for (int i = 0; i < 3; i++)
-        if (lu[i]) au[i] = fmin(au[i], bj_factor(pc[i], pc[i] + dot3(r0, &gu[3 * i]), umax[i], umin[i], e2u));
-      if (lr) ar = fmin(ar, bj_factor(rc, rc + dot3(r0, gr), rmax, rmin, e2r));
-      if (lp) ap = fmin(ap, bj_factor(pc[3], pc[3] + dot3(r0, gpr), pmax, pmin, e2p));
-      if (lh && do_visc) ah = fmin(ah, bj_factor(pc[5], pc[5] + dot3(r0, gh), hmax, hmin, e2h));
+        if (lu[i]) bj_min(bu[i], pc[i], pc[i] + dot3(r0, &gu[3 * i]), umax[i], umin[i], e2u);
+      if (lr) bj_min(br, rc, rc + dot3(r0, gr), rmax, rmin, e2r);
+      if (lp) bj_min(bp, pc[3], pc[3] + dot3(r0, gpr), pmax, pmin, e2p);
+      if (lh && do_visc) bj_min(bh, pc[5], pc[5] + dot3(r0, gh), hmax, hmin, e2h);
     }
+    for (int i = 0; i < 3; i++) au[i] = bu[i].n / bu[i].d;
+    ar = br.n / br.d;
+    ap = bp.n / bp.d;
+    ah = bh.n / bh.d;
     for (int i = 0; i < 3; i++)
       if (!lu[i]) au[i] = 0.0;
     if (!lr) ar = 0.0;

@@ -133,6 +133,10 @@ typedef struct jg_params {
    * every step, so the converged field does not depend on it.  Cases without a
    * turbulence model, captured linear solvers (JACOBI, SGS, LINE, LUSGS). */
   int jac_lag;
+  /* GX, GY, GZ: the gravity of JoeWithModels::sourceHook / sourceHookCoupled
+   * (src/joe/JoeWithModels.h:111-152), added to the momentum and energy rows of the
+   * residual and to the diagonal blocks (zero: none) */
+  double gravity[3];
 } jg_params;
 /* AUSMDV (Wada & Liou, calcEulerFlux_AUSMDV / calcEulerFluxMatrices_AUSMDV,
  * UgpWithCvCompFlow.cpp:879-1322): the AUSMD / AUSMV blend, the entropy fix for

@@ -142,6 +142,7 @@ class JoeGpuCase : public Base {
     q.ls_max_iter = t->getInt("MAX_ITER");
     q.ls_abs = t->getDouble("ABS_RESID");
     q.ls_rel = t->getDouble("REL_RESID");
+    for (int i = 0; i < 3; i++) q.gravity[i] = this->gravity[i];  /* GX, GY, GZ of sourceHook */
     q.precision = gpu_precision;
     q.renumber = gpu_renumber;
     q.jac_lag = 1;

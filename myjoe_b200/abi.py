@@ -46,7 +46,7 @@ class jg_params(C.Structure):
                 ("precision", C.c_int), ("nscal", C.c_int), ("turb_model", C.c_int), ("renumber", C.c_int),
                 ("grad_scheme", C.c_int),
                 ("ausm_type", C.c_int), ("shock_fix", C.c_int), ("shock_flag", C.c_int), ("entropy_fix", C.c_int),
-                ("jac_lag", C.c_int)]
+                ("jac_lag", C.c_int), ("gravity", C.c_double * 3)]
 
 
 class jg_serve_config(C.Structure):
@@ -77,6 +77,8 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False, jac_la
     """jac_lag: form the flux Jacobian blocks every jac_lag-th step (1: every step, as the reference)"""
     q = jg_params()
     q.jac_lag = int(jac_lag)
+    for i, g in enumerate((p.GX, p.GY, p.GZ)):
+        q.gravity[i] = g
     q.gamma = p.GAMMA
     q.R_gas = p.R_gas
     q.Pr = p.PR

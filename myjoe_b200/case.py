@@ -66,6 +66,9 @@ class JoeParams:
     ENTROPY_FIX: str = "EXPANSION_FAN"  # or NONE
     VISC_LIMITER: bool = True
     SYMM_BC: str = "ORIGINAL_NUMERIC"
+    GX: float = 0.0                     # gravity of sourceHook (GX, GY, GZ)
+    GY: float = 0.0
+    GZ: float = 0.0
     TIME_STEP: str = "MAX_BASED"
     CFL: float = 1.0
     CFL_RAMP: Tuple[int, int, float, float] = (100, 10, 1.0, 100.0)
@@ -130,6 +133,7 @@ class JoeParams:
                 "YES" if self.LIMITER else "NO", self.EPS),
             "VISC_LIMITER = %s" % ("YES" if self.VISC_LIMITER else "NO"),
             "SYMM_BC = %s" % self.SYMM_BC,
+            "GX = %.17g" % self.GX, "GY = %.17g" % self.GY, "GZ = %.17g" % self.GZ,
             "TIME_STEP = %s" % self.TIME_STEP,
             "TIME_INTEGRATION = BACKWARD_EULER",
             "CFL = %.17g" % self.CFL,

@@ -234,6 +234,8 @@ static Params make_params(const jg_params& q) {
   p.gamma = q.gamma;
   p.R = q.R_gas;
   p.cp = p.gamma * p.R / (p.gamma - 1.0);
+  for (int i = 0; i < 3; i++) p.gravity[i] = q.gravity[i];
+  p.has_gravity = q.gravity[0] != 0.0 || q.gravity[1] != 0.0 || q.gravity[2] != 0.0;
   p.Pr = q.Pr;
   p.PrTurb = q.PrTurb;
   p.mu_mode = q.mu_mode;

@@ -37,6 +37,26 @@ __device__ __forceinline__ void prefetch_cell_jac(const State& st, int c, bool v
   if (visc) prefetch_l1(&st.guv[9 * c]);
 }
 
+// sourceHook / sourceHookCoupled (JoeWithModels.h:111-152): gravity in cell c's momentum and
+// energy rows of the residual (after the fluxes) ...
+__device__ __forceinline__ void gravity_rhs(const Params& p, const Mesh& m, const State& st, int c, double* rhs) {
+  if (!p.has_gravity) return;
+  const double vol = m.vol[c], rho = st.q[5 * c];
+  const double* ru = &st.q[5 * c + 1];
+  for (int i = 0; i < 3; i++) rhs[1 + i] += vol * rho * p.gravity[i];
+  rhs[4] += vol * (p.gravity[0] * ru[0] + p.gravity[1] * ru[1] + p.gravity[2] * ru[2]);
+}
+// ... and in its diagonal block (B x B row-major, after the flux matrices)
+template <int B>
+__device__ __forceinline__ void gravity_diag(const Params& p, const Mesh& m, int c, double* Dm) {
+  if (!p.has_gravity) return;
+  const double vol = m.vol[c];
+  for (int i = 0; i < 3; i++) {
+    Dm[B * (1 + i)] -= vol * p.gravity[i];
+    Dm[B * 4 + 1 + i] -= vol * p.gravity[i];
+  }
+}
+
 // the unit normal and area of face f (normVec3d of fa_normal, formed once per mesh by k_face_geo)
 __device__ __forceinline__ void unit_normal(const Mesh& m, int f, double nV[3], double& area) {
   const double* u = &m.fa_u[4 * f];

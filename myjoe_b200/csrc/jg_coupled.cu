@@ -1090,6 +1090,7 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
       }
     }
   }
+  gravity_rhs(p, m, st, c, rhs);  // sourceHookCoupled
   // model sources: sourceHookRansTurbCoupled (TurbModel_SA.h:359-434; TurbModel_KOMSST.h:306-340)
   double dsrc[NS];
   {
@@ -1142,6 +1143,7 @@ __global__ void __launch_bounds__(128) k_flux_c(Mesh m, Params p, State st, Turb
   if (implicit) {
     double Dm[BB];
     for (int e = 0; e < BB; e++) Dm[e] = sD[e * bd + tid];
+    gravity_diag<B>(p, m, c, Dm);
     for (int q = 0; q < NS; q++) Dm[(B + 1) * (5 + q)] -= dsrc[q];
     if (for_step) {
       double tmp = m.vol[c] / st.local_dt[c];

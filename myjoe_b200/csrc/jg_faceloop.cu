@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(TB) k_res(Mesh m, Params p, State st, int for_
   if (FL > 1)
     for (int i = 0; i < 5; i++) rhs[i] = lanes_sum<FL>(rhs[i]);
   if (active && lane == 0) {
+    gravity_rhs(p, m, st, c, rhs);
     for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
     if (for_step)
       for (int i = 0; i < 5; i++) st.b[5 * c + i] = p.under_relax * rhs[i];
@@ -280,6 +281,7 @@ __global__ void __launch_bounds__(TB, jac_min_blocks<BT, KIND>()) k_jac(Mesh m, 
   const int N = m.ncv;
   double Dm[25];
   for (int e = 0; e < 25; e++) Dm[e] = (double)sd[e * TB];
+  gravity_diag<5>(p, m, c, Dm);
   if (sched && st.D0) {
     BT* D0 = (BT*)st.D0;
     for (int e = 0; e < 25; e++) D0[(size_t)e * N + c] = (BT)Dm[e];

@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, 
     __syncwarp();
   }
   if (active && lane == 0) {
+    gravity_rhs(p, m, st, c, rhs);
     for (int i = 0; i < 5; i++) st.rhs[5 * c + i] = rhs[i];
     if (implicit) {
       double Dm[25];
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux(Mesh m, Params p, State st, 
         for (int l = 1; l < CL; l++) d += sD[e * bd + t + l];
         Dm[e] = (double)d;
       }
+      gravity_diag<5>(p, m, c, Dm);
       if (for_step) {
         double tmp = m.vol[c] / st.local_dt[c];
         for (int i = 0; i < 5; i++) Dm[6 * i] += tmp;

@@ -142,6 +142,8 @@ struct Turb {
 struct Params {
   double gamma, R, Pr, PrTurb;
   double cp;        // gamma R / (gamma - 1), the enthalpy per kelvin (set with gamma and R)
+  double gravity[3];  // GX, GY, GZ of sourceHook; has_gravity: any of them non-zero
+  int has_gravity;
   int mu_mode, flux;
   double mu_ref, mu_pow, SL_T, SL_S, T_ref;
   int second_order, limiter;

@@ -375,7 +375,8 @@ class JoeGpuBatch(JoeGpu):
         self.jp = make_params(self.params, precision, renumber, jac_lag)
         for k, (_, prm) in enumerate(cases[1:], 1):
             q = make_params(prm, precision, renumber, jac_lag)
-            diff = [f for f, _ in jg_params._fields_ if getattr(q, f) != getattr(self.jp, f)]
+            val = lambda x: list(x) if isinstance(x, C.Array) else x  # noqa: E731 (array fields by value)
+            diff = [f for f, _ in jg_params._fields_ if val(getattr(q, f)) != val(getattr(self.jp, f))]
             if diff:
                 raise ValueError("case %d differs from case 0 in the batch-wide settings %s" % (k, diff))
         arr = (jg_mesh * len(cases))(*[ma.mesh for ma in self.mas])

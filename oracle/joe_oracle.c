@@ -1942,6 +1942,24 @@ void jo_calc_rhs(jo_case *h, double *rr, double *ru, double *rE, double *A, int 
   memset(h->fscale, 0, sizeof(double) * 5 * h->ncv);
   calc_euler_flux(h, rr, ru, rE, A, implicit);
   if (h->p.mu_ref > 0.0) calc_viscous_flux(h, ru, rE, A, implicit);
+  /* sourceHook: gravity (JoeWithModels.h:111-129) */
+  const double *g = h->p.gravity;
+  for (int c = 0; c < h->ncv; c++) {
+    double vol = h->m.cv_volume[c];
+    ru[3 * c + 0] += vol * h->rho[c] * g[0];
+    ru[3 * c + 1] += vol * h->rho[c] * g[1];
+    ru[3 * c + 2] += vol * h->rho[c] * g[2];
+    rE[c] += vol * (g[0] * h->rhou[3 * c + 0] + g[1] * h->rhou[3 * c + 1] + g[2] * h->rhou[3 * c + 2]);
+    if (A && implicit) {
+      double *a = &A[25 * (size_t)h->m.nbocv_i[c]];
+      a[5 * 1 + 0] -= vol * g[0];
+      a[5 * 2 + 0] -= vol * g[1];
+      a[5 * 3 + 0] -= vol * g[2];
+      a[5 * 4 + 1] -= vol * g[0];
+      a[5 * 4 + 2] -= vol * g[1];
+      a[5 * 4 + 3] -= vol * g[2];
+    }
+  }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -3522,6 +3540,26 @@ void jo_calc_rhs_coupled(jo_case *h, double *rhs, double *A, int implicit) {
     }
   }
   free(flag);
+  /* sourceHookCoupled: gravity (JoeWithModels.h:134-152) */
+  {
+    const double *g = p->gravity;
+    for (int c = 0; c < h->ncv; c++) {
+      double vol = m->cv_volume[c];
+      rhs[B * c + 1] += vol * h->rho[c] * g[0];
+      rhs[B * c + 2] += vol * h->rho[c] * g[1];
+      rhs[B * c + 3] += vol * h->rho[c] * g[2];
+      rhs[B * c + 4] += vol * (g[0] * h->rhou[3 * c + 0] + g[1] * h->rhou[3 * c + 1] + g[2] * h->rhou[3 * c + 2]);
+      if (implicit) {
+        double *a = &A[(size_t)BB * m->nbocv_i[c]];
+        a[B * 1 + 0] -= vol * g[0];
+        a[B * 2 + 0] -= vol * g[1];
+        a[B * 3 + 0] -= vol * g[2];
+        a[B * 4 + 1] -= vol * g[0];
+        a[B * 4 + 2] -= vol * g[1];
+        a[B * 4 + 3] -= vol * g[2];
+      }
+    }
+  }
   /* source terms: sourceHookRansTurbCoupled (TurbModel_SA.h:359-434; TurbModel_KOMSST.h:306-340) */
   for (int c = 0; c < h->ncv; c++) {
     size_t d0 = (size_t)BB * m->nbocv_i[c];

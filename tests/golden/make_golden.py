@@ -57,6 +57,9 @@ def cases():
                                                                           SPACE_INTEGRATION="HLLC",
                                                                           VISC_LIMITER=False)
     yield "plate_roe", rawp, prmp
+    # gravity (sourceHook, GX/GY/GZ), large enough to stand out of the face fluxes
+    yield "bump_hllc_gravity", raw, dataclasses.replace(prm, GX=300.0, GY=-5000.0, GZ=40.0)
+    yield "plate_roe_gravity", rawp, dataclasses.replace(prmp, GX=0.0, GY=-5000.0, GZ=0.0)
     # Haenel & Schwane (SPACE_INTEGRATION = HAENEL): second order, laminar, first order with NEW_NUMERIC symmetry
     # Green-Gauss gradients (GRAD_RECONSTRUCTION SCHEME=GREENGAUSS, the reference's default scheme)
     yield "bump_hllc_greengauss", raw, dataclasses.replace(prm, GRAD_SCHEME="GREENGAUSS")
@@ -121,6 +124,8 @@ def sa_cases():
         prmc, bcs=bc_n, SECOND_ORDER=False, SYMM_BC="NEW_NUMERIC", SPACE_INTEGRATION="AUSMD",
         SHOCK_FIX_TYPE="NONE", ENTROPY_FIX="NONE")
     yield "sa_bump_haenel_farfield", raw, dataclasses.replace(prm, SPACE_INTEGRATION="HAENEL")
+    # gravity (sourceHookCoupled, GX/GY/GZ)
+    yield "sa_bump_gravity", raw, dataclasses.replace(prm, GX=300.0, GY=-5000.0, GZ=40.0)
     yield "sa_mixed_bump_haenel_symm_original", rawm, dataclasses.replace(prmm, SPACE_INTEGRATION="HAENEL",
                                                                           SYMM_BC="ORIGINAL_NUMERIC")
 

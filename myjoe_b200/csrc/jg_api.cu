@@ -692,6 +692,27 @@ static int build(jg_case* h, const jg_mesh* mesh, const jg_params* q) {
     const size_t nc = std::max<size_t>(cv.size(), 1);
     RC(upload(h, &L.off, off.data(), off.size()));
     RC(upload(h, &L.cv, cv.data(), nc));
+    {
+      // the ELL row of each coupling along the lines, so that the factorisations read the blocks
+      // directly instead of searching the rows
+      std::vector<int> jlo(nc, -1), jup(nc, -1);
+      auto ell_row = [&](int row, int nbc) {
+        int found = -1, cnt = 0;
+        for (int j = 0; j < ncols[row]; j++)
+          if (h->col_nb[h->cell_cols[row] + j] == nbc) {
+            if (!cnt) found = j;
+            cnt++;
+          }
+        return cnt == 0 ? -1 : cnt > 1 ? -2 : h->ell_off[row / SLICE] + found;
+      };
+      for (int l = 0; l < L.nlines; l++)
+        for (int k = off[l] + 1; k < off[l + 1]; k++) {
+          jlo[k] = ell_row(cv[k], cv[k - 1]);
+          jup[k] = ell_row(cv[k - 1], cv[k]);
+        }
+      RC(upload(h, &L.jlo, jlo.data(), nc));
+      RC(upload(h, &L.jup, jup.data(), nc));
+    }
     if (q->lin_solver == JG_LS_BCGSTAB_LINELET) {
       RC(dmalloc(h, &L.inv, 25 * nc));
       RC(dmalloc(h, &L.low, 25 * nc));
@@ -832,7 +853,7 @@ static size_t footprint(const jg_mesh* mesh, const jg_params* q, const std::vect
     std::vector<int> off, cv;
     multi_cell_lines(mesh, face_old, off, cv, q->lin_solver == JG_LS_LINE);
     const size_t nc = std::max<size_t>(cv.size(), 1);
-    b += alloc_round(off.size() * i) + alloc_round(nc * i);
+    b += alloc_round(off.size() * i) + 3 * alloc_round(nc * i);
     if (q->lin_solver == JG_LS_BCGSTAB_LINELET)
       b += 3 * alloc_round(25 * nc * d) + alloc_round(5 * nc * d);
     else

@@ -690,20 +690,21 @@ __device__ void visc_flux_c(double* Fv, VFC<NS>& vf, const VSideC<NS>& a, const 
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) g[i][j] = 0.5 * (a.gu[3 * i + j] + b.gu[3 * i + j]);
   double fC[3] = {nV[0] - alpha * sV[0], nV[1] - alpha * sV[1], nV[2] - alpha * sV[2]};
+  const double aos = alpha / smag;  // the normal-derivative weight, one division for all terms
   double muT = mul + mut;
   Fv[0] = 0.0;
   for (int i = 0; i < 3; i++)
-    vf.tn[i] = muT * (alpha * (b.u[i] - a.u[i]) / smag + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
+    vf.tn[i] = muT * ((b.u[i] - a.u[i]) * aos + g[i][0] * fC[0] + g[0][i] * nV[0] + g[i][1] * fC[1] +
                       g[1][i] * nV[1] + g[i][2] * fC[2] + g[2][i] * nV[2]);
   double tmp = 2.0 / 3.0 * muT * (g[0][0] + g[1][1] + g[2][2]);
   tmp += 1.0 / 3.0 * (a.rho + b.rho) * kine_fa;
   for (int i = 0; i < 3; i++) vf.tn[i] -= tmp * nV[i];
   for (int i = 0; i < 3; i++) Fv[1 + i] = -area * vf.tn[i];
   vf.keff = lamOcp + mut / PrTurb;
-  double enth = vf.keff * (alpha * (b.h - a.h) / smag + 0.5 * ((a.gh[0] + b.gh[0]) * fC[0] +
+  double enth = vf.keff * ((b.h - a.h) * aos + 0.5 * ((a.gh[0] + b.gh[0]) * fC[0] +
                                                              (a.gh[1] + b.gh[1]) * fC[1] +
                                                              (a.gh[2] + b.gh[2]) * fC[2]));
-  double psi = muT * (alpha * (b.k - a.k) / smag);
+  double psi = muT * ((b.k - a.k) * aos);
   Fv[4] = -area * (enth + vf.tn[0] * u_fa[0] + vf.tn[1] * u_fa[1] + vf.tn[2] * u_fa[2] + psi);
   for (int s = 0; s < NS; s++) {
     double g0[3] = {0.0, 0.0, 0.0}, g1[3] = {0.0, 0.0, 0.0};
@@ -711,13 +712,13 @@ __device__ void visc_flux_c(double* Fv, VFC<NS>& vf, const VSideC<NS>& a, const 
       for (int i = 0; i < 3; i++) g0[i] = a.gs[s][i];
     if (b.gs[s])
       for (int i = 0; i < 3; i++) g1[i] = b.gs[s][i];
-    Fv[5 + s] = -area * diffTerm[s] * diff[s] * (alpha * (b.sc[s] - a.sc[s]) / smag +
+    Fv[5 + s] = -area * diffTerm[s] * diff[s] * ((b.sc[s] - a.sc[s]) * aos +
                                                  0.5 * ((g0[0] + g1[0]) * fC[0] + (g0[1] + g1[1]) * fC[1] +
                                                         (g0[2] + g1[2]) * fC[2]));
     vf.dd[s] = diffTerm[s] * diff[s];
   }
   vf.muT = muT;
-  vf.aas = area * alpha / smag;
+  vf.aas = area * aos;
 }
 
 // acc += sgn * (A0 (side 0) or A1 (side 1)) of calcViscousFluxCoupled, from the state of that side

@@ -261,6 +261,11 @@ struct Lines {
   int nlines;
   const int* off;  // [nlines+1]
   const int* cv;   // [off[nlines]]
+  // per line position k > off[l]: the ELL row index of the block coupling cv[k] to cv[k-1] in
+  // cv[k]'s row (jlo) and of the block coupling cv[k-1] to cv[k] in cv[k-1]'s row (jup); -1: no
+  // coupling, -2: several faces between the two cells (their blocks are summed by a search)
+  const int* jlo;
+  const int* jup;
   // BCGSTAB_LINELET (5x5, FP64)
   double* inv;     // [off[nlines]][25]
   double* low;     // [off[nlines]][25] (position 0 of a line unused)

@@ -158,6 +158,11 @@ __device__ double ell_block(const Mesh& m, const double* O, int row, int col, in
     if (m.ell_nb[(size_t)j * SLICE + lane] == col) v += O[((size_t)j * 25 + e) * SLICE + lane];
   return v;
 }
+// the block at ELL row j (Lines::jlo / jup), or the search where the two cells share several faces
+__device__ __forceinline__ double ell_block_j(const Mesh& m, const double* O, int row, int col, int j, int e) {
+  if (j >= 0) return O[((size_t)j * 25 + e) * SLICE + row % SLICE];
+  return j == -1 ? 0.0 : ell_block(m, O, row, col, e);
+}
 
 __global__ void __launch_bounds__(32 * LW) k_line_factor(Mesh m, State st, Lines L) {
   __shared__ double sh[LW][5][25];
@@ -188,8 +193,8 @@ __global__ void __launch_bounds__(32 * LW) k_line_factor(Mesh m, State st, Lines
     if (i == n) break;
     const int cp = L.cv[p0 + i - 1], c = L.cv[p0 + i];
     if (lane < 25) {
-      lo[e] = ell_block(m, O, c, cp, e);
-      up[e] = ell_block(m, O, cp, c, e);
+      lo[e] = ell_block_j(m, O, c, cp, L.jlo[p0 + i], e);
+      up[e] = ell_block_j(m, O, cp, c, L.jup[p0 + i], e);
       L.up[(size_t)(p0 + i) * 25 + e] = up[e];
     }
     __syncwarp();
@@ -277,57 +282,12 @@ void launch_line_precond(const Mesh& m, const State& st, const Lines& L, const d
 //                 lines r is left in x' for
 //   k_lsolve:     the block Thomas substitutions of each line, in place.
 // k_lfactor computes the line factors once per step from D and the ELL
-// blocks, in FP64 arithmetic, and stores them in BT.
+// blocks, in FP64 arithmetic, and stores them in BT.  (The LINE relaxation has
+// no reference counterpart; the reference's own line solver, BCGSTAB_LINELET,
+// keeps the reference's ludeco/luinv arithmetic in k_line_factor above.)
 // ---------------------------------------------------------------------------
 namespace jg {
 namespace {
-
-// inverse of a B x B block by the reference's LU (ludeco / luinv pattern), column `col`
-template <int B>
-__device__ void lu_inverse_col(const double* M, int col, double* out) {
-  double A[B * B];
-#pragma unroll
-  for (int q = 0; q < B * B; q++) A[q] = M[q];
-#pragma unroll
-  for (int jc = 1; jc < B; jc++) A[jc] /= A[0];
-#pragma unroll
-  for (int jrjc = 1; jrjc < B; jrjc++) {
-#pragma unroll
-    for (int jr = jrjc; jr < B; jr++) {
-      double sum = A[B * jr + jrjc];
-#pragma unroll
-      for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jr + jm] * A[B * jm + jrjc];
-      A[B * jr + jrjc] = sum;
-    }
-#pragma unroll
-    for (int jc = jrjc + 1; jc < B; jc++) {  // empty on the last row
-      double sum = A[B * jrjc + jc];
-#pragma unroll
-      for (int jm = 0; jm < jrjc; jm++) sum -= A[B * jrjc + jm] * A[B * jm + jc];
-      A[B * jrjc + jc] = sum / A[B * jrjc + jrjc];
-    }
-  }
-  double c[B];
-#pragma unroll
-  for (int i = 0; i < B; i++) c[i] = (i == col) ? 1.0 : 0.0;
-  c[0] = c[0] / A[0];
-#pragma unroll
-  for (int jr = 1; jr < B; jr++) {
-    double sum = c[jr];
-#pragma unroll
-    for (int jm = 0; jm < jr; jm++) sum -= A[B * jr + jm] * c[jm];
-    c[jr] = sum / A[B * jr + jr];
-  }
-#pragma unroll
-  for (int jr = B - 2; jr >= 0; jr--) {
-    double sum = c[jr];
-#pragma unroll
-    for (int jm = B - 1; jm > jr; jm--) sum -= A[B * jr + jm] * c[jm];
-    c[jr] = sum;
-  }
-#pragma unroll
-  for (int i = 0; i < B; i++) out[i] = c[i];
-}
 
 template <typename BT, int B>
 __device__ double ell_block_b(const Mesh& m, const BT* O, int row, int col, int e) {
@@ -337,15 +297,26 @@ __device__ double ell_block_b(const Mesh& m, const BT* O, int row, int col, int 
     if (m.ell_nb[(size_t)j * SLICE + lane] == col) v += (double)O[((size_t)j * B * B + e) * SLICE + lane];
   return v;
 }
+template <typename BT, int B>
+__device__ __forceinline__ double ell_block_bj(const Mesh& m, const BT* O, int row, int col, int j, int e) {
+  if (j >= 0) return (double)O[((size_t)j * B * B + e) * SLICE + row % SLICE];
+  return j == -1 ? 0.0 : ell_block_b<BT, B>(m, O, row, col, e);
+}
 
+// The block Thomas factors along one line per warp: inv_i = (the eliminated diagonal block)^-1,
+// low_i = A(c_i, c_i-1) inv_i-1, up_i = A(c_i-1, c_i).  The elimination is serial along the line,
+// so each step is kept short: the eliminated block is inverted in place by all lanes together
+// (Gauss-Jordan without pivoting, the reference's ludeco/luinv having none either: B pivot
+// steps, each one shared-memory read per entry), and the next step's blocks (its coupling
+// blocks and diagonal block) are loaded while the current step computes.
 template <typename BT, int B>
 __global__ void __launch_bounds__(32 * LW) k_lfactor(Mesh m, State st, Lines L) {
-  constexpr int BB = B * B;
-  __shared__ double sh[LW][5][BB];
+  constexpr int BB = B * B, EP = (BB + 31) / 32;  // entries per lane
+  __shared__ double sh[LW][4][BB];
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int line = blockIdx.x * LW + w;
   if (line >= L.nlines) return;
-  double *b = sh[w][0], *inv = sh[w][1], *lo = sh[w][2], *up = sh[w][3], *mh = sh[w][4];
+  double *b = sh[w][0], *lo = sh[w][1], *up = sh[w][2], *mh = sh[w][3];
   const int p0 = L.off[line], n = L.off[line + 1] - p0;
   const int N = m.ncv;
   const BT* D = (const BT*)st.D;
@@ -354,36 +325,72 @@ __global__ void __launch_bounds__(32 * LW) k_lfactor(Mesh m, State st, Lines L) 
   BT* Llow = (BT*)L.blow;
   BT* Lup = (BT*)L.bup;
   for (int e = lane; e < BB; e += 32) b[e] = (double)D[(size_t)e * N + L.cv[p0]];
+  // the next step's operands, a step ahead: coupling blocks and diagonal block of position 1
+  double nlo[EP], nup[EP], nd[EP];
+  auto load_step = [&](int i) {
+    const int cp = L.cv[p0 + i - 1], c = L.cv[p0 + i];
+    const int jl = L.jlo[p0 + i], ju = L.jup[p0 + i];
+#pragma unroll
+    for (int t = 0; t < EP; t++) {
+      const int e = lane + 32 * t;
+      if (e < BB) {
+        nlo[t] = ell_block_bj<BT, B>(m, O, c, cp, jl, e);
+        nup[t] = ell_block_bj<BT, B>(m, O, cp, c, ju, e);
+        nd[t] = (double)D[(size_t)e * N + c];
+      }
+    }
+  };
+  if (n > 1) load_step(1);
   __syncwarp();
   for (int i = 1;; i++) {
-    if (lane < B) {
-      double col[B];
-      lu_inverse_col<B>(b, lane, col);
+    // b <- b^-1 in place
 #pragma unroll
-      for (int q = 0; q < B; q++) inv[B * q + lane] = col[q];
+    for (int k = 0; k < B; k++) {
+      const double rp = 1.0 / b[B * k + k];
+      double nv[EP];
+#pragma unroll
+      for (int t = 0; t < EP; t++) {
+        const int e = lane + 32 * t, ri = e / B, cj = e % B;
+        if (e < BB) {
+          if (ri == k) nv[t] = (cj == k) ? rp : b[e] * rp;
+          else nv[t] = (cj == k) ? -b[B * ri + k] * rp : b[e] - b[B * ri + k] * (b[B * k + cj] * rp);
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < EP; t++)
+        if (lane + 32 * t < BB) b[lane + 32 * t] = nv[t];
+      __syncwarp();
     }
-    __syncwarp();
-    for (int e = lane; e < BB; e += 32) Linv[(size_t)(p0 + i - 1) * BB + e] = (BT)inv[e];
+    for (int e = lane; e < BB; e += 32) Linv[(size_t)(p0 + i - 1) * BB + e] = (BT)b[e];
     if (i == n) break;
-    const int cp = L.cv[p0 + i - 1], c = L.cv[p0 + i];
-    for (int e = lane; e < BB; e += 32) {
-      lo[e] = ell_block_b<BT, B>(m, O, c, cp, e);
-      up[e] = ell_block_b<BT, B>(m, O, cp, c, e);
-      Lup[(size_t)(p0 + i) * BB + e] = (BT)up[e];
+    // this step's coupling blocks (loaded a step ahead), the next step's requested now
+#pragma unroll
+    for (int t = 0; t < EP; t++) {
+      const int e = lane + 32 * t;
+      if (e < BB) {
+        lo[e] = nlo[t];
+        up[e] = nup[t];
+        Lup[(size_t)(p0 + i) * BB + e] = (BT)nup[t];
+      }
     }
+    double dc[EP];
+#pragma unroll
+    for (int t = 0; t < EP; t++) dc[t] = nd[t];
+    if (i + 1 < n) load_step(i + 1);
     __syncwarp();
     for (int e = lane; e < BB; e += 32) {
       const int r = e / B, k = e % B;
       double s = 0.0;
 #pragma unroll
-      for (int q = 0; q < B; q++) s += lo[B * r + q] * inv[B * q + k];
+      for (int q = 0; q < B; q++) s += lo[B * r + q] * b[B * q + k];
       mh[e] = s;
       Llow[(size_t)(p0 + i) * BB + e] = (BT)s;
     }
     __syncwarp();
-    double bn[2];
+    double bn[EP];
 #pragma unroll
-    for (int t = 0; t < 2; t++) {
+    for (int t = 0; t < EP; t++) {
       const int e = lane + 32 * t;
       bn[t] = 0.0;
       if (e < BB) {
@@ -391,12 +398,12 @@ __global__ void __launch_bounds__(32 * LW) k_lfactor(Mesh m, State st, Lines L) 
         double s = 0.0;
 #pragma unroll
         for (int q = 0; q < B; q++) s += mh[B * r + q] * up[B * q + k];
-        bn[t] = (double)D[(size_t)e * N + c] - s;
+        bn[t] = dc[t] - s;
       }
     }
     __syncwarp();
 #pragma unroll
-    for (int t = 0; t < 2; t++)
+    for (int t = 0; t < EP; t++)
       if (lane + 32 * t < BB) b[lane + 32 * t] = bn[t];
     __syncwarp();
   }
@@ -440,12 +447,15 @@ __global__ void __launch_bounds__(B * 32) k_lrelax_rhs(Mesh m, State st, Lines L
   }
 }
 
-// x (cells of a line) = T_line^-1 r, r read from x; one warp per line, lanes < B hold the rows
+// x (cells of a line) = T_line^-1 r, r read from x; one warp per line, lanes < B hold the rows.
+// The chain along a line is serial, but the operands of its steps (a matrix row, the cell id, the
+// right-hand side) do not depend on it: they are loaded LK steps at a time, all loads of a chunk
+// issued together, the next chunk's cell ids a chunk ahead, so one memory latency is spent per LK
+// steps instead of per step.
+constexpr int LK = 4;
+
 template <typename BT, int B>
 __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restrict__ x) {
-  // The chain along a line is serial; the operands of step i+1 (a matrix row,
-  // the cell id, the right-hand side) do not depend on it, so each is loaded
-  // one step ahead to overlap its latency with the current step.
   constexpr int BB = B * B;
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int line = blockIdx.x * LW + w;
@@ -461,27 +471,33 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
   // forward: v_0 = r_0, v_i = r_i - low_i v_{i-1}
   BT v = x[r * N + L.cv[p0]];
   if (row) Lv[(size_t)p0 * B + r] = v;
-  BT mn[B], xn = 0;
-  if (n > 1) {
+  int cn[LK];  // the cell ids of the next chunk
 #pragma unroll
-    for (int q = 0; q < B; q++) mn[q] = Llow[(size_t)(p0 + 1) * BB + B * r + q];
-    xn = x[r * N + L.cv[p0 + 1]];
-  }
-  for (int i = 1; i < n; i++) {
-    BT mi[B];
+  for (int t = 0; t < LK; t++) cn[t] = (1 + t < n) ? L.cv[p0 + 1 + t] : 0;
+  for (int i0 = 1; i0 < n; i0 += LK) {
+    BT mi[LK][B], xi[LK];
 #pragma unroll
-    for (int q = 0; q < B; q++) mi[q] = mn[q];
-    const BT xi = xn;
-    if (i + 1 < n) {
+    for (int t = 0; t < LK; t++) {
+      const int i = i0 + t;
+      if (i < n) {
 #pragma unroll
-      for (int q = 0; q < B; q++) mn[q] = Llow[(size_t)(p0 + i + 1) * BB + B * r + q];
-      xn = x[r * N + L.cv[p0 + i + 1]];
+        for (int q = 0; q < B; q++) mi[t][q] = Llow[(size_t)(p0 + i) * BB + B * r + q];
+        xi[t] = x[r * N + cn[t]];
+      }
     }
-    BT s = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s += mi[q] * __shfl_sync(0xffffffffu, v, q);
-    v = xi - s;
-    if (row) Lv[(size_t)(p0 + i) * B + r] = v;
+    for (int t = 0; t < LK; t++) cn[t] = (i0 + LK + t < n) ? L.cv[p0 + i0 + LK + t] : 0;
+#pragma unroll
+    for (int t = 0; t < LK; t++) {
+      const int i = i0 + t;
+      if (i < n) {
+        BT s = 0;
+#pragma unroll
+        for (int q = 0; q < B; q++) s += mi[t][q] * __shfl_sync(0xffffffffu, v, q);
+        v = xi[t] - s;
+        if (row) Lv[(size_t)(p0 + i) * B + r] = v;
+      }
+    }
   }
   // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - up_{i+1} y_{i+1})
   BT yv = 0;
@@ -491,44 +507,38 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
     for (int q = 0; q < B; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
   }
   if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
-  BT un[B], in[B], vn = 0;
-  int cn = 0;
-  if (n > 1) {
+  __syncwarp();  // the forward pass's Lv stores are read back below
+  for (int i0 = n - 2; i0 >= 0; i0 -= LK) {
+    BT ui[LK][B], ii[LK][B], vi[LK];
+    int ci[LK];
 #pragma unroll
-    for (int q = 0; q < B; q++) {
-      un[q] = Lup[(size_t)(p0 + n - 1) * BB + B * r + q];
-      in[q] = Linv[(size_t)(p0 + n - 2) * BB + B * r + q];
-    }
-    vn = Lv[(size_t)(p0 + n - 2) * B + r];
-    cn = L.cv[p0 + n - 2];
-  }
-  for (int i = n - 2; i >= 0; i--) {
-    BT ui[B], ii[B];
+    for (int t = 0; t < LK; t++) {
+      const int i = i0 - t;
+      if (i >= 0) {
 #pragma unroll
-    for (int q = 0; q < B; q++) {
-      ui[q] = un[q];
-      ii[q] = in[q];
-    }
-    const BT vi = vn;
-    const int ci = cn;
-    if (i > 0) {
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        un[q] = Lup[(size_t)(p0 + i) * BB + B * r + q];
-        in[q] = Linv[(size_t)(p0 + i - 1) * BB + B * r + q];
+        for (int q = 0; q < B; q++) {
+          ui[t][q] = Lup[(size_t)(p0 + i + 1) * BB + B * r + q];
+          ii[t][q] = Linv[(size_t)(p0 + i) * BB + B * r + q];
+        }
+        vi[t] = Lv[(size_t)(p0 + i) * B + r];
+        ci[t] = L.cv[p0 + i];
       }
-      vn = Lv[(size_t)(p0 + i - 1) * B + r];
-      cn = L.cv[p0 + i - 1];
     }
-    BT s2 = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s2 += ui[q] * __shfl_sync(0xffffffffu, yv, q);
-    const BT a1 = vi - s2;
-    BT s = 0;
+    for (int t = 0; t < LK; t++) {
+      const int i = i0 - t;
+      if (i >= 0) {
+        BT s2 = 0;
 #pragma unroll
-    for (int q = 0; q < B; q++) s += ii[q] * __shfl_sync(0xffffffffu, a1, q);
-    yv = s;
-    if (row) x[r * N + ci] = yv;
+        for (int q = 0; q < B; q++) s2 += ui[t][q] * __shfl_sync(0xffffffffu, yv, q);
+        const BT a1 = vi[t] - s2;
+        BT s = 0;
+#pragma unroll
+        for (int q = 0; q < B; q++) s += ii[t][q] * __shfl_sync(0xffffffffu, a1, q);
+        yv = s;
+        if (row) x[r * N + ci[t]] = yv;
+      }
+    }
   }
 }
 

@@ -447,42 +447,55 @@ __global__ void __launch_bounds__(B * 32) k_lrelax_rhs(Mesh m, State st, Lines L
   }
 }
 
-// x (cells of a line) = T_line^-1 r, r read from x; one warp per line, lanes < B hold the rows.
-// The chain along a line is serial, but the operands of its steps (a matrix row, the cell id, the
-// right-hand side) do not depend on it: they are loaded LK steps at a time, all loads of a chunk
-// issued together, the next chunk's cell ids a chunk ahead, so one memory latency is spent per LK
-// steps instead of per step.
+// x (cells of a line) = T_line^-1 r, r read from x.  Four lines per warp, eight lanes per line
+// (lanes < B of a group hold the rows of its blocks): the chain along a line is serial, so a
+// warp's lines advance together, each step costing one warp's latency for four lines.  The
+// operands of the steps (a matrix row, the cell id, the right-hand side) do not depend on the
+// chain: they are loaded LK steps at a time, all loads of a chunk issued together, the next
+// chunk's cell ids a chunk ahead, so one memory latency is spent per LK steps.  The shuffles run
+// on every lane; a group past the end of its line only skips the update.
 constexpr int LK = 4;
+constexpr int LG = 8;         // lanes per line
+constexpr int LPW = 32 / LG;  // lines per warp
 
 template <typename BT, int B>
 __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restrict__ x) {
+  static_assert(B <= LG, "a line's rows fit its lane group");
   constexpr int BB = B * B;
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int line = blockIdx.x * LW + w;
-  if (line >= L.nlines) return;
-  const int p0 = L.off[line], n = L.off[line + 1] - p0;
+  const int r = lane % LG;
+  const int line = (blockIdx.x * LW + w) * LPW + lane / LG;
+  const bool has = line < L.nlines;
+  const int p0 = has ? L.off[line] : 0, n = has ? L.off[line + 1] - p0 : 0;
+  const bool row = has && r < B;
+  const int rr = r < B ? r : 0;  // lanes past the rows mirror row 0 and never store
+  int nmax = n;
+  for (int o = LG; o < 32; o *= 2) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+  if (nmax == 0) return;  // the whole warp (no line of its own)
   const size_t N = m.ncv;
-  const int r = lane % B;
-  const bool row = lane < B;
   const BT* Linv = (const BT*)L.binv;
   const BT* Llow = (const BT*)L.blow;
   const BT* Lup = (const BT*)L.bup;
   BT* Lv = (BT*)L.bv;
   // forward: v_0 = r_0, v_i = r_i - low_i v_{i-1}
-  BT v = x[r * N + L.cv[p0]];
+  BT v = has ? x[rr * N + L.cv[p0]] : BT(0);
   if (row) Lv[(size_t)p0 * B + r] = v;
   int cn[LK];  // the cell ids of the next chunk
 #pragma unroll
   for (int t = 0; t < LK; t++) cn[t] = (1 + t < n) ? L.cv[p0 + 1 + t] : 0;
-  for (int i0 = 1; i0 < n; i0 += LK) {
+  for (int i0 = 1; i0 < nmax; i0 += LK) {
     BT mi[LK][B], xi[LK];
 #pragma unroll
     for (int t = 0; t < LK; t++) {
       const int i = i0 + t;
       if (i < n) {
 #pragma unroll
-        for (int q = 0; q < B; q++) mi[t][q] = Llow[(size_t)(p0 + i) * BB + B * r + q];
-        xi[t] = x[r * N + cn[t]];
+        for (int q = 0; q < B; q++) mi[t][q] = Llow[(size_t)(p0 + i) * BB + B * rr + q];
+        xi[t] = x[rr * N + cn[t]];
+      } else {
+#pragma unroll
+        for (int q = 0; q < B; q++) mi[t][q] = BT(0);
+        xi[t] = BT(0);
       }
     }
 #pragma unroll
@@ -490,51 +503,61 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
 #pragma unroll
     for (int t = 0; t < LK; t++) {
       const int i = i0 + t;
-      if (i < n) {
-        BT s = 0;
+      BT s = 0;
 #pragma unroll
-        for (int q = 0; q < B; q++) s += mi[t][q] * __shfl_sync(0xffffffffu, v, q);
+      for (int q = 0; q < B; q++) s += mi[t][q] * __shfl_sync(0xffffffffu, v, q, LG);
+      if (i < n) {
         v = xi[t] - s;
         if (row) Lv[(size_t)(p0 + i) * B + r] = v;
       }
     }
   }
-  // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - up_{i+1} y_{i+1})
+  // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - up_{i+1} y_{i+1}); step j of the
+  // warp is position n-2-j of each line
   BT yv = 0;
   {
-    const BT* I = &Linv[(size_t)(p0 + n - 1) * BB + B * r];
+    BT vq[B];
 #pragma unroll
-    for (int q = 0; q < B; q++) yv += I[q] * __shfl_sync(0xffffffffu, v, q);
+    for (int q = 0; q < B; q++) vq[q] = __shfl_sync(0xffffffffu, v, q, LG);
+    if (has) {
+      const BT* I = &Linv[(size_t)(p0 + n - 1) * BB + B * rr];
+#pragma unroll
+      for (int q = 0; q < B; q++) yv += I[q] * vq[q];
+      if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
+    }
   }
-  if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
-  __syncwarp();  // the forward pass's Lv stores are read back below
-  for (int i0 = n - 2; i0 >= 0; i0 -= LK) {
+  for (int j0 = 0; j0 < nmax - 1; j0 += LK) {
     BT ui[LK][B], ii[LK][B], vi[LK];
     int ci[LK];
 #pragma unroll
     for (int t = 0; t < LK; t++) {
-      const int i = i0 - t;
+      const int i = n - 2 - (j0 + t);
       if (i >= 0) {
 #pragma unroll
         for (int q = 0; q < B; q++) {
-          ui[t][q] = Lup[(size_t)(p0 + i + 1) * BB + B * r + q];
-          ii[t][q] = Linv[(size_t)(p0 + i) * BB + B * r + q];
+          ui[t][q] = Lup[(size_t)(p0 + i + 1) * BB + B * rr + q];
+          ii[t][q] = Linv[(size_t)(p0 + i) * BB + B * rr + q];
         }
-        vi[t] = Lv[(size_t)(p0 + i) * B + r];
+        vi[t] = Lv[(size_t)(p0 + i) * B + rr];
         ci[t] = L.cv[p0 + i];
+      } else {
+#pragma unroll
+        for (int q = 0; q < B; q++) ui[t][q] = ii[t][q] = BT(0);
+        vi[t] = BT(0);
+        ci[t] = 0;
       }
     }
 #pragma unroll
     for (int t = 0; t < LK; t++) {
-      const int i = i0 - t;
+      const int i = n - 2 - (j0 + t);
+      BT s2 = 0;
+#pragma unroll
+      for (int q = 0; q < B; q++) s2 += ui[t][q] * __shfl_sync(0xffffffffu, yv, q, LG);
+      const BT a1 = vi[t] - s2;
+      BT s = 0;
+#pragma unroll
+      for (int q = 0; q < B; q++) s += ii[t][q] * __shfl_sync(0xffffffffu, a1, q, LG);
       if (i >= 0) {
-        BT s2 = 0;
-#pragma unroll
-        for (int q = 0; q < B; q++) s2 += ui[t][q] * __shfl_sync(0xffffffffu, yv, q);
-        const BT a1 = vi[t] - s2;
-        BT s = 0;
-#pragma unroll
-        for (int q = 0; q < B; q++) s += ii[t][q] * __shfl_sync(0xffffffffu, a1, q);
         yv = s;
         if (row) x[r * N + ci[t]] = yv;
       }
@@ -550,7 +573,7 @@ void line_relax(const Mesh& m, State& st, const Lines& L, int sweeps, cudaStream
     BT* xin = (BT*)((it % 2 == 0) ? st.x1 : st.x0);
     BT* xout = (BT*)((it % 2 == 0) ? st.x0 : st.x1);
     k_lrelax_rhs<BT, B><<<m.nslices, B * SLICE, 0, s>>>(m, st, L, xin, xout, it == 0);
-    if (L.nlines) k_lsolve<BT, B><<<lb, 32 * LW, 0, s>>>(m, L, xout);
+    if (L.nlines) k_lsolve<BT, B><<<(L.nlines + LW * LPW - 1) / (LW * LPW), 32 * LW, 0, s>>>(m, L, xout);
   }
 }
 

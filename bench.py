@@ -238,7 +238,8 @@ def hbm_leg(hcase, nsteps=20):
 
 
 CONFIG3_WORKLOAD = ("precision form: SA-RANS channel bump M 0.7, Re 3e6, shuffled mixed prism/hex mesh 512x400x8 "
-                    "(88 prism rows, stretch 1.02; 1,998,848 cells) renumbered by the handle, HLLC + viscous, "
+                    "(88 prism rows, stretch 1.02; 1,998,848 cells) renumbered by the handle (RCM, each LINE line's cells "
+                    "consecutive), HLLC + viscous, "
                     "6x6 coupled blocks, LINE x10, FP64 and mixed")
 
 
@@ -257,7 +258,7 @@ def run_config3(args):
     out = {"metric": "cell-iters/s", "unit": "cell-iters/s", "workload": CONFIG3_WORKLOAD, "cells": g.ncv,
            "steps": args.steps, "l2": "working set above L2 (no flush)"}
     for prec, name in ((0, "fp64"), (1, "mixed")):
-        j = solver.JoeGpu(g, prm, precision=prec, renumber=True)
+        j = solver.JoeGpu(g, prm, precision=prec, renumber=args.config3_renumber)
         j.set_state(*st0)
         j.set_scalars(np.full(g.ncv, prm.NUSA_INITIAL))
         j.runBackwardEuler(max(args.warmup, 3))
@@ -326,6 +327,8 @@ def main():
     ap.add_argument("--jac-lag", type=int, default=4, help="serving arm: flux Jacobian every k-th step")
     ap.add_argument("--no-hbm-leg", dest="hbm_leg", action="store_false",
                     help="skip the 2M-cell HBM-scale leg")
+    ap.add_argument("--config3-renumber", type=int, default=3, choices=[1, 3],
+                    help="config3's cell order: 1 RCM, 3 RCM with each LINE line consecutive (default)")
     ap.add_argument("--workload", default="plate", choices=["plate", "config3"],
                     help="plate: the headline line; config3: the 2M-cell precision-form workload (own line)")
     args = ap.parse_args()

@@ -171,7 +171,14 @@ enum { JG_GRAD_LSQ = 0, JG_GRAD_GREENGAUSS = 1, JG_GRAD_SDWLS = 2 };
 /* JG_RENUMBER_RCM_COLOR: the RCM order grouped by Gauss-Seidel colour, so that each colour
  * pass of the SGS relaxation reads a contiguous part of the matrix; the same colour classes,
  * so SGS gives the same bits as with JG_RENUMBER_RCM. */
-enum { JG_RENUMBER_NONE = 0, JG_RENUMBER_RCM = 1, JG_RENUMBER_RCM_COLOR = 2 };
+/* JG_RENUMBER_RCM_LINES: the RCM order with the cells of each LINE relaxation line made
+ * consecutive, in line order from the wall (each line placed where RCM meets its first cell;
+ * the lines are the handle's own, built from the WALL zones by the relaxed rule of
+ * JG_LS_LINE).  The line factorisation and substitutions then stream each line's blocks, and
+ * the gathers of a cell's off-line neighbours read the next line's consecutive cells.  Per-cell
+ * operations keep their operands and order, so results are those of JG_RENUMBER_RCM; a mesh
+ * without WALL faces gets the RCM order. */
+enum { JG_RENUMBER_NONE = 0, JG_RENUMBER_RCM = 1, JG_RENUMBER_RCM_COLOR = 2, JG_RENUMBER_RCM_LINES = 3 };
 /* turbulence models, with the reference's default constants:
  *   JG_TURB_SA  Spalart-Allmaras (src/joe/turbModels/TurbModel_SA.h): nscal 1, nuSA (1e-10 .. 1)
  *   JG_TURB_SST Menter k-omega SST (TurbModel_KOMSST.h): nscal 2, kine (1e-10 .. 1e10) and
@@ -353,7 +360,8 @@ int jg_case_device_bytes(jg_case_t *h, double *bytes);
 /* The cell order jg_create uses with params.renumber = method:
  * cell_old[ncv] = the caller's id of each cell in the handle's order.  Host
  * only (no device needed).  For JG_RENUMBER_RCM: reverse Cuthill-McKee over
- * the nbocv graph, each connected component from a pseudo-peripheral cell. */
+ * the nbocv graph, each connected component from a pseudo-peripheral cell;
+ * JG_RENUMBER_RCM_COLOR and JG_RENUMBER_RCM_LINES as above. */
 int jg_renumber_cells(const jg_mesh *mesh, int method, int *cell_old);
 
 /* Serving form (no reference counterpart; the reference solves one case per

@@ -113,7 +113,7 @@ def make_params(p: JoeParams, precision: int = 0, renumber: bool = False, jac_la
     q.precision = precision
     q.nscal = p.nscal
     q.turb_model = {"SA": 1, "SST": 2}.get(p.TURB_MODEL, 0)
-    q.renumber = int(renumber)   # False/True: none/RCM; 2: RCM grouped by Gauss-Seidel colour
+    q.renumber = int(renumber)   # False/True: none/RCM; 2: RCM grouped by Gauss-Seidel colour; 3: RCM, LINE lines consecutive
     q.grad_scheme = {"LEASTSQUARES": 0, "GREENGAUSS": 1, "SDWLS": 2}[p.GRAD_SCHEME]
     if q.grad_scheme == 2:
         q.limiter = 0   # SDWLS applies no limiter (limiterNavierS = 0, UgpWithCvCompFlow.h:275-280)

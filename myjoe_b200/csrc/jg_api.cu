@@ -214,18 +214,24 @@ static std::vector<std::vector<int>> wall_zone_faces(const jg_mesh* mesh, const 
   return zs;
 }
 
-// the lines of two or more cells of initializeLinelet
+// the lines of two or more cells of initializeLinelet, longest first: the line kernels give a
+// warp one line (factors) or four (substitutions), and lines of equal length side by side keep
+// the warps of a block, and the lanes of a warp, busy to the same step (each line's elimination
+// is independent of the others, so their order changes no result)
 static void multi_cell_lines(const jg_mesh* mesh, const std::vector<int>& face_old, std::vector<int>& off,
                              std::vector<int>& cv, bool relaxed) {
   std::vector<int> o, c;
   build_lines(*mesh, wall_zone_faces(mesh, face_old), o, c, relaxed);
+  std::vector<int> ls;
+  for (size_t l = 0; l + 1 < o.size(); l++)
+    if (o[l + 1] - o[l] >= 2) ls.push_back((int)l);
+  std::stable_sort(ls.begin(), ls.end(), [&](int a, int b) { return o[a + 1] - o[a] > o[b + 1] - o[b]; });
   off.assign(1, 0);
   cv.clear();
-  for (size_t l = 0; l + 1 < o.size(); l++)
-    if (o[l + 1] - o[l] >= 2) {
-      cv.insert(cv.end(), c.begin() + o[l], c.begin() + o[l + 1]);
-      off.push_back((int)cv.size());
-    }
+  for (int l : ls) {
+    cv.insert(cv.end(), c.begin() + o[l], c.begin() + o[l + 1]);
+    off.push_back((int)cv.size());
+  }
 }
 
 static Params make_params(const jg_params& q) {
@@ -306,7 +312,7 @@ static int check_params(const jg_params* q) {
     return set_err(JG_ERR_ARG, "Green-Gauss and SDWLS gradients: cases without a turbulence model");
   if (q->grad_scheme == JG_GRAD_SDWLS && q->limiter)
     return set_err(JG_ERR_ARG, "SDWLS gradients take no limiter (limiter = 0)");
-  if (q->renumber != JG_RENUMBER_NONE && q->renumber != JG_RENUMBER_RCM && q->renumber != JG_RENUMBER_RCM_COLOR)
+  if (q->renumber < JG_RENUMBER_NONE || q->renumber > JG_RENUMBER_RCM_LINES)
     return set_err(JG_ERR_ARG, "unsupported renumbering %d", q->renumber);
   if (!(q->gamma > 1.0) || !(q->R_gas > 0.0)) return set_err(JG_ERR_ARG, "bad gas constants");
   if (q->jac_lag < 0) return set_err(JG_ERR_ARG, "bad Jacobian lag %d", q->jac_lag);

@@ -310,6 +310,8 @@ struct Renumbering {
 };
 int rcm_order(const jg_mesh& m, std::vector<int>& cell_old);
 int rcm_color_order(const jg_mesh& m, std::vector<int>& cell_old);
+int rcm_lines_order(const jg_mesh& m, std::vector<int>& cell_old);
+int cell_order(const jg_mesh& m, int method, std::vector<int>& cell_old);
 int renumber_mesh(const jg_mesh& in, int method, MeshOwned& out, Renumbering& r);
 }  // namespace jg
 

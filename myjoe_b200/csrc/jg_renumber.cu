@@ -26,6 +26,12 @@
 // pass of multicolour Gauss-Seidel reads a contiguous range of slices of the
 // implicit matrix instead of every slice with only some lanes active; its
 // sweeps are bit-identical to the RCM order's.
+//
+// JG_RENUMBER_RCM_LINES makes the cells of each LINE relaxation line
+// consecutive in the RCM order (a line is placed where RCM meets the first of
+// its cells), so that the line kernels stream each line's blocks and the
+// off-line neighbours of a line's consecutive cells are the next line's
+// consecutive cells.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -175,15 +181,71 @@ int rcm_color_order(const jg_mesh& m, std::vector<int>& cell_old) {
   return JG_OK;
 }
 
+// The RCM order with every line of the LINE relaxation made consecutive: walking the RCM order,
+// the first cell met of a line brings in the whole line, in line order from its wall cell.  The
+// lines are those a handle builds (the relaxed rule from every WALL zone's faces in the caller's
+// order), which depend on the mesh's connectivity and geometry only, not on its cell ids, so a
+// handle finds the same lines in the renumbered mesh.
+int rcm_lines_order(const jg_mesh& m, std::vector<int>& cell_old) {
+  int rc = rcm_order(m, cell_old);
+  if (rc != JG_OK) return rc;
+  const int N = m.ncv;
+  std::vector<std::vector<int>> walls;
+  for (int z = 0; z < m.nzones; z++)
+    if (m.zones[z].kind == JG_BC_WALL) {
+      if (m.zones[z].ifa_f < 0 || m.zones[z].ifa_l >= m.nfa_b)
+        return record_error(JG_ERR_ARG, "zone face range outside the boundary faces");
+      for (int i = m.zones[z].ifa_f; i <= m.zones[z].ifa_l; i++)
+        if (m.cvofa[2 * i] < 0 || m.cvofa[2 * i] >= N) return record_error(JG_ERR_ARG, "a boundary face has a cell id out of range");
+      std::vector<int> f;
+      for (int i = m.zones[z].ifa_f; i <= m.zones[z].ifa_l; i++) f.push_back(i);
+      walls.push_back(std::move(f));
+    }
+  std::vector<int> off, cv;
+  rc = build_lines(m, walls, off, cv, true);
+  if (rc != JG_OK) return rc;
+  std::vector<int> line_of(N, -1);
+  for (size_t l = 0; l + 1 < off.size(); l++)
+    if (off[l + 1] - off[l] >= 2)
+      for (int k = off[l]; k < off[l + 1]; k++) line_of[cv[k]] = (int)l;
+  std::vector<char> placed(N, 0);
+  std::vector<int> out;
+  out.reserve(N);
+  for (int c : cell_old) {
+    if (placed[c]) continue;
+    const int l = line_of[c];
+    if (l < 0) {
+      out.push_back(c);
+      placed[c] = 1;
+      continue;
+    }
+    for (int k = off[l]; k < off[l + 1]; k++) {
+      out.push_back(cv[k]);
+      placed[cv[k]] = 1;
+    }
+  }
+  cell_old.swap(out);
+  return JG_OK;
+}
+
+int cell_order(const jg_mesh& m, int method, std::vector<int>& cell_old) {
+  switch (method) {
+    case JG_RENUMBER_RCM: return rcm_order(m, cell_old);
+    case JG_RENUMBER_RCM_COLOR: return rcm_color_order(m, cell_old);
+    case JG_RENUMBER_RCM_LINES: return rcm_lines_order(m, cell_old);
+    default: return record_error(JG_ERR_ARG, "unknown renumbering method");
+  }
+}
+
 int renumber_mesh(const jg_mesh& in, int method, MeshOwned& o, Renumbering& r) {
   const int N = in.ncv, nfa = in.nfa, nfa_b = in.nfa_b, nbs = in.nbocv_s;
-  if (method != JG_RENUMBER_RCM && method != JG_RENUMBER_RCM_COLOR)
+  if (method != JG_RENUMBER_RCM && method != JG_RENUMBER_RCM_COLOR && method != JG_RENUMBER_RCM_LINES)
     return record_error(JG_ERR_ARG, "unknown renumbering method");
   for (int f = nfa_b; f < nfa; f++) {
     int c0 = in.cvofa[2 * f], c1 = in.cvofa[2 * f + 1];
     if (c0 < 0 || c0 >= N || c1 < 0 || c1 >= N) return record_error(JG_ERR_ARG, "an internal face has a cell id out of range");
   }
-  int rc = method == JG_RENUMBER_RCM ? rcm_order(in, r.cell_old) : rcm_color_order(in, r.cell_old);
+  int rc = cell_order(in, method, r.cell_old);
   if (rc != JG_OK) return rc;
   std::vector<int> cell_new(N);
   for (int c = 0; c < N; c++) cell_new[r.cell_old[c]] = c;
@@ -267,7 +329,7 @@ int renumber_mesh(const jg_mesh& in, int method, MeshOwned& o, Renumbering& r) {
 
 extern "C" int jg_renumber_cells(const jg_mesh* mesh, int method, int* cell_old) {
   if (!mesh || !cell_old) return jg::record_error(JG_ERR_ARG, "null argument");
-  if (method != JG_RENUMBER_RCM && method != JG_RENUMBER_RCM_COLOR)
+  if (method != JG_RENUMBER_RCM && method != JG_RENUMBER_RCM_COLOR && method != JG_RENUMBER_RCM_LINES)
     return jg::record_error(JG_ERR_ARG, "unknown renumbering method");
   if (mesh->ncv <= 0 || mesh->nbocv_s < mesh->ncv) return jg::record_error(JG_ERR_ARG, "inconsistent mesh sizes");
   for (int f = mesh->nfa_b; f < mesh->nfa; f++) {
@@ -276,7 +338,7 @@ extern "C" int jg_renumber_cells(const jg_mesh* mesh, int method, int* cell_old)
       return jg::record_error(JG_ERR_ARG, "an internal face has a cell id out of range");
   }
   std::vector<int> order;
-  int rc = method == JG_RENUMBER_RCM ? jg::rcm_order(*mesh, order) : jg::rcm_color_order(*mesh, order);
+  int rc = jg::cell_order(*mesh, method, order);
   if (rc != JG_OK) return rc;
   std::copy(order.begin(), order.end(), cell_old);
   return JG_OK;

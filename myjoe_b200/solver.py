@@ -23,7 +23,7 @@ _lib = None
 
 FLUX_SPLIT = 32        # JG_FLUX_SPLIT: face-loop shapes split into a residual and a Jacobian kernel
 FLUX_CL1_3BLK = 17     # JG_FLUX_CL1_3BLK
-RENUMBER_RCM, RENUMBER_RCM_COLOR = 1, 2   # jg_params.renumber
+RENUMBER_RCM, RENUMBER_RCM_COLOR, RENUMBER_RCM_LINES = 1, 2, 3   # jg_params.renumber
 JG_ERR = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory", -4: "non-physical state",
           -5: "no CUDA device", -6: "file error"}
 

@@ -172,3 +172,30 @@ def test_color_grouped_order_gives_the_rcm_sgs_bits():
             np.testing.assert_array_equal(x, y)
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("turb", ["NONE", "SA"])
+def test_line_grouped_order_gives_the_rcm_line_relaxation_bits(turb):
+    """JG_RENUMBER_RCM_LINES makes each LINE relaxation line consecutive; the lines and
+    every per-cell operation are those of the RCM handle, so LINE steps (5x5 laminar and
+    6x6 coupled SA, FP64 and mixed) give its states bit for bit."""
+    from myjoe_b200 import case, solver
+    _, g, prm = case.sa_bump_case(48, 40, 2, stretch=1.1, n_prism=8, bump_h=0.05, alternate=True,
+                                  shuffle=True, seed=3)
+    prm = dataclasses.replace(prm, LINEAR_SOLVER_NS="LINE", LS_MAX_ITER=5, CFL=5.0, CFL_RAMP=(5, 5, 1.2, 50.0))
+    if turb == "NONE":
+        prm = dataclasses.replace(prm, TURB_MODEL="NONE", scalar_bcs={})
+    st = case.perturbed_state(g.x_cv, prm, 0.0)
+    for precision in (0, 1):
+        hs = [solver.JoeGpu(g, prm, precision=precision, renumber=m)
+              for m in (solver.RENUMBER_RCM, solver.RENUMBER_RCM_LINES)]
+        for j in hs:
+            j.set_state(*st)
+            if turb == "SA":
+                j.set_scalars(np.full(g.ncv, prm.NUSA_INITIAL))
+        ra, rb = (j.runBackwardEuler(12) for j in hs)
+        np.testing.assert_allclose(rb, ra, rtol=1e-13, atol=0.0)
+        for x, y in zip(hs[0].get_state(), hs[1].get_state()):
+            np.testing.assert_array_equal(x, y)
+        for j in hs:
+            j.close()

@@ -49,3 +49,35 @@ def test_relaxed_lines_extend_the_reference_lines_on_hexahedra():
     for l in range(len(ao) - 1):
         ref, rel = ac[ao[l]:ao[l + 1]], bc[bo[l]:bo[l + 1]]
         assert len(rel) >= len(ref) and np.array_equal(rel[:len(ref)], ref)
+
+
+def test_rcm_lines_order_makes_each_line_consecutive():
+    """JG_RENUMBER_RCM_LINES: the RCM order in which the first cell met of each LINE
+    relaxation line (two or more cells) brings in the whole line, in line order from its
+    wall cell; the lines are those of the relaxed rule on the caller's mesh (the oracle's)."""
+    from myjoe_b200 import solver
+    _, g, prm = case.sa_bump_case(48, 40, 2, stretch=1.1, n_prism=8, bump_h=0.05, alternate=True,
+                                  shuffle=True, seed=3)
+    o = Oracle(g, dataclasses.replace(prm, TURB_MODEL="NONE", scalar_bcs={}))
+    off, cv = o.relax_lines()
+    rcm = solver.renumber_cells(g, prm, solver.RENUMBER_RCM)
+    got = solver.renumber_cells(g, prm, solver.RENUMBER_RCM_LINES)
+    assert np.array_equal(np.sort(got), np.arange(g.ncv))
+    line_of = np.full(g.ncv, -1)
+    for l in range(len(off) - 1):
+        if off[l + 1] - off[l] >= 2:
+            line_of[cv[off[l]:off[l + 1]]] = l
+    want, placed = [], np.zeros(g.ncv, bool)
+    for c in rcm:
+        if placed[c]:
+            continue
+        seg = [c] if line_of[c] < 0 else list(cv[off[line_of[c]]:off[line_of[c] + 1]])
+        want += seg
+        placed[seg] = True
+    np.testing.assert_array_equal(got, np.array(want))
+    pos = np.empty(g.ncv, int)
+    pos[got] = np.arange(g.ncv)
+    for l in range(len(off) - 1):
+        seg = pos[cv[off[l]:off[l + 1]]]
+        assert np.all(np.diff(seg) == 1)
+    assert (line_of >= 0).mean() > 0.6

@@ -987,6 +987,7 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
     // case-local cell order of every case is kept for the per-case state and scalar calls
     std::vector<MeshOwned> mo(ncases);
     std::vector<jg_mesh> rm(ncases);
+    std::vector<std::vector<int>> fold(ncases);
     for (int k = 0; k < ncases && rc == JG_OK; k++) {
       Renumbering r;
       rc = renumber_mesh(meshes[k], params->renumber, mo[k], r);
@@ -994,9 +995,24 @@ int jg_batch_create(int ncases, const jg_mesh* meshes, const jg_params* params, 
         mo[k].bind();
         rm[k] = mo[k].m;
         h->case_cell_old.insert(h->case_cell_old.end(), r.cell_old.begin(), r.cell_old.end());
+        fold[k].swap(r.face_old);
       }
     }
     if (rc == JG_OK) rc = concat_meshes(ncases, rm.data(), cat, h->case_off, h->case_nfa_b_off);
+    if (rc == JG_OK) {
+      // each concatenated face's id in the concatenation of the caller's meshes, so that the WALL
+      // faces are taken in each case's own face order (the order in which lines grow and wall
+      // distances break ties, as the case alone takes them)
+      const int NB = h->case_nfa_b_off[ncases];
+      std::vector<int> int_off(ncases + 1, 0);
+      for (int k = 0; k < ncases; k++) int_off[k + 1] = int_off[k] + (meshes[k].nfa - meshes[k].nfa_b);
+      h->rn.face_old.assign((size_t)cat.m.nfa, 0);
+      for (int k = 0; k < ncases; k++) {
+        const int nb = meshes[k].nfa_b;
+        auto gf = [&](int f) { return f < nb ? h->case_nfa_b_off[k] + f : NB + int_off[k] + (f - nb); };
+        for (int f = 0; f < meshes[k].nfa; f++) h->rn.face_old[gf(f)] = gf(fold[k][f]);
+      }
+    }
     if (rc == JG_OK) rc = build(h, &cat.m, params);
     if (rc == JG_OK) {
       const int* d = nullptr;

@@ -218,3 +218,36 @@ def test_renumbered_turbulence_batch_scalars_in_caller_order():
             np.testing.assert_array_equal(x, y)
         np.testing.assert_array_equal(np.asarray(b.get_case_scalars(k)).reshape(alone[k][1].shape), alone[k][1])
     b.close()
+
+
+def test_line_grouped_batch_is_bitwise_equal_to_alone():
+    """SA cases relaxed by LINE in a batch renumbered case by case with
+    JG_RENUMBER_RCM_LINES (each case's lines from its own walls, consecutive in
+    its own order): per case the state, the scalars and the residual history
+    equal the case alone with the same order and alone with plain RCM."""
+    cs = turb_cases("sa", "LINE")
+    nsteps = 8
+    runs = {}
+    for method in (solver.RENUMBER_RCM, solver.RENUMBER_RCM_LINES):
+        out = []
+        for g, prm in cs:
+            j = solver.JoeGpu(g, prm, precision=1, renumber=method)
+            j.set_state(*case.perturbed_state(g.x_cv, prm, 0.02))
+            j.set_scalars(_phi0(g, prm))
+            r = j.runBackwardEuler(nsteps)
+            out.append((j.get_state(), j.get_scalars(), r))
+            j.close()
+        runs[method] = out
+    b = solver.JoeGpuBatch(cs, precision=1, renumber=solver.RENUMBER_RCM_LINES)
+    for k, (g, prm) in enumerate(cs):
+        b.set_case_state(k, *case.perturbed_state(g.x_cv, prm, 0.02))
+        b.set_case_scalars(k, _phi0(g, prm))
+    rb = b.runBackwardEulerCases(nsteps)
+    for k in range(len(cs)):
+        for ref in (runs[solver.RENUMBER_RCM_LINES][k], runs[solver.RENUMBER_RCM][k]):
+            for x, y in zip(b.get_case_state(k), ref[0]):
+                np.testing.assert_array_equal(x, y)
+            np.testing.assert_array_equal(b.get_case_scalars(k), ref[1])
+        np.testing.assert_array_equal(rb[:, k, :], runs[solver.RENUMBER_RCM_LINES][k][2])
+        np.testing.assert_allclose(rb[:, k, :], runs[solver.RENUMBER_RCM][k][2], rtol=1e-13, atol=0.0)
+    b.close()

@@ -451,9 +451,10 @@ __global__ void __launch_bounds__(B * 32) k_lrelax_rhs(Mesh m, State st, Lines L
 // (lanes < B of a group hold the rows of its blocks): the chain along a line is serial, so a
 // warp's lines advance together, each step costing one warp's latency for four lines.  The
 // operands of the steps (a matrix row, the cell id, the right-hand side) do not depend on the
-// chain: they are loaded LK steps at a time, all loads of a chunk issued together, the next
-// chunk's cell ids a chunk ahead, so one memory latency is spent per LK steps.  The shuffles run
-// on every lane; a group past the end of its line only skips the update.
+// chain: they are loaded LK steps at a time into one of two register sets, the next chunk's
+// loads issued before the current chunk's steps compute (and its cell ids a chunk earlier), so a
+// chunk's memory latency runs under the previous chunk's arithmetic.  The shuffles run on every lane; a group past the end of its
+// line only skips the update.
 constexpr int LK = 4;
 constexpr int LG = 8;         // lanes per line
 constexpr int LPW = 32 / LG;  // lines per warp
@@ -462,6 +463,7 @@ template <typename BT, int B>
 __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restrict__ x) {
   static_assert(B <= LG, "a line's rows fit its lane group");
   constexpr int BB = B * B;
+  constexpr int K = sizeof(BT) * B > 48 ? LK / 2 : LK;  // steps per chunk (FP64 7x7: two register sets fit at LK / 2)
   const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int r = lane % LG;
   const int line = (blockIdx.x * LW + w) * LPW + lane / LG;
@@ -480,13 +482,14 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
   // forward: v_0 = r_0, v_i = r_i - low_i v_{i-1}
   BT v = has ? x[rr * N + L.cv[p0]] : BT(0);
   if (row) Lv[(size_t)p0 * B + r] = v;
-  int cn[LK];  // the cell ids of the next chunk
+  // the operands of steps i0 .. i0 + K - 1 (past the line's end: zeros), called chunk after
+  // chunk; their cell ids were loaded by the call before, and this call loads the next chunk's
+  int cn[K];
 #pragma unroll
-  for (int t = 0; t < LK; t++) cn[t] = (1 + t < n) ? L.cv[p0 + 1 + t] : 0;
-  for (int i0 = 1; i0 < nmax; i0 += LK) {
-    BT mi[LK][B], xi[LK];
+  for (int t = 0; t < K; t++) cn[t] = (1 + t < n) ? L.cv[p0 + 1 + t] : 0;
+  auto load_fwd = [&](int i0, BT(&mi)[K][B], BT(&xi)[K]) {
 #pragma unroll
-    for (int t = 0; t < LK; t++) {
+    for (int t = 0; t < K; t++) {
       const int i = i0 + t;
       if (i < n) {
 #pragma unroll
@@ -499,9 +502,11 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
       }
     }
 #pragma unroll
-    for (int t = 0; t < LK; t++) cn[t] = (i0 + LK + t < n) ? L.cv[p0 + i0 + LK + t] : 0;
+    for (int t = 0; t < K; t++) cn[t] = (i0 + K + t < n) ? L.cv[p0 + i0 + K + t] : 0;
+  };
+  auto step_fwd = [&](int i0, const BT(&mi)[K][B], const BT(&xi)[K]) {
 #pragma unroll
-    for (int t = 0; t < LK; t++) {
+    for (int t = 0; t < K; t++) {
       const int i = i0 + t;
       BT s = 0;
 #pragma unroll
@@ -510,6 +515,17 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
         v = xi[t] - s;
         if (row) Lv[(size_t)(p0 + i) * B + r] = v;
       }
+    }
+  };
+  {
+    BT ma[K][B], xa[K], mb[K][B], xb[K];
+    load_fwd(1, ma, xa);
+    for (int i0 = 1; i0 < nmax; i0 += 2 * K) {
+      if (i0 + K < nmax) load_fwd(i0 + K, mb, xb);
+      step_fwd(i0, ma, xa);
+      if (i0 + K >= nmax) break;
+      if (i0 + 2 * K < nmax) load_fwd(i0 + 2 * K, ma, xa);
+      step_fwd(i0 + K, mb, xb);
     }
   }
   // backward: y_{n-1} = inv_{n-1} v_{n-1}, y_i = inv_i (v_i - up_{i+1} y_{i+1}); step j of the
@@ -526,11 +542,9 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
       if (row) x[r * N + L.cv[p0 + n - 1]] = yv;
     }
   }
-  for (int j0 = 0; j0 < nmax - 1; j0 += LK) {
-    BT ui[LK][B], ii[LK][B], vi[LK];
-    int ci[LK];
+  auto load_bwd = [&](int j0, BT(&ui)[K][B], BT(&ii)[K][B], BT(&vi)[K], int(&ci)[K]) {
 #pragma unroll
-    for (int t = 0; t < LK; t++) {
+    for (int t = 0; t < K; t++) {
       const int i = n - 2 - (j0 + t);
       if (i >= 0) {
 #pragma unroll
@@ -547,8 +561,10 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
         ci[t] = 0;
       }
     }
+  };
+  auto step_bwd = [&](int j0, const BT(&ui)[K][B], const BT(&ii)[K][B], const BT(&vi)[K], const int(&ci)[K]) {
 #pragma unroll
-    for (int t = 0; t < LK; t++) {
+    for (int t = 0; t < K; t++) {
       const int i = n - 2 - (j0 + t);
       BT s2 = 0;
 #pragma unroll
@@ -561,6 +577,18 @@ __global__ void __launch_bounds__(32 * LW) k_lsolve(Mesh m, Lines L, BT* __restr
         yv = s;
         if (row) x[r * N + ci[t]] = yv;
       }
+    }
+  };
+  {
+    BT ua[K][B], ia[K][B], va[K], ub[K][B], ib[K][B], vb[K];
+    int ca[K], cb[K];
+    load_bwd(0, ua, ia, va, ca);
+    for (int j0 = 0; j0 < nmax - 1; j0 += 2 * K) {
+      if (j0 + K < nmax - 1) load_bwd(j0 + K, ub, ib, vb, cb);
+      step_bwd(j0, ua, ia, va, ca);
+      if (j0 + K >= nmax - 1) break;
+      if (j0 + 2 * K < nmax - 1) load_bwd(j0 + 2 * K, ua, ia, va, ca);
+      step_bwd(j0 + K, ub, ib, vb, cb);
     }
   }
 }

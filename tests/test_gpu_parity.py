@@ -145,13 +145,16 @@ def test_linear_solve_reference_solvers(golden):
         assert nrel(dq_g, g["dq"].reshape(-1, 5)) <= 1e-10
 
 
+# the fixtures written with BCGSTAB_LINELET (they carry the reference's lines)
+LINELET = [p for p in GOLDEN if "line_off" in np.load(p, allow_pickle=True).files]
+
+
+@pytest.mark.parametrize("golden", LINELET, indirect=True, ids=[os.path.basename(p)[:-4] for p in LINELET])
 def test_linelet_solve_converged(golden):
     """BCGSTAB_LINELET driven to convergence on the reference's system
     against the oracle, and fewer iterations than the block-diagonal
     preconditioner where the lines are long."""
     g = golden
-    if "line_off" not in g:
-        pytest.skip("not a BCGSTAB_LINELET fixture")
     A = g["A"].copy()
     vol_dt = g["cv_volume"] / g["local_dt"]
     for i in range(5):

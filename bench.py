@@ -295,7 +295,7 @@ def build_converge_cases(args, rank, world):
 
 
 def converge_leg(cases, args):
-    """The north-star comparison on one GPU: the same case list through the plain FP64 drop-in
+    """Converged solves per hour on one GPU: the same case list through the plain FP64 drop-in
     (one case at a time, Jacobian every step) and through the serving form (mixed precision,
     lagged Jacobian, many cases resident)."""
     from myjoe_b200 import serve

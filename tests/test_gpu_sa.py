@@ -13,7 +13,7 @@ precision.
 Tolerances: model arrays and residual components 1e-11 normwise (max error /
 max magnitude of the array; the GPU's pow/tanh may differ from glibc's by an
 ulp); Jacobian 1e-11 normwise per block entry; steps 1e-10 normwise;
-converged fields 1e-8 relative L2, the north-star bar for both precisions.
+converged fields 1e-8 relative L2 in both precisions (FP64 and mixed).
 """
 import dataclasses
 import glob
